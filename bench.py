@@ -1,0 +1,457 @@
+#!/usr/bin/env python
+"""Benchmark of the BVH build-and-query path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Headline workload (the 10M-point configuration): a step is one Morton
+(radix, 63-bit) BVH build, leaf threshold 1, over 10,000,000 uniformly
+distributed points (seeded, U[0,1]^3), inputs already in HBM.  `value` is
+build throughput in Mprims/s summed over ranks (each rank builds its own
+10M-point set: weak scaling, no data-path collective).  The line also
+carries, measured in the same run:
+  * e2e        the same build through the public API from pinned host
+               boxes, the tree copied back to host every step;
+  * roofline   for the dominant kernel (CUDA events on the library's own
+               stream via the libbq phase profiler), against the measured
+               HBM copy bandwidth;
+  * components spatial-median build, 10M closest-point and 10M kNN(k=16)
+               queries, triangle-mesh distance forward+adjoint, the
+               reference's own GPU kernels compiled for sm_100a;
+  * cpu_baseline the reference's host builder (cpuBuilder) on a 1M-point
+               sample, one core.
+Inputs (240 MB of boxes) are larger than the 126 MB L2, so no flush is
+needed between steps.
+
+--impl reference times the reference's CPU build path on this host with
+all cores (concurrent cpuBuilder builds of a 1M-point sample) and prints
+the same metric.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "build Mprims/s + kNN/closest-pt Mqueries/s @10M pts; batched fwd+bwd queries/s"
+N_POINTS = 10_000_000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_POINTS)
+    ap.add_argument("--no-components", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                                          "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(", ") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        mine = [r for r in rows if self.uuid and r[0].strip() in self.uuid] or rows
+        sm = [float(r[1].split()[0]) for r in mine if len(r) > 2 and r[1].split()[0].replace(".", "").isdigit()]
+        mx = [float(r[2].split()[0]) for r in mine if len(r) > 2 and r[2].split()[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in mine:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].strip() == "Active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(mine)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    from cubql_b200 import workloads as W
+    from oracle.oracle import RefCPU, have_ref_cpu, Oracle
+    sample = 1_000_000
+    boxes = W.point_boxes(W.uniform_points(sample))
+    threads = os.cpu_count() or 1
+    if have_ref_cpu():
+        r = RefCPU()
+        kind = "reference"
+        run = lambda: r.build_throughput(boxes, 0, threads, 1)  # noqa: E731
+    else:
+        o = Oracle()
+        kind = "port"
+        threads = 1
+        run = lambda: _timed(lambda: o.cpu_build(boxes, 0))  # noqa: E731
+    for _ in range(args.warmup):
+        run()
+    secs = [run() for _ in range(args.steps)]
+    t = sum(secs) / len(secs)
+    value = threads * sample / t / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mprims/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "Morton-order BVH build of uniform points U[0,1]^3 (reference: host cpuBuilder, "
+                                   "spatial median, leaf 1)", "points": sample, "sample_of": args.n,
+                       "parallelism": f"{threads} concurrent host builds"},
+            "cpu_baseline": {"value": value, "unit": "Mprims/s", "cores": threads, "kind": kind,
+                             "sample": f"{threads} concurrent cpuBuilder builds of {sample} uniform points per step"},
+            "e2e": {"value": value, "unit": "Mprims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def _timed(fn):
+    t0 = time.perf_counter()
+    fn()
+    return time.perf_counter() - t0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+HBM_FALLBACK = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/ncu_summary.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_summary.json")) as f:
+            return json.load(f).get(kernel, {}).get("dram_bytes_per_launch_scaled")
+    except Exception:
+        return None
+
+
+class CBuild:
+    """Direct C-ABI build loop with the library's own stream-ordered
+    allocator (no Python in the way between steps)."""
+
+    def __init__(self, bq, boxes, n):
+        import ctypes
+        self.bq, self.ctypes = bq, ctypes
+        self.boxes, self.n = boxes, n
+        self.cfg = bq.bq_build_config(1 << 15, 0, 0)
+
+    def step(self, stream):
+        c = self.bq.bq_bvh3f()
+        rc = self.bq._lib.bq_build_morton63_f3(self.ctypes.byref(c), self.ctypes.c_void_p(self.boxes.data_ptr()),
+                                               self.n, self.ctypes.byref(self.cfg), None, stream)
+        self.bq._check(rc)
+        self.bq._check(self.bq._lib.bq_free_f3(self.ctypes.byref(c), None, stream))
+
+
+def time_loop(fn, steps, warmup, world):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    return e0.elapsed_time(e1) / steps
+
+
+# algorithmic bytes per element of each libbq phase (Morton build)
+PHASE_BYTES = {
+    "morton.bounds": 24,            # box read
+    "morton.keygen": 24 + 12,       # box read, key + id written
+    "sort.onesweep64": 24,          # per pass: key+id read, key+id written
+    "morton.delta": 8 + 1 + 4,      # keys read, split level + slot written
+    "morton.agglomerate": 4 + 24 + 1 + 64 + 32,  # id, box gather, level, 2N nodes written, siblings read
+}
+
+
+def components(bq, W, torch, pts_np, tp, boxes_t, comp):
+    import numpy as np
+    n = len(pts_np)
+    stream = torch.cuda.current_stream()
+
+    def ev_time(fn, reps=3, warm=1):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    # spatial-median build, leaf 8
+    def smb():
+        bq.gpuBuilder(boxes_t, bq.BuildConfig(makeLeafThreshold=8)).free()
+    ms = ev_time(smb)
+    comp["spatial_median_build"] = {"ms": ms, "Mprims_s": n / ms / 1e3, "leaf": 8,
+                                    "vs_published_reference_13ms": 13.0 / ms}
+    # queries on the Morton tree (leaf 1)
+    bvh = bq.cuda.radixBuilder(boxes_t)
+    qs = torch.from_numpy(W.uniform_points(n, W.SEED_QUERIES)).cuda()
+    ms = ev_time(lambda: bq.points.findClosest(bvh, tp, qs))
+    comp["closest_point"] = {"ms": ms, "Mqueries_s": n / ms / 1e3, "queries": n}
+    ms = ev_time(lambda: bq.points.findKNN(bvh, tp, qs, 16))
+    comp["knn16"] = {"ms": ms, "Mqueries_s": n / ms / 1e3, "queries": n, "k": 16}
+    with bq.profile() as prof:
+        bq.points.findClosest(bvh, tp, qs)
+        bq.points.findKNN(bvh, tp, qs, 16)
+    comp["query_phases_ms"] = {k: round(v[1], 4) for k, v in prof.table.items()}
+    del qs
+    bvh.free()
+    # triangle-mesh distance forward + adjoint (icosphere, 1,310,720 triangles, 4M queries)
+    verts, tris = W.icosphere(8)
+    tv, tt = torch.from_numpy(verts).cuda(), torch.from_numpy(tris).cuda()
+    tq = torch.from_numpy(W.uniform_points(4_000_000, W.SEED_QUERIES, -1.5, 1.5)).cuda()
+    g1 = torch.ones(len(tq), device="cuda")
+
+    def fwd():
+        b = bq.cuda.radixBuilder(bq.triangles.boxes(tt, tv))
+        out = bq.triangles.findClosest(b, tt, tv, tq)
+        b.free()
+        return out
+
+    def fwdbwd():
+        ids, d, _ = fwd()
+        bq.triangles.distanceBackward(tt, tv, tq, ids, g1)
+
+    tb = bq.cuda.radixBuilder(bq.triangles.boxes(tt, tv))
+    ms_f = ev_time(lambda: bq.triangles.findClosest(tb, tt, tv, tq))
+    ids, _, _ = bq.triangles.findClosest(tb, tt, tv, tq)
+    ms_b = ev_time(lambda: bq.triangles.distanceBackward(tt, tv, tq, ids, g1))
+    h = 1e-3
+
+    def fd():  # forward + central differences for the query gradient: 7 forwards
+        bq.triangles.findClosest(tb, tt, tv, tq)
+        for a in range(3):
+            for s in (h, -h):
+                qq = tq.clone()
+                qq[:, a] += s
+                bq.triangles.findClosest(tb, tt, tv, qq)
+    ms_fd = ev_time(fd, reps=2)
+    comp["triangle_distance"] = {"triangles": int(len(tris)), "queries": int(len(tq)), "forward_ms": ms_f,
+                                 "backward_ms": ms_b, "fwd_bwd_queries_s": len(tq) / (ms_f + ms_b) * 1e3,
+                                 "forward_plus_fd_ms": ms_fd, "speedup_vs_forward_plus_fd": ms_fd / (ms_f + ms_b)}
+    tb.free()
+
+
+def reference_gpu(comp, pts_np, W):
+    from oracle.oracle import RefGPU, have_ref_gpu
+    if not have_ref_gpu():
+        comp["reference_gpu"] = {"unavailable": "oracle/_ref/libref_gpu.so not built"}
+        return
+    r = RefGPU()
+    n = len(pts_np)
+    out = {}
+    out["radixBuilder_ms"] = r.time_build(RefGPU.RADIX, pts_np, 0, reps=3)
+    out["gpuBuilder_leaf8_ms"] = r.time_build(RefGPU.SPATIAL_MEDIAN, pts_np, 8, reps=3)
+    out["gpuBuilder_leaf1_ms"] = r.time_build(RefGPU.SPATIAL_MEDIAN, pts_np, 0, reps=3)
+    qs = W.uniform_points(n, W.SEED_QUERIES)
+    out["findClosest_ms"] = r.time_query(RefGPU.RADIX, pts_np, qs, 0, reps=2)
+    out["findKNN16_ms"] = r.time_query(RefGPU.RADIX, pts_np, qs, 16, reps=2)
+    out["note"] = "reference kernels compiled for sm_100a, same points, one thread per query <<<ceil(Q/128),128>>>"
+    comp["reference_gpu"] = out
+
+
+def run_ours(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    import cubql_b200 as bq
+    from cubql_b200 import workloads as W
+
+    n = args.n
+    pts_np = W.uniform_points(n, W.SEED_DATA + rank)
+    boxes_np = W.point_boxes(pts_np)
+    tp = torch.from_numpy(pts_np).cuda()
+    boxes_t = torch.from_numpy(boxes_np).cuda()
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    cb = CBuild(bq, boxes_t, n)
+
+    props = torch.cuda.get_device_properties(local)
+    uuid = str(getattr(props, "uuid", ""))
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    ms = time_loop(lambda: cb.step(sptr), args.steps, args.warmup, world)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms, world)
+    value = world * n / ms_max / 1e3  # Mprims/s
+
+    # per-phase breakdown of the same step (library events on its stream)
+    with bq.profile() as prof:
+        for _ in range(max(3, min(args.steps, 10))):
+            cb.step(sptr)
+    steps_prof = max(3, min(args.steps, 10))
+    table = prof.table
+    launches_per_step = sum(v[0] for v in table.values()) / steps_prof
+    peak, peak_kind = hbm_peak()
+    kernels = {}
+    for name, (launches, tms) in table.items():
+        per = tms / launches
+        bytes_per = PHASE_BYTES.get(name, 0) * n
+        kernels[name] = {"launches_per_step": launches / steps_prof, "ms_per_launch": per,
+                         "share": tms / sum(v[1] for v in table.values()),
+                         "alg_bytes_per_launch": bytes_per,
+                         "GB_s": bytes_per / per / 1e6 if bytes_per else None,
+                         "frac_of_measured_hbm": (bytes_per / per / 1e6 / peak) if bytes_per else None}
+    dom = max(table.items(), key=lambda kv: kv[1][1])[0]
+    dk = kernels[dom]
+    build_bytes = 288 * n + 64 * 2 * n  # the fixed accounting model: 288 N + 64 M, M = 2N
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": dk["GB_s"], "peak": peak, "unit": "GB/s",
+                "frac": dk["frac_of_measured_hbm"], "traffic": ncu_traffic(dom), "peak_source": peak_kind,
+                "whole_build": {"alg_bytes": build_bytes, "GB_s": build_bytes / ms / 1e6,
+                                "frac": build_bytes / ms / 1e6 / peak}}
+
+    # end to end through the public API: pinned host boxes -> tree on host
+    host_boxes = torch.from_numpy(boxes_np).pin_memory()
+    dev_boxes = torch.empty_like(boxes_t)
+    host_nodes = torch.empty((2 * n, 8), dtype=torch.float32).pin_memory()
+    host_prims = torch.empty(n, dtype=torch.int32).pin_memory()
+
+    def e2e_step():
+        dev_boxes.copy_(host_boxes, non_blocking=True)
+        b = bq.cuda.radixBuilder(dev_boxes)
+        host_nodes[: b.numNodes].copy_(b.nodes_tensor(), non_blocking=True)
+        host_prims[: b.numPrims].copy_(b.primids_tensor(), non_blocking=True)
+        b.free()
+    e2e_ms = max_over_ranks(time_loop(e2e_step, max(3, args.steps // 2), 2, world), world)
+    e2e = {"value": world * n / e2e_ms / 1e3, "unit": "Mprims/s", "h2d_bytes_per_step": 24 * n,
+           "d2h_bytes_per_step": 32 * 2 * n + 4 * n, "ms_per_step": e2e_ms,
+           "path": "cubql_b200.cuda.radixBuilder (C ABI bq_build_morton63_f3), pinned host buffers"}
+    del host_nodes, host_prims, host_boxes, dev_boxes
+
+    comp = {}
+    cpu_baseline = None
+    if rank == 0 and not args.no_components:
+        components(bq, W, torch, pts_np, tp, boxes_t, comp)
+        reference_gpu(comp, pts_np, W)
+    if rank == 0:
+        cpu_baseline = cpu_leg(W, pts_np)
+    barrier(world)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Mprims/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "Morton (radix, 63-bit) BVH build over uniform points U[0,1]^3, leaf 1",
+                           "points_per_gpu": n, "seed": W.SEED_DATA, "parallelism": f"{world} independent builds",
+                           "l2": "inputs (240 MB boxes per GPU) larger than the 126 MB L2; no flush"},
+                "e2e": e2e, "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu_baseline,
+                "gpu_launches": int(round(launches_per_step * args.steps)), "clocks": clk, "components": comp}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_leg(W, pts_np):
+    from oracle.oracle import Oracle, RefCPU, have_ref_cpu
+    sample = 1_000_000
+    boxes = W.point_boxes(pts_np[:sample])
+    if have_ref_cpu():
+        r = RefCPU()
+        kind = "reference"
+        fn = lambda: r.build(boxes, 0)  # noqa: E731
+    else:
+        o = Oracle()
+        kind = "port"
+        fn = lambda: o.cpu_build(boxes, 0)  # noqa: E731
+    fn()
+    secs = [_timed(fn) for _ in range(3)]
+    t = statistics.median(secs)
+    return {"value": sample / t / 1e6, "unit": "Mprims/s", "cores": 1, "kind": kind,
+            "sample": f"cpuBuilder (spatial median, leaf 1) over the first {sample} of the benchmark's points, "
+                      f"median of 3 builds, {t:.3f} s each"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,396 @@
+"""cubql_b200 -- B200-native BVH build-and-query (host side).
+
+Python mirror of the cuBQL entry points for the BinaryBVH<float,3> path,
+calling the CUDA library libbq.so through its C ABI (include/bq.h):
+
+    cuBQL::gpuBuilder            -> gpuBuilder(boxes, BuildConfig)
+    cuBQL::cuda::radixBuilder    -> cuda.radixBuilder(boxes, BuildConfig)
+    cuBQL::cuda::free            -> cuda.free(bvh)
+    gpuBuilder_impl::refit       -> refit(bvh, boxes)
+    points::findClosest          -> points.findClosest(bvh, points, queries)
+    points::findKNN              -> points.findKNN(bvh, points, queries, k)
+    triangles::findClosest       -> triangles.findClosest(bvh, tris, verts, queries)
+    (no reference counterpart)   -> triangles.distanceBackward(...)
+
+Device memory, streams and tensors come from PyTorch; the work is done by
+the sm_100a kernels of libbq.so.  There is no CPU fallback: importing
+this package fails if libbq.so is missing.
+"""
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbq.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: build it with `python cubql_b200/build.py` "
+                      "(there is no fallback implementation)")
+_lib = ctypes.CDLL(LIB_PATH)
+
+# ---------------------------------------------------------------------------
+# constants (include/bq.h)
+# ---------------------------------------------------------------------------
+BQ_OK = 0
+BQ_ERR_INVALID_ARGUMENT = 1
+BQ_ERR_CUDA = 2
+BQ_ERR_ALLOC = 3
+BQ_ERR_STACK_OVERFLOW = 4
+BQ_ERR_TIMEOUT = 5
+BQ_ERR_UNSUPPORTED = 6
+TIES_LOWEST_ID = 0
+TIES_REFERENCE = 1
+
+
+class BQError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libbq error {code}: {msg}")
+        self.code = code
+
+
+class bq_bvh3f(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_void_p), ("numNodes", ctypes.c_uint32),
+                ("primIDs", ctypes.c_void_p), ("numPrims", ctypes.c_uint32)]
+
+
+class bq_build_config(ctypes.Structure):
+    _fields_ = [("maxAllowedLeafSize", ctypes.c_int), ("makeLeafThreshold", ctypes.c_int),
+                ("buildMethod", ctypes.c_int)]
+
+
+MALLOC_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t,
+                             ctypes.c_void_p)
+FREE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
+
+
+class bq_allocator(ctypes.Structure):
+    _fields_ = [("ctx", ctypes.c_void_p), ("malloc", MALLOC_FN), ("free", FREE_FN)]
+
+
+class bq_query_config(ctypes.Structure):
+    _fields_ = [("tieMode", ctypes.c_int), ("stackDepth", ctypes.c_int), ("blockSize", ctypes.c_int),
+                ("reorder", ctypes.c_int), ("queriesPerWarp", ctypes.c_int)]
+
+
+_P = ctypes.c_void_p
+_U = ctypes.c_uint32
+_I = ctypes.c_int
+_F = ctypes.c_float
+_SIGS = {
+    "bq_build_morton63_f3": [ctypes.POINTER(bq_bvh3f), _P, _U, ctypes.POINTER(bq_build_config),
+                             ctypes.POINTER(bq_allocator), _P],
+    "bq_build_spatial_median_f3": [ctypes.POINTER(bq_bvh3f), _P, _U, ctypes.POINTER(bq_build_config),
+                                   ctypes.POINTER(bq_allocator), _P],
+    "bq_refit_f3": [ctypes.POINTER(bq_bvh3f), _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_free_f3": [ctypes.POINTER(bq_bvh3f), ctypes.POINTER(bq_allocator), _P],
+    "bq_closest_point_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _F, ctypes.POINTER(bq_query_config), _P, _P,
+                            ctypes.POINTER(bq_allocator), _P],
+    "bq_knn_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _I, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
+                  ctypes.POINTER(bq_allocator), _P],
+    "bq_tri_closest_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _P, _U, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
+                          ctypes.POINTER(bq_allocator), _P],
+    "bq_tri_distance_bwd_f3": [_P, _P, _U, _P, _U, _P, _P, _P, _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_tri_boxes_f3": [_P, _P, _U, _P, _P],
+    "bq_points_to_boxes_f3": [_P, _U, _P, _P],
+    "bq_last_error_string": [],
+    "bq_version": [],
+    "bq_profile_enable": [_I],
+    "bq_profile_reset": [],
+    "bq_profile_count": [],
+    "bq_profile_entry": [_I, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_uint64),
+                         ctypes.POINTER(ctypes.c_double)],
+}
+for _name, _args in _SIGS.items():
+    _fn = getattr(_lib, _name)
+    _fn.argtypes = _args
+    _fn.restype = ctypes.c_char_p if _name == "bq_last_error_string" else ctypes.c_int
+
+
+def exported_symbols():
+    """Names of the C entry points this package binds."""
+    return list(_SIGS)
+
+
+def _check(code):
+    if code != BQ_OK:
+        raise BQError(code, _lib.bq_last_error_string().decode())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+# ---------------------------------------------------------------------------
+# torch-backed allocator: every buffer libbq allocates is a torch tensor
+# ---------------------------------------------------------------------------
+class TorchAllocator:
+    """bq_allocator whose blocks come from PyTorch's caching allocator.
+
+    Blocks are uint8 CUDA tensors kept alive in `live` until libbq frees
+    them; `view(ptr)` returns the tensor behind a pointer libbq handed out.
+    Replaces cuBQL::GpuMemoryResource (cuBQL/builder/cuda.h:31-78)."""
+
+    def __init__(self, device=None):
+        self.device = torch.device(device or "cuda")
+        self.live = {}
+        self._m = MALLOC_FN(self._malloc)
+        self._f = FREE_FN(self._free)
+        self.c = bq_allocator(None, self._m, self._f)
+
+    def _malloc(self, ctx, out, size, stream):
+        try:
+            t = torch.empty(max(int(size), 1), dtype=torch.uint8, device=self.device)
+        except Exception:  # out of memory: report through the status code
+            return 1
+        self.live[t.data_ptr()] = t
+        out[0] = t.data_ptr()
+        return 0
+
+    def _free(self, ctx, ptr, stream):
+        self.live.pop(ptr, None)
+        return 0
+
+    def view(self, ptr, dtype, count):
+        base = self.live[ptr]
+        return base[: count * torch.empty((), dtype=dtype).element_size()].view(dtype)
+
+
+_default_alloc = {}
+
+
+def default_allocator():
+    dev = torch.cuda.current_device()
+    if dev not in _default_alloc:
+        _default_alloc[dev] = TorchAllocator(torch.device("cuda", dev))
+    return _default_alloc[dev]
+
+
+# ---------------------------------------------------------------------------
+# BVH container (cuBQL/bvh.h:71-111)
+# ---------------------------------------------------------------------------
+class BuildConfig:
+    """cuBQL::BuildConfig (cuBQL/bvh.h:31-64)."""
+    SPATIAL_MEDIAN = 0
+
+    def __init__(self, makeLeafThreshold=0, maxAllowedLeafSize=1 << 15, buildMethod=0):
+        self.makeLeafThreshold = makeLeafThreshold
+        self.maxAllowedLeafSize = maxAllowedLeafSize
+        self.buildMethod = buildMethod
+
+    def c(self):
+        return bq_build_config(self.maxAllowedLeafSize, self.makeLeafThreshold, self.buildMethod)
+
+
+NODE_DTYPE = None  # numpy structured dtype, set lazily
+
+
+def node_dtype():
+    import numpy as np
+    global NODE_DTYPE
+    if NODE_DTYPE is None:
+        NODE_DTYPE = np.dtype([("lower", "<f4", 3), ("upper", "<f4", 3), ("admin", "<u8")])
+        assert NODE_DTYPE.itemsize == 32
+    return NODE_DTYPE
+
+
+class BinaryBVH:
+    """BinaryBVH<float,3>: nodes (32 B each) and primIDs in device memory."""
+
+    def __init__(self, c, allocator):
+        self.c = c
+        self.allocator = allocator
+
+    @property
+    def numNodes(self):
+        return self.c.numNodes
+
+    @property
+    def numPrims(self):
+        return self.c.numPrims
+
+    def nodes_tensor(self):
+        """(numNodes, 8) float32 view: lower xyz, upper xyz, admin as 2 words."""
+        if self.c.numNodes == 0:
+            return torch.empty((0, 8), dtype=torch.float32, device="cuda")
+        return self.allocator.view(self.c.nodes, torch.float32, 8 * self.c.numNodes).view(-1, 8)
+
+    def primids_tensor(self):
+        if self.c.numPrims == 0:
+            return torch.empty((0,), dtype=torch.int32, device="cuda")
+        return self.allocator.view(self.c.primIDs, torch.int32, self.c.numPrims)
+
+    def to_host(self):
+        """(nodes as a numpy structured array, primIDs as uint32)."""
+        import numpy as np
+        torch.cuda.synchronize()
+        if self.c.numNodes == 0:
+            return np.zeros(0, dtype=node_dtype()), np.zeros(0, dtype=np.uint32)
+        nodes = self.nodes_tensor().cpu().numpy().view(node_dtype()).reshape(-1)
+        prims = self.primids_tensor().cpu().numpy().view(np.uint32)
+        return nodes, prims
+
+    def free(self):
+        if self.c.nodes or self.c.primIDs:
+            _check(_lib.bq_free_f3(ctypes.byref(self.c), ctypes.byref(self.allocator.c), _stream()))
+
+
+def _as_boxes(boxes):
+    if boxes.dtype != torch.float32 or not boxes.is_cuda:
+        raise TypeError("boxes must be a float32 CUDA tensor of shape (N, 6)")
+    return boxes.contiguous().view(-1, 6)
+
+
+def _build(fn, boxes, config, allocator):
+    boxes = _as_boxes(boxes)
+    allocator = allocator or default_allocator()
+    cfg = (config or BuildConfig()).c()
+    c = bq_bvh3f()
+    _check(fn(ctypes.byref(c), _ptr(boxes), boxes.shape[0], ctypes.byref(cfg), ctypes.byref(allocator.c), _stream()))
+    bvh = BinaryBVH(c, allocator)
+    bvh._boxes = boxes  # keep the input alive for refits
+    return bvh
+
+
+def gpuBuilder(boxes, config=None, allocator=None):
+    """cuBQL::gpuBuilder (cuBQL/builder/cuda.h:91-99): spatial-median build."""
+    return _build(_lib.bq_build_spatial_median_f3, boxes, config, allocator)
+
+
+def refit(bvh, boxes):
+    """gpuBuilder_impl::refit (cuBQL/builder/cuda/sm_builder.h:677-693)."""
+    boxes = _as_boxes(boxes)
+    _check(_lib.bq_refit_f3(ctypes.byref(bvh.c), _ptr(boxes), ctypes.byref(bvh.allocator.c), _stream()))
+
+
+class cuda:
+    """cuBQL::cuda:: entry points."""
+
+    @staticmethod
+    def radixBuilder(boxes, config=None, allocator=None):
+        """cuBQL::cuda::radixBuilder (cuBQL/builder/cuda.h:134-140), 63-bit keys."""
+        return _build(_lib.bq_build_morton63_f3, boxes, config, allocator)
+
+    @staticmethod
+    def free(bvh):
+        """cuBQL::cuda::free (cuBQL/builder/cuda.h:158-161)."""
+        bvh.free()
+
+
+def query_config(tieMode=TIES_LOWEST_ID, stackDepth=64, blockSize=128, reorder=1, queriesPerWarp=32):
+    return bq_query_config(tieMode, stackDepth, blockSize, reorder, queriesPerWarp)
+
+
+def _vec3(t, name):
+    if t.dtype != torch.float32 or not t.is_cuda:
+        raise TypeError(f"{name} must be a float32 CUDA tensor of shape (N, 3)")
+    return t.contiguous().view(-1, 3)
+
+
+class points:
+    @staticmethod
+    def findClosest(bvh, data, queries, maxSqrDist=float("inf"), qcfg=None):
+        """points::findClosest (cuBQL/queries/points/findClosest.h:336-360), batched.
+        Returns (ids int32, sqrDist float32); -1 / inf where nothing is closer
+        than maxSqrDist."""
+        data, queries = _vec3(data, "points"), _vec3(queries, "queries")
+        nq = queries.shape[0]
+        ids = torch.empty(nq, dtype=torch.int32, device=queries.device)
+        d = torch.empty(nq, dtype=torch.float32, device=queries.device)
+        q = qcfg or query_config()
+        _check(_lib.bq_closest_point_f3(ctypes.byref(bvh.c), _ptr(data), _ptr(queries), nq, maxSqrDist,
+                                        ctypes.byref(q), _ptr(ids), _ptr(d), ctypes.byref(bvh.allocator.c),
+                                        _stream()))
+        return ids, d
+
+    @staticmethod
+    def findKNN(bvh, data, queries, k, maxSqrDist=float("inf"), qcfg=None):
+        """points::findKNN (cuBQL/queries/points/knn.h:75-116), batched.
+        Returns (ids (nq,k) int32, sqrDist (nq,k) float32, numFound (nq,) int32)."""
+        data, queries = _vec3(data, "points"), _vec3(queries, "queries")
+        nq = queries.shape[0]
+        ids = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
+        d = torch.empty((nq, k), dtype=torch.float32, device=queries.device)
+        nf = torch.empty(nq, dtype=torch.int32, device=queries.device)
+        q = qcfg or query_config()
+        _check(_lib.bq_knn_f3(ctypes.byref(bvh.c), _ptr(data), _ptr(queries), nq, k, maxSqrDist, ctypes.byref(q),
+                              _ptr(ids), _ptr(d), _ptr(nf), ctypes.byref(bvh.allocator.c), _stream()))
+        return ids, d, nf
+
+
+class triangles:
+    @staticmethod
+    def boxes(tris, verts):
+        """Triangle::bounds() for every triangle (cuBQL/queries/triangles/Triangle.h:40-41)."""
+        nt = tris.shape[0]
+        out = torch.empty((nt, 6), dtype=torch.float32, device=verts.device)
+        _check(_lib.bq_tri_boxes_f3(_ptr(tris.contiguous()), _ptr(verts.contiguous()), nt, _ptr(out), _stream()))
+        return out
+
+    @staticmethod
+    def findClosest(bvh, tris, verts, queries, maxSqrDist=float("inf"), qcfg=None):
+        """triangles::findClosest (cuBQL/queries/triangles/findClosest.h:132-152), batched.
+        Returns (ids, sqrDist, P)."""
+        queries = _vec3(queries, "queries")
+        nq = queries.shape[0]
+        ids = torch.empty(nq, dtype=torch.int32, device=queries.device)
+        d = torch.empty(nq, dtype=torch.float32, device=queries.device)
+        P = torch.empty((nq, 3), dtype=torch.float32, device=queries.device)
+        q = qcfg or query_config()
+        _check(_lib.bq_tri_closest_f3(ctypes.byref(bvh.c), _ptr(tris.contiguous()), _ptr(verts.contiguous()),
+                                      _ptr(queries), nq, maxSqrDist, ctypes.byref(q), _ptr(ids), _ptr(d), _ptr(P),
+                                      ctypes.byref(bvh.allocator.c), _stream()))
+        return ids, d, P
+
+    @staticmethod
+    def distanceBackward(tris, verts, queries, ids, gradSqr, allocator=None):
+        """Adjoint of findClosest's squared distance (no reference counterpart).
+        Returns (gradQueries (nq,3), gradVerts (nv,3))."""
+        allocator = allocator or default_allocator()
+        nq = queries.shape[0]
+        nv = verts.shape[0]
+        gq = torch.empty((nq, 3), dtype=torch.float32, device=queries.device)
+        gv = torch.empty((nv, 3), dtype=torch.float32, device=queries.device)
+        _check(_lib.bq_tri_distance_bwd_f3(_ptr(tris.contiguous()), _ptr(verts.contiguous()), nv,
+                                           _ptr(queries.contiguous()), nq, _ptr(ids.contiguous()),
+                                           _ptr(gradSqr.contiguous()), _ptr(gq), _ptr(gv), ctypes.byref(allocator.c),
+                                           _stream()))
+        return gq, gv
+
+
+def points_to_boxes(pts):
+    """box3f().including(p) per point (testing/points/closestPoint.cu:22-29)."""
+    pts = _vec3(pts, "points")
+    out = torch.empty((pts.shape[0], 6), dtype=torch.float32, device=pts.device)
+    _check(_lib.bq_points_to_boxes_f3(_ptr(pts), pts.shape[0], _ptr(out), _stream()))
+    return out
+
+
+def version():
+    return _lib.bq_version()
+
+
+class profile:
+    """Phase profiler (CUDA events around every kernel phase of libbq calls
+    made by this thread).  Usage:  with profile() as prof: ...;  prof.table
+    maps phase name -> (launches, milliseconds)."""
+
+    def __enter__(self):
+        _check(_lib.bq_profile_reset())
+        _check(_lib.bq_profile_enable(1))
+        self.table = {}
+        return self
+
+    def __exit__(self, *exc):
+        torch.cuda.synchronize()
+        _check(_lib.bq_profile_enable(0))
+        for i in range(_lib.bq_profile_count()):
+            name, launches, ms = ctypes.c_char_p(), ctypes.c_uint64(), ctypes.c_double()
+            _check(_lib.bq_profile_entry(i, ctypes.byref(name), ctypes.byref(launches), ctypes.byref(ms)))
+            self.table[name.value.decode()] = (launches.value, ms.value)
+        _check(_lib.bq_profile_reset())
+        return False

@@ -1,0 +1,173 @@
+// bq_capi.cu -- the extern "C" entry points declared in include/bq.h:
+// argument checks, stream/allocator plumbing, dispatch to the kernels.
+#include <mutex>
+
+#include "bq_internal.cuh"
+
+namespace bq {
+int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
+int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
+int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al);
+int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
+                  const bq_query_config *qcfg, int32_t *ids, float *d, Alloc &al);
+int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, int k, float maxSqr,
+        const bq_query_config *qcfg, int32_t *ids, float *d, int32_t *numFound, Alloc &al);
+int tri_closest(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, const float *queries, uint32_t nq,
+                float maxSqr, const bq_query_config *qcfg, int32_t *ids, float *d, float *P, Alloc &al);
+int tri_distance_bwd(const int32_t *tris, const float *verts, uint32_t numVerts, const float *queries, uint32_t nq,
+                     const int32_t *ids, const float *gradSqr, float *gradQ, float *gradV, Alloc &al);
+int tri_boxes(const int32_t *tris, const float *verts, uint32_t nt, bq_box3f *boxes, cudaStream_t s);
+int points_to_boxes(const float *points, uint32_t n, bq_box3f *boxes, cudaStream_t s);
+
+namespace {
+// Like the reference's AsyncGpuMemoryResource (cuBQL/builder/cuda.h:52-72):
+// keep freed stream-ordered memory in the device's default pool instead
+// of returning it to the driver at every synchronisation.
+void keep_pool_memory()
+{
+  static std::mutex m;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> g(m);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done[dev] = true;
+}
+
+Alloc make_alloc(const bq_allocator *a, bq_stream_t s)
+{
+  if (!a || !a->malloc) keep_pool_memory();
+  Alloc al;
+  al.a = (a && a->malloc && a->free) ? a : nullptr;
+  al.s = (cudaStream_t)s;
+  return al;
+}
+
+bool misaligned(const void *p, size_t a) { return ((uintptr_t)p) % a != 0; }
+
+int check_tree(const bq_bvh3f *bvh)
+{
+  if (!bvh) return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh is NULL");
+  if (bvh->numNodes && (!bvh->nodes || !bvh->primIDs))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh has nodes but NULL arrays");
+  if (bvh->numNodes && misaligned(bvh->nodes, 16))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh->nodes must be 16-byte aligned");
+  return BQ_OK;
+}
+
+int check_build(const bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n)
+{
+  if (!bvh) return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh is NULL");
+  if (n && !boxes) return set_error(BQ_ERR_INVALID_ARGUMENT, "boxes is NULL");
+  if (n && misaligned(boxes, 8)) return set_error(BQ_ERR_INVALID_ARGUMENT, "boxes must be 8-byte aligned");
+  if (n >= (1u << 30)) return set_error(BQ_ERR_INVALID_ARGUMENT, "at most 2^30-1 primitives per build");
+  return BQ_OK;
+}
+} // namespace
+} // namespace bq
+
+using namespace bq;
+
+extern "C" {
+
+int bq_build_morton63_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
+                         const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_build(bvh, boxes, numPrims));
+  Alloc al = make_alloc(alloc, stream);
+  return build_morton63(bvh, boxes, numPrims, cfg, al);
+}
+
+int bq_build_spatial_median_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
+                               const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_build(bvh, boxes, numPrims));
+  if (cfg && cfg->buildMethod != BQ_SPATIAL_MEDIAN)
+    return set_error(BQ_ERR_UNSUPPORTED, "only the spatial-median method is implemented for this entry point");
+  Alloc al = make_alloc(alloc, stream);
+  return build_spatial_median(bvh, boxes, numPrims, cfg, al);
+}
+
+int bq_refit_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (bvh->numNodes && !boxes) return set_error(BQ_ERR_INVALID_ARGUMENT, "boxes is NULL");
+  Alloc al = make_alloc(alloc, stream);
+  return refit(bvh, boxes, al);
+}
+
+int bq_free_f3(bq_bvh3f *bvh, const bq_allocator *alloc, bq_stream_t stream)
+{
+  if (!bvh) return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh is NULL");
+  Alloc al = make_alloc(alloc, stream);
+  int s1 = al.free_bytes(bvh->primIDs);
+  int s2 = al.free_bytes(bvh->nodes);
+  bvh->primIDs = nullptr;
+  bvh->nodes = nullptr;
+  bvh->numNodes = 0;
+  bvh->numPrims = 0;
+  return s1 != BQ_OK ? s1 : s2;
+}
+
+int bq_closest_point_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries,
+                        float maxSqrDist, const bq_query_config *qcfg, int32_t *ids, float *sqrDist,
+                        const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (numQueries && (!queries || !ids || !sqrDist || (bvh->numNodes && !points)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return closest_point(bvh, points, queries, numQueries, maxSqrDist, qcfg, ids, sqrDist, al);
+}
+
+int bq_knn_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries, int k,
+              float maxSqrDist, const bq_query_config *qcfg, int32_t *ids, float *sqrDist, int32_t *numFound,
+              const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (numQueries && (!queries || !ids || !sqrDist || (bvh->numNodes && !points)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return knn(bvh, points, queries, numQueries, k, maxSqrDist, qcfg, ids, sqrDist, numFound, al);
+}
+
+int bq_tri_closest_f3(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, const float *queries,
+                      uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg, int32_t *ids,
+                      float *sqrDist, float *P, const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (numQueries && (!queries || !ids || !sqrDist || (bvh->numNodes && (!tris || !verts))))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return tri_closest(bvh, tris, verts, queries, numQueries, maxSqrDist, qcfg, ids, sqrDist, P, al);
+}
+
+int bq_tri_distance_bwd_f3(const int32_t *tris, const float *verts, uint32_t numVerts, const float *queries,
+                           uint32_t numQueries, const int32_t *ids, const float *gradSqr, float *gradQueries,
+                           float *gradVerts, const bq_allocator *alloc, bq_stream_t stream)
+{
+  if (numQueries && (!tris || !verts || !queries || !ids || !gradSqr || !gradQueries))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  if (numVerts && !gradVerts) return set_error(BQ_ERR_INVALID_ARGUMENT, "gradVerts is NULL");
+  Alloc al = make_alloc(alloc, stream);
+  return tri_distance_bwd(tris, verts, numVerts, queries, numQueries, ids, gradSqr, gradQueries, gradVerts, al);
+}
+
+int bq_tri_boxes_f3(const int32_t *tris, const float *verts, uint32_t numTris, bq_box3f *boxes, bq_stream_t stream)
+{
+  if (numTris && (!tris || !verts || !boxes)) return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  return tri_boxes(tris, verts, numTris, boxes, (cudaStream_t)stream);
+}
+
+int bq_points_to_boxes_f3(const float *points, uint32_t numPoints, bq_box3f *boxes, bq_stream_t stream)
+{
+  if (numPoints && (!points || !boxes)) return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  return points_to_boxes(points, numPoints, boxes, (cudaStream_t)stream);
+}
+
+} // extern "C"

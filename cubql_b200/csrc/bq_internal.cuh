@@ -1,0 +1,265 @@
+// bq_internal.cuh -- shared device/host helpers of libbq (sm_100a only).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/bq.h"
+
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ < 1000)
+#error "libbq is written for sm_100a (B200) only"
+#endif
+
+namespace bq {
+
+// ------------------------------------------------------------------
+// errors: every entry point returns a status and records a message
+// ------------------------------------------------------------------
+int set_error(int code, const std::string &msg);
+int cuda_error(cudaError_t e, const char *what);
+
+#define BQ_CUDA(x)                                  \
+  do {                                              \
+    cudaError_t e_ = (x);                           \
+    if (e_ != cudaSuccess) return ::bq::cuda_error(e_, #x); \
+  } while (0)
+
+#define BQ_TRY(x)                 \
+  do {                            \
+    int s_ = (x);                 \
+    if (s_ != BQ_OK) return s_;   \
+  } while (0)
+
+// device-side error bits (or-ed into a per-call status word)
+enum : uint32_t {
+  DEV_ERR_TIMEOUT = 1u,        // a bounded spin wait gave up
+  DEV_ERR_STACK = 2u,          // a deep-stack fallback query still overflowed
+  DEV_ERR_RANGE = 4u,          // an index fell outside its buffer (skipped)
+};
+
+// ------------------------------------------------------------------
+// allocation through the caller's bq_allocator (or cudaMallocAsync)
+// ------------------------------------------------------------------
+struct Alloc {
+  const bq_allocator *a;
+  cudaStream_t s;
+  int malloc_bytes(void **p, size_t bytes);
+  int free_bytes(void *p);
+  template <typename T>
+  int get(T **p, size_t count) { return malloc_bytes((void **)p, sizeof(T) * (count ? count : 1)); }
+};
+
+// RAII list of temporaries freed (stream-ordered) at scope exit
+struct TempSet {
+  Alloc &al;
+  void *ptrs[32];
+  int n = 0;
+  explicit TempSet(Alloc &a) : al(a) {}
+  template <typename T>
+  int get(T **p, size_t count)
+  {
+    int s = al.get(p, count);
+    if (s == BQ_OK) ptrs[n++] = (void *)*p;
+    return s;
+  }
+  ~TempSet()
+  {
+    for (int i = n - 1; i >= 0; i--) al.free_bytes(ptrs[i]);
+  }
+};
+
+// ------------------------------------------------------------------
+// node layout: BinaryBVH<float,3>::Node as two 16-byte halves
+//   a = lower.x lower.y lower.z upper.x
+//   b = upper.y upper.z admin.lo admin.hi
+// ------------------------------------------------------------------
+struct __align__(16) Node {
+  float4 a, b;
+};
+static_assert(sizeof(Node) == 32, "node size");
+static_assert(sizeof(bq_node3f) == 32, "C node size");
+static_assert(sizeof(bq_box3f) == 24, "C box size");
+
+__host__ __device__ inline uint64_t make_admin(uint64_t offset, uint32_t count)
+{
+  return offset | ((uint64_t)count << 48);
+}
+
+__device__ __forceinline__ uint64_t node_admin(const Node &n)
+{
+  return ((uint64_t)__float_as_uint(n.b.w) << 32) | __float_as_uint(n.b.z);
+}
+__device__ __forceinline__ uint32_t admin_count(uint64_t a) { return (uint32_t)(a >> 48); }
+__device__ __forceinline__ uint64_t admin_offset(uint64_t a) { return a & 0xFFFFFFFFFFFFull; }
+
+__device__ __forceinline__ Node make_node(float lx, float ly, float lz, float hx, float hy, float hz, uint64_t admin)
+{
+  Node n;
+  n.a = make_float4(lx, ly, lz, hx);
+  n.b = make_float4(hy, hz, __uint_as_float((uint32_t)admin), __uint_as_float((uint32_t)(admin >> 32)));
+  return n;
+}
+
+// read-only, L1-cached 32-byte node load (two 16-byte vector loads)
+__device__ __forceinline__ Node ldg_node(const Node *p)
+{
+  Node n;
+  n.a = __ldg(&p->a);
+  n.b = __ldg(&p->b);
+  return n;
+}
+
+// L2-only load (for data written by other blocks of the same kernel)
+__device__ __forceinline__ Node ldcg_node(const Node *p)
+{
+  Node n;
+  n.a = __ldcg(&p->a);
+  n.b = __ldcg(&p->b);
+  return n;
+}
+
+// ------------------------------------------------------------------
+// order-preserving float <-> int32 (min/max over encoded ints equals a
+// total-order min/max over the floats; -0 < +0)
+// ------------------------------------------------------------------
+__host__ __device__ __forceinline__ int32_t enc_f(float f)
+{
+#ifdef __CUDA_ARCH__
+  int32_t b = __float_as_int(f);
+#else
+  int32_t b;
+  memcpy(&b, &f, 4);
+#endif
+  return (b & (int32_t)0x80000000) ? (b ^ 0x7fffffff) : b;
+}
+__host__ __device__ __forceinline__ float dec_f(int32_t b)
+{
+  b = (b & (int32_t)0x80000000) ? (b ^ 0x7fffffff) : b;
+#ifdef __CUDA_ARCH__
+  return __int_as_float(b);
+#else
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+#endif
+}
+
+// ------------------------------------------------------------------
+// squared distances with the FMA shapes the reference's device code
+// compiles to (pinned against the reference kernels on B200):
+//   fSqrDistance_rd(vec3f,vec3f) = x*x+y*y+z*z
+//     (cuBQL/math/conservativeDistances.h:60-100)
+//   shrinkingRadiusQuery::fSqrDistance_rd(vec3f,box3f) = dot(v,v)
+//     (cuBQL/traversal/shrinkingRadiusQuery.h:253-259, vec.h:459-466)
+// Written with explicit intrinsics so surrounding code cannot change
+// the contraction.
+// ------------------------------------------------------------------
+__device__ __forceinline__ float sqr_pp(float px, float py, float pz, float qx, float qy, float qz)
+{
+  const float x = __fsub_rn(px, qx), y = __fsub_rn(py, qy), z = __fsub_rn(pz, qz);
+  return __fmaf_rn(z, z, __fmaf_rn(x, x, __fmul_rn(y, y)));
+}
+
+__device__ __forceinline__ float sqr_pbox(float qx, float qy, float qz, float lx, float ly, float lz, float hx,
+                                          float hy, float hz)
+{
+  const float vx = __fsub_rn(fminf(fmaxf(qx, lx), hx), qx);
+  const float vy = __fsub_rn(fminf(fmaxf(qy, ly), hy), qy);
+  const float vz = __fsub_rn(fminf(fmaxf(qz, lz), hz), qz);
+  return __fmaf_rn(vz, vz, __fmaf_rn(vy, vy, __fmul_rn(vx, vx)));
+}
+
+// ------------------------------------------------------------------
+// Morton helpers: 21 bits spread to every third bit of a u64
+// ------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint64_t spread21(uint64_t x)
+{
+  x &= 0x1fffffull;
+  x = (x | (x << 32)) & 0x001f00000000ffffull;
+  x = (x | (x << 16)) & 0x001f0000ff0000ffull;
+  x = (x | (x << 8)) & 0x100f00f00f00f00full;
+  x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+  x = (x | (x << 2)) & 0x1249249249249249ull;
+  return x;
+}
+
+// 10 bits spread to every third bit of a u32
+__host__ __device__ __forceinline__ uint32_t spread10(uint32_t x)
+{
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+// quantised cell as in the reference's Quantizer<float,D>::quantize
+// (cuBQL/builder/cuda/radix.h:55-62): float->uint truncation
+// (saturating, NaN -> 0), clamped to 2^bits - 1
+__device__ __forceinline__ uint32_t quant_cell(float c, float bias, float scale, uint32_t maxCell)
+{
+  const float f = __fmul_rn(__fsub_rn(c, bias), scale);
+  return min(__float2uint_rz(f), maxCell);
+}
+
+// per-build summary written by the bounds pass
+struct BuildState {
+  int32_t cbLo[3], cbHi[3];  // encoded centroid bounds of valid prims
+  uint32_t numValid;
+  float bias[3];
+  float scale;
+  uint32_t ticket;            // last-block-done counter (self-resetting)
+  uint32_t err;               // DEV_ERR_* bits
+  uint32_t numNodes;          // written by the topology pass
+  uint32_t pad[2];
+};
+
+inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+int num_sms();
+
+// ------------------------------------------------------------------
+// phase profiler (the counterpart of the reference's CUBQL_PROFILE,
+// cuBQL/builder/cuda/sm_builder.h:24-66): when enabled, CUDA events
+// bracket each named phase on the call's stream; prof_flush() (after the
+// stream synchronised) turns them into per-name launch counts and times.
+// Off by default; costs one branch per phase when off.
+// ------------------------------------------------------------------
+bool prof_enabled();
+void prof_record(const char *name, cudaStream_t s, bool begin, int launches);
+void prof_flush();
+struct ProfScope {
+  const char *name;
+  cudaStream_t s;
+  int launches;
+  bool on;
+  ProfScope(const char *n, cudaStream_t st, int nLaunches = 1) : name(n), s(st), launches(nLaunches), on(prof_enabled())
+  {
+    if (on) prof_record(name, s, true, launches);
+  }
+  ~ProfScope()
+  {
+    if (on) prof_record(name, s, false, launches);
+  }
+};
+
+// ------------------------------------------------------------------
+// onesweep LSD radix sort (bq_sort.cu)
+// ------------------------------------------------------------------
+// Sorts (key, value) pairs by bits [beginBit, endBit) of the key, stably.
+// keys/vals are double buffers: input in [0], result in [*outSel].
+// The element count is nDev[0] when nDev is given (nMax bounds it),
+// else nMax.  dHist (optional) holds the per-pass 256-bin digit
+// histograms, already counted by the producer of the keys.
+int onesweep_sort_u64(uint64_t *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit,
+                      int endBit, const uint32_t *dHist, int *outSel, uint32_t *dErr, Alloc &al);
+int onesweep_sort_u32(uint32_t *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit,
+                      int endBit, const uint32_t *dHist, int *outSel, uint32_t *dErr, Alloc &al);
+
+// exclusive scan of u32 values (reduce-then-scan, no waits); total -> *dTotal
+int exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint32_t nMax, const uint32_t *nDev, uint32_t *dTotal,
+                       Alloc &al);
+
+} // namespace bq

@@ -1,0 +1,523 @@
+// bq_morton.cu -- Morton (radix) BVH builder with 63-bit keys.
+//
+// Builds the same tree as cuBQL::cuda::radixBuilder<float,3>
+// (cuBQL/builder/cuda/radix.h:591-771), without its per-level host loop:
+//
+//   k_bounds      centroid bounds of the valid prims, valid count per block
+//                 and, in the last block to finish, the global bounds,
+//                 the per-block compaction offsets and the quantizer
+//                 (radix.h:185-241 fillBuildState/finishBuildState)
+//   k_keygen      stable compaction of valid prims, 63-bit Morton keys
+//                 (radix.h:41-62 Quantizer, 283-421 key generation) and the
+//                 8 digit histograms the sort needs
+//   onesweep sort stable (key, primID) sort, 8 digit passes (bq_sort.cu)
+//   k_delta       one byte per adjacent key pair: the level at which the
+//                 reference's top-down split would separate them
+//   k_agglomerate bottom-up construction of topology and boxes in one pass
+//
+// Why the bottom-up pass gives the reference's tree: createNodes/findSplit
+// (radix.h:446-570) split a key range [b,e) at the first key that has the
+// highest bit in which keys[b] and keys[e-1] differ.  That bit flips exactly
+// once inside the range, so the split is the unique adjacent pair whose
+// highest differing bit is the largest in the range: the tree is the
+// Cartesian (max-rooted) tree of the adjacent-pair "delta" array.  Runs of
+// equal keys are split at (b+e)/2 recursively (radix.h:455-465); giving
+// each split position inside a run the value 63 - (its depth in that
+// midpoint recursion), below every real delta (64 + bit index), keeps the
+// Cartesian-tree characterisation exact.  A Cartesian tree can be built
+// bottom-up: a node covering [l,r] is the child of the split at whichever
+// boundary (l or r+1) carries the smaller delta.  Each thread starts at one
+// leaf and climbs; at every parent the first arriving thread parks its
+// range end in a slot and stops, the second merges both children and goes
+// on, so every node is written exactly once and nothing waits.
+//
+// Node numbering: the children of the split between sorted positions s-1
+// and s go to nodes[2s], nodes[2s+1] (node 0 = root, node 1 unused), which
+// is a valid BinaryBVH layout with 2*numValid nodes.  It differs from the
+// reference's numbering, which its atomic allocation makes
+// run-dependent anyway; trees are compared after BFS renumbering.
+//
+// Leaf thresholds above 1 (radix.h:525-530) first build the full tree, then
+// collapse every subtree of at most `thr` prims into one leaf with a scan
+// over the kept inner nodes.
+#include <algorithm>
+#include <climits>
+#include <cfloat>
+
+#include "bq_internal.cuh"
+
+namespace bq {
+namespace {
+
+constexpr int MB_BLOCK = 256;
+constexpr int MB_UNROLL = 4;
+constexpr uint32_t SLOT_EMPTY = 0xffffffffu;
+
+struct __align__(16) Partial {
+  int32_t lo[3], hi[3];
+  uint32_t cnt, pad;
+};
+
+__device__ __forceinline__ void load_box(const bq_box3f *boxes, uint64_t i, float &lx, float &ly, float &lz,
+                                         float &hx, float &hy, float &hz)
+{
+  const float2 *p = reinterpret_cast<const float2 *>(boxes + i);
+  const float2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+  lx = a.x; ly = a.y; lz = b.x; hx = b.y; hy = c.x; hz = c.y;
+}
+
+// box.center() = (lower+upper)/2 (cuBQL/math/box.h:146-147)
+__device__ __forceinline__ float ctr(float lo, float hi) { return __fdiv_rn(__fadd_rn(lo, hi), 2.0f); }
+
+// ------------------------------------------------------------------
+// pass 1: bounds
+// ------------------------------------------------------------------
+__global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
+                                                     Partial *__restrict__ partials, uint32_t *__restrict__ blockOff,
+                                                     BuildState *st, uint32_t *__restrict__ hist, int histWords)
+{
+  __shared__ int32_t sLo[3][MB_BLOCK / 32], sHi[3][MB_BLOCK / 32];
+  __shared__ uint32_t sCnt[MB_BLOCK / 32];
+  __shared__ uint32_t sLast;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t end = min((uint64_t)n, begin + chunk);
+  int32_t lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
+  uint32_t cnt = 0;
+  for (uint64_t i0 = begin + threadIdx.x; i0 < end; i0 += (uint64_t)MB_BLOCK * MB_UNROLL) {
+    float b[MB_UNROLL][6];
+#pragma unroll
+    for (int u = 0; u < MB_UNROLL; u++) {
+      uint64_t i = i0 + (uint64_t)u * MB_BLOCK;
+      if (i < end) load_box(boxes, i, b[u][0], b[u][1], b[u][2], b[u][3], b[u][4], b[u][5]);
+      else b[u][0] = 1.f, b[u][3] = 0.f;  // empty
+    }
+#pragma unroll
+    for (int u = 0; u < MB_UNROLL; u++) {
+      if (!(b[u][0] > b[u][3])) {  // box.empty() is lower.x > upper.x (box.h:139)
+        int32_t cx = enc_f(ctr(b[u][0], b[u][3])), cy = enc_f(ctr(b[u][1], b[u][4])), cz = enc_f(ctr(b[u][2], b[u][5]));
+        lo0 = min(lo0, cx); lo1 = min(lo1, cy); lo2 = min(lo2, cz);
+        hi0 = max(hi0, cx); hi1 = max(hi1, cy); hi2 = max(hi2, cz);
+        cnt++;
+      }
+    }
+  }
+  lo0 = __reduce_min_sync(0xffffffffu, lo0); lo1 = __reduce_min_sync(0xffffffffu, lo1);
+  lo2 = __reduce_min_sync(0xffffffffu, lo2); hi0 = __reduce_max_sync(0xffffffffu, hi0);
+  hi1 = __reduce_max_sync(0xffffffffu, hi1); hi2 = __reduce_max_sync(0xffffffffu, hi2);
+  cnt = __reduce_add_sync(0xffffffffu, cnt);
+  if (lane == 0) {
+    sLo[0][warp] = lo0; sLo[1][warp] = lo1; sLo[2][warp] = lo2;
+    sHi[0][warp] = hi0; sHi[1][warp] = hi1; sHi[2][warp] = hi2;
+    sCnt[warp] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Partial p;
+    for (int d = 0; d < 3; d++) { p.lo[d] = INT_MAX; p.hi[d] = INT_MIN; }
+    p.cnt = 0;
+    p.pad = 0;
+    for (int w = 0; w < MB_BLOCK / 32; w++) {
+      for (int d = 0; d < 3; d++) { p.lo[d] = min(p.lo[d], sLo[d][w]); p.hi[d] = max(p.hi[d], sHi[d][w]); }
+      p.cnt += sCnt[w];
+    }
+    partials[blockIdx.x] = p;
+    __threadfence();
+    sLast = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!sLast) return;
+  // ---- last block: global reduction, compaction offsets, quantizer ----
+  __threadfence();
+  __shared__ uint32_t sScan[MB_BLOCK / 32];
+  uint32_t carry = 0;
+  int32_t glo[3] = {INT_MAX, INT_MAX, INT_MAX}, ghi[3] = {INT_MIN, INT_MIN, INT_MIN};
+  for (uint32_t b0 = 0; b0 < gridDim.x; b0 += MB_BLOCK) {
+    uint32_t b = b0 + threadIdx.x;
+    uint32_t c = 0;
+    if (b < gridDim.x) {
+      const Partial *pp = partials + b;
+      c = __ldcg(&pp->cnt);
+      for (int d = 0; d < 3; d++) {
+        glo[d] = min(glo[d], __ldcg(&pp->lo[d]));
+        ghi[d] = max(ghi[d], __ldcg(&pp->hi[d]));
+      }
+    }
+    // block exclusive scan of c
+    uint32_t x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) sScan[warp] = x;
+    __syncthreads();
+    uint32_t wbase = 0, tot = 0;
+    for (int w = 0; w < MB_BLOCK / 32; w++) {
+      if (w < warp) wbase += sScan[w];
+      tot += sScan[w];
+    }
+    if (b < gridDim.x) blockOff[b] = carry + wbase + x - c;
+    carry += tot;
+    __syncthreads();
+  }
+  for (int d = 0; d < 3; d++) {
+    glo[d] = __reduce_min_sync(0xffffffffu, glo[d]);
+    ghi[d] = __reduce_max_sync(0xffffffffu, ghi[d]);
+  }
+  if (lane == 0)
+    for (int d = 0; d < 3; d++) { sLo[d][warp] = glo[d]; sHi[d][warp] = ghi[d]; }
+  __syncthreads();
+  for (int i = threadIdx.x; i < histWords; i += MB_BLOCK) hist[i] = 0;
+  if (threadIdx.x == 0) {
+    float lo[3], sz[3];
+    for (int d = 0; d < 3; d++) {
+      int32_t a = INT_MAX, b = INT_MIN;
+      for (int w = 0; w < MB_BLOCK / 32; w++) { a = min(a, sLo[d][w]); b = max(b, sHi[d][w]); }
+      if (carry == 0) { a = enc_f(FLT_MAX); b = enc_f(-FLT_MAX); }  // AtomicBox::set_empty
+      st->cbLo[d] = a;
+      st->cbHi[d] = b;
+      lo[d] = dec_f(a);
+      sz[d] = __fsub_rn(dec_f(b), lo[d]);
+    }
+    // Quantizer<float,3>::init (radix.h:46-53)
+    const float ext = fmaxf(fmaxf(sz[0], sz[1]), sz[2]);
+    const float rc = __fdiv_rn(1.0f, fmaxf(ext, 1e-20f));
+    for (int d = 0; d < 3; d++) st->bias[d] = lo[d];
+    st->scale = __fmul_rn(2097152.0f, rc);
+    st->numValid = carry;
+    st->ticket = 0;
+  }
+}
+
+// ------------------------------------------------------------------
+// pass 2: keys, compaction, digit histograms
+// ------------------------------------------------------------------
+__global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
+                                                     const uint32_t *__restrict__ blockOff, const BuildState *st,
+                                                     uint64_t *__restrict__ keys, uint32_t *__restrict__ ids,
+                                                     uint32_t *__restrict__ hist)
+{
+  __shared__ uint32_t sHist[8 * 256];
+  __shared__ uint32_t sWarpCnt[MB_UNROLL][MB_BLOCK / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = threadIdx.x; i < 8 * 256; i += MB_BLOCK) sHist[i] = 0;
+  const float bx = st->bias[0], by = st->bias[1], bz = st->bias[2], sc = st->scale;
+  uint32_t running = blockOff[blockIdx.x];
+  const uint64_t begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t end = min((uint64_t)n, begin + chunk);
+  __syncthreads();
+  const uint32_t lt = (1u << lane) - 1u;
+  for (uint64_t i0 = begin; i0 < end; i0 += (uint64_t)MB_BLOCK * MB_UNROLL) {
+    float b[MB_UNROLL][6];
+    bool valid[MB_UNROLL];
+    uint32_t wpre[MB_UNROLL];
+#pragma unroll
+    for (int u = 0; u < MB_UNROLL; u++) {
+      uint64_t i = i0 + (uint64_t)u * MB_BLOCK + threadIdx.x;
+      valid[u] = false;
+      if (i < end) {
+        load_box(boxes, i, b[u][0], b[u][1], b[u][2], b[u][3], b[u][4], b[u][5]);
+        valid[u] = !(b[u][0] > b[u][3]);
+      }
+      uint32_t bal = __ballot_sync(0xffffffffu, valid[u]);
+      wpre[u] = __popc(bal & lt);
+      if (lane == 0) sWarpCnt[u][warp] = __popc(bal);
+    }
+    __syncthreads();
+    uint32_t base[MB_UNROLL];
+    uint32_t acc = running;
+#pragma unroll
+    for (int u = 0; u < MB_UNROLL; u++) {
+      uint32_t wb = 0, tot = 0;
+#pragma unroll
+      for (int w = 0; w < MB_BLOCK / 32; w++) {
+        uint32_t c = sWarpCnt[u][w];
+        wb += (w < warp) ? c : 0;
+        tot += c;
+      }
+      base[u] = acc + wb;
+      acc += tot;
+    }
+    running = acc;
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < MB_UNROLL; u++) {
+      if (!valid[u]) continue;
+      const float cx = ctr(b[u][0], b[u][3]), cy = ctr(b[u][1], b[u][4]), cz = ctr(b[u][2], b[u][5]);
+      const uint64_t key = spread21(quant_cell(cx, bx, sc, 2097151u)) |
+                           (spread21(quant_cell(cy, by, sc, 2097151u)) << 1) |
+                           (spread21(quant_cell(cz, bz, sc, 2097151u)) << 2);
+      const uint32_t pos = base[u] + wpre[u];
+      keys[pos] = key;
+      ids[pos] = (uint32_t)(i0 + (uint64_t)u * MB_BLOCK + threadIdx.x);
+#pragma unroll
+      for (int p = 0; p < 8; p++) atomicAdd(&sHist[p * 256 + ((key >> (8 * p)) & 0xff)], 1u);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 8 * 256; i += MB_BLOCK)
+    if (sHist[i]) atomicAdd(&hist[i], sHist[i]);
+}
+
+// ------------------------------------------------------------------
+// pass 3: adjacent-pair split levels
+// ------------------------------------------------------------------
+// split level of the boundary between sorted positions i and i+1
+__device__ __forceinline__ uint8_t split_level(const uint64_t *__restrict__ keys, uint32_t nv, uint32_t i)
+{
+  const uint64_t a = keys[i], b = keys[i + 1];
+  if (a != b) return (uint8_t)(64 + (63 - __clzll(a ^ b)));
+  // equal keys: the run [r0, r1) containing i, i+1 (binary searches)
+  uint32_t lo = 0, hi = i;  // first index with key >= a
+  while (lo < hi) {
+    uint32_t m = lo + ((hi - lo) >> 1);
+    if (keys[m] < a) lo = m + 1; else hi = m;
+  }
+  const uint32_t r0 = lo;
+  lo = i + 1; hi = nv;      // first index with key > a
+  while (lo < hi) {
+    uint32_t m = lo + ((hi - lo) >> 1);
+    if (keys[m] <= a) lo = m + 1; else hi = m;
+  }
+  const uint32_t r1 = lo;
+  // depth of split position s = i+1 in the (b+e)/2 recursion over [r0,r1)
+  const uint64_t s = (uint64_t)i + 1;
+  uint64_t bb = r0, ee = r1;
+  int depth = 0;
+  while (true) {
+    const uint64_t m = (bb + ee) / 2;
+    if (s == m) break;
+    if (s < m) ee = m; else bb = m;
+    depth++;
+  }
+  return (uint8_t)(63 - depth);
+}
+
+__global__ void __launch_bounds__(256) k_delta(const uint64_t *__restrict__ keys, const uint32_t *nvPtr,
+                                               uint8_t *__restrict__ delta, uint32_t *__restrict__ slot)
+{
+  const uint32_t nv = *nvPtr;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  slot[i] = SLOT_EMPTY;
+  if (i + 1 < nv) delta[i] = split_level(keys, nv, i);
+}
+
+// ------------------------------------------------------------------
+// pass 4: bottom-up topology + boxes (one thread per sorted prim)
+// ------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_agglomerate(const uint8_t *__restrict__ delta, uint32_t *__restrict__ slot,
+                                                     const uint32_t *__restrict__ ids,
+                                                     const bq_box3f *__restrict__ boxes, Node *nodes,
+                                                     const uint32_t *nvPtr, uint2 *__restrict__ ranges)
+{
+  const uint32_t nv = *nvPtr;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && nv >= 1) nodes[1] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0);
+  if (i >= nv) return;
+  float lx, ly, lz, hx, hy, hz;
+  load_box(boxes, ids[i], lx, ly, lz, hx, hy, hz);
+  uint32_t l = i, r = i;
+  uint64_t admin = make_admin(i, 1);
+  while (true) {
+    if (l == 0 && r == nv - 1) {
+      nodes[0] = make_node(lx, ly, lz, hx, hy, hz, admin);
+      return;
+    }
+    // parent = split at the lower of the two boundary levels
+    const bool leftChild = (l == 0) ? true : (r == nv - 1) ? false : (__ldg(&delta[l - 1]) > __ldg(&delta[r]));
+    const uint32_t s = leftChild ? r + 1 : l;
+    const uint32_t myPos = 2 * s + (leftChild ? 0 : 1);
+    nodes[myPos] = make_node(lx, ly, lz, hx, hy, hz, admin);
+    __threadfence();
+    const uint32_t other = atomicExch(&slot[s], leftChild ? l : r);
+    if (other == SLOT_EMPTY) return;  // sibling not done yet: it will carry on
+    __threadfence();
+    const Node sib = ldcg_node(&nodes[myPos ^ 1]);
+    if (leftChild) {  // union(left, right) in the reference's operand order (sm_builder.h:669-670)
+      lx = fminf(lx, sib.a.x); ly = fminf(ly, sib.a.y); lz = fminf(lz, sib.a.z);
+      hx = fmaxf(hx, sib.a.w); hy = fmaxf(hy, sib.b.x); hz = fmaxf(hz, sib.b.y);
+      r = other;
+    } else {
+      lx = fminf(sib.a.x, lx); ly = fminf(sib.a.y, ly); lz = fminf(sib.a.z, lz);
+      hx = fmaxf(sib.a.w, hx); hy = fmaxf(sib.b.x, hy); hz = fmaxf(sib.b.y, hz);
+      l = other;
+    }
+    if (ranges) ranges[s] = make_uint2(l, r);
+    admin = make_admin(2ull * s, 0);
+  }
+}
+
+// ------------------------------------------------------------------
+// leaf threshold > 1: collapse small subtrees of the full tree
+// ------------------------------------------------------------------
+__global__ void k_kept(const uint2 *__restrict__ ranges, const uint32_t *nvPtr, int thr, uint32_t *__restrict__ kept)
+{
+  const uint32_t nv = *nvPtr;
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x + 1;  // split positions 1..nv-1
+  if (s >= nv) return;
+  const uint2 rg = ranges[s];
+  kept[s - 1] = (rg.y - rg.x + 1 > (uint32_t)thr) ? 1u : 0u;
+}
+
+__global__ void k_collapse(const Node *__restrict__ full, const uint2 *__restrict__ ranges,
+                           const uint32_t *__restrict__ kept, const uint32_t *__restrict__ rank, const uint32_t *nvPtr,
+                           int thr, Node *__restrict__ out)
+{
+  const uint32_t nv = *nvPtr;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    Node root = full[0];
+    uint64_t a;
+    if (nv > (uint32_t)thr) {
+      const uint32_t s0 = (uint32_t)(admin_offset(node_admin(root)) >> 1);
+      a = make_admin(2ull + 2ull * rank[s0 - 1], 0);
+    } else {
+      a = make_admin(0, nv);
+    }
+    out[0] = make_node(root.a.x, root.a.y, root.a.z, root.a.w, root.b.x, root.b.y, a);
+    out[1] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0);
+  }
+  const uint32_t s = t + 1;
+  if (s >= nv || !kept[s - 1]) return;
+  const uint2 rg = ranges[s];
+  const uint64_t base = 2ull + 2ull * rank[s - 1];
+#pragma unroll
+  for (int side = 0; side < 2; side++) {
+    const Node c = full[2ull * s + side];
+    const uint32_t cl = side ? s : rg.x, cr = side ? rg.y : s - 1;
+    const uint32_t sz = cr - cl + 1;
+    uint64_t a;
+    if (sz > (uint32_t)thr) {
+      const uint32_t cs = (uint32_t)(admin_offset(node_admin(c)) >> 1);
+      a = make_admin(2ull + 2ull * rank[cs - 1], 0);
+    } else {
+      a = make_admin(cl, sz);
+    }
+    out[base + side] = make_node(c.a.x, c.a.y, c.a.z, c.a.w, c.b.x, c.b.y, a);
+  }
+}
+
+} // namespace
+
+// ------------------------------------------------------------------
+// host entry
+// ------------------------------------------------------------------
+int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al)
+{
+  const int maxLeaf = cfg ? cfg->maxAllowedLeafSize : (1 << 15);
+  const int mlt = cfg ? cfg->makeLeafThreshold : 0;
+  const int thr = mlt > 0 ? std::min(mlt, maxLeaf) : 1;  // radix.h:599-602
+  if (thr < 1 || thr > 65535)
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "leaf threshold must be in [1, 65535] (16-bit leaf count)");
+  bvh->nodes = nullptr; bvh->primIDs = nullptr; bvh->numNodes = 0; bvh->numPrims = 0;
+  if (n == 0) return BQ_OK;
+
+  const int sms = num_sms();
+  int grid = std::max(1, std::min(div_up(n, MB_BLOCK * MB_UNROLL), sms * 4));
+  uint32_t chunk = (uint32_t)div_up(div_up(n, grid), MB_BLOCK * MB_UNROLL) * (MB_BLOCK * MB_UNROLL);
+  grid = div_up(n, chunk);
+
+  TempSet tmp(al);
+  BuildState *st = nullptr;
+  Partial *partials = nullptr;
+  uint32_t *blockOff = nullptr, *hist = nullptr, *slot = nullptr;
+  uint64_t *keysA = nullptr, *keysB = nullptr;
+  uint8_t *delta = nullptr;
+  BQ_TRY(tmp.get(&st, 1));
+  BQ_TRY(tmp.get(&partials, grid));
+  BQ_TRY(tmp.get(&blockOff, grid));
+  BQ_TRY(tmp.get(&hist, 8 * 256));
+  BQ_TRY(tmp.get(&keysA, n));
+  BQ_TRY(tmp.get(&keysB, n));
+  BQ_TRY(tmp.get(&delta, n));
+  BQ_TRY(tmp.get(&slot, n));
+  uint32_t *idsA = nullptr, *idsB = nullptr;
+  Node *nodes = nullptr;
+  BQ_TRY(al.get(&idsA, n));
+  int s = al.get(&idsB, n);
+  if (s != BQ_OK) { al.free_bytes(idsA); return s; }
+  auto fail = [&](int code) {
+    al.free_bytes(idsA); al.free_bytes(idsB); al.free_bytes(nodes);
+    return code;
+  };
+  if (thr == 1) {
+    if ((s = al.get(&nodes, 2ull * n)) != BQ_OK) return fail(s);
+  }
+  cudaError_t ce = cudaMemsetAsync(st, 0, sizeof(BuildState), al.s);
+  if (ce != cudaSuccess) return fail(cuda_error(ce, "memset"));
+
+  {
+    ProfScope ps("morton.bounds", al.s);
+    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, 8 * 256);
+  }
+  {
+    ProfScope ps("morton.keygen", al.s);
+    k_keygen<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
+  }
+  if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_bounds/k_keygen"));
+
+  uint64_t *keys2[2] = {keysA, keysB};
+  uint32_t *ids2[2] = {idsA, idsB};
+  int sel = 0;
+  if ((s = onesweep_sort_u64(keys2, ids2, n, &st->numValid, 0, 63, hist, &sel, &st->err, al)) != BQ_OK)
+    return fail(s);
+  uint64_t *keys = keys2[sel];
+  uint32_t *ids = ids2[sel];
+  uint32_t *idsOther = ids2[sel ^ 1];
+
+  {
+    ProfScope ps("morton.delta", al.s);
+    k_delta<<<div_up(n, 256), 256, 0, al.s>>>(keys, &st->numValid, delta, slot);
+  }
+  if (thr == 1) {
+    ProfScope ps("morton.agglomerate", al.s);
+    k_agglomerate<<<div_up(n, 256), 256, 0, al.s>>>(delta, slot, ids, boxes, nodes, &st->numValid, nullptr);
+    if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_agglomerate"));
+  } else {
+    Node *full = nullptr;
+    uint2 *ranges = nullptr;
+    uint32_t *kept = nullptr, *rank = nullptr, *total = nullptr;
+    TempSet tmp2(al);
+    if ((s = tmp2.get(&full, 2ull * n)) != BQ_OK) return fail(s);
+    if ((s = tmp2.get(&ranges, n)) != BQ_OK) return fail(s);
+    if ((s = tmp2.get(&kept, n)) != BQ_OK) return fail(s);
+    if ((s = tmp2.get(&rank, n)) != BQ_OK) return fail(s);
+    if ((s = tmp2.get(&total, 1)) != BQ_OK) return fail(s);
+    if ((ce = cudaMemsetAsync(kept, 0, sizeof(uint32_t) * n, al.s)) != cudaSuccess) return fail(cuda_error(ce, "memset"));
+    k_agglomerate<<<div_up(n, 256), 256, 0, al.s>>>(delta, slot, ids, boxes, full, &st->numValid, ranges);
+    k_kept<<<div_up(n, 256), 256, 0, al.s>>>(ranges, &st->numValid, thr, kept);
+    if ((s = exclusive_scan_u32(kept, rank, n > 1 ? n - 1 : 1, nullptr, total, al)) != BQ_OK) return fail(s);
+    // the number of kept inner nodes decides the output size
+    uint32_t hostTotal = 0, hostNv = 0;
+    cudaMemcpyAsync(&hostTotal, total, 4, cudaMemcpyDeviceToHost, al.s);
+    cudaMemcpyAsync(&hostNv, &st->numValid, 4, cudaMemcpyDeviceToHost, al.s);
+    if ((ce = cudaStreamSynchronize(al.s)) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
+    const uint64_t numNodes = hostNv > (uint32_t)thr ? 2ull + 2ull * hostTotal : 2ull;
+    if ((s = al.get(&nodes, numNodes)) != BQ_OK) return fail(s);
+    k_collapse<<<div_up(n, 256), 256, 0, al.s>>>(full, ranges, kept, rank, &st->numValid, thr, nodes);
+    if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_collapse"));
+    if (hostNv > 0) bvh->numNodes = (uint32_t)numNodes;
+  }
+  struct { uint32_t nv, err; } h = {0, 0};
+  cudaMemcpyAsync(&h.nv, &st->numValid, 4, cudaMemcpyDeviceToHost, al.s);
+  cudaMemcpyAsync(&h.err, &st->err, 4, cudaMemcpyDeviceToHost, al.s);
+  if ((ce = cudaStreamSynchronize(al.s)) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
+  if (h.err & DEV_ERR_TIMEOUT) return fail(set_error(BQ_ERR_TIMEOUT, "radix sort look-back timed out"));
+  if (h.err) return fail(set_error(BQ_ERR_CUDA, "device-side range check failed in the Morton build"));
+  al.free_bytes(idsOther);
+  if (h.nv == 0) {
+    al.free_bytes(ids);
+    al.free_bytes(nodes);
+    bvh->numNodes = 0;
+    return BQ_OK;
+  }
+  bvh->nodes = reinterpret_cast<bq_node3f *>(nodes);
+  bvh->primIDs = ids;
+  bvh->numPrims = h.nv;
+  if (thr == 1) bvh->numNodes = 2 * h.nv;
+  return BQ_OK;
+}
+
+} // namespace bq

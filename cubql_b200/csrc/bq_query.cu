@@ -1,0 +1,391 @@
+// bq_query.cu -- batched closest-point and kNN queries over point BVHs.
+//
+// The reference exposes these as per-thread device functions
+// (cuBQL/queries/points/findClosest.h:181-226 findClosest_withBlackList,
+// cuBQL/queries/points/knn.h:75-116 findKNN) that user kernels call one
+// thread per query in input order.  Here one call answers a whole batch:
+//
+//   k_query_keys   30-bit Morton code of every query inside the root box
+//   onesweep sort  queries reordered along the curve, so neighbouring
+//                  threads walk nearly the same nodes (L1/L2 reuse, less
+//                  divergence)
+//   k_closest / k_knn
+//                  one thread per query, shrinking-radius traversal with a
+//                  local-memory stack (bq_traverse.cuh); kNN keeps its
+//                  sorted top-k in registers
+//   *_deep         queries whose stack overflowed are re-run with a deep
+//                  stack in global memory instead of returning a wrong
+//                  answer (the reference returns early, :475-478)
+#include <algorithm>
+
+#include "bq_traverse.cuh"
+
+namespace bq {
+namespace {
+
+constexpr int DEEP_THREADS = 2048;
+constexpr int DEEP_STACK = 1024;
+
+__global__ void k_query_keys(const Node *__restrict__ nodes, const float *__restrict__ queries, uint32_t nq,
+                             uint32_t *__restrict__ keys, uint32_t *__restrict__ idx)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nq) return;
+  const Node root = ldg_node(nodes);
+  const float lx = root.a.x, ly = root.a.y, lz = root.a.z;
+  const float ext = fmaxf(fmaxf(root.a.w - lx, root.b.x - ly), root.b.y - lz);
+  const float sc = 1024.0f / fmaxf(ext, 1e-20f);
+  const float *q = queries + 3ull * t;
+  const uint32_t cx = min(__float2uint_rz((q[0] - lx) * sc), 1023u);
+  const uint32_t cy = min(__float2uint_rz((q[1] - ly) * sc), 1023u);
+  const uint32_t cz = min(__float2uint_rz((q[2] - lz) * sc), 1023u);
+  keys[t] = spread10(cx) | (spread10(cy) << 1) | (spread10(cz) << 2);
+  idx[t] = t;
+}
+
+// ------------------------------------------------------------------
+// closest point
+// ------------------------------------------------------------------
+template <int TIE>
+struct CPLeaf {
+  const uint32_t *__restrict__ primIDs;
+  const float *__restrict__ points;
+  float qx, qy, qz;
+  float best;
+  int32_t id;
+  __device__ __forceinline__ float operator()(uint64_t off, uint32_t cnt)
+  {
+    for (uint32_t j = 0; j < cnt; j++) {
+      const uint32_t pid = __ldg(primIDs + off + j);
+      const float *p = points + 3ull * pid;
+      const float d = sqr_pp(__ldg(p), __ldg(p + 1), __ldg(p + 2), qx, qy, qz);
+      const bool take = (TIE == TIE_REFERENCE) ? (d < best)  // findClosest.h:211-218
+                                               : (d < best || (d == best && id >= 0 && (int32_t)pid < id));
+      if (take) {
+        best = d;
+        id = (int32_t)pid;
+      }
+    }
+    return best;
+  }
+};
+
+template <int TIE, typename Stack>
+__device__ __forceinline__ bool run_cp(const Node *nodes, const uint32_t *primIDs, const float *points,
+                                       const float *queries, uint32_t qi, float maxSqr, Stack &st, int32_t *outIds,
+                                       float *outD)
+{
+  const float *q = queries + 3ull * qi;
+  CPLeaf<TIE> leaf{primIDs, points, __ldg(q), __ldg(q + 1), __ldg(q + 2), maxSqr, -1};
+  if (!traverse<TIE>(nodes, leaf.qx, leaf.qy, leaf.qz, maxSqr, st, leaf)) return false;
+  outIds[qi] = leaf.id;
+  outD[qi] = leaf.id >= 0 ? leaf.best : INFINITY;
+  return true;
+}
+
+template <int TIE, int STACK>
+__global__ void __launch_bounds__(128) k_closest(const Node *__restrict__ nodes, const uint32_t *__restrict__ primIDs,
+                                                 const float *__restrict__ points, const float *__restrict__ queries,
+                                                 const uint32_t *__restrict__ order, uint32_t nq, float maxSqr,
+                                                 int32_t *__restrict__ outIds, float *__restrict__ outD,
+                                                 uint32_t *__restrict__ ovfList, uint32_t *ovfCount)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nq) return;
+  const uint32_t qi = order ? __ldg(order + t) : t;
+  LocalStack<STACK> st;
+  if (!run_cp<TIE>(nodes, primIDs, points, queries, qi, maxSqr, st, outIds, outD))
+    ovfList[atomicAdd(ovfCount, 1u)] = qi;
+}
+
+template <int TIE>
+__global__ void k_closest_deep(const Node *__restrict__ nodes, const uint32_t *__restrict__ primIDs,
+                               const float *__restrict__ points, const float *__restrict__ queries, float maxSqr,
+                               int32_t *__restrict__ outIds, float *__restrict__ outD, const uint32_t *ovfList,
+                               const uint32_t *ovfCount, StackEntry *stacks, uint32_t *err)
+{
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t cnt = *ovfCount;
+  for (uint32_t w = tid; w < cnt; w += gridDim.x * blockDim.x) {
+    const uint32_t qi = ovfList[w];
+    GlobalStack st{stacks + (size_t)tid * DEEP_STACK, DEEP_STACK, 0};
+    if (!run_cp<TIE>(nodes, primIDs, points, queries, qi, maxSqr, st, outIds, outD)) {
+      outIds[qi] = -1;
+      outD[qi] = INFINITY;
+      atomicOr(err, DEV_ERR_STACK);
+    }
+  }
+}
+
+// ------------------------------------------------------------------
+// kNN
+// ------------------------------------------------------------------
+template <int K, int TIE>
+struct KnnLeaf {
+  const uint32_t *__restrict__ primIDs;
+  const float *__restrict__ points;
+  float qx, qy, qz;
+  float maxSqr;
+  KnnList<K, TIE> list;
+  __device__ __forceinline__ float operator()(uint64_t off, uint32_t cnt)
+  {
+    for (uint32_t j = 0; j < cnt; j++) {
+      const uint32_t pid = __ldg(primIDs + off + j);
+      const float *p = points + 3ull * pid;
+      const float d = sqr_pp(__ldg(p), __ldg(p + 1), __ldg(p + 2), qx, qy, qz);
+      if (TIE == TIE_LOWEST && !(d < maxSqr)) continue;
+      list.offer(d, (int32_t)pid);
+    }
+    // knn::Result.sqrDistMax: the radius until k are found, then the k-th
+    return fminf(maxSqr, list.worst());
+  }
+};
+
+template <int K, int TIE, typename Stack>
+__device__ __forceinline__ bool run_knn(const Node *nodes, const uint32_t *primIDs, const float *points,
+                                        const float *queries, uint32_t qi, int k, float maxSqr, Stack &st,
+                                        int32_t *outIds, float *outD, int32_t *numFound)
+{
+  const float *q = queries + 3ull * qi;
+  KnnLeaf<K, TIE> leaf;
+  leaf.primIDs = primIDs;
+  leaf.points = points;
+  leaf.qx = __ldg(q);
+  leaf.qy = __ldg(q + 1);
+  leaf.qz = __ldg(q + 2);
+  leaf.maxSqr = maxSqr;
+  leaf.list.init(k);
+  if (!traverse<TIE>(nodes, leaf.qx, leaf.qy, leaf.qz, maxSqr, st, leaf)) return false;
+  int found = 0;
+  int32_t *oi = outIds + (size_t)qi * k;
+  float *od = outD + (size_t)qi * k;
+#pragma unroll
+  for (int j = 0; j < K; j++) {
+    if (j >= K - k) {
+      const bool real = leaf.list.I[j] != 0x7fffffff && leaf.list.D[j] != INFINITY;
+      oi[j - (K - k)] = real ? leaf.list.I[j] : -1;
+      od[j - (K - k)] = real ? leaf.list.D[j] : INFINITY;
+      found += real ? 1 : 0;
+    }
+  }
+  if (numFound) numFound[qi] = found;
+  return true;
+}
+
+template <int K, int TIE, int STACK>
+__global__ void __launch_bounds__(128) k_knn(const Node *__restrict__ nodes, const uint32_t *__restrict__ primIDs,
+                                             const float *__restrict__ points, const float *__restrict__ queries,
+                                             const uint32_t *__restrict__ order, uint32_t nq, int k, float maxSqr,
+                                             int32_t *__restrict__ outIds, float *__restrict__ outD,
+                                             int32_t *__restrict__ numFound, uint32_t *__restrict__ ovfList,
+                                             uint32_t *ovfCount)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nq) return;
+  const uint32_t qi = order ? __ldg(order + t) : t;
+  LocalStack<STACK> st;
+  if (!run_knn<K, TIE>(nodes, primIDs, points, queries, qi, k, maxSqr, st, outIds, outD, numFound))
+    ovfList[atomicAdd(ovfCount, 1u)] = qi;
+}
+
+template <int K, int TIE>
+__global__ void k_knn_deep(const Node *__restrict__ nodes, const uint32_t *__restrict__ primIDs,
+                           const float *__restrict__ points, const float *__restrict__ queries, int k, float maxSqr,
+                           int32_t *__restrict__ outIds, float *__restrict__ outD, int32_t *__restrict__ numFound,
+                           const uint32_t *ovfList, const uint32_t *ovfCount, StackEntry *stacks, uint32_t *err)
+{
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t cnt = *ovfCount;
+  for (uint32_t w = tid; w < cnt; w += gridDim.x * blockDim.x) {
+    const uint32_t qi = ovfList[w];
+    GlobalStack st{stacks + (size_t)tid * DEEP_STACK, DEEP_STACK, 0};
+    if (!run_knn<K, TIE>(nodes, primIDs, points, queries, qi, k, maxSqr, st, outIds, outD, numFound)) {
+      for (int j = 0; j < k; j++) {
+        outIds[(size_t)qi * k + j] = -1;
+        outD[(size_t)qi * k + j] = INFINITY;
+      }
+      if (numFound) numFound[qi] = 0;
+      atomicOr(err, DEV_ERR_STACK);
+    }
+  }
+}
+
+__global__ void k_fill_empty(uint32_t nq, int k, int32_t *ids, float *d, int32_t *numFound)
+{
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (uint64_t)nq * k) return;
+  ids[t] = -1;
+  d[t] = INFINITY;
+  if (numFound && t < nq) numFound[t] = 0;
+}
+
+// ------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------
+struct QueryScratch {
+  uint32_t *order = nullptr;
+  uint32_t *ovfList = nullptr, *ovfCount = nullptr, *err = nullptr;
+  StackEntry *deep = nullptr;
+};
+
+int prepare(const bq_bvh3f *bvh, const float *queries, uint32_t nq, bool reorder, TempSet &tmp, Alloc &al,
+            QueryScratch &qs)
+{
+  BQ_TRY(tmp.get(&qs.ovfList, nq));
+  BQ_TRY(tmp.get(&qs.ovfCount, 2));
+  qs.err = qs.ovfCount + 1;
+  BQ_TRY(tmp.get(&qs.deep, (size_t)DEEP_THREADS * DEEP_STACK));
+  BQ_CUDA(cudaMemsetAsync(qs.ovfCount, 0, 8, al.s));
+  if (reorder && nq > 1) {
+    uint32_t *keys[2], *idx[2];
+    BQ_TRY(tmp.get(&keys[0], nq));
+    BQ_TRY(tmp.get(&keys[1], nq));
+    BQ_TRY(tmp.get(&idx[0], nq));
+    BQ_TRY(tmp.get(&idx[1], nq));
+    {
+      ProfScope ps("query.keys", al.s);
+      k_query_keys<<<div_up(nq, 256), 256, 0, al.s>>>((const Node *)bvh->nodes, queries, nq, keys[0], idx[0]);
+    }
+    BQ_CUDA(cudaGetLastError());
+    int sel = 0;
+    BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, 0, 30, nullptr, &sel, qs.err, al));
+    qs.order = idx[sel];
+  }
+  return BQ_OK;
+}
+
+int finish(QueryScratch &qs, Alloc &al)
+{
+  // the only host synchronisation: read the device error word
+  uint32_t err = 0;
+  BQ_CUDA(cudaMemcpyAsync(&err, qs.err, 4, cudaMemcpyDeviceToHost, al.s));
+  BQ_CUDA(cudaStreamSynchronize(al.s));
+  if (err & DEV_ERR_STACK) return set_error(BQ_ERR_STACK_OVERFLOW, "query exceeded the deep fallback stack");
+  if (err & DEV_ERR_TIMEOUT) return set_error(BQ_ERR_TIMEOUT, "query reordering sort timed out");
+  return BQ_OK;
+}
+
+template <int TIE, int STACK>
+void launch_cp(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
+               int block, int32_t *ids, float *d, QueryScratch &qs, cudaStream_t s)
+{
+  const Node *nodes = (const Node *)bvh->nodes;
+  {
+    ProfScope ps("query.closest", s);
+    k_closest<TIE, STACK><<<div_up(nq, block), block, 0, s>>>(nodes, bvh->primIDs, points, queries, qs.order, nq,
+                                                             maxSqr, ids, d, qs.ovfList, qs.ovfCount);
+  }
+  ProfScope ps("query.deep", s);
+  k_closest_deep<TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, maxSqr, ids, d,
+                                                         qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+}
+
+template <int K, int TIE, int STACK>
+void launch_knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, int k, float maxSqr,
+                int block, int32_t *ids, float *d, int32_t *nf, QueryScratch &qs, cudaStream_t s)
+{
+  const Node *nodes = (const Node *)bvh->nodes;
+  {
+    ProfScope ps("query.knn", s);
+    k_knn<K, TIE, STACK><<<div_up(nq, block), block, 0, s>>>(nodes, bvh->primIDs, points, queries, qs.order, nq, k,
+                                                            maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount);
+  }
+  ProfScope ps("query.deep", s);
+  k_knn_deep<K, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d, nf,
+                                                        qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+}
+
+template <int K, int TIE>
+void dispatch_knn_stack(int stack, const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq,
+                        int k, float maxSqr, int block, int32_t *ids, float *d, int32_t *nf, QueryScratch &qs,
+                        cudaStream_t s)
+{
+  if (stack <= 32) launch_knn<K, TIE, 32>(bvh, points, queries, nq, k, maxSqr, block, ids, d, nf, qs, s);
+  else if (stack <= 64) launch_knn<K, TIE, 64>(bvh, points, queries, nq, k, maxSqr, block, ids, d, nf, qs, s);
+  else launch_knn<K, TIE, 128>(bvh, points, queries, nq, k, maxSqr, block, ids, d, nf, qs, s);
+}
+
+template <int K>
+void dispatch_knn_tie(int tie, int stack, const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq,
+                      int k, float maxSqr, int block, int32_t *ids, float *d, int32_t *nf, QueryScratch &qs,
+                      cudaStream_t s)
+{
+  if (tie == BQ_TIES_REFERENCE)
+    dispatch_knn_stack<K, TIE_REFERENCE>(stack, bvh, points, queries, nq, k, maxSqr, block, ids, d, nf, qs, s);
+  else
+    dispatch_knn_stack<K, TIE_LOWEST>(stack, bvh, points, queries, nq, k, maxSqr, block, ids, d, nf, qs, s);
+}
+
+} // namespace
+
+int query_config(const bq_query_config *q, bq_query_config &out)
+{
+  out.tieMode = q ? q->tieMode : BQ_TIES_LOWEST_ID;
+  out.stackDepth = (q && q->stackDepth) ? q->stackDepth : 64;
+  out.blockSize = (q && q->blockSize) ? q->blockSize : 128;
+  out.reorder = q ? q->reorder : 1;
+  out.queriesPerWarp = (q && q->queriesPerWarp) ? q->queriesPerWarp : 32;
+  if (out.tieMode != BQ_TIES_LOWEST_ID && out.tieMode != BQ_TIES_REFERENCE)
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "tieMode must be BQ_TIES_LOWEST_ID or BQ_TIES_REFERENCE");
+  if (out.stackDepth != 32 && out.stackDepth != 64 && out.stackDepth != 128)
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "stackDepth must be 32, 64 or 128");
+  if (out.blockSize != 64 && out.blockSize != 128)
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "blockSize must be 64 or 128");
+  if (out.queriesPerWarp != 32) return set_error(BQ_ERR_UNSUPPORTED, "queriesPerWarp must be 32");
+  return BQ_OK;
+}
+
+int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
+                  const bq_query_config *qcfg, int32_t *ids, float *d, Alloc &al)
+{
+  bq_query_config c;
+  BQ_TRY(query_config(qcfg, c));
+  if (nq == 0) return BQ_OK;
+  if (bvh->numNodes == 0) {
+    k_fill_empty<<<div_up(nq, 256), 256, 0, al.s>>>(nq, 1, ids, d, nullptr);
+    BQ_CUDA(cudaGetLastError());
+    return BQ_OK;
+  }
+  TempSet tmp(al);
+  QueryScratch qs;
+  BQ_TRY(prepare(bvh, queries, nq, c.reorder != 0, tmp, al, qs));
+  const int tie = c.tieMode, st = c.stackDepth, b = c.blockSize;
+  if (tie == BQ_TIES_REFERENCE) {
+    if (st == 32) launch_cp<TIE_REFERENCE, 32>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
+    else if (st == 64) launch_cp<TIE_REFERENCE, 64>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
+    else launch_cp<TIE_REFERENCE, 128>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
+  } else {
+    if (st == 32) launch_cp<TIE_LOWEST, 32>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
+    else if (st == 64) launch_cp<TIE_LOWEST, 64>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
+    else launch_cp<TIE_LOWEST, 128>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
+  }
+  BQ_CUDA(cudaGetLastError());
+  return finish(qs, al);
+}
+
+int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, int k, float maxSqr,
+        const bq_query_config *qcfg, int32_t *ids, float *d, int32_t *numFound, Alloc &al)
+{
+  bq_query_config c;
+  BQ_TRY(query_config(qcfg, c));
+  if (k < 1 || k > 64) return set_error(BQ_ERR_INVALID_ARGUMENT, "k must be in [1, 64]");
+  if (nq == 0) return BQ_OK;
+  if (bvh->numNodes == 0) {
+    k_fill_empty<<<div_up((uint64_t)nq * k, 256), 256, 0, al.s>>>(nq, k, ids, d, numFound);
+    BQ_CUDA(cudaGetLastError());
+    return BQ_OK;
+  }
+  TempSet tmp(al);
+  QueryScratch qs;
+  BQ_TRY(prepare(bvh, queries, nq, c.reorder != 0, tmp, al, qs));
+  const int tie = c.tieMode, st = c.stackDepth, b = c.blockSize;
+  if (k <= 4) dispatch_knn_tie<4>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
+  else if (k <= 8) dispatch_knn_tie<8>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
+  else if (k <= 16) dispatch_knn_tie<16>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
+  else if (k <= 32) dispatch_knn_tie<32>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
+  else dispatch_knn_tie<64>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
+  BQ_CUDA(cudaGetLastError());
+  return finish(qs, al);
+}
+
+} // namespace bq

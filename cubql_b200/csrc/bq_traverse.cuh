@@ -1,0 +1,156 @@
+// bq_traverse.cuh -- shrinking-radius stack traversal over a BinaryBVH.
+//
+// Same visiting order as cuBQL::shrinkingRadiusQuery::forEachLeaf
+// (cuBQL/traversal/shrinkingRadiusQuery.h:409-508): both children of an
+// inner node are loaded (2 x 32 B, each as two 16-byte vector loads), the
+// nearer one is descended (ties to child 1), the farther one is pushed when
+// it is inside the cull radius, leaves report a new radius, and popped
+// entries are skipped once the radius has shrunk below them.
+//
+// TIE selects the comparison rules:
+//   TIE_REFERENCE: exactly the reference's (cull at >=, push at <, pop at <=),
+//     so results match its kernels bit for bit, ties included;
+//   TIE_LOWEST:    nodes at exactly the cull distance are kept, so a leaf
+//     functor can prefer the lowest primID among equal distances.
+#pragma once
+
+#include "bq_internal.cuh"
+
+namespace bq {
+
+enum { TIE_LOWEST = 0, TIE_REFERENCE = 1 };
+
+struct StackEntry {
+  uint32_t idx;
+  float dist;
+};
+
+// fixed-size stack in local memory
+template <int N>
+struct LocalStack {
+  StackEntry e[N];
+  int sp = 0;
+  __device__ __forceinline__ bool push(uint32_t i, float d)
+  {
+    if (sp >= N) return false;
+    e[sp].idx = i;
+    e[sp].dist = d;
+    sp++;
+    return true;
+  }
+  __device__ __forceinline__ bool empty() const { return sp == 0; }
+  __device__ __forceinline__ StackEntry pop() { return e[--sp]; }
+};
+
+// deep stack in a caller-provided global-memory slice
+struct GlobalStack {
+  StackEntry *e;
+  int cap;
+  int sp = 0;
+  __device__ __forceinline__ bool push(uint32_t i, float d)
+  {
+    if (sp >= cap) return false;
+    e[sp].idx = i;
+    e[sp].dist = d;
+    sp++;
+    return true;
+  }
+  __device__ __forceinline__ bool empty() const { return sp == 0; }
+  __device__ __forceinline__ StackEntry pop() { return e[--sp]; }
+};
+
+__device__ __forceinline__ uint64_t ldg_admin(const Node *p)
+{
+  const float4 b = __ldg(&p->b);
+  return ((uint64_t)__float_as_uint(b.w) << 32) | __float_as_uint(b.z);
+}
+
+// Leaf functor contract: float operator()(uint64_t offset, uint32_t count)
+// processes primIDs[offset .. offset+count) and returns the new cull
+// radius proposal.  Returns false if the stack overflowed (the query then
+// has to be re-run with a deeper stack; its partial state is discarded).
+template <int TIE, typename Stack, typename Leaf>
+__device__ __forceinline__ bool traverse(const Node *__restrict__ nodes, float qx, float qy, float qz, float cull,
+                                         Stack &stack, Leaf &leaf)
+{
+  uint64_t admin = ldg_admin(nodes);
+  while (true) {
+    bool dead = false;
+    while (admin_count(admin) == 0) {
+      const uint64_t off = admin_offset(admin);
+      const Node n0 = ldg_node(nodes + off);
+      const Node n1 = ldg_node(nodes + off + 1);
+      const float d0 = sqr_pbox(qx, qy, qz, n0.a.x, n0.a.y, n0.a.z, n0.a.w, n0.b.x, n0.b.y);
+      const float d1 = sqr_pbox(qx, qy, qz, n1.a.x, n1.a.y, n1.a.z, n1.a.w, n1.b.x, n1.b.y);
+      const float dmin = fminf(d0, d1), dmax = fmaxf(d0, d1);
+      if (TIE == TIE_REFERENCE ? (dmin >= cull) : (dmin > cull)) {
+        dead = true;
+        break;
+      }
+      uint32_t farID;
+      if (d0 < d1) {
+        admin = node_admin(n0);
+        farID = (uint32_t)off + 1;
+      } else {
+        admin = node_admin(n1);
+        farID = (uint32_t)off;
+      }
+      if (TIE == TIE_REFERENCE ? (dmax < cull) : (dmax <= cull)) {
+        if (!stack.push(farID, dmax)) return false;
+      }
+    }
+    if (!dead) cull = fminf(cull, leaf(admin_offset(admin), admin_count(admin)));
+    while (true) {
+      if (stack.empty()) return true;
+      const StackEntry e = stack.pop();
+      if (e.dist <= cull) {
+        admin = ldg_admin(nodes + e.idx);
+        break;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------
+// candidate lists kept in registers
+// ------------------------------------------------------------------
+template <int TIE>
+__device__ __forceinline__ bool cand_before(float d, int32_t id, float D, int32_t I)
+{
+  if (TIE == TIE_REFERENCE) return d < D;  // insert after equal distances (common/knn.h:67-71)
+  return d < D || (d == D && id < I);
+}
+
+// sorted list of K (distance, id) pairs; slots [0, K-k) hold sentinels
+// below every candidate so the k-th best always sits at index K-1
+template <int K, int TIE>
+struct KnnList {
+  float D[K];
+  int32_t I[K];
+  __device__ __forceinline__ void init(int k)
+  {
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+      const bool sentinel = j < K - k;
+      D[j] = sentinel ? -1.0f : INFINITY;
+      I[j] = sentinel ? -1 : 0x7fffffff;
+    }
+  }
+  __device__ __forceinline__ float worst() const { return D[K - 1]; }
+  // insert if it belongs to the list
+  __device__ __forceinline__ void offer(float d, int32_t id)
+  {
+    if (!cand_before<TIE>(d, id, D[K - 1], I[K - 1])) return;
+#pragma unroll
+    for (int j = K - 1; j >= 0; j--) {
+      const bool fromPrev = (j > 0) && cand_before<TIE>(d, id, D[j > 0 ? j - 1 : 0], I[j > 0 ? j - 1 : 0]);
+      const bool here = cand_before<TIE>(d, id, D[j], I[j]);
+      const float nd = fromPrev ? D[j > 0 ? j - 1 : 0] : (here ? d : D[j]);
+      const int32_t ni = fromPrev ? I[j > 0 ? j - 1 : 0] : (here ? id : I[j]);
+      D[j] = nd;
+      I[j] = ni;
+    }
+  }
+};
+
+} // namespace bq

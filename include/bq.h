@@ -1,0 +1,200 @@
+/*
+ * bq.h -- C ABI of the B200-native BVH build-and-query library (libbq.so).
+ *
+ * Drop-in for the BinaryBVH<float,3> build-and-query path of cuBQL
+ * (Ssz990220/cuBQL).  Every entry point:
+ *   - runs on the caller's CUDA stream (`bq_stream_t` is a cudaStream_t;
+ *     NULL is the legacy default stream),
+ *   - takes DEVICE pointers for all array arguments,
+ *   - returns an int status (BQ_OK or one of the BQ_ERR_* codes below);
+ *     bq_last_error_string() gives the message of the calling thread's
+ *     last failure.  Nothing aborts or raises.
+ * The library keeps no mutable global state between calls except the
+ * per-thread error string, so calls on different streams may run
+ * concurrently.
+ *
+ * Memory layout (identical to the reference, so trees built here can be
+ * traversed by the reference's device code and vice versa):
+ *   bq_box3f   == cuBQL::box3f              (cuBQL/math/box.h:60-179), 24 B
+ *   bq_node3f  == BinaryBVH<float,3>::Node  (cuBQL/bvh.h:78-102), 32 B,
+ *                 offsetAndCount = offset (bits 0..47) | count (bits 48..63);
+ *                 count 0 = inner node whose children are nodes[offset],
+ *                 nodes[offset+1]; count > 0 = leaf holding
+ *                 primIDs[offset .. offset+count).
+ *                 Node 0 is the root, node 1 is unused.
+ *   bq_bvh3f   == BinaryBVH<float,3>        (cuBQL/bvh.h:71-111)
+ */
+#ifndef BQ_H
+#define BQ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BQ_VERSION 100
+
+/* status codes */
+#define BQ_OK 0
+#define BQ_ERR_INVALID_ARGUMENT 1 /* bad pointer, size, alignment or config */
+#define BQ_ERR_CUDA 2             /* a CUDA runtime call failed */
+#define BQ_ERR_ALLOC 3            /* the allocator returned an error */
+#define BQ_ERR_STACK_OVERFLOW 4   /* a query exceeded even the deep fallback stack */
+#define BQ_ERR_TIMEOUT 5          /* a bounded device-side wait gave up */
+#define BQ_ERR_UNSUPPORTED 6
+
+/* build methods (cuBQL/bvh.h:38-55 BuildConfig::BuildMethod) */
+#define BQ_SPATIAL_MEDIAN 0
+#define BQ_MORTON63 16 /* cuda::radixBuilder */
+#define BQ_MORTON30 17 /* cuda::rebinRadixBuilder */
+
+/* query tie rules */
+#define BQ_TIES_LOWEST_ID 0 /* equal FP32 distances -> lowest primID (default) */
+#define BQ_TIES_REFERENCE 1 /* exactly the reference's traversal-order rules */
+
+typedef void *bq_stream_t; /* cudaStream_t */
+
+typedef struct bq_box3f {
+  float lower[3];
+  float upper[3];
+} bq_box3f;
+
+typedef struct bq_node3f {
+  float lower[3];
+  float upper[3];
+  uint64_t offsetAndCount;
+} bq_node3f;
+
+typedef struct bq_bvh3f {
+  bq_node3f *nodes;
+  uint32_t numNodes;
+  uint32_t *primIDs;
+  uint32_t numPrims;
+} bq_bvh3f;
+
+/* mirrors cuBQL::BuildConfig (cuBQL/bvh.h:31-64) */
+typedef struct bq_build_config {
+  int maxAllowedLeafSize; /* default 1<<15 */
+  int makeLeafThreshold;  /* 0 = builder default (1) */
+  int buildMethod;        /* BQ_SPATIAL_MEDIAN (gpuBuilder only) */
+} bq_build_config;
+
+/* replaces cuBQL::GpuMemoryResource (cuBQL/builder/cuda.h:31-78).
+   NULL = cudaMallocAsync / cudaFreeAsync on the call's stream. */
+typedef struct bq_allocator {
+  void *ctx;
+  int (*malloc)(void *ctx, void **ptr, size_t size, bq_stream_t stream); /* 0 on success */
+  int (*free)(void *ctx, void *ptr, bq_stream_t stream);
+} bq_allocator;
+
+/* traversal knobs; NULL = defaults (ties lowest-ID, Morton-ordered
+   queries, autotuned launch shape) */
+typedef struct bq_query_config {
+  int tieMode;       /* BQ_TIES_LOWEST_ID or BQ_TIES_REFERENCE */
+  int stackDepth;    /* fast-path stack entries: 32, 64 or 128 (0 = 64) */
+  int blockSize;     /* threads per block: 64..512 (0 = 128) */
+  int reorder;       /* 1 = process queries in Morton order, 0 = input order */
+  int queriesPerWarp;/* 32 = one thread per query (only value so far; 0 = 32) */
+} bq_query_config;
+
+/* ---------------------------------------------------------------- */
+/* builders                                                           */
+/* ---------------------------------------------------------------- */
+
+/* Morton/radix builder with 63-bit keys.  Replaces
+   cuBQL::cuda::radixBuilder<float,3> (cuBQL/builder/cuda.h:134-140,
+   implementation cuBQL/builder/cuda/radix.h:591-771).  The tree equals
+   the reference's node for node after BFS renumbering.  Empty boxes
+   (lower.x > upper.x) are left out.  Allocates bvh->nodes and
+   bvh->primIDs with `alloc`; synchronises `stream` once at the end to
+   learn the node count. */
+int bq_build_morton63_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
+                         const bq_allocator *alloc, bq_stream_t stream);
+
+/* Spatial-median builder.  Replaces cuBQL::gpuBuilder<float,3>
+   (cuBQL/builder/cuda.h:91-99, cuBQL/builder/cuda/gpu_builder.h:31-67,
+   cuBQL/builder/cuda/sm_builder.h:469-614). */
+int bq_build_spatial_median_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
+                               const bq_allocator *alloc, bq_stream_t stream);
+
+/* Recomputes every node box bottom-up from `boxes`.  Replaces
+   gpuBuilder_impl::refit (cuBQL/builder/cuda/sm_builder.h:677-693). */
+int bq_refit_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_allocator *alloc, bq_stream_t stream);
+
+/* Frees a tree built by this library.  Replaces cuBQL::cuda::free
+   (cuBQL/builder/cuda.h:158-161, cuBQL/builder/cuda/gpu_builder.h:79-90). */
+int bq_free_f3(bq_bvh3f *bvh, const bq_allocator *alloc, bq_stream_t stream);
+
+/* ---------------------------------------------------------------- */
+/* queries (batched; the reference offers per-thread device functions */
+/* that user kernels call one thread per query)                        */
+/* ---------------------------------------------------------------- */
+
+/* Closest data point per query.  Replaces a user kernel calling
+   cuBQL::points::findClosest (cuBQL/queries/points/findClosest.h:336-360)
+   once per query, e.g. testing/points/closestPoint.cu:37-58.
+   ids[q] = closest primID or -1 if none within maxSqrDist (strictly
+   closer); sqrDist[q] = its FP32 squared distance or +inf. */
+int bq_closest_point_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries,
+                        float maxSqrDist, const bq_query_config *qcfg, int32_t *ids, float *sqrDist,
+                        const bq_allocator *alloc, bq_stream_t stream);
+
+/* k nearest data points per query (1 <= k <= 64), ascending by squared
+   distance.  Replaces cuBQL::points::findKNN
+   (cuBQL/queries/points/knn.h:75-116).  ids/sqrDist are numQueries*k
+   (row per query; unfilled slots -1 / +inf); numFound may be NULL. */
+int bq_knn_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries, int k,
+              float maxSqrDist, const bq_query_config *qcfg, int32_t *ids, float *sqrDist, int32_t *numFound,
+              const bq_allocator *alloc, bq_stream_t stream);
+
+/* Closest triangle per query over an indexed mesh (tris: int32 triples
+   into verts: float triples).  Replaces cuBQL::triangles::findClosest
+   (cuBQL/queries/triangles/findClosest.h:132-152).  P may be NULL. */
+int bq_tri_closest_f3(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, const float *queries,
+                      uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg, int32_t *ids,
+                      float *sqrDist, float *P, const bq_allocator *alloc, bq_stream_t stream);
+
+/* Adjoint of bq_tri_closest_f3's sqrDist: given gradSqr (dL/dsqrDist per
+   query) and the forward's ids, writes gradQueries (numQueries*3) and
+   OVERWRITES gradVerts (numVerts*3).  Vertex contributions are sorted by
+   vertex id and summed in a fixed order: no float atomics, bitwise
+   reproducible.  No counterpart in the reference (it has no gradients). */
+int bq_tri_distance_bwd_f3(const int32_t *tris, const float *verts, uint32_t numVerts, const float *queries,
+                           uint32_t numQueries, const int32_t *ids, const float *gradSqr, float *gradQueries,
+                           float *gradVerts, const bq_allocator *alloc, bq_stream_t stream);
+
+/* ---------------------------------------------------------------- */
+/* input helpers                                                      */
+/* ---------------------------------------------------------------- */
+
+/* boxes[t] = bounds of triangle t (Triangle::bounds(),
+   cuBQL/queries/triangles/Triangle.h:40-41). */
+int bq_tri_boxes_f3(const int32_t *tris, const float *verts, uint32_t numTris, bq_box3f *boxes, bq_stream_t stream);
+
+/* boxes[i] = the degenerate box of point i (box3f().including(p), as
+   testing/points/closestPoint.cu:22-29 prepares point data). */
+int bq_points_to_boxes_f3(const float *points, uint32_t numPoints, bq_box3f *boxes, bq_stream_t stream);
+
+/* ---------------------------------------------------------------- */
+/* misc                                                               */
+/* ---------------------------------------------------------------- */
+const char *bq_last_error_string(void);
+int bq_version(void);
+
+/* Phase profiler, the counterpart of the reference's CUBQL_PROFILE
+   switch (cuBQL/builder/cuda/sm_builder.h:24-66, 505-607).  While enabled,
+   every library call brackets its kernel phases with CUDA events on its
+   stream; totals are kept per calling thread and per phase name.  The
+   returned name stays valid until the next bq_profile_reset(). */
+int bq_profile_enable(int on);
+int bq_profile_reset(void);
+int bq_profile_count(void);
+int bq_profile_entry(int index, const char **name, uint64_t *launches, double *ms);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* BQ_H */

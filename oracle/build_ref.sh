@@ -1,0 +1,21 @@
+#!/bin/sh
+# Compiles the reference library's own code paths, directly from the
+# unmodified reference sources at $REF (default /root/reference), into
+# oracle/_ref/.  Test / baseline infrastructure only; nothing from the
+# reference is copied into this repository.
+#   libref_cpu.so  cpuBuilder + host findClosest/findKNN/triangles (g++)
+#   libref_gpu.so  gpuBuilder, radixBuilder, rebinRadixBuilder and the
+#                  per-thread query device functions, for sm_100a (nvcc)
+# Both are built with FMA contraction as each compiler does by default for
+# that code: g++ on x86-64 (no -mfma) emits none, nvcc contracts.
+set -e
+REF="${REF:-/root/reference}"
+here="$(cd "$(dirname "$0")" && pwd)"
+if [ ! -d "$REF/cuBQL" ]; then
+  echo "reference sources not found at $REF; keeping existing oracle/_ref" >&2
+  exit 0
+fi
+mkdir -p "$here/_ref"
+g++ -std=c++17 -O2 -fPIC -shared -I"$REF" -w -o "$here/_ref/libref_cpu.so" "$here/ref_cpu.cpp" -lpthread
+/usr/local/cuda/bin/nvcc -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC -shared \
+    -I"$REF" -w -o "$here/_ref/libref_gpu.so" "$here/ref_gpu.cu"

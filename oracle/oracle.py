@@ -1,0 +1,402 @@
+"""ctypes bindings of the CPU oracle and of the compiled reference.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and
+by bench.py's CPU-baseline / reference legs, never by the product package.
+
+  liboracle.so  C restatement of the reference algorithms (bq_oracle.c)
+  libref_cpu.so the reference's host code, compiled from its sources
+  libref_gpu.so the reference's GPU builders and query device functions,
+                compiled for sm_100a from its sources (needs a GPU to run)
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_CPU_SO = os.path.join(HERE, "_ref", "libref_cpu.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libref_gpu.so")
+
+NODE = np.dtype([("lower", "<f4", 3), ("upper", "<f4", 3), ("admin", "<u8")])
+assert NODE.itemsize == 32
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def build():
+    """Compile the oracle (always) and the reference libraries (if the
+    reference sources are present)."""
+    import subprocess
+    subprocess.run(["sh", os.path.join(HERE, "build_oracle.sh")], check=True)
+    subprocess.run(["sh", os.path.join(HERE, "build_ref.sh")], check=True)
+
+
+_libs = {}
+
+
+def _load(path):
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (run oracle/build_oracle.sh / build_ref.sh)")
+        _libs[path] = ctypes.CDLL(path)
+    return _libs[path]
+
+
+def have_ref_cpu():
+    return os.path.exists(REF_CPU_SO)
+
+
+def have_ref_gpu():
+    return os.path.exists(REF_GPU_SO)
+
+
+def offsets(nodes):
+    return (nodes["admin"] & np.uint64(0xFFFFFFFFFFFF)).astype(np.int64)
+
+
+def counts(nodes):
+    return (nodes["admin"] >> np.uint64(48)).astype(np.int64)
+
+
+# ---------------------------------------------------------------------------
+# C restatement
+# ---------------------------------------------------------------------------
+class Oracle:
+    def __init__(self):
+        self.lib = _load(ORACLE_SO)
+
+    def uniform_points(self, n, seed, lo=0.0, hi=1.0):
+        out = np.empty((n, 3), dtype=np.float32)
+        self.lib.orc_uniform_points(ctypes.c_uint32(n), ctypes.c_uint32(seed), ctypes.c_double(lo),
+                                    ctypes.c_double(hi), _p(out))
+        return out
+
+    def _tree(self, fn, boxes, *args):
+        boxes = _f32(boxes).reshape(-1, 6)
+        n = boxes.shape[0]
+        nodes = np.zeros(2 * n + 2, dtype=NODE)
+        prims = np.zeros(max(n, 1), dtype=np.uint32)
+        nn, npr = ctypes.c_uint32(), ctypes.c_uint32()
+        rc = fn(_p(boxes), ctypes.c_uint32(n), *args, _p(nodes), _p(prims), ctypes.byref(nn), ctypes.byref(npr))
+        assert rc == 0
+        return nodes[: nn.value].copy(), prims[: npr.value].copy()
+
+    def radix_build(self, boxes, makeLeafThreshold=0, maxAllowedLeafSize=1 << 15, keys=False):
+        boxes = _f32(boxes).reshape(-1, 6)
+        n = boxes.shape[0]
+        nodes = np.zeros(2 * n + 2, dtype=NODE)
+        prims = np.zeros(max(n, 1), dtype=np.uint32)
+        k = np.zeros(max(n, 1), dtype=np.uint64)
+        nn, npr = ctypes.c_uint32(), ctypes.c_uint32()
+        rc = self.lib.orc_radix_build(_p(boxes), ctypes.c_uint32(n), ctypes.c_int(makeLeafThreshold),
+                                      ctypes.c_int(maxAllowedLeafSize), _p(nodes), _p(prims), ctypes.byref(nn),
+                                      ctypes.byref(npr), _p(k))
+        assert rc == 0
+        out = (nodes[: nn.value].copy(), prims[: npr.value].copy())
+        return out + (k[: npr.value].copy(),) if keys else out
+
+    def sm_build(self, boxes, makeLeafThreshold=0):
+        return self._tree(self.lib.orc_sm_build, boxes, ctypes.c_int(makeLeafThreshold))
+
+    def cpu_build(self, boxes, makeLeafThreshold=0):
+        return self._tree(self.lib.orc_cpu_build, boxes, ctypes.c_int(makeLeafThreshold))
+
+    def canonicalize(self, nodes, prims):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        out = np.zeros(len(nodes), dtype=NODE)
+        outp = np.zeros(max(len(prims), 1), dtype=np.uint32)
+        npr = ctypes.c_uint32()
+        rc = self.lib.orc_canonicalize(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), _p(out), _p(outp),
+                                       ctypes.byref(npr))
+        if rc != 0:
+            raise ValueError(f"tree is not a valid BinaryBVH (canonicalize rc={rc})")
+        return out, outp[: npr.value].copy()
+
+    def closest_point(self, nodes, prims, points, queries, maxSqr=np.inf, fma_mode=1, tie_mode=0, stack=64):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        ovf = np.zeros(nq, dtype=np.uint8)
+        vis = np.zeros(nq, dtype=np.uint32)
+        self.lib.orc_closest_point(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), _p(points), _p(queries),
+                                   ctypes.c_uint32(nq), ctypes.c_float(maxSqr), ctypes.c_int(fma_mode),
+                                   ctypes.c_int(tie_mode), ctypes.c_int(stack), _p(ids), _p(d), _p(ovf), _p(vis))
+        return ids, d, ovf.astype(bool), vis
+
+    def knn(self, nodes, prims, points, queries, k, maxSqr=np.inf, fma_mode=1, tie_mode=0, stack=64):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros((nq, k), dtype=np.int32)
+        d = np.zeros((nq, k), dtype=np.float32)
+        nf = np.zeros(nq, dtype=np.int32)
+        ovf = np.zeros(nq, dtype=np.uint8)
+        self.lib.orc_knn(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), _p(points), _p(queries),
+                         ctypes.c_uint32(nq), ctypes.c_int(k), ctypes.c_float(maxSqr), ctypes.c_int(fma_mode),
+                         ctypes.c_int(tie_mode), ctypes.c_int(stack), _p(ids), _p(d), _p(nf), _p(ovf))
+        return ids, d, nf, ovf.astype(bool)
+
+    def sqr_pp(self, p, q, fma_mode):
+        f = self.lib.orc_sqr_pp
+        f.restype = ctypes.c_float
+        p, q = _f32(p), _f32(q)
+        return np.array([f(_p(p[i]), _p(q[i]), ctypes.c_int(fma_mode)) for i in range(len(p))], dtype=np.float32)
+
+    def sqr_pbox(self, q, boxes, fma_mode):
+        f = self.lib.orc_sqr_pbox
+        f.restype = ctypes.c_float
+        q, boxes = _f32(q), _f32(boxes)
+        return np.array([f(_p(q[i]), _p(boxes[i, :3].copy()), _p(boxes[i, 3:].copy()), ctypes.c_int(fma_mode))
+                         for i in range(len(q))], dtype=np.float32)
+
+    def tri_closest(self, nodes, prims, tris, verts, queries, maxSqr=np.inf):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        tris = np.ascontiguousarray(tris, dtype=np.int32)
+        verts, queries = _f32(verts), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        P = np.zeros((nq, 3), dtype=np.float32)
+        self.lib.orc_tri_closest(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), _p(tris), _p(verts),
+                                 _p(queries), ctypes.c_uint32(nq), ctypes.c_float(maxSqr), _p(ids), _p(d), _p(P))
+        return ids, d, P
+
+    def tri_brute_f64(self, tris, verts, queries):
+        tris = np.ascontiguousarray(tris, dtype=np.int32)
+        verts, queries = _f32(verts), _f32(queries)
+        nq = queries.shape[0]
+        d = np.zeros(nq, dtype=np.float64)
+        ids = np.zeros(nq, dtype=np.int32)
+        self.lib.orc_tri_brute_f64(_p(tris), _p(verts), ctypes.c_uint32(len(tris)), _p(queries), ctypes.c_uint32(nq),
+                                   _p(d), _p(ids))
+        return d, ids
+
+    def tri_grad_f64(self, tris, verts, queries, ids, grad_sqr):
+        tris = np.ascontiguousarray(tris, dtype=np.int32)
+        verts, queries = _f32(verts), _f32(queries)
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        g = _f32(grad_sqr)
+        nq = queries.shape[0]
+        gq = np.zeros((nq, 3), dtype=np.float64)
+        gv = np.zeros((verts.shape[0], 3), dtype=np.float64)
+        self.lib.orc_tri_grad_f64(_p(tris), _p(verts), _p(queries), ctypes.c_uint32(nq), _p(ids), _p(g), _p(gq),
+                                  _p(gv))
+        return gq, gv
+
+    def tri_cp_f64(self, a, b, c, p):
+        f = self.lib.orc_tri_cp_f64
+        f.restype = ctypes.c_double
+        arr = [np.ascontiguousarray(x, dtype=np.float64) for x in (a, b, c, p)]
+        w = np.zeros(3, dtype=np.float64)
+        d = f(*[_p(x) for x in arr], _p(w))
+        return d, w
+
+
+# ---------------------------------------------------------------------------
+# the reference itself
+# ---------------------------------------------------------------------------
+class RefCPU:
+    def __init__(self):
+        self.lib = _load(REF_CPU_SO)
+
+    def build(self, boxes, makeLeafThreshold=0):
+        boxes = _f32(boxes).reshape(-1, 6)
+        n = boxes.shape[0]
+        nodes = np.zeros(2 * n + 2, dtype=NODE)
+        prims = np.zeros(max(n, 1), dtype=np.uint32)
+        nn, npr = ctypes.c_uint32(), ctypes.c_uint32()
+        self.lib.ref_cpu_build(_p(boxes), ctypes.c_uint32(n), ctypes.c_int(makeLeafThreshold), _p(nodes), _p(prims),
+                               ctypes.byref(nn), ctypes.byref(npr))
+        return nodes[: nn.value].copy(), prims[: npr.value].copy()
+
+    def build_throughput(self, boxes, makeLeafThreshold, threads, reps):
+        """Wall seconds for `threads` concurrent builds, `reps` each."""
+        boxes = _f32(boxes).reshape(-1, 6)
+        sec = ctypes.c_double()
+        self.lib.ref_cpu_build_throughput(_p(boxes), ctypes.c_uint32(boxes.shape[0]), ctypes.c_int(makeLeafThreshold),
+                                          ctypes.c_int(threads), ctypes.c_int(reps), ctypes.byref(sec))
+        return sec.value
+
+    def closest_point(self, nodes, prims, points, queries, maxSqr=np.inf, threads=1):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        self.lib.ref_cpu_closest(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), ctypes.c_uint32(len(prims)),
+                                 _p(points), _p(queries), ctypes.c_uint32(nq), ctypes.c_float(maxSqr), _p(ids), _p(d),
+                                 ctypes.c_int(threads))
+        return ids, d
+
+    def knn(self, nodes, prims, points, queries, k, maxSqr=np.inf, threads=1):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros((nq, k), dtype=np.int32)
+        d = np.zeros((nq, k), dtype=np.float32)
+        nf = np.zeros(nq, dtype=np.int32)
+        self.lib.ref_cpu_knn(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), ctypes.c_uint32(len(prims)),
+                             _p(points), _p(queries), ctypes.c_uint32(nq), ctypes.c_int(k), ctypes.c_float(maxSqr),
+                             _p(ids), _p(d), _p(nf), ctypes.c_int(threads))
+        return ids, d, nf
+
+    def tri_closest(self, nodes, prims, tris, verts, queries, maxSqr=np.inf, threads=1):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        tris = np.ascontiguousarray(tris, dtype=np.int32)
+        verts, queries = _f32(verts), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        P = np.zeros((nq, 3), dtype=np.float32)
+        self.lib.ref_cpu_tri_closest(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), ctypes.c_uint32(len(prims)),
+                                     _p(tris), ctypes.c_uint32(len(tris)), _p(verts), _p(queries), ctypes.c_uint32(nq),
+                                     ctypes.c_float(maxSqr), _p(ids), _p(d), _p(P), ctypes.c_int(threads))
+        return ids, d, P
+
+
+class RefGPU:
+    """The reference's GPU code (runs only where a GPU is present)."""
+    RADIX, SPATIAL_MEDIAN, REBIN = 0, 1, 2
+
+    def __init__(self):
+        self.lib = _load(REF_GPU_SO)
+
+    def build(self, method, boxes, makeLeafThreshold=0):
+        boxes = _f32(boxes).reshape(-1, 6)
+        n = boxes.shape[0]
+        nodes = np.zeros(2 * n + 2, dtype=NODE)
+        prims = np.zeros(max(n, 1), dtype=np.uint32)
+        nn, npr = ctypes.c_uint32(), ctypes.c_uint32()
+        rc = self.lib.ref_gpu_build(ctypes.c_int(method), _p(boxes), ctypes.c_uint32(n),
+                                    ctypes.c_int(makeLeafThreshold), _p(nodes), _p(prims), ctypes.byref(nn),
+                                    ctypes.byref(npr))
+        assert rc == 0, "reference GPU build failed"
+        return nodes[: nn.value].copy(), prims[: npr.value].copy()
+
+    def closest_point(self, nodes, prims, points, queries, maxSqr=np.inf):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        rc = self.lib.ref_gpu_closest(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), ctypes.c_uint32(len(prims)),
+                                      _p(points), ctypes.c_uint32(len(points)), _p(queries), ctypes.c_uint32(nq),
+                                      ctypes.c_float(maxSqr), _p(ids), _p(d))
+        assert rc == 0
+        return ids, d
+
+    def knn(self, nodes, prims, points, queries, k, maxSqr=np.inf):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros((nq, k), dtype=np.int32)
+        d = np.zeros((nq, k), dtype=np.float32)
+        nf = np.zeros(nq, dtype=np.int32)
+        rc = self.lib.ref_gpu_knn(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), ctypes.c_uint32(len(prims)),
+                                  _p(points), ctypes.c_uint32(len(points)), _p(queries), ctypes.c_uint32(nq),
+                                  ctypes.c_int(k), ctypes.c_float(maxSqr), _p(ids), _p(d), _p(nf))
+        assert rc == 0
+        return ids, d, nf
+
+    def tri_closest(self, nodes, prims, tris, verts, queries, maxSqr=np.inf):
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        tris = np.ascontiguousarray(tris, dtype=np.int32)
+        verts, queries = _f32(verts), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        P = np.zeros((nq, 3), dtype=np.float32)
+        rc = self.lib.ref_gpu_tri_closest(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims),
+                                          ctypes.c_uint32(len(prims)), _p(tris), ctypes.c_uint32(len(tris)), _p(verts),
+                                          _p(queries), ctypes.c_uint32(nq), ctypes.c_float(maxSqr), _p(ids), _p(d),
+                                          _p(P))
+        assert rc == 0
+        return ids, d, P
+
+    def pin(self, a, b, boxes):
+        a, b, boxes = _f32(a), _f32(b), _f32(boxes)
+        n = len(a)
+        pp = np.zeros(n, dtype=np.float32)
+        pb = np.zeros(n, dtype=np.float32)
+        rc = self.lib.ref_gpu_pin(_p(a), _p(b), _p(boxes), ctypes.c_uint32(n), _p(pp), _p(pb))
+        assert rc == 0
+        return pp, pb
+
+    def time_build(self, method, points, makeLeafThreshold=0, reps=5):
+        points = _f32(points)
+        ms = ctypes.c_float()
+        rc = self.lib.ref_gpu_time_build(ctypes.c_int(method), _p(points), ctypes.c_uint32(len(points)),
+                                         ctypes.c_int(makeLeafThreshold), ctypes.c_int(reps), ctypes.byref(ms))
+        assert rc == 0
+        return ms.value
+
+    def time_query(self, method, points, queries, kind, makeLeafThreshold=0, reps=5):
+        points, queries = _f32(points), _f32(queries)
+        ms = ctypes.c_float()
+        rc = self.lib.ref_gpu_time_query(ctypes.c_int(method), _p(points), ctypes.c_uint32(len(points)),
+                                         ctypes.c_int(makeLeafThreshold), _p(queries), ctypes.c_uint32(len(queries)),
+                                         ctypes.c_int(kind), ctypes.c_int(reps), ctypes.byref(ms))
+        assert rc == 0
+        return ms.value
+
+
+# ---------------------------------------------------------------------------
+# structural invariants (testing/bvh/checkBuilders.cu:64-108)
+# ---------------------------------------------------------------------------
+def check_tree(nodes, prims, boxes, max_leaf=None, expect_prims=None, node1_unused=True):
+    """Raises AssertionError unless: node 0 is the root, every valid prim
+    is reached exactly once through the leaves, every node box equals the
+    exact union of its children's (or prims') boxes, leaf counts respect
+    max_leaf, and offsets stay in range."""
+    boxes = np.asarray(boxes, dtype=np.float32).reshape(-1, 6)
+    nn = len(nodes)
+    if nn == 0:
+        assert expect_prims in (None, 0)
+        return
+    off, cnt = offsets(nodes), counts(nodes)
+    seen = np.zeros(len(boxes), dtype=np.int64)
+    stack = [0]
+    visited = 0
+    while stack:
+        i = stack.pop()
+        visited += 1
+        assert not (node1_unused and i == 1), "node 1 must be unused"
+        lo, hi = nodes["lower"][i], nodes["upper"][i]
+        if cnt[i]:
+            assert max_leaf is None or cnt[i] <= max_leaf, f"leaf {i} has {cnt[i]} prims"
+            assert off[i] + cnt[i] <= len(prims)
+            ids = prims[off[i]: off[i] + cnt[i]]
+            seen[ids] += 1
+            b = boxes[ids]
+            assert np.array_equal(lo, b[:, :3].min(0)) and np.array_equal(hi, b[:, 3:].max(0)), f"leaf {i} box"
+        else:
+            c = off[i]
+            assert (2 if node1_unused else 1) <= c and c + 1 < nn, f"inner node {i} child offset {c}"
+            stack += [c, c + 1]
+            assert np.array_equal(lo, np.minimum(nodes["lower"][c], nodes["lower"][c + 1])), f"node {i} lower"
+            assert np.array_equal(hi, np.maximum(nodes["upper"][c], nodes["upper"][c + 1])), f"node {i} upper"
+        assert visited <= nn, "cycle"
+    valid = ~(boxes[:, 0] > boxes[:, 3])
+    assert np.all(seen[valid] == 1), "every valid prim exactly once"
+    assert np.all(seen[~valid] == 0), "no empty prim in a leaf"
+    if expect_prims is not None:
+        assert int(seen.sum()) == expect_prims

@@ -1,0 +1,315 @@
+// ref_gpu.cu -- C entry points over the reference library's own GPU code.
+//
+// TEST / BASELINE INFRASTRUCTURE ONLY.  Compiled by oracle/build_ref.sh
+// with nvcc for sm_100a directly against the unmodified reference headers
+// (never copied into this repository) into oracle/_ref/libref_gpu.so.
+// The parity tests use it as the ground truth the CUDA library must match
+// bit for bit; the comparison benchmark times it as "the reference's
+// generic kernels compiled for sm_100a".
+//
+// All entry points take and return HOST arrays and manage device memory
+// themselves, except the timing functions, which report CUDA-event times.
+//
+// Reference code wrapped here:
+//   cuBQL::gpuBuilder           cuBQL/builder/cuda/gpu_builder.h:31-67
+//   cuBQL::cuda::radixBuilder   cuBQL/builder/cuda/radix.h:760-771
+//   cuBQL::cuda::rebinRadixBuilder cuBQL/builder/cuda/rebinMortonBuilder.h:1478-1487
+//   points::findClosest / findKNN, triangles::findClosest (device functions,
+//   launched one thread per query as testing/points/closestPoint.cu:37-58)
+#define CUBQL_GPU_BUILDER_IMPLEMENTATION 1
+#include "cuBQL/bvh.h"
+#include "cuBQL/builder/cuda/radix.h"
+#include "cuBQL/builder/cuda/rebinMortonBuilder.h"
+#include "cuBQL/queries/points/findClosest.h"
+#include "cuBQL/queries/points/knn.h"
+#include "cuBQL/queries/triangles/findClosest.h"
+
+#include <cstdio>
+#include <vector>
+
+using namespace cuBQL;
+
+#define RCHECK(x)                                                                  \
+  do {                                                                             \
+    cudaError_t e_ = (x);                                                          \
+    if (e_ != cudaSuccess) {                                                       \
+      fprintf(stderr, "ref_gpu: %s failed: %s\n", #x, cudaGetErrorString(e_));     \
+      return -1;                                                                   \
+    }                                                                              \
+  } while (0)
+
+namespace {
+template <typename T>
+T *dalloc_copy(const T *h, size_t n)
+{
+  T *d = nullptr;
+  if (cudaMalloc((void **)&d, sizeof(T) * (n ? n : 1)) != cudaSuccess) return nullptr;
+  if (n && h) cudaMemcpy(d, h, sizeof(T) * n, cudaMemcpyHostToDevice);
+  return d;
+}
+
+struct DeviceTree {
+  bvh3f bvh;
+  int upload(const void *nodes, uint32_t numNodes, const uint32_t *primIDs, uint32_t numPrims)
+  {
+    bvh.nodes = (bvh3f::Node *)dalloc_copy((const char *)nodes, sizeof(bvh3f::Node) * (size_t)numNodes);
+    bvh.primIDs = dalloc_copy(primIDs, numPrims);
+    bvh.numNodes = numNodes;
+    bvh.numPrims = numPrims;
+    return (bvh.nodes && bvh.primIDs) ? 0 : -1;
+  }
+  ~DeviceTree()
+  {
+    cudaFree(bvh.nodes);
+    cudaFree(bvh.primIDs);
+  }
+};
+
+__global__ void k_closest(bvh3f bvh, const vec3f *pts, const vec3f *qs, int nq, float maxSqr, int *ids,
+                          float *dists)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= nq) return;
+  int id = points::findClosest(bvh, pts, qs[tid], maxSqr);
+  ids[tid] = id;
+  dists[tid] = id < 0 ? INFINITY : fSqrDistance_rd(pts[id], qs[tid]);
+}
+
+template <int KMAX>
+__global__ void k_knn(bvh3f bvh, const vec3f *pts, const vec3f *qs, int nq, int k, float maxSqr, int *ids,
+                      float *dists, int *numFound)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= nq) return;
+  knn::Candidate c[KMAX];
+  knn::Result r = points::findKNN(c, k, bvh, pts, qs[tid], maxSqr);
+  for (int j = 0; j < k; j++) {
+    ids[(size_t)tid * k + j] = j < r.numFound ? c[j].primID : -1;
+    dists[(size_t)tid * k + j] = j < r.numFound ? c[j].sqrDist : INFINITY;
+  }
+  numFound[tid] = r.numFound;
+}
+
+__global__ void k_tri(bvh3f bvh, const Triangle *tris, const vec3f *qs, int nq, float maxSqr, int *ids,
+                      float *dists, vec3f *P)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= nq) return;
+  triangles::FCPResult r;
+  r.clear(maxSqr);
+  r.P = vec3f(0.f, 0.f, 0.f);
+  triangles::findClosest(r, bvh, tris, qs[tid]);
+  ids[tid] = r.primID;
+  dists[tid] = r.primID < 0 ? INFINITY : r.sqrDist;
+  P[tid] = r.P;
+}
+
+__global__ void k_pin(const vec3f *a, const vec3f *b, const box3f *bx, int n, float *pp, float *pbox)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= n) return;
+  pp[tid] = fSqrDistance_rd(a[tid], b[tid]);
+  pbox[tid] = shrinkingRadiusQuery::fSqrDistance_rd(a[tid], bx[tid]);
+}
+
+__global__ void k_points_to_boxes(const vec3f *pts, box3f *boxes, int n)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= n) return;
+  boxes[tid] = box3f().including(pts[tid]);
+}
+
+int run_build(int method, const box3f *d_boxes, uint32_t n, int leafThr, bvh3f &bvh)
+{
+  BuildConfig cfg;
+  cfg.makeLeafThreshold = leafThr;
+  if (method == 0)
+    cuBQL::cuda::radixBuilder(bvh, d_boxes, n, cfg);
+  else if (method == 1)
+    gpuBuilder(bvh, d_boxes, n, cfg);
+  else
+    cuBQL::cuda::rebinRadixBuilder(bvh, d_boxes, n, cfg);
+  return 0;
+}
+} // namespace
+
+extern "C" {
+
+int ref_gpu_node_size(void) { return (int)sizeof(bvh3f::Node); }
+
+// method: 0 radixBuilder, 1 gpuBuilder (spatial median), 2 rebinRadixBuilder.
+// nodesOut must hold 2n+2 nodes, primIDsOut n entries.
+int ref_gpu_build(int method, const float *boxes, uint32_t n, int makeLeafThreshold, void *nodesOut,
+                  uint32_t *primIDsOut, uint32_t *numNodes, uint32_t *numPrims)
+{
+  box3f *d_boxes = dalloc_copy((const box3f *)boxes, n);
+  if (!d_boxes) return -1;
+  bvh3f bvh;
+  run_build(method, d_boxes, n, makeLeafThreshold, bvh);
+  RCHECK(cudaDeviceSynchronize());
+  *numNodes = bvh.numNodes;
+  *numPrims = bvh.numPrims;
+  if (bvh.numNodes) RCHECK(cudaMemcpy(nodesOut, bvh.nodes, sizeof(bvh3f::Node) * bvh.numNodes, cudaMemcpyDeviceToHost));
+  if (bvh.numPrims) RCHECK(cudaMemcpy(primIDsOut, bvh.primIDs, sizeof(uint32_t) * bvh.numPrims, cudaMemcpyDeviceToHost));
+  if (bvh.numNodes) cuBQL::cuda::free(bvh);
+  cudaFree(d_boxes);
+  return 0;
+}
+
+int ref_gpu_closest(const void *nodes, uint32_t numNodes, const uint32_t *primIDs, uint32_t numPrims,
+                    const float *points, uint32_t np, const float *queries, uint32_t nq, float maxSqr, int32_t *ids,
+                    float *dists)
+{
+  DeviceTree t;
+  if (t.upload(nodes, numNodes, primIDs, numPrims)) return -1;
+  vec3f *dp = dalloc_copy((const vec3f *)points, np), *dq = dalloc_copy((const vec3f *)queries, nq);
+  int *di = dalloc_copy<int>(nullptr, nq);
+  float *dd = dalloc_copy<float>(nullptr, nq);
+  k_closest<<<(nq + 127) / 128, 128>>>(t.bvh, dp, dq, (int)nq, maxSqr, di, dd);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(ids, di, sizeof(int) * nq, cudaMemcpyDeviceToHost);
+  cudaMemcpy(dists, dd, sizeof(float) * nq, cudaMemcpyDeviceToHost);
+  cudaFree(dp); cudaFree(dq); cudaFree(di); cudaFree(dd);
+  return 0;
+}
+
+int ref_gpu_knn(const void *nodes, uint32_t numNodes, const uint32_t *primIDs, uint32_t numPrims,
+                const float *points, uint32_t np, const float *queries, uint32_t nq, int k, float maxSqr,
+                int32_t *ids, float *dists, int32_t *numFound)
+{
+  if (k < 1 || k > 64) return -1;
+  DeviceTree t;
+  if (t.upload(nodes, numNodes, primIDs, numPrims)) return -1;
+  vec3f *dp = dalloc_copy((const vec3f *)points, np), *dq = dalloc_copy((const vec3f *)queries, nq);
+  int *di = dalloc_copy<int>(nullptr, (size_t)nq * k), *dn = dalloc_copy<int>(nullptr, nq);
+  float *dd = dalloc_copy<float>(nullptr, (size_t)nq * k);
+  if (k <= 16)
+    k_knn<16><<<(nq + 127) / 128, 128>>>(t.bvh, dp, dq, (int)nq, k, maxSqr, di, dd, dn);
+  else
+    k_knn<64><<<(nq + 127) / 128, 128>>>(t.bvh, dp, dq, (int)nq, k, maxSqr, di, dd, dn);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(ids, di, sizeof(int) * nq * k, cudaMemcpyDeviceToHost);
+  cudaMemcpy(dists, dd, sizeof(float) * nq * k, cudaMemcpyDeviceToHost);
+  cudaMemcpy(numFound, dn, sizeof(int) * nq, cudaMemcpyDeviceToHost);
+  cudaFree(dp); cudaFree(dq); cudaFree(di); cudaFree(dd); cudaFree(dn);
+  return 0;
+}
+
+int ref_gpu_tri_closest(const void *nodes, uint32_t numNodes, const uint32_t *primIDs, uint32_t numPrims,
+                        const int32_t *tris, uint32_t nt, const float *verts, const float *queries, uint32_t nq,
+                        float maxSqr, int32_t *ids, float *dists, float *P)
+{
+  DeviceTree t;
+  if (t.upload(nodes, numNodes, primIDs, numPrims)) return -1;
+  std::vector<Triangle> T(nt);
+  const vec3f *V = (const vec3f *)verts;
+  for (uint32_t i = 0; i < nt; i++) {
+    T[i].a = V[tris[3 * i + 0]];
+    T[i].b = V[tris[3 * i + 1]];
+    T[i].c = V[tris[3 * i + 2]];
+  }
+  Triangle *dt = dalloc_copy(T.data(), nt);
+  vec3f *dq = dalloc_copy((const vec3f *)queries, nq), *dP = dalloc_copy<vec3f>(nullptr, nq);
+  int *di = dalloc_copy<int>(nullptr, nq);
+  float *dd = dalloc_copy<float>(nullptr, nq);
+  k_tri<<<(nq + 127) / 128, 128>>>(t.bvh, dt, dq, (int)nq, maxSqr, di, dd, dP);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(ids, di, sizeof(int) * nq, cudaMemcpyDeviceToHost);
+  cudaMemcpy(dists, dd, sizeof(float) * nq, cudaMemcpyDeviceToHost);
+  if (P) cudaMemcpy(P, dP, sizeof(vec3f) * nq, cudaMemcpyDeviceToHost);
+  cudaFree(dt); cudaFree(dq); cudaFree(dP); cudaFree(di); cudaFree(dd);
+  return 0;
+}
+
+// The two distance expressions the reference's device code uses, evaluated
+// by the reference's own functions, to pin their FMA contraction.
+int ref_gpu_pin(const float *a, const float *b, const float *boxes, uint32_t n, float *pp, float *pbox)
+{
+  vec3f *da = dalloc_copy((const vec3f *)a, n), *db = dalloc_copy((const vec3f *)b, n);
+  box3f *dbx = dalloc_copy((const box3f *)boxes, n);
+  float *d1 = dalloc_copy<float>(nullptr, n), *d2 = dalloc_copy<float>(nullptr, n);
+  k_pin<<<(n + 127) / 128, 128>>>(da, db, dbx, (int)n, d1, d2);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(pp, d1, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  cudaMemcpy(pbox, d2, sizeof(float) * n, cudaMemcpyDeviceToHost);
+  cudaFree(da); cudaFree(db); cudaFree(dbx); cudaFree(d1); cudaFree(d2);
+  return 0;
+}
+
+// Times the reference's GPU builders on point boxes already resident in
+// device memory: one warm-up build, then `reps` builds, CUDA events around
+// each (the builders' own host syncs included, as a user sees them).
+// ms_out receives the mean build time.
+int ref_gpu_time_build(int method, const float *points, uint32_t n, int makeLeafThreshold, int reps,
+                       float *ms_out)
+{
+  vec3f *dp = dalloc_copy((const vec3f *)points, n);
+  box3f *db = dalloc_copy<box3f>(nullptr, n);
+  if (!dp || !db) return -1;
+  k_points_to_boxes<<<(n + 127) / 128, 128>>>(dp, db, (int)n);
+  RCHECK(cudaDeviceSynchronize());
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float total = 0.f;
+  for (int r = -1; r < reps; r++) {
+    bvh3f bvh;
+    cudaEventRecord(e0);
+    run_build(method, db, n, makeLeafThreshold, bvh);
+    cudaEventRecord(e1);
+    RCHECK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r >= 0) total += ms;
+    cuBQL::cuda::free(bvh);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(dp);
+  cudaFree(db);
+  *ms_out = total / (reps > 0 ? reps : 1);
+  return 0;
+}
+
+// Times one-thread-per-query reference kernels over a tree built with
+// `method` on the points: kind 0 closest point, kind k>0 kNN with that k.
+int ref_gpu_time_query(int method, const float *points, uint32_t n, int makeLeafThreshold, const float *queries,
+                       uint32_t nq, int kind, int reps, float *ms_out)
+{
+  vec3f *dp = dalloc_copy((const vec3f *)points, n), *dq = dalloc_copy((const vec3f *)queries, nq);
+  box3f *db = dalloc_copy<box3f>(nullptr, n);
+  int k = kind > 0 ? kind : 1;
+  int *di = dalloc_copy<int>(nullptr, (size_t)nq * k), *dn = dalloc_copy<int>(nullptr, nq);
+  float *dd = dalloc_copy<float>(nullptr, (size_t)nq * k);
+  if (!dp || !dq || !db || !di || !dn || !dd) return -1;
+  k_points_to_boxes<<<(n + 127) / 128, 128>>>(dp, db, (int)n);
+  bvh3f bvh;
+  run_build(method, db, n, makeLeafThreshold, bvh);
+  RCHECK(cudaDeviceSynchronize());
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float total = 0.f;
+  for (int r = -1; r < reps; r++) {
+    cudaEventRecord(e0);
+    if (kind == 0)
+      k_closest<<<(nq + 127) / 128, 128>>>(bvh, dp, dq, (int)nq, INFINITY, di, dd);
+    else if (k <= 16)
+      k_knn<16><<<(nq + 127) / 128, 128>>>(bvh, dp, dq, (int)nq, k, INFINITY, di, dd, dn);
+    else
+      k_knn<64><<<(nq + 127) / 128, 128>>>(bvh, dp, dq, (int)nq, k, INFINITY, di, dd, dn);
+    cudaEventRecord(e1);
+    RCHECK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r >= 0) total += ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cuBQL::cuda::free(bvh);
+  cudaFree(dp); cudaFree(dq); cudaFree(db); cudaFree(di); cudaFree(dn); cudaFree(dd);
+  *ms_out = total / (reps > 0 ? reps : 1);
+  return 0;
+}
+
+} // extern "C"

@@ -1,0 +1,102 @@
+"""Writes the golden fixtures of tests/golden/ from the reference itself.
+
+  python tests/golden/make_golden.py cpu   # here: the reference's host code
+  python tests/golden/make_golden.py gpu   # on a B200: the reference's GPU
+                                           # builders and query kernels
+
+Both read oracle/_ref/ (the reference compiled from its own sources by
+oracle/build_ref.sh).  Inputs are the seeded generators of
+cubql_b200.workloads; trees are stored after BFS renumbering
+(orc_canonicalize), because the reference's GPU builders number nodes in a
+run-dependent order.
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from cubql_b200 import workloads as W  # noqa: E402
+from oracle.oracle import Oracle  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def inputs():
+    p = W.uniform_points(3000)
+    q = W.uniform_points(600, W.SEED_QUERIES, -0.1, 1.1)
+    g = W.gmm_points(3000)
+    gq = W.gmm_points(600, seed=W.SEED_GMM + 100)
+    verts, tris = W.icosphere(2)
+    tq = W.uniform_points(400, W.SEED_QUERIES, -1.5, 1.5)
+    return p, q, g, gq, verts, tris, tq
+
+
+def cpu():
+    from oracle.oracle import RefCPU
+    r = RefCPU()
+    p, q, g, gq, verts, tris, tq = inputs()
+    out = {}
+    for name, pts, qs in (("u", p, q), ("g", g, gq)):
+        b = W.point_boxes(pts)
+        for thr in (0, 8):
+            n, pr = r.build(b, thr)
+            out[f"{name}_cpu{thr}_nodes"] = n.view(np.uint8)
+            out[f"{name}_cpu{thr}_prims"] = pr
+        n, pr = r.build(b, 8)
+        ids, d = r.closest_point(n, pr, pts, qs)
+        out[f"{name}_cp_ids"], out[f"{name}_cp_d"] = ids, d
+        for k in (5, 16):
+            ki, kd, kn = r.knn(n, pr, pts, qs, k)
+            out[f"{name}_knn{k}_ids"], out[f"{name}_knn{k}_d"], out[f"{name}_knn{k}_n"] = ki, kd, kn
+    tb = np.stack([verts[tris].min(1), verts[tris].max(1)], 1).reshape(-1, 6)
+    n, pr = r.build(tb, 4)
+    ids, d, P = r.tri_closest(n, pr, tris, verts, tq)
+    out["tri_nodes"], out["tri_prims"] = n.view(np.uint8), pr
+    out["tri_ids"], out["tri_d"], out["tri_P"] = ids, d, P
+    np.savez_compressed(os.path.join(HERE, "ref_cpu.npz"), **out)
+
+
+def gpu():
+    from oracle.oracle import RefGPU
+    r = RefGPU()
+    o = Oracle()
+    p, q, g, gq, verts, tris, tq = inputs()
+    out = {}
+    for name, pts, qs in (("u", p, q), ("g", g, gq)):
+        b = W.point_boxes(pts)
+        for method, mname in ((RefGPU.RADIX, "radix"), (RefGPU.SPATIAL_MEDIAN, "sm")):
+            for thr in (0, 8):
+                n, pr = r.build(method, b, thr)
+                cn, cp = o.canonicalize(n, pr)
+                out[f"{name}_{mname}{thr}_nodes"] = cn.view(np.uint8)
+                out[f"{name}_{mname}{thr}_prims"] = cp
+        n, pr = r.build(RefGPU.RADIX, b, 0)
+        ids, d = r.closest_point(n, pr, pts, qs)
+        out[f"{name}_cp_ids"], out[f"{name}_cp_d"] = ids, d
+        ki, kd, kn = r.knn(n, pr, pts, qs, 16)
+        out[f"{name}_knn16_ids"], out[f"{name}_knn16_d"], out[f"{name}_knn16_n"] = ki, kd, kn
+        cn, cp = o.canonicalize(n, pr)
+        out[f"{name}_querytree_nodes"], out[f"{name}_querytree_prims"] = cn.view(np.uint8), cp
+    # FMA shape of the two distance expressions
+    a = W.uniform_points(4096, 5, -2, 2)
+    bb = W.uniform_points(4096, 6, -2, 2)
+    lo = W.uniform_points(4096, 7, -1, 1)
+    hi = lo + np.abs(W.uniform_points(4096, 8, 0, 1))
+    boxes = np.concatenate([lo, hi], 1)
+    pp, pb = r.pin(a, bb, boxes)
+    out["pin_a"], out["pin_b"], out["pin_boxes"], out["pin_pp"], out["pin_pbox"] = a, bb, boxes, pp, pb
+    tb = np.stack([verts[tris].min(1), verts[tris].max(1)], 1).reshape(-1, 6)
+    n, pr = r.build(RefGPU.RADIX, tb, 0)
+    ids, d, P = r.tri_closest(n, pr, tris, verts, tq)
+    cn, cp = o.canonicalize(n, pr)
+    out["tri_nodes"], out["tri_prims"] = cn.view(np.uint8), cp
+    out["tri_ids"], out["tri_d"], out["tri_P"] = ids, d, P
+    dest = sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu.npz")
+    np.savez_compressed(dest, **out)
+
+
+if __name__ == "__main__":
+    {"cpu": cpu, "gpu": gpu}[sys.argv[1]]()

@@ -1,0 +1,160 @@
+"""Builders on the GPU against the oracle and the reference's own GPU
+builders.  Morton trees must be identical node for node (after BFS
+renumbering); spatial-median trees must satisfy the reference's structural
+invariants and equal the oracle's canonical tree."""
+import numpy as np
+import pytest
+import torch
+
+from cubql_b200 import workloads as W
+from oracle.oracle import check_tree
+from tests.helpers import boxes_np, same_tree
+
+pytestmark = pytest.mark.gpu
+
+
+def _dist(dist, n):
+    if dist == "uniform" or dist == "invalid":
+        return W.uniform_points(n)
+    if dist == "gmm":
+        return W.gmm_points(n)
+    if dist == "dupes":
+        return np.repeat(W.uniform_points(max(n // 10, 1)), 10, axis=0)[:n]
+    if dist == "line":  # all on one axis-aligned line: degenerate centroid boxes
+        p = np.zeros((n, 3), np.float32)
+        p[:, 0] = W.uniform_points(n)[:, 0]
+        return p
+    raise ValueError(dist)
+
+
+def _boxes(dist, n):
+    b = boxes_np(_dist(dist, n))
+    if dist == "invalid":
+        b[::5, 0] = 2.0
+        b[::5, 3] = 1.0
+    return b
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 17, 1000, 4096, 65537])
+@pytest.mark.parametrize("dist", ["uniform", "gmm", "dupes", "invalid", "line"])
+def test_morton_matches_oracle(bq, oracle, n, dist):
+    b = _boxes(dist, n)
+    bvh = bq.cuda.radixBuilder(torch.from_numpy(b).cuda())
+    gn, gp = bvh.to_host()
+    on, op = oracle.radix_build(b)
+    assert bvh.numNodes == len(on) and bvh.numPrims == len(op)
+    ok, msg = same_tree(oracle, gn, gp, on, op)
+    assert ok, msg
+    bvh.free()
+
+
+@pytest.mark.parametrize("thr", [2, 3, 8, 33])
+@pytest.mark.parametrize("dist", ["uniform", "gmm", "dupes"])
+def test_morton_leaf_threshold_matches_oracle(bq, oracle, thr, dist):
+    b = _boxes(dist, 20000)
+    bvh = bq.cuda.radixBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=thr))
+    gn, gp = bvh.to_host()
+    on, op = oracle.radix_build(b, thr)
+    ok, msg = same_tree(oracle, gn, gp, on, op)
+    assert ok, msg
+    check_tree(gn, gp, b, max_leaf=thr)
+
+
+@pytest.mark.parametrize("dist", ["uniform", "gmm"])
+def test_morton_matches_reference_gpu_builder(bq, oracle, ref_gpu, dist):
+    b = _boxes(dist, 200000)
+    for thr in (0, 8):
+        bvh = bq.cuda.radixBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=thr))
+        gn, gp = bvh.to_host()
+        rn, rp = ref_gpu.build(ref_gpu.RADIX, b, thr)
+        ok, msg = same_tree(oracle, gn, gp, rn, rp)
+        assert ok, f"thr {thr}: {msg}"
+
+
+def test_morton_full_size_10m(bq, oracle):
+    """The benchmark workload itself: 10M uniform points, leaf 1."""
+    b = boxes_np(W.uniform_points(10_000_000))
+    bvh = bq.cuda.radixBuilder(torch.from_numpy(b).cuda())
+    gn, gp = bvh.to_host()
+    on, op = oracle.radix_build(b)
+    assert len(gn) == 20_000_000
+    ok, msg = same_tree(oracle, gn, gp, on, op)
+    assert ok, msg
+
+
+def test_morton_is_deterministic(bq):
+    b = torch.from_numpy(_boxes("gmm", 300000)).cuda()
+    a = bq.cuda.radixBuilder(b).to_host()
+    c = bq.cuda.radixBuilder(b).to_host()
+    assert a[0].tobytes() == c[0].tobytes() and np.array_equal(a[1], c[1])
+
+
+def test_empty_and_all_invalid(bq):
+    bvh = bq.cuda.radixBuilder(torch.zeros((0, 6), dtype=torch.float32, device="cuda"))
+    assert bvh.numNodes == 0 and bvh.numPrims == 0
+    b = _boxes("uniform", 100)
+    b[:, 0] = 2.0
+    b[:, 3] = 1.0
+    bvh = bq.cuda.radixBuilder(torch.from_numpy(b).cuda())
+    assert bvh.numNodes == 0 and bvh.numPrims == 0
+    bvh = bq.gpuBuilder(torch.from_numpy(b).cuda())
+    assert bvh.numNodes == 0
+
+
+@pytest.mark.parametrize("thr", [0, 1, 8])
+@pytest.mark.parametrize("dist", ["uniform", "gmm", "dupes", "invalid", "line"])
+def test_spatial_median_invariants_and_oracle(bq, oracle, thr, dist):
+    b = _boxes(dist, 30000)
+    bvh = bq.gpuBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=thr))
+    gn, gp = bvh.to_host()
+    valid = ~(b[:, 0] > b[:, 3])
+    assert bvh.numPrims == len(b)
+    check_tree(gn, gp[: valid.sum()], b, max_leaf=max(thr, 1))
+    assert np.array_equal(np.sort(gp[valid.sum():]), np.nonzero(~valid)[0])
+    on, op = oracle.sm_build(b, thr)
+    ok, msg = same_tree(oracle, gn, gp[: valid.sum()], on, op[: valid.sum()])
+    assert ok, msg
+
+
+def test_spatial_median_matches_reference_gpu_builder(bq, oracle, ref_gpu):
+    """Tie-free input: the reference's tree is determined, ours must equal it."""
+    b = _boxes("uniform", 200000)
+    for thr in (0, 8):
+        bvh = bq.gpuBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=thr))
+        gn, gp = bvh.to_host()
+        rn, rp = ref_gpu.build(ref_gpu.SPATIAL_MEDIAN, b, thr)
+        ok, msg = same_tree(oracle, gn, gp, rn, rp)
+        assert ok, f"thr {thr}: {msg}"
+
+
+def test_spatial_median_reference_invariants_on_degenerate_input(bq, oracle, ref_gpu):
+    """Where the reference itself is racy (dim == -1 nodes) both trees pass
+    the invariants and have the same number of nodes."""
+    b = _boxes("dupes", 50000)
+    bvh = bq.gpuBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=8))
+    gn, gp = bvh.to_host()
+    rn, rp = ref_gpu.build(ref_gpu.SPATIAL_MEDIAN, b, 8)
+    check_tree(gn, gp, b, max_leaf=8)
+    check_tree(rn, rp, b, max_leaf=8)
+    assert len(gn) == len(rn)
+
+
+def test_spatial_median_full_size_10m(bq, oracle):
+    b = boxes_np(W.uniform_points(10_000_000))
+    bvh = bq.gpuBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=8))
+    gn, gp = bvh.to_host()
+    on, op = oracle.sm_build(b, 8)
+    ok, msg = same_tree(oracle, gn, gp, on, op)
+    assert ok, msg
+
+
+@pytest.mark.parametrize("builder", ["morton", "sm"])
+def test_refit_after_moving_prims(bq, oracle, builder):
+    pts = W.uniform_points(50000)
+    b = torch.from_numpy(boxes_np(pts)).cuda()
+    bvh = bq.cuda.radixBuilder(b, bq.BuildConfig(makeLeafThreshold=4)) if builder == "morton" else \
+        bq.gpuBuilder(b, bq.BuildConfig(makeLeafThreshold=4))
+    moved = boxes_np(pts + np.float32(0.01) * W.uniform_points(50000, 99, -1, 1))
+    bq.refit(bvh, torch.from_numpy(moved).cuda())
+    gn, gp = bvh.to_host()
+    check_tree(gn, gp, moved, max_leaf=4)

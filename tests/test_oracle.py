@@ -1,0 +1,211 @@
+"""CPU-only checks: the oracle (C restatement) against the reference's own
+outputs (golden fixtures made by tests/golden/make_golden.py from the
+reference compiled from its sources), plus the oracle's own invariants."""
+import os
+
+import numpy as np
+import pytest
+
+from cubql_b200 import workloads as W
+from oracle.oracle import NODE, check_tree
+from tests.helpers import boxes_np, fp64_closest, same_tree, tri_boxes_np
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _load(name):
+    path = os.path.join(GOLD, name)
+    if not os.path.exists(path):
+        pytest.skip(f"{name} not generated")
+    return np.load(path)
+
+
+def test_generator_matches_c_restatement(oracle):
+    for seed, lo, hi in ((W.SEED_DATA, 0.0, 1.0), (W.SEED_QUERIES, -0.1, 1.1), (3, -1.5, 1.5)):
+        a = W.uniform_points(5000, seed, lo, hi)
+        b = oracle.uniform_points(5000, seed, lo, hi)
+        assert np.array_equal(a, b)
+
+
+def test_cpu_builder_matches_reference(oracle):
+    g = _load("ref_cpu.npz")
+    p, q, gp, gq, verts, tris, tq = _inputs()
+    for name, pts in (("u", p), ("g", gp)):
+        for thr in (0, 8):
+            n, pr = oracle.cpu_build(boxes_np(pts), thr)
+            assert n.view(np.uint8).tobytes() == g[f"{name}_cpu{thr}_nodes"].tobytes()
+            assert np.array_equal(pr, g[f"{name}_cpu{thr}_prims"])
+
+
+def _inputs():
+    p = W.uniform_points(3000)
+    q = W.uniform_points(600, W.SEED_QUERIES, -0.1, 1.1)
+    g = W.gmm_points(3000)
+    gq = W.gmm_points(600, seed=W.SEED_GMM + 100)
+    verts, tris = W.icosphere(2)
+    tq = W.uniform_points(400, W.SEED_QUERIES, -1.5, 1.5)
+    return p, q, g, gq, verts, tris, tq
+
+
+def test_host_queries_match_reference(oracle):
+    """Reference host build (no FMA on x86-64) + reference traversal rules."""
+    g = _load("ref_cpu.npz")
+    p, q, gp, gq, *_ = _inputs()
+    for name, pts, qs in (("u", p, q), ("g", gp, gq)):
+        n = g[f"{name}_cpu8_nodes"].view(NODE)
+        pr = g[f"{name}_cpu8_prims"]
+        ids, d, ovf, _ = oracle.closest_point(n, pr, pts, qs, fma_mode=0, tie_mode=1)
+        assert not ovf.any()
+        assert np.array_equal(ids, g[f"{name}_cp_ids"]) and np.array_equal(d, g[f"{name}_cp_d"])
+        for k in (5, 16):
+            ki, kd, kn, _ = oracle.knn(n, pr, pts, qs, k, fma_mode=0, tie_mode=1)
+            assert np.array_equal(ki, g[f"{name}_knn{k}_ids"])
+            assert np.array_equal(kd, g[f"{name}_knn{k}_d"])
+            assert np.array_equal(kn, g[f"{name}_knn{k}_n"])
+
+
+def test_host_triangles_match_reference(oracle):
+    g = _load("ref_cpu.npz")
+    *_, verts, tris, tq = _inputs()
+    n = g["tri_nodes"].view(NODE)
+    ids, d, P = oracle.tri_closest(n, g["tri_prims"], tris, verts, tq)
+    assert np.array_equal(ids, g["tri_ids"])
+    assert np.array_equal(d, g["tri_d"])
+    assert np.array_equal(P, g["tri_P"])
+
+
+def test_gpu_reference_trees_match_oracle(oracle):
+    """Pins the Morton and spatial-median restatements on the reference's
+    GPU builders (fixtures produced on a B200)."""
+    g = _load("ref_gpu.npz")
+    p, q, gp, gq, *_ = _inputs()
+    for name, pts in (("u", p), ("g", gp)):
+        b = boxes_np(pts)
+        for thr in (0, 8):
+            n, pr = oracle.radix_build(b, thr)
+            ok, msg = same_tree(oracle, n, pr, g[f"{name}_radix{thr}_nodes"].view(NODE), g[f"{name}_radix{thr}_prims"])
+            assert ok, f"radix {name} thr {thr}: {msg}"
+    # spatial median: identical wherever no node is degenerate (uniform data)
+    for thr in (0, 8):
+        n, pr = oracle.sm_build(boxes_np(p), thr)
+        ok, msg = same_tree(oracle, n, pr, g[f"u_sm{thr}_nodes"].view(NODE), g[f"u_sm{thr}_prims"])
+        assert ok, f"spatial median thr {thr}: {msg}"
+
+
+def test_gpu_reference_distance_contraction(oracle):
+    """The FMA shapes the oracle uses for fma_mode=1 equal what nvcc made of
+    the reference's two distance expressions on a B200."""
+    g = _load("ref_gpu.npz")
+    assert np.array_equal(oracle.sqr_pp(g["pin_a"], g["pin_b"], 1), g["pin_pp"])
+    assert np.array_equal(oracle.sqr_pbox(g["pin_a"], g["pin_boxes"], 1), g["pin_pbox"])
+
+
+def test_gpu_reference_queries_match_oracle(oracle):
+    g = _load("ref_gpu.npz")
+    p, q, gp, gq, *_ = _inputs()
+    for name, pts, qs in (("u", p, q), ("g", gp, gq)):
+        n = g[f"{name}_querytree_nodes"].view(NODE)
+        pr = g[f"{name}_querytree_prims"]
+        ids, d, ovf, _ = oracle.closest_point(n, pr, pts, qs, fma_mode=1, tie_mode=1)
+        assert not ovf.any()
+        assert np.array_equal(ids, g[f"{name}_cp_ids"]) and np.array_equal(d, g[f"{name}_cp_d"])
+        ki, kd, kn, _ = oracle.knn(n, pr, pts, qs, 16, fma_mode=1, tie_mode=1)
+        assert np.array_equal(ki, g[f"{name}_knn16_ids"]) and np.array_equal(kd, g[f"{name}_knn16_d"])
+        assert np.array_equal(kn, g[f"{name}_knn16_n"])
+
+
+@pytest.mark.parametrize("thr", [0, 1, 3, 8])
+@pytest.mark.parametrize("dist", ["uniform", "gmm", "dupes", "invalid"])
+def test_radix_oracle_invariants(oracle, thr, dist):
+    pts = _dist(dist, 4000)
+    b = boxes_np(pts)
+    if dist == "invalid":
+        b[::7, 0] = 2.0
+        b[::7, 3] = 1.0
+    n, pr = oracle.radix_build(b, thr)
+    check_tree(n, pr, b, max_leaf=max(thr, 1))
+
+
+@pytest.mark.parametrize("thr", [0, 1, 8])
+@pytest.mark.parametrize("dist", ["uniform", "gmm", "dupes", "invalid"])
+def test_spatial_median_oracle_invariants(oracle, thr, dist):
+    pts = _dist(dist, 4000)
+    b = boxes_np(pts)
+    if dist == "invalid":
+        b[::7, 0] = 2.0
+        b[::7, 3] = 1.0
+    n, pr = oracle.sm_build(b, thr)
+    valid = ~(b[:, 0] > b[:, 3])
+    check_tree(n, pr[: valid.sum()], b, max_leaf=max(thr, 1))
+
+
+def _dist(dist, n):
+    if dist == "uniform" or dist == "invalid":
+        return W.uniform_points(n)
+    if dist == "gmm":
+        return W.gmm_points(n)
+    pts = W.uniform_points(n // 10)
+    return np.repeat(pts, 10, axis=0)  # every point ten times
+
+
+def test_edge_sizes(oracle):
+    for n in (1, 2, 3, 5):
+        b = boxes_np(W.uniform_points(n))
+        nr, pr = oracle.radix_build(b)
+        assert len(nr) == 2 * n and sorted(pr.tolist()) == list(range(n))
+        check_tree(nr, pr, b, max_leaf=1)
+        ns, ps = oracle.sm_build(b)
+        check_tree(ns, ps, b, max_leaf=1)
+    nr, pr = oracle.radix_build(np.zeros((0, 6), np.float32))
+    assert len(nr) == 0 and len(pr) == 0
+
+
+def test_lowest_id_rule_is_tree_independent(oracle):
+    pts = W.gmm_points(4000)
+    qs = W.gmm_points(500, seed=123)
+    b = boxes_np(pts)
+    a = oracle.knn(*oracle.radix_build(b), pts, qs, 8, tie_mode=0)
+    c = oracle.knn(*oracle.sm_build(b, 8), pts, qs, 8, tie_mode=0)
+    d = oracle.knn(*oracle.cpu_build(b, 3), pts, qs, 8, tie_mode=0)
+    for x in (c, d):
+        assert np.array_equal(a[0], x[0]) and np.array_equal(a[1], x[1])
+
+
+def test_closest_within_fp64(oracle):
+    pts = W.uniform_points(5000)
+    qs = W.uniform_points(700, W.SEED_QUERIES, -0.1, 1.1)
+    ids, d, _, _ = oracle.closest_point(*oracle.radix_build(boxes_np(pts)), pts, qs)
+    d64, i64 = fp64_closest(pts, qs)
+    assert np.all(np.abs(d - d64) <= 1e-6 * d64 + 1e-30)
+
+
+def test_canonicalize_idempotent(oracle):
+    b = boxes_np(W.uniform_points(3000))
+    c1 = oracle.canonicalize(*oracle.radix_build(b, 4))
+    c2 = oracle.canonicalize(*c1)
+    assert c1[0].tobytes() == c2[0].tobytes() and np.array_equal(c1[1], c2[1])
+
+
+def test_adjoint_formula_matches_finite_differences(oracle):
+    """FP64 analytic gradient of the point-to-triangle squared distance
+    against FP64 central differences (tolerance 1e-5 relative)."""
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        a, b, c = rng.normal(size=(3, 3))
+        p = rng.normal(size=3) * 1.5
+        d0, w = oracle.tri_cp_f64(a, b, c, p)
+        X = w[0] * a + w[1] * b + w[2] * c
+        gq = 2 * (p - X)
+        h = 1e-6
+        fd = np.zeros(3)
+        for i in range(3):
+            e = np.zeros(3)
+            e[i] = h
+            fd[i] = (oracle.tri_cp_f64(a, b, c, p + e)[0] - oracle.tri_cp_f64(a, b, c, p - e)[0]) / (2 * h)
+        assert np.allclose(gq, fd, rtol=1e-5, atol=1e-7)
+        fa = np.zeros(3)
+        for i in range(3):
+            e = np.zeros(3)
+            e[i] = h
+            fa[i] = (oracle.tri_cp_f64(a + e, b, c, p)[0] - oracle.tri_cp_f64(a - e, b, c, p)[0]) / (2 * h)
+        assert np.allclose(-w[0] * gq, fa, rtol=1e-5, atol=1e-6)
