@@ -65,6 +65,14 @@ __device__ __forceinline__ uint64_t ldg_admin(const Node *p)
   return ((uint64_t)__float_as_uint(b.w) << 32) | __float_as_uint(b.z);
 }
 
+// In TIE_LOWEST mode node distances are compared against the cull radius
+// widened by 2^-20 relative: a node box distance and the distance to a
+// point inside it are rounded differently (each carries a few ulp of
+// error), so without the slack a node holding an equally close point with
+// a lower id could be culled by one ulp.  The slack only adds visits; the
+// answer is decided by the exact per-prim comparisons.
+__device__ __forceinline__ float lowest_slack(float c) { return __fmaf_rn(c, 0x1p-20f, c); }
+
 // Leaf functor contract: float operator()(uint64_t offset, uint32_t count)
 // processes primIDs[offset .. offset+count) and returns the new cull
 // radius proposal.  Returns false if the stack overflowed (the query then
@@ -83,7 +91,8 @@ __device__ __forceinline__ bool traverse(const Node *__restrict__ nodes, float q
       const float d0 = sqr_pbox(qx, qy, qz, n0.a.x, n0.a.y, n0.a.z, n0.a.w, n0.b.x, n0.b.y);
       const float d1 = sqr_pbox(qx, qy, qz, n1.a.x, n1.a.y, n1.a.z, n1.a.w, n1.b.x, n1.b.y);
       const float dmin = fminf(d0, d1), dmax = fmaxf(d0, d1);
-      if (TIE == TIE_REFERENCE ? (dmin >= cull) : (dmin > cull)) {
+      const float cs = TIE == TIE_REFERENCE ? cull : lowest_slack(cull);
+      if (TIE == TIE_REFERENCE ? (dmin >= cull) : (dmin > cs)) {
         dead = true;
         break;
       }
@@ -95,7 +104,7 @@ __device__ __forceinline__ bool traverse(const Node *__restrict__ nodes, float q
         admin = node_admin(n1);
         farID = (uint32_t)off;
       }
-      if (TIE == TIE_REFERENCE ? (dmax < cull) : (dmax <= cull)) {
+      if (TIE == TIE_REFERENCE ? (dmax < cull) : (dmax <= cs)) {
         if (!stack.push(farID, dmax)) return false;
       }
     }
@@ -103,7 +112,7 @@ __device__ __forceinline__ bool traverse(const Node *__restrict__ nodes, float q
     while (true) {
       if (stack.empty()) return true;
       const StackEntry e = stack.pop();
-      if (e.dist <= cull) {
+      if (e.dist <= (TIE == TIE_REFERENCE ? cull : lowest_slack(cull))) {
         admin = ldg_admin(nodes + e.idx);
         break;
       }

@@ -630,6 +630,11 @@ static float knn_visit(knn_state *s, uint32_t pid)
 
 typedef struct { uint32_t idx; float dist; } stk_e;
 
+/* tie_mode 0 compares node distances against the radius widened by 2^-20
+   relative (node-box and point distances round differently); only the
+   set of visited nodes changes, never the answer */
+static float lowest_slack(float c) { return fmaf(c, 0x1p-20f, c); }
+
 static void traverse(const onode *nodes, const uint32_t *primIDs, const float *q, float maxSqr,
                      knn_state *s, int stackLimit, int *overflow, uint32_t *visitedNodes)
 {
@@ -648,12 +653,13 @@ static void traverse(const onode *nodes, const uint32_t *primIDs, const float *q
       float d0 = sqr_pbox(q, n0->lo, n0->hi, s->fma_mode);
       float d1 = sqr_pbox(q, n1->lo, n1->hi, s->fma_mode);
       float dmin = fminf(d0, d1), dmax = fmaxf(d0, d1);
-      int dead = tie == 1 ? (dmin >= cull) : (dmin > cull);
+      float cs = tie == 1 ? cull : lowest_slack(cull);
+      int dead = tie == 1 ? (dmin >= cull) : (dmin > cs);
       if (dead) { admin = 0; break; }
       uint32_t farID;
       if (d0 < d1) { admin = n0->admin; farID = i1; }
       else { admin = n1->admin; farID = i0; }
-      int both = tie == 1 ? (dmax < cull) : (dmax <= cull);
+      int both = tie == 1 ? (dmax < cull) : (dmax <= cs);
       if (both) {
         if (sp >= (size_t)stackLimit && !*overflow) *overflow = 1;
         if (sp == cap) { cap *= 2; stack = (stk_e *)realloc(stack, sizeof(stk_e) * cap); }
@@ -674,7 +680,7 @@ static void traverse(const onode *nodes, const uint32_t *primIDs, const float *q
     for (;;) {
       if (sp == 0) { free(stack); return; }
       stk_e e = stack[--sp];
-      if (e.dist <= cull) { admin = nodes[e.idx].admin; break; }
+      if (e.dist <= (tie == 1 ? cull : lowest_slack(cull))) { admin = nodes[e.idx].admin; break; }
     }
   }
 }
@@ -728,12 +734,13 @@ int orc_closest_point(const onode *nodes, uint32_t numNodes, const uint32_t *pri
           float d0 = sqr_pbox(q, n0->lo, n0->hi, fma_mode);
           float d1 = sqr_pbox(q, n1->lo, n1->hi, fma_mode);
           float dmin = fminf(d0, d1), dmax = fmaxf(d0, d1);
-          int dead = tie_mode == 1 ? (dmin >= cull) : (dmin > cull);
+          float cs = tie_mode == 1 ? cull : lowest_slack(cull);
+          int dead = tie_mode == 1 ? (dmin >= cull) : (dmin > cs);
           if (dead) { admin = 0; break; }
           uint32_t farID;
           if (d0 < d1) { admin = n0->admin; farID = i1; }
           else { admin = n1->admin; farID = i0; }
-          int both = tie_mode == 1 ? (dmax < cull) : (dmax <= cull);
+          int both = tie_mode == 1 ? (dmax < cull) : (dmax <= cs);
           if (both) {
             if (sp >= (size_t)stackLimit) of = 1;
             if (sp == cap) { cap *= 2; stack = (stk_e *)realloc(stack, sizeof(stk_e) * cap); }
@@ -757,7 +764,7 @@ int orc_closest_point(const onode *nodes, uint32_t numNodes, const uint32_t *pri
         int popped = 0;
         while (sp) {
           stk_e e = stack[--sp];
-          if (e.dist <= cull) { admin = nodes[e.idx].admin; popped = 1; break; }
+          if (e.dist <= (tie_mode == 1 ? cull : lowest_slack(cull))) { admin = nodes[e.idx].admin; popped = 1; break; }
         }
         if (!popped) break;
       }

@@ -14,13 +14,21 @@ def tri_boxes_np(verts, tris):
     return np.concatenate([v.min(1), v.max(1)], 1).astype(np.float32)
 
 
-def same_tree(oracle, a_nodes, a_prims, b_nodes, b_prims):
-    """Bit-exact equality after BFS renumbering (node 1 ignored)."""
+def same_tree(oracle, a_nodes, a_prims, b_nodes, b_prims, boxes=None):
+    """Bit-exact equality after BFS renumbering (node 1 ignored).  With
+    `boxes`, leaf prim sequences are compared through the prims' boxes, so
+    identical prims may trade places (the reference's spatial-median
+    builder sends identical prims to either side in atomic order)."""
     ca, pa = oracle.canonicalize(a_nodes, a_prims)
     cb, pb = oracle.canonicalize(b_nodes, b_prims)
     if len(ca) != len(cb):
         return False, f"node count {len(ca)} != {len(cb)}"
-    if not np.array_equal(pa, pb):
+    if boxes is not None:
+        bx = np.asarray(boxes, dtype=np.float32).reshape(-1, 6)
+        same = np.array_equal(bx[pa], bx[pb]) and np.array_equal(np.sort(pa), np.sort(pb))
+    else:
+        same = np.array_equal(pa, pb)
+    if not same:
         return False, f"leaf prim sequences differ at {np.nonzero(pa != pb)[0][:5]}"
     ca, cb = ca.copy(), cb.copy()
     if len(ca) > 1:

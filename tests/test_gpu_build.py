@@ -117,13 +117,16 @@ def test_spatial_median_invariants_and_oracle(bq, oracle, thr, dist):
 
 
 def test_spatial_median_matches_reference_gpu_builder(bq, oracle, ref_gpu):
-    """Tie-free input: the reference's tree is determined, ours must equal it."""
+    """Uniform input: the reference's tree is determined up to the order of
+    exactly identical prims (the seeded generator repeats a point whenever
+    two indices get the same TEA seed, ~5 pairs per 200K points, and the
+    reference deals identical prims to the two sides in atomic order)."""
     b = _boxes("uniform", 200000)
     for thr in (0, 8):
         bvh = bq.gpuBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=thr))
         gn, gp = bvh.to_host()
         rn, rp = ref_gpu.build(ref_gpu.SPATIAL_MEDIAN, b, thr)
-        ok, msg = same_tree(oracle, gn, gp, rn, rp)
+        ok, msg = same_tree(oracle, gn, gp, rn, rp, boxes=b)
         assert ok, f"thr {thr}: {msg}"
 
 
