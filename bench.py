@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_POINTS)
     ap.add_argument("--no-components", action="store_true")
+    ap.add_argument("--only-build", action="store_true",
+                    help="time the build loop only (no profile pass, e2e, components or CPU leg): "
+                         "the short program the ncu captures run")
     return ap.parse_args()
 
 
@@ -358,6 +361,14 @@ def run_ours(args):
     clk = clocks.stop()
     ms_max = max_over_ranks(ms, world)
     value = world * n / ms_max / 1e3  # Mprims/s
+    if args.only_build:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "Mprims/s", "ms_per_step": ms_max,
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "only_build": True}))
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
 
     # per-phase breakdown of the same step (library events on its stream)
     with bq.profile() as prof:

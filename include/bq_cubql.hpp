@@ -1,0 +1,159 @@
+// bq_cubql.hpp -- drop-in C++ front end with cuBQL's own call signatures.
+//
+// Include this after (or instead of) the cuBQL builder header and call the
+// functions in namespace bq_cubql the way cuBQL's are called; the work runs
+// in libbq.so (include/bq.h).  The functions are templates over the
+// caller's types, so cuBQL's headers are not needed to compile this file,
+// but the types must have cuBQL's layout (checked by static_assert):
+//
+//   BinaryBVH<float,3>   {Node *nodes; uint32 numNodes; uint32 *primIDs;
+//                         uint32 numPrims}, Node = 32 bytes   (cuBQL/bvh.h:71-111)
+//   box_t<float,3>       24 bytes                              (cuBQL/math/box.h:60-179)
+//   BuildConfig          {int maxAllowedLeafSize, makeLeafThreshold, buildMethod}
+//                                                              (cuBQL/bvh.h:31-64)
+//   GpuMemoryResource    virtual malloc(void**, size_t, cudaStream_t),
+//                        virtual free(void*, cudaStream_t)     (cuBQL/builder/cuda.h:31-78)
+//
+// Error behaviour follows the reference: a failing call reports the
+// message and raises SIGINT (cuBQL/math/common.h:134-149) unless
+// BQ_CUBQL_THROW is defined, in which case it throws std::runtime_error.
+#pragma once
+
+#include <cuda_runtime_api.h>
+
+#include <csignal>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include "bq.h"
+
+namespace bq_cubql {
+
+inline void check(int status, const char *what)
+{
+  if (status == BQ_OK) return;
+  std::string msg = std::string(what) + ": " + bq_last_error_string();
+#ifdef BQ_CUBQL_THROW
+  throw std::runtime_error(msg);
+#else
+  std::fprintf(stderr, "%s\n", msg.c_str());
+  std::raise(SIGINT);
+#endif
+}
+
+// bq_allocator that forwards to a cuBQL GpuMemoryResource
+template <class MemRes>
+struct ResourceAdapter {
+  static int mallocFn(void *ctx, void **ptr, size_t size, bq_stream_t s)
+  {
+    return static_cast<MemRes *>(ctx)->malloc(ptr, size, (cudaStream_t)s) == cudaSuccess ? 0 : 1;
+  }
+  static int freeFn(void *ctx, void *ptr, bq_stream_t s)
+  {
+    return static_cast<MemRes *>(ctx)->free(ptr, (cudaStream_t)s) == cudaSuccess ? 0 : 1;
+  }
+  static bq_allocator make(MemRes &m) { return bq_allocator{&m, &mallocFn, &freeFn}; }
+};
+
+template <class BVH>
+inline bq_bvh3f to_c(const BVH &b)
+{
+  static_assert(sizeof(typename BVH::Node) == 32, "BinaryBVH<float,3>::Node layout");
+  return bq_bvh3f{(bq_node3f *)b.nodes, b.numNodes, b.primIDs, b.numPrims};
+}
+
+template <class BVH>
+inline void from_c(BVH &b, const bq_bvh3f &c)
+{
+  b.nodes = (typename BVH::Node *)c.nodes;
+  b.numNodes = c.numNodes;
+  b.primIDs = c.primIDs;
+  b.numPrims = c.numPrims;
+}
+
+template <class Cfg>
+inline bq_build_config to_c_cfg(const Cfg &c)
+{
+  return bq_build_config{c.maxAllowedLeafSize, c.makeLeafThreshold, (int)c.buildMethod};
+}
+
+/*! cuBQL::gpuBuilder (cuBQL/builder/cuda.h:91-99): spatial median */
+template <class BVH, class Box, class Cfg, class MemRes>
+inline void gpuBuilder(BVH &bvh, const Box *boxes, uint32_t numBoxes, Cfg cfg, cudaStream_t s, MemRes &mem)
+{
+  static_assert(sizeof(Box) == 24, "box_t<float,3> layout");
+  bq_bvh3f c{};
+  bq_build_config cc = to_c_cfg(cfg);
+  bq_allocator a = ResourceAdapter<MemRes>::make(mem);
+  check(bq_build_spatial_median_f3(&c, (const bq_box3f *)boxes, numBoxes, &cc, &a, s), "gpuBuilder");
+  from_c(bvh, c);
+}
+
+namespace cuda {
+/*! cuBQL::cuda::radixBuilder (cuBQL/builder/cuda.h:134-140) */
+template <class BVH, class Box, class Cfg, class MemRes>
+inline void radixBuilder(BVH &bvh, const Box *boxes, uint32_t numPrims, Cfg cfg, cudaStream_t s, MemRes &mem)
+{
+  static_assert(sizeof(Box) == 24, "box_t<float,3> layout");
+  bq_bvh3f c{};
+  bq_build_config cc = to_c_cfg(cfg);
+  bq_allocator a = ResourceAdapter<MemRes>::make(mem);
+  check(bq_build_morton63_f3(&c, (const bq_box3f *)boxes, numPrims, &cc, &a, s), "radixBuilder");
+  from_c(bvh, c);
+}
+
+/*! cuBQL::cuda::free (cuBQL/builder/cuda.h:158-161) */
+template <class BVH, class MemRes>
+inline void free(BVH &bvh, cudaStream_t s, MemRes &mem)
+{
+  bq_bvh3f c = to_c(bvh);
+  bq_allocator a = ResourceAdapter<MemRes>::make(mem);
+  check(bq_free_f3(&c, &a, s), "free");
+  cudaStreamSynchronize(s);  // cuda::free synchronises (gpu_builder.h:86)
+  from_c(bvh, c);
+}
+} // namespace cuda
+
+/*! gpuBuilder_impl::refit (cuBQL/builder/cuda/sm_builder.h:677-693) */
+template <class BVH, class Box, class MemRes>
+inline void refit(BVH &bvh, const Box *boxes, cudaStream_t s, MemRes &mem)
+{
+  bq_bvh3f c = to_c(bvh);
+  bq_allocator a = ResourceAdapter<MemRes>::make(mem);
+  check(bq_refit_f3(&c, (const bq_box3f *)boxes, &a, s), "refit");
+}
+
+namespace points {
+/*! batched cuBQL::points::findClosest: one call for all queries; ids -1
+    where nothing is strictly closer than maxSqrDist.  Ties go to the
+    lowest primID unless tieMode is BQ_TIES_REFERENCE. */
+template <class BVH, class Vec>
+inline void findClosest(const BVH &bvh, const Vec *points, const Vec *queries, uint32_t numQueries, int32_t *ids,
+                        float *sqrDist, float maxSqrDist = INFINITY, cudaStream_t s = 0,
+                        int tieMode = BQ_TIES_LOWEST_ID)
+{
+  static_assert(sizeof(Vec) == 12, "vec3f layout");
+  bq_bvh3f c = to_c(bvh);
+  bq_query_config q{tieMode, 0, 0, 1, 0};
+  check(bq_closest_point_f3(&c, (const float *)points, (const float *)queries, numQueries, maxSqrDist, &q, ids,
+                            sqrDist, nullptr, s),
+        "findClosest");
+}
+
+/*! batched cuBQL::points::findKNN; ids/sqrDist are numQueries*k */
+template <class BVH, class Vec>
+inline void findKNN(const BVH &bvh, const Vec *points, const Vec *queries, uint32_t numQueries, int k, int32_t *ids,
+                    float *sqrDist, int32_t *numFound, float maxSqrDist = INFINITY, cudaStream_t s = 0,
+                    int tieMode = BQ_TIES_LOWEST_ID)
+{
+  static_assert(sizeof(Vec) == 12, "vec3f layout");
+  bq_bvh3f c = to_c(bvh);
+  bq_query_config q{tieMode, 0, 0, 1, 0};
+  check(bq_knn_f3(&c, (const float *)points, (const float *)queries, numQueries, k, maxSqrDist, &q, ids, sqrDist,
+                  numFound, nullptr, s),
+        "findKNN");
+}
+} // namespace points
+
+} // namespace bq_cubql

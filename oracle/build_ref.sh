@@ -19,3 +19,7 @@ mkdir -p "$here/_ref"
 g++ -std=c++17 -O2 -fPIC -shared -I"$REF" -w -o "$here/_ref/libref_cpu.so" "$here/ref_cpu.cpp" -lpthread
 /usr/local/cuda/bin/nvcc -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC -shared \
     -I"$REF" -w -o "$here/_ref/libref_gpu.so" "$here/ref_gpu.cu"
+# drop-in check: the reference's types and query kernel over libbq trees
+/usr/local/cuda/bin/nvcc -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC -shared \
+    -I"$REF" -I"$here/../include" -w -o "$here/_ref/libref_shim.so" "$here/ref_shim.cu" \
+    -L"$here/../cubql_b200" -lbq -Xlinker -rpath -Xlinker '$ORIGIN/../../cubql_b200'

@@ -400,3 +400,31 @@ def check_tree(nodes, prims, boxes, max_leaf=None, expect_prims=None, node1_unus
     assert np.all(seen[~valid] == 0), "no empty prim in a leaf"
     if expect_prims is not None:
         assert int(seen.sum()) == expect_prims
+
+
+REF_SHIM_SO = os.path.join(HERE, "_ref", "libref_shim.so")
+
+
+def have_ref_shim():
+    return os.path.exists(REF_SHIM_SO)
+
+
+class RefShim:
+    """The reference's types and findClosest kernel over trees built through
+    include/bq_cubql.hpp (needs a GPU)."""
+
+    def __init__(self):
+        self.lib = _load(REF_SHIM_SO)
+
+    def compare(self, points, queries):
+        points, queries = _f32(points), _f32(queries)
+        nq = len(queries)
+        ri = np.zeros(nq, np.int32)
+        rd = np.zeros(nq, np.float32)
+        oi = np.zeros(nq, np.int32)
+        od = np.zeros(nq, np.float32)
+        nn = np.zeros(2, np.uint32)
+        rc = self.lib.ref_shim_compare(_p(points), ctypes.c_uint32(len(points)), _p(queries), ctypes.c_uint32(nq),
+                                       _p(ri), _p(rd), _p(oi), _p(od), _p(nn))
+        assert rc == 0
+        return ri, rd, oi, od, nn
