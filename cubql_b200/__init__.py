@@ -83,6 +83,7 @@ _SIGS = {
     "bq_build_spatial_median_f3": [ctypes.POINTER(bq_bvh3f), _P, _U, ctypes.POINTER(bq_build_config),
                                    ctypes.POINTER(bq_allocator), _P],
     "bq_refit_f3": [ctypes.POINTER(bq_bvh3f), _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_refit_noalloc_f3": [ctypes.POINTER(bq_bvh3f), _P, _P],
     "bq_free_f3": [ctypes.POINTER(bq_bvh3f), ctypes.POINTER(bq_allocator), _P],
     "bq_closest_point_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _F, ctypes.POINTER(bq_query_config), _P, _P,
                             ctypes.POINTER(bq_allocator), _P],

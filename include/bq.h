@@ -123,6 +123,20 @@ int bq_build_spatial_median_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t nu
    gpuBuilder_impl::refit (cuBQL/builder/cuda/sm_builder.h:677-693). */
 int bq_refit_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_allocator *alloc, bq_stream_t stream);
 
+/* bq_refit_f3 without any device allocation (no counterpart in the
+   reference).  For callers that may not allocate device memory when they
+   refit: an application that reserved all GPU memory for its own pool up
+   front, a real-time loop where cudaMalloc could stall or fail mid-frame,
+   or a framework that only permits allocation during its set-up.  Its
+   scratch (two words per node) is one fixed array inside the library,
+   sized for BQ_NOALLOC_REFIT_MAX_NODES nodes (8 MiB held on every GPU that
+   loads the library until exit).  Larger trees are rejected with
+   BQ_ERR_INVALID_ARGUMENT.  The first call on a device looks up the
+   array's address; make it before any stream capture.  All calls share
+   the array: calls that overlap on the GPU race, so serialise them. */
+#define BQ_NOALLOC_REFIT_MAX_NODES (1u << 20)
+int bq_refit_noalloc_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, bq_stream_t stream);
+
 /* Frees a tree built by this library.  Replaces cuBQL::cuda::free
    (cuBQL/builder/cuda.h:158-161, cuBQL/builder/cuda/gpu_builder.h:79-90). */
 int bq_free_f3(bq_bvh3f *bvh, const bq_allocator *alloc, bq_stream_t stream);
