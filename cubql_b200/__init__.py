@@ -68,6 +68,11 @@ class bq_allocator(ctypes.Structure):
     _fields_ = [("ctx", ctypes.c_void_p), ("malloc", MALLOC_FN), ("free", FREE_FN)]
 
 
+class bq_tuning(ctypes.Structure):
+    _fields_ = [("makeLeafThreshold", ctypes.c_int), ("stackDepth", ctypes.c_int), ("blockSize", ctypes.c_int),
+                ("queriesPerWarp", ctypes.c_int), ("buildMs", ctypes.c_float), ("queryMs", ctypes.c_float)]
+
+
 class bq_query_config(ctypes.Structure):
     _fields_ = [("tieMode", ctypes.c_int), ("stackDepth", ctypes.c_int), ("blockSize", ctypes.c_int),
                 ("reorder", ctypes.c_int), ("queriesPerWarp", ctypes.c_int)]
@@ -92,6 +97,14 @@ _SIGS = {
     "bq_tri_closest_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _P, _U, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
                           ctypes.POINTER(bq_allocator), _P],
     "bq_tri_distance_bwd_f3": [_P, _P, _U, _P, _U, _P, _P, _P, _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_batched_build_morton63_f3": [_P, _P, _U, _U, ctypes.POINTER(bq_build_config), _P, _P, _P, _P,
+                                     ctypes.POINTER(bq_allocator), _P],
+    "bq_batched_knn_f3": [_P, _P, _P, _P, _P, _U, _U, _I, _F, ctypes.POINTER(bq_query_config), _P, _P, _P, _P,
+                          ctypes.POINTER(bq_allocator), _P],
+    "bq_batched_refit_f3": [_P, _P, _U, _U, _P, _P, _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_batched_tri_closest_f3": [_P, _P, _P, _P, _P, _P, _U, _U, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
+                                  _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_autotune_batched_knn_f3": [_P, _P, _P, _U, _U, _P, _P, _U, _I, _P, ctypes.POINTER(bq_allocator), _P],
     "bq_tri_boxes_f3": [_P, _P, _U, _P, _P],
     "bq_points_to_boxes_f3": [_P, _U, _P, _P],
     "bq_last_error_string": [],
@@ -361,6 +374,112 @@ class triangles:
                                            _ptr(gradSqr.contiguous()), _ptr(gq), _ptr(gv), ctypes.byref(allocator.c),
                                            _stream()))
         return gq, gv
+
+
+class Batch:
+    """Many clouds built in one pass (bq_batched_build_morton63_f3).
+
+    `boxes` (N,6) holds the clouds back to back; `offsets` (numSegs+1,)
+    int32/uint32 gives each cloud's first box.  Every cloud's tree equals
+    cuda.radixBuilder on that cloud alone; `tree(s)` views it as a
+    BinaryBVH-like object.  Buffers are torch tensors owned by the batch."""
+
+    def __init__(self, boxes, offsets, config=None, allocator=None, stream_alloc_null=False):
+        boxes = _as_boxes(boxes)
+        self.boxes = boxes
+        self.offsets = offsets.to(device=boxes.device, dtype=torch.int32).contiguous()
+        self.numSegs = self.offsets.numel() - 1
+        n = boxes.shape[0]
+        self.nodes = torch.empty((2 * max(n, 1), 8), dtype=torch.float32, device=boxes.device)
+        self.primIDs = torch.empty(max(n, 1), dtype=torch.int32, device=boxes.device)
+        self.bvhs = torch.empty((max(self.numSegs, 1), 4), dtype=torch.int64, device=boxes.device)
+        self.err = torch.zeros(1, dtype=torch.int32, device=boxes.device)
+        cfg = (config or BuildConfig()).c()
+        alloc = None if stream_alloc_null else ctypes.byref((allocator or default_allocator()).c)
+        _check(_lib.bq_batched_build_morton63_f3(_ptr(boxes), _ptr(self.offsets), self.numSegs, n, ctypes.byref(cfg),
+                                                 _ptr(self.nodes), _ptr(self.primIDs), _ptr(self.bvhs),
+                                                 _ptr(self.err), alloc, _stream()))
+
+    def descriptors(self):
+        """(numNodes, numPrims, nodeOffset, primOffset) per cloud, on the host."""
+        torch.cuda.synchronize()
+        d = self.bvhs.cpu().numpy()
+        nodes_base = self.nodes.data_ptr()
+        prim_base = self.primIDs.data_ptr()
+        out = []
+        for s in range(self.numSegs):
+            p_nodes, nn_np = int(d[s, 0]), int(d[s, 1]) & 0xFFFFFFFF
+            p_prims, npr = int(d[s, 2]), int(d[s, 3]) & 0xFFFFFFFF
+            out.append((nn_np, npr, (p_nodes - nodes_base) // 32 if nn_np else 0,
+                        (p_prims - prim_base) // 4 if npr else 0))
+        return out
+
+    def tree_host(self, s):
+        """(nodes numpy structured array, primIDs uint32) of cloud s."""
+        import numpy as np
+        nn, npr, no, po = self.descriptors()[s]
+        nodes = self.nodes[no: no + nn].cpu().numpy().view(node_dtype()).reshape(-1)
+        prims = self.primIDs[po: po + npr].cpu().numpy().view(np.uint32)
+        return nodes, prims
+
+
+def batched_refit(batch, boxes, allocator=None, stream_alloc_null=False):
+    """bq_batched_refit_f3: refit every tree of `batch` to new boxes."""
+    boxes = _as_boxes(boxes)
+    alloc = None if stream_alloc_null else ctypes.byref((allocator or default_allocator()).c)
+    _check(_lib.bq_batched_refit_f3(_ptr(batch.bvhs), _ptr(batch.offsets), batch.numSegs, boxes.shape[0],
+                                    _ptr(batch.nodes), _ptr(batch.primIDs), _ptr(boxes), alloc, _stream()))
+
+
+def batched_tri_closest(batch, tris, verts, queries, queryOffsets, maxSqrDist=float("inf"), qcfg=None,
+                        allocator=None, stream_alloc_null=False):
+    """bq_batched_tri_closest_f3 over a Batch built on triangle boxes; returns
+    (global triangle ids, sqrDist, P)."""
+    queries = _vec3(queries, "queries")
+    nq = queries.shape[0]
+    ids = torch.empty(nq, dtype=torch.int32, device=queries.device)
+    d = torch.empty(nq, dtype=torch.float32, device=queries.device)
+    P = torch.empty((nq, 3), dtype=torch.float32, device=queries.device)
+    qoff = queryOffsets.to(device=queries.device, dtype=torch.int32).contiguous()
+    q = qcfg or query_config()
+    alloc = None if stream_alloc_null else ctypes.byref((allocator or default_allocator()).c)
+    _check(_lib.bq_batched_tri_closest_f3(_ptr(batch.bvhs), _ptr(batch.offsets), _ptr(tris.contiguous()),
+                                          _ptr(verts.contiguous()), _ptr(queries), _ptr(qoff), batch.numSegs, nq,
+                                          maxSqrDist, ctypes.byref(q), _ptr(ids), _ptr(d), _ptr(P), _ptr(batch.err),
+                                          alloc, _stream()))
+    return ids, d, P
+
+
+def batched_knn(batch, points, pointOffsets, queries, queryOffsets, k, maxSqrDist=float("inf"), qcfg=None,
+                allocator=None, stream_alloc_null=False):
+    """bq_batched_knn_f3: ids are cloud-local.  Returns (ids, sqrDist, numFound)."""
+    points, queries = _vec3(points, "points"), _vec3(queries, "queries")
+    nq = queries.shape[0]
+    ids = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
+    d = torch.empty((nq, k), dtype=torch.float32, device=queries.device)
+    nf = torch.empty(nq, dtype=torch.int32, device=queries.device)
+    poff = pointOffsets.to(device=queries.device, dtype=torch.int32).contiguous()
+    qoff = queryOffsets.to(device=queries.device, dtype=torch.int32).contiguous()
+    q = qcfg or query_config()
+    alloc = None if stream_alloc_null else ctypes.byref((allocator or default_allocator()).c)
+    _check(_lib.bq_batched_knn_f3(_ptr(batch.bvhs), _ptr(poff), _ptr(points), _ptr(queries), _ptr(qoff),
+                                  batch.numSegs, nq, k, maxSqrDist, ctypes.byref(q), _ptr(ids), _ptr(d), _ptr(nf),
+                                  _ptr(batch.err), alloc, _stream()))
+    return ids, d, nf
+
+
+def autotune_batched_knn(boxes, points, offsets, queries, queryOffsets, k):
+    """bq_autotune_batched_knn_f3: the fastest (leaf, stack, block,
+    queriesPerWarp) for this batch; returns a dict."""
+    boxes = _as_boxes(boxes)
+    points, queries = _vec3(points, "points"), _vec3(queries, "queries")
+    off = offsets.to(device=boxes.device, dtype=torch.int32).contiguous()
+    qoff = queryOffsets.to(device=boxes.device, dtype=torch.int32).contiguous()
+    best = bq_tuning()
+    _check(_lib.bq_autotune_batched_knn_f3(_ptr(boxes), _ptr(points), _ptr(off), off.numel() - 1, boxes.shape[0],
+                                           _ptr(queries), _ptr(qoff), queries.shape[0], k, ctypes.byref(best), None,
+                                           _stream()))
+    return {f: getattr(best, f) for f, _ in bq_tuning._fields_}
 
 
 def points_to_boxes(pts):

@@ -1,0 +1,228 @@
+// bq_agglom.cuh -- bottom-up construction of a radix tree and its boxes.
+//
+// Input: sorted prims (ids), and for every adjacent pair (i, i+1) a split
+// level delta[i] (bq_morton.cu explains why the tree built from these
+// levels is the reference radixBuilder's tree).  A node covering sorted
+// positions [l, r] is the child of the split at whichever of its two
+// boundaries carries the lower level; its box is the union of its
+// children's.  Children of split s are stored at nodes[2s], nodes[2s+1]
+// (relative to the node block of the prim range), the root at the block's
+// first node, the block's second node unused.
+//
+// Two kernels:
+//   k_agg_local   one CTA per chunk of AGG_CHUNK sorted prims.  Threads
+//                 start at their leaf and climb; the first child to reach
+//                 a split parks its range end and box in shared memory and
+//                 stops, the second merges and climbs on.  Everything
+//                 below the chunk's boundaries is finished here with
+//                 block-scope synchronisation only.  A node whose parent
+//                 split lies on a chunk boundary is handed to the global
+//                 phase (at most two per chunk); children parked at a split
+//                 whose sibling reaches outside the chunk are published to
+//                 the global slot array.
+//   k_agg_global  one thread per handed-over node continues the climb with
+//                 device-scope acquire/release exchanges on global slots.
+// With SEG, the prims form independent ranges (clouds) [b0, e0); each
+// climb ends at its range's root and never crosses into a neighbour.
+#pragma once
+
+#include <cuda/atomic>
+
+#include "bq_internal.cuh"
+
+namespace bq {
+
+// first index of the run of key a ending at or after position i (keys[i] == a),
+// not before lo: galloping search (runs are short), then binary search
+__device__ __forceinline__ uint32_t run_begin(const uint64_t *__restrict__ keys, uint32_t lo, uint32_t i, uint64_t a)
+{
+  uint32_t step = 1, hi = i;  // keys[hi] == a
+  while (hi > lo) {
+    const uint32_t probe = hi - min(step, hi - lo);
+    if (keys[probe] != a) { lo = probe + 1; break; }
+    hi = probe;
+    step <<= 1;
+  }
+  while (lo < hi) {  // first index in [lo, hi] with key == a
+    const uint32_t m = lo + ((hi - lo) >> 1);
+    if (keys[m] < a) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+// one past the last index of the run of key a (keys[i] == a), at most hi
+__device__ __forceinline__ uint32_t run_end(const uint64_t *__restrict__ keys, uint32_t i, uint32_t hi, uint64_t a)
+{
+  uint32_t step = 1, lo = i + 1;  // keys[lo-1] == a
+  while (lo < hi) {
+    const uint32_t probe = lo - 1 + min(step, hi - lo + 1);
+    if (probe >= hi || keys[probe] != a) { hi = min(probe, hi); break; }
+    lo = probe + 1;
+    step <<= 1;
+  }
+  while (lo < hi) {  // first index in [lo, hi) with key > a
+    const uint32_t m = lo + ((hi - lo) >> 1);
+    if (keys[m] <= a) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+constexpr int AGG_CHUNK = 512;
+constexpr uint32_t AGG_EMPTY = 0xffffffffu;
+
+// prim range of position i: [0, nv) or the cloud containing i
+template <bool SEG>
+__device__ __forceinline__ void agg_range(uint32_t i, uint32_t nv, const uint32_t *__restrict__ off, uint32_t numSegs,
+                                          uint32_t &b0, uint32_t &e0)
+{
+  if (!SEG) {
+    b0 = 0;
+    e0 = nv;
+    return;
+  }
+  uint32_t lo = 0, hi = numSegs;
+  while (hi - lo > 1) {
+    const uint32_t m = (lo + hi) >> 1;
+    if (__ldg(off + m) <= i) lo = m; else hi = m;
+  }
+  b0 = __ldg(off + lo);
+  e0 = __ldg(off + lo + 1);
+}
+
+struct AggBox {
+  float lx, ly, lz, hx, hy, hz;
+};
+
+__device__ __forceinline__ AggBox agg_union(const AggBox &left, const AggBox &right)
+{
+  // min(l,r) / max(l,r) in the reference's operand order (sm_builder.h:669-670)
+  return AggBox{fminf(left.lx, right.lx), fminf(left.ly, right.ly), fminf(left.lz, right.lz),
+                fmaxf(left.hx, right.hx), fmaxf(left.hy, right.hy), fmaxf(left.hz, right.hz)};
+}
+
+struct AggArgs {
+  const uint8_t *delta;   // split level of pair (i, i+1)
+  uint32_t *slot;         // global slots, AGG_EMPTY on entry
+  const uint32_t *ids;    // sorted prim ids (global indices)
+  const bq_box3f *boxes;
+  Node *nodes;            // output (full tree layout)
+  uint32_t *primIDsOut;   // SEG: cloud-local prim ids are written here
+  const uint32_t *nvPtr;  // number of sorted prims
+  uint2 *ranges;          // optional: [l, r] of every split's node
+  uint2 *pending;         // 2 per chunk: nodes handed to the global phase
+  const uint32_t *off;    // SEG: cloud offsets
+  uint32_t numSegs;
+};
+
+template <bool SEG>
+__global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgs a)
+{
+  __shared__ uint32_t sSlot[AGG_CHUNK + 1];
+  __shared__ AggBox sBox[AGG_CHUNK + 1][2];
+  const uint32_t nv = *a.nvPtr;
+  const uint32_t c0 = blockIdx.x * AGG_CHUNK;
+  if (c0 >= nv) return;  // whole CTA: no barrier below is skipped by part of it
+  const uint32_t cEnd = c0 + AGG_CHUNK;  // first split position outside the chunk
+  for (int j = threadIdx.x; j <= AGG_CHUNK; j += blockDim.x) sSlot[j] = AGG_EMPTY;
+  if (threadIdx.x < 2) a.pending[2 * blockIdx.x + threadIdx.x] = make_uint2(AGG_EMPTY, AGG_EMPTY);
+  __syncthreads();
+  const uint32_t i = c0 + threadIdx.x;
+  if (i < nv) {
+    uint32_t b0, e0;
+    agg_range<SEG>(i, nv, a.off, a.numSegs, b0, e0);
+    const uint64_t nodeBase = SEG ? 2ull * b0 : 0ull;
+    const uint32_t id = __ldg(a.ids + i);
+    if (SEG) a.primIDsOut[i] = id - b0;
+    if (i == b0) a.nodes[nodeBase + 1] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0);
+    const float2 *bp = reinterpret_cast<const float2 *>(a.boxes + id);
+    const float2 p0 = __ldg(bp), p1 = __ldg(bp + 1), p2 = __ldg(bp + 2);
+    AggBox box{p0.x, p0.y, p1.x, p1.y, p2.x, p2.y};
+    uint32_t l = i, r = i;
+    uint64_t admin = make_admin(i - b0, 1);
+    while (true) {
+      if (l == b0 && r == e0 - 1) {  // root of the whole range
+        a.nodes[nodeBase] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
+        break;
+      }
+      const bool leftChild =
+          (l == b0) ? true : (r == e0 - 1) ? false : (__ldg(a.delta + l - 1) > __ldg(a.delta + r));
+      const uint32_t s = leftChild ? r + 1 : l;
+      const uint32_t side = leftChild ? 0 : 1;
+      a.nodes[2ull * s + side] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
+      if (s <= c0 || s >= cEnd) {  // sibling outside the chunk: global phase
+        a.pending[2 * blockIdx.x + (s <= c0 ? 0 : 1)] = make_uint2(l, r);
+        break;
+      }
+      const uint32_t js = s - c0;
+      sBox[js][side] = box;
+      __threadfence_block();
+      const uint32_t other = atomicExch(&sSlot[js], leftChild ? l : r);
+      if (other == AGG_EMPTY) break;  // parked; the sibling (here or in the global phase) carries on
+      __threadfence_block();
+      const AggBox sib = sBox[js][side ^ 1];
+      box = leftChild ? agg_union(box, sib) : agg_union(sib, box);
+      if (leftChild) r = other; else l = other;
+      if (a.ranges) a.ranges[s] = make_uint2(l, r);
+      admin = make_admin(2ull * s - nodeBase, 0);
+    }
+  }
+  __syncthreads();
+  // children parked at splits whose sibling never came: publish for the global phase
+  for (int j = threadIdx.x + 1; j < AGG_CHUNK; j += blockDim.x) {
+    const uint32_t v = sSlot[j];
+    if (v != AGG_EMPTY) a.slot[c0 + j] = v;
+  }
+}
+
+template <bool SEG>
+__global__ void k_agg_global(AggArgs a, uint32_t numPending)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= numPending) return;
+  const uint32_t nv = *a.nvPtr;
+  if ((uint64_t)(t / 2) * AGG_CHUNK >= nv) return;  // chunk had no prims: entry never written
+  const uint2 pr = a.pending[t];
+  if (pr.x == AGG_EMPTY) return;
+  uint32_t l = pr.x, r = pr.y;
+  uint32_t b0, e0;
+  agg_range<SEG>(l, nv, a.off, a.numSegs, b0, e0);
+  const uint64_t nodeBase = SEG ? 2ull * b0 : 0ull;
+  // the node was written by the local phase: recover its box and admin
+  bool leftChild = (l == b0) ? true : (r == e0 - 1) ? false : (__ldg(a.delta + l - 1) > __ldg(a.delta + r));
+  uint32_t s = leftChild ? r + 1 : l;
+  const Node me = ldcg_node(a.nodes + 2ull * s + (leftChild ? 0 : 1));
+  AggBox box{me.a.x, me.a.y, me.a.z, me.a.w, me.b.x, me.b.y};
+  uint64_t admin = node_admin(me);
+  while (true) {
+    if (l == b0 && r == e0 - 1) {
+      a.nodes[nodeBase] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
+      return;
+    }
+    leftChild = (l == b0) ? true : (r == e0 - 1) ? false : (__ldg(a.delta + l - 1) > __ldg(a.delta + r));
+    s = leftChild ? r + 1 : l;
+    const uint64_t myPos = 2ull * s + (leftChild ? 0 : 1);
+    a.nodes[myPos] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> slotRef(a.slot[s]);
+    const uint32_t other = slotRef.exchange(leftChild ? l : r, cuda::memory_order_acq_rel);
+    if (other == AGG_EMPTY) return;
+    const Node sn = ldcg_node(a.nodes + (myPos ^ 1));
+    const AggBox sib{sn.a.x, sn.a.y, sn.a.z, sn.a.w, sn.b.x, sn.b.y};
+    box = leftChild ? agg_union(box, sib) : agg_union(sib, box);
+    if (leftChild) r = other; else l = other;
+    if (a.ranges) a.ranges[s] = make_uint2(l, r);
+    admin = make_admin(2ull * s - nodeBase, 0);
+  }
+}
+
+// launches both phases for nvMax (upper bound of *nvPtr) prims
+template <bool SEG>
+inline int agglomerate(AggArgs a, uint32_t nvMax, cudaStream_t s)
+{
+  const int chunks = div_up(nvMax, AGG_CHUNK);
+  k_agg_local<SEG><<<chunks, AGG_CHUNK, 0, s>>>(a);
+  k_agg_global<SEG><<<div_up(2 * chunks, 128), 128, 0, s>>>(a, 2u * chunks);
+  BQ_CUDA(cudaGetLastError());
+  return BQ_OK;
+}
+
+} // namespace bq

@@ -35,6 +35,7 @@
 #include <climits>
 #include <cfloat>
 
+#include "bq_agglom.cuh"
 #include "bq_traverse.cuh"
 
 namespace bq {
@@ -179,18 +180,8 @@ __device__ __forceinline__ uint8_t seg_split_level(const uint64_t *__restrict__ 
 {
   const uint64_t a = keys[i], b = keys[i + 1];
   if (a != b) return (uint8_t)(64 + (63 - __clzll(a ^ b)));
-  uint32_t lo = b0, hi = i;
-  while (lo < hi) {
-    uint32_t m = lo + ((hi - lo) >> 1);
-    if (keys[m] < a) lo = m + 1; else hi = m;
-  }
-  const uint32_t r0 = lo;
-  lo = i + 1; hi = e0;
-  while (lo < hi) {
-    uint32_t m = lo + ((hi - lo) >> 1);
-    if (keys[m] <= a) lo = m + 1; else hi = m;
-  }
-  const uint32_t r1 = lo;
+  const uint32_t r0 = run_begin(keys, b0, i, a);
+  const uint32_t r1 = run_end(keys, i + 1, e0, a);
   // the reference splits the run [r0,r1) at (b+e)/2 with cloud-local b,e
   const uint64_t s = (uint64_t)i + 1 - b0;
   uint64_t bb = r0 - b0, ee = r1 - b0;
@@ -213,54 +204,6 @@ __global__ void k_seg_delta(const uint64_t *__restrict__ keys, uint32_t n, const
   const uint32_t s = seg_of(off, numSegs, i);
   const uint32_t b0 = __ldg(off + s), e0 = __ldg(off + s + 1);
   if (i + 1 < e0) delta[i] = seg_split_level(keys, b0, e0, i);
-}
-
-// bottom-up build, one thread per sorted prim, bounded by its cloud
-__global__ void __launch_bounds__(256) k_seg_agglomerate(const uint8_t *__restrict__ delta, uint32_t *__restrict__ slot,
-                                                         const uint32_t *__restrict__ ids,
-                                                         const bq_box3f *__restrict__ boxes, uint32_t n,
-                                                         const uint32_t *__restrict__ off, uint32_t numSegs,
-                                                         Node *nodes, uint32_t *__restrict__ primIDs,
-                                                         uint2 *__restrict__ ranges)
-{
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint32_t sg = seg_of(off, numSegs, i);
-  const uint32_t b0 = __ldg(off + sg), e0 = __ldg(off + sg + 1);
-  const uint64_t nodeBase = 2ull * b0;
-  const uint32_t id = ids[i];
-  primIDs[i] = id - b0;
-  if (i == b0) nodes[nodeBase + 1] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0);
-  const bq_box3f bx = boxes[id];
-  float lx = bx.lower[0], ly = bx.lower[1], lz = bx.lower[2], hx = bx.upper[0], hy = bx.upper[1], hz = bx.upper[2];
-  uint32_t l = i, r = i;
-  uint64_t admin = make_admin(i - b0, 1);
-  while (true) {
-    if (l == b0 && r == e0 - 1) {
-      nodes[nodeBase] = make_node(lx, ly, lz, hx, hy, hz, admin);
-      return;
-    }
-    const bool leftChild = (l == b0) ? true : (r == e0 - 1) ? false : (__ldg(&delta[l - 1]) > __ldg(&delta[r]));
-    const uint32_t s = leftChild ? r + 1 : l;
-    const uint64_t myPos = 2ull * s + (leftChild ? 0 : 1);
-    nodes[myPos] = make_node(lx, ly, lz, hx, hy, hz, admin);
-    __threadfence();
-    const uint32_t other = atomicExch(&slot[s], leftChild ? l : r);
-    if (other == SLOT_EMPTY) return;
-    __threadfence();
-    const Node sib = ldcg_node(&nodes[myPos ^ 1]);
-    if (leftChild) {
-      lx = fminf(lx, sib.a.x); ly = fminf(ly, sib.a.y); lz = fminf(lz, sib.a.z);
-      hx = fmaxf(hx, sib.a.w); hy = fmaxf(hy, sib.b.x); hz = fmaxf(hz, sib.b.y);
-      r = other;
-    } else {
-      lx = fminf(sib.a.x, lx); ly = fminf(sib.a.y, ly); lz = fminf(sib.a.z, lz);
-      hx = fmaxf(sib.a.w, hx); hy = fmaxf(sib.b.x, hy); hz = fmaxf(sib.b.y, hz);
-      l = other;
-    }
-    if (ranges) ranges[s] = make_uint2(l, r);
-    admin = make_admin(2ull * s - nodeBase, 0);
-  }
 }
 
 // leaf threshold > 1: kept inner nodes (split positions inside clouds)
@@ -605,18 +548,23 @@ int batched_build_morton63(const bq_box3f *boxes, const uint32_t *off, uint32_t 
     ProfScope ps("batch.delta", al.s);
     k_seg_delta<<<div_up(n, 256), 256, 0, al.s>>>(fkeys, n, off, numSegs, delta, slot);
   }
+  uint2 *pending = nullptr;
+  BQ_TRY(tmp.get(&pending, 2ull * div_up(n, AGG_CHUNK)));
+  // the prim count on the device is the last cloud offset (no host copy,
+  // so the sequence stays capturable)
+  AggArgs ag{delta, slot, fids, boxes, (Node *)nodesOut, primIDs, off + numSegs, nullptr, pending, off, numSegs};
   if (thr == 1) {
-    ProfScope ps("batch.agglomerate", al.s);
-    k_seg_agglomerate<<<div_up(n, 256), 256, 0, al.s>>>(delta, slot, fids, boxes, n, off, numSegs, (Node *)nodesOut,
-                                                        primIDs, nullptr);
+    ProfScope ps("batch.agglomerate", al.s, 2);
+    BQ_TRY(agglomerate<true>(ag, n, al.s));
   } else {
     BQ_TRY(tmp.get(&full, 2ull * n));
     BQ_TRY(tmp.get(&ranges, n));
     BQ_TRY(tmp.get(&kept, n + 1ull));
     BQ_TRY(tmp.get(&rank, n + 1ull));
     ProfScope ps("batch.agglomerate", al.s, 4);
-    k_seg_agglomerate<<<div_up(n, 256), 256, 0, al.s>>>(delta, slot, fids, boxes, n, off, numSegs, full, primIDs,
-                                                        ranges);
+    ag.nodes = full;
+    ag.ranges = ranges;
+    BQ_TRY(agglomerate<true>(ag, n, al.s));
     k_seg_kept<<<div_up(n, 256), 256, 0, al.s>>>(ranges, n, off, numSegs, thr, kept);
     BQ_CUDA(cudaMemsetAsync(kept + n, 0, 4, al.s));
     BQ_TRY(exclusive_scan_u32(kept, rank, n + 1, nullptr, nullptr, al));
@@ -629,12 +577,12 @@ int batched_build_morton63(const bq_box3f *boxes, const uint32_t *off, uint32_t 
 
 int batched_knn(const bq_bvh3f *bvhs, const uint32_t *poff, const float *points, const float *queries,
                 const uint32_t *qoff, uint32_t numSegs, uint32_t nq, int k, float maxSqr, const bq_query_config *qcfg,
-                int chunk, int32_t *ids, float *d, int32_t *nf, uint32_t *errOut, Alloc &al)
+                int32_t *ids, float *d, int32_t *nf, uint32_t *errOut, Alloc &al)
 {
   bq_query_config c;
   BQ_TRY(query_config(qcfg, c));
+  const int chunk = c.queriesPerWarp;
   if (k < 1 || k > 64) return set_error(BQ_ERR_INVALID_ARGUMENT, "k must be in [1, 64]");
-  if (chunk < 32 || chunk > 4096 || chunk % 32) return set_error(BQ_ERR_INVALID_ARGUMENT, "chunk must be a multiple of 32");
   if (nq == 0 || numSegs == 0) return BQ_OK;
   TempSet tmp(al);
   uint64_t *keys[2];
@@ -678,6 +626,60 @@ int batched_knn(const bq_bvh3f *bvhs, const uint32_t *poff, const float *points,
   else s = BQ_SEG_KNN(64);
 #undef BQ_SEG_KNN
   return s;
+}
+
+// ------------------------------------------------------------------
+// autotuner: time every knob combination on the caller's inputs
+// ------------------------------------------------------------------
+int autotune_batched_knn(const bq_box3f *boxes, const float *points, const uint32_t *off, uint32_t numSegs,
+                         uint32_t n, const float *queries, const uint32_t *qoff, uint32_t nq, int k, bq_tuning *best,
+                         Alloc &al)
+{
+  if (!best) return set_error(BQ_ERR_INVALID_ARGUMENT, "best is NULL");
+  TempSet tmp(al);
+  bq_node3f *nodes = nullptr;
+  uint32_t *prims = nullptr;
+  bq_bvh3f *bvhs = nullptr;
+  int32_t *ids = nullptr;
+  float *d = nullptr;
+  BQ_TRY(tmp.get(&nodes, 2ull * n + 2));
+  BQ_TRY(tmp.get(&prims, n + 1ull));
+  BQ_TRY(tmp.get(&bvhs, numSegs));
+  BQ_TRY(tmp.get(&ids, (size_t)nq * k));
+  BQ_TRY(tmp.get(&d, (size_t)nq * k));
+  cudaEvent_t e[3];
+  for (auto &x : e) BQ_CUDA(cudaEventCreate(&x));
+  const int leaves[] = {1, 2, 4, 8}, stacks[] = {32, 64}, blocks[] = {64, 128}, grabs[] = {32, 128};
+  float bestMs = INFINITY;
+  int status = BQ_OK;
+  for (int lf : leaves) {
+    bq_build_config bc{1 << 15, lf, BQ_SPATIAL_MEDIAN};
+    for (int st : stacks)
+      for (int bl : blocks)
+        for (int gr : grabs) {
+          bq_query_config qc{BQ_TIES_LOWEST_ID, st, bl, 1, gr};
+          float tb = 0.f, tq = 0.f;
+          for (int rep = 0; rep < 2 && status == BQ_OK; rep++) {  // rep 0 warms up
+            cudaEventRecord(e[0], al.s);
+            status = batched_build_morton63(boxes, off, numSegs, n, &bc, nodes, prims, bvhs, nullptr, al);
+            cudaEventRecord(e[1], al.s);
+            if (status == BQ_OK)
+              status = batched_knn(bvhs, off, points, queries, qoff, numSegs, nq, k, INFINITY, &qc, ids, d, nullptr,
+                                   nullptr, al);
+            cudaEventRecord(e[2], al.s);
+            cudaEventSynchronize(e[2]);
+            cudaEventElapsedTime(&tb, e[0], e[1]);
+            cudaEventElapsedTime(&tq, e[1], e[2]);
+          }
+          if (status != BQ_OK) break;
+          if (tb + tq < bestMs) {
+            bestMs = tb + tq;
+            *best = bq_tuning{lf, st, bl, gr, tb, tq};
+          }
+        }
+  }
+  for (auto &x : e) cudaEventDestroy(x);
+  return status;
 }
 
 } // namespace bq

@@ -18,6 +18,20 @@ int tri_distance_bwd(const int32_t *tris, const float *verts, uint32_t numVerts,
                      const int32_t *ids, const float *gradSqr, float *gradQ, float *gradV, Alloc &al);
 int tri_boxes(const int32_t *tris, const float *verts, uint32_t nt, bq_box3f *boxes, cudaStream_t s);
 int points_to_boxes(const float *points, uint32_t n, bq_box3f *boxes, cudaStream_t s);
+int batched_build_morton63(const bq_box3f *boxes, const uint32_t *off, uint32_t numSegs, uint32_t n,
+                           const bq_build_config *cfg, bq_node3f *nodesOut, uint32_t *primIDs, bq_bvh3f *bvhs,
+                           uint32_t *errOut, Alloc &al);
+int batched_knn(const bq_bvh3f *bvhs, const uint32_t *poff, const float *points, const float *queries,
+                const uint32_t *qoff, uint32_t numSegs, uint32_t nq, int k, float maxSqr, const bq_query_config *qcfg,
+                int32_t *ids, float *d, int32_t *nf, uint32_t *errOut, Alloc &al);
+int batched_refit(const bq_bvh3f *bvhs, const uint32_t *off, uint32_t numSegs, uint32_t numPrims, bq_node3f *nodes,
+                  const uint32_t *primIDs, const bq_box3f *boxes, Alloc &al);
+int batched_tri_closest(const bq_bvh3f *bvhs, const uint32_t *triOff, const int32_t *tris, const float *verts,
+                        const float *queries, const uint32_t *qoff, uint32_t numSegs, uint32_t nq, float maxSqr,
+                        const bq_query_config *qcfg, int32_t *ids, float *d, float *P, uint32_t *errOut, Alloc &al);
+int autotune_batched_knn(const bq_box3f *boxes, const float *points, const uint32_t *off, uint32_t numSegs,
+                         uint32_t n, const float *queries, const uint32_t *qoff, uint32_t nq, int k, bq_tuning *best,
+                         Alloc &al);
 
 namespace {
 // Like the reference's AsyncGpuMemoryResource (cuBQL/builder/cuda.h:52-72):
@@ -156,6 +170,68 @@ int bq_tri_distance_bwd_f3(const int32_t *tris, const float *verts, uint32_t num
   if (numVerts && !gradVerts) return set_error(BQ_ERR_INVALID_ARGUMENT, "gradVerts is NULL");
   Alloc al = make_alloc(alloc, stream);
   return tri_distance_bwd(tris, verts, numVerts, queries, numQueries, ids, gradSqr, gradQueries, gradVerts, al);
+}
+
+int bq_batched_build_morton63_f3(const bq_box3f *boxes, const uint32_t *segOffsets, uint32_t numSegs,
+                                 uint32_t numPrims, const bq_build_config *cfg, bq_node3f *nodes, uint32_t *primIDs,
+                                 bq_bvh3f *bvhs, uint32_t *deviceErr, const bq_allocator *alloc, bq_stream_t stream)
+{
+  if (numSegs && (!segOffsets || !bvhs)) return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  if (numPrims && (!boxes || !nodes || !primIDs)) return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  if (numPrims && misaligned(boxes, 8)) return set_error(BQ_ERR_INVALID_ARGUMENT, "boxes must be 8-byte aligned");
+  if (numPrims && misaligned(nodes, 16)) return set_error(BQ_ERR_INVALID_ARGUMENT, "nodes must be 16-byte aligned");
+  if (numPrims >= (1u << 30)) return set_error(BQ_ERR_INVALID_ARGUMENT, "at most 2^30-1 primitives per batch");
+  Alloc al = make_alloc(alloc, stream);
+  return batched_build_morton63(boxes, segOffsets, numSegs, numPrims, cfg, nodes, primIDs, bvhs, deviceErr, al);
+}
+
+int bq_batched_knn_f3(const bq_bvh3f *bvhs, const uint32_t *pointOffsets, const float *points, const float *queries,
+                      const uint32_t *queryOffsets, uint32_t numSegs, uint32_t numQueries, int k, float maxSqrDist,
+                      const bq_query_config *qcfg, int32_t *ids, float *sqrDist, int32_t *numFound,
+                      uint32_t *deviceErr, const bq_allocator *alloc, bq_stream_t stream)
+{
+  if (numQueries && (!bvhs || !pointOffsets || !points || !queries || !queryOffsets || !ids || !sqrDist))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  if (numQueries >= (1u << 30)) return set_error(BQ_ERR_INVALID_ARGUMENT, "at most 2^30-1 queries per batch");
+  Alloc al = make_alloc(alloc, stream);
+  return batched_knn(bvhs, pointOffsets, points, queries, queryOffsets, numSegs, numQueries, k, maxSqrDist, qcfg, ids,
+                     sqrDist, numFound, deviceErr, al);
+}
+
+int bq_batched_refit_f3(const bq_bvh3f *bvhs, const uint32_t *segOffsets, uint32_t numSegs, uint32_t numPrims,
+                        bq_node3f *nodes, const uint32_t *primIDs, const bq_box3f *boxes, const bq_allocator *alloc,
+                        bq_stream_t stream)
+{
+  if (numPrims && (!bvhs || !segOffsets || !nodes || !primIDs || !boxes))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  if (numPrims >= (1u << 30)) return set_error(BQ_ERR_INVALID_ARGUMENT, "at most 2^30-1 primitives per batch");
+  Alloc al = make_alloc(alloc, stream);
+  return batched_refit(bvhs, segOffsets, numSegs, numPrims, nodes, primIDs, boxes, al);
+}
+
+int bq_batched_tri_closest_f3(const bq_bvh3f *bvhs, const uint32_t *triOffsets, const int32_t *tris,
+                              const float *verts, const float *queries, const uint32_t *queryOffsets,
+                              uint32_t numSegs, uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg,
+                              int32_t *ids, float *sqrDist, float *P, uint32_t *deviceErr, const bq_allocator *alloc,
+                              bq_stream_t stream)
+{
+  if (numQueries && (!bvhs || !triOffsets || !tris || !verts || !queries || !queryOffsets || !ids || !sqrDist))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return batched_tri_closest(bvhs, triOffsets, tris, verts, queries, queryOffsets, numSegs, numQueries, maxSqrDist,
+                             qcfg, ids, sqrDist, P, deviceErr, al);
+}
+
+int bq_autotune_batched_knn_f3(const bq_box3f *boxes, const float *points, const uint32_t *segOffsets,
+                               uint32_t numSegs, uint32_t numPrims, const float *queries, const uint32_t *queryOffsets,
+                               uint32_t numQueries, int k, bq_tuning *best, const bq_allocator *alloc,
+                               bq_stream_t stream)
+{
+  if (!boxes || !points || !segOffsets || !queries || !queryOffsets || !best)
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL argument");
+  Alloc al = make_alloc(alloc, stream);
+  return autotune_batched_knn(boxes, points, segOffsets, numSegs, numPrims, queries, queryOffsets, numQueries, k,
+                              best, al);
 }
 
 int bq_tri_boxes_f3(const int32_t *tris, const float *verts, uint32_t numTris, bq_box3f *boxes, bq_stream_t stream)

@@ -13,7 +13,9 @@
 //   onesweep sort stable (key, primID) sort, 8 digit passes (bq_sort.cu)
 //   k_delta       one byte per adjacent key pair: the level at which the
 //                 reference's top-down split would separate them
-//   k_agglomerate bottom-up construction of topology and boxes in one pass
+//   agglomerate   bottom-up construction of topology and boxes
+//                 (bq_agglom.cuh: per-chunk in shared memory, then the few
+//                 chunk-crossing nodes device-wide)
 //
 // Why the bottom-up pass gives the reference's tree: createNodes/findSplit
 // (radix.h:446-570) split a key range [b,e) at the first key that has the
@@ -44,7 +46,7 @@
 #include <climits>
 #include <cfloat>
 
-#include "bq_internal.cuh"
+#include "bq_agglom.cuh"
 
 namespace bq {
 namespace {
@@ -268,19 +270,9 @@ __device__ __forceinline__ uint8_t split_level(const uint64_t *__restrict__ keys
 {
   const uint64_t a = keys[i], b = keys[i + 1];
   if (a != b) return (uint8_t)(64 + (63 - __clzll(a ^ b)));
-  // equal keys: the run [r0, r1) containing i, i+1 (binary searches)
-  uint32_t lo = 0, hi = i;  // first index with key >= a
-  while (lo < hi) {
-    uint32_t m = lo + ((hi - lo) >> 1);
-    if (keys[m] < a) lo = m + 1; else hi = m;
-  }
-  const uint32_t r0 = lo;
-  lo = i + 1; hi = nv;      // first index with key > a
-  while (lo < hi) {
-    uint32_t m = lo + ((hi - lo) >> 1);
-    if (keys[m] <= a) lo = m + 1; else hi = m;
-  }
-  const uint32_t r1 = lo;
+  // equal keys: the run [r0, r1) containing i, i+1
+  const uint32_t r0 = run_begin(keys, 0, i, a);
+  const uint32_t r1 = run_end(keys, i + 1, nv, a);
   // depth of split position s = i+1 in the (b+e)/2 recursion over [r0,r1)
   const uint64_t s = (uint64_t)i + 1;
   uint64_t bb = r0, ee = r1;
@@ -302,51 +294,6 @@ __global__ void __launch_bounds__(256) k_delta(const uint64_t *__restrict__ keys
   if (i >= nv) return;
   slot[i] = SLOT_EMPTY;
   if (i + 1 < nv) delta[i] = split_level(keys, nv, i);
-}
-
-// ------------------------------------------------------------------
-// pass 4: bottom-up topology + boxes (one thread per sorted prim)
-// ------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_agglomerate(const uint8_t *__restrict__ delta, uint32_t *__restrict__ slot,
-                                                     const uint32_t *__restrict__ ids,
-                                                     const bq_box3f *__restrict__ boxes, Node *nodes,
-                                                     const uint32_t *nvPtr, uint2 *__restrict__ ranges)
-{
-  const uint32_t nv = *nvPtr;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0 && nv >= 1) nodes[1] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0);
-  if (i >= nv) return;
-  float lx, ly, lz, hx, hy, hz;
-  load_box(boxes, ids[i], lx, ly, lz, hx, hy, hz);
-  uint32_t l = i, r = i;
-  uint64_t admin = make_admin(i, 1);
-  while (true) {
-    if (l == 0 && r == nv - 1) {
-      nodes[0] = make_node(lx, ly, lz, hx, hy, hz, admin);
-      return;
-    }
-    // parent = split at the lower of the two boundary levels
-    const bool leftChild = (l == 0) ? true : (r == nv - 1) ? false : (__ldg(&delta[l - 1]) > __ldg(&delta[r]));
-    const uint32_t s = leftChild ? r + 1 : l;
-    const uint32_t myPos = 2 * s + (leftChild ? 0 : 1);
-    nodes[myPos] = make_node(lx, ly, lz, hx, hy, hz, admin);
-    __threadfence();
-    const uint32_t other = atomicExch(&slot[s], leftChild ? l : r);
-    if (other == SLOT_EMPTY) return;  // sibling not done yet: it will carry on
-    __threadfence();
-    const Node sib = ldcg_node(&nodes[myPos ^ 1]);
-    if (leftChild) {  // union(left, right) in the reference's operand order (sm_builder.h:669-670)
-      lx = fminf(lx, sib.a.x); ly = fminf(ly, sib.a.y); lz = fminf(lz, sib.a.z);
-      hx = fmaxf(hx, sib.a.w); hy = fmaxf(hy, sib.b.x); hz = fmaxf(hz, sib.b.y);
-      r = other;
-    } else {
-      lx = fminf(sib.a.x, lx); ly = fminf(sib.a.y, ly); lz = fminf(sib.a.z, lz);
-      hx = fmaxf(sib.a.w, hx); hy = fmaxf(sib.b.x, hy); hz = fmaxf(sib.b.y, hz);
-      l = other;
-    }
-    if (ranges) ranges[s] = make_uint2(l, r);
-    admin = make_admin(2ull * s, 0);
-  }
 }
 
 // ------------------------------------------------------------------
@@ -471,10 +418,12 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
     ProfScope ps("morton.delta", al.s);
     k_delta<<<div_up(n, 256), 256, 0, al.s>>>(keys, &st->numValid, delta, slot);
   }
+  uint2 *pending = nullptr;
+  if ((s = tmp.get(&pending, 2ull * div_up(n, AGG_CHUNK))) != BQ_OK) return fail(s);
+  AggArgs ag{delta, slot, ids, boxes, nodes, nullptr, &st->numValid, nullptr, pending, nullptr, 0};
   if (thr == 1) {
-    ProfScope ps("morton.agglomerate", al.s);
-    k_agglomerate<<<div_up(n, 256), 256, 0, al.s>>>(delta, slot, ids, boxes, nodes, &st->numValid, nullptr);
-    if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_agglomerate"));
+    ProfScope ps("morton.agglomerate", al.s, 2);
+    if ((s = agglomerate<false>(ag, n, al.s)) != BQ_OK) return fail(s);
   } else {
     Node *full = nullptr;
     uint2 *ranges = nullptr;
@@ -486,7 +435,9 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
     if ((s = tmp2.get(&rank, n)) != BQ_OK) return fail(s);
     if ((s = tmp2.get(&total, 1)) != BQ_OK) return fail(s);
     if ((ce = cudaMemsetAsync(kept, 0, sizeof(uint32_t) * n, al.s)) != cudaSuccess) return fail(cuda_error(ce, "memset"));
-    k_agglomerate<<<div_up(n, 256), 256, 0, al.s>>>(delta, slot, ids, boxes, full, &st->numValid, ranges);
+    ag.nodes = full;
+    ag.ranges = ranges;
+    if ((s = agglomerate<false>(ag, n, al.s)) != BQ_OK) return fail(s);
     k_kept<<<div_up(n, 256), 256, 0, al.s>>>(ranges, &st->numValid, thr, kept);
     if ((s = exclusive_scan_u32(kept, rank, n > 1 ? n - 1 : 1, nullptr, total, al)) != BQ_OK) return fail(s);
     // the number of kept inner nodes decides the output size

@@ -331,7 +331,8 @@ int query_config(const bq_query_config *q, bq_query_config &out)
     return set_error(BQ_ERR_INVALID_ARGUMENT, "stackDepth must be 32, 64 or 128");
   if (out.blockSize != 64 && out.blockSize != 128)
     return set_error(BQ_ERR_INVALID_ARGUMENT, "blockSize must be 64 or 128");
-  if (out.queriesPerWarp != 32) return set_error(BQ_ERR_UNSUPPORTED, "queriesPerWarp must be 32");
+  if (out.queriesPerWarp < 32 || out.queriesPerWarp > 1024 || out.queriesPerWarp % 32)
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "queriesPerWarp must be a multiple of 32 up to 1024");
   return BQ_OK;
 }
 

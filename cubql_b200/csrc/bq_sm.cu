@@ -267,22 +267,33 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   uint32_t *pnCur = pnA, *pnNext = pnB;
   SmNode *listCur = listA, *listNext = listB;
   while (K > 0) {
-    ProfScope ps("sm.level", al.s, 14);
-    k_sm_select<<<div_up(K, 128), 128, 0, al.s>>>(listCur, K, thr, pcCur, isSplit, splitCount, dim, pos, tb, tnodes,
-                                                  primIDs);
-    if ((s = exclusive_scan_u32(isSplit, rank, K, nullptr, counts + 1, al)) != BQ_OK) return fail(s);
-    if ((s = exclusive_scan_u32(splitCount, nextBegin, K, nullptr, counts + 2, al)) != BQ_OK) return fail(s);
-    k_sm_flags<<<div_up(A, 256), 256, 0, al.s>>>(pcCur, pnCur, A, listCur, isSplit, dim, pos, tb, right);
-    if ((s = exclusive_scan_u32(right, right, A + 1, nullptr, nullptr, al)) != BQ_OK) return fail(s);
-    k_sm_children<<<div_up(K, 128), 128, 0, al.s>>>(listCur, K, isSplit, rank, nextBegin, right, nodeBase, listNext,
-                                                    tnodes);
-    k_sm_scatter<<<div_up(A, 256), 256, 0, al.s>>>(pcCur, pnCur, A, listCur, isSplit, dim, pos, tb, rank, nextBegin,
-                                                   right, pcNext, pnNext);
-    if ((ce = cudaMemcpyAsync(hc + 1, counts + 1, 8, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess)
-      return fail(cuda_error(ce, "copy"));
-    if ((ce = cudaStreamSynchronize(al.s)) != cudaSuccess) return fail(cuda_error(ce, "sync"));
+    {
+      ProfScope ps("sm.nodes", al.s, 7);
+      k_sm_select<<<div_up(K, 128), 128, 0, al.s>>>(listCur, K, thr, pcCur, isSplit, splitCount, dim, pos, tb, tnodes,
+                                                    primIDs);
+      if ((s = exclusive_scan_u32(isSplit, rank, K, nullptr, counts + 1, al)) != BQ_OK) return fail(s);
+      if ((s = exclusive_scan_u32(splitCount, nextBegin, K, nullptr, counts + 2, al)) != BQ_OK) return fail(s);
+    }
+    {
+      ProfScope ps("sm.partition", al.s, 6);
+      k_sm_flags<<<div_up(A, 256), 256, 0, al.s>>>(pcCur, pnCur, A, listCur, isSplit, dim, pos, tb, right);
+      if ((s = exclusive_scan_u32(right, right, A + 1, nullptr, nullptr, al)) != BQ_OK) return fail(s);
+      k_sm_children<<<div_up(K, 128), 128, 0, al.s>>>(listCur, K, isSplit, rank, nextBegin, right, nodeBase,
+                                                      listNext, tnodes);
+      k_sm_scatter<<<div_up(A, 256), 256, 0, al.s>>>(pcCur, pnCur, A, listCur, isSplit, dim, pos, tb, rank,
+                                                     nextBegin, right, pcNext, pnNext);
+    }
+    {
+      ProfScope ps("sm.sync", al.s, 0);
+      if ((ce = cudaMemcpyAsync(hc + 1, counts + 1, 8, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess)
+        return fail(cuda_error(ce, "copy"));
+      if ((ce = cudaStreamSynchronize(al.s)) != cudaSuccess) return fail(cuda_error(ce, "sync"));
+    }
     const uint32_t S = hc[1], An = hc[2];
-    if (S > 0) k_sm_bounds<<<div_up(An, SB_TILE), 256, 0, al.s>>>(pcNext, pnNext, An, listNext);
+    if (S > 0) {
+      ProfScope ps("sm.bounds", al.s);
+      k_sm_bounds<<<div_up(An, SB_TILE), 256, 0, al.s>>>(pcNext, pnNext, An, listNext);
+    }
     if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "spatial median level"));
     nodeBase += 2 * S;
     K = 2 * S;

@@ -112,22 +112,27 @@ struct PassCtl {
 };
 
 template <typename KeyT, int ITEMS>
-__global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const KeyT *__restrict__ keysIn, KeyT *__restrict__ keysOut,
-                                                         const uint32_t *__restrict__ valsIn,
-                                                         uint32_t *__restrict__ valsOut, uint32_t nHost,
-                                                         const uint32_t *nDev, int shift, PassCtl ctl)
+__global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restrict__ keysIn, KeyT *__restrict__ keysOut,
+                                                            const uint32_t *__restrict__ valsIn,
+                                                            uint32_t *__restrict__ valsOut, uint32_t nHost,
+                                                            const uint32_t *nDev, int shift, PassCtl ctl)
 {
   const uint32_t n = nDev ? *nDev : nHost;
   constexpr int TILE = SORT_BLOCK * ITEMS;
   constexpr int WARP_ITEMS = 32 * ITEMS;
+  // dynamic shared memory: keys [TILE], then values [TILE]; the per-warp
+  // digit histograms live in the value region until the local positions
+  // are known (they are dead before the first value is stored)
   extern __shared__ __align__(16) unsigned char smem[];
-  KeyT *sKeys = (KeyT *)smem;                                      // TILE keys (values reuse it)
-  uint32_t *sWarpHist = (uint32_t *)(smem + sizeof(KeyT) * TILE);  // SORT_WARPS * 257
+  KeyT *sKeys = (KeyT *)smem;
+  uint32_t *sVals = (uint32_t *)(smem + sizeof(KeyT) * TILE);
+  uint32_t *sWarpHist = sVals;  // SORT_WARPS * 257 <= TILE
   __shared__ uint32_t sTileStart[256];
   __shared__ uint32_t sGlobalBase[256];
   __shared__ uint32_t sWarpSums[SORT_WARPS];
   __shared__ uint32_t sTile;
   __shared__ uint32_t sBad;
+  static_assert(SORT_WARPS * 257 <= TILE, "histograms must fit in the value region");
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
@@ -137,53 +142,44 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const KeyT *__restrict_
   for (int i = threadIdx.x; i < SORT_WARPS * 257; i += SORT_BLOCK) sWarpHist[i] = 0;
   __syncthreads();
   const uint32_t tile = sTile;
-  const uint64_t tileBase = (uint64_t)tile * TILE;
-  const uint64_t warpBase = tileBase + (uint64_t)warp * WARP_ITEMS;
+  const uint64_t warpBase = (uint64_t)tile * TILE + (uint64_t)warp * WARP_ITEMS;
 
-  // 1. load (warp-contiguous sub-tiles)
+  // 1. keys (warp-contiguous sub-tiles, coalesced)
   KeyT key[ITEMS];
-  uint32_t dig[ITEMS];
 #pragma unroll
   for (int r = 0; r < ITEMS; r++) {
-    uint64_t idx = warpBase + (uint64_t)r * 32 + lane;
-    if (idx < n) {
-      key[r] = keysIn[idx];
-      dig[r] = digit_of(key[r], shift);
-    } else {
-      key[r] = 0;
-      dig[r] = 256;  // out-of-range items: a dummy bin that is never written
-    }
+    const uint64_t idx = warpBase + (uint64_t)r * 32 + lane;
+    key[r] = idx < n ? keysIn[idx] : (KeyT)0;
   }
 
-  // 2. stable warp-level ranking
+  // 2. stable ranking inside each warp
   uint32_t *wh = sWarpHist + warp * 257;
   const uint32_t ltMask = lanemask_lt();
-  uint32_t rank[ITEMS];
+  uint32_t pos[ITEMS];  // rank within warp and digit, later the tile-local position
 #pragma unroll
   for (int r = 0; r < ITEMS; r++) {
-    const uint32_t peers = __match_any_sync(0xffffffffu, dig[r]);
-    const uint32_t base = wh[dig[r]];
+    const bool valid = warpBase + (uint64_t)r * 32 + lane < n;
+    const uint32_t d = valid ? digit_of(key[r], shift) : 256u;  // 256: never written
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t base = wh[d];
     __syncwarp();
-    if ((peers & ~(ltMask | (1u << lane))) == 0)  // highest lane of the peer group
-      wh[dig[r]] = base + __popc(peers);
+    if ((peers & ~(ltMask | (1u << lane))) == 0) wh[d] = base + __popc(peers);  // highest lane of the group
     __syncwarp();
-    rank[r] = base + __popc(peers & ltMask);
+    pos[r] = base + __popc(peers & ltMask);
   }
   __syncthreads();
 
-  // per digit: warp-exclusive offsets and tile totals
-  const int d = threadIdx.x;  // one digit per thread
+  // per digit (thread d): warp-exclusive offsets and tile totals
+  const int d = threadIdx.x;
   uint32_t cnt = 0;
 #pragma unroll
   for (int w = 0; w < SORT_WARPS; w++) {
-    uint32_t c = sWarpHist[w * 257 + d];
+    const uint32_t c = sWarpHist[w * 257 + d];
     sWarpHist[w * 257 + d] = cnt;
     cnt += c;
   }
   uint32_t tileTotal;
-  const uint32_t tStart = block_excl_scan_256(cnt, sWarpSums, &tileTotal);
-  sTileStart[d] = tStart;
-  // global digit start of this pass
+  sTileStart[d] = block_excl_scan_256(cnt, sWarpSums, &tileTotal);
   uint32_t histTotal;
   const uint32_t gStart = block_excl_scan_256(ctl.hist[d], sWarpSums, &histTotal);
 
@@ -225,44 +221,43 @@ __global__ void __launch_bounds__(SORT_BLOCK) k_onesweep(const KeyT *__restrict_
   __syncthreads();
   if (sBad) return;  // a wait timed out: leave the output untouched, report
 
-  // local positions
-  uint32_t lpos[ITEMS];
-#pragma unroll
-  for (int r = 0; r < ITEMS; r++)
-    lpos[r] = dig[r] < 256 ? sTileStart[dig[r]] + sWarpHist[warp * 257 + dig[r]] + rank[r] : 0xffffffffu;
-
-  // 4a. keys through shared memory
-#pragma unroll
-  for (int r = 0; r < ITEMS; r++)
-    if (lpos[r] != 0xffffffffu) sKeys[lpos[r]] = key[r];
-  __syncthreads();
-  uint32_t gpos[ITEMS];
+  // 4. tile-local positions; then keys and values through shared memory
 #pragma unroll
   for (int r = 0; r < ITEMS; r++) {
+    const bool valid = warpBase + (uint64_t)r * 32 + lane < n;
+    const uint32_t dd = digit_of(key[r], shift);
+    pos[r] = valid ? sTileStart[dd] + sWarpHist[warp * 257 + dd] + pos[r] : 0xffffffffu;
+  }
+  __syncthreads();  // histograms dead: the value region may be written now
+#pragma unroll
+  for (int r = 0; r < ITEMS; r++)
+    if (pos[r] != 0xffffffffu) sKeys[pos[r]] = key[r];
+  uint32_t val[ITEMS];
+#pragma unroll
+  for (int r = 0; r < ITEMS; r++) {
+    const uint64_t idx = warpBase + (uint64_t)r * 32 + lane;
+    val[r] = pos[r] != 0xffffffffu ? valsIn[idx] : 0u;
+  }
+#pragma unroll
+  for (int r = 0; r < ITEMS; r++)
+    if (pos[r] != 0xffffffffu) sVals[pos[r]] = val[r];
+  __syncthreads();
+  // 5. scatter: consecutive tile positions of one digit go to consecutive
+  // global positions
+#pragma unroll 4
+  for (int r = 0; r < ITEMS; r++) {
     const uint32_t p = threadIdx.x + r * SORT_BLOCK;
-    gpos[r] = 0xffffffffu;
     if (p < tileTotal) {
-      KeyT k = sKeys[p];
-      uint32_t dd = digit_of(k, shift);
-      uint32_t g = sGlobalBase[dd] + (p - sTileStart[dd]);
-      gpos[r] = g;
-      if (g < n) keysOut[g] = k;
-      else atomicOr(ctl.err, DEV_ERR_RANGE);
+      const KeyT k = sKeys[p];
+      const uint32_t dd = digit_of(k, shift);
+      const uint32_t g = sGlobalBase[dd] + (p - sTileStart[dd]);
+      if (g < n) {
+        keysOut[g] = k;
+        valsOut[g] = sVals[p];
+      } else {
+        atomicOr(ctl.err, DEV_ERR_RANGE);
+      }
     }
-  }
-  __syncthreads();
-  // 4b. values through the same buffer
-  uint32_t *sVals = (uint32_t *)smem;
-#pragma unroll
-  for (int r = 0; r < ITEMS; r++) {
-    uint64_t idx = warpBase + (uint64_t)r * 32 + lane;
-    if (lpos[r] != 0xffffffffu) sVals[lpos[r]] = valsIn[idx];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int r = 0; r < ITEMS; r++) {
-    const uint32_t p = threadIdx.x + r * SORT_BLOCK;
-    if (gpos[r] < n) valsOut[gpos[r]] = sVals[p];
   }
 }
 
@@ -293,7 +288,7 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
                                                                                 numPasses, hist);
     BQ_CUDA(cudaGetLastError());
   }
-  const size_t smemBytes = sizeof(KeyT) * TILE + sizeof(uint32_t) * SORT_WARPS * 257;
+  const size_t smemBytes = (sizeof(KeyT) + sizeof(uint32_t)) * TILE;
   BQ_CUDA(cudaFuncSetAttribute(k_onesweep<KeyT, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes));
   int sel = 0;
   for (int p = 0; p < numPasses; p++) {

@@ -104,3 +104,64 @@ def icosphere(level, seed=SEED_MESH, amp=0.05):
     scale = np.float32(1.0) + np.float32(amp) * u
     out = (verts.astype(np.float32) * scale[:, None]).astype(np.float32)
     return out, faces.astype(np.int32)
+
+
+def cloud_batch(num=512, lo=1000, hi=200000, queries_per_cloud=50000, seed=SEED_BATCH):
+    """Batched workload: `num` clouds with sizes floor(exp(U[ln lo, ln hi])),
+    each by a seeded coin flip either uniform in [0,1]^3 or an 8-cluster
+    Gaussian mixture (sigma 0.02), plus `queries_per_cloud` uniform queries
+    per cloud.  Returns (points (N,3), offsets (num+1,), queries (Q,3),
+    query offsets (num+1,)), clouds stored back to back."""
+    u = lcg_streams(num, seed, 2).astype(np.float64)
+    sizes = np.floor(np.exp(np.log(lo) + u[:, 0] * (np.log(hi) - np.log(lo)))).astype(np.int64)
+    pts, qs = [], []
+    for c in range(num):
+        n = int(sizes[c])
+        s = seed * 1000 + c
+        if u[c, 1] < 0.5:
+            p = uniform_points(n, s)
+        else:
+            cen = lcg_streams(8, s ^ 0x2545F491, 3).astype(np.float64)
+            v = lcg_streams(n, s, 7).astype(np.float64)
+            k = np.minimum((v[:, 0] * 8).astype(np.int64), 7)
+            g = np.sqrt(-2.0 * np.log(np.maximum(v[:, 1:4], 1e-12))) * np.cos(2.0 * np.pi * v[:, 4:7])
+            p = (cen[k] + 0.02 * g).astype(np.float32)
+        pts.append(p)
+        qs.append(uniform_points(queries_per_cloud, s ^ 0x68E31DA4))
+    off = np.zeros(num + 1, dtype=np.int64)
+    off[1:] = np.cumsum(sizes)
+    qoff = np.arange(num + 1, dtype=np.int64) * queries_per_cloud
+    return np.concatenate(pts), off, np.concatenate(qs), qoff
+
+
+_ICO_CACHE = {}
+
+
+def mesh_batch(num=128, lo=2000, hi=100000, queries_per_mesh=50000, seed=SEED_MESH):
+    """Batched-mesh workload: `num` icosphere-derived meshes with target
+    triangle counts log-uniform in [lo, hi]; each takes the smallest
+    icosphere level with at least that many faces and keeps its first
+    `target` faces (open meshes allowed), plus `queries_per_mesh` queries
+    uniform in [-1.5, 1.5]^3.  Returns (verts (V,3), tris (T,3) int32 with
+    global vertex indices, tri offsets (num+1,), queries (Q,3), query
+    offsets (num+1,))."""
+    u = lcg_streams(num, seed, 1)[:, 0].astype(np.float64)
+    targets = np.floor(np.exp(np.log(lo) + u * (np.log(hi) - np.log(lo)))).astype(np.int64)
+    verts, tris, qs = [], [], []
+    vbase = 0
+    toff = [0]
+    for m in range(num):
+        level = 0
+        while 20 * 4 ** level < targets[m]:
+            level += 1
+        key = (level, seed * 1000 + m)
+        v, t = icosphere(level, seed=seed * 1000 + m)
+        t = t[: targets[m]]
+        verts.append(v)
+        tris.append(t + vbase)
+        vbase += len(v)
+        toff.append(toff[-1] + len(t))
+        qs.append(uniform_points(queries_per_mesh, seed * 7919 + m, -1.5, 1.5))
+    qoff = np.arange(num + 1, dtype=np.int64) * queries_per_mesh
+    return (np.concatenate(verts), np.concatenate(tris).astype(np.int32), np.array(toff, dtype=np.int64),
+            np.concatenate(qs), qoff)

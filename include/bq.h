@@ -96,7 +96,8 @@ typedef struct bq_query_config {
   int stackDepth;    /* fast-path stack entries: 32, 64 or 128 (0 = 64) */
   int blockSize;     /* threads per block: 64..512 (0 = 128) */
   int reorder;       /* 1 = process queries in Morton order, 0 = input order */
-  int queriesPerWarp;/* 32 = one thread per query (only value so far; 0 = 32) */
+  int queriesPerWarp;/* one thread per query; queries a warp takes per work grab in the
+                        persistent batched kernel (multiple of 32, <= 1024; 0 = 32) */
 } bq_query_config;
 
 /* ---------------------------------------------------------------- */
@@ -178,6 +179,77 @@ int bq_tri_closest_f3(const bq_bvh3f *bvh, const int32_t *tris, const float *ver
 int bq_tri_distance_bwd_f3(const int32_t *tris, const float *verts, uint32_t numVerts, const float *queries,
                            uint32_t numQueries, const int32_t *ids, const float *gradSqr, float *gradQueries,
                            float *gradVerts, const bq_allocator *alloc, bq_stream_t stream);
+
+/* ---------------------------------------------------------------- */
+/* batches of clouds (no counterpart in the reference, which builds    */
+/* and queries one cloud per call)                                      */
+/* ---------------------------------------------------------------- */
+
+/* Builds one Morton63 BVH per cloud for numSegs clouds stored back to
+   back: cloud s owns boxes[segOffsets[s] .. segOffsets[s+1]) (segOffsets:
+   device array of numSegs+1 entries, segOffsets[numSegs] == numPrims).
+   Each cloud's tree is exactly bq_build_morton63_f3's tree for that cloud
+   alone.  Outputs go to caller buffers: nodes (2*numPrims entries; cloud s
+   uses the block starting at 2*segOffsets[s]), primIDs (numPrims entries,
+   cloud-local ids) and bvhs (device array of numSegs descriptors pointing
+   into those buffers).  Every box must be non-empty.  No host
+   synchronisation: the call can be captured in a CUDA graph (use the
+   NULL allocator or a capture-safe one).  deviceErr (may be NULL) receives
+   BQ device error bits; it is not read back. */
+int bq_batched_build_morton63_f3(const bq_box3f *boxes, const uint32_t *segOffsets, uint32_t numSegs,
+                                 uint32_t numPrims, const bq_build_config *cfg, bq_node3f *nodes, uint32_t *primIDs,
+                                 bq_bvh3f *bvhs, uint32_t *deviceErr, const bq_allocator *alloc, bq_stream_t stream);
+
+/* k nearest points per query over a batch built by the call above.
+   Queries are stored cloud by cloud (queryOffsets: device, numSegs+1
+   entries); query q of cloud s searches only cloud s (whose points start
+   at points + 3*pointOffsets[s]).  ids are cloud-local.  A persistent
+   work-stealing kernel answers the whole batch; qcfg->queriesPerWarp
+   (a multiple of 32, default 32) is the number of queries a warp takes
+   per grab.  No host synchronisation. */
+int bq_batched_knn_f3(const bq_bvh3f *bvhs, const uint32_t *pointOffsets, const float *points, const float *queries,
+                      const uint32_t *queryOffsets, uint32_t numSegs, uint32_t numQueries, int k, float maxSqrDist,
+                      const bq_query_config *qcfg, int32_t *ids, float *sqrDist, int32_t *numFound,
+                      uint32_t *deviceErr, const bq_allocator *alloc, bq_stream_t stream);
+
+/* Refits every tree of a batch (after its boxes moved): segOffsets,
+   nodes, primIDs and bvhs as produced by bq_batched_build_morton63_f3;
+   boxes holds the batch's boxes back to back.  One launch pair for all
+   trees, no host synchronisation. */
+int bq_batched_refit_f3(const bq_bvh3f *bvhs, const uint32_t *segOffsets, uint32_t numSegs, uint32_t numPrims,
+                        bq_node3f *nodes, const uint32_t *primIDs, const bq_box3f *boxes, const bq_allocator *alloc,
+                        bq_stream_t stream);
+
+/* Closest triangle per query over a batch of meshes built with
+   bq_batched_build_morton63_f3 over triangle boxes: mesh s owns triangles
+   tris[triOffsets[s] .. triOffsets[s+1]) (int32 vertex indices into one
+   shared verts array); its queries are queries[queryOffsets[s] ..
+   queryOffsets[s+1]).  ids are GLOBAL triangle indices (so
+   bq_tri_distance_bwd_f3 can run on the shared arrays); -1 / +inf when
+   nothing is within maxSqrDist.  No host synchronisation. */
+int bq_batched_tri_closest_f3(const bq_bvh3f *bvhs, const uint32_t *triOffsets, const int32_t *tris,
+                              const float *verts, const float *queries, const uint32_t *queryOffsets,
+                              uint32_t numSegs, uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg,
+                              int32_t *ids, float *sqrDist, float *P, uint32_t *deviceErr, const bq_allocator *alloc,
+                              bq_stream_t stream);
+
+/* Launch-shape autotuner for a batched build + kNN workload: times every
+   combination of leaf threshold {1,2,4,8}, stack depth {32,64}, block
+   size {64,128} and queries per warp {32,128} on the given inputs (CUDA
+   events, after one warm-up) and returns the fastest.  With the default
+   tie rule the answers do not depend on these knobs, only the time. */
+typedef struct bq_tuning {
+  int makeLeafThreshold;
+  int stackDepth;
+  int blockSize;
+  int queriesPerWarp;
+  float buildMs;
+  float queryMs;
+} bq_tuning;
+int bq_autotune_batched_knn_f3(const bq_box3f *boxes, const float *points, const uint32_t *segOffsets,
+                               uint32_t numSegs, uint32_t numPrims, const float *queries, const uint32_t *queryOffsets,
+                               uint32_t numQueries, int k, bq_tuning *best, const bq_allocator *alloc,
+                               bq_stream_t stream);
 
 /* ---------------------------------------------------------------- */
 /* input helpers                                                      */

@@ -994,3 +994,203 @@ int orc_tri_grad_f64(const int32_t *tris, const float *verts, const float *queri
   }
   return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* rebinning Morton builder, 30-bit keys (cuBQL/builder/cuda/          */
+/* rebinMortonBuilder.h:1161-1488), restated level-synchronously with   */
+/* children allocated in node order (canonical BFS-like numbering).     */
+/* ------------------------------------------------------------------ */
+static uint32_t spread3_10(uint32_t x)
+{
+  uint32_t r = 0;
+  for (int i = 0; i < 10; i++) r |= ((x >> i) & 1u) << (3 * i);
+  return r;
+}
+
+/* Quantizer<float,3> with 10 bits (rebinMortonBuilder.h:33-61) over a
+   centroid domain lo/hi */
+static uint32_t morton30(const float c[3], const float lo[3], const float hi[3])
+{
+  float sz[3];
+  for (int d = 0; d < 3; d++) sz[d] = hi[d] - lo[d];
+  float ext = fmaxf(fmaxf(sz[0], sz[1]), sz[2]);
+  float scale = 1024.0f * (1.0f / fmaxf(ext, 1e-20f));
+  uint32_t cell[3];
+  for (int d = 0; d < 3; d++) {
+    float f = (c[d] - lo[d]) * scale;
+    uint32_t u = !(f > 0.0f) ? 0u : (f >= 4294967296.0f ? 0xFFFFFFFFu : (uint32_t)f);
+    cell[d] = u < 1023u ? u : 1023u;
+  }
+  return spread3_10(cell[0]) | (spread3_10(cell[1]) << 1) | (spread3_10(cell[2]) << 2);
+}
+
+/* findSplit on 32-bit keys (rebinMortonBuilder.h:566-590) */
+static int find_split32(int64_t *split, const uint32_t *keys, int64_t begin, int64_t end)
+{
+  uint32_t fk = keys[begin], lk = keys[end - 1];
+  if (fk == lk) return 0;
+  int nm = __builtin_clz(fk ^ lk);
+  uint32_t sk = (uint32_t)(lk & (0xFFFFFFFFull << (31 - nm)));
+  while (end > begin) {
+    int64_t mid = (begin + end) / 2;
+    if (keys[mid] < sk) begin = mid + 1; else end = mid;
+  }
+  *split = begin;
+  return 1;
+}
+
+/* centroid domain of prims[b..e) */
+static void range_domain(const obox *boxes, const uint32_t *ids, uint64_t b, uint64_t e, float lo[3], float hi[3])
+{
+  for (int d = 0; d < 3; d++) { lo[d] = INFINITY; hi[d] = -INFINITY; }
+  for (uint64_t i = b; i < e; i++) {
+    float c[3];
+    box_center(&boxes[ids[i]], c);
+    for (int d = 0; d < 3; d++) { lo[d] = fminf(lo[d], c[d]); hi[d] = fmaxf(hi[d], c[d]); }
+  }
+}
+
+typedef struct { uint32_t a, b; uint8_t open; } rnode; /* open: [a,b); done: {offset a, count b} */
+
+int orc_rebin_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int maxAllowedLeafSize, onode *nodes,
+                    uint32_t *primIDs, uint32_t *numNodes, uint32_t *numPrims)
+{
+  int thr = makeLeafThreshold > 0
+              ? (makeLeafThreshold < maxAllowedLeafSize ? makeLeafThreshold : maxAllowedLeafSize)
+              : 1;
+  int32_t cbLo[3], cbHi[3];
+  for (int d = 0; d < 3; d++) { cbLo[d] = enc_f(FLT_MAX); cbHi[d] = enc_f(-FLT_MAX); }
+  uint32_t nv = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    if (box_empty(&boxes[i])) continue;
+    float c[3];
+    box_center(&boxes[i], c);
+    for (int d = 0; d < 3; d++) {
+      int32_t e = enc_f(c[d]);
+      if (e < cbLo[d]) cbLo[d] = e;
+      if (e > cbHi[d]) cbHi[d] = e;
+    }
+    nv++;
+  }
+  if (nv == 0) { *numNodes = 0; *numPrims = 0; return 0; }
+  float glo[3], ghi[3];
+  for (int d = 0; d < 3; d++) { glo[d] = dec_f(cbLo[d]); ghi[d] = dec_f(cbHi[d]); }
+  uint64_t *k64 = (uint64_t *)malloc(sizeof(uint64_t) * nv);
+  uint32_t *keys = (uint32_t *)malloc(sizeof(uint32_t) * nv);
+  uint32_t j = 0;
+  for (uint32_t i = 0; i < n; i++) {               /* computeUnsortedKeysAndPrimIDs (:503-533) */
+    if (box_empty(&boxes[i])) continue;
+    float c[3];
+    box_center(&boxes[i], c);
+    k64[j] = morton30(c, glo, ghi);
+    primIDs[j] = i;
+    j++;
+  }
+  stable_sort_pairs(k64, primIDs, nv, 0, 32);      /* SortPairs bits [0,32) (:1235-1257) */
+  for (uint32_t i = 0; i < nv; i++) keys[i] = (uint32_t)k64[i];
+  uint64_t cap = 2ull * nv + 2;
+  rnode *t = (rnode *)calloc(cap, sizeof(rnode));
+  t[0].a = 0; t[0].b = nv; t[0].open = 1;          /* initNodes (:674-687) */
+  uint64_t alloc = 2;
+  /* broad phase with rebinning restarts (:1283-1393); the first pass
+     sees the root only, a restart sees every node allocated so far */
+  uint64_t done = 0, upTo = 1;
+  for (;;) {
+    while (done < upTo) {
+      uint64_t end = upTo;
+      for (uint64_t id = done; id < end; id++) {
+        if (id == 1 || !t[id].open) continue;
+        uint32_t b = t[id].a, e = t[id].b, size = e - b;
+        int64_t split;
+        if ((int64_t)size <= thr) { t[id].a = b; t[id].b = size; t[id].open = 0; }
+        else if (size <= 32) { /* leaves broad phase, stays open */ }
+        else if (!find_split32(&split, keys, b, e)) { /* rebin job, stays open */ }
+        else {
+          uint64_t c = alloc; alloc += 2;
+          t[c].a = b; t[c].b = (uint32_t)split; t[c].open = 1;
+          t[c + 1].a = (uint32_t)split; t[c + 1].b = e; t[c + 1].open = 1;
+          t[id].a = (uint32_t)c; t[id].b = 0; t[id].open = 0;
+        }
+      }
+      done = end;
+      upTo = alloc;
+    }
+    /* rebin every still-open node larger than the broad-phase limit */
+    int jobs = 0;
+    for (uint64_t id = 0; id < alloc; id++) {
+      if (id == 1 || !t[id].open) continue;
+      uint32_t b = t[id].a, e = t[id].b;
+      if (e - b <= 32) continue;
+      jobs++;
+      float lo[3], hi[3];
+      range_domain(boxes, primIDs, b, e, lo, hi);
+      int degenerate = lo[0] == hi[0] && lo[1] == hi[1] && lo[2] == hi[2];
+      uint64_t *nk = (uint64_t *)malloc(sizeof(uint64_t) * (e - b));
+      uint32_t *nid = (uint32_t *)malloc(sizeof(uint32_t) * (e - b));
+      for (uint32_t i = b; i < e; i++) {           /* rebinCreateNewKeysAndPrimIDs (:1022-1063) */
+        float c[3];
+        box_center(&boxes[primIDs[i]], c);
+        nk[i - b] = degenerate ? (i - b) : morton30(c, lo, hi);
+        nid[i - b] = primIDs[i];
+      }
+      stable_sort_pairs(nk, nid, e - b, 0, 32);    /* sort by (range, morton), stable */
+      for (uint32_t i = b; i < e; i++) { keys[i] = (uint32_t)nk[i - b]; primIDs[i] = nid[i - b]; }
+      free(nk);
+      free(nid);
+    }
+    if (!jobs) break;
+    done = 0;
+    upTo = alloc;
+  }
+  /* thread phase (:766-872, :1413-1426) */
+  {
+    done = 0;
+    while (done < alloc) {
+      uint64_t end = alloc;
+      for (uint64_t id = done; id < end; id++) {
+        if (id == 1 || !t[id].open) continue;
+        uint32_t b = t[id].a, e = t[id].b, size = e - b;
+        int64_t split;
+        int doSplit = 0;
+        if ((int64_t)size <= thr) { t[id].a = b; t[id].b = size; t[id].open = 0; continue; }
+        if (find_split32(&split, keys, b, e)) doSplit = 1;
+        else {
+          float lo[3], hi[3];
+          range_domain(boxes, primIDs, b, e, lo, hi);
+          int degenerate = lo[0] == hi[0] && lo[1] == hi[1] && lo[2] == hi[2];
+          for (uint32_t i = b; i < e; i++) {
+            float c[3];
+            box_center(&boxes[primIDs[i]], c);
+            keys[i] = degenerate ? (i - b) : morton30(c, lo, hi);
+          }
+          for (uint32_t x = b; x < e; x++)         /* bubbleSort (:756-764), not stable */
+            for (uint32_t y = x + 1; y < e; y++)
+              if (keys[y] < keys[x]) {
+                uint32_t tk = keys[x]; keys[x] = keys[y]; keys[y] = tk;
+                uint32_t ti = primIDs[x]; primIDs[x] = primIDs[y]; primIDs[y] = ti;
+              }
+          if (find_split32(&split, keys, b, e)) doSplit = 1;
+          else { t[id].a = b; t[id].b = size; t[id].open = 0; continue; }
+        }
+        if (doSplit) {
+          uint64_t c = alloc; alloc += 2;
+          t[c].a = b; t[c].b = (uint32_t)split; t[c].open = 1;
+          t[c + 1].a = (uint32_t)split; t[c + 1].b = e; t[c + 1].open = 1;
+          t[id].a = (uint32_t)c; t[id].b = 0; t[id].open = 0;
+        }
+      }
+      done = end;
+    }
+  }
+  for (uint64_t i = 0; i < alloc; i++) {
+    memset(&nodes[i], 0, sizeof(onode));
+    nodes[i].admin = (i == 1) ? 0 : ADMIN(t[i].a, t[i].b);
+  }
+  *numNodes = (uint32_t)alloc;
+  *numPrims = nv;
+  refit_tree(nodes, *numNodes, primIDs, boxes);
+  free(t);
+  free(keys);
+  free(k64);
+  return 0;
+}

@@ -102,6 +102,10 @@ class Oracle:
         out = (nodes[: nn.value].copy(), prims[: npr.value].copy())
         return out + (k[: npr.value].copy(),) if keys else out
 
+    def rebin_build(self, boxes, makeLeafThreshold=0, maxAllowedLeafSize=1 << 15):
+        return self._tree(self.lib.orc_rebin_build, boxes, ctypes.c_int(makeLeafThreshold),
+                          ctypes.c_int(maxAllowedLeafSize))
+
     def sm_build(self, boxes, makeLeafThreshold=0):
         return self._tree(self.lib.orc_sm_build, boxes, ctypes.c_int(makeLeafThreshold))
 
