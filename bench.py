@@ -115,9 +115,16 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def weak_value(units_per_rank, ms_max, world):
+    """Whole-job throughput in M units/s: every rank processes the same
+    number of units; the job takes as long as its slowest rank."""
+    return world * units_per_rank / ms_max / 1e3
 
 
 def barrier(world):
@@ -261,6 +268,14 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
     ms = ev_time(smb)
     comp["spatial_median_build"] = {"ms": ms, "Mprims_s": n / ms / 1e3, "leaf": 8,
                                     "vs_published_reference_13ms": 13.0 / ms}
+    with bq.profile() as prof:
+        smb()
+    comp["spatial_median_build"]["phases_ms"] = {k: round(v[1], 4) for k, v in prof.table.items()}
+
+    def smb1():
+        bq.gpuBuilder(boxes_t, bq.BuildConfig(makeLeafThreshold=1)).free()
+    ms = ev_time(smb1)
+    comp["spatial_median_build_leaf1"] = {"ms": ms, "Mprims_s": n / ms / 1e3, "leaf": 1}
     # queries on the Morton tree (leaf 1)
     bvh = bq.cuda.radixBuilder(boxes_t)
     qs = torch.from_numpy(W.uniform_points(n, W.SEED_QUERIES)).cuda()
@@ -360,7 +375,7 @@ def run_ours(args):
     ms = time_loop(lambda: cb.step(sptr), args.steps, args.warmup, world)
     clk = clocks.stop()
     ms_max = max_over_ranks(ms, world)
-    value = world * n / ms_max / 1e3  # Mprims/s
+    value = weak_value(n, ms_max, world)
     if args.only_build:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "Mprims/s", "ms_per_step": ms_max,

@@ -5,6 +5,7 @@ calling the CUDA library libbq.so through its C ABI (include/bq.h):
 
     cuBQL::gpuBuilder            -> gpuBuilder(boxes, BuildConfig)
     cuBQL::cuda::radixBuilder    -> cuda.radixBuilder(boxes, BuildConfig)
+    cuBQL::cuda::rebinRadixBuilder -> cuda.rebinRadixBuilder(boxes, BuildConfig)
     cuBQL::cuda::free            -> cuda.free(bvh)
     gpuBuilder_impl::refit       -> refit(bvh, boxes)
     points::findClosest          -> points.findClosest(bvh, points, queries)
@@ -85,6 +86,8 @@ _F = ctypes.c_float
 _SIGS = {
     "bq_build_morton63_f3": [ctypes.POINTER(bq_bvh3f), _P, _U, ctypes.POINTER(bq_build_config),
                              ctypes.POINTER(bq_allocator), _P],
+    "bq_build_rebin_morton30_f3": [ctypes.POINTER(bq_bvh3f), _P, _U, ctypes.POINTER(bq_build_config),
+                                   ctypes.POINTER(bq_allocator), _P],
     "bq_build_spatial_median_f3": [ctypes.POINTER(bq_bvh3f), _P, _U, ctypes.POINTER(bq_build_config),
                                    ctypes.POINTER(bq_allocator), _P],
     "bq_refit_f3": [ctypes.POINTER(bq_bvh3f), _P, ctypes.POINTER(bq_allocator), _P],
@@ -288,6 +291,12 @@ class cuda:
     def radixBuilder(boxes, config=None, allocator=None):
         """cuBQL::cuda::radixBuilder (cuBQL/builder/cuda.h:134-140), 63-bit keys."""
         return _build(_lib.bq_build_morton63_f3, boxes, config, allocator)
+
+    @staticmethod
+    def rebinRadixBuilder(boxes, config=None, allocator=None):
+        """cuBQL::cuda::rebinRadixBuilder (cuBQL/builder/cuda.h:143-154), 30-bit
+        keys with rebinning of equal-key runs."""
+        return _build(_lib.bq_build_rebin_morton30_f3, boxes, config, allocator)
 
     @staticmethod
     def free(bvh):

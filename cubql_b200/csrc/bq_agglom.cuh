@@ -100,8 +100,9 @@ __device__ __forceinline__ AggBox agg_union(const AggBox &left, const AggBox &ri
                 fmaxf(left.hx, right.hx), fmaxf(left.hy, right.hy), fmaxf(left.hz, right.hz)};
 }
 
-struct AggArgs {
-  const uint8_t *delta;   // split level of pair (i, i+1)
+template <typename LevT>
+struct AggArgsT {
+  const LevT *delta;      // split level of pair (i, i+1)
   uint32_t *slot;         // global slots, AGG_EMPTY on entry
   const uint32_t *ids;    // sorted prim ids (global indices)
   const bq_box3f *boxes;
@@ -113,9 +114,10 @@ struct AggArgs {
   const uint32_t *off;    // SEG: cloud offsets
   uint32_t numSegs;
 };
+using AggArgs = AggArgsT<uint8_t>;
 
-template <bool SEG>
-__global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgs a)
+template <bool SEG, typename LevT>
+__global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
 {
   __shared__ uint32_t sSlot[AGG_CHUNK + 1];
   __shared__ AggBox sBox[AGG_CHUNK + 1][2];
@@ -174,8 +176,8 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgs a)
   }
 }
 
-template <bool SEG>
-__global__ void k_agg_global(AggArgs a, uint32_t numPending)
+template <bool SEG, typename LevT>
+__global__ void k_agg_global(AggArgsT<LevT> a, uint32_t numPending)
 {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numPending) return;
@@ -214,13 +216,14 @@ __global__ void k_agg_global(AggArgs a, uint32_t numPending)
   }
 }
 
-// launches both phases for nvMax (upper bound of *nvPtr) prims
-template <bool SEG>
-inline int agglomerate(AggArgs a, uint32_t nvMax, cudaStream_t s)
+// launches both phases for nvMax (upper bound of *nvPtr) prims; split
+// levels are 8-bit (Morton-63 builders) or 16-bit (rebin builder)
+template <bool SEG, typename LevT>
+inline int agglomerate(AggArgsT<LevT> a, uint32_t nvMax, cudaStream_t s)
 {
   const int chunks = div_up(nvMax, AGG_CHUNK);
-  k_agg_local<SEG><<<chunks, AGG_CHUNK, 0, s>>>(a);
-  k_agg_global<SEG><<<div_up(2 * chunks, 128), 128, 0, s>>>(a, 2u * chunks);
+  k_agg_local<SEG, LevT><<<chunks, AGG_CHUNK, 0, s>>>(a);
+  k_agg_global<SEG, LevT><<<div_up(2 * chunks, 128), 128, 0, s>>>(a, 2u * chunks);
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }

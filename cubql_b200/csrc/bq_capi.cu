@@ -6,6 +6,7 @@
 
 namespace bq {
 int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
+int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
 int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
 int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al);
 int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
@@ -95,6 +96,14 @@ int bq_build_morton63_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims
   BQ_TRY(check_build(bvh, boxes, numPrims));
   Alloc al = make_alloc(alloc, stream);
   return build_morton63(bvh, boxes, numPrims, cfg, al);
+}
+
+int bq_build_rebin_morton30_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
+                               const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_build(bvh, boxes, numPrims));
+  Alloc al = make_alloc(alloc, stream);
+  return build_rebin_morton30(bvh, boxes, numPrims, cfg, al);
 }
 
 int bq_build_spatial_median_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,

@@ -145,6 +145,30 @@ __host__ __device__ __forceinline__ float dec_f(int32_t b)
 #endif
 }
 
+// Block-wide min/max of encoded coordinates, merged into lohi[0..2] (min)
+// and lohi[3..5] (max) with one atomic per block and component.  Every
+// thread of the block (BLOCK threads, full warps) must call it.
+template <int BLOCK>
+__device__ __forceinline__ void block_merge_bounds(const int32_t lo[3], const int32_t hi[3], int32_t *lohi)
+{
+  __shared__ int32_t sRed[6][BLOCK / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const int32_t mn = __reduce_min_sync(0xffffffffu, lo[d]);
+    const int32_t mx = __reduce_max_sync(0xffffffffu, hi[d]);
+    if (lane == 0) { sRed[d][warp] = mn; sRed[3 + d][warp] = mx; }
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const bool isMin = threadIdx.x < 3;
+    int32_t v = isMin ? INT_MAX : INT_MIN;
+    for (int w = 0; w < BLOCK / 32; w++) v = isMin ? min(v, sRed[threadIdx.x][w]) : max(v, sRed[threadIdx.x][w]);
+    if (isMin && v != INT_MAX) atomicMin(&lohi[threadIdx.x], v);
+    if (!isMin && v != INT_MIN) atomicMax(&lohi[threadIdx.x], v);
+  }
+}
+
 // ------------------------------------------------------------------
 // squared distances with the FMA shapes the reference's device code
 // compiles to (pinned against the reference kernels on B200):

@@ -6,32 +6,40 @@
 // centre >= pos go right); a node whose centroid bounds are flat or too thin
 // to split (dim == -1) deals its prims to the two sides alternately.
 //
-// Different mechanics, B200-first: the reference re-reads every prim at
-// every level and grows child counts and centroid boxes with global
-// atomics (shared-memory ones for the first 512 new nodes).  Here each
-// level works on a compacted array holding only the prims of still-open
-// nodes, stored as float4 (centre xyz, primID):
-//   k_sm_select    per open node: leaf (prims copied to their final slots)
-//                  or split plane
-//   scans          child numbering (BFS order, like a level-synchronous
-//                  allocator) and the next level's compacted layout
-//   k_sm_flags     per prim: side; one scan of the right-side flags gives
-//                  every prim its stable position inside its child
-//   k_sm_children  per split node: child ranges, child node ids
-//   k_sm_scatter   per prim: move to the next level's array
-//   k_sm_bounds    per tile: centroid bounds of the children, reduced in
-//                  shared memory; one atomicMin/Max per (tile, node) merges
-//                  tiles (min/max is order-independent: deterministic)
+// Different mechanics, B200-first.  The reference re-reads every prim at
+// every level, grows child counts and centroid boxes with global atomics
+// and syncs the host once per level down to the leaves.  Here:
+//   * prims live as float4 (centre xyz, primID) in one of two buffers and
+//     are partitioned stably, so every node owns a contiguous range and the
+//     final prim order is the in-order leaf order;
+//   * node slots follow from the partition: the children of a node split at
+//     prim position m go to slots 2m, 2m+1 (root at 0) -- no allocation
+//     counters; one scan over the used split positions compacts the slots at
+//     the end (children of the k-th used split at nodes 2+2k, 2+2k+1; node 1
+//     stays unused, as in the reference);
+//   * nodes with more than SM_WARP_MAX prims are split level by level over
+//     the whole GPU in tiles of SM_TILE prims: k_sm_count (right-side count
+//     per tile), one scan, k_sm_children, k_sm_scatter (stable scatter that
+//     also reduces the children's centroid bounds per tile and merges them
+//     with one atomicMin/Max per tile -- min/max is order-independent, so
+//     the result is deterministic);
+//   * every subtree of at most SM_WARP_MAX prims is finished by one warp
+//     (k_sm_warp), depth first, smaller child first with the larger one on a
+//     per-warp shared-memory stack; a node of up to 32 prims is held in
+//     registers, one prim per lane, and its whole subtree is partitioned
+//     with ballots and a 512-byte shared exchange buffer.
 // Degenerate nodes send their k-th prim (primID order) to side
-// (t0 + k) & 1, where t0 is the encoded centroid lower-z: that is the
-// start value of the reference's tie-break counter, which aliases that
-// field (sm_builder.h:82-103, 362-364), so child sizes match it exactly.
-// Leaves list their prims in ascending primID order, like the
+// (t0 + k) & 1, where t0 is the encoded centroid lower-z: that is the start
+// value of the reference's tie-break counter, which aliases that field
+// (sm_builder.h:82-103, 362-364), so child sizes match it exactly.  The
+// partitions are stable, so "k-th in the node" is the k-th in primID order
+// and leaves list their prims in ascending primID order, like the
 // reference's final (nodeID, primID) sort (sm_builder.h:565-605).
-// One small device-to-host read per level decides when to stop.
 #include <algorithm>
 #include <climits>
 #include <cfloat>
+#include <cstring>
+#include <vector>
 
 #include "bq_internal.cuh"
 
@@ -40,15 +48,112 @@ int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al);
 
 namespace {
 
+constexpr uint32_t SM_WARP_MAX = 4096;  // subtrees up to this size: one warp
+constexpr uint32_t SM_TILE = 4096;      // prims per tile in the global levels
+constexpr int SM_BLOCK = 256;           // global-level kernels
+constexpr int SMW_BLOCK = 128;          // warp-phase kernel
+constexpr int SMW_WARPS = SMW_BLOCK / 32;
+constexpr int SMW_STACK = 24;           // >= log2(SM_WARP_MAX) + 1
+
+// A node still to be split: prim range [b, e) in buffer `parity`, its slot,
+// and its prims' centroid bounds (encoded, see enc_f).
 struct SmNode {
-  uint32_t cbegin, count, fbegin, nodeID;
+  uint32_t b, e, slot, parity;
   int32_t lo[3], hi[3];
 };
+static_assert(sizeof(SmNode) == 40, "SmNode size");
 
-constexpr int SB_TILE = 1024;
+struct SmTile {
+  uint32_t node, begin, end;
+};
+
+struct SmSplit {
+  int dim;
+  float pos;
+  uint32_t tb;
+};
 
 __device__ __forceinline__ float ctr2(float lo, float hi) { return __fdiv_rn(__fadd_rn(lo, hi), 2.0f); }
 
+// selectSplits (sm_builder.h:192-219)
+__device__ __forceinline__ SmSplit choose_split(const SmNode &nd)
+{
+  float widestWidth = 0.f, wLo = 0.f, wHi = 0.f, wCtr = 0.f;
+  int widestDim = -1;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    const float l = dec_f(nd.lo[d]), h = dec_f(nd.hi[d]);
+    const float width = __fsub_rn(h, l);
+    if (width <= widestWidth) continue;
+    const float c = __fmul_rn(0.5f, __fadd_rn(h, l));
+    widestWidth = width; widestDim = d; wLo = l; wHi = h; wCtr = c;
+  }
+  SmSplit s;
+  s.dim = (widestDim < 0 || wCtr == wLo || wCtr == wHi) ? -1 : widestDim;
+  s.pos = wCtr;
+  s.tb = (uint32_t)nd.lo[2];
+  return s;
+}
+
+__device__ __forceinline__ uint32_t side_of(const float4 c, uint32_t rankInNode, const SmSplit &s)
+{
+  if (s.dim < 0) return (s.tb + rankInNode) & 1u;
+  const float v = s.dim == 0 ? c.x : (s.dim == 1 ? c.y : c.z);
+  return v >= s.pos ? 1u : 0u;
+}
+
+// running encoded min/max of the two children, without dynamic indexing
+struct SideBounds {
+  int32_t lo0[3], hi0[3], lo1[3], hi1[3];
+  __device__ __forceinline__ void init()
+  {
+#pragma unroll
+    for (int d = 0; d < 3; d++) { lo0[d] = lo1[d] = INT_MAX; hi0[d] = hi1[d] = INT_MIN; }
+  }
+  __device__ __forceinline__ void add(const float4 c, uint32_t side)
+  {
+    const int32_t e[3] = {enc_f(c.x), enc_f(c.y), enc_f(c.z)};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      lo0[d] = side ? lo0[d] : min(lo0[d], e[d]);
+      hi0[d] = side ? hi0[d] : max(hi0[d], e[d]);
+      lo1[d] = side ? min(lo1[d], e[d]) : lo1[d];
+      hi1[d] = side ? max(hi1[d], e[d]) : hi1[d];
+    }
+  }
+  __device__ __forceinline__ void warp_reduce()
+  {
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      lo0[d] = __reduce_min_sync(0xffffffffu, lo0[d]);
+      hi0[d] = __reduce_max_sync(0xffffffffu, hi0[d]);
+      lo1[d] = __reduce_min_sync(0xffffffffu, lo1[d]);
+      hi1[d] = __reduce_max_sync(0xffffffffu, hi1[d]);
+    }
+  }
+};
+
+__device__ __forceinline__ void internal_node(Node *out, uint32_t *used, uint32_t slot, uint32_t m)
+{
+  out[slot] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, make_admin(2ull * m, 0));
+  used[m] = 1;
+}
+
+__device__ __forceinline__ void child_pair(const SmNode &nd, uint32_t m, const SideBounds &sb, SmNode &c0, SmNode &c1)
+{
+  c0.b = nd.b; c0.e = m; c0.slot = 2 * m; c0.parity = nd.parity ^ 1u;
+  c1.b = m; c1.e = nd.e; c1.slot = 2 * m + 1; c1.parity = nd.parity ^ 1u;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    c0.lo[d] = sb.lo0[d]; c0.hi[d] = sb.hi0[d];
+    c1.lo[d] = sb.lo1[d]; c1.hi[d] = sb.hi1[d];
+  }
+}
+
+// ------------------------------------------------------------------
+// set-up: valid prims compacted (primID order) as float4, invalid ones
+// listed after them in primIDs, root centroid bounds
+// ------------------------------------------------------------------
 __global__ void k_sm_valid(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t *__restrict__ valid)
 {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -58,151 +163,319 @@ __global__ void k_sm_valid(const bq_box3f *__restrict__ boxes, uint32_t n, uint3
   valid[i] = (a.x <= b.y) ? 1u : 0u;  // initPrims: lower.x <= upper.x (sm_builder.h:134)
 }
 
-__global__ void k_sm_init(const bq_box3f *__restrict__ boxes, uint32_t n, const uint32_t *__restrict__ vpos,
-                          const uint32_t *nvPtr, float4 *__restrict__ pc, uint32_t *__restrict__ pn,
-                          uint32_t *__restrict__ primIDs, SmNode *root)
+// grid-stride over the prims with blocks of 256 (the block reduction needs
+// every thread); root bounds merged once per block
+__global__ void __launch_bounds__(256) k_sm_init(const bq_box3f *__restrict__ boxes, uint32_t n,
+                                                 const uint32_t *__restrict__ vpos, const uint32_t *nvPtr,
+                                                 float4 *__restrict__ pc, uint32_t *__restrict__ primIDs,
+                                                 int32_t *rootLoHi)
 {
   const uint32_t nv = *nvPtr;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) {
-    root->cbegin = 0; root->count = nv; root->fbegin = 0; root->nodeID = 0;
-    for (int d = 0; d < 3; d++) { root->lo[d] = INT_MAX; root->hi[d] = INT_MIN; }
+  int32_t lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const bq_box3f b = boxes[i];
+    const uint32_t p = vpos[i];
+    if (b.lower[0] <= b.upper[0]) {
+      const float4 c = make_float4(ctr2(b.lower[0], b.upper[0]), ctr2(b.lower[1], b.upper[1]),
+                                   ctr2(b.lower[2], b.upper[2]), __uint_as_float((uint32_t)i));
+      pc[p] = c;
+      const int32_t e[3] = {enc_f(c.x), enc_f(c.y), enc_f(c.z)};
+#pragma unroll
+      for (int d = 0; d < 3; d++) { lo[d] = min(lo[d], e[d]); hi[d] = max(hi[d], e[d]); }
+    } else {
+      primIDs[nv + ((uint32_t)i - p)] = (uint32_t)i;  // invalid prims after all valid ones, ascending
+    }
   }
-  if (i >= n) return;
-  const bq_box3f b = boxes[i];
-  const uint32_t p = vpos[i];
-  if (b.lower[0] <= b.upper[0]) {
-    pc[p] = make_float4(ctr2(b.lower[0], b.upper[0]), ctr2(b.lower[1], b.upper[1]), ctr2(b.lower[2], b.upper[2]),
-                        __uint_as_float(i));
-    pn[p] = 0;
-  } else {
-    primIDs[nv + (i - p)] = i;  // invalid prims after all valid ones, ascending
+  block_merge_bounds<256>(lo, hi, rootLoHi);
+}
+
+// ------------------------------------------------------------------
+// global levels (nodes with more than SM_WARP_MAX prims)
+// ------------------------------------------------------------------
+__global__ void __launch_bounds__(SM_BLOCK) k_sm_count(const SmNode *__restrict__ nodes, const SmTile *__restrict__ tiles,
+                                                       uint32_t numTiles, const float4 *__restrict__ buf0,
+                                                       const float4 *__restrict__ buf1, uint32_t *__restrict__ tileRight)
+{
+  __shared__ uint32_t sCnt[SM_BLOCK / 32];
+  const SmTile t = tiles[blockIdx.x];
+  const SmNode nd = nodes[t.node];
+  const SmSplit sp = choose_split(nd);
+  const float4 *src = nd.parity ? buf1 : buf0;
+  uint32_t c = 0;
+#pragma unroll 4
+  for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += SM_BLOCK) c += side_of(src[i], i - nd.b, sp);
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0) sCnt[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t s = 0;
+    for (int w = 0; w < SM_BLOCK / 32; w++) s += sCnt[w];
+    tileRight[blockIdx.x] = s;
+    if (blockIdx.x == 0) tileRight[numTiles] = 0;  // the scan's total slot
   }
 }
 
-__global__ void k_sm_select(const SmNode *__restrict__ list, uint32_t K, int thr, const float4 *__restrict__ pc,
-                            uint32_t *__restrict__ isSplit, uint32_t *__restrict__ splitCount, int *__restrict__ dimArr,
-                            float *__restrict__ posArr, uint32_t *__restrict__ tbArr, Node *__restrict__ out,
-                            uint32_t *__restrict__ primIDs)
+// per node: the split position, the internal node, the two child records
+// (bounds start empty; k_sm_scatter fills them)
+__global__ void k_sm_children(const SmNode *__restrict__ nodes, uint32_t K, const uint32_t *__restrict__ firstTile,
+                              const uint32_t *__restrict__ rightScan, Node *__restrict__ out,
+                              uint32_t *__restrict__ used, SmNode *__restrict__ next)
 {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K) return;
-  const SmNode nd = list[k];
-  if ((int64_t)nd.count <= thr) {  // selectSplits: leaf (sm_builder.h:183-191)
-    out[nd.nodeID] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, make_admin(nd.fbegin, nd.count));
-    for (uint32_t j = 0; j < nd.count; j++) primIDs[nd.fbegin + j] = __float_as_uint(pc[nd.cbegin + j].w);
-    isSplit[k] = 0;
-    splitCount[k] = 0;
-    return;
-  }
-  float widestWidth = 0.f, wLo = 0.f, wHi = 0.f, wCtr = 0.f;
-  int widestDim = -1;
-#pragma unroll
-  for (int d = 0; d < 3; d++) {  // sm_builder.h:192-219
-    const float lo = dec_f(nd.lo[d]), hi = dec_f(nd.hi[d]);
-    const float width = __fsub_rn(hi, lo);
-    if (width <= widestWidth) continue;
-    const float ctr = __fmul_rn(0.5f, __fadd_rn(hi, lo));
-    widestWidth = width; widestDim = d; wLo = lo; wHi = hi; wCtr = ctr;
-  }
-  dimArr[k] = (widestDim < 0 || wCtr == wLo || wCtr == wHi) ? -1 : widestDim;
-  posArr[k] = wCtr;
-  tbArr[k] = (uint32_t)nd.lo[2];
-  isSplit[k] = 1;
-  splitCount[k] = nd.count;
-}
-
-__device__ __forceinline__ int sm_side(const float4 c, uint32_t rankInNode, int dim, float pos, uint32_t tb)
-{
-  if (dim < 0) return (int)((tb + rankInNode) & 1u);
-  const float v = dim == 0 ? c.x : (dim == 1 ? c.y : c.z);
-  return v >= pos ? 1 : 0;
-}
-
-__global__ void k_sm_flags(const float4 *__restrict__ pc, const uint32_t *__restrict__ pn, uint32_t A,
-                           const SmNode *__restrict__ list, const uint32_t *__restrict__ isSplit,
-                           const int *__restrict__ dimArr, const float *__restrict__ posArr,
-                           const uint32_t *__restrict__ tbArr, uint32_t *__restrict__ right)
-{
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) right[A] = 0;
-  if (i >= A) return;
-  const uint32_t k = pn[i];
-  uint32_t r = 0;
-  if (isSplit[k]) r = (uint32_t)sm_side(pc[i], i - list[k].cbegin, dimArr[k], posArr[k], tbArr[k]);
-  right[i] = r;
-}
-
-__global__ void k_sm_children(const SmNode *__restrict__ list, uint32_t K, const uint32_t *__restrict__ isSplit,
-                              const uint32_t *__restrict__ rank, const uint32_t *__restrict__ nextBegin,
-                              const uint32_t *__restrict__ Rx, uint32_t nodeBase, SmNode *__restrict__ next,
-                              Node *__restrict__ out)
-{
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= K || !isSplit[k]) return;
-  const SmNode nd = list[k];
-  const uint32_t nR = Rx[nd.cbegin + nd.count] - Rx[nd.cbegin];
-  const uint32_t nL = nd.count - nR;
-  const uint32_t r = rank[k];
-  const uint32_t child = nodeBase + 2 * r;
-  out[nd.nodeID] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, make_admin(child, 0));
+  const SmNode nd = nodes[k];
+  const uint32_t nR = rightScan[firstTile[k + 1]] - rightScan[firstTile[k]];
+  const uint32_t m = nd.e - nR;  // left child is [b, m)
+  internal_node(out, used, nd.slot, m);
+  SideBounds sb;
+  sb.init();
   SmNode c0, c1;
-  c0.cbegin = nextBegin[k]; c0.count = nL; c0.fbegin = nd.fbegin; c0.nodeID = child;
-  c1.cbegin = nextBegin[k] + nL; c1.count = nR; c1.fbegin = nd.fbegin + nL; c1.nodeID = child + 1;
-  for (int d = 0; d < 3; d++) { c0.lo[d] = c1.lo[d] = INT_MAX; c0.hi[d] = c1.hi[d] = INT_MIN; }
-  next[2 * r] = c0;
-  next[2 * r + 1] = c1;
+  child_pair(nd, m, sb, c0, c1);
+  next[2 * k] = c0;
+  next[2 * k + 1] = c1;
 }
 
-__global__ void k_sm_scatter(const float4 *__restrict__ pc, const uint32_t *__restrict__ pn, uint32_t A,
-                             const SmNode *__restrict__ list, const uint32_t *__restrict__ isSplit,
-                             const int *__restrict__ dimArr, const float *__restrict__ posArr,
-                             const uint32_t *__restrict__ tbArr, const uint32_t *__restrict__ rank,
-                             const uint32_t *__restrict__ nextBegin, const uint32_t *__restrict__ Rx,
-                             float4 *__restrict__ pcNext, uint32_t *__restrict__ pnNext)
+__global__ void __launch_bounds__(SM_BLOCK) k_sm_scatter(const SmNode *__restrict__ nodes,
+                                                         const SmTile *__restrict__ tiles,
+                                                         const uint32_t *__restrict__ firstTile,
+                                                         const uint32_t *__restrict__ rightScan, float4 *buf0,
+                                                         float4 *buf1, SmNode *next)
 {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A) return;
-  const uint32_t k = pn[i];
-  if (!isSplit[k]) return;
-  const SmNode nd = list[k];
-  const float4 c = pc[i];
-  const int side = sm_side(c, i - nd.cbegin, dimArr[k], posArr[k], tbArr[k]);
-  const uint32_t rb = Rx[nd.cbegin];
-  const uint32_t rBefore = Rx[i] - rb;
-  const uint32_t nL = nd.count - (Rx[nd.cbegin + nd.count] - rb);
-  const uint32_t dest = side ? nextBegin[k] + nL + rBefore : nextBegin[k] + (i - nd.cbegin) - rBefore;
-  pcNext[dest] = c;
-  pnNext[dest] = 2 * rank[k] + side;
-}
-
-__global__ void __launch_bounds__(256) k_sm_bounds(const float4 *__restrict__ pc, const uint32_t *__restrict__ pn,
-                                                   uint32_t A, SmNode *__restrict__ list)
-{
-  __shared__ int32_t sLo[3][SB_TILE], sHi[3][SB_TILE];
-  const uint32_t t0 = blockIdx.x * SB_TILE;
-  const uint32_t t1 = min(A, t0 + SB_TILE);
-  const uint32_t first = pn[t0];
-  const uint32_t nLocal = pn[t1 - 1] - first + 1;  // pn is non-decreasing
-  for (uint32_t j = threadIdx.x; j < nLocal; j += blockDim.x)
-    for (int d = 0; d < 3; d++) { sLo[d][j] = INT_MAX; sHi[d][j] = INT_MIN; }
-  __syncthreads();
-  for (uint32_t i = t0 + threadIdx.x; i < t1; i += blockDim.x) {
-    const float4 c = pc[i];
-    const uint32_t j = pn[i] - first;
-    const int32_t e0 = enc_f(c.x), e1 = enc_f(c.y), e2 = enc_f(c.z);
-    atomicMin(&sLo[0][j], e0); atomicMin(&sLo[1][j], e1); atomicMin(&sLo[2][j], e2);
-    atomicMax(&sHi[0][j], e0); atomicMax(&sHi[1][j], e1); atomicMax(&sHi[2][j], e2);
+  __shared__ uint32_t sWarp[SM_BLOCK / 32];
+  __shared__ int32_t sRed[12][SM_BLOCK / 32];
+  const SmTile t = tiles[blockIdx.x];
+  const SmNode nd = nodes[t.node];
+  const SmSplit sp = choose_split(nd);
+  const float4 *src = nd.parity ? buf1 : buf0;
+  float4 *dst = nd.parity ? buf0 : buf1;
+  const uint32_t nodeRight0 = rightScan[firstTile[t.node]];
+  const uint32_t m = nd.e - (rightScan[firstTile[t.node + 1]] - nodeRight0);
+  uint32_t rBefore = rightScan[blockIdx.x] - nodeRight0;  // this node's rights before the tile
+  uint32_t lBefore = (t.begin - nd.b) - rBefore;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  SideBounds sb;
+  sb.init();
+  for (uint32_t base = t.begin; base < t.end; base += SM_BLOCK) {
+    const uint32_t i = base + threadIdx.x;
+    const bool valid = i < t.end;
+    float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t side = 0;
+    if (valid) {
+      c = src[i];
+      side = side_of(c, i - nd.b, sp);
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, valid && side);
+    if (lane == 0) sWarp[warp] = __popc(bal);
+    __syncthreads();
+    uint32_t rw = 0, rtot = 0;
+#pragma unroll
+    for (int w = 0; w < SM_BLOCK / 32; w++) {
+      const uint32_t x = sWarp[w];
+      rw += (w < warp) ? x : 0u;
+      rtot += x;
+    }
+    if (valid) {
+      const uint32_t rMine = rw + __popc(bal & lt);  // rights of this chunk before me
+      dst[side ? m + rBefore + rMine : nd.b + lBefore + (threadIdx.x - rMine)] = c;
+      sb.add(c, side);
+    }
+    const uint32_t chunk = min((uint32_t)SM_BLOCK, t.end - base);
+    rBefore += rtot;
+    lBefore += chunk - rtot;
+    __syncthreads();
   }
-  __syncthreads();
-  for (uint32_t j = threadIdx.x; j < nLocal; j += blockDim.x) {
-    if (sLo[0][j] == INT_MAX && sHi[0][j] == INT_MIN) continue;
-    SmNode *nd = list + first + j;
+  sb.warp_reduce();
+  if (lane == 0) {
+#pragma unroll
     for (int d = 0; d < 3; d++) {
-      atomicMin(&nd->lo[d], sLo[d][j]);
-      atomicMax(&nd->hi[d], sHi[d][j]);
+      sRed[d][warp] = sb.lo0[d]; sRed[3 + d][warp] = sb.hi0[d];
+      sRed[6 + d][warp] = sb.lo1[d]; sRed[9 + d][warp] = sb.hi1[d];
     }
   }
+  __syncthreads();
+  if (threadIdx.x < 12) {
+    const int j = threadIdx.x, comp = j % 6;
+    const bool isMin = comp < 3;
+    int32_t v = isMin ? INT_MAX : INT_MIN;
+    for (int w = 0; w < SM_BLOCK / 32; w++) v = isMin ? min(v, sRed[j][w]) : max(v, sRed[j][w]);
+    SmNode *child = next + 2 * t.node + (j / 6);
+    if (isMin) {
+      if (v != INT_MAX) atomicMin(&child->lo[comp], v);
+    } else {
+      if (v != INT_MIN) atomicMax(&child->hi[comp - 3], v);
+    }
+  }
+}
+
+// ------------------------------------------------------------------
+// warp phase: whole subtrees of at most SM_WARP_MAX prims
+// ------------------------------------------------------------------
+__device__ __forceinline__ void leaf_node(Node *out, uint32_t slot, uint32_t b, uint32_t count)
+{
+  out[slot] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, make_admin(b, count));
+}
+
+// A node of 2..32 prims: lane j holds the prim at position nd.b + j, the
+// whole subtree is built in registers.  Stack entries go to stk[0..].
+__device__ void sm_small_subtree(const SmNode &root, const float4 *src, int thr, float4 *xbuf, SmNode *stk,
+                                 int stackLeft, Node *__restrict__ out, uint32_t *__restrict__ primIDs,
+                                 uint32_t *__restrict__ used, uint32_t *err)
+{
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t base = root.b, cnt = root.e - root.b;
+  float4 c = lane < (int)cnt ? src[base + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t pos = base + lane;
+  SmNode cur = root;
+  int sp = 0;
+  while (true) {
+    const uint32_t count = cur.e - cur.b;
+    if ((int64_t)count <= thr) {
+      if (lane == 0) leaf_node(out, cur.slot, cur.b, count);
+      if (sp == 0) break;
+      __syncwarp();
+      cur = stk[--sp];
+      __syncwarp();
+      continue;
+    }
+    const SmSplit spl = choose_split(cur);
+    const bool in = pos >= cur.b && pos < cur.e;
+    const uint32_t side = in ? side_of(c, pos - cur.b, spl) : 0u;
+    const uint32_t balR = __ballot_sync(0xffffffffu, in && side);
+    const uint32_t balL = __ballot_sync(0xffffffffu, in && !side);
+    const uint32_t m = cur.e - __popc(balR);
+    SideBounds sb;
+    sb.init();
+    if (in) sb.add(c, side);
+    sb.warp_reduce();
+    const uint32_t dest = !in ? (uint32_t)lane
+                              : (side ? (m - base) + __popc(balR & lt) : (cur.b - base) + __popc(balL & lt));
+    xbuf[dest] = c;
+    __syncwarp();
+    c = xbuf[lane];
+    __syncwarp();
+    if (lane == 0) internal_node(out, used, cur.slot, m);
+    SmNode c0, c1;
+    child_pair(cur, m, sb, c0, c1);
+    const bool leftSmaller = (m - cur.b) <= (cur.e - m);
+    if (sp >= stackLeft) {  // unreachable: the stacked child is always the larger one
+      if (lane == 0) atomicOr(err, DEV_ERR_RANGE);
+      break;
+    }
+    if (lane == 0) stk[sp] = leftSmaller ? c1 : c0;
+    sp++;
+    cur = leftSmaller ? c0 : c1;
+  }
+  if (lane < (int)cnt) primIDs[base + lane] = __float_as_uint(c.w);
+  __syncwarp();
+}
+
+// one warp per task; grid = div_up(numTasks * 32, SMW_BLOCK)
+__global__ void __launch_bounds__(SMW_BLOCK) k_sm_warp(const SmNode *__restrict__ tasks, uint32_t numTasks, int thr,
+                                                       float4 *buf0, float4 *buf1, Node *__restrict__ out,
+                                                       uint32_t *__restrict__ primIDs, uint32_t *__restrict__ used,
+                                                       uint32_t *err)
+{
+  __shared__ SmNode sStack[SMW_WARPS][SMW_STACK];
+  __shared__ float4 sX[SMW_WARPS][32];
+  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= numTasks) return;  // whole warps leave together
+  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  SmNode *stk = sStack[wb];
+  int sp = 0;
+  SmNode cur = tasks[w];
+  while (true) {
+    const uint32_t count = cur.e - cur.b;
+    const float4 *src = cur.parity ? buf1 : buf0;
+    float4 *dst = cur.parity ? buf0 : buf1;
+    if ((int64_t)count <= thr || count <= 32) {
+      if ((int64_t)count <= thr) {  // leaf: its prims are final
+        for (uint32_t i = cur.b + lane; i < cur.e; i += 32) primIDs[i] = __float_as_uint(src[i].w);
+        if (lane == 0) leaf_node(out, cur.slot, cur.b, count);
+      } else {
+        sm_small_subtree(cur, src, thr, sX[wb], stk + sp, SMW_STACK - sp, out, primIDs, used, err);
+      }
+      if (sp == 0) return;
+      __syncwarp();
+      cur = stk[--sp];
+      __syncwarp();
+      continue;
+    }
+    const SmSplit spl = choose_split(cur);
+    // pass 1: right-side count
+    uint32_t nR = 0;
+#pragma unroll 4
+    for (uint32_t i = cur.b + lane; i < cur.e; i += 32) nR += side_of(src[i], i - cur.b, spl);
+    nR = __reduce_add_sync(0xffffffffu, nR);
+    const uint32_t m = cur.e - nR;
+    // pass 2: stable scatter + children's bounds, 128 prims per round
+    uint32_t lB = 0, rB = 0;
+    SideBounds sb;
+    sb.init();
+    for (uint32_t base = cur.b; base < cur.e; base += 128) {
+      float4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint32_t i = base + 32u * u + lane;
+        v[u] = i < cur.e ? src[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint32_t i = base + 32u * u + lane;
+        const bool valid = i < cur.e;
+        const uint32_t s = valid ? side_of(v[u], i - cur.b, spl) : 0u;
+        const uint32_t balR = __ballot_sync(0xffffffffu, valid && s);
+        const uint32_t balL = __ballot_sync(0xffffffffu, valid && !s);
+        if (valid) {
+          dst[s ? m + rB + __popc(balR & lt) : cur.b + lB + __popc(balL & lt)] = v[u];
+          sb.add(v[u], s);
+        }
+        rB += __popc(balR);
+        lB += __popc(balL);
+      }
+    }
+    sb.warp_reduce();
+    if (lane == 0) internal_node(out, used, cur.slot, m);
+    SmNode c0, c1;
+    child_pair(cur, m, sb, c0, c1);
+    const bool leftSmaller = (m - cur.b) <= (cur.e - m);
+    if (sp >= SMW_STACK) {  // unreachable: the stacked child is always the larger one
+      if (lane == 0) atomicOr(err, DEV_ERR_RANGE);
+      return;
+    }
+    if (lane == 0) stk[sp] = leftSmaller ? c1 : c0;
+    sp++;
+    cur = leftSmaller ? c0 : c1;
+    __syncwarp();  // this warp's scatter is visible to its own next pass
+  }
+}
+
+// ------------------------------------------------------------------
+// slot compaction: split m's children move from 2m, 2m+1 to 2+2*rank[m]
+// ------------------------------------------------------------------
+__device__ __forceinline__ Node sm_remap(const Node &c, const uint32_t *__restrict__ rank)
+{
+  const uint64_t a = node_admin(c);
+  if (admin_count(a)) return c;
+  const uint32_t cm = (uint32_t)(admin_offset(a) >> 1);
+  return make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, make_admin(2ull + 2ull * rank[cm], 0));
+}
+
+__global__ void k_sm_compact(const Node *__restrict__ full, const uint32_t *__restrict__ used,
+                             const uint32_t *__restrict__ rank, uint32_t nv, Node *__restrict__ out)
+{
+  const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m == 0) {
+    out[0] = sm_remap(full[0], rank);
+    out[1] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0);
+    return;
+  }
+  if (m >= nv || !used[m]) return;
+  const uint64_t pair = 2ull + 2ull * rank[m];
+  out[pair] = sm_remap(full[2ull * m], rank);
+  out[pair + 1] = sm_remap(full[2ull * m + 1], rank);
 }
 
 } // namespace
@@ -217,101 +490,142 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   if (n == 0) return BQ_OK;  // gpu_builder.h:39
 
   TempSet tmp(al);
-  uint32_t *valid = nullptr, *vpos = nullptr, *counts = nullptr, *pnA = nullptr, *pnB = nullptr, *right = nullptr;
-  float4 *pcA = nullptr, *pcB = nullptr;
-  SmNode *listA = nullptr, *listB = nullptr;
-  uint32_t *isSplit = nullptr, *splitCount = nullptr, *rank = nullptr, *nextBegin = nullptr, *tb = nullptr;
-  int *dim = nullptr;
-  float *pos = nullptr;
-  Node *tnodes = nullptr;
+  uint32_t *valid = nullptr, *vpos = nullptr, *ctl = nullptr, *used = nullptr;
+  float4 *buf0 = nullptr, *buf1 = nullptr;
   BQ_TRY(tmp.get(&valid, n));
   BQ_TRY(tmp.get(&vpos, n));
-  BQ_TRY(tmp.get(&counts, 4));  // [0] valid count, [1] #splits, [2] next active count
-  BQ_TRY(tmp.get(&pcA, n));
-  BQ_TRY(tmp.get(&pcB, n));
-  BQ_TRY(tmp.get(&pnA, n));
-  BQ_TRY(tmp.get(&pnB, n));
-  BQ_TRY(tmp.get(&right, n + 1ull));
-  BQ_TRY(tmp.get(&listA, n));
-  BQ_TRY(tmp.get(&listB, n));
-  BQ_TRY(tmp.get(&isSplit, n));
-  BQ_TRY(tmp.get(&splitCount, n));
-  BQ_TRY(tmp.get(&rank, n));
-  BQ_TRY(tmp.get(&nextBegin, n));
-  BQ_TRY(tmp.get(&tb, n));
-  BQ_TRY(tmp.get(&dim, n));
-  BQ_TRY(tmp.get(&pos, n));
-  BQ_TRY(tmp.get(&tnodes, 2ull * n + 2));
+  BQ_TRY(tmp.get(&ctl, 8));  // [0] valid count [1] device error bits [2..7] root centroid bounds
+  BQ_TRY(tmp.get(&buf0, n));
+  BQ_TRY(tmp.get(&buf1, n));
+  BQ_TRY(tmp.get(&used, n));
   uint32_t *primIDs = nullptr;
   BQ_TRY(al.get(&primIDs, n));
   auto fail = [&](int code) {
     al.free_bytes(primIDs);
     return code;
   };
-  cudaError_t ce;
   int s;
-  k_sm_valid<<<div_up(n, 256), 256, 0, al.s>>>(boxes, n, valid);
-  if ((s = exclusive_scan_u32(valid, vpos, n, nullptr, counts, al)) != BQ_OK) return fail(s);
-  k_sm_init<<<div_up(n, 256), 256, 0, al.s>>>(boxes, n, vpos, counts, pcA, pnA, primIDs, listA);
-  uint32_t hc[4] = {0, 0, 0, 0};
-  if ((ce = cudaMemcpyAsync(hc, counts, 4, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess) return fail(cuda_error(ce, "copy"));
-  if ((ce = cudaStreamSynchronize(al.s)) != cudaSuccess) return fail(cuda_error(ce, "sync"));
-  const uint32_t nv = hc[0];
+  cudaError_t ce;
+  const int32_t ctlInit[8] = {0, 0, INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+  if ((ce = cudaMemcpyAsync(ctl, ctlInit, 32, cudaMemcpyHostToDevice, al.s)) != cudaSuccess ||
+      (ce = cudaMemsetAsync(used, 0, sizeof(uint32_t) * n, al.s)) != cudaSuccess)
+    return fail(cuda_error(ce, "spatial median set-up"));
+  {
+    ProfScope ps("sm.setup", al.s, 5);
+    k_sm_valid<<<div_up(n, 256), 256, 0, al.s>>>(boxes, n, valid);
+    if ((s = exclusive_scan_u32(valid, vpos, n, nullptr, ctl, al)) != BQ_OK) return fail(s);
+    k_sm_init<<<std::min(div_up(n, 256), num_sms() * 8), 256, 0, al.s>>>(boxes, n, vpos, ctl, buf0, primIDs,
+                                                                       (int32_t *)(ctl + 2));
+  }
+  int32_t hctl[8];
+  if ((ce = cudaMemcpyAsync(hctl, ctl, 32, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
+      (ce = cudaStreamSynchronize(al.s)) != cudaSuccess)
+    return fail(cuda_error(ce, "spatial median set-up"));
+  const uint32_t nv = (uint32_t)hctl[0];
   if (nv == 0) {  // nothing to build over
     al.free_bytes(primIDs);
     return BQ_OK;
   }
-  uint32_t A = nv, K = 1, nodeBase = 2;
-  k_sm_bounds<<<div_up(A, SB_TILE), 256, 0, al.s>>>(pcA, pnA, A, listA);
-  float4 *pcCur = pcA, *pcNext = pcB;
-  uint32_t *pnCur = pnA, *pnNext = pnB;
-  SmNode *listCur = listA, *listNext = listB;
-  while (K > 0) {
+  Node *full = nullptr;
+  if ((s = tmp.get(&full, 2ull * nv)) != BQ_OK) return fail(s);
+
+  // ---- global levels ----
+  std::vector<SmNode> level(1), tasks;
+  level[0].b = 0; level[0].e = nv; level[0].slot = 0; level[0].parity = 0;
+  for (int d = 0; d < 3; d++) { level[0].lo[d] = hctl[2 + d]; level[0].hi[d] = hctl[5 + d]; }
+  TempSet lvlTmp(al);
+  uint8_t *dLevel = nullptr;  // [K SmNode][K+1 first tile][T SmTile], 16-byte aligned parts
+  SmNode *dNext = nullptr;
+  uint32_t *dRight = nullptr;
+  size_t capBytes = 0, capNext = 0, capRight = 0;
+  std::vector<uint8_t> hLevel;
+  while (true) {
+    std::vector<SmNode> big;
+    for (const SmNode &nd : level) {
+      const uint32_t c = nd.e - nd.b;
+      if (c > SM_WARP_MAX && (int64_t)c > thr) big.push_back(nd);
+      else tasks.push_back(nd);
+    }
+    if (big.empty()) break;
+    const uint32_t K = (uint32_t)big.size();
+    std::vector<uint32_t> first(K + 1);
+    std::vector<SmTile> tiles;
+    for (uint32_t k = 0; k < K; k++) {
+      first[k] = (uint32_t)tiles.size();
+      for (uint64_t b0 = big[k].b; b0 < big[k].e; b0 += SM_TILE)
+        tiles.push_back(SmTile{k, (uint32_t)b0, (uint32_t)std::min<uint64_t>(big[k].e, b0 + SM_TILE)});
+    }
+    first[K] = (uint32_t)tiles.size();
+    const uint32_t T = (uint32_t)tiles.size();
+    const size_t offFirst = ((sizeof(SmNode) * K + 15) / 16) * 16;
+    const size_t offTiles = offFirst + ((sizeof(uint32_t) * (K + 1) + 15) / 16) * 16;
+    const size_t bytes = offTiles + sizeof(SmTile) * T;
+    if (bytes > capBytes) {
+      capBytes = std::max(bytes, 2 * capBytes);
+      if ((s = lvlTmp.get(&dLevel, capBytes)) != BQ_OK) return fail(s);
+    }
+    if (2ull * K > capNext) {
+      capNext = std::max<size_t>(2ull * K, 2 * capNext);
+      if ((s = lvlTmp.get(&dNext, capNext)) != BQ_OK) return fail(s);
+    }
+    if (T + 1ull > capRight) {
+      capRight = std::max<size_t>(T + 1ull, 2 * capRight);
+      if ((s = lvlTmp.get(&dRight, capRight)) != BQ_OK) return fail(s);
+    }
+    hLevel.resize(bytes);
+    std::memcpy(hLevel.data(), big.data(), sizeof(SmNode) * K);
+    std::memcpy(hLevel.data() + offFirst, first.data(), sizeof(uint32_t) * (K + 1));
+    std::memcpy(hLevel.data() + offTiles, tiles.data(), sizeof(SmTile) * T);
+    const SmNode *dNodes = reinterpret_cast<const SmNode *>(dLevel);
+    const uint32_t *dFirst = reinterpret_cast<const uint32_t *>(dLevel + offFirst);
+    const SmTile *dTiles = reinterpret_cast<const SmTile *>(dLevel + offTiles);
     {
-      ProfScope ps("sm.nodes", al.s, 7);
-      k_sm_select<<<div_up(K, 128), 128, 0, al.s>>>(listCur, K, thr, pcCur, isSplit, splitCount, dim, pos, tb, tnodes,
-                                                    primIDs);
-      if ((s = exclusive_scan_u32(isSplit, rank, K, nullptr, counts + 1, al)) != BQ_OK) return fail(s);
-      if ((s = exclusive_scan_u32(splitCount, nextBegin, K, nullptr, counts + 2, al)) != BQ_OK) return fail(s);
+      ProfScope ps("sm.level", al.s, 6);
+      if ((ce = cudaMemcpyAsync(dLevel, hLevel.data(), bytes, cudaMemcpyHostToDevice, al.s)) != cudaSuccess)
+        return fail(cuda_error(ce, "upload level"));
+      k_sm_count<<<T, SM_BLOCK, 0, al.s>>>(dNodes, dTiles, T, buf0, buf1, dRight);
+      if ((s = exclusive_scan_u32(dRight, dRight, T + 1, nullptr, nullptr, al)) != BQ_OK) return fail(s);
+      k_sm_children<<<div_up(K, 128), 128, 0, al.s>>>(dNodes, K, dFirst, dRight, full, used, dNext);
+      k_sm_scatter<<<T, SM_BLOCK, 0, al.s>>>(dNodes, dTiles, dFirst, dRight, buf0, buf1, dNext);
+      if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "spatial median level"));
     }
-    {
-      ProfScope ps("sm.partition", al.s, 6);
-      k_sm_flags<<<div_up(A, 256), 256, 0, al.s>>>(pcCur, pnCur, A, listCur, isSplit, dim, pos, tb, right);
-      if ((s = exclusive_scan_u32(right, right, A + 1, nullptr, nullptr, al)) != BQ_OK) return fail(s);
-      k_sm_children<<<div_up(K, 128), 128, 0, al.s>>>(listCur, K, isSplit, rank, nextBegin, right, nodeBase,
-                                                      listNext, tnodes);
-      k_sm_scatter<<<div_up(A, 256), 256, 0, al.s>>>(pcCur, pnCur, A, listCur, isSplit, dim, pos, tb, rank,
-                                                     nextBegin, right, pcNext, pnNext);
-    }
-    {
-      ProfScope ps("sm.sync", al.s, 0);
-      if ((ce = cudaMemcpyAsync(hc + 1, counts + 1, 8, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess)
-        return fail(cuda_error(ce, "copy"));
-      if ((ce = cudaStreamSynchronize(al.s)) != cudaSuccess) return fail(cuda_error(ce, "sync"));
-    }
-    const uint32_t S = hc[1], An = hc[2];
-    if (S > 0) {
-      ProfScope ps("sm.bounds", al.s);
-      k_sm_bounds<<<div_up(An, SB_TILE), 256, 0, al.s>>>(pcNext, pnNext, An, listNext);
-    }
-    if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "spatial median level"));
-    nodeBase += 2 * S;
-    K = 2 * S;
-    A = An;
-    std::swap(pcCur, pcNext);
-    std::swap(pnCur, pnNext);
-    std::swap(listCur, listNext);
+    level.resize(2ull * K);
+    if ((ce = cudaMemcpyAsync(level.data(), dNext, sizeof(SmNode) * 2 * K, cudaMemcpyDeviceToHost, al.s)) !=
+            cudaSuccess ||
+        (ce = cudaStreamSynchronize(al.s)) != cudaSuccess)
+      return fail(cuda_error(ce, "download level"));
   }
-  const uint32_t numNodes = nodeBase;
+  // ---- warp phase ----
+  {
+    SmNode *dTasks = nullptr;
+    if ((s = tmp.get(&dTasks, tasks.size())) != BQ_OK) return fail(s);
+    if ((ce = cudaMemcpyAsync(dTasks, tasks.data(), sizeof(SmNode) * tasks.size(), cudaMemcpyHostToDevice, al.s)) !=
+        cudaSuccess)
+      return fail(cuda_error(ce, "upload tasks"));
+    ProfScope ps("sm.warps", al.s);
+    const uint32_t nt = (uint32_t)tasks.size();
+    k_sm_warp<<<div_up((long long)nt * 32, SMW_BLOCK), SMW_BLOCK, 0, al.s>>>(dTasks, nt, thr, buf0, buf1, full,
+                                                                              primIDs, used, ctl + 1);
+    if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_sm_warp"));
+  }
+  // ---- slot compaction ----
+  uint32_t *rank = nullptr;
+  if ((s = tmp.get(&rank, nv)) != BQ_OK) return fail(s);
+  {
+    ProfScope ps("sm.rank", al.s, 3);
+    if ((s = exclusive_scan_u32(used, rank, nv, nullptr, ctl + 2, al)) != BQ_OK) return fail(s);
+  }
+  uint32_t hres[2];
+  if ((ce = cudaMemcpyAsync(hres, ctl + 1, 8, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
+      (ce = cudaStreamSynchronize(al.s)) != cudaSuccess)
+    return fail(cuda_error(ce, "spatial median"));
+  if (hres[0]) return fail(set_error(BQ_ERR_CUDA, "spatial-median warp phase failed a range check"));
+  const uint32_t numNodes = 2 + 2 * hres[1];
   Node *nodes = nullptr;
   if ((s = al.get(&nodes, numNodes)) != BQ_OK) return fail(s);
-  if ((ce = cudaMemcpyAsync(nodes, tnodes, sizeof(Node) * numNodes, cudaMemcpyDeviceToDevice, al.s)) != cudaSuccess) {
-    al.free_bytes(nodes);
-    return fail(cuda_error(ce, "copy nodes"));
-  }
-  if ((ce = cudaMemsetAsync(nodes + 1, 0, sizeof(Node), al.s)) != cudaSuccess) {
-    al.free_bytes(nodes);
-    return fail(cuda_error(ce, "memset"));
+  {
+    ProfScope ps("sm.compact", al.s);
+    k_sm_compact<<<div_up(nv, 256), 256, 0, al.s>>>(full, used, rank, nv, nodes);
   }
   bvh->nodes = reinterpret_cast<bq_node3f *>(nodes);
   bvh->numNodes = numNodes;

@@ -114,6 +114,19 @@ typedef struct bq_query_config {
 int bq_build_morton63_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
                          const bq_allocator *alloc, bq_stream_t stream);
 
+/* Rebinning Morton builder with 30-bit keys.  Replaces
+   cuBQL::cuda::rebinRadixBuilder<float,3> (cuBQL/builder/cuda.h:143-154,
+   implementation cuBQL/builder/cuda/rebinMortonBuilder.h:1161-1488).
+   Runs of more than 32 prims with equal keys get new keys over their own
+   centroid bounds (stable sort); smaller ones are rebinned with the
+   reference's exchange sort.  The tree and prim order equal the
+   reference's after BFS renumbering for inputs without empty boxes.
+   Where the reference would rebin forever (a run whose centroid bounds
+   are narrower than 1e-20 but not a point) the rebin depth stops at 40
+   and the run is split by position. */
+int bq_build_rebin_morton30_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
+                               const bq_allocator *alloc, bq_stream_t stream);
+
 /* Spatial-median builder.  Replaces cuBQL::gpuBuilder<float,3>
    (cuBQL/builder/cuda.h:91-99, cuBQL/builder/cuda/gpu_builder.h:31-67,
    cuBQL/builder/cuda/sm_builder.h:469-614). */

@@ -103,6 +103,18 @@ inline void radixBuilder(BVH &bvh, const Box *boxes, uint32_t numPrims, Cfg cfg,
   from_c(bvh, c);
 }
 
+/*! cuBQL::cuda::rebinRadixBuilder (cuBQL/builder/cuda.h:143-154) */
+template <class BVH, class Box, class Cfg, class MemRes>
+inline void rebinRadixBuilder(BVH &bvh, const Box *boxes, uint32_t numPrims, Cfg cfg, cudaStream_t s, MemRes &mem)
+{
+  static_assert(sizeof(Box) == 24, "box_t<float,3> layout");
+  bq_bvh3f c{};
+  bq_build_config cc = to_c_cfg(cfg);
+  bq_allocator a = ResourceAdapter<MemRes>::make(mem);
+  check(bq_build_rebin_morton30_f3(&c, (const bq_box3f *)boxes, numPrims, &cc, &a, s), "rebinRadixBuilder");
+  from_c(bvh, c);
+}
+
 /*! cuBQL::cuda::free (cuBQL/builder/cuda.h:158-161) */
 template <class BVH, class MemRes>
 inline void free(BVH &bvh, cudaStream_t s, MemRes &mem)

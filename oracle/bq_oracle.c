@@ -1095,6 +1095,7 @@ int orc_rebin_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int ma
   /* broad phase with rebinning restarts (:1283-1393); the first pass
      sees the root only, a restart sees every node allocated so far */
   uint64_t done = 0, upTo = 1;
+  int restart = 0;
   for (;;) {
     while (done < upTo) {
       uint64_t end = upTo;
@@ -1115,8 +1116,13 @@ int orc_rebin_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int ma
       done = end;
       upTo = alloc;
     }
-    /* rebin every still-open node larger than the broad-phase limit */
+    /* rebin every still-open node larger than the broad-phase limit; the
+       reference would restart forever on a run whose centroid bounds are
+       narrower than 1e-20 but not a point: from depth 40 on, runs are
+       keyed by position (the library's documented cap) */
     int jobs = 0;
+    restart++;
+    const int atCap = restart >= 40;
     for (uint64_t id = 0; id < alloc; id++) {
       if (id == 1 || !t[id].open) continue;
       uint32_t b = t[id].a, e = t[id].b;
@@ -1130,7 +1136,7 @@ int orc_rebin_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int ma
       for (uint32_t i = b; i < e; i++) {           /* rebinCreateNewKeysAndPrimIDs (:1022-1063) */
         float c[3];
         box_center(&boxes[primIDs[i]], c);
-        nk[i - b] = degenerate ? (i - b) : morton30(c, lo, hi);
+        nk[i - b] = (degenerate || atCap) ? (i - b) : morton30(c, lo, hi);
         nid[i - b] = primIDs[i];
       }
       stable_sort_pairs(nk, nid, e - b, 0, 32);    /* sort by (range, morton), stable */

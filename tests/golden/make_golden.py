@@ -3,6 +3,8 @@
   python tests/golden/make_golden.py cpu   # here: the reference's host code
   python tests/golden/make_golden.py gpu   # on a B200: the reference's GPU
                                            # builders and query kernels
+  python tests/golden/make_golden.py gpu_rebin   # on a B200: the reference's
+                                           # rebinRadixBuilder trees
 
 Both read oracle/_ref/ (the reference compiled from its own sources by
 oracle/build_ref.sh).  Inputs are the seeded generators of
@@ -98,5 +100,32 @@ def gpu():
     np.savez_compressed(dest, **out)
 
 
+def rebin_inputs():
+    """Uniform, GMM, and a tight cluster inside a wide cloud (many equal
+    30-bit Morton keys: exercises the rebin restarts)."""
+    u = W.uniform_points(3000)
+    g = W.gmm_points(3000)
+    wide = W.uniform_points(1000, 21, -1000.0, 1000.0)
+    tight = W.uniform_points(3000, 22, 0.0, 1e-3)
+    return (("u", u), ("g", g), ("c", np.concatenate([wide, tight]).astype(np.float32)))
+
+
+def gpu_rebin():
+    from oracle.oracle import RefGPU
+    r = RefGPU()
+    o = Oracle()
+    out = {}
+    for name, pts in rebin_inputs():
+        b = W.point_boxes(pts)
+        out[f"{name}_points"] = pts
+        for thr in (0, 8):
+            n, pr = r.build(RefGPU.REBIN, b, thr)
+            cn, cp = o.canonicalize(n, pr)
+            out[f"{name}_rebin{thr}_nodes"] = cn.view(np.uint8)
+            out[f"{name}_rebin{thr}_prims"] = cp
+    dest = sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu_rebin.npz")
+    np.savez_compressed(dest, **out)
+
+
 if __name__ == "__main__":
-    {"cpu": cpu, "gpu": gpu}[sys.argv[1]]()
+    {"cpu": cpu, "gpu": gpu, "gpu_rebin": gpu_rebin}[sys.argv[1]]()

@@ -101,7 +101,7 @@ def test_empty_and_all_invalid(bq):
     assert bvh.numNodes == 0
 
 
-@pytest.mark.parametrize("thr", [0, 1, 8])
+@pytest.mark.parametrize("thr", [0, 1, 8, 40, 5000])
 @pytest.mark.parametrize("dist", ["uniform", "gmm", "dupes", "invalid", "line"])
 def test_spatial_median_invariants_and_oracle(bq, oracle, thr, dist):
     b = _boxes(dist, 30000)
@@ -114,6 +114,20 @@ def test_spatial_median_invariants_and_oracle(bq, oracle, thr, dist):
     on, op = oracle.sm_build(b, thr)
     ok, msg = same_tree(oracle, gn, gp[: valid.sum()], on, op[: valid.sum()])
     assert ok, msg
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 31, 32, 33, 64, 4095, 4096, 4097, 8193])
+def test_spatial_median_small_and_boundary_sizes(bq, oracle, n):
+    """Sizes around the one-warp register subtree (32) and the one-warp
+    subtree limit (4096)."""
+    b = _boxes("gmm", n)
+    for thr in (0, 3):
+        bvh = bq.gpuBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=thr))
+        gn, gp = bvh.to_host()
+        check_tree(gn, gp, b, max_leaf=max(thr, 1))
+        on, op = oracle.sm_build(b, thr)
+        ok, msg = same_tree(oracle, gn, gp, on, op)
+        assert ok, f"thr {thr}: {msg}"
 
 
 def test_spatial_median_matches_reference_gpu_builder(bq, oracle, ref_gpu):

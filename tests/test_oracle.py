@@ -209,3 +209,23 @@ def test_adjoint_formula_matches_finite_differences(oracle):
             e[i] = h
             fa[i] = (oracle.tri_cp_f64(a + e, b, c, p)[0] - oracle.tri_cp_f64(a - e, b, c, p)[0]) / (2 * h)
         assert np.allclose(-w[0] * gq, fa, rtol=1e-5, atol=1e-6)
+
+
+def test_rebin_restatement_matches_reference_gpu_trees(oracle):
+    """orc_rebin_build against the reference's rebinRadixBuilder run on a
+    B200 (fixtures: uniform, GMM and a tight cluster inside a wide cloud,
+    which forces nested rebins); trees after BFS renumbering, bit for bit,
+    leaf prim order included."""
+    g = _load("ref_gpu_rebin.npz")
+    for name in ("u", "g", "c"):
+        b = boxes_np(g[f"{name}_points"])
+        for thr in (0, 8):
+            n, pr = oracle.rebin_build(b, thr)
+            cn, cp = oracle.canonicalize(n, pr)
+            ref = g[f"{name}_rebin{thr}_nodes"].view(NODE).copy()
+            cn = cn.copy()
+            cn[1] = np.zeros(1, dtype=NODE)
+            ref[1] = np.zeros(1, dtype=NODE)
+            assert np.array_equal(cp, g[f"{name}_rebin{thr}_prims"]), (name, thr)
+            assert cn.tobytes() == ref.tobytes(), (name, thr)
+            check_tree(n, pr, b, max_leaf=max(thr, 32))
