@@ -276,6 +276,15 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
         bq.gpuBuilder(boxes_t, bq.BuildConfig(makeLeafThreshold=1)).free()
     ms = ev_time(smb1)
     comp["spatial_median_build_leaf1"] = {"ms": ms, "Mprims_s": n / ms / 1e3, "leaf": 1}
+
+    # rebinning Morton-30 build, leaf 1
+    def rbb():
+        bq.cuda.rebinRadixBuilder(boxes_t).free()
+    ms = ev_time(rbb)
+    comp["rebin_morton30_build"] = {"ms": ms, "Mprims_s": n / ms / 1e3, "leaf": 1}
+    with bq.profile() as prof:
+        rbb()
+    comp["rebin_morton30_build"]["phases_ms"] = {k: round(v[1], 4) for k, v in prof.table.items()}
     # queries on the Morton tree (leaf 1)
     bvh = bq.cuda.radixBuilder(boxes_t)
     qs = torch.from_numpy(W.uniform_points(n, W.SEED_QUERIES)).cuda()
@@ -325,6 +334,96 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
     tb.free()
 
 
+def _ev_time(torch, fn, reps=3, warm=1):
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def batched_components(bq, W, torch, comp):
+    """The two batched workloads: 512 point clouds (about 19M points, 25.6M
+    kNN(16) queries; one segmented build + one query launch replayed from a
+    CUDA graph, against a per-cloud loop of single builds and queries), and
+    a 100-step fitting loop over 128 triangle meshes (6.4M queries per step:
+    triangle boxes, batched refit, batched closest triangle, adjoint,
+    vertex update)."""
+    import numpy as np
+    pts, off, qs, qoff = W.cloud_batch()
+    n, nq = len(pts), len(qs)
+    b = torch.from_numpy(W.point_boxes(pts)).cuda()
+    tp, tq = torch.from_numpy(pts).cuda(), torch.from_numpy(qs).cuda()
+    toff, tqoff = torch.from_numpy(off).cuda().int(), torch.from_numpy(qoff).cuda().int()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):  # first use of the stream-ordered pool, outside the capture
+        bq.batched_knn(bq.Batch(b, toff, stream_alloc_null=True), tp, toff, tq, tqoff, 16, stream_alloc_null=True)
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        gbatch = bq.Batch(b, toff, stream_alloc_null=True)
+        gout = bq.batched_knn(gbatch, tp, toff, tq, tqoff, 16, stream_alloc_null=True)
+    ms_graph = _ev_time(torch, graph.replay)
+    ms_build = _ev_time(torch, lambda: bq.Batch(b, toff))
+    bat = bq.Batch(b, toff)
+    ms_query = _ev_time(torch, lambda: bq.batched_knn(bat, tp, toff, tq, tqoff, 16))
+
+    def loop():
+        for c in range(len(off) - 1):
+            sl, ql = slice(int(off[c]), int(off[c + 1])), slice(int(qoff[c]), int(qoff[c + 1]))
+            t = bq.cuda.radixBuilder(b[sl])
+            bq.points.findKNN(t, tp[sl], tq[ql], 16)
+            t.free()
+    ms_loop = _ev_time(torch, loop, reps=1, warm=1)
+    same = True
+    for c in (0, len(off) // 2, len(off) - 2):  # spot check: batched answers == per-cloud answers
+        sl, ql = slice(int(off[c]), int(off[c + 1])), slice(int(qoff[c]), int(qoff[c + 1]))
+        t = bq.cuda.radixBuilder(b[sl])
+        si, sd, _ = bq.points.findKNN(t, tp[sl], tq[ql], 16)
+        same &= bool(torch.equal(si, gout[0][ql]) and torch.equal(sd, gout[1][ql]))
+        t.free()
+    del graph
+    comp["batched_knn_512_clouds"] = {
+        "clouds": len(off) - 1, "points": n, "queries": nq, "k": 16,
+        "graph_ms": ms_graph, "build_ms": ms_build, "query_ms": ms_query,
+        "Mqueries_s": nq / ms_graph / 1e3, "build_Mprims_s": n / ms_build / 1e3,
+        "per_cloud_loop_ms": ms_loop, "speedup_vs_per_cloud_loop": ms_loop / ms_graph,
+        "matches_per_cloud_answers": same}
+    del b, tp, tq, bat, gbatch, gout
+
+    verts, tris, toffm, qsm, qoffm = W.mesh_batch()
+    tv, tt = torch.from_numpy(verts).cuda(), torch.from_numpy(tris).cuda()
+    tqm = torch.from_numpy(qsm).cuda()
+    toff_t, qoff_t = torch.from_numpy(toffm).cuda().int(), torch.from_numpy(qoffm).cuda().int()
+    batch = bq.Batch(bq.triangles.boxes(tt, tv), toff_t)
+    g = torch.full((len(qsm),), 1.0 / len(qsm), device="cuda")
+    state = {"v": tv}
+
+    def step():
+        v = state["v"]
+        boxes = bq.triangles.boxes(tt, v)
+        bq.batched_refit(batch, boxes)
+        ids, d, _ = bq.batched_tri_closest(batch, tt, v, tqm, qoff_t)
+        _, gv = bq.triangles.distanceBackward(tt, v, tqm, ids, g)
+        state["v"] = v - 0.5 * gv
+        return ids, d
+    ms_step = _ev_time(torch, step, reps=100, warm=3)
+    ids, d = step()
+    fresh = bq.Batch(bq.triangles.boxes(tt, state["v"]), toff_t)
+    fi, fd, _ = bq.batched_tri_closest(fresh, tt, state["v"], tqm, qoff_t)
+    ids2, d2, _ = bq.batched_tri_closest(batch, tt, state["v"], tqm, qoff_t)
+    comp["fit_loop_128_meshes"] = {
+        "meshes": len(toffm) - 1, "triangles": int(len(tris)), "queries_per_step": int(len(qsm)), "steps": 100,
+        "ms_per_step": ms_step, "fwd_bwd_queries_s": len(qsm) / ms_step * 1e3,
+        "refit_forward_equals_rebuild": bool(torch.equal(ids2, fi) and torch.equal(d2, fd))}
+
+
 def reference_gpu(comp, pts_np, W):
     from oracle.oracle import RefGPU, have_ref_gpu
     if not have_ref_gpu():
@@ -336,6 +435,7 @@ def reference_gpu(comp, pts_np, W):
     out["radixBuilder_ms"] = r.time_build(RefGPU.RADIX, pts_np, 0, reps=3)
     out["gpuBuilder_leaf8_ms"] = r.time_build(RefGPU.SPATIAL_MEDIAN, pts_np, 8, reps=3)
     out["gpuBuilder_leaf1_ms"] = r.time_build(RefGPU.SPATIAL_MEDIAN, pts_np, 0, reps=3)
+    out["rebinRadixBuilder_ms"] = r.time_build(RefGPU.REBIN, pts_np, 0, reps=3)
     qs = W.uniform_points(n, W.SEED_QUERIES)
     out["findClosest_ms"] = r.time_query(RefGPU.RADIX, pts_np, qs, 0, reps=2)
     out["findKNN16_ms"] = r.time_query(RefGPU.RADIX, pts_np, qs, 16, reps=2)
@@ -411,27 +511,13 @@ def run_ours(args):
                                 "frac": build_bytes / ms / 1e6 / peak}}
 
     # end to end through the public API: pinned host boxes -> tree on host
-    host_boxes = torch.from_numpy(boxes_np).pin_memory()
-    dev_boxes = torch.empty_like(boxes_t)
-    host_nodes = torch.empty((2 * n, 8), dtype=torch.float32).pin_memory()
-    host_prims = torch.empty(n, dtype=torch.int32).pin_memory()
-
-    def e2e_step():
-        dev_boxes.copy_(host_boxes, non_blocking=True)
-        b = bq.cuda.radixBuilder(dev_boxes)
-        host_nodes[: b.numNodes].copy_(b.nodes_tensor(), non_blocking=True)
-        host_prims[: b.numPrims].copy_(b.primids_tensor(), non_blocking=True)
-        b.free()
-    e2e_ms = max_over_ranks(time_loop(e2e_step, max(3, args.steps // 2), 2, world), world)
-    e2e = {"value": world * n / e2e_ms / 1e3, "unit": "Mprims/s", "h2d_bytes_per_step": 24 * n,
-           "d2h_bytes_per_step": 32 * 2 * n + 4 * n, "ms_per_step": e2e_ms,
-           "path": "cubql_b200.cuda.radixBuilder (C ABI bq_build_morton63_f3), pinned host buffers"}
-    del host_nodes, host_prims, host_boxes, dev_boxes
+    e2e = e2e_pipelined(bq, torch, boxes_np, n, max(4, args.steps // 2), 2, world)
 
     comp = {}
     cpu_baseline = None
     if rank == 0 and not args.no_components:
         components(bq, W, torch, pts_np, tp, boxes_t, comp)
+        batched_components(bq, W, torch, comp)
         reference_gpu(comp, pts_np, W)
     if rank == 0:
         cpu_baseline = cpu_leg(W, pts_np)
@@ -449,6 +535,58 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def e2e_pipelined(bq, torch, boxes_np, n, steps, warmup, world):
+    """The build through the public API (cubql_b200.cuda.radixBuilder) with
+    host buffers: every step copies its boxes host->device, builds, and
+    copies the whole tree (nodes + primIDs) device->host.  Consecutive steps
+    alternate between two streams, so one step's tree download overlaps the
+    next step's upload and build (separate copy engines per direction).
+    Timed with CUDA events around all steps, on the device."""
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    host_boxes = [torch.from_numpy(boxes_np).pin_memory() for _ in range(2)]
+    dev_boxes = [torch.empty((n, 6), dtype=torch.float32, device="cuda") for _ in range(2)]
+    host_nodes = [torch.empty((2 * n, 8), dtype=torch.float32).pin_memory() for _ in range(2)]
+    host_prims = [torch.empty(n, dtype=torch.int32).pin_memory() for _ in range(2)]
+    trees = [None, None]
+
+    def step(i):
+        k = i % 2
+        with torch.cuda.stream(streams[k]):
+            if trees[k] is not None:
+                trees[k].free()  # stream-ordered: after that tree's download
+            dev_boxes[k].copy_(host_boxes[k], non_blocking=True)
+            b = bq.cuda.radixBuilder(dev_boxes[k])
+            host_nodes[k][: b.numNodes].copy_(b.nodes_tensor(), non_blocking=True)
+            host_prims[k][: b.numPrims].copy_(b.primids_tensor(), non_blocking=True)
+            trees[k] = b
+
+    for i in range(warmup):
+        step(i)
+    torch.cuda.synchronize()
+    barrier(world)
+    cur = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(cur)
+    for s in streams:
+        s.wait_event(e0)
+    for i in range(steps):
+        step(i)
+    for s in streams:
+        cur.wait_stream(s)
+    e1.record(cur)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1) / steps, world)
+    for b in trees:
+        if b is not None:
+            b.free()
+    torch.cuda.synchronize()
+    return {"value": weak_value(n, ms, world), "unit": "Mprims/s", "h2d_bytes_per_step": 24 * n,
+            "d2h_bytes_per_step": 32 * 2 * n + 4 * n, "ms_per_step": ms, "steps": steps,
+            "path": "cubql_b200.cuda.radixBuilder (C ABI bq_build_morton63_f3) from pinned host boxes, whole tree "
+                    "copied back every step; consecutive steps on two streams (upload/build/download overlap)"}
 
 
 def cpu_leg(W, pts_np):

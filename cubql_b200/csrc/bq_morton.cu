@@ -9,8 +9,15 @@
 //                 (radix.h:185-241 fillBuildState/finishBuildState)
 //   k_keygen      stable compaction of valid prims, 63-bit Morton keys
 //                 (radix.h:41-62 Quantizer, 283-421 key generation) and the
-//                 8 digit histograms the sort needs
-//   onesweep sort stable (key, primID) sort, 8 digit passes (bq_sort.cu)
+//                 digit histograms of the top key bits
+//   onesweep sort stable (key, primID) sort on key bits [32, 63) only: 4
+//                 digit passes instead of 8 (bq_sort.cu)
+//   k_fix_runs    runs of equal top bits are then ordered by the low 32
+//                 bits, stably: runs of up to 32 prims by one thread each
+//                 (on uniform data nearly all runs are of 1-3 prims),
+//                 longer runs by one segmented composite-key sort of just
+//                 their prims ((run, low bits) keys).  The result is the
+//                 full stable 63-bit order, as cub's SortPairs gives
 //   k_delta       one byte per adjacent key pair: the level at which the
 //                 reference's top-down split would separate them
 //   agglomerate   bottom-up construction of topology and boxes
@@ -54,6 +61,9 @@ namespace {
 constexpr int MB_BLOCK = 256;
 constexpr int MB_UNROLL = 4;
 constexpr uint32_t SLOT_EMPTY = 0xffffffffu;
+constexpr int MB_SORT_BEGIN = 32;   // the global sort covers key bits [32, 63)
+constexpr int MB_HIST_PASSES = 4;   // its digit passes
+constexpr uint32_t MB_THREAD_RUN = 32;  // longest run of equal top bits one thread orders
 
 struct __align__(16) Partial {
   int32_t lo[3], hi[3];
@@ -200,10 +210,10 @@ __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict_
                                                      uint64_t *__restrict__ keys, uint32_t *__restrict__ ids,
                                                      uint32_t *__restrict__ hist)
 {
-  __shared__ uint32_t sHist[8 * 256];
+  __shared__ uint32_t sHist[MB_HIST_PASSES * 256];
   __shared__ uint32_t sWarpCnt[MB_UNROLL][MB_BLOCK / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < 8 * 256; i += MB_BLOCK) sHist[i] = 0;
+  for (int i = threadIdx.x; i < MB_HIST_PASSES * 256; i += MB_BLOCK) sHist[i] = 0;
   const float bx = st->bias[0], by = st->bias[1], bz = st->bias[2], sc = st->scale;
   uint32_t running = blockOff[blockIdx.x];
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
@@ -254,12 +264,137 @@ __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict_
       keys[pos] = key;
       ids[pos] = (uint32_t)(i0 + (uint64_t)u * MB_BLOCK + threadIdx.x);
 #pragma unroll
-      for (int p = 0; p < 8; p++) atomicAdd(&sHist[p * 256 + ((key >> (8 * p)) & 0xff)], 1u);
+      for (int p = 0; p < MB_HIST_PASSES; p++)
+        atomicAdd(&sHist[p * 256 + ((key >> (MB_SORT_BEGIN + 8 * p)) & 0xff)], 1u);
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < 8 * 256; i += MB_BLOCK)
+  for (int i = threadIdx.x; i < MB_HIST_PASSES * 256; i += MB_BLOCK)
     if (sHist[i]) atomicAdd(&hist[i], sHist[i]);
+}
+
+// ------------------------------------------------------------------
+// runs of equal top key bits: order them by the low 32 bits, stably
+// ------------------------------------------------------------------
+struct RunStats {
+  uint32_t count, elems, maxSize, pad;
+};
+
+// one past the last index j >= i with keys[j] >> 32 == hi (keys[i] >> 32 == hi)
+__device__ __forceinline__ uint32_t hi_run_end(const uint64_t *__restrict__ keys, uint32_t i, uint32_t hi, uint32_t n)
+{
+  uint32_t step = 1, lo = i + 1, up = n;
+  while (lo < up) {
+    const uint32_t probe = lo - 1 + min(step, up - lo + 1);
+    if (probe >= up || (uint32_t)(keys[probe] >> 32) != hi) { up = min(probe, up); break; }
+    lo = probe + 1;
+    step <<= 1;
+  }
+  while (lo < up) {
+    const uint32_t m = lo + ((up - lo) >> 1);
+    if ((uint32_t)(keys[m] >> 32) == hi) lo = m + 1; else up = m;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) k_fix_runs(uint64_t *keys, uint32_t *ids, const uint32_t *nvPtr,
+                                                  RunStats *rs, uint4 *runs, uint32_t maxRuns)
+{
+  const uint32_t nv = *nvPtr;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  // the four neighbouring keys are independent loads (no dependent chain in
+  // the common cases: runs of one and of two)
+  const uint64_t k0 = keys[i];
+  const uint64_t km = i > 0 ? keys[i - 1] : ~k0;
+  const uint64_t k1 = i + 1 < nv ? keys[i + 1] : ~k0;
+  const uint64_t k2 = i + 2 < nv ? keys[i + 2] : ~k0;
+  const uint32_t hi = (uint32_t)(k0 >> 32);
+  if ((uint32_t)(km >> 32) == hi) return;  // not the first of its run
+  if ((uint32_t)(k1 >> 32) != hi) return;  // a run of one
+  if ((uint32_t)(k2 >> 32) != hi) {        // a run of two
+    if ((uint32_t)k0 > (uint32_t)k1) {
+      const uint32_t a = ids[i], b = ids[i + 1];
+      keys[i] = k1; keys[i + 1] = k0;
+      ids[i] = b; ids[i + 1] = a;
+    }
+    return;
+  }
+  const uint32_t size = hi_run_end(keys, i, hi, nv) - i;
+  if (size > MB_THREAD_RUN) {
+    const uint32_t slot = atomicAdd(&rs->count, 1u);
+    if (slot < maxRuns) runs[slot] = make_uint4(i, size, hi, 0);
+    else atomicOr(&rs->pad, 1u);  // cannot happen: maxRuns = nv / (MB_THREAD_RUN + 1) + 1
+    atomicAdd(&rs->elems, size);
+    atomicMax(&rs->maxSize, size);
+    return;
+  }
+  uint32_t lo[MB_THREAD_RUN], id[MB_THREAD_RUN];
+  bool sorted = true;
+  for (uint32_t j = 0; j < size; j++) {
+    lo[j] = (uint32_t)keys[i + j];
+    id[j] = ids[i + j];
+    if (j && lo[j] < lo[j - 1]) sorted = false;
+  }
+  if (sorted) return;  // e.g. identical keys: already in stable order
+  for (uint32_t a = 1; a < size; a++) {  // insertion sort: stable
+    const uint32_t x = lo[a], y = id[a];
+    uint32_t b = a;
+    while (b > 0 && lo[b - 1] > x) {
+      lo[b] = lo[b - 1];
+      id[b] = id[b - 1];
+      b--;
+    }
+    lo[b] = x;
+    id[b] = y;
+  }
+  for (uint32_t j = 0; j < size; j++) {
+    keys[i + j] = ((uint64_t)hi << 32) | lo[j];
+    ids[i + j] = id[j];
+  }
+}
+
+__global__ void k_run_sizes(const uint4 *__restrict__ runs, uint32_t numRuns, uint32_t *__restrict__ sizes)
+{
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < numRuns) sizes[r] = runs[r].y;
+}
+
+// the run of compacted slot t: last run whose offset is <= t
+__device__ __forceinline__ uint32_t run_of(const uint32_t *__restrict__ off, uint32_t numRuns, uint32_t t)
+{
+  uint32_t lo = 0, hi = numRuns;
+  while (hi - lo > 1) {
+    const uint32_t m = (lo + hi) >> 1;
+    if (__ldg(off + m) <= t) lo = m; else hi = m;
+  }
+  return lo;
+}
+
+__global__ void k_run_gather(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off, uint32_t numRuns,
+                             uint32_t numSlots, const uint64_t *__restrict__ keys, const uint32_t *__restrict__ ids,
+                             uint64_t *__restrict__ kk, uint32_t *__restrict__ vv)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= numSlots) return;
+  const uint32_t r = run_of(off, numRuns, t);
+  const uint32_t pos = runs[r].x + (t - off[r]);
+  kk[t] = ((uint64_t)r << 32) | (uint32_t)keys[pos];
+  vv[t] = ids[pos];
+}
+
+__global__ void k_run_scatter(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off, uint32_t numSlots,
+                              const uint64_t *__restrict__ kk, const uint32_t *__restrict__ vv,
+                              uint64_t *__restrict__ keys, uint32_t *__restrict__ ids)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= numSlots) return;
+  const uint64_t k = kk[t];
+  const uint32_t r = (uint32_t)(k >> 32);
+  const uint4 run = runs[r];
+  const uint32_t pos = run.x + (t - off[r]);
+  keys[pos] = ((uint64_t)run.z << 32) | (uint32_t)k;
+  ids[pos] = vv[t];
 }
 
 // ------------------------------------------------------------------
@@ -349,6 +484,52 @@ __global__ void k_collapse(const Node *__restrict__ full, const uint2 *__restric
 } // namespace
 
 // ------------------------------------------------------------------
+// low-bit order inside runs of equal top bits (after the 4-pass sort)
+// ------------------------------------------------------------------
+namespace {
+int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *spareIds, uint32_t n,
+                  const uint32_t *nvDev, uint32_t *err, Alloc &al)
+{
+  const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
+  TempSet tmp(al);
+  RunStats *rs = nullptr;
+  uint4 *runs = nullptr;
+  BQ_TRY(tmp.get(&rs, 1));
+  BQ_TRY(tmp.get(&runs, maxRuns));
+  BQ_CUDA(cudaMemsetAsync(rs, 0, sizeof(RunStats), al.s));
+  {
+    ProfScope ps("morton.runs", al.s);
+    k_fix_runs<<<div_up(n, 256), 256, 0, al.s>>>(keys, ids, nvDev, rs, runs, maxRuns);
+  }
+  RunStats h{};
+  BQ_CUDA(cudaMemcpyAsync(&h, rs, sizeof(h), cudaMemcpyDeviceToHost, al.s));
+  BQ_CUDA(cudaStreamSynchronize(al.s));
+  if (h.pad) return set_error(BQ_ERR_CUDA, "run list overflow in the Morton build");
+  if (h.count == 0) return BQ_OK;
+  // runs longer than MB_THREAD_RUN: one stable sort of (run, low 32 bits)
+  // over just their prims, written back into each run's range
+  const uint32_t R = h.count, P = h.elems;
+  uint32_t *off = nullptr;
+  BQ_TRY(tmp.get(&off, R + 1ull));
+  k_run_sizes<<<div_up(R, 256), 256, 0, al.s>>>(runs, R, off);
+  BQ_TRY(exclusive_scan_u32(off, off, R, nullptr, off + R, al));
+  uint64_t *kk[2] = {spareKeys, nullptr};
+  uint32_t *vv[2] = {spareIds, nullptr};
+  BQ_TRY(tmp.get(&kk[1], P));
+  BQ_TRY(tmp.get(&vv[1], P));
+  ProfScope ps("morton.longruns", al.s, 2);
+  k_run_gather<<<div_up(P, 256), 256, 0, al.s>>>(runs, off, R, P, keys, ids, kk[0], vv[0]);
+  int runBits = 0;
+  while (runBits < 32 && ((R - 1) >> runBits)) runBits++;
+  int ksel = 0;
+  BQ_TRY(onesweep_sort_u64(kk, vv, P, nullptr, 0, 32 + runBits, nullptr, &ksel, err, al));
+  k_run_scatter<<<div_up(P, 256), 256, 0, al.s>>>(runs, off, P, kk[ksel], vv[ksel], keys, ids);
+  BQ_CUDA(cudaGetLastError());
+  return BQ_OK;
+}
+} // namespace
+
+// ------------------------------------------------------------------
 // host entry
 // ------------------------------------------------------------------
 int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al)
@@ -375,7 +556,7 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   BQ_TRY(tmp.get(&st, 1));
   BQ_TRY(tmp.get(&partials, grid));
   BQ_TRY(tmp.get(&blockOff, grid));
-  BQ_TRY(tmp.get(&hist, 8 * 256));
+  BQ_TRY(tmp.get(&hist, MB_HIST_PASSES * 256));
   BQ_TRY(tmp.get(&keysA, n));
   BQ_TRY(tmp.get(&keysB, n));
   BQ_TRY(tmp.get(&delta, n));
@@ -397,7 +578,7 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
 
   {
     ProfScope ps("morton.bounds", al.s);
-    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, 8 * 256);
+    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, MB_HIST_PASSES * 256);
   }
   {
     ProfScope ps("morton.keygen", al.s);
@@ -408,11 +589,13 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   uint64_t *keys2[2] = {keysA, keysB};
   uint32_t *ids2[2] = {idsA, idsB};
   int sel = 0;
-  if ((s = onesweep_sort_u64(keys2, ids2, n, &st->numValid, 0, 63, hist, &sel, &st->err, al)) != BQ_OK)
+  if ((s = onesweep_sort_u64(keys2, ids2, n, &st->numValid, MB_SORT_BEGIN, 63, hist, &sel, &st->err, al)) != BQ_OK)
     return fail(s);
   uint64_t *keys = keys2[sel];
   uint32_t *ids = ids2[sel];
   uint32_t *idsOther = ids2[sel ^ 1];
+  if ((s = sort_low_bits(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, &st->err, al)) != BQ_OK)
+    return fail(s);
 
   {
     ProfScope ps("morton.delta", al.s);

@@ -10,7 +10,8 @@
 //   1. loads its keys (warp-contiguous, coalesced),
 //   2. ranks them stably with __match_any_sync: per warp, per round of 32
 //      consecutive keys, peers with the same digit share one update of a
-//      warp-private digit histogram in shared memory,
+//      warp-private digit histogram in shared memory; each warp runs two
+//      such chains (first and second half of its keys) interleaved,
 //   3. publishes its 256 digit counts and resolves its global digit
 //      offsets by decoupled look-back over earlier tiles (one thread per
 //      digit; every wait is bounded and aborts the whole pass on timeout),
@@ -120,26 +121,30 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
   const uint32_t n = nDev ? *nDev : nHost;
   constexpr int TILE = SORT_BLOCK * ITEMS;
   constexpr int WARP_ITEMS = 32 * ITEMS;
-  // dynamic shared memory: keys [TILE], then values [TILE]; the per-warp
-  // digit histograms live in the value region until the local positions
-  // are known (they are dead before the first value is stored)
+  // dynamic shared memory: keys [TILE], then values [TILE]; the digit
+  // histograms (two per warp) overlay both until the local positions are
+  // known (they are dead before the first key is stored)
   extern __shared__ __align__(16) unsigned char smem[];
   KeyT *sKeys = (KeyT *)smem;
   uint32_t *sVals = (uint32_t *)(smem + sizeof(KeyT) * TILE);
-  uint32_t *sWarpHist = sVals;  // SORT_WARPS * 257 <= TILE
+  uint32_t *sWarpHist = (uint32_t *)smem;  // SORT_WARPS * 2 histograms of 257
   __shared__ uint32_t sTileStart[256];
   __shared__ uint32_t sGlobalBase[256];
   __shared__ uint32_t sWarpSums[SORT_WARPS];
   __shared__ uint32_t sTile;
   __shared__ uint32_t sBad;
-  static_assert(SORT_WARPS * 257 <= TILE, "histograms must fit in the value region");
+  constexpr int NHIST = SORT_WARPS * 2;
+  constexpr int HALF = ITEMS / 2;
+  static_assert(ITEMS % 2 == 0, "two ranking chains of ITEMS/2 rounds");
+  static_assert(TILE <= 0xffff, "tile positions are packed in 16 bits");
+  static_assert(NHIST * 257 * 4 <= (sizeof(KeyT) + 4) * TILE, "histograms must fit in the tile buffers");
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
     sTile = atomicAdd(ctl.tileCtr, 1u);
     sBad = 0;
   }
-  for (int i = threadIdx.x; i < SORT_WARPS * 257; i += SORT_BLOCK) sWarpHist[i] = 0;
+  for (int i = threadIdx.x; i < NHIST * 257; i += SORT_BLOCK) sWarpHist[i] = 0;
   __syncthreads();
   const uint32_t tile = sTile;
   const uint64_t warpBase = (uint64_t)tile * TILE + (uint64_t)warp * WARP_ITEMS;
@@ -152,20 +157,32 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
     key[r] = idx < n ? keysIn[idx] : (KeyT)0;
   }
 
-  // 2. stable ranking inside each warp
-  uint32_t *wh = sWarpHist + warp * 257;
+  // 2. stable ranking inside each warp, as two independent chains (rounds
+  // [0, HALF) and [HALF, ITEMS), each with its own digit histogram) so that
+  // the shared-memory round trips of one overlap those of the other
+  uint32_t *wh0 = sWarpHist + (2 * warp) * 257;
+  uint32_t *wh1 = wh0 + 257;
   const uint32_t ltMask = lanemask_lt();
-  uint32_t pos[ITEMS];  // rank within warp and digit, later the tile-local position
+  const uint32_t geMask = ~ltMask;
+  // pos2[r]: low half for item r, high half for item r + HALF -- the rank
+  // within (warp, chain, digit), later the tile-local position (< 2^16;
+  // 0xffff marks an item past the end)
+  uint32_t pos2[HALF];
 #pragma unroll
-  for (int r = 0; r < ITEMS; r++) {
-    const bool valid = warpBase + (uint64_t)r * 32 + lane < n;
-    const uint32_t d = valid ? digit_of(key[r], shift) : 256u;  // 256: never written
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    const uint32_t base = wh[d];
+  for (int r = 0; r < HALF; r++) {
+    const bool v0 = warpBase + (uint64_t)r * 32 + lane < n;
+    const bool v1 = warpBase + (uint64_t)(r + HALF) * 32 + lane < n;
+    const uint32_t d0 = v0 ? digit_of(key[r], shift) : 256u;  // 256: padding slot, never read back
+    const uint32_t d1 = v1 ? digit_of(key[r + HALF], shift) : 256u;
+    const uint32_t p0 = __match_any_sync(0xffffffffu, d0);
+    const uint32_t p1 = __match_any_sync(0xffffffffu, d1);
+    const uint32_t b0 = wh0[d0];
+    const uint32_t b1 = wh1[d1];
     __syncwarp();
-    if ((peers & ~(ltMask | (1u << lane))) == 0) wh[d] = base + __popc(peers);  // highest lane of the group
+    if ((p0 & geMask) == (1u << lane)) wh0[d0] = b0 + __popc(p0);  // highest lane of the group
+    if ((p1 & geMask) == (1u << lane)) wh1[d1] = b1 + __popc(p1);
     __syncwarp();
-    pos[r] = base + __popc(peers & ltMask);
+    pos2[r] = (b0 + __popc(p0 & ltMask)) | ((b1 + __popc(p1 & ltMask)) << 16);
   }
   __syncthreads();
 
@@ -173,9 +190,9 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
   const int d = threadIdx.x;
   uint32_t cnt = 0;
 #pragma unroll
-  for (int w = 0; w < SORT_WARPS; w++) {
-    const uint32_t c = sWarpHist[w * 257 + d];
-    sWarpHist[w * 257 + d] = cnt;
+  for (int h = 0; h < NHIST; h++) {  // (warp, chain) in tile order
+    const uint32_t c = sWarpHist[h * 257 + d];
+    sWarpHist[h * 257 + d] = cnt;
     cnt += c;
   }
   uint32_t tileTotal;
@@ -187,7 +204,7 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
   uint32_t *st = ctl.status;
   if (tile == 0) {
     __stcg(&st[d], ST_INC | cnt);
-    sGlobalBase[d] = gStart;
+    sGlobalBase[d] = gStart - sTileStart[d];  // global position = this + tile position
   } else {
     __stcg(&st[(uint64_t)tile * 256 + d], ST_AGG | cnt);
     uint32_t excl = 0;
@@ -216,31 +233,42 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
     } else {
       __stcg(&st[(uint64_t)tile * 256 + d], ST_INC | (excl + cnt));
     }
-    sGlobalBase[d] = gStart + excl;
+    sGlobalBase[d] = gStart + excl - sTileStart[d];
   }
   __syncthreads();
   if (sBad) return;  // a wait timed out: leave the output untouched, report
 
   // 4. tile-local positions; then keys and values through shared memory
 #pragma unroll
-  for (int r = 0; r < ITEMS; r++) {
-    const bool valid = warpBase + (uint64_t)r * 32 + lane < n;
-    const uint32_t dd = digit_of(key[r], shift);
-    pos[r] = valid ? sTileStart[dd] + sWarpHist[warp * 257 + dd] + pos[r] : 0xffffffffu;
+  for (int r = 0; r < HALF; r++) {
+    uint32_t lo = pos2[r] & 0xffffu, hi = pos2[r] >> 16;
+    const bool v0 = warpBase + (uint64_t)r * 32 + lane < n;
+    const bool v1 = warpBase + (uint64_t)(r + HALF) * 32 + lane < n;
+    const uint32_t d0 = digit_of(key[r], shift), d1 = digit_of(key[r + HALF], shift);
+    lo = v0 ? sTileStart[d0] + sWarpHist[(2 * warp) * 257 + d0] + lo : 0xffffu;
+    hi = v1 ? sTileStart[d1] + sWarpHist[(2 * warp + 1) * 257 + d1] + hi : 0xffffu;
+    pos2[r] = lo | (hi << 16);
   }
-  __syncthreads();  // histograms dead: the value region may be written now
+  __syncthreads();  // histograms dead: the tile buffers may be written now
 #pragma unroll
-  for (int r = 0; r < ITEMS; r++)
-    if (pos[r] != 0xffffffffu) sKeys[pos[r]] = key[r];
+  for (int r = 0; r < HALF; r++) {
+    const uint32_t lo = pos2[r] & 0xffffu, hi = pos2[r] >> 16;
+    if (lo != 0xffffu) sKeys[lo] = key[r];
+    if (hi != 0xffffu) sKeys[hi] = key[r + HALF];
+  }
   uint32_t val[ITEMS];
 #pragma unroll
-  for (int r = 0; r < ITEMS; r++) {
-    const uint64_t idx = warpBase + (uint64_t)r * 32 + lane;
-    val[r] = pos[r] != 0xffffffffu ? valsIn[idx] : 0u;
+  for (int r = 0; r < HALF; r++) {
+    const uint64_t i0 = warpBase + (uint64_t)r * 32 + lane, i1 = warpBase + (uint64_t)(r + HALF) * 32 + lane;
+    val[r] = (pos2[r] & 0xffffu) != 0xffffu ? valsIn[i0] : 0u;
+    val[r + HALF] = (pos2[r] >> 16) != 0xffffu ? valsIn[i1] : 0u;
   }
 #pragma unroll
-  for (int r = 0; r < ITEMS; r++)
-    if (pos[r] != 0xffffffffu) sVals[pos[r]] = val[r];
+  for (int r = 0; r < HALF; r++) {
+    const uint32_t lo = pos2[r] & 0xffffu, hi = pos2[r] >> 16;
+    if (lo != 0xffffu) sVals[lo] = val[r];
+    if (hi != 0xffffu) sVals[hi] = val[r + HALF];
+  }
   __syncthreads();
   // 5. scatter: consecutive tile positions of one digit go to consecutive
   // global positions
@@ -250,7 +278,7 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
     if (p < tileTotal) {
       const KeyT k = sKeys[p];
       const uint32_t dd = digit_of(k, shift);
-      const uint32_t g = sGlobalBase[dd] + (p - sTileStart[dd]);
+      const uint32_t g = sGlobalBase[dd] + p;  // unsigned wrap-around is intended
       if (g < n) {
         keysOut[g] = k;
         valsOut[g] = sVals[p];
