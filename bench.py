@@ -347,6 +347,45 @@ def _ev_time(torch, fn, reps=3, warm=1):
     return a.elapsed_time(b) / reps
 
 
+def c1_component(bq, W, torch, comp, pts_np, tp, boxes_t):
+    """The 1M-point configuration: spatial-median build (leaf 8) and 1M
+    closest-point queries, ours against the reference's GPU builder and
+    kernel (sm_100a) and the reference's host builder and query (one core,
+    and all cores for the query)."""
+    n1 = 1_000_000
+    b1, tp1 = boxes_t[:n1], tp[:n1]
+    q1 = W.uniform_points(n1, W.SEED_QUERIES, -0.1, 1.1)
+    tq1 = torch.from_numpy(q1).cuda()
+    cfg = bq.BuildConfig(makeLeafThreshold=8)
+    ms_b = _ev_time(torch, lambda: bq.gpuBuilder(b1, cfg).free())
+    t = bq.gpuBuilder(b1, cfg)
+    ms_q = _ev_time(torch, lambda: bq.points.findClosest(t, tp1, tq1))
+    t.free()
+    out = {"points": n1, "queries": n1, "leaf": 8, "build_ms": ms_b, "closest_point_ms": ms_q,
+           "build_Mprims_s": n1 / ms_b / 1e3, "Mqueries_s": n1 / ms_q / 1e3}
+    from oracle.oracle import RefCPU, RefGPU, have_ref_cpu, have_ref_gpu
+    if have_ref_gpu():
+        r = RefGPU()
+        out["reference_gpu_build_ms"] = r.time_build(RefGPU.SPATIAL_MEDIAN, pts_np[:n1], 8, reps=3)
+        out["reference_gpu_closest_point_ms"] = r.time_query(RefGPU.SPATIAL_MEDIAN, pts_np[:n1], q1, 0, 8, reps=3)
+    if have_ref_cpu():
+        rc = RefCPU()
+        bx = W.point_boxes(pts_np[:n1])
+        t0 = time.perf_counter()
+        nodes, prims = rc.build(bx, 8)
+        out["reference_cpu_build_ms"] = (time.perf_counter() - t0) * 1e3
+        sample = 100_000
+        t0 = time.perf_counter()
+        rc.closest_point(nodes, prims, pts_np[:n1], q1[:sample], threads=1)
+        out["reference_cpu_closest_point_ms_1core"] = (time.perf_counter() - t0) * 1e3 * n1 / sample
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        rc.closest_point(nodes, prims, pts_np[:n1], q1, threads=threads)
+        out["reference_cpu_closest_point_ms_allcores"] = (time.perf_counter() - t0) * 1e3
+        out["host_threads"] = threads
+    comp["c1_1M_points_leaf8"] = out
+
+
 def batched_components(bq, W, torch, comp):
     """The two batched workloads: 512 point clouds (about 19M points, 25.6M
     kNN(16) queries; one segmented build + one query launch replayed from a
@@ -414,10 +453,13 @@ def batched_components(bq, W, torch, comp):
         state["v"] = v - 0.5 * gv
         return ids, d
     ms_step = _ev_time(torch, step, reps=100, warm=3)
-    ids, d = step()
-    fresh = bq.Batch(bq.triangles.boxes(tt, state["v"]), toff_t)
-    fi, fd, _ = bq.batched_tri_closest(fresh, tt, state["v"], tqm, qoff_t)
-    ids2, d2, _ = bq.batched_tri_closest(batch, tt, state["v"], tqm, qoff_t)
+    # the refitted trees against trees rebuilt from scratch, at the current vertices
+    v = state["v"]
+    boxes = bq.triangles.boxes(tt, v)
+    bq.batched_refit(batch, boxes)
+    ids2, d2, _ = bq.batched_tri_closest(batch, tt, v, tqm, qoff_t)
+    fresh = bq.Batch(boxes, toff_t)
+    fi, fd, _ = bq.batched_tri_closest(fresh, tt, v, tqm, qoff_t)
     comp["fit_loop_128_meshes"] = {
         "meshes": len(toffm) - 1, "triangles": int(len(tris)), "queries_per_step": int(len(qsm)), "steps": 100,
         "ms_per_step": ms_step, "fwd_bwd_queries_s": len(qsm) / ms_step * 1e3,
@@ -517,6 +559,7 @@ def run_ours(args):
     cpu_baseline = None
     if rank == 0 and not args.no_components:
         components(bq, W, torch, pts_np, tp, boxes_t, comp)
+        c1_component(bq, W, torch, comp, pts_np, tp, boxes_t)
         batched_components(bq, W, torch, comp)
         reference_gpu(comp, pts_np, W)
     if rank == 0:

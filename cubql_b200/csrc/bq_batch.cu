@@ -607,7 +607,7 @@ int batched_knn(const bq_bvh3f *bvhs, const uint32_t *poff, const float *points,
   const uint32_t *order = nullptr;
   const uint64_t *skeys = keys[0];
   if (c.reorder) {
-    BQ_TRY(onesweep_sort_u64(keys, idx, nq, nullptr, 0, 32 + segBits, nullptr, &sel, dErr, al));
+    BQ_TRY(onesweep_sort_u64(keys, idx, nq, nullptr, 6, 32 + segBits, nullptr, &sel, dErr, al));  // order only
     order = idx[sel];
     skeys = keys[sel];
   }

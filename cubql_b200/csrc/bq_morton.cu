@@ -10,14 +10,15 @@
 //   k_keygen      stable compaction of valid prims, 63-bit Morton keys
 //                 (radix.h:41-62 Quantizer, 283-421 key generation) and the
 //                 digit histograms of the top key bits
-//   onesweep sort stable (key, primID) sort on key bits [32, 63) only: 4
+//   onesweep sort stable (key, primID) sort on key bits [39, 63) only: 3
 //                 digit passes instead of 8 (bq_sort.cu)
-//   k_fix_runs    runs of equal top bits are then ordered by the low 32
+//   k_fix_runs    runs of equal top bits are then ordered by the low 39
 //                 bits, stably: runs of up to 32 prims by one thread each
-//                 (on uniform data nearly all runs are of 1-3 prims),
+//                 (on uniform data nearly all runs are of 1-4 prims),
 //                 longer runs by one segmented composite-key sort of just
 //                 their prims ((run, low bits) keys).  The result is the
-//                 full stable 63-bit order, as cub's SortPairs gives
+//                 full stable 63-bit order, as cub's SortPairs gives.  The
+//                 same kernel writes the split levels (below) and slots
 //   k_delta       one byte per adjacent key pair: the level at which the
 //                 reference's top-down split would separate them
 //   agglomerate   bottom-up construction of topology and boxes
@@ -61,8 +62,10 @@ namespace {
 constexpr int MB_BLOCK = 256;
 constexpr int MB_UNROLL = 4;
 constexpr uint32_t SLOT_EMPTY = 0xffffffffu;
-constexpr int MB_SORT_BEGIN = 32;   // the global sort covers key bits [32, 63)
-constexpr int MB_HIST_PASSES = 4;   // its digit passes
+constexpr int MB_SORT_BEGIN = 39;   // the global sort covers key bits [39, 63): 24 bits
+constexpr int MB_HIST_PASSES = 3;   // its digit passes
+constexpr uint64_t MB_LOW_MASK = (1ull << MB_SORT_BEGIN) - 1;  // bits ordered inside runs
+__device__ __forceinline__ uint32_t key_hi(uint64_t k) { return (uint32_t)(k >> MB_SORT_BEGIN); }
 constexpr uint32_t MB_THREAD_RUN = 32;  // longest run of equal top bits one thread orders
 
 struct __align__(16) Partial {
@@ -274,83 +277,131 @@ __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict_
 }
 
 // ------------------------------------------------------------------
-// runs of equal top key bits: order them by the low 32 bits, stably
+// runs of equal top key bits: order them by the low bits, stably
 // ------------------------------------------------------------------
 struct RunStats {
   uint32_t count, elems, maxSize, pad;
 };
 
-// one past the last index j >= i with keys[j] >> 32 == hi (keys[i] >> 32 == hi)
+// one past the last index j >= i with key_hi(keys[j]) == hi (key_hi(keys[i]) == hi)
 __device__ __forceinline__ uint32_t hi_run_end(const uint64_t *__restrict__ keys, uint32_t i, uint32_t hi, uint32_t n)
 {
   uint32_t step = 1, lo = i + 1, up = n;
   while (lo < up) {
     const uint32_t probe = lo - 1 + min(step, up - lo + 1);
-    if (probe >= up || (uint32_t)(keys[probe] >> 32) != hi) { up = min(probe, up); break; }
+    if (probe >= up || key_hi(keys[probe]) != hi) { up = min(probe, up); break; }
     lo = probe + 1;
     step <<= 1;
   }
   while (lo < up) {
     const uint32_t m = lo + ((up - lo) >> 1);
-    if ((uint32_t)(keys[m] >> 32) == hi) lo = m + 1; else up = m;
+    if (key_hi(keys[m]) == hi) lo = m + 1; else up = m;
   }
   return lo;
 }
 
+// split level of two different keys (highest differing bit + 64)
+__device__ __forceinline__ uint8_t key_level(uint64_t a, uint64_t b) { return (uint8_t)(64 + (63 - __clzll(a ^ b))); }
+
+// level of split position s inside the run [r0, r1) of equal keys: 63 minus
+// its depth in the (b+e)/2 recursion of radix.h:455-465
+__device__ __forceinline__ uint8_t equal_run_level(uint64_t r0, uint64_t r1, uint64_t s)
+{
+  int depth = 0;
+  while (true) {
+    const uint64_t m = (r0 + r1) / 2;
+    if (s == m) break;
+    if (s < m) r1 = m; else r0 = m;
+    depth++;
+  }
+  return (uint8_t)(63 - depth);
+}
+
+// One thread per sorted position i (keys sorted on bits [MB_SORT_BEGIN, 63)
+// only):
+//   * initialises the agglomeration slot of i;
+//   * writes the split level of the pair (i, i+1) when the two lie in
+//     different runs of equal top bits -- their highest differing bit is in
+//     the top bits, so the order inside the runs does not change it;
+//   * the first thread of a run of up to MB_THREAD_RUN prims orders the run
+//     on the low bits (stable insertion sort) and writes the levels of the
+//     pairs inside it; longer runs are listed for a segmented sort (their
+//     inner levels are written by k_delta afterwards).
 __global__ void __launch_bounds__(256) k_fix_runs(uint64_t *keys, uint32_t *ids, const uint32_t *nvPtr,
+                                                  uint8_t *__restrict__ delta, uint32_t *__restrict__ slot,
                                                   RunStats *rs, uint4 *runs, uint32_t maxRuns)
 {
   const uint32_t nv = *nvPtr;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
+  slot[i] = SLOT_EMPTY;
   // the four neighbouring keys are independent loads (no dependent chain in
   // the common cases: runs of one and of two)
   const uint64_t k0 = keys[i];
   const uint64_t km = i > 0 ? keys[i - 1] : ~k0;
   const uint64_t k1 = i + 1 < nv ? keys[i + 1] : ~k0;
   const uint64_t k2 = i + 2 < nv ? keys[i + 2] : ~k0;
-  const uint32_t hi = (uint32_t)(k0 >> 32);
-  if ((uint32_t)(km >> 32) == hi) return;  // not the first of its run
-  if ((uint32_t)(k1 >> 32) != hi) return;  // a run of one
-  if ((uint32_t)(k2 >> 32) != hi) {        // a run of two
-    if ((uint32_t)k0 > (uint32_t)k1) {
-      const uint32_t a = ids[i], b = ids[i + 1];
+  const uint32_t hi = key_hi(k0);
+  if (i + 1 < nv && key_hi(k1) != hi) delta[i] = key_level(k0, k1);  // pair across two runs
+  if (key_hi(km) == hi) return;  // not the first of its run
+  if (key_hi(k1) != hi) return;  // a run of one
+  if (key_hi(k2) != hi) {        // a run of two
+    uint64_t a = k0, b = k1;
+    if (k0 > k1) {
+      const uint32_t ia = ids[i], ib = ids[i + 1];
       keys[i] = k1; keys[i + 1] = k0;
-      ids[i] = b; ids[i + 1] = a;
+      ids[i] = ib; ids[i + 1] = ia;
+      a = k1; b = k0;
     }
+    delta[i] = a != b ? key_level(a, b) : (uint8_t)63;  // equal: the midpoint of [i, i+2)
     return;
   }
   const uint32_t size = hi_run_end(keys, i, hi, nv) - i;
   if (size > MB_THREAD_RUN) {
-    const uint32_t slot = atomicAdd(&rs->count, 1u);
-    if (slot < maxRuns) runs[slot] = make_uint4(i, size, hi, 0);
+    const uint32_t slotIdx = atomicAdd(&rs->count, 1u);
+    if (slotIdx < maxRuns) runs[slotIdx] = make_uint4(i, size, hi, 0);
     else atomicOr(&rs->pad, 1u);  // cannot happen: maxRuns = nv / (MB_THREAD_RUN + 1) + 1
     atomicAdd(&rs->elems, size);
     atomicMax(&rs->maxSize, size);
     return;
   }
-  uint32_t lo[MB_THREAD_RUN], id[MB_THREAD_RUN];
+  // whole keys (the top bits are equal inside the run) and ids
+  uint64_t kr[MB_THREAD_RUN];
+  uint32_t id[MB_THREAD_RUN];
   bool sorted = true;
   for (uint32_t j = 0; j < size; j++) {
-    lo[j] = (uint32_t)keys[i + j];
+    kr[j] = keys[i + j];
     id[j] = ids[i + j];
-    if (j && lo[j] < lo[j - 1]) sorted = false;
+    if (j && kr[j] < kr[j - 1]) sorted = false;
   }
-  if (sorted) return;  // e.g. identical keys: already in stable order
-  for (uint32_t a = 1; a < size; a++) {  // insertion sort: stable
-    const uint32_t x = lo[a], y = id[a];
-    uint32_t b = a;
-    while (b > 0 && lo[b - 1] > x) {
-      lo[b] = lo[b - 1];
-      id[b] = id[b - 1];
-      b--;
+  if (!sorted) {
+    for (uint32_t a = 1; a < size; a++) {  // insertion sort: stable
+      const uint64_t x = kr[a];
+      const uint32_t y = id[a];
+      uint32_t b = a;
+      while (b > 0 && kr[b - 1] > x) {
+        kr[b] = kr[b - 1];
+        id[b] = id[b - 1];
+        b--;
+      }
+      kr[b] = x;
+      id[b] = y;
     }
-    lo[b] = x;
-    id[b] = y;
+    for (uint32_t j = 0; j < size; j++) {
+      keys[i + j] = kr[j];
+      ids[i + j] = id[j];
+    }
   }
-  for (uint32_t j = 0; j < size; j++) {
-    keys[i + j] = ((uint64_t)hi << 32) | lo[j];
-    ids[i + j] = id[j];
+  // levels of the pairs inside the run
+  for (uint32_t j = 0; j + 1 < size; j++) {
+    if (kr[j] != kr[j + 1]) {
+      delta[i + j] = key_level(kr[j], kr[j + 1]);
+    } else {
+      uint32_t e0 = j, e1 = j + 2;
+      while (e0 > 0 && kr[e0 - 1] == kr[j]) e0--;
+      while (e1 < size && kr[e1] == kr[j]) e1++;
+      delta[i + j] = equal_run_level(i + e0, i + e1, (uint64_t)i + j + 1);
+    }
   }
 }
 
@@ -379,7 +430,7 @@ __global__ void k_run_gather(const uint4 *__restrict__ runs, const uint32_t *__r
   if (t >= numSlots) return;
   const uint32_t r = run_of(off, numRuns, t);
   const uint32_t pos = runs[r].x + (t - off[r]);
-  kk[t] = ((uint64_t)r << 32) | (uint32_t)keys[pos];
+  kk[t] = ((uint64_t)r << MB_SORT_BEGIN) | (keys[pos] & MB_LOW_MASK);
   vv[t] = ids[pos];
 }
 
@@ -390,10 +441,10 @@ __global__ void k_run_scatter(const uint4 *__restrict__ runs, const uint32_t *__
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numSlots) return;
   const uint64_t k = kk[t];
-  const uint32_t r = (uint32_t)(k >> 32);
+  const uint32_t r = (uint32_t)(k >> MB_SORT_BEGIN);
   const uint4 run = runs[r];
   const uint32_t pos = run.x + (t - off[r]);
-  keys[pos] = ((uint64_t)run.z << 32) | (uint32_t)k;
+  keys[pos] = ((uint64_t)run.z << MB_SORT_BEGIN) | (k & MB_LOW_MASK);
   ids[pos] = vv[t];
 }
 
@@ -487,9 +538,13 @@ __global__ void k_collapse(const Node *__restrict__ full, const uint2 *__restric
 // low-bit order inside runs of equal top bits (after the 4-pass sort)
 // ------------------------------------------------------------------
 namespace {
+// Orders the runs of equal top bits and writes every split level and slot;
+// *longRuns tells whether runs above MB_THREAD_RUN were sorted (their inner
+// levels are then still to be written).
 int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *spareIds, uint32_t n,
-                  const uint32_t *nvDev, uint32_t *err, Alloc &al)
+                  const uint32_t *nvDev, uint8_t *delta, uint32_t *slot, uint32_t *err, bool *longRuns, Alloc &al)
 {
+  *longRuns = false;
   const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
   TempSet tmp(al);
   RunStats *rs = nullptr;
@@ -499,14 +554,15 @@ int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *
   BQ_CUDA(cudaMemsetAsync(rs, 0, sizeof(RunStats), al.s));
   {
     ProfScope ps("morton.runs", al.s);
-    k_fix_runs<<<div_up(n, 256), 256, 0, al.s>>>(keys, ids, nvDev, rs, runs, maxRuns);
+    k_fix_runs<<<div_up(n, 256), 256, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs, maxRuns);
   }
   RunStats h{};
   BQ_CUDA(cudaMemcpyAsync(&h, rs, sizeof(h), cudaMemcpyDeviceToHost, al.s));
   BQ_CUDA(cudaStreamSynchronize(al.s));
   if (h.pad) return set_error(BQ_ERR_CUDA, "run list overflow in the Morton build");
   if (h.count == 0) return BQ_OK;
-  // runs longer than MB_THREAD_RUN: one stable sort of (run, low 32 bits)
+  *longRuns = true;
+  // runs longer than MB_THREAD_RUN: one stable sort of (run, low bits)
   // over just their prims, written back into each run's range
   const uint32_t R = h.count, P = h.elems;
   uint32_t *off = nullptr;
@@ -521,8 +577,9 @@ int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *
   k_run_gather<<<div_up(P, 256), 256, 0, al.s>>>(runs, off, R, P, keys, ids, kk[0], vv[0]);
   int runBits = 0;
   while (runBits < 32 && ((R - 1) >> runBits)) runBits++;
+  if (runBits > 64 - MB_SORT_BEGIN) return set_error(BQ_ERR_UNSUPPORTED, "too many long runs of equal keys");
   int ksel = 0;
-  BQ_TRY(onesweep_sort_u64(kk, vv, P, nullptr, 0, 32 + runBits, nullptr, &ksel, err, al));
+  BQ_TRY(onesweep_sort_u64(kk, vv, P, nullptr, 0, MB_SORT_BEGIN + runBits, nullptr, &ksel, err, al));
   k_run_scatter<<<div_up(P, 256), 256, 0, al.s>>>(runs, off, P, kk[ksel], vv[ksel], keys, ids);
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
@@ -594,10 +651,12 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   uint64_t *keys = keys2[sel];
   uint32_t *ids = ids2[sel];
   uint32_t *idsOther = ids2[sel ^ 1];
-  if ((s = sort_low_bits(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, &st->err, al)) != BQ_OK)
+  bool longRuns = false;
+  if ((s = sort_low_bits(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err, &longRuns,
+                         al)) != BQ_OK)
     return fail(s);
 
-  {
+  if (longRuns) {  // levels inside the long runs (rewrites all levels and slots)
     ProfScope ps("morton.delta", al.s);
     k_delta<<<div_up(n, 256), 256, 0, al.s>>>(keys, &st->numValid, delta, slot);
   }

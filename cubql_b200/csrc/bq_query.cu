@@ -6,9 +6,9 @@
 // thread per query in input order.  Here one call answers a whole batch:
 //
 //   k_query_keys   30-bit Morton code of every query inside the root box
-//   onesweep sort  queries reordered along the curve, so neighbouring
-//                  threads walk nearly the same nodes (L1/L2 reuse, less
-//                  divergence)
+//   onesweep sort  queries reordered along the curve (top 24 key bits),
+//                  so neighbouring threads walk nearly the same nodes
+//                  (L1/L2 reuse, less divergence)
 //   k_closest / k_knn
 //                  one thread per query, shrinking-radius traversal with a
 //                  local-memory stack (bq_traverse.cuh); kNN keeps its
@@ -248,7 +248,8 @@ int prepare(const bq_bvh3f *bvh, const float *queries, uint32_t nq, bool reorder
     }
     BQ_CUDA(cudaGetLastError());
     int sel = 0;
-    BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, 0, 30, nullptr, &sel, qs.err, al));
+    // the order only steers performance: the top 24 key bits (3 passes) suffice
+    BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, 6, 30, nullptr, &sel, qs.err, al));
     qs.order = idx[sel];
   }
   return BQ_OK;

@@ -284,16 +284,61 @@ __global__ void k_rb_newlevels(const RebinJob *__restrict__ jobs, const uint32_t
 // thread phase (threadPhaseCreateNodes, :766-872): one thread per run of
 // thr < size <= 32 equal keys
 // ------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_rb_thread(const uint32_t *__restrict__ starts, const uint32_t *numRunsPtr,
-                                                   int thr, const bq_box3f *__restrict__ boxes,
-                                                   uint32_t *__restrict__ ids, uint16_t *__restrict__ lev,
-                                                   uint8_t *__restrict__ forced)
+// If position i starts a run of at least two prims (level 0 between them),
+// its size, counted up to `cap` + 1 at most; else 0.
+__device__ __forceinline__ uint32_t run_size_at(const uint16_t *__restrict__ lev, uint32_t i, uint32_t nv, uint32_t cap)
 {
-  const uint32_t R = *numRunsPtr;
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= R) return;
-  const uint32_t start = starts[r], size = starts[r + 1] - start;
+  if (i + 1 >= nv || (i > 0 && lev[i - 1] == 0) || lev[i] != 0) return 0;
+  uint32_t size = 2;
+  while (size <= cap && i + size - 1 < nv - 1 && lev[i + size - 1] == 0) size++;
+  return size;
+}
+
+// counts the runs the broad phase must rebin (more than bigMin prims)
+__global__ void k_rb_detect(const uint16_t *__restrict__ lev, const uint32_t *nvPtr, uint32_t bigMin,
+                            uint32_t *numBig)
+{
+  const uint32_t nv = *nvPtr;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  if (run_size_at(lev, i, nv, bigMin) > bigMin) atomicAdd(numBig, 1u);
+}
+
+// one thread per run start; runs of thr < size <= 32 (the broad phase has
+// left no larger unresolved run)
+__global__ void __launch_bounds__(128) k_rb_thread(const uint32_t *nvPtr, int thr, const bq_box3f *__restrict__ boxes,
+                                                   uint32_t *__restrict__ ids, uint16_t *__restrict__ lev,
+                                                   uint8_t *__restrict__ forced, uint32_t *numForced)
+{
+  const uint32_t nv = *nvPtr;
+  const uint32_t start = blockIdx.x * blockDim.x + threadIdx.x;
+  if (start >= nv) return;
+  const uint32_t size = run_size_at(lev, start, nv, REBIN_THREAD_MAX);
   if ((int64_t)size <= thr || size > (uint32_t)REBIN_THREAD_MAX) return;
+  if (size == 2) {
+    // the common case (pairs of identical or near prims): the steps below
+    // for two prims, each centroid read once
+    const uint32_t i0 = ids[start], i1 = ids[start + 1];
+    const float3 c0 = rb_center(boxes, i0), c1 = rb_center(boxes, i1);
+    uint32_t k0 = 0, k1 = 1;  // a point domain keys by position
+    if (!(c0.x == c1.x && c0.y == c1.y && c0.z == c1.z)) {
+      const Quant30 q = make_quant30(fminf(c0.x, c1.x), fminf(c0.y, c1.y), fminf(c0.z, c1.z), fmaxf(c0.x, c1.x),
+                                     fmaxf(c0.y, c1.y), fmaxf(c0.z, c1.z));
+      k0 = morton30(c0, q);
+      k1 = morton30(c1, q);
+    }
+    if (k1 < k0) {  // the exchange sort of two keys
+      ids[start] = i1;
+      ids[start + 1] = i0;
+    }
+    if (k0 == k1) {
+      forced[start] = 1;
+      atomicAdd(numForced, 1u);
+    } else {
+      lev[start] = (uint16_t)32;  // split at depth 0 of the run
+    }
+    return;
+  }
   uint32_t key[REBIN_THREAD_MAX], id[REBIN_THREAD_MAX];
   for (uint32_t i = 0; i < size; i++) {
     key[i] = 0;  // the run's keys are all equal: only equality matters below
@@ -331,6 +376,7 @@ __global__ void __launch_bounds__(128) k_rb_thread(const uint32_t *__restrict__ 
           }
       if (key[b] == key[e - 1]) {  // still no split: a leaf, whatever its size
         for (uint32_t i = b; i + 1 < e; i++) forced[start + i] = 1;
+        atomicAdd(numForced, 1u);
         continue;
       }
     }
@@ -428,7 +474,7 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   uint8_t *forced = nullptr;
   BQ_TRY(tmp.get(&valid, n));
   BQ_TRY(tmp.get(&vpos, n));
-  BQ_TRY(tmp.get(&ctl, 16));  // [0] nv [1] err [2..7] bounds [8] runs [9] jobs [10] job prims
+  BQ_TRY(tmp.get(&ctl, 16));  // [0] nv [1] err [2..7] bounds [8] runs [9] jobs [10] job prims [11] thread leaves
   BQ_TRY(tmp.get(&keysA, n));
   BQ_TRY(tmp.get(&keysB, n));
   BQ_TRY(tmp.get(&idsB, n));
@@ -477,33 +523,32 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   uint32_t *bigRank = nullptr, *bigOff = nullptr, *jobOff = nullptr, *vv[2] = {nullptr, nullptr};
   uint64_t *kk[2] = {nullptr, nullptr};
   RebinJob *jobs = nullptr;
-  BQ_TRY(tmp.get(&flag, n));
-  BQ_TRY(tmp.get(&runIdx, n));
-  BQ_TRY(tmp.get(&starts, n + 1ull));
-  BQ_TRY(tmp.get(&big, n));
-  BQ_TRY(tmp.get(&bigSize, n));
-  BQ_TRY(tmp.get(&bigRank, n));
-  BQ_TRY(tmp.get(&bigOff, n));
   const uint32_t bigMin = (uint32_t)std::max(REBIN_THREAD_MAX, thr);
   uint32_t hnv = 0;
   for (int depth = 0;; depth++) {
-    ProfScope ps("rebin.runs", al.s, 13);
-    k_rb_run_flags<<<div_up(n, 256), 256, 0, al.s>>>(lev, nvDev, flag);
-    if ((s = exclusive_scan_u32(flag, runIdx, n, nvDev, ctl + 8, al)) != BQ_OK) return fail(s);
-    k_rb_run_starts<<<div_up(n, 256), 256, 0, al.s>>>(flag, runIdx, nvDev, starts);
-    k_rb_big<<<div_up(n, 256), 256, 0, al.s>>>(starts, ctl + 8, bigMin, big, bigSize);
-    if ((s = exclusive_scan_u32(big, bigRank, n, ctl + 8, ctl + 9, al)) != BQ_OK) return fail(s);
-    if ((s = exclusive_scan_u32(bigSize, bigOff, n, ctl + 8, ctl + 10, al)) != BQ_OK) return fail(s);
-    uint32_t h[11];
+    // one cheap pass decides whether any run still needs a broad-phase rebin
+    if ((ce = cudaMemsetAsync(ctl + 9, 0, 4, al.s)) != cudaSuccess) return fail(cuda_error(ce, "memset"));
+    {
+      ProfScope ps("rebin.detect", al.s);
+      k_rb_detect<<<div_up(n, 256), 256, 0, al.s>>>(lev, nvDev, bigMin, ctl + 9);
+    }
+    uint32_t h[10];
     if ((ce = cudaMemcpyAsync(h, ctl, sizeof(h), cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
         (ce = cudaStreamSynchronize(al.s)) != cudaSuccess)
       return fail(cuda_error(ce, "rebin runs"));
     hnv = h[0];
     if (h[1] & DEV_ERR_TIMEOUT) return fail(set_error(BQ_ERR_TIMEOUT, "radix sort look-back timed out"));
     if (h[1]) return fail(set_error(BQ_ERR_CUDA, "device-side range check failed in the rebin build"));
-    const uint32_t numJobs = h[9], numSlots = h[10];
-    if (hnv == 0 || numJobs == 0) break;
+    if (hnv == 0 || h[9] == 0) break;
+    // list the runs and the ones to rebin (their prims, compacted)
     if (!jobs) {
+      if ((s = tmp.get(&flag, n)) != BQ_OK) return fail(s);
+      if ((s = tmp.get(&runIdx, n)) != BQ_OK) return fail(s);
+      if ((s = tmp.get(&starts, n + 1ull)) != BQ_OK) return fail(s);
+      if ((s = tmp.get(&big, n)) != BQ_OK) return fail(s);
+      if ((s = tmp.get(&bigSize, n)) != BQ_OK) return fail(s);
+      if ((s = tmp.get(&bigRank, n)) != BQ_OK) return fail(s);
+      if ((s = tmp.get(&bigOff, n)) != BQ_OK) return fail(s);
       if ((s = tmp.get(&jobs, n)) != BQ_OK) return fail(s);
       if ((s = tmp.get(&jobOff, n)) != BQ_OK) return fail(s);
       if ((s = tmp.get(&kk[0], n)) != BQ_OK) return fail(s);
@@ -511,6 +556,20 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
       if ((s = tmp.get(&vv[0], n)) != BQ_OK) return fail(s);
       if ((s = tmp.get(&vv[1], n)) != BQ_OK) return fail(s);
     }
+    {
+      ProfScope ps("rebin.runs", al.s, 12);
+      k_rb_run_flags<<<div_up(n, 256), 256, 0, al.s>>>(lev, nvDev, flag);
+      if ((s = exclusive_scan_u32(flag, runIdx, n, nvDev, ctl + 8, al)) != BQ_OK) return fail(s);
+      k_rb_run_starts<<<div_up(n, 256), 256, 0, al.s>>>(flag, runIdx, nvDev, starts);
+      k_rb_big<<<div_up(n, 256), 256, 0, al.s>>>(starts, ctl + 8, bigMin, big, bigSize);
+      if ((s = exclusive_scan_u32(big, bigRank, n, ctl + 8, ctl + 9, al)) != BQ_OK) return fail(s);
+      if ((s = exclusive_scan_u32(bigSize, bigOff, n, ctl + 8, ctl + 10, al)) != BQ_OK) return fail(s);
+    }
+    uint32_t hj[2];
+    if ((ce = cudaMemcpyAsync(hj, ctl + 9, sizeof(hj), cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
+        (ce = cudaStreamSynchronize(al.s)) != cudaSuccess)
+      return fail(cuda_error(ce, "rebin runs"));
+    const uint32_t numJobs = hj[0], numSlots = hj[1];
     const int next = depth + 1;
     const bool cap = next >= REBIN_MAX_DEPTH;
     ProfScope ps2("rebin.rebin", al.s, 5);
@@ -532,19 +591,47 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     return BQ_OK;
   }
   // ---- thread phase ----
+  if ((ce = cudaMemsetAsync(ctl + 11, 0, 4, al.s)) != cudaSuccess) return fail(cuda_error(ce, "memset"));
   if (thr < REBIN_THREAD_MAX) {
     ProfScope ps("rebin.thread", al.s);
-    k_rb_thread<<<div_up(n, 128), 128, 0, al.s>>>(starts, ctl + 8, thr, boxes, ids, lev, forced);
+    k_rb_thread<<<div_up(hnv, 128), 128, 0, al.s>>>(nvDev, thr, boxes, ids, lev, forced, ctl + 11);
+  }
+  uint2 *pending = nullptr;
+  if ((s = tmp.get(&pending, 2ull * div_up(hnv, AGG_CHUNK))) != BQ_OK) return fail(s);
+  // ---- leaf threshold 1: the full tree is the result unless the thread
+  // phase made leaves of several prims ----
+  if (thr == 1) {
+    if ((s = al.get(&nodes, 2ull * hnv)) != BQ_OK) return fail(s);
+    {
+      ProfScope ps("rebin.agglomerate", al.s, 2);
+      AggArgsT<uint16_t> ag{lev, slot, ids, boxes, nodes, nullptr, nvDev, nullptr, pending, nullptr, 0};
+      if ((s = agglomerate<false>(ag, hnv, al.s)) != BQ_OK) return fail(s);
+    }
+    uint32_t hf[12];
+    if ((ce = cudaMemcpyAsync(hf, ctl, sizeof(hf), cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
+        (ce = cudaStreamSynchronize(al.s)) != cudaSuccess)
+      return fail(cuda_error(ce, "rebin sync"));
+    if (hf[1]) return fail(set_error(BQ_ERR_CUDA, "device-side check failed in the rebin build"));
+    if (hf[11] == 0) {
+      bvh->nodes = reinterpret_cast<bq_node3f *>(nodes);
+      bvh->numNodes = 2 * hnv;
+      bvh->primIDs = ids;
+      bvh->numPrims = hnv;
+      return BQ_OK;
+    }
+    al.free_bytes(nodes);  // rare: multi-prim leaves, go through the collapse below
+    nodes = nullptr;
+    if ((ce = cudaMemsetAsync(slot, 0xff, sizeof(uint32_t) * hnv, al.s)) != cudaSuccess)
+      return fail(cuda_error(ce, "memset"));
   }
   // ---- full tree, then collapse ----
   Node *full = nullptr;
-  uint2 *ranges = nullptr, *pending = nullptr;
+  uint2 *ranges = nullptr;
   uint32_t *kept = nullptr, *rank = nullptr;
   if ((s = tmp.get(&full, 2ull * hnv)) != BQ_OK) return fail(s);
   if ((s = tmp.get(&ranges, hnv)) != BQ_OK) return fail(s);
   if ((s = tmp.get(&kept, hnv)) != BQ_OK) return fail(s);
   if ((s = tmp.get(&rank, hnv)) != BQ_OK) return fail(s);
-  if ((s = tmp.get(&pending, 2ull * div_up(hnv, AGG_CHUNK))) != BQ_OK) return fail(s);
   {
     ProfScope ps("rebin.agglomerate", al.s, 2);
     AggArgsT<uint16_t> ag{lev, slot, ids, boxes, full, nullptr, nvDev, ranges, pending, nullptr, 0};

@@ -340,7 +340,7 @@ int tri_closest(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, co
     BQ_TRY(tmp.get(&idx[1], nq));
     k_tri_keys<<<div_up(nq, 256), 256, 0, al.s>>>(nodes, queries, nq, keys[0], idx[0]);
     int sel = 0;
-    BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, 0, 30, nullptr, &sel, err, al));
+    BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, 6, 30, nullptr, &sel, err, al));  // order only: top 24 bits
     order = idx[sel];
   }
   const int b = c.blockSize;
