@@ -50,6 +50,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_POINTS)
     ap.add_argument("--no-components", action="store_true")
+    ap.add_argument("--only-queries", action="store_true",
+                    help="build one tree, then time closest-point and kNN(16) queries only (the short program "
+                         "the query ncu captures run)")
+    ap.add_argument("--queries", type=int, default=N_POINTS, help="query count for --only-queries")
     ap.add_argument("--only-build", action="store_true",
                     help="time the build loop only (no profile pass, e2e, components or CPU leg): "
                          "the short program the ncu captures run")
@@ -509,6 +513,20 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     sptr = ctypes.c_void_p(stream.cuda_stream)
     cb = CBuild(bq, boxes_t, n)
+
+    if args.only_queries:
+        bvh = bq.cuda.radixBuilder(boxes_t)
+        qs = torch.from_numpy(W.uniform_points(args.queries, W.SEED_QUERIES)).cuda()
+        ms_cp = time_loop(lambda: bq.points.findClosest(bvh, tp, qs), args.steps, args.warmup, world)
+        ms_knn = time_loop(lambda: bq.points.findKNN(bvh, tp, qs, 16), args.steps, args.warmup, world)
+        if rank == 0:
+            print(json.dumps({"only_queries": True, "points": n, "queries": args.queries, "closest_point_ms": ms_cp,
+                              "knn16_ms": ms_knn}))
+        bvh.free()
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
 
     props = torch.cuda.get_device_properties(local)
     uuid = str(getattr(props, "uuid", ""))

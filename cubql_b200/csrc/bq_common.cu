@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_reduce(const uint32_t *in, 
                                                             uint32_t *blockSums)
 {
   __shared__ uint32_t sh[8];
-  const uint32_t n = nDev ? *nDev : nMax;
+  const uint32_t n = nDev ? min(*nDev, nMax) : nMax;  // never past the buffers
   const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
   uint32_t s = 0;
 #pragma unroll
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_final(const uint32_t *in, u
                                                            const uint32_t *nDev, const uint32_t *blockOffsets)
 {
   __shared__ uint32_t sh[8];
-  const uint32_t n = nDev ? *nDev : nMax;
+  const uint32_t n = nDev ? min(*nDev, nMax) : nMax;  // never past the buffers
   const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
   uint32_t v[SCAN_ITEMS], s = 0;
 #pragma unroll

@@ -356,6 +356,50 @@ __global__ void __launch_bounds__(256) k_fix_runs(uint64_t *keys, uint32_t *ids,
     delta[i] = a != b ? key_level(a, b) : (uint8_t)63;  // equal: the midpoint of [i, i+2)
     return;
   }
+  const uint64_t k3 = i + 3 < nv ? keys[i + 3] : ~k0;
+  const uint64_t k4 = i + 4 < nv ? keys[i + 4] : ~k0;
+  if (key_hi(k4) != hi) {  // a run of three or four: kept in registers
+    const uint32_t size = key_hi(k3) == hi ? 4u : 3u;
+    uint64_t r[4] = {k0, k1, k2, size == 4 ? k3 : ~0ull};  // ~0: above every key, stays last
+    uint32_t d[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) d[j] = (uint32_t)j < size ? ids[i + j] : 0u;
+    bool moved = false;
+#pragma unroll
+    for (int pass = 0; pass < 3; pass++)  // bubble sort: swaps on > only, so stable
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+        if (r[j] > r[j + 1]) {
+          const uint64_t t = r[j]; r[j] = r[j + 1]; r[j + 1] = t;
+          const uint32_t u = d[j]; d[j] = d[j + 1]; d[j + 1] = u;
+          moved = true;
+        }
+    if (moved) {
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if ((uint32_t)j < size) {
+          keys[i + j] = r[j];
+          ids[i + j] = d[j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      if ((uint32_t)j + 1 >= size) break;
+      if (r[j] != r[j + 1]) {
+        delta[i + j] = key_level(r[j], r[j + 1]);
+      } else {
+        int e0 = j, e1 = j + 2;  // the run of keys equal to r[j] (constant indices only)
+#pragma unroll
+        for (int t = 2; t >= 0; t--)
+          if (t < j && e0 == t + 1 && r[t] == r[j]) e0 = t;
+#pragma unroll
+        for (int t = 2; t < 4; t++)
+          if (t >= j + 2 && e1 == t && (uint32_t)t < size && r[t] == r[j]) e1 = t + 1;
+        delta[i + j] = equal_run_level(i + e0, i + e1, (uint64_t)i + j + 1);
+      }
+    }
+    return;
+  }
   const uint32_t size = hi_run_end(keys, i, hi, nv) - i;
   if (size > MB_THREAD_RUN) {
     const uint32_t slotIdx = atomicAdd(&rs->count, 1u);

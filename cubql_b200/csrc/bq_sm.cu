@@ -18,13 +18,16 @@
 //     the end (children of the k-th used split at nodes 2+2k, 2+2k+1; node 1
 //     stays unused, as in the reference);
 //   * nodes with more than SM_WARP_MAX prims are split level by level over
-//     the whole GPU in tiles of SM_TILE prims: k_sm_count (right-side count
-//     per tile), one scan, k_sm_children, k_sm_scatter (stable scatter that
-//     also reduces the children's centroid bounds per tile and merges them
-//     with one atomicMin/Max per tile -- min/max is order-independent, so
-//     the result is deterministic);
+//     the whole GPU in tiles of SM_TILE prims: k_sm_tiles + one scan (tile
+//     offsets), k_sm_count (right-side count per tile), one scan,
+//     k_sm_children, k_sm_scatter (stable scatter that also reduces the
+//     children's centroid bounds per tile and merges them with one
+//     atomicMin/Max per tile -- min/max is order-independent, so the result
+//     is deterministic), k_sm_classify (children to the next level's list or
+//     to the warp tasks).  Lists and counts stay in device memory; the host
+//     reads the counters only every SM_LEVELS_PER_CHECK levels;
 //   * every subtree of at most SM_WARP_MAX prims is finished by one warp
-//     (k_sm_warp), depth first, smaller child first with the larger one on a
+//     of a persistent grid (k_sm_warp takes tasks from a counter), depth first, smaller child first with the larger one on a
 //     per-warp shared-memory stack; a node of up to 32 prims is held in
 //     registers, one prim per lane, and its whole subtree is partitioned
 //     with ballots and a 512-byte shared exchange buffer.
@@ -54,6 +57,7 @@ constexpr int SM_BLOCK = 256;           // global-level kernels
 constexpr int SMW_BLOCK = 128;          // warp-phase kernel
 constexpr int SMW_WARPS = SMW_BLOCK / 32;
 constexpr int SMW_STACK = 24;           // >= log2(SM_WARP_MAX) + 1
+constexpr int SM_LEVELS_PER_CHECK = 4;  // global levels between two host looks at the counters
 
 // A node still to be split: prim range [b, e) in buffer `parity`, its slot,
 // and its prims' centroid bounds (encoded, see enc_f).
@@ -192,12 +196,68 @@ __global__ void __launch_bounds__(256) k_sm_init(const bq_box3f *__restrict__ bo
 // ------------------------------------------------------------------
 // global levels (nodes with more than SM_WARP_MAX prims)
 // ------------------------------------------------------------------
-__global__ void __launch_bounds__(SM_BLOCK) k_sm_count(const SmNode *__restrict__ nodes, const SmTile *__restrict__ tiles,
-                                                       uint32_t numTiles, const float4 *__restrict__ buf0,
+// Device-side state of the global levels.  The big-node lists ping-pong
+// between two buffers; their counts, the current level's tile count and
+// the warp-phase task list live here, so levels run without the host.
+struct SmCtl {
+  uint32_t bigCount[2];  // nodes in big list 0 / 1
+  uint32_t numTiles;     // tiles of the current level (scan total)
+  uint32_t scanLen;      // numTiles + 1
+  uint32_t taskCount;    // subtrees waiting for the warp phase
+  uint32_t grab;         // warp-phase task counter
+  uint32_t err;          // DEV_ERR_RANGE on a broken capacity bound
+  uint32_t pad;
+};
+
+// tiles of a level: node k owns tiles [first[k], first[k+1]) (last: numTiles)
+struct SmTileInfo {
+  uint32_t node, begin, end;
+};
+__device__ __forceinline__ uint32_t first_end(const uint32_t *__restrict__ first, uint32_t K, uint32_t T, uint32_t k)
+{
+  return k + 1 < K ? first[k + 1] : T;
+}
+__device__ __forceinline__ SmTileInfo tile_info(const SmNode *__restrict__ nodes, const uint32_t *__restrict__ first,
+                                                uint32_t K, uint32_t t)
+{
+  uint32_t lo = 0, hi = K;  // last node whose first tile is <= t
+  while (hi - lo > 1) {
+    const uint32_t m = (lo + hi) >> 1;
+    if (first[m] <= t) lo = m; else hi = m;
+  }
+  SmTileInfo r;
+  r.node = lo;
+  r.begin = nodes[lo].b + (t - first[lo]) * SM_TILE;
+  r.end = min(nodes[lo].e, r.begin + SM_TILE);
+  return r;
+}
+
+// tiles per big node of the current list
+__global__ void k_sm_tiles(const SmNode *__restrict__ nodes, SmCtl *ctl, int cur, uint32_t cap,
+                           uint32_t *__restrict__ tileCount)
+{
+  const uint32_t K = ctl->bigCount[cur];
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k == 0 && K > cap) atomicOr(&ctl->err, DEV_ERR_RANGE);
+  if (k >= K || k >= cap) return;
+  tileCount[k] = (nodes[k].e - nodes[k].b + SM_TILE - 1) / SM_TILE;
+}
+
+// grid: maxTiles blocks; blocks past the level's tile count leave at once
+__global__ void __launch_bounds__(SM_BLOCK) k_sm_count(const SmNode *__restrict__ nodes,
+                                                       const uint32_t *__restrict__ first, SmCtl *ctl, int cur,
+                                                       uint32_t maxTiles, const float4 *__restrict__ buf0,
                                                        const float4 *__restrict__ buf1, uint32_t *__restrict__ tileRight)
 {
   __shared__ uint32_t sCnt[SM_BLOCK / 32];
-  const SmTile t = tiles[blockIdx.x];
+  const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (T >= maxTiles) atomicOr(&ctl->err, DEV_ERR_RANGE);
+    else tileRight[T] = 0;  // the scan's total slot
+    ctl->scanLen = min(T, maxTiles - 1) + 1;
+  }
+  if (blockIdx.x >= T || blockIdx.x >= maxTiles - 1) return;  // whole block
+  const SmTileInfo t = tile_info(nodes, first, K, blockIdx.x);
   const SmNode nd = nodes[t.node];
   const SmSplit sp = choose_split(nd);
   const float4 *src = nd.parity ? buf1 : buf0;
@@ -211,20 +271,20 @@ __global__ void __launch_bounds__(SM_BLOCK) k_sm_count(const SmNode *__restrict_
     uint32_t s = 0;
     for (int w = 0; w < SM_BLOCK / 32; w++) s += sCnt[w];
     tileRight[blockIdx.x] = s;
-    if (blockIdx.x == 0) tileRight[numTiles] = 0;  // the scan's total slot
   }
 }
 
 // per node: the split position, the internal node, the two child records
 // (bounds start empty; k_sm_scatter fills them)
-__global__ void k_sm_children(const SmNode *__restrict__ nodes, uint32_t K, const uint32_t *__restrict__ firstTile,
-                              const uint32_t *__restrict__ rightScan, Node *__restrict__ out,
-                              uint32_t *__restrict__ used, SmNode *__restrict__ next)
+__global__ void k_sm_children(const SmNode *__restrict__ nodes, const SmCtl *ctl, int cur, uint32_t cap,
+                              const uint32_t *__restrict__ first, const uint32_t *__restrict__ rightScan,
+                              Node *__restrict__ out, uint32_t *__restrict__ used, SmNode *__restrict__ next)
 {
+  const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= K) return;
+  if (k >= K || k >= cap) return;
   const SmNode nd = nodes[k];
-  const uint32_t nR = rightScan[firstTile[k + 1]] - rightScan[firstTile[k]];
+  const uint32_t nR = rightScan[first_end(first, K, T, k)] - rightScan[first[k]];
   const uint32_t m = nd.e - nR;  // left child is [b, m)
   internal_node(out, used, nd.slot, m);
   SideBounds sb;
@@ -236,20 +296,22 @@ __global__ void k_sm_children(const SmNode *__restrict__ nodes, uint32_t K, cons
 }
 
 __global__ void __launch_bounds__(SM_BLOCK) k_sm_scatter(const SmNode *__restrict__ nodes,
-                                                         const SmTile *__restrict__ tiles,
-                                                         const uint32_t *__restrict__ firstTile,
+                                                         const uint32_t *__restrict__ first, const SmCtl *ctl,
+                                                         int cur, uint32_t maxTiles,
                                                          const uint32_t *__restrict__ rightScan, float4 *buf0,
                                                          float4 *buf1, SmNode *next)
 {
   __shared__ uint32_t sWarp[SM_BLOCK / 32];
   __shared__ int32_t sRed[12][SM_BLOCK / 32];
-  const SmTile t = tiles[blockIdx.x];
+  const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
+  if (blockIdx.x >= T || blockIdx.x >= maxTiles - 1) return;  // whole block
+  const SmTileInfo t = tile_info(nodes, first, K, blockIdx.x);
   const SmNode nd = nodes[t.node];
   const SmSplit sp = choose_split(nd);
   const float4 *src = nd.parity ? buf1 : buf0;
   float4 *dst = nd.parity ? buf0 : buf1;
-  const uint32_t nodeRight0 = rightScan[firstTile[t.node]];
-  const uint32_t m = nd.e - (rightScan[firstTile[t.node + 1]] - nodeRight0);
+  const uint32_t nodeRight0 = rightScan[first[t.node]];
+  const uint32_t m = nd.e - (rightScan[first_end(first, K, T, t.node)] - nodeRight0);
   uint32_t rBefore = rightScan[blockIdx.x] - nodeRight0;  // this node's rights before the tile
   uint32_t lBefore = (t.begin - nd.b) - rBefore;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -371,21 +433,15 @@ __device__ void sm_small_subtree(const SmNode &root, const float4 *src, int thr,
   __syncwarp();
 }
 
-// one warp per task; grid = div_up(numTasks * 32, SMW_BLOCK)
-__global__ void __launch_bounds__(SMW_BLOCK) k_sm_warp(const SmNode *__restrict__ tasks, uint32_t numTasks, int thr,
-                                                       float4 *buf0, float4 *buf1, Node *__restrict__ out,
-                                                       uint32_t *__restrict__ primIDs, uint32_t *__restrict__ used,
-                                                       uint32_t *err)
+// one subtree of at most SM_WARP_MAX prims, by the calling warp; stk and
+// xbuf are the warp's shared-memory stack and exchange buffer
+__device__ void sm_warp_task(SmNode cur, int thr, float4 *buf0, float4 *buf1, Node *__restrict__ out,
+                             uint32_t *__restrict__ primIDs, uint32_t *__restrict__ used, uint32_t *err, SmNode *stk,
+                             float4 *xbuf)
 {
-  __shared__ SmNode sStack[SMW_WARPS][SMW_STACK];
-  __shared__ float4 sX[SMW_WARPS][32];
-  const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= numTasks) return;  // whole warps leave together
-  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
-  SmNode *stk = sStack[wb];
   int sp = 0;
-  SmNode cur = tasks[w];
   while (true) {
     const uint32_t count = cur.e - cur.b;
     const float4 *src = cur.parity ? buf1 : buf0;
@@ -395,7 +451,7 @@ __global__ void __launch_bounds__(SMW_BLOCK) k_sm_warp(const SmNode *__restrict_
         for (uint32_t i = cur.b + lane; i < cur.e; i += 32) primIDs[i] = __float_as_uint(src[i].w);
         if (lane == 0) leaf_node(out, cur.slot, cur.b, count);
       } else {
-        sm_small_subtree(cur, src, thr, sX[wb], stk + sp, SMW_STACK - sp, out, primIDs, used, err);
+        sm_small_subtree(cur, src, thr, xbuf, stk + sp, SMW_STACK - sp, out, primIDs, used, err);
       }
       if (sp == 0) return;
       __syncwarp();
@@ -449,6 +505,45 @@ __global__ void __launch_bounds__(SMW_BLOCK) k_sm_warp(const SmNode *__restrict_
     sp++;
     cur = leftSmaller ? c0 : c1;
     __syncwarp();  // this warp's scatter is visible to its own next pass
+  }
+}
+
+// persistent grid: each warp takes the next waiting subtree until none is left
+__global__ void __launch_bounds__(SMW_BLOCK) k_sm_warp(const SmNode *__restrict__ tasks, SmCtl *ctl, uint32_t taskCap,
+                                                       int thr, float4 *buf0, float4 *buf1, Node *__restrict__ out,
+                                                       uint32_t *__restrict__ primIDs, uint32_t *__restrict__ used)
+{
+  __shared__ SmNode sStack[SMW_WARPS][SMW_STACK];
+  __shared__ float4 sX[SMW_WARPS][32];
+  const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+  const uint32_t numTasks = min(ctl->taskCount, taskCap);
+  while (true) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(&ctl->grab, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= numTasks) return;  // whole warp
+    sm_warp_task(tasks[t], thr, buf0, buf1, out, primIDs, used, &ctl->err, sStack[wb], sX[wb]);
+    __syncwarp();
+  }
+}
+
+// children of the level's big nodes: to the next big list or to the tasks
+__global__ void k_sm_classify(const SmNode *__restrict__ next, SmCtl *ctl, int cur, uint32_t cap, int thr,
+                              SmNode *__restrict__ bigNext, SmNode *__restrict__ tasks, uint32_t taskCap)
+{
+  const uint32_t K = min(ctl->bigCount[cur], cap);
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= 2 * K) return;
+  const SmNode c = next[j];
+  const uint32_t size = c.e - c.b;
+  if (size > SM_WARP_MAX && (int64_t)size > thr) {
+    const uint32_t at = atomicAdd(&ctl->bigCount[cur ^ 1], 1u);
+    if (at < cap) bigNext[at] = c;
+    else atomicOr(&ctl->err, DEV_ERR_RANGE);  // cannot happen: big nodes are disjoint and above SM_WARP_MAX
+  } else {
+    const uint32_t at = atomicAdd(&ctl->taskCount, 1u);
+    if (at < taskCap) tasks[at] = c;
+    else atomicOr(&ctl->err, DEV_ERR_RANGE);  // the host flushes the tasks before this can happen
   }
 }
 
@@ -529,85 +624,73 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   Node *full = nullptr;
   if ((s = tmp.get(&full, 2ull * nv)) != BQ_OK) return fail(s);
 
-  // ---- global levels ----
-  std::vector<SmNode> level(1), tasks;
-  level[0].b = 0; level[0].e = nv; level[0].slot = 0; level[0].parity = 0;
-  for (int d = 0; d < 3; d++) { level[0].lo[d] = hctl[2 + d]; level[0].hi[d] = hctl[5 + d]; }
-  TempSet lvlTmp(al);
-  uint8_t *dLevel = nullptr;  // [K SmNode][K+1 first tile][T SmTile], 16-byte aligned parts
-  SmNode *dNext = nullptr;
-  uint32_t *dRight = nullptr;
-  size_t capBytes = 0, capNext = 0, capRight = 0;
-  std::vector<uint8_t> hLevel;
-  while (true) {
-    std::vector<SmNode> big;
-    for (const SmNode &nd : level) {
-      const uint32_t c = nd.e - nd.b;
-      if (c > SM_WARP_MAX && (int64_t)c > thr) big.push_back(nd);
-      else tasks.push_back(nd);
-    }
-    if (big.empty()) break;
-    const uint32_t K = (uint32_t)big.size();
-    std::vector<uint32_t> first(K + 1);
-    std::vector<SmTile> tiles;
-    for (uint32_t k = 0; k < K; k++) {
-      first[k] = (uint32_t)tiles.size();
-      for (uint64_t b0 = big[k].b; b0 < big[k].e; b0 += SM_TILE)
-        tiles.push_back(SmTile{k, (uint32_t)b0, (uint32_t)std::min<uint64_t>(big[k].e, b0 + SM_TILE)});
-    }
-    first[K] = (uint32_t)tiles.size();
-    const uint32_t T = (uint32_t)tiles.size();
-    const size_t offFirst = ((sizeof(SmNode) * K + 15) / 16) * 16;
-    const size_t offTiles = offFirst + ((sizeof(uint32_t) * (K + 1) + 15) / 16) * 16;
-    const size_t bytes = offTiles + sizeof(SmTile) * T;
-    if (bytes > capBytes) {
-      capBytes = std::max(bytes, 2 * capBytes);
-      if ((s = lvlTmp.get(&dLevel, capBytes)) != BQ_OK) return fail(s);
-    }
-    if (2ull * K > capNext) {
-      capNext = std::max<size_t>(2ull * K, 2 * capNext);
-      if ((s = lvlTmp.get(&dNext, capNext)) != BQ_OK) return fail(s);
-    }
-    if (T + 1ull > capRight) {
-      capRight = std::max<size_t>(T + 1ull, 2 * capRight);
-      if ((s = lvlTmp.get(&dRight, capRight)) != BQ_OK) return fail(s);
-    }
-    hLevel.resize(bytes);
-    std::memcpy(hLevel.data(), big.data(), sizeof(SmNode) * K);
-    std::memcpy(hLevel.data() + offFirst, first.data(), sizeof(uint32_t) * (K + 1));
-    std::memcpy(hLevel.data() + offTiles, tiles.data(), sizeof(SmTile) * T);
-    const SmNode *dNodes = reinterpret_cast<const SmNode *>(dLevel);
-    const uint32_t *dFirst = reinterpret_cast<const uint32_t *>(dLevel + offFirst);
-    const SmTile *dTiles = reinterpret_cast<const SmTile *>(dLevel + offTiles);
+  // ---- global levels, driven from device memory ----
+  // Big nodes (more than SM_WARP_MAX prims) of one level are disjoint, so a
+  // level holds at most cap of them and at most maxTiles tiles.  The host
+  // looks at the counters only every SM_LEVELS_PER_CHECK levels; a level
+  // with no big node left costs only its (empty) launches.
+  const uint32_t cap = nv / (SM_WARP_MAX + 1) + 1;
+  const uint32_t maxTiles = nv / SM_TILE + cap + 2;
+  const uint32_t taskCap = std::max<uint32_t>(16 * cap, 4096) + 2 * SM_LEVELS_PER_CHECK * cap;
+  SmCtl *sc = nullptr;
+  SmNode *bigList[2] = {nullptr, nullptr}, *next = nullptr, *tasks = nullptr;
+  uint32_t *tileCount = nullptr, *first = nullptr, *tileRight = nullptr;
+  if ((s = tmp.get(&sc, 1)) != BQ_OK || (s = tmp.get(&bigList[0], cap)) != BQ_OK ||
+      (s = tmp.get(&bigList[1], cap)) != BQ_OK || (s = tmp.get(&next, 2ull * cap)) != BQ_OK ||
+      (s = tmp.get(&tasks, taskCap)) != BQ_OK || (s = tmp.get(&tileCount, cap)) != BQ_OK ||
+      (s = tmp.get(&first, cap)) != BQ_OK || (s = tmp.get(&tileRight, maxTiles)) != BQ_OK)
+    return fail(s);
+  SmNode root;
+  root.b = 0; root.e = nv; root.slot = 0; root.parity = 0;
+  for (int d = 0; d < 3; d++) { root.lo[d] = hctl[2 + d]; root.hi[d] = hctl[5 + d]; }
+  const bool rootBig = nv > SM_WARP_MAX && (int64_t)nv > thr;
+  SmCtl hsc{};
+  hsc.bigCount[0] = rootBig ? 1u : 0u;
+  hsc.taskCount = rootBig ? 0u : 1u;
+  if ((ce = cudaMemcpyAsync(rootBig ? bigList[0] : tasks, &root, sizeof(root), cudaMemcpyHostToDevice, al.s)) !=
+          cudaSuccess ||
+      (ce = cudaMemcpyAsync(sc, &hsc, sizeof(hsc), cudaMemcpyHostToDevice, al.s)) != cudaSuccess)
+    return fail(cuda_error(ce, "spatial median set-up"));
+  const int warpGrid = num_sms() * 8;
+  auto warp_phase = [&]() -> int {  // every waiting subtree, then an empty task list
+    ProfScope ps("sm.warps", al.s);
+    k_sm_warp<<<warpGrid, SMW_BLOCK, 0, al.s>>>(tasks, sc, taskCap, thr, buf0, buf1, full, primIDs, used);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemsetAsync(&sc->taskCount, 0, 2 * sizeof(uint32_t), al.s);  // taskCount, grab
+    return e == cudaSuccess ? BQ_OK : cuda_error(e, "k_sm_warp");
+  };
+  int cur = 0;
+  for (int level = 0; rootBig; level++) {
     {
-      ProfScope ps("sm.level", al.s, 6);
-      if ((ce = cudaMemcpyAsync(dLevel, hLevel.data(), bytes, cudaMemcpyHostToDevice, al.s)) != cudaSuccess)
-        return fail(cuda_error(ce, "upload level"));
-      k_sm_count<<<T, SM_BLOCK, 0, al.s>>>(dNodes, dTiles, T, buf0, buf1, dRight);
-      if ((s = exclusive_scan_u32(dRight, dRight, T + 1, nullptr, nullptr, al)) != BQ_OK) return fail(s);
-      k_sm_children<<<div_up(K, 128), 128, 0, al.s>>>(dNodes, K, dFirst, dRight, full, used, dNext);
-      k_sm_scatter<<<T, SM_BLOCK, 0, al.s>>>(dNodes, dTiles, dFirst, dRight, buf0, buf1, dNext);
-      if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "spatial median level"));
+      ProfScope ps("sm.level", al.s, 11);
+      k_sm_tiles<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, tileCount);
+      if ((s = exclusive_scan_u32(tileCount, first, cap, &sc->bigCount[cur], &sc->numTiles, al)) != BQ_OK)
+        return fail(s);
+      k_sm_count<<<maxTiles, SM_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, buf0, buf1, tileRight);
+      if ((s = exclusive_scan_u32(tileRight, tileRight, maxTiles, &sc->scanLen, nullptr, al)) != BQ_OK)
+        return fail(s);
+      k_sm_children<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, first, tileRight, full, used,
+                                                       next);
+      k_sm_scatter<<<maxTiles, SM_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, tileRight, buf0, buf1,
+                                                     next);
+      k_sm_classify<<<div_up(2ull * cap, 128), 128, 0, al.s>>>(next, sc, cur, cap, thr, bigList[cur ^ 1], tasks,
+                                                               taskCap);
+      if ((ce = cudaMemsetAsync(&sc->bigCount[cur], 0, sizeof(uint32_t), al.s)) != cudaSuccess ||
+          (ce = cudaGetLastError()) != cudaSuccess)
+        return fail(cuda_error(ce, "spatial median level"));
     }
-    level.resize(2ull * K);
-    if ((ce = cudaMemcpyAsync(level.data(), dNext, sizeof(SmNode) * 2 * K, cudaMemcpyDeviceToHost, al.s)) !=
-            cudaSuccess ||
+    cur ^= 1;
+    if ((level + 1) % SM_LEVELS_PER_CHECK) continue;
+    if ((ce = cudaMemcpyAsync(&hsc, sc, sizeof(hsc), cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
         (ce = cudaStreamSynchronize(al.s)) != cudaSuccess)
-      return fail(cuda_error(ce, "download level"));
+      return fail(cuda_error(ce, "spatial median levels"));
+    if (hsc.err) return fail(set_error(BQ_ERR_CUDA, "spatial-median level failed a capacity check"));
+    if (hsc.bigCount[cur] == 0) break;
+    // the next SM_LEVELS_PER_CHECK levels add at most 2 * cap tasks each
+    if (hsc.taskCount + 2ull * SM_LEVELS_PER_CHECK * cap > taskCap && (s = warp_phase()) != BQ_OK) return fail(s);
   }
   // ---- warp phase ----
-  {
-    SmNode *dTasks = nullptr;
-    if ((s = tmp.get(&dTasks, tasks.size())) != BQ_OK) return fail(s);
-    if ((ce = cudaMemcpyAsync(dTasks, tasks.data(), sizeof(SmNode) * tasks.size(), cudaMemcpyHostToDevice, al.s)) !=
-        cudaSuccess)
-      return fail(cuda_error(ce, "upload tasks"));
-    ProfScope ps("sm.warps", al.s);
-    const uint32_t nt = (uint32_t)tasks.size();
-    k_sm_warp<<<div_up((long long)nt * 32, SMW_BLOCK), SMW_BLOCK, 0, al.s>>>(dTasks, nt, thr, buf0, buf1, full,
-                                                                              primIDs, used, ctl + 1);
-    if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_sm_warp"));
-  }
+  if ((s = warp_phase()) != BQ_OK) return fail(s);
   // ---- slot compaction ----
   uint32_t *rank = nullptr;
   if ((s = tmp.get(&rank, nv)) != BQ_OK) return fail(s);
@@ -615,11 +698,12 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     ProfScope ps("sm.rank", al.s, 3);
     if ((s = exclusive_scan_u32(used, rank, nv, nullptr, ctl + 2, al)) != BQ_OK) return fail(s);
   }
-  uint32_t hres[2];
+  uint32_t hres[2], herr = 0;
   if ((ce = cudaMemcpyAsync(hres, ctl + 1, 8, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
+      (ce = cudaMemcpyAsync(&herr, &sc->err, 4, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
       (ce = cudaStreamSynchronize(al.s)) != cudaSuccess)
     return fail(cuda_error(ce, "spatial median"));
-  if (hres[0]) return fail(set_error(BQ_ERR_CUDA, "spatial-median warp phase failed a range check"));
+  if (hres[0] || herr) return fail(set_error(BQ_ERR_CUDA, "spatial-median build failed a range or capacity check"));
   const uint32_t numNodes = 2 + 2 * hres[1];
   Node *nodes = nullptr;
   if ((s = al.get(&nodes, numNodes)) != BQ_OK) return fail(s);
