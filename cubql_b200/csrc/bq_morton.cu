@@ -317,32 +317,20 @@ __device__ __forceinline__ uint8_t equal_run_level(uint64_t r0, uint64_t r1, uin
   return (uint8_t)(63 - depth);
 }
 
-// One thread per sorted position i (keys sorted on bits [MB_SORT_BEGIN, 63)
-// only):
-//   * initialises the agglomeration slot of i;
-//   * writes the split level of the pair (i, i+1) when the two lie in
-//     different runs of equal top bits -- their highest differing bit is in
-//     the top bits, so the order inside the runs does not change it;
-//   * the first thread of a run of up to MB_THREAD_RUN prims orders the run
-//     on the low bits (stable insertion sort) and writes the levels of the
-//     pairs inside it; longer runs are listed for a segmented sort (their
-//     inner levels are written by k_delta afterwards).
-__global__ void __launch_bounds__(256) k_fix_runs(uint64_t *keys, uint32_t *ids, const uint32_t *nvPtr,
-                                                  uint8_t *__restrict__ delta, uint32_t *__restrict__ slot,
-                                                  RunStats *rs, uint4 *runs, uint32_t maxRuns)
+// The first position i of a run of at least two prims with equal top bits
+// (keys sorted on bits [MB_SORT_BEGIN, 63) only): orders the run on the low
+// bits (stable) and writes the levels of the pairs inside it.  Runs of up
+// to MB_THREAD_RUN prims are done here; longer ones are listed for a
+// segmented sort (their inner levels are written by k_delta afterwards).
+__device__ __forceinline__ void fix_run_at(uint32_t i, uint32_t nv, uint64_t *keys, uint32_t *ids,
+                                           uint8_t *__restrict__ delta, RunStats *rs, uint4 *runs, uint32_t maxRuns)
 {
-  const uint32_t nv = *nvPtr;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nv) return;
-  slot[i] = SLOT_EMPTY;
-  // the four neighbouring keys are independent loads (no dependent chain in
-  // the common cases: runs of one and of two)
+  // the neighbouring keys are independent loads
   const uint64_t k0 = keys[i];
   const uint64_t km = i > 0 ? keys[i - 1] : ~k0;
   const uint64_t k1 = i + 1 < nv ? keys[i + 1] : ~k0;
   const uint64_t k2 = i + 2 < nv ? keys[i + 2] : ~k0;
   const uint32_t hi = key_hi(k0);
-  if (i + 1 < nv && key_hi(k1) != hi) delta[i] = key_level(k0, k1);  // pair across two runs
   if (key_hi(km) == hi) return;  // not the first of its run
   if (key_hi(k1) != hi) return;  // a run of one
   if (key_hi(k2) != hi) {        // a run of two
@@ -447,6 +435,45 @@ __global__ void __launch_bounds__(256) k_fix_runs(uint64_t *keys, uint32_t *ids,
       delta[i + j] = equal_run_level(i + e0, i + e1, (uint64_t)i + j + 1);
     }
   }
+}
+
+// Every sorted position: its agglomeration slot, and the split level of
+// the pair (i, i+1) when the two lie in different runs of equal top bits
+// (their highest differing bit is in the top bits, so the order inside the
+// runs does not change it).  Each warp covers FR_ITEMS * 32 consecutive
+// positions, collects the run starts among them in shared memory and then
+// hands one run to each lane, so the run work is not left to a few lanes
+// of a mostly idle warp.
+constexpr int FR_BLOCK = 256;
+constexpr int FR_ITEMS = 4;
+__global__ void __launch_bounds__(FR_BLOCK) k_fix_runs(uint64_t *keys, uint32_t *ids, const uint32_t *nvPtr,
+                                                       uint8_t *__restrict__ delta, uint32_t *__restrict__ slot,
+                                                       RunStats *rs, uint4 *runs, uint32_t maxRuns)
+{
+  __shared__ uint32_t sStarts[FR_BLOCK / 32][FR_ITEMS * 32];
+  const uint32_t nv = *nvPtr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t warpBase = ((uint64_t)blockIdx.x * (FR_BLOCK / 32) + warp) * (FR_ITEMS * 32);
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t numStarts = 0;
+#pragma unroll
+  for (int u = 0; u < FR_ITEMS; u++) {
+    const uint64_t i = warpBase + (uint64_t)u * 32 + lane;
+    bool start = false;
+    if (i < nv) {
+      slot[i] = SLOT_EMPTY;
+      const uint64_t k0 = keys[i];
+      const uint32_t hi = key_hi(k0);
+      const bool nextSame = i + 1 < nv && key_hi(keys[i + 1]) == hi;
+      if (i + 1 < nv && !nextSame) delta[i] = key_level(k0, keys[i + 1]);  // pair across two runs
+      start = nextSame && (i == 0 || key_hi(keys[i - 1]) != hi);
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, start);
+    if (start) sStarts[warp][numStarts + __popc(bal & lt)] = (uint32_t)i;
+    numStarts += __popc(bal);
+  }
+  __syncwarp();
+  for (uint32_t k = lane; k < numStarts; k += 32) fix_run_at(sStarts[warp][k], nv, keys, ids, delta, rs, runs, maxRuns);
 }
 
 __global__ void k_run_sizes(const uint4 *__restrict__ runs, uint32_t numRuns, uint32_t *__restrict__ sizes)
@@ -598,7 +625,8 @@ int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *
   BQ_CUDA(cudaMemsetAsync(rs, 0, sizeof(RunStats), al.s));
   {
     ProfScope ps("morton.runs", al.s);
-    k_fix_runs<<<div_up(n, 256), 256, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs, maxRuns);
+    k_fix_runs<<<div_up(n, FR_BLOCK * FR_ITEMS), FR_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs,
+                                                                     maxRuns);
   }
   RunStats h{};
   BQ_CUDA(cudaMemcpyAsync(&h, rs, sizeof(h), cudaMemcpyDeviceToHost, al.s));

@@ -304,17 +304,11 @@ __global__ void k_rb_detect(const uint16_t *__restrict__ lev, const uint32_t *nv
   if (run_size_at(lev, i, nv, bigMin) > bigMin) atomicAdd(numBig, 1u);
 }
 
-// one thread per run start; runs of thr < size <= 32 (the broad phase has
-// left no larger unresolved run)
-__global__ void __launch_bounds__(128) k_rb_thread(const uint32_t *nvPtr, int thr, const bq_box3f *__restrict__ boxes,
-                                                   uint32_t *__restrict__ ids, uint16_t *__restrict__ lev,
-                                                   uint8_t *__restrict__ forced, uint32_t *numForced)
+// the run [start, start + size) of thr < size <= 32 prims, by one thread
+__device__ void rb_thread_run(uint32_t start, uint32_t size, int thr, const bq_box3f *__restrict__ boxes,
+                              uint32_t *__restrict__ ids, uint16_t *__restrict__ lev, uint8_t *__restrict__ forced,
+                              uint32_t *numForced)
 {
-  const uint32_t nv = *nvPtr;
-  const uint32_t start = blockIdx.x * blockDim.x + threadIdx.x;
-  if (start >= nv) return;
-  const uint32_t size = run_size_at(lev, start, nv, REBIN_THREAD_MAX);
-  if ((int64_t)size <= thr || size > (uint32_t)REBIN_THREAD_MAX) return;
   if (size == 2) {
     // the common case (pairs of identical or near prims): the steps below
     // for two prims, each centroid read once
@@ -390,6 +384,53 @@ __global__ void __launch_bounds__(128) k_rb_thread(const uint32_t *nvPtr, int th
     stack[sp++] = Item{(uint8_t)b, (uint8_t)sp2, (uint8_t)(it.depth + 1)};
   }
   for (uint32_t i = 0; i < size; i++) ids[start + i] = id[i];
+}
+
+// The thread phase runs as two kernels: the levels are read to find the
+// runs before any run writes its new levels (a finder that ran beside the
+// run work could mistake a half-written run for a new one).
+// k_rb_find_runs: each warp looks at RT_ITEMS * 32 consecutive positions
+// and appends the runs of thr < size <= 32 prims that start there (one
+// atomic per warp); k_rb_thread then gives one listed run to each thread.
+constexpr int RT_BLOCK = 128;
+constexpr int RT_ITEMS = 4;
+__global__ void __launch_bounds__(RT_BLOCK) k_rb_find_runs(const uint32_t *nvPtr, int thr,
+                                                           const uint16_t *__restrict__ lev, uint2 *__restrict__ list,
+                                                           uint32_t *listCount)
+{
+  const uint32_t nv = *nvPtr;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t warpBase = ((uint64_t)blockIdx.x * (RT_BLOCK / 32) + warp) * (RT_ITEMS * 32);
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t size[RT_ITEMS], bal[RT_ITEMS], total = 0;
+#pragma unroll
+  for (int u = 0; u < RT_ITEMS; u++) {
+    const uint64_t i = warpBase + (uint64_t)u * 32 + lane;
+    size[u] = i < nv ? run_size_at(lev, (uint32_t)i, nv, REBIN_THREAD_MAX) : 0u;
+    const bool mine = (int64_t)size[u] > thr && size[u] <= (uint32_t)REBIN_THREAD_MAX;
+    bal[u] = __ballot_sync(0xffffffffu, mine);
+    total += __popc(bal[u]);
+  }
+  if (total == 0) return;  // whole warp
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(listCount, total);
+  base = __shfl_sync(0xffffffffu, base, 0);
+#pragma unroll
+  for (int u = 0; u < RT_ITEMS; u++) {
+    if ((bal[u] >> lane) & 1u) list[base + __popc(bal[u] & lt)] = make_uint2((uint32_t)(warpBase + u * 32 + lane), size[u]);
+    base += __popc(bal[u]);
+  }
+}
+
+__global__ void __launch_bounds__(RT_BLOCK) k_rb_thread(const uint2 *__restrict__ list, const uint32_t *listCount,
+                                                        uint32_t listCap, int thr, const bq_box3f *__restrict__ boxes,
+                                                        uint32_t *__restrict__ ids, uint16_t *__restrict__ lev,
+                                                        uint8_t *__restrict__ forced, uint32_t *numForced)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= min(*listCount, listCap)) return;
+  const uint2 r = list[t];
+  rb_thread_run(r.x, r.y, thr, boxes, ids, lev, forced, numForced);
 }
 
 // ------------------------------------------------------------------
@@ -475,6 +516,7 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   BQ_TRY(tmp.get(&valid, n));
   BQ_TRY(tmp.get(&vpos, n));
   BQ_TRY(tmp.get(&ctl, 16));  // [0] nv [1] err [2..7] bounds [8] runs [9] jobs [10] job prims [11] thread leaves
+                              // [12] thread-phase runs
   BQ_TRY(tmp.get(&keysA, n));
   BQ_TRY(tmp.get(&keysB, n));
   BQ_TRY(tmp.get(&idsB, n));
@@ -593,8 +635,15 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   // ---- thread phase ----
   if ((ce = cudaMemsetAsync(ctl + 11, 0, 4, al.s)) != cudaSuccess) return fail(cuda_error(ce, "memset"));
   if (thr < REBIN_THREAD_MAX) {
-    ProfScope ps("rebin.thread", al.s);
-    k_rb_thread<<<div_up(hnv, 128), 128, 0, al.s>>>(nvDev, thr, boxes, ids, lev, forced, ctl + 11);
+    ProfScope ps("rebin.thread", al.s, 2);
+    // runs of at least two prims: at most hnv / 2 of them
+    const uint32_t listCap = hnv / 2 + 1;
+    uint2 *list = nullptr;
+    if ((s = tmp.get(&list, listCap)) != BQ_OK) return fail(s);
+    if ((ce = cudaMemsetAsync(ctl + 12, 0, 4, al.s)) != cudaSuccess) return fail(cuda_error(ce, "memset"));
+    k_rb_find_runs<<<div_up(hnv, RT_BLOCK * RT_ITEMS), RT_BLOCK, 0, al.s>>>(nvDev, thr, lev, list, ctl + 12);
+    k_rb_thread<<<div_up(listCap, RT_BLOCK), RT_BLOCK, 0, al.s>>>(list, ctl + 12, listCap, thr, boxes, ids, lev,
+                                                                 forced, ctl + 11);
   }
   uint2 *pending = nullptr;
   if ((s = tmp.get(&pending, 2ull * div_up(hnv, AGG_CHUNK))) != BQ_OK) return fail(s);

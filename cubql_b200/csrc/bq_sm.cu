@@ -57,7 +57,7 @@ constexpr int SM_BLOCK = 256;           // global-level kernels
 constexpr int SMW_BLOCK = 128;          // warp-phase kernel
 constexpr int SMW_WARPS = SMW_BLOCK / 32;
 constexpr int SMW_STACK = 24;           // >= log2(SM_WARP_MAX) + 1
-constexpr int SM_LEVELS_PER_CHECK = 4;  // global levels between two host looks at the counters
+constexpr int SM_LEVELS_PER_CHECK = 2;  // global levels between two host looks at the counters
 
 // A node still to be split: prim range [b, e) in buffer `parity`, its slot,
 // and its prims' centroid bounds (encoded, see enc_f).
@@ -627,11 +627,16 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   // ---- global levels, driven from device memory ----
   // Big nodes (more than SM_WARP_MAX prims) of one level are disjoint, so a
   // level holds at most cap of them and at most maxTiles tiles.  The host
-  // looks at the counters only every SM_LEVELS_PER_CHECK levels; a level
-  // with no big node left costs only its (empty) launches.
+  // looks at the counters first when perfectly balanced splits would be
+  // done, then every SM_LEVELS_PER_CHECK levels; a level with no big node
+  // left costs only its (empty) launches.  Every level adds at most 2 * cap
+  // warp tasks, which bounds the task list between two looks.
   const uint32_t cap = nv / (SM_WARP_MAX + 1) + 1;
   const uint32_t maxTiles = nv / SM_TILE + cap + 2;
-  const uint32_t taskCap = std::max<uint32_t>(16 * cap, 4096) + 2 * SM_LEVELS_PER_CHECK * cap;
+  int nextCheck = 1;
+  while (nextCheck < 62 && ((uint64_t)SM_WARP_MAX << nextCheck) < nv) nextCheck++;
+  const uint32_t taskCap =
+      std::max<uint32_t>(16 * cap, 4096) + 2 * cap * (uint32_t)std::max(nextCheck, SM_LEVELS_PER_CHECK);
   SmCtl *sc = nullptr;
   SmNode *bigList[2] = {nullptr, nullptr}, *next = nullptr, *tasks = nullptr;
   uint32_t *tileCount = nullptr, *first = nullptr, *tileRight = nullptr;
@@ -680,7 +685,8 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
         return fail(cuda_error(ce, "spatial median level"));
     }
     cur ^= 1;
-    if ((level + 1) % SM_LEVELS_PER_CHECK) continue;
+    if (level + 1 < nextCheck) continue;
+    nextCheck = level + 1 + SM_LEVELS_PER_CHECK;
     if ((ce = cudaMemcpyAsync(&hsc, sc, sizeof(hsc), cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
         (ce = cudaStreamSynchronize(al.s)) != cudaSuccess)
       return fail(cuda_error(ce, "spatial median levels"));
