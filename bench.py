@@ -301,6 +301,18 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
         bq.points.findKNN(bvh, tp, qs, 16)
     comp["query_phases_ms"] = {k: round(v[1], 4) for k, v in prof.table.items()}
     del qs
+    # nearest other point of every data point (findClosest_exludeSelf)
+    ms = ev_time(lambda: bq.points.findClosest_exludeSelf(bvh, tp, tp))
+    comp["closest_point_exclude_self"] = {"ms": ms, "Mqueries_s": n / ms / 1e3, "queries": n}
+    # fixed-box queries: 1M boxes of half size 0.00585 (about 16 points each), count + scan + fill
+    qb = box_queries(W, 1_000_000)
+    qbt = torch.from_numpy(qb).cuda()
+    ms = ev_time(lambda: bq.fixedBoxQuery.findPrims(bvh, boxes_t, qbt))
+    off, _ = bq.fixedBoxQuery.findPrims(bvh, boxes_t, qbt)
+    comp["box_query"] = {"ms": ms, "Mqueries_s": len(qb) / ms / 1e3, "queries": len(qb),
+                         "results": int(off[-1]), "half_size": BOX_HALF,
+                         "path": "fixedBoxQuery.findPrims: count kernel, cumsum, host read of the total, fill kernel"}
+    del qbt, off
     bvh.free()
     # triangle-mesh distance forward + adjoint (icosphere, 1,310,720 triangles, 4M queries)
     verts, tris = W.icosphere(8)
@@ -470,6 +482,16 @@ def batched_components(bq, W, torch, comp):
         "refit_forward_equals_rebuild": bool(torch.equal(ids2, fi) and torch.equal(d2, fd))}
 
 
+BOX_HALF = 0.00585
+
+
+def box_queries(W, nq):
+    """nq query boxes of half size BOX_HALF around uniform centres."""
+    import numpy as np
+    c = W.uniform_points(nq, W.SEED_QUERIES)
+    return np.concatenate([c - BOX_HALF, c + BOX_HALF], 1).astype(np.float32)
+
+
 def reference_gpu(comp, pts_np, W):
     from oracle.oracle import RefGPU, have_ref_gpu
     if not have_ref_gpu():
@@ -485,6 +507,9 @@ def reference_gpu(comp, pts_np, W):
     qs = W.uniform_points(n, W.SEED_QUERIES)
     out["findClosest_ms"] = r.time_query(RefGPU.RADIX, pts_np, qs, 0, reps=2)
     out["findKNN16_ms"] = r.time_query(RefGPU.RADIX, pts_np, qs, 16, reps=2)
+    out["findClosest_exludeSelf_ms"] = r.time_query(RefGPU.RADIX, pts_np, pts_np, -1, reps=2)
+    out["fixedBoxQuery_count_fill_ms"], out["fixedBoxQuery_results"] = r.time_box_query(
+        RefGPU.RADIX, pts_np, box_queries(W, 1_000_000), reps=2)
     out["note"] = "reference kernels compiled for sm_100a, same points, one thread per query <<<ceil(Q/128),128>>>"
     comp["reference_gpu"] = out
 

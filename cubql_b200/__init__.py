@@ -95,6 +95,13 @@ _SIGS = {
     "bq_free_f3": [ctypes.POINTER(bq_bvh3f), ctypes.POINTER(bq_allocator), _P],
     "bq_closest_point_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _F, ctypes.POINTER(bq_query_config), _P, _P,
                             ctypes.POINTER(bq_allocator), _P],
+    "bq_closest_point_exclude_id_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _P, _F, ctypes.POINTER(bq_query_config),
+                                       _P, _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_closest_point_exclude_self_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _F, ctypes.POINTER(bq_query_config),
+                                         _P, _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_box_query_count_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_box_query_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _P, ctypes.c_uint64, _P, ctypes.POINTER(bq_allocator),
+                        _P],
     "bq_knn_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _I, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
                   ctypes.POINTER(bq_allocator), _P],
     "bq_tri_closest_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _P, _U, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
@@ -331,6 +338,37 @@ class points:
         return ids, d
 
     @staticmethod
+    def findClosest_exludeID(bvh, data, queries, excludeIds, maxSqrDist=float("inf"), qcfg=None):
+        """points::findClosest_exludeID (cuBQL/queries/points/findClosest.h:278-305),
+        batched: query q never returns prim excludeIds[q] (-1: no exclusion)."""
+        data, queries = _vec3(data, "points"), _vec3(queries, "queries")
+        nq = queries.shape[0]
+        ex = excludeIds.to(device=queries.device, dtype=torch.int32).contiguous()
+        if ex.numel() != nq:
+            raise ValueError("excludeIds needs one entry per query")
+        ids = torch.empty(nq, dtype=torch.int32, device=queries.device)
+        d = torch.empty(nq, dtype=torch.float32, device=queries.device)
+        q = qcfg or query_config()
+        _check(_lib.bq_closest_point_exclude_id_f3(ctypes.byref(bvh.c), _ptr(data), _ptr(queries), nq, _ptr(ex),
+                                                   maxSqrDist, ctypes.byref(q), _ptr(ids), _ptr(d),
+                                                   ctypes.byref(bvh.allocator.c), _stream()))
+        return ids, d
+
+    @staticmethod
+    def findClosest_exludeSelf(bvh, data, queries, maxSqrDist=float("inf"), qcfg=None):
+        """points::findClosest_exludeSelf (cuBQL/queries/points/findClosest.h:307-334),
+        batched: data points equal to the query are skipped."""
+        data, queries = _vec3(data, "points"), _vec3(queries, "queries")
+        nq = queries.shape[0]
+        ids = torch.empty(nq, dtype=torch.int32, device=queries.device)
+        d = torch.empty(nq, dtype=torch.float32, device=queries.device)
+        q = qcfg or query_config()
+        _check(_lib.bq_closest_point_exclude_self_f3(ctypes.byref(bvh.c), _ptr(data), _ptr(queries), nq, maxSqrDist,
+                                                     ctypes.byref(q), _ptr(ids), _ptr(d),
+                                                     ctypes.byref(bvh.allocator.c), _stream()))
+        return ids, d
+
+    @staticmethod
     def findKNN(bvh, data, queries, k, maxSqrDist=float("inf"), qcfg=None):
         """points::findKNN (cuBQL/queries/points/knn.h:75-116), batched.
         Returns (ids (nq,k) int32, sqrDist (nq,k) float32, numFound (nq,) int32)."""
@@ -343,6 +381,41 @@ class points:
         _check(_lib.bq_knn_f3(ctypes.byref(bvh.c), _ptr(data), _ptr(queries), nq, k, maxSqrDist, ctypes.byref(q),
                               _ptr(ids), _ptr(d), _ptr(nf), ctypes.byref(bvh.allocator.c), _stream()))
         return ids, d, nf
+
+
+class fixedBoxQuery:
+    """cuBQL::fixedBoxQuery::forEachPrim (cuBQL/traversal/fixedBoxQuery.h:143-156)
+    with a per-prim box test, batched over query boxes: the prims whose box
+    overlaps each query box (closed intervals, cuBQL/math/box.h:208-212)."""
+
+    @staticmethod
+    def count(bvh, boxes, queryBoxes):
+        """bq_box_query_count_f3: uint32 (nq,) number of overlapping prims."""
+        boxes, queryBoxes = _as_boxes(boxes), _as_boxes(queryBoxes)
+        nq = queryBoxes.shape[0]
+        counts = torch.empty(nq, dtype=torch.int32, device=queryBoxes.device)
+        _check(_lib.bq_box_query_count_f3(ctypes.byref(bvh.c), _ptr(boxes), _ptr(queryBoxes), nq, _ptr(counts),
+                                          ctypes.byref(bvh.allocator.c), _stream()))
+        return counts
+
+    @staticmethod
+    def findPrims(bvh, boxes, queryBoxes):
+        """Both passes: returns (offsets int64 (nq+1,), ids int32); the prims of
+        query q are ids[offsets[q]:offsets[q+1]] in the reference's visiting
+        order (forEachLeaf: depth first, first child first)."""
+        boxes, queryBoxes = _as_boxes(boxes), _as_boxes(queryBoxes)
+        nq = queryBoxes.shape[0]
+        counts = fixedBoxQuery.count(bvh, boxes, queryBoxes)
+        offsets = torch.zeros(nq + 1, dtype=torch.int64, device=queryBoxes.device)
+        torch.cumsum(counts.to(torch.int64), 0, out=offsets[1:])
+        total = int(offsets[-1].item())
+        if total >= 1 << 32:
+            raise BQError(1, "box query results exceed 2^32 entries")
+        ids = torch.empty(max(total, 1), dtype=torch.int32, device=queryBoxes.device)
+        off32 = offsets[:-1].to(torch.int32).contiguous()
+        _check(_lib.bq_box_query_f3(ctypes.byref(bvh.c), _ptr(boxes), _ptr(queryBoxes), nq, _ptr(off32), total,
+                                    _ptr(ids), ctypes.byref(bvh.allocator.c), _stream()))
+        return offsets, ids[:total]
 
 
 class triangles:

@@ -9,8 +9,13 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
 int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
 int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
 int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al);
+int box_query_count(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t nq,
+                    uint32_t *counts, Alloc &al);
+int box_query_fill(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t nq,
+                   const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al);
 int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
-                  const bq_query_config *qcfg, int32_t *ids, float *d, Alloc &al);
+                  const bq_query_config *qcfg, int32_t *ids, float *d, Alloc &al,
+                  const int32_t *excludeIds = nullptr, int excludeSelf = 0);
 int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, int k, float maxSqr,
         const bq_query_config *qcfg, int32_t *ids, float *d, int32_t *numFound, Alloc &al);
 int tri_closest(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, const float *queries, uint32_t nq,
@@ -146,6 +151,49 @@ int bq_closest_point_f3(const bq_bvh3f *bvh, const float *points, const float *q
     return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
   Alloc al = make_alloc(alloc, stream);
   return closest_point(bvh, points, queries, numQueries, maxSqrDist, qcfg, ids, sqrDist, al);
+}
+
+int bq_closest_point_exclude_id_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries,
+                                   const int32_t *excludeIds, float maxSqrDist, const bq_query_config *qcfg,
+                                   int32_t *ids, float *sqrDist, const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (numQueries && (!queries || !ids || !sqrDist || !excludeIds || (bvh->numNodes && !points)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return closest_point(bvh, points, queries, numQueries, maxSqrDist, qcfg, ids, sqrDist, al, excludeIds, 0);
+}
+
+int bq_closest_point_exclude_self_f3(const bq_bvh3f *bvh, const float *points, const float *queries,
+                                     uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg, int32_t *ids,
+                                     float *sqrDist, const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (numQueries && (!queries || !ids || !sqrDist || (bvh->numNodes && !points)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return closest_point(bvh, points, queries, numQueries, maxSqrDist, qcfg, ids, sqrDist, al, nullptr, 1);
+}
+
+int bq_box_query_count_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t numQueries,
+                          uint32_t *counts, const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (numQueries && (!queryBoxes || !counts || (bvh->numNodes && !boxes)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return box_query_count(bvh, boxes, queryBoxes, numQueries, counts, al);
+}
+
+int bq_box_query_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t numQueries,
+                    const uint32_t *offsets, uint64_t capacity, int32_t *ids, const bq_allocator *alloc,
+                    bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (numQueries && (!queryBoxes || !offsets || (bvh->numNodes && !boxes) || (capacity && !ids)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return box_query_fill(bvh, boxes, queryBoxes, numQueries, offsets, capacity, ids, al);
 }
 
 int bq_knn_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries, int k,

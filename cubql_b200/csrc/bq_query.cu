@@ -53,12 +53,17 @@ struct CPLeaf {
   float qx, qy, qz;
   float best;
   int32_t id;
+  int32_t skipId;  // blacklisted prim (findClosest_exludeID), -1: none
+  int skipSelf;    // skip points equal to the query (findClosest_exludeSelf)
   __device__ __forceinline__ float operator()(uint64_t off, uint32_t cnt)
   {
     for (uint32_t j = 0; j < cnt; j++) {
       const uint32_t pid = __ldg(primIDs + off + j);
       const float *p = points + 3ull * pid;
-      const float d = sqr_pp(__ldg(p), __ldg(p + 1), __ldg(p + 2), qx, qy, qz);
+      const float px = __ldg(p), py = __ldg(p + 1), pz = __ldg(p + 2);
+      // blacklisted candidates are passed over (findClosest.h:200-203)
+      if ((int32_t)pid == skipId || (skipSelf && px == qx && py == qy && pz == qz)) continue;
+      const float d = sqr_pp(px, py, pz, qx, qy, qz);
       const bool take = (TIE == TIE_REFERENCE) ? (d < best)  // findClosest.h:211-218
                                                : (d < best || (d == best && id >= 0 && (int32_t)pid < id));
       if (take) {
@@ -70,13 +75,21 @@ struct CPLeaf {
   }
 };
 
+// blacklist of a closest-point call: per-query excluded ids, or points
+// equal to the query
+struct CpExclude {
+  const int32_t *ids;
+  int self;
+};
+
 template <int TIE, typename Stack>
 __device__ __forceinline__ bool run_cp(const Node *nodes, const uint32_t *primIDs, const float *points,
                                        const float *queries, uint32_t qi, float maxSqr, Stack &st, int32_t *outIds,
-                                       float *outD)
+                                       float *outD, CpExclude ex)
 {
   const float *q = queries + 3ull * qi;
-  CPLeaf<TIE> leaf{primIDs, points, __ldg(q), __ldg(q + 1), __ldg(q + 2), maxSqr, -1};
+  CPLeaf<TIE> leaf{primIDs, points, __ldg(q), __ldg(q + 1), __ldg(q + 2), maxSqr, -1,
+                   ex.ids ? __ldg(ex.ids + qi) : -1, ex.self};
   if (!traverse<TIE>(nodes, leaf.qx, leaf.qy, leaf.qz, maxSqr, st, leaf)) return false;
   outIds[qi] = leaf.id;
   outD[qi] = leaf.id >= 0 ? leaf.best : INFINITY;
@@ -88,13 +101,13 @@ __global__ void __launch_bounds__(128) k_closest(const Node *__restrict__ nodes,
                                                  const float *__restrict__ points, const float *__restrict__ queries,
                                                  const uint32_t *__restrict__ order, uint32_t nq, float maxSqr,
                                                  int32_t *__restrict__ outIds, float *__restrict__ outD,
-                                                 uint32_t *__restrict__ ovfList, uint32_t *ovfCount)
+                                                 uint32_t *__restrict__ ovfList, uint32_t *ovfCount, CpExclude ex)
 {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const uint32_t qi = order ? __ldg(order + t) : t;
   LocalStack<STACK> st;
-  if (!run_cp<TIE>(nodes, primIDs, points, queries, qi, maxSqr, st, outIds, outD))
+  if (!run_cp<TIE>(nodes, primIDs, points, queries, qi, maxSqr, st, outIds, outD, ex))
     ovfList[atomicAdd(ovfCount, 1u)] = qi;
 }
 
@@ -102,14 +115,14 @@ template <int TIE>
 __global__ void k_closest_deep(const Node *__restrict__ nodes, const uint32_t *__restrict__ primIDs,
                                const float *__restrict__ points, const float *__restrict__ queries, float maxSqr,
                                int32_t *__restrict__ outIds, float *__restrict__ outD, const uint32_t *ovfList,
-                               const uint32_t *ovfCount, StackEntry *stacks, uint32_t *err)
+                               const uint32_t *ovfCount, StackEntry *stacks, uint32_t *err, CpExclude ex)
 {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t cnt = *ovfCount;
   for (uint32_t w = tid; w < cnt; w += gridDim.x * blockDim.x) {
     const uint32_t qi = ovfList[w];
     GlobalStack st{stacks + (size_t)tid * DEEP_STACK, DEEP_STACK, 0};
-    if (!run_cp<TIE>(nodes, primIDs, points, queries, qi, maxSqr, st, outIds, outD)) {
+    if (!run_cp<TIE>(nodes, primIDs, points, queries, qi, maxSqr, st, outIds, outD, ex)) {
       outIds[qi] = -1;
       outD[qi] = INFINITY;
       atomicOr(err, DEV_ERR_STACK);
@@ -268,17 +281,17 @@ int finish(QueryScratch &qs, Alloc &al)
 
 template <int TIE, int STACK>
 void launch_cp(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
-               int block, int32_t *ids, float *d, QueryScratch &qs, cudaStream_t s)
+               int block, int32_t *ids, float *d, QueryScratch &qs, cudaStream_t s, CpExclude ex)
 {
   const Node *nodes = (const Node *)bvh->nodes;
   {
     ProfScope ps("query.closest", s);
     k_closest<TIE, STACK><<<div_up(nq, block), block, 0, s>>>(nodes, bvh->primIDs, points, queries, qs.order, nq,
-                                                             maxSqr, ids, d, qs.ovfList, qs.ovfCount);
+                                                             maxSqr, ids, d, qs.ovfList, qs.ovfCount, ex);
   }
   ProfScope ps("query.deep", s);
   k_closest_deep<TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, maxSqr, ids, d,
-                                                         qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+                                                         qs.ovfList, qs.ovfCount, qs.deep, qs.err, ex);
 }
 
 template <int K, int TIE, int STACK>
@@ -338,8 +351,10 @@ int query_config(const bq_query_config *q, bq_query_config &out)
 }
 
 int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
-                  const bq_query_config *qcfg, int32_t *ids, float *d, Alloc &al)
+                  const bq_query_config *qcfg, int32_t *ids, float *d, Alloc &al, const int32_t *excludeIds,
+                  int excludeSelf)
 {
+  const CpExclude ex{excludeIds, excludeSelf};
   bq_query_config c;
   BQ_TRY(query_config(qcfg, c));
   if (nq == 0) return BQ_OK;
@@ -353,13 +368,13 @@ int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries
   BQ_TRY(prepare(bvh, queries, nq, c.reorder != 0, tmp, al, qs));
   const int tie = c.tieMode, st = c.stackDepth, b = c.blockSize;
   if (tie == BQ_TIES_REFERENCE) {
-    if (st == 32) launch_cp<TIE_REFERENCE, 32>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
-    else if (st == 64) launch_cp<TIE_REFERENCE, 64>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
-    else launch_cp<TIE_REFERENCE, 128>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
+    if (st == 32) launch_cp<TIE_REFERENCE, 32>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s, ex);
+    else if (st == 64) launch_cp<TIE_REFERENCE, 64>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s, ex);
+    else launch_cp<TIE_REFERENCE, 128>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s, ex);
   } else {
-    if (st == 32) launch_cp<TIE_LOWEST, 32>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
-    else if (st == 64) launch_cp<TIE_LOWEST, 64>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
-    else launch_cp<TIE_LOWEST, 128>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s);
+    if (st == 32) launch_cp<TIE_LOWEST, 32>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s, ex);
+    else if (st == 64) launch_cp<TIE_LOWEST, 64>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s, ex);
+    else launch_cp<TIE_LOWEST, 128>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s, ex);
   }
   BQ_CUDA(cudaGetLastError());
   return finish(qs, al);

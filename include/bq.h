@@ -169,6 +169,41 @@ int bq_closest_point_f3(const bq_bvh3f *bvh, const float *points, const float *q
                         float maxSqrDist, const bq_query_config *qcfg, int32_t *ids, float *sqrDist,
                         const bq_allocator *alloc, bq_stream_t stream);
 
+/* Closest data point per query, skipping one prim per query: excludeIds
+   (device array of numQueries ints) names the prim query q must not return
+   (-1: none).  Replaces cuBQL::points::findClosest_exludeID
+   (cuBQL/queries/points/findClosest.h:278-305) in a user kernel; the
+   typical use is "nearest other point" with the data points as queries. */
+int bq_closest_point_exclude_id_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries,
+                                   const int32_t *excludeIds, float maxSqrDist, const bq_query_config *qcfg,
+                                   int32_t *ids, float *sqrDist, const bq_allocator *alloc, bq_stream_t stream);
+
+/* Closest data point per query among the points not equal to the query
+   (every coordinate equal).  Replaces cuBQL::points::findClosest_exludeSelf
+   (cuBQL/queries/points/findClosest.h:307-334) in a user kernel. */
+int bq_closest_point_exclude_self_f3(const bq_bvh3f *bvh, const float *points, const float *queries,
+                                     uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg, int32_t *ids,
+                                     float *sqrDist, const bq_allocator *alloc, bq_stream_t stream);
+
+/* Fixed-box query, first pass: counts[q] = the number of prims whose box
+   (boxes: the boxes the tree was built over) overlaps queryBoxes[q]
+   (closed intervals, box_t::overlaps, cuBQL/math/box.h:208-212).  Replaces
+   a user kernel calling cuBQL::fixedBoxQuery::forEachPrim
+   (cuBQL/traversal/fixedBoxQuery.h:143-156) with a lambda that tests the
+   prim's box.  Synchronises the stream (reports a traversal that would
+   need more than 128 stack entries as BQ_ERR_STACK_OVERFLOW). */
+int bq_box_query_count_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t numQueries,
+                          uint32_t *counts, const bq_allocator *alloc, bq_stream_t stream);
+
+/* Fixed-box query, second pass: the ids of query q go to
+   ids[offsets[q] .. offsets[q+1]) (offsets: the exclusive prefix sum of the
+   first pass's counts; the last query ends at `capacity`, the length of
+   ids), in the reference's visiting order (forEachLeaf, depth first, first
+   child first).  Synchronises the stream. */
+int bq_box_query_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t numQueries,
+                    const uint32_t *offsets, uint64_t capacity, int32_t *ids, const bq_allocator *alloc,
+                    bq_stream_t stream);
+
 /* k nearest data points per query (1 <= k <= 64), ascending by squared
    distance.  Replaces cuBQL::points::findKNN
    (cuBQL/queries/points/knn.h:75-116).  ids/sqrDist are numQueries*k

@@ -166,6 +166,66 @@ inline void findKNN(const BVH &bvh, const Vec *points, const Vec *queries, uint3
                   numFound, nullptr, s),
         "findKNN");
 }
+
+/*! batched cuBQL::points::findClosest_exludeID (findClosest.h:278-305):
+    query i never returns prim excludeIds[i] (-1: nothing excluded) */
+template <class BVH, class Vec>
+inline void findClosest_exludeID(const BVH &bvh, const Vec *points, const Vec *queries, uint32_t numQueries,
+                                 const int32_t *excludeIds, int32_t *ids, float *sqrDist,
+                                 float maxSqrDist = INFINITY, cudaStream_t s = 0, int tieMode = BQ_TIES_LOWEST_ID)
+{
+  static_assert(sizeof(Vec) == 12, "vec3f layout");
+  bq_bvh3f c = to_c(bvh);
+  bq_query_config q{tieMode, 0, 0, 1, 0};
+  check(bq_closest_point_exclude_id_f3(&c, (const float *)points, (const float *)queries, numQueries, excludeIds,
+                                       maxSqrDist, &q, ids, sqrDist, nullptr, s),
+        "findClosest_exludeID");
+}
+
+/*! batched cuBQL::points::findClosest_exludeSelf (findClosest.h:307-334):
+    data points equal to the query point are skipped */
+template <class BVH, class Vec>
+inline void findClosest_exludeSelf(const BVH &bvh, const Vec *points, const Vec *queries, uint32_t numQueries,
+                                   int32_t *ids, float *sqrDist, float maxSqrDist = INFINITY, cudaStream_t s = 0,
+                                   int tieMode = BQ_TIES_LOWEST_ID)
+{
+  static_assert(sizeof(Vec) == 12, "vec3f layout");
+  bq_bvh3f c = to_c(bvh);
+  bq_query_config q{tieMode, 0, 0, 1, 0};
+  check(bq_closest_point_exclude_self_f3(&c, (const float *)points, (const float *)queries, numQueries, maxSqrDist,
+                                         &q, ids, sqrDist, nullptr, s),
+        "findClosest_exludeSelf");
+}
 } // namespace points
+
+namespace fixedBoxQuery {
+/*! batched cuBQL::fixedBoxQuery::forEachPrim (traversal/fixedBoxQuery.h:139-156)
+    with a lambda that keeps prims whose box overlaps the query box.  First
+    pass: counts[i] = the number of such prims for queryBoxes[i]. */
+template <class BVH, class Box>
+inline void countPrims(const BVH &bvh, const Box *boxes, const Box *queryBoxes, uint32_t numQueries,
+                       uint32_t *counts, cudaStream_t s = 0)
+{
+  static_assert(sizeof(Box) == 24, "box3f layout");
+  bq_bvh3f c = to_c(bvh);
+  check(bq_box_query_count_f3(&c, (const bq_box3f *)boxes, (const bq_box3f *)queryBoxes, numQueries, counts,
+                              nullptr, s),
+        "fixedBoxQuery::countPrims");
+}
+
+/*! second pass: the prims of query i go to ids[offsets[i] ..], in the
+    order forEachPrim visits them; offsets is the exclusive prefix sum of
+    the counts and `capacity` the length of ids */
+template <class BVH, class Box>
+inline void findPrims(const BVH &bvh, const Box *boxes, const Box *queryBoxes, uint32_t numQueries,
+                      const uint32_t *offsets, uint64_t capacity, int32_t *ids, cudaStream_t s = 0)
+{
+  static_assert(sizeof(Box) == 24, "box3f layout");
+  bq_bvh3f c = to_c(bvh);
+  check(bq_box_query_f3(&c, (const bq_box3f *)boxes, (const bq_box3f *)queryBoxes, numQueries, offsets, capacity,
+                        ids, nullptr, s),
+        "fixedBoxQuery::findPrims");
+}
+} // namespace fixedBoxQuery
 
 } // namespace bq_cubql

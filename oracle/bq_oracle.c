@@ -709,10 +709,15 @@ int orc_knn(const onode *nodes, uint32_t numNodes, const uint32_t *primIDs, cons
 
 /* closest point (findClosest.h:181-226, 336-360).  tie_mode 1 accepts a
    candidate only when strictly closer; tie_mode 0 also takes an equally
-   close candidate with a lower primID.  Not found: id -1, dist +inf. */
-int orc_closest_point(const onode *nodes, uint32_t numNodes, const uint32_t *primIDs, const float *points,
-                      const float *queries, uint32_t nq, float maxSqr, int fma_mode, int tie_mode,
-                      int stackLimit, int32_t *ids, float *dists, uint8_t *overflowed, uint32_t *visits)
+   close candidate with a lower primID.  Not found: id -1, dist +inf.
+   Blacklists (findClosest_withBlackList, findClosest.h:181-226): with
+   excludeIds, query i skips prim excludeIds[i] (when >= 0;
+   findClosest_exludeID, :278-305); with excludeSelf, every query skips the
+   points equal to itself (findClosest_exludeSelf, :307-334). */
+static int closest_impl(const onode *nodes, uint32_t numNodes, const uint32_t *primIDs, const float *points,
+                        const float *queries, uint32_t nq, float maxSqr, int fma_mode, int tie_mode,
+                        int stackLimit, const int32_t *excludeIds, int excludeSelf, int32_t *ids, float *dists,
+                        uint8_t *overflowed, uint32_t *visits)
 {
   for (uint32_t i = 0; i < nq; i++) {
     const float *q = queries + 3 * (size_t)i;
@@ -753,7 +758,10 @@ int orc_closest_point(const onode *nodes, uint32_t numNodes, const uint32_t *pri
           float leaf = INFINITY;
           for (uint32_t j = 0; j < cnt; j++) {
             uint32_t pid = primIDs[off + j];
-            float d = sqr_pp(points + 3 * (size_t)pid, q, fma_mode);
+            const float *pp = points + 3 * (size_t)pid;
+            if (excludeIds && excludeIds[i] >= 0 && (int32_t)pid == excludeIds[i]) continue;
+            if (excludeSelf && pp[0] == q[0] && pp[1] == q[1] && pp[2] == q[2]) continue;
+            float d = sqr_pp(pp, q, fma_mode);
             int take = tie_mode == 1 ? (d < bestD)
                                      : (d < bestD || (best >= 0 && d == bestD && (int32_t)pid < best));
             if (take) { bestD = d; best = (int32_t)pid; }
@@ -776,6 +784,87 @@ int orc_closest_point(const onode *nodes, uint32_t numNodes, const uint32_t *pri
     if (visits) visits[i] = nvis;
   }
   return 0;
+}
+
+int orc_closest_point(const onode *nodes, uint32_t numNodes, const uint32_t *primIDs, const float *points,
+                      const float *queries, uint32_t nq, float maxSqr, int fma_mode, int tie_mode,
+                      int stackLimit, int32_t *ids, float *dists, uint8_t *overflowed, uint32_t *visits)
+{
+  return closest_impl(nodes, numNodes, primIDs, points, queries, nq, maxSqr, fma_mode, tie_mode, stackLimit, NULL, 0,
+                      ids, dists, overflowed, visits);
+}
+
+int orc_closest_point_exclude(const onode *nodes, uint32_t numNodes, const uint32_t *primIDs, const float *points,
+                              const float *queries, uint32_t nq, float maxSqr, int fma_mode, int tie_mode,
+                              const int32_t *excludeIds, int excludeSelf, int32_t *ids, float *dists)
+{
+  return closest_impl(nodes, numNodes, primIDs, points, queries, nq, maxSqr, fma_mode, tie_mode, 1 << 30,
+                      excludeIds, excludeSelf, ids, dists, NULL, NULL);
+}
+
+/* ------------------------------------------------------------------ */
+/* fixed-box query: fixedBoxQuery::forEachLeaf over a BinaryBVH         */
+/* (cuBQL/traversal/fixedBoxQuery.h:73-137) with forEachPrim's per-prim */
+/* loop (:139-156), the lambda keeping prims whose own box overlaps the */
+/* query box; overlap is box_t::overlaps (cuBQL/math/box.h:208-212).    */
+/* ------------------------------------------------------------------ */
+static int box_ov(const float *qlo, const float *qhi, const float *lo, const float *hi)
+{
+  return !(qhi[0] < lo[0] || qhi[1] < lo[1] || qhi[2] < lo[2] || hi[0] < qlo[0] || hi[1] < qlo[1] ||
+           hi[2] < qlo[2]);
+}
+
+/* For query q the overlapping prims go to ids[offsets[q] ..] in visiting
+   order (pass ids = NULL to count only); counts[q] gets their number.
+   Returns 0, or -1 when a traversal needs more than stackLimit entries. */
+int orc_box_query(const onode *nodes, uint32_t numNodes, const uint32_t *primIDs, const obox *boxes,
+                  const obox *queryBoxes, uint32_t nq, int stackLimit, uint32_t *counts, const uint64_t *offsets,
+                  int32_t *ids)
+{
+  uint64_t *stack = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(stackLimit > 0 ? stackLimit : 1));
+  int rc = 0;
+  if (!stack) return -1;
+  for (uint32_t q = 0; q < nq; q++) {
+    const float *qlo = queryBoxes[q].lo, *qhi = queryBoxes[q].hi;
+    uint32_t c = 0;
+    int sp = 0;
+    if (numNodes == 0) { counts[q] = 0; continue; }
+    uint64_t node = nodes[0].admin;
+    for (;;) {
+      int leaf = 1;
+      while (ADMIN_CNT(node) == 0) {
+        const onode *n0 = &nodes[ADMIN_OFF(node)], *n1 = n0 + 1;
+        int o0 = box_ov(qlo, qhi, n0->lo, n0->hi), o1 = box_ov(qlo, qhi, n1->lo, n1->hi);
+        if (o0) {
+          if (o1) {
+            if (sp >= stackLimit) { rc = -1; goto next; }
+            stack[sp++] = n1->admin;
+          }
+          node = n0->admin;
+        } else if (o1) {
+          node = n1->admin;
+        } else {
+          leaf = 0;
+          break;
+        }
+      }
+      if (leaf) {
+        for (uint32_t j = 0; j < ADMIN_CNT(node); j++) {
+          uint32_t pid = primIDs[ADMIN_OFF(node) + j];
+          if (box_ov(qlo, qhi, boxes[pid].lo, boxes[pid].hi)) {
+            if (ids) ids[offsets[q] + c] = (int32_t)pid;
+            c++;
+          }
+        }
+      }
+      if (sp == 0) break;
+      node = stack[--sp];
+    }
+  next:
+    counts[q] = c;
+  }
+  free(stack);
+  return rc;
 }
 
 /* ------------------------------------------------------------------ */

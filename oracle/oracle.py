@@ -138,6 +138,42 @@ class Oracle:
                                    ctypes.c_int(tie_mode), ctypes.c_int(stack), _p(ids), _p(d), _p(ovf), _p(vis))
         return ids, d, ovf.astype(bool), vis
 
+    def closest_point_exclude(self, nodes, prims, points, queries, exclude_ids=None, exclude_self=False,
+                              maxSqr=np.inf, fma_mode=1, tie_mode=0):
+        """findClosest_exludeID (one prim id per query, -1: none) or
+        findClosest_exludeSelf (points equal to the query), findClosest.h:278-334."""
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        ex = None if exclude_ids is None else np.ascontiguousarray(exclude_ids, dtype=np.int32)
+        self.lib.orc_closest_point_exclude(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), _p(points), _p(queries),
+                                           ctypes.c_uint32(nq), ctypes.c_float(maxSqr), ctypes.c_int(fma_mode),
+                                           ctypes.c_int(tie_mode), _p(ex) if ex is not None else None,
+                                           ctypes.c_int(1 if exclude_self else 0), _p(ids), _p(d))
+        return ids, d
+
+    def box_query(self, nodes, prims, boxes, query_boxes, stack=1 << 20):
+        """fixedBoxQuery::forEachPrim with a per-prim box test
+        (fixedBoxQuery.h:73-156): returns (offsets int64 (nq+1,), ids int32)
+        in visiting order; raises on a traversal deeper than `stack`."""
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        boxes, qb = _f32(boxes).reshape(-1, 6), _f32(query_boxes).reshape(-1, 6)
+        nq = qb.shape[0]
+        counts = np.zeros(nq, dtype=np.uint32)
+        args = (_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), _p(boxes), _p(qb), ctypes.c_uint32(nq),
+                ctypes.c_int(stack))
+        if self.lib.orc_box_query(*args, _p(counts), None, None) != 0:
+            raise RuntimeError("box query traversal stack exceeded")
+        offsets = np.zeros(nq + 1, dtype=np.uint64)
+        np.cumsum(counts, out=offsets[1:])
+        ids = np.zeros(max(int(offsets[-1]), 1), dtype=np.int32)
+        self.lib.orc_box_query(*args, _p(counts), _p(offsets), _p(ids))
+        return offsets.astype(np.int64), ids[:int(offsets[-1])]
+
     def knn(self, nodes, prims, points, queries, k, maxSqr=np.inf, fma_mode=1, tie_mode=0, stack=64):
         nodes = np.ascontiguousarray(nodes, dtype=NODE)
         prims = np.ascontiguousarray(prims, dtype=np.uint32)
@@ -246,6 +282,21 @@ class RefCPU:
                                  ctypes.c_int(threads))
         return ids, d
 
+    def closest_point_exclude(self, nodes, prims, points, queries, exclude_ids=None, maxSqr=np.inf, threads=1):
+        """points::findClosest_exludeID (exclude_ids given) or
+        points::findClosest_exludeSelf (exclude_ids None)."""
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        ex = None if exclude_ids is None else np.ascontiguousarray(exclude_ids, dtype=np.int32)
+        self.lib.ref_cpu_closest_exclude(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), ctypes.c_uint32(len(prims)),
+                                         _p(points), _p(queries), ctypes.c_uint32(nq), ctypes.c_float(maxSqr),
+                                         _p(ex) if ex is not None else None, _p(ids), _p(d), ctypes.c_int(threads))
+        return ids, d
+
     def knn(self, nodes, prims, points, queries, k, maxSqr=np.inf, threads=1):
         nodes = np.ascontiguousarray(nodes, dtype=NODE)
         prims = np.ascontiguousarray(prims, dtype=np.uint32)
@@ -306,6 +357,40 @@ class RefGPU:
         assert rc == 0
         return ids, d
 
+    def closest_point_exclude(self, nodes, prims, points, queries, exclude_ids=None, maxSqr=np.inf):
+        """The reference's findClosest_exludeID (exclude_ids given) or
+        findClosest_exludeSelf kernel, one thread per query."""
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        ex = None if exclude_ids is None else np.ascontiguousarray(exclude_ids, dtype=np.int32)
+        rc = self.lib.ref_gpu_closest_exclude(_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims),
+                                              ctypes.c_uint32(len(prims)), _p(points), ctypes.c_uint32(len(points)),
+                                              _p(queries), ctypes.c_uint32(nq), ctypes.c_float(maxSqr),
+                                              _p(ex) if ex is not None else None, _p(ids), _p(d))
+        assert rc == 0
+        return ids, d
+
+    def box_query(self, nodes, prims, boxes, query_boxes):
+        """The reference's fixedBoxQuery::forEachPrim in a kernel, one thread
+        per query box, keeping prims whose box overlaps: (offsets, ids)."""
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        boxes, qb = _f32(boxes).reshape(-1, 6), _f32(query_boxes).reshape(-1, 6)
+        nq = qb.shape[0]
+        counts = np.zeros(nq, dtype=np.uint32)
+        args = (_p(nodes), ctypes.c_uint32(len(nodes)), _p(prims), ctypes.c_uint32(len(prims)), _p(boxes),
+                ctypes.c_uint32(len(boxes)), _p(qb), ctypes.c_uint32(nq), _p(counts))
+        assert self.lib.ref_gpu_box_query(*args, None, None) == 0
+        offsets = np.zeros(nq + 1, dtype=np.uint64)
+        np.cumsum(counts, out=offsets[1:])
+        ids = np.zeros(max(int(offsets[-1]), 1), dtype=np.int32)
+        assert self.lib.ref_gpu_box_query(*args, _p(offsets), _p(ids)) == 0
+        return offsets.astype(np.int64), ids[:int(offsets[-1])]
+
     def knn(self, nodes, prims, points, queries, k, maxSqr=np.inf):
         nodes = np.ascontiguousarray(nodes, dtype=NODE)
         prims = np.ascontiguousarray(prims, dtype=np.uint32)
@@ -361,6 +446,17 @@ class RefGPU:
                                          ctypes.c_int(kind), ctypes.c_int(reps), ctypes.byref(ms))
         assert rc == 0
         return ms.value
+
+    def time_box_query(self, method, points, query_boxes, makeLeafThreshold=0, reps=5):
+        """(ms of count + fill kernels, total results) for the reference box
+        query over a tree built on the point boxes."""
+        points, qb = _f32(points), _f32(query_boxes).reshape(-1, 6)
+        ms, tot = ctypes.c_float(), ctypes.c_uint64()
+        rc = self.lib.ref_gpu_time_box_query(ctypes.c_int(method), _p(points), ctypes.c_uint32(len(points)),
+                                             ctypes.c_int(makeLeafThreshold), _p(qb), ctypes.c_uint32(len(qb)),
+                                             ctypes.c_int(reps), ctypes.byref(ms), ctypes.byref(tot))
+        assert rc == 0
+        return ms.value, tot.value
 
 
 # ---------------------------------------------------------------------------

@@ -120,6 +120,25 @@ int ref_cpu_closest(const void *nodes, uint32_t numNodes, const uint32_t *primID
   return 0;
 }
 
+// closest point with the reference's blacklists: excludeIds != NULL ->
+// points::findClosest_exludeID(excludeIds[i], ...), else
+// points::findClosest_exludeSelf (findClosest.h:278-334)
+int ref_cpu_closest_exclude(const void *nodes, uint32_t numNodes, const uint32_t *primIDs, uint32_t numPrims,
+                            const float *points, const float *queries, uint32_t nq, float maxSqr,
+                            const int32_t *excludeIds, int32_t *ids, float *dists, int nthreads)
+{
+  bvh3f bvh = view(nodes, numNodes, primIDs, numPrims);
+  const vec3f *pts = (const vec3f *)points;
+  const vec3f *qs = (const vec3f *)queries;
+  parallel_for(nq, nthreads, [&](uint32_t i) {
+    const int id = excludeIds ? points::findClosest_exludeID(excludeIds[i], bvh, pts, qs[i], maxSqr)
+                              : points::findClosest_exludeSelf(bvh, pts, qs[i], maxSqr);
+    ids[i] = id;
+    dists[i] = id < 0 ? INFINITY : fSqrDistance_rd(pts[id], qs[i]);
+  });
+  return 0;
+}
+
 // kNN per query (k <= 64): ids/dists nq*k (unfilled: -1/+inf), numFound nq.
 int ref_cpu_knn(const void *nodes, uint32_t numNodes, const uint32_t *primIDs, uint32_t numPrims,
                 const float *points, const float *queries, uint32_t nq, int k, float maxSqr, int32_t *ids,

@@ -16,6 +16,8 @@
 //   cuBQL::cuda::rebinRadixBuilder cuBQL/builder/cuda/rebinMortonBuilder.h:1478-1487
 //   points::findClosest / findKNN, triangles::findClosest (device functions,
 //   launched one thread per query as testing/points/closestPoint.cu:37-58)
+//   fixedBoxQuery::forEachPrim  cuBQL/traversal/fixedBoxQuery.h:139-156, with
+//   a lambda that keeps prims whose box overlaps the query box
 #define CUBQL_GPU_BUILDER_IMPLEMENTATION 1
 #include "cuBQL/bvh.h"
 #include "cuBQL/builder/cuda/radix.h"
@@ -23,6 +25,7 @@
 #include "cuBQL/queries/points/findClosest.h"
 #include "cuBQL/queries/points/knn.h"
 #include "cuBQL/queries/triangles/findClosest.h"
+#include "cuBQL/traversal/fixedBoxQuery.h"
 
 #include <cstdio>
 #include <vector>
@@ -73,6 +76,37 @@ __global__ void k_closest(bvh3f bvh, const vec3f *pts, const vec3f *qs, int nq, 
   int id = points::findClosest(bvh, pts, qs[tid], maxSqr);
   ids[tid] = id;
   dists[tid] = id < 0 ? INFINITY : fSqrDistance_rd(pts[id], qs[tid]);
+}
+
+// excl != nullptr: findClosest_exludeID(excl[tid]); else findClosest_exludeSelf
+__global__ void k_closest_exclude(bvh3f bvh, const vec3f *pts, const vec3f *qs, int nq, float maxSqr,
+                                  const int *excl, int *ids, float *dists)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= nq) return;
+  int id = excl ? points::findClosest_exludeID(excl[tid], bvh, pts, qs[tid], maxSqr)
+                : points::findClosest_exludeSelf(bvh, pts, qs[tid], maxSqr);
+  ids[tid] = id;
+  dists[tid] = id < 0 ? INFINITY : fSqrDistance_rd(pts[id], qs[tid]);
+}
+
+// offsets == nullptr: count pass (counts[tid]); else fill ids[offsets[tid]..]
+__global__ void k_box(bvh3f bvh, const box3f *boxes, const box3f *qb, int nq, const unsigned long long *offsets,
+                      unsigned *counts, int *ids)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= nq) return;
+  const box3f q = qb[tid];
+  unsigned c = 0;
+  auto perPrim = [&](uint32_t primID) -> int {
+    if (q.overlaps(boxes[primID])) {
+      if (offsets) ids[offsets[tid] + c] = (int)primID;
+      c++;
+    }
+    return CUBQL_CONTINUE_TRAVERSAL;
+  };
+  fixedBoxQuery::forEachPrim(perPrim, bvh, q);
+  counts[tid] = c;
 }
 
 template <int KMAX>
@@ -170,6 +204,48 @@ int ref_gpu_closest(const void *nodes, uint32_t numNodes, const uint32_t *primID
   cudaMemcpy(ids, di, sizeof(int) * nq, cudaMemcpyDeviceToHost);
   cudaMemcpy(dists, dd, sizeof(float) * nq, cudaMemcpyDeviceToHost);
   cudaFree(dp); cudaFree(dq); cudaFree(di); cudaFree(dd);
+  return 0;
+}
+
+int ref_gpu_closest_exclude(const void *nodes, uint32_t numNodes, const uint32_t *primIDs, uint32_t numPrims,
+                            const float *points, uint32_t np, const float *queries, uint32_t nq, float maxSqr,
+                            const int32_t *excludeIds, int32_t *ids, float *dists)
+{
+  DeviceTree t;
+  if (t.upload(nodes, numNodes, primIDs, numPrims)) return -1;
+  vec3f *dp = dalloc_copy((const vec3f *)points, np), *dq = dalloc_copy((const vec3f *)queries, nq);
+  int *dx = excludeIds ? dalloc_copy((const int *)excludeIds, nq) : nullptr;
+  int *di = dalloc_copy<int>(nullptr, nq);
+  float *dd = dalloc_copy<float>(nullptr, nq);
+  k_closest_exclude<<<(nq + 127) / 128, 128>>>(t.bvh, dp, dq, (int)nq, maxSqr, dx, di, dd);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(ids, di, sizeof(int) * nq, cudaMemcpyDeviceToHost);
+  cudaMemcpy(dists, dd, sizeof(float) * nq, cudaMemcpyDeviceToHost);
+  cudaFree(dp); cudaFree(dq); cudaFree(di); cudaFree(dd);
+  if (dx) cudaFree(dx);
+  return 0;
+}
+
+// Both passes of the reference box query; offsets (nq+1) and ids are host
+// arrays sized by the caller after a count-only call (ids == NULL).
+int ref_gpu_box_query(const void *nodes, uint32_t numNodes, const uint32_t *primIDs, uint32_t numPrims,
+                      const float *boxes, uint32_t nb, const float *queryBoxes, uint32_t nq, uint32_t *counts,
+                      const uint64_t *offsets, int32_t *ids)
+{
+  DeviceTree t;
+  if (t.upload(nodes, numNodes, primIDs, numPrims)) return -1;
+  box3f *db = dalloc_copy((const box3f *)boxes, nb), *dq = dalloc_copy((const box3f *)queryBoxes, nq);
+  unsigned *dc = dalloc_copy<unsigned>(nullptr, nq);
+  unsigned long long *doff = ids ? dalloc_copy((const unsigned long long *)offsets, nq + 1) : nullptr;
+  const size_t total = ids ? offsets[nq] : 0;
+  int *di = ids ? dalloc_copy<int>(nullptr, total) : nullptr;
+  k_box<<<(nq + 127) / 128, 128>>>(t.bvh, db, dq, (int)nq, doff, dc, di);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(counts, dc, sizeof(unsigned) * nq, cudaMemcpyDeviceToHost);
+  if (ids && total) cudaMemcpy(ids, di, sizeof(int) * total, cudaMemcpyDeviceToHost);
+  cudaFree(db); cudaFree(dq); cudaFree(dc);
+  if (doff) cudaFree(doff);
+  if (di) cudaFree(di);
   return 0;
 }
 
@@ -292,7 +368,9 @@ int ref_gpu_time_query(int method, const float *points, uint32_t n, int makeLeaf
   float total = 0.f;
   for (int r = -1; r < reps; r++) {
     cudaEventRecord(e0);
-    if (kind == 0)
+    if (kind == -1)
+      k_closest_exclude<<<(nq + 127) / 128, 128>>>(bvh, dp, dq, (int)nq, INFINITY, nullptr, di, dd);
+    else if (kind == 0)
       k_closest<<<(nq + 127) / 128, 128>>>(bvh, dp, dq, (int)nq, INFINITY, di, dd);
     else if (k <= 16)
       k_knn<16><<<(nq + 127) / 128, 128>>>(bvh, dp, dq, (int)nq, k, INFINITY, di, dd, dn);
@@ -309,6 +387,51 @@ int ref_gpu_time_query(int method, const float *points, uint32_t n, int makeLeaf
   cuBQL::cuda::free(bvh);
   cudaFree(dp); cudaFree(dq); cudaFree(db); cudaFree(di); cudaFree(dn); cudaFree(dd);
   *ms_out = total / (reps > 0 ? reps : 1);
+  return 0;
+}
+
+// Times the reference box query (count kernel + fill kernel, offsets from
+// an untimed count pass) over a tree of `method` built on point boxes.
+int ref_gpu_time_box_query(int method, const float *points, uint32_t n, int makeLeafThreshold,
+                           const float *queryBoxes, uint32_t nq, int reps, float *ms_out, uint64_t *total_out)
+{
+  vec3f *dp = dalloc_copy((const vec3f *)points, n);
+  box3f *db = dalloc_copy<box3f>(nullptr, n), *dq = dalloc_copy((const box3f *)queryBoxes, nq);
+  unsigned *dc = dalloc_copy<unsigned>(nullptr, nq);
+  unsigned long long *doff = dalloc_copy<unsigned long long>(nullptr, nq + 1);
+  if (!dp || !db || !dq || !dc || !doff) return -1;
+  k_points_to_boxes<<<(n + 127) / 128, 128>>>(dp, db, (int)n);
+  bvh3f bvh;
+  run_build(method, db, n, makeLeafThreshold, bvh);
+  k_box<<<(nq + 127) / 128, 128>>>(bvh, db, dq, (int)nq, nullptr, dc, nullptr);
+  RCHECK(cudaDeviceSynchronize());
+  std::vector<unsigned> hc(nq);
+  std::vector<unsigned long long> ho(nq + 1, 0);
+  cudaMemcpy(hc.data(), dc, sizeof(unsigned) * nq, cudaMemcpyDeviceToHost);
+  for (uint32_t i = 0; i < nq; i++) ho[i + 1] = ho[i] + hc[i];
+  cudaMemcpy(doff, ho.data(), sizeof(unsigned long long) * (nq + 1), cudaMemcpyHostToDevice);
+  int *di = dalloc_copy<int>(nullptr, ho[nq]);
+  if (!di) return -1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float total = 0.f;
+  for (int r = -1; r < reps; r++) {
+    cudaEventRecord(e0);
+    k_box<<<(nq + 127) / 128, 128>>>(bvh, db, dq, (int)nq, nullptr, dc, nullptr);
+    k_box<<<(nq + 127) / 128, 128>>>(bvh, db, dq, (int)nq, doff, dc, di);
+    cudaEventRecord(e1);
+    RCHECK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r >= 0) total += ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cuBQL::cuda::free(bvh);
+  cudaFree(dp); cudaFree(db); cudaFree(dq); cudaFree(dc); cudaFree(doff); cudaFree(di);
+  *ms_out = total / (reps > 0 ? reps : 1);
+  *total_out = ho[nq];
   return 0;
 }
 

@@ -5,6 +5,8 @@
                                            # builders and query kernels
   python tests/golden/make_golden.py gpu_rebin   # on a B200: the reference's
                                            # rebinRadixBuilder trees
+  python tests/golden/make_golden.py gpu_boxquery   # on a B200: the
+                                           # reference's fixedBoxQuery results
 
 Both read oracle/_ref/ (the reference compiled from its own sources by
 oracle/build_ref.sh).  Inputs are the seeded generators of
@@ -50,6 +52,13 @@ def cpu():
         n, pr = r.build(b, 8)
         ids, d = r.closest_point(n, pr, pts, qs)
         out[f"{name}_cp_ids"], out[f"{name}_cp_d"] = ids, d
+        # blacklists: exclude one id per query (here the query's own index, on
+        # queries that are data points) or every point at the query position
+        sq = pts[:400]
+        out[f"{name}_exself_ids"], out[f"{name}_exself_d"] = r.closest_point_exclude(n, pr, pts, sq)
+        exid = np.arange(400, dtype=np.int32)
+        exid[::7] = -1
+        out[f"{name}_exid_ids"], out[f"{name}_exid_d"] = r.closest_point_exclude(n, pr, pts, sq, exclude_ids=exid)
         for k in (5, 16):
             ki, kd, kn = r.knn(n, pr, pts, qs, k)
             out[f"{name}_knn{k}_ids"], out[f"{name}_knn{k}_d"], out[f"{name}_knn{k}_n"] = ki, kd, kn
@@ -127,5 +136,36 @@ def gpu_rebin():
     np.savez_compressed(dest, **out)
 
 
+def boxquery_inputs():
+    """Point boxes (uniform) and boxes with extents (GMM centres, half sizes
+    up to 0.02), each with 500 query boxes of three sizes, some outside."""
+    rng = np.random.default_rng(7)
+    u = W.point_boxes(W.uniform_points(3000))
+    g = W.gmm_points(3000, offset=0.0)
+    h = rng.uniform(0.0, 0.02, size=g.shape).astype(np.float32)
+    e = np.concatenate([g - h, g + h], 1).astype(np.float32)
+    c = W.uniform_points(500, W.SEED_QUERIES, -0.1, 1.1)
+    qh = np.repeat(np.array([0.0, 0.01, 0.08], np.float32), [100, 200, 200])[:, None] * np.ones((1, 3), np.float32)
+    q = np.concatenate([c - qh, c + qh], 1).astype(np.float32)
+    return (("u", u, q), ("e", e, q))
+
+
+def gpu_boxquery():
+    from oracle.oracle import RefGPU
+    r = RefGPU()
+    o = Oracle()
+    out = {}
+    for name, boxes, q in boxquery_inputs():
+        out[f"{name}_boxes"], out[f"{name}_queries"] = boxes, q
+        for thr in (0, 8):
+            n, pr = r.build(RefGPU.RADIX, boxes, thr)
+            cn, cp = o.canonicalize(n, pr)
+            off, ids = r.box_query(cn, cp, boxes, q)
+            out[f"{name}{thr}_nodes"], out[f"{name}{thr}_prims"] = cn.view(np.uint8), cp
+            out[f"{name}{thr}_offsets"], out[f"{name}{thr}_ids"] = off, ids
+    dest = sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu_boxquery.npz")
+    np.savez_compressed(dest, **out)
+
+
 if __name__ == "__main__":
-    {"cpu": cpu, "gpu": gpu, "gpu_rebin": gpu_rebin}[sys.argv[1]]()
+    {"cpu": cpu, "gpu": gpu, "gpu_rebin": gpu_rebin, "gpu_boxquery": gpu_boxquery}[sys.argv[1]]()

@@ -170,3 +170,47 @@ def test_full_size_10m_queries(bq, oracle):
     kdh = kd.cpu().numpy()
     assert np.all(np.diff(kdh, axis=1) >= 0) and np.all(kn.cpu().numpy() == 16)
     assert np.array_equal(kdh[:, 0], d.cpu().numpy())
+
+
+@pytest.mark.parametrize("tie", [0, 1])
+@pytest.mark.parametrize("dist", ["uniform", "gmm", "dupes"])
+def test_closest_exclude_variants_match_oracle(bq, oracle, tie, dist):
+    """findClosest_exludeID / findClosest_exludeSelf (findClosest.h:278-334)
+    with the data points as queries ("nearest other point"), bit for bit
+    against the oracle with the same tie rule; on "dupes" exclude-self
+    skips every copy of the point and exclude-id only the query's own one."""
+    pts, _ = _data(dist, 40000, 1)
+    qs = pts[::4].copy()
+    bvh = _tree(bq, "morton", pts)
+    n, pr = bvh.to_host()
+    tp, tq = torch.from_numpy(pts).cuda(), torch.from_numpy(qs).cuda()
+    qc = bq.query_config(tieMode=tie)
+    exid = np.arange(0, len(pts), 4, dtype=np.int32)
+    exid[::9] = -1
+    ids, d = bq.points.findClosest_exludeID(bvh, tp, tq, torch.from_numpy(exid), qcfg=qc)
+    oi, od = oracle.closest_point_exclude(n, pr, pts, qs, exclude_ids=exid, fma_mode=1, tie_mode=tie)
+    assert np.array_equal(ids.cpu().numpy(), oi) and np.array_equal(d.cpu().numpy(), od)
+    ids, d = bq.points.findClosest_exludeSelf(bvh, tp, tq, qcfg=qc)
+    oi, od = oracle.closest_point_exclude(n, pr, pts, qs, exclude_self=True, fma_mode=1, tie_mode=tie)
+    assert np.array_equal(ids.cpu().numpy(), oi) and np.array_equal(d.cpu().numpy(), od)
+    assert (d.cpu().numpy() > 0).all()  # no query finds a copy of itself
+
+
+@pytest.mark.parametrize("dist", ["uniform", "gmm"])
+def test_closest_exclude_variants_match_reference_kernels(bq, oracle, ref_gpu, dist):
+    """The reference's own findClosest_exludeID / _exludeSelf kernels,
+    compiled for sm_100a, on our tree: identical ids and distances under the
+    reference tie rule."""
+    pts, _ = _data(dist, 40000, 1)
+    qs = pts[1::5].copy()
+    bvh = _tree(bq, "morton", pts)
+    n, pr = bvh.to_host()
+    tp, tq = torch.from_numpy(pts).cuda(), torch.from_numpy(qs).cuda()
+    qc = bq.query_config(tieMode=1)
+    exid = np.arange(1, len(pts), 5, dtype=np.int32)
+    ids, d = bq.points.findClosest_exludeID(bvh, tp, tq, torch.from_numpy(exid), qcfg=qc)
+    ri, rd = ref_gpu.closest_point_exclude(n, pr, pts, qs, exclude_ids=exid)
+    assert np.array_equal(ids.cpu().numpy(), ri) and np.array_equal(d.cpu().numpy(), rd)
+    ids, d = bq.points.findClosest_exludeSelf(bvh, tp, tq, qcfg=qc)
+    ri, rd = ref_gpu.closest_point_exclude(n, pr, pts, qs)
+    assert np.array_equal(ids.cpu().numpy(), ri) and np.array_equal(d.cpu().numpy(), rd)

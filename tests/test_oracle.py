@@ -229,3 +229,68 @@ def test_rebin_restatement_matches_reference_gpu_trees(oracle):
             assert np.array_equal(cp, g[f"{name}_rebin{thr}_prims"]), (name, thr)
             assert cn.tobytes() == ref.tobytes(), (name, thr)
             check_tree(n, pr, b, max_leaf=max(thr, 32))
+
+
+def test_exclude_blacklists_match_reference(oracle):
+    """findClosest_exludeID / findClosest_exludeSelf (findClosest.h:278-334)
+    restated in the oracle, against the reference's host code: 400 queries
+    that are data points, excluding their own index (every 7th: -1, nothing
+    excluded) or every point at their position."""
+    g = _load("ref_cpu.npz")
+    p, q, gp, gq, *_ = _inputs()
+    for name, pts in (("u", p), ("g", gp)):
+        n = g[f"{name}_cpu8_nodes"].view(NODE)
+        pr = g[f"{name}_cpu8_prims"]
+        sq = pts[:400]
+        ids, d = oracle.closest_point_exclude(n, pr, pts, sq, exclude_self=True, fma_mode=0, tie_mode=1)
+        assert np.array_equal(ids, g[f"{name}_exself_ids"]) and np.array_equal(d, g[f"{name}_exself_d"])
+        exid = np.arange(400, dtype=np.int32)
+        exid[::7] = -1
+        ids, d = oracle.closest_point_exclude(n, pr, pts, sq, exclude_ids=exid, fma_mode=0, tie_mode=1)
+        assert np.array_equal(ids, g[f"{name}_exid_ids"]) and np.array_equal(d, g[f"{name}_exid_d"])
+        assert (ids[exid >= 0] != exid[exid >= 0]).all()
+
+
+def _brute_box(boxes, q):
+    lo, hi = boxes[:, :3], boxes[:, 3:]
+    return ~((q[None, 3:] < lo).any(1) | (hi < q[None, :3]).any(1))
+
+
+def test_box_query_oracle_matches_brute_force(oracle):
+    """fixedBoxQuery restated (fixedBoxQuery.h:73-156, per-prim box test):
+    each query's prims are exactly the closed-interval overlaps, each once;
+    point boxes and boxes with extents, several leaf sizes, query boxes
+    that are points, small, large, outside everything or inverted."""
+    rng = np.random.default_rng(3)
+    c = W.gmm_points(4000, offset=0.0)
+    h = rng.uniform(0, 0.01, size=c.shape).astype(np.float32)
+    for boxes in (boxes_np(W.uniform_points(4000)), np.concatenate([c - h, c + h], 1).astype(np.float32)):
+        qc = W.uniform_points(300, W.SEED_QUERIES, -0.2, 1.2)
+        qh = rng.choice(np.float32([0, 0.005, 0.05, 0.3, -0.01]), size=(300, 1)).astype(np.float32)
+        q = np.concatenate([qc - qh, qc + qh], 1).astype(np.float32)
+        q[0] = [5, 5, 5, 6, 6, 6]
+        q[1] = [-1, -1, -1, 2, 2, 2]
+        for thr in (0, 1, 8):
+            n, pr = oracle.radix_build(boxes, thr)
+            off, ids = oracle.box_query(n, pr, boxes, q)
+            assert off[0] == 0 and off[1] == 0 and off[2] - off[1] == len(boxes)
+            for i in range(len(q)):
+                got = ids[off[i]:off[i + 1]]
+                assert len(np.unique(got)) == len(got)
+                assert np.array_equal(np.sort(got), np.nonzero(_brute_box(boxes, q[i]))[0]), (thr, i)
+
+
+def test_box_query_matches_reference_gpu_fixtures(oracle):
+    """The oracle's box query against the reference's fixedBoxQuery kernel
+    run on a B200 (fixtures over the reference's radix trees, BFS
+    renumbered): same prims in the same visiting order."""
+    g = _load("ref_gpu_boxquery.npz")
+    for name in ("u", "e"):
+        boxes, q = g[f"{name}_boxes"], g[f"{name}_queries"]
+        for thr in (0, 8):
+            n = g[f"{name}{thr}_nodes"].view(NODE)
+            pr = g[f"{name}{thr}_prims"]
+            off, ids = oracle.box_query(n, pr, boxes, q)
+            assert np.array_equal(off, g[f"{name}{thr}_offsets"]), (name, thr)
+            assert np.array_equal(ids, g[f"{name}{thr}_ids"]), (name, thr)
+            assert off[-1] > 2 * len(q)
