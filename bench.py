@@ -300,6 +300,18 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
         bq.points.findClosest(bvh, tp, qs)
         bq.points.findKNN(bvh, tp, qs, 16)
     comp["query_phases_ms"] = {k: round(v[1], 4) for k, v in prof.table.items()}
+    # wide trees: gpuBuilder(WideBVH<float,3,W>) with the default config (leaf 1) and closest point
+    for width in (4, 8):
+        ms_b = ev_time(lambda: bq.gpuBuilderWide(boxes_t, width).free())
+        wb = bq.gpuBuilderWide(boxes_t, width)
+        ms_q = ev_time(lambda: bq.points.findClosest(wb, tp, qs))
+        with bq.profile() as prof:
+            bq.gpuBuilderWide(boxes_t, width).free()
+            bq.points.findClosest(wb, tp, qs)
+        comp[f"wide{width}"] = {"build_ms": ms_b, "build_Mprims_s": n / ms_b / 1e3, "wide_nodes": wb.numNodes,
+                                "closest_point_ms": ms_q, "Mqueries_s": n / ms_q / 1e3, "queries": n,
+                                "phases_ms": {k: round(v[1], 4) for k, v in prof.table.items()}}
+        wb.free()
     del qs
     # nearest other point of every data point (findClosest_exludeSelf)
     ms = ev_time(lambda: bq.points.findClosest_exludeSelf(bvh, tp, tp))
@@ -508,6 +520,10 @@ def reference_gpu(comp, pts_np, W):
     out["findClosest_ms"] = r.time_query(RefGPU.RADIX, pts_np, qs, 0, reps=2)
     out["findKNN16_ms"] = r.time_query(RefGPU.RADIX, pts_np, qs, 16, reps=2)
     out["findClosest_exludeSelf_ms"] = r.time_query(RefGPU.RADIX, pts_np, pts_np, -1, reps=2)
+    out["gpuBuilder_wide4_ms"] = r.time_build(RefGPU.WIDE4, pts_np, 0, reps=2)
+    out["gpuBuilder_wide8_ms"] = r.time_build(RefGPU.WIDE8, pts_np, 0, reps=2)
+    out["findClosest_wide4_ms"] = r.time_wide_query(4, pts_np, qs, 0, reps=2)
+    out["findClosest_wide8_ms"] = r.time_wide_query(8, pts_np, qs, 0, reps=2)
     out["fixedBoxQuery_count_fill_ms"], out["fixedBoxQuery_results"] = r.time_box_query(
         RefGPU.RADIX, pts_np, box_queries(W, 1_000_000), reps=2)
     out["note"] = "reference kernels compiled for sm_100a, same points, one thread per query <<<ceil(Q/128),128>>>"

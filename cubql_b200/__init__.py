@@ -55,6 +55,11 @@ class bq_bvh3f(ctypes.Structure):
                 ("primIDs", ctypes.c_void_p), ("numPrims", ctypes.c_uint32)]
 
 
+class bq_wide_bvh3f(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_void_p), ("numNodes", ctypes.c_uint32), ("primIDs", ctypes.c_void_p),
+                ("numPrims", ctypes.c_uint32)]
+
+
 class bq_build_config(ctypes.Structure):
     _fields_ = [("maxAllowedLeafSize", ctypes.c_int), ("makeLeafThreshold", ctypes.c_int),
                 ("buildMethod", ctypes.c_int)]
@@ -102,6 +107,17 @@ _SIGS = {
     "bq_box_query_count_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _P, ctypes.POINTER(bq_allocator), _P],
     "bq_box_query_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _P, ctypes.c_uint64, _P, ctypes.POINTER(bq_allocator),
                         _P],
+    "bq_build_wide_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, _P, _U, ctypes.POINTER(bq_build_config),
+                         ctypes.POINTER(bq_allocator), _P],
+    "bq_collapse_wide_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, ctypes.POINTER(bq_bvh3f), ctypes.POINTER(bq_allocator),
+                            _P],
+    "bq_wide_free_f3": [ctypes.POINTER(bq_wide_bvh3f), ctypes.POINTER(bq_allocator), _P],
+    "bq_wide_closest_point_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, _P, _P, _U, _F, ctypes.POINTER(bq_query_config),
+                                 _P, _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_wide_box_query_count_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, _P, _P, _U, _P, ctypes.POINTER(bq_allocator),
+                                   _P],
+    "bq_wide_box_query_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, _P, _P, _U, _P, ctypes.c_uint64, _P,
+                             ctypes.POINTER(bq_allocator), _P],
     "bq_knn_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _I, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
                   ctypes.POINTER(bq_allocator), _P],
     "bq_tri_closest_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _P, _U, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
@@ -263,6 +279,40 @@ class BinaryBVH:
             _check(_lib.bq_free_f3(ctypes.byref(self.c), ctypes.byref(self.allocator.c), _stream()))
 
 
+class WideBVH:
+    """WideBVH<float,3,width>: numNodes wide nodes of `width` 32-byte slots
+    (box + valid/offset/count word) and primIDs in device memory."""
+
+    def __init__(self, c, width, allocator):
+        self.c = c
+        self.width = width
+        self.allocator = allocator
+
+    @property
+    def numNodes(self):
+        return self.c.numNodes
+
+    @property
+    def numPrims(self):
+        return self.c.numPrims
+
+    def to_host(self):
+        """(slots as a numpy structured array of numNodes*width records whose
+        `admin` field is the slot word, primIDs as uint32)."""
+        import numpy as np
+        torch.cuda.synchronize()
+        if self.c.numNodes == 0:
+            return np.zeros(0, dtype=node_dtype()), np.zeros(0, dtype=np.uint32)
+        slots = self.allocator.view(self.c.nodes, torch.float32, 8 * self.width * self.c.numNodes)
+        slots = slots.cpu().numpy().view(node_dtype()).reshape(-1)
+        prims = self.allocator.view(self.c.primIDs, torch.int32, self.c.numPrims).cpu().numpy().view(np.uint32)
+        return slots, prims
+
+    def free(self):
+        if self.c.nodes or self.c.primIDs:
+            _check(_lib.bq_wide_free_f3(ctypes.byref(self.c), ctypes.byref(self.allocator.c), _stream()))
+
+
 def _as_boxes(boxes):
     if boxes.dtype != torch.float32 or not boxes.is_cuda:
         raise TypeError("boxes must be a float32 CUDA tensor of shape (N, 6)")
@@ -283,6 +333,27 @@ def _build(fn, boxes, config, allocator):
 def gpuBuilder(boxes, config=None, allocator=None):
     """cuBQL::gpuBuilder (cuBQL/builder/cuda.h:91-99): spatial-median build."""
     return _build(_lib.bq_build_spatial_median_f3, boxes, config, allocator)
+
+
+def gpuBuilderWide(boxes, width=4, config=None, allocator=None):
+    """cuBQL::gpuBuilder(WideBVH<float,3,width>&, ...) (cuBQL/builder/cuda.h:100-116,
+    cuBQL/builder/cuda/wide_gpu_builder.h:162-213): spatial-median build
+    collapsed to `width` (2, 4 or 8) children per node."""
+    boxes = _as_boxes(boxes)
+    allocator = allocator or default_allocator()
+    cfg = (config or BuildConfig()).c()
+    c = bq_wide_bvh3f()
+    _check(_lib.bq_build_wide_f3(ctypes.byref(c), width, _ptr(boxes), boxes.shape[0], ctypes.byref(cfg),
+                                 ctypes.byref(allocator.c), _stream()))
+    return WideBVH(c, width, allocator)
+
+
+def collapse(bvh, width=4):
+    """bq_collapse_wide_f3: a WideBVH from any BinaryBVH (own primIDs copy)."""
+    c = bq_wide_bvh3f()
+    _check(_lib.bq_collapse_wide_f3(ctypes.byref(c), width, ctypes.byref(bvh.c), ctypes.byref(bvh.allocator.c),
+                                    _stream()))
+    return WideBVH(c, width, bvh.allocator)
 
 
 def refit(bvh, boxes):
@@ -332,6 +403,11 @@ class points:
         ids = torch.empty(nq, dtype=torch.int32, device=queries.device)
         d = torch.empty(nq, dtype=torch.float32, device=queries.device)
         q = qcfg or query_config()
+        if isinstance(bvh, WideBVH):  # findClosest(WideBVH) (findClosest.h:363-386)
+            _check(_lib.bq_wide_closest_point_f3(ctypes.byref(bvh.c), bvh.width, _ptr(data), _ptr(queries), nq,
+                                                 maxSqrDist, ctypes.byref(q), _ptr(ids), _ptr(d),
+                                                 ctypes.byref(bvh.allocator.c), _stream()))
+            return ids, d
         _check(_lib.bq_closest_point_f3(ctypes.byref(bvh.c), _ptr(data), _ptr(queries), nq, maxSqrDist,
                                         ctypes.byref(q), _ptr(ids), _ptr(d), ctypes.byref(bvh.allocator.c),
                                         _stream()))
@@ -394,6 +470,10 @@ class fixedBoxQuery:
         boxes, queryBoxes = _as_boxes(boxes), _as_boxes(queryBoxes)
         nq = queryBoxes.shape[0]
         counts = torch.empty(nq, dtype=torch.int32, device=queryBoxes.device)
+        if isinstance(bvh, WideBVH):
+            _check(_lib.bq_wide_box_query_count_f3(ctypes.byref(bvh.c), bvh.width, _ptr(boxes), _ptr(queryBoxes), nq,
+                                                   _ptr(counts), ctypes.byref(bvh.allocator.c), _stream()))
+            return counts
         _check(_lib.bq_box_query_count_f3(ctypes.byref(bvh.c), _ptr(boxes), _ptr(queryBoxes), nq, _ptr(counts),
                                           ctypes.byref(bvh.allocator.c), _stream()))
         return counts
@@ -413,6 +493,11 @@ class fixedBoxQuery:
             raise BQError(1, "box query results exceed 2^32 entries")
         ids = torch.empty(max(total, 1), dtype=torch.int32, device=queryBoxes.device)
         off32 = offsets[:-1].to(torch.int32).contiguous()
+        if isinstance(bvh, WideBVH):
+            _check(_lib.bq_wide_box_query_f3(ctypes.byref(bvh.c), bvh.width, _ptr(boxes), _ptr(queryBoxes), nq,
+                                             _ptr(off32), total, _ptr(ids), ctypes.byref(bvh.allocator.c),
+                                             _stream()))
+            return offsets, ids[:total]
         _check(_lib.bq_box_query_f3(ctypes.byref(bvh.c), _ptr(boxes), _ptr(queryBoxes), nq, _ptr(off32), total,
                                     _ptr(ids), ctypes.byref(bvh.allocator.c), _stream()))
         return offsets, ids[:total]

@@ -10,13 +10,18 @@
 // lambda is done here against the prim boxes, so a query reports exactly
 // the prims whose boxes overlap its box, in the reference's visiting order.
 //
+// Over a WideBVH (fixedBoxQuery.h:161-277) the walk is depth first over
+// the slots of each wide node in order: a valid slot whose box overlaps is
+// entered (an inner slot pushes the resume point, node and next slot) or
+// its leaf visited.
+//
 // One thread per query.  Two passes with the same traversal: k_box_count
 // (how many prims per query) and k_box_fill (their ids at the caller's
 // per-query offsets).  Every stack push is bounded; a query whose traversal
 // would need more than BOX_STACK entries is reported with DEV_ERR_STACK
 // and its count set to 0 (the reference's fixed 64-entry stack would
 // overflow silently).
-#include "bq_internal.cuh"
+#include "bq_wide.cuh"
 
 namespace bq {
 namespace {
@@ -74,6 +79,58 @@ __device__ __forceinline__ bool box_traverse(const Node *__restrict__ nodes, con
   }
 }
 
+// fixedBoxQuery::forEachLeaf over a WideBVH (:161-230), same contract as
+// box_traverse.  A stack entry is (wide node << 8 | slot to resume at).
+template <int W, typename Fn>
+__device__ __forceinline__ bool wide_box_traverse(const Node *__restrict__ slots, const uint32_t *__restrict__ primIDs,
+                                                  const bq_box3f *__restrict__ boxes, const float q[6], Fn &fn)
+{
+  uint64_t stack[BOX_STACK];
+  int sp = 0;
+  uint64_t node = 0;
+  uint32_t c = 0;
+  while (true) {
+    const Node sl = ldg_node(slots + node * W + c);
+    const uint64_t word = node_admin(sl);
+    if (wslot_valid(word) && box_overlaps(q, sl.a.x, sl.a.y, sl.a.z, sl.a.w, sl.b.x, sl.b.y)) {
+      const uint32_t cnt = wslot_count(word);
+      if (cnt == 0) {
+        if (c + 1 < W) {
+          if (sp >= BOX_STACK) return false;
+          stack[sp++] = (node << 8) | (c + 1);
+        }
+        node = wslot_offset(word);
+        c = 0;
+        continue;
+      }
+      const uint64_t off = wslot_offset(word);
+      for (uint32_t j = 0; j < cnt; j++) {
+        const uint32_t pid = __ldg(primIDs + off + j);
+        const bq_box3f b = boxes[pid];
+        if (box_overlaps(q, b.lower[0], b.lower[1], b.lower[2], b.upper[0], b.upper[1], b.upper[2])) fn(pid);
+      }
+    }
+    if (c + 1 < W) {
+      c++;
+    } else if (sp > 0) {
+      const uint64_t e = stack[--sp];
+      node = e >> 8;
+      c = (uint32_t)(e & 0xFF);
+    } else {
+      return true;
+    }
+  }
+}
+
+// W == 0: binary tree, else a W-wide tree
+template <int W, typename Fn>
+__device__ __forceinline__ bool any_box_traverse(const Node *__restrict__ nodes, const uint32_t *__restrict__ primIDs,
+                                                 const bq_box3f *__restrict__ boxes, const float q[6], Fn &fn)
+{
+  if constexpr (W == 0) return box_traverse(nodes, primIDs, boxes, q, fn);
+  else return wide_box_traverse<W>(nodes, primIDs, boxes, q, fn);
+}
+
 __device__ __forceinline__ void load_query(const bq_box3f *__restrict__ qb, uint32_t i, float q[6])
 {
   const bq_box3f b = qb[i];
@@ -81,6 +138,7 @@ __device__ __forceinline__ void load_query(const bq_box3f *__restrict__ qb, uint
   q[3] = b.upper[0]; q[4] = b.upper[1]; q[5] = b.upper[2];
 }
 
+template <int W>
 __global__ void __launch_bounds__(128) k_box_count(const Node *__restrict__ nodes, const uint32_t *__restrict__ primIDs,
                                                    const bq_box3f *__restrict__ boxes,
                                                    const bq_box3f *__restrict__ queryBoxes, uint32_t nq,
@@ -92,13 +150,14 @@ __global__ void __launch_bounds__(128) k_box_count(const Node *__restrict__ node
   load_query(queryBoxes, i, q);
   uint32_t c = 0;
   auto fn = [&](uint32_t) { c++; };
-  if (!box_traverse(nodes, primIDs, boxes, q, fn)) {
+  if (!any_box_traverse<W>(nodes, primIDs, boxes, q, fn)) {
     c = 0;
     atomicOr(err, DEV_ERR_STACK);
   }
   counts[i] = c;
 }
 
+template <int W>
 __global__ void __launch_bounds__(128) k_box_fill(const Node *__restrict__ nodes, const uint32_t *__restrict__ primIDs,
                                                   const bq_box3f *__restrict__ boxes,
                                                   const bq_box3f *__restrict__ queryBoxes, uint32_t nq,
@@ -117,7 +176,50 @@ __global__ void __launch_bounds__(128) k_box_fill(const Node *__restrict__ nodes
     if (at < end) ids[at++] = (int32_t)pid;
     else over = true;
   };
-  if (!box_traverse(nodes, primIDs, boxes, q, fn) || over) atomicOr(err, over ? DEV_ERR_RANGE : DEV_ERR_STACK);
+  if (!any_box_traverse<W>(nodes, primIDs, boxes, q, fn) || over) atomicOr(err, over ? DEV_ERR_RANGE : DEV_ERR_STACK);
+}
+
+
+template <int W>
+int count_impl(const Node *nodes, const uint32_t *primIDs, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+               uint32_t nq, uint32_t *counts, Alloc &al)
+{
+  TempSet tmp(al);
+  uint32_t *err = nullptr;
+  BQ_TRY(tmp.get(&err, 1));
+  BQ_CUDA(cudaMemsetAsync(err, 0, 4, al.s));
+  {
+    ProfScope ps("boxquery.count", al.s);
+    k_box_count<W><<<div_up(nq, 128), 128, 0, al.s>>>(nodes, primIDs, boxes, queryBoxes, nq, counts, err);
+  }
+  BQ_CUDA(cudaGetLastError());
+  uint32_t herr = 0;
+  BQ_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, al.s));
+  BQ_CUDA(cudaStreamSynchronize(al.s));
+  if (herr) return set_error(BQ_ERR_STACK_OVERFLOW, "a box query needed more than 128 traversal stack entries");
+  return BQ_OK;
+}
+
+template <int W>
+int fill_impl(const Node *nodes, const uint32_t *primIDs, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+              uint32_t nq, const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al)
+{
+  TempSet tmp(al);
+  uint32_t *err = nullptr;
+  BQ_TRY(tmp.get(&err, 1));
+  BQ_CUDA(cudaMemsetAsync(err, 0, 4, al.s));
+  {
+    ProfScope ps("boxquery.fill", al.s);
+    k_box_fill<W><<<div_up(nq, 128), 128, 0, al.s>>>(nodes, primIDs, boxes, queryBoxes, nq, offsets, capacity, ids,
+                                                      err);
+  }
+  BQ_CUDA(cudaGetLastError());
+  uint32_t herr = 0;
+  BQ_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, al.s));
+  BQ_CUDA(cudaStreamSynchronize(al.s));
+  if (herr & DEV_ERR_RANGE) return set_error(BQ_ERR_INVALID_ARGUMENT, "box query results exceed the given offsets");
+  if (herr) return set_error(BQ_ERR_STACK_OVERFLOW, "a box query needed more than 128 traversal stack entries");
+  return BQ_OK;
 }
 
 } // namespace
@@ -130,43 +232,40 @@ int box_query_count(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *
     BQ_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nq, al.s));
     return BQ_OK;
   }
-  TempSet tmp(al);
-  uint32_t *err = nullptr;
-  BQ_TRY(tmp.get(&err, 1));
-  BQ_CUDA(cudaMemsetAsync(err, 0, 4, al.s));
-  {
-    ProfScope ps("boxquery.count", al.s);
-    k_box_count<<<div_up(nq, 128), 128, 0, al.s>>>((const Node *)bvh->nodes, bvh->primIDs, boxes, queryBoxes, nq,
-                                                    counts, err);
-  }
-  BQ_CUDA(cudaGetLastError());
-  uint32_t herr = 0;
-  BQ_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, al.s));
-  BQ_CUDA(cudaStreamSynchronize(al.s));
-  if (herr) return set_error(BQ_ERR_STACK_OVERFLOW, "a box query needed more than 128 traversal stack entries");
-  return BQ_OK;
+  return count_impl<0>((const Node *)bvh->nodes, bvh->primIDs, boxes, queryBoxes, nq, counts, al);
 }
 
 int box_query_fill(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t nq,
                    const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al)
 {
   if (nq == 0 || bvh->numNodes == 0) return BQ_OK;
-  TempSet tmp(al);
-  uint32_t *err = nullptr;
-  BQ_TRY(tmp.get(&err, 1));
-  BQ_CUDA(cudaMemsetAsync(err, 0, 4, al.s));
-  {
-    ProfScope ps("boxquery.fill", al.s);
-    k_box_fill<<<div_up(nq, 128), 128, 0, al.s>>>((const Node *)bvh->nodes, bvh->primIDs, boxes, queryBoxes, nq,
-                                                   offsets, capacity, ids, err);
+  return fill_impl<0>((const Node *)bvh->nodes, bvh->primIDs, boxes, queryBoxes, nq, offsets, capacity, ids, al);
+}
+
+int wide_box_query_count(const bq_wide_bvh3f *bvh, int W, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                         uint32_t nq, uint32_t *counts, Alloc &al)
+{
+  if (W != 2 && W != 4 && W != 8) return set_error(BQ_ERR_INVALID_ARGUMENT, "width must be 2, 4 or 8");
+  if (nq == 0) return BQ_OK;
+  if (bvh->numNodes == 0) {
+    BQ_CUDA(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nq, al.s));
+    return BQ_OK;
   }
-  BQ_CUDA(cudaGetLastError());
-  uint32_t herr = 0;
-  BQ_CUDA(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, al.s));
-  BQ_CUDA(cudaStreamSynchronize(al.s));
-  if (herr & DEV_ERR_RANGE) return set_error(BQ_ERR_INVALID_ARGUMENT, "box query results exceed the given offsets");
-  if (herr) return set_error(BQ_ERR_STACK_OVERFLOW, "a box query needed more than 128 traversal stack entries");
-  return BQ_OK;
+  const Node *n = (const Node *)bvh->nodes;
+  if (W == 2) return count_impl<2>(n, bvh->primIDs, boxes, queryBoxes, nq, counts, al);
+  if (W == 4) return count_impl<4>(n, bvh->primIDs, boxes, queryBoxes, nq, counts, al);
+  return count_impl<8>(n, bvh->primIDs, boxes, queryBoxes, nq, counts, al);
+}
+
+int wide_box_query_fill(const bq_wide_bvh3f *bvh, int W, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                        uint32_t nq, const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al)
+{
+  if (W != 2 && W != 4 && W != 8) return set_error(BQ_ERR_INVALID_ARGUMENT, "width must be 2, 4 or 8");
+  if (nq == 0 || bvh->numNodes == 0) return BQ_OK;
+  const Node *n = (const Node *)bvh->nodes;
+  if (W == 2) return fill_impl<2>(n, bvh->primIDs, boxes, queryBoxes, nq, offsets, capacity, ids, al);
+  if (W == 4) return fill_impl<4>(n, bvh->primIDs, boxes, queryBoxes, nq, offsets, capacity, ids, al);
+  return fill_impl<8>(n, bvh->primIDs, boxes, queryBoxes, nq, offsets, capacity, ids, al);
 }
 
 } // namespace bq

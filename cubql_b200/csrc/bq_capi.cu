@@ -13,6 +13,14 @@ int box_query_count(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *
                     uint32_t *counts, Alloc &al);
 int box_query_fill(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t nq,
                    const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al);
+int wide_box_query_count(const bq_wide_bvh3f *bvh, int W, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                         uint32_t nq, uint32_t *counts, Alloc &al);
+int wide_box_query_fill(const bq_wide_bvh3f *bvh, int W, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                        uint32_t nq, const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al);
+int collapse_wide(const bq_bvh3f *bin, int W, bq_wide_bvh3f *out, bool copyPrims, Alloc &al);
+int build_wide(bq_wide_bvh3f *out, int W, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
+int wide_closest_point(const bq_wide_bvh3f *bvh, int W, const float *points, const float *queries, uint32_t nq,
+                       float maxSqr, const bq_query_config *qcfg, int32_t *ids, float *d, Alloc &al);
 int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
                   const bq_query_config *qcfg, int32_t *ids, float *d, Alloc &al,
                   const int32_t *excludeIds = nullptr, int excludeSelf = 0);
@@ -80,6 +88,17 @@ int check_tree(const bq_bvh3f *bvh)
   return BQ_OK;
 }
 
+int check_wide(const bq_wide_bvh3f *bvh, int width)
+{
+  if (!bvh) return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh is NULL");
+  if (width != 2 && width != 4 && width != 8) return set_error(BQ_ERR_INVALID_ARGUMENT, "width must be 2, 4 or 8");
+  if (bvh->numNodes && (!bvh->nodes || !bvh->primIDs))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh has nodes but NULL arrays");
+  if (bvh->numNodes && misaligned(bvh->nodes, 16))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh->nodes must be 16-byte aligned");
+  return BQ_OK;
+}
+
 int check_build(const bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n)
 {
   if (!bvh) return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh is NULL");
@@ -140,6 +159,73 @@ int bq_free_f3(bq_bvh3f *bvh, const bq_allocator *alloc, bq_stream_t stream)
   bvh->numNodes = 0;
   bvh->numPrims = 0;
   return s1 != BQ_OK ? s1 : s2;
+}
+
+int bq_build_wide_f3(bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes, uint32_t numPrims,
+                     const bq_build_config *cfg, const bq_allocator *alloc, bq_stream_t stream)
+{
+  if (!bvh) return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh is NULL");
+  bq_bvh3f probe{};
+  BQ_TRY(check_build(&probe, boxes, numPrims));
+  if (cfg && cfg->buildMethod != BQ_SPATIAL_MEDIAN)
+    return set_error(BQ_ERR_UNSUPPORTED, "wide trees are built by the spatial-median method (collapse others)");
+  Alloc al = make_alloc(alloc, stream);
+  return build_wide(bvh, width, boxes, numPrims, cfg, al);
+}
+
+int bq_collapse_wide_f3(bq_wide_bvh3f *wide, int width, const bq_bvh3f *binary, const bq_allocator *alloc,
+                        bq_stream_t stream)
+{
+  if (!wide) return set_error(BQ_ERR_INVALID_ARGUMENT, "wide is NULL");
+  BQ_TRY(check_tree(binary));
+  Alloc al = make_alloc(alloc, stream);
+  return collapse_wide(binary, width, wide, true, al);
+}
+
+int bq_wide_free_f3(bq_wide_bvh3f *bvh, const bq_allocator *alloc, bq_stream_t stream)
+{
+  if (!bvh) return set_error(BQ_ERR_INVALID_ARGUMENT, "bvh is NULL");
+  Alloc al = make_alloc(alloc, stream);
+  int s1 = al.free_bytes(bvh->primIDs);
+  int s2 = al.free_bytes(bvh->nodes);
+  bvh->primIDs = nullptr;
+  bvh->nodes = nullptr;
+  bvh->numNodes = 0;
+  bvh->numPrims = 0;
+  return s1 != BQ_OK ? s1 : s2;
+}
+
+int bq_wide_closest_point_f3(const bq_wide_bvh3f *bvh, int width, const float *points, const float *queries,
+                             uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg, int32_t *ids,
+                             float *sqrDist, const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_wide(bvh, width));
+  if (numQueries && (!queries || !ids || !sqrDist || (bvh->numNodes && !points)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return wide_closest_point(bvh, width, points, queries, numQueries, maxSqrDist, qcfg, ids, sqrDist, al);
+}
+
+int bq_wide_box_query_count_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes,
+                               const bq_box3f *queryBoxes, uint32_t numQueries, uint32_t *counts,
+                               const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_wide(bvh, width));
+  if (numQueries && (!queryBoxes || !counts || (bvh->numNodes && !boxes)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return wide_box_query_count(bvh, width, boxes, queryBoxes, numQueries, counts, al);
+}
+
+int bq_wide_box_query_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                         uint32_t numQueries, const uint32_t *offsets, uint64_t capacity, int32_t *ids,
+                         const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_wide(bvh, width));
+  if (numQueries && (!queryBoxes || !offsets || (bvh->numNodes && !boxes) || (capacity && !ids)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return wide_box_query_fill(bvh, width, boxes, queryBoxes, numQueries, offsets, capacity, ids, al);
 }
 
 int bq_closest_point_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries,

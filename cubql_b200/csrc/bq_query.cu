@@ -18,22 +18,19 @@
 //                  answer (the reference returns early, :475-478)
 #include <algorithm>
 
-#include "bq_traverse.cuh"
+#include "bq_query.cuh"
 
 namespace bq {
 namespace {
 
-constexpr int DEEP_THREADS = 2048;
-constexpr int DEEP_STACK = 1024;
-
-__global__ void k_query_keys(const Node *__restrict__ nodes, const float *__restrict__ queries, uint32_t nq,
+// rootBox: lower xyz, upper xyz (the first 24 bytes of a binary root node)
+__global__ void k_query_keys(const float *__restrict__ rootBox, const float *__restrict__ queries, uint32_t nq,
                              uint32_t *__restrict__ keys, uint32_t *__restrict__ idx)
 {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
-  const Node root = ldg_node(nodes);
-  const float lx = root.a.x, ly = root.a.y, lz = root.a.z;
-  const float ext = fmaxf(fmaxf(root.a.w - lx, root.b.x - ly), root.b.y - lz);
+  const float lx = __ldg(rootBox), ly = __ldg(rootBox + 1), lz = __ldg(rootBox + 2);
+  const float ext = fmaxf(fmaxf(__ldg(rootBox + 3) - lx, __ldg(rootBox + 4) - ly), __ldg(rootBox + 5) - lz);
   const float sc = 1024.0f / fmaxf(ext, 1e-20f);
   const float *q = queries + 3ull * t;
   const uint32_t cx = min(__float2uint_rz((q[0] - lx) * sc), 1023u);
@@ -42,45 +39,6 @@ __global__ void k_query_keys(const Node *__restrict__ nodes, const float *__rest
   keys[t] = spread10(cx) | (spread10(cy) << 1) | (spread10(cz) << 2);
   idx[t] = t;
 }
-
-// ------------------------------------------------------------------
-// closest point
-// ------------------------------------------------------------------
-template <int TIE>
-struct CPLeaf {
-  const uint32_t *__restrict__ primIDs;
-  const float *__restrict__ points;
-  float qx, qy, qz;
-  float best;
-  int32_t id;
-  int32_t skipId;  // blacklisted prim (findClosest_exludeID), -1: none
-  int skipSelf;    // skip points equal to the query (findClosest_exludeSelf)
-  __device__ __forceinline__ float operator()(uint64_t off, uint32_t cnt)
-  {
-    for (uint32_t j = 0; j < cnt; j++) {
-      const uint32_t pid = __ldg(primIDs + off + j);
-      const float *p = points + 3ull * pid;
-      const float px = __ldg(p), py = __ldg(p + 1), pz = __ldg(p + 2);
-      // blacklisted candidates are passed over (findClosest.h:200-203)
-      if ((int32_t)pid == skipId || (skipSelf && px == qx && py == qy && pz == qz)) continue;
-      const float d = sqr_pp(px, py, pz, qx, qy, qz);
-      const bool take = (TIE == TIE_REFERENCE) ? (d < best)  // findClosest.h:211-218
-                                               : (d < best || (d == best && id >= 0 && (int32_t)pid < id));
-      if (take) {
-        best = d;
-        id = (int32_t)pid;
-      }
-    }
-    return best;
-  }
-};
-
-// blacklist of a closest-point call: per-query excluded ids, or points
-// equal to the query
-struct CpExclude {
-  const int32_t *ids;
-  int self;
-};
 
 template <int TIE, typename Stack>
 __device__ __forceinline__ bool run_cp(const Node *nodes, const uint32_t *primIDs, const float *points,
@@ -223,62 +181,6 @@ __global__ void k_knn_deep(const Node *__restrict__ nodes, const uint32_t *__res
   }
 }
 
-__global__ void k_fill_empty(uint32_t nq, int k, int32_t *ids, float *d, int32_t *numFound)
-{
-  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (uint64_t)nq * k) return;
-  ids[t] = -1;
-  d[t] = INFINITY;
-  if (numFound && t < nq) numFound[t] = 0;
-}
-
-// ------------------------------------------------------------------
-// host side
-// ------------------------------------------------------------------
-struct QueryScratch {
-  uint32_t *order = nullptr;
-  uint32_t *ovfList = nullptr, *ovfCount = nullptr, *err = nullptr;
-  StackEntry *deep = nullptr;
-};
-
-int prepare(const bq_bvh3f *bvh, const float *queries, uint32_t nq, bool reorder, TempSet &tmp, Alloc &al,
-            QueryScratch &qs)
-{
-  BQ_TRY(tmp.get(&qs.ovfList, nq));
-  BQ_TRY(tmp.get(&qs.ovfCount, 2));
-  qs.err = qs.ovfCount + 1;
-  BQ_TRY(tmp.get(&qs.deep, (size_t)DEEP_THREADS * DEEP_STACK));
-  BQ_CUDA(cudaMemsetAsync(qs.ovfCount, 0, 8, al.s));
-  if (reorder && nq > 1) {
-    uint32_t *keys[2], *idx[2];
-    BQ_TRY(tmp.get(&keys[0], nq));
-    BQ_TRY(tmp.get(&keys[1], nq));
-    BQ_TRY(tmp.get(&idx[0], nq));
-    BQ_TRY(tmp.get(&idx[1], nq));
-    {
-      ProfScope ps("query.keys", al.s);
-      k_query_keys<<<div_up(nq, 256), 256, 0, al.s>>>((const Node *)bvh->nodes, queries, nq, keys[0], idx[0]);
-    }
-    BQ_CUDA(cudaGetLastError());
-    int sel = 0;
-    // the order only steers performance: the top 24 key bits (3 passes) suffice
-    BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, 6, 30, nullptr, &sel, qs.err, al));
-    qs.order = idx[sel];
-  }
-  return BQ_OK;
-}
-
-int finish(QueryScratch &qs, Alloc &al)
-{
-  // the only host synchronisation: read the device error word
-  uint32_t err = 0;
-  BQ_CUDA(cudaMemcpyAsync(&err, qs.err, 4, cudaMemcpyDeviceToHost, al.s));
-  BQ_CUDA(cudaStreamSynchronize(al.s));
-  if (err & DEV_ERR_STACK) return set_error(BQ_ERR_STACK_OVERFLOW, "query exceeded the deep fallback stack");
-  if (err & DEV_ERR_TIMEOUT) return set_error(BQ_ERR_TIMEOUT, "query reordering sort timed out");
-  return BQ_OK;
-}
-
 template <int TIE, int STACK>
 void launch_cp(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
                int block, int32_t *ids, float *d, QueryScratch &qs, cudaStream_t s, CpExclude ex)
@@ -332,6 +234,53 @@ void dispatch_knn_tie(int tie, int stack, const bq_bvh3f *bvh, const float *poin
 
 } // namespace
 
+__global__ void k_fill_empty(uint32_t nq, int k, int32_t *ids, float *d, int32_t *numFound)
+{
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (uint64_t)nq * k) return;
+  ids[t] = -1;
+  d[t] = INFINITY;
+  if (numFound && t < nq) numFound[t] = 0;
+}
+
+int prepare_queries(const float *rootBox, const float *queries, uint32_t nq, bool reorder, TempSet &tmp, Alloc &al,
+                    QueryScratch &qs)
+{
+  BQ_TRY(tmp.get(&qs.ovfList, nq));
+  BQ_TRY(tmp.get(&qs.ovfCount, 2));
+  qs.err = qs.ovfCount + 1;
+  BQ_TRY(tmp.get(&qs.deep, (size_t)DEEP_THREADS * DEEP_STACK));
+  BQ_CUDA(cudaMemsetAsync(qs.ovfCount, 0, 8, al.s));
+  if (reorder && nq > 1) {
+    uint32_t *keys[2], *idx[2];
+    BQ_TRY(tmp.get(&keys[0], nq));
+    BQ_TRY(tmp.get(&keys[1], nq));
+    BQ_TRY(tmp.get(&idx[0], nq));
+    BQ_TRY(tmp.get(&idx[1], nq));
+    {
+      ProfScope ps("query.keys", al.s);
+      k_query_keys<<<div_up(nq, 256), 256, 0, al.s>>>(rootBox, queries, nq, keys[0], idx[0]);
+    }
+    BQ_CUDA(cudaGetLastError());
+    int sel = 0;
+    // the order only steers performance: the top 24 key bits (3 passes) suffice
+    BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, 6, 30, nullptr, &sel, qs.err, al));
+    qs.order = idx[sel];
+  }
+  return BQ_OK;
+}
+
+int finish_queries(QueryScratch &qs, Alloc &al)
+{
+  // the only host synchronisation: read the device error word
+  uint32_t err = 0;
+  BQ_CUDA(cudaMemcpyAsync(&err, qs.err, 4, cudaMemcpyDeviceToHost, al.s));
+  BQ_CUDA(cudaStreamSynchronize(al.s));
+  if (err & DEV_ERR_STACK) return set_error(BQ_ERR_STACK_OVERFLOW, "query exceeded the deep fallback stack");
+  if (err & DEV_ERR_TIMEOUT) return set_error(BQ_ERR_TIMEOUT, "query reordering sort timed out");
+  return BQ_OK;
+}
+
 int query_config(const bq_query_config *q, bq_query_config &out)
 {
   out.tieMode = q ? q->tieMode : BQ_TIES_LOWEST_ID;
@@ -365,7 +314,7 @@ int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries
   }
   TempSet tmp(al);
   QueryScratch qs;
-  BQ_TRY(prepare(bvh, queries, nq, c.reorder != 0, tmp, al, qs));
+  BQ_TRY(prepare_queries((const float *)bvh->nodes, queries, nq, c.reorder != 0, tmp, al, qs));
   const int tie = c.tieMode, st = c.stackDepth, b = c.blockSize;
   if (tie == BQ_TIES_REFERENCE) {
     if (st == 32) launch_cp<TIE_REFERENCE, 32>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s, ex);
@@ -377,7 +326,7 @@ int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries
     else launch_cp<TIE_LOWEST, 128>(bvh, points, queries, nq, maxSqr, b, ids, d, qs, al.s, ex);
   }
   BQ_CUDA(cudaGetLastError());
-  return finish(qs, al);
+  return finish_queries(qs, al);
 }
 
 int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, int k, float maxSqr,
@@ -394,7 +343,7 @@ int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t
   }
   TempSet tmp(al);
   QueryScratch qs;
-  BQ_TRY(prepare(bvh, queries, nq, c.reorder != 0, tmp, al, qs));
+  BQ_TRY(prepare_queries((const float *)bvh->nodes, queries, nq, c.reorder != 0, tmp, al, qs));
   const int tie = c.tieMode, st = c.stackDepth, b = c.blockSize;
   if (k <= 4) dispatch_knn_tie<4>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
   else if (k <= 8) dispatch_knn_tie<8>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
@@ -402,7 +351,7 @@ int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t
   else if (k <= 32) dispatch_knn_tie<32>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
   else dispatch_knn_tie<64>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
   BQ_CUDA(cudaGetLastError());
-  return finish(qs, al);
+  return finish_queries(qs, al);
 }
 
 } // namespace bq

@@ -156,6 +156,51 @@ int bq_refit_noalloc_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, bq_stream_t 
 int bq_free_f3(bq_bvh3f *bvh, const bq_allocator *alloc, bq_stream_t stream);
 
 /* ---------------------------------------------------------------- */
+/* wide BVHs: WideBVH<float,3,W> (cuBQL/bvh.h:113-141), W = 4 or 8    */
+/* ---------------------------------------------------------------- */
+/* One child slot of a wide node (WideBVH::Node::Child, cuBQL/bvh.h:124-131),
+   32 B: the child's box, then one 64-bit word with bit 0 = valid,
+   bits 1..45 = offset (the wide node id of an inner child, or the first
+   primIDs index of a leaf), bits 46..61 = count (0: inner child).  A wide
+   node is W consecutive slots; unused slots have valid = 0, an empty box
+   (+inf lower, -inf upper), offset 0xFFFFFFFF and count 0xFFFF, as the
+   reference writes them.  Node 0 is the root. */
+typedef struct bq_wide_child3f {
+  float lower[3];
+  float upper[3];
+  uint64_t validOffsetCount;
+} bq_wide_child3f;
+
+/* == WideBVH<float,3,W> (nodes: numNodes * W slots) */
+typedef struct bq_wide_bvh3f {
+  bq_wide_child3f *nodes;
+  uint32_t numNodes;
+  uint32_t *primIDs;
+  uint32_t numPrims;
+} bq_wide_bvh3f;
+
+/* Spatial-median build collapsed into a width-W tree.  Replaces
+   cuBQL::gpuBuilder(WideBVH<float,3,W>&, ...) (cuBQL/builder/cuda.h:104-113,
+   cuBQL/builder/cuda/wide_gpu_builder.h:162-213): every inner binary node
+   at a depth that is a multiple of log2(W) becomes a wide node whose
+   slots are the frontier of its treelet, in the reference's slot order.
+   Wide nodes are numbered by the index of their binary root (the
+   reference numbers them in atomic order, so its numbering varies from
+   run to run).  Synchronises the stream. */
+int bq_build_wide_f3(bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes, uint32_t numPrims,
+                     const bq_build_config *cfg, const bq_allocator *alloc, bq_stream_t stream);
+
+/* Collapses an existing binary tree (any builder) into a width-W tree
+   with its own copy of the primIDs; `binary` stays valid.  Synchronises
+   the stream. */
+int bq_collapse_wide_f3(bq_wide_bvh3f *wide, int width, const bq_bvh3f *binary, const bq_allocator *alloc,
+                        bq_stream_t stream);
+
+/* Frees a wide tree.  Replaces cuBQL::cuda::free(WideBVH&)
+   (cuBQL/builder/cuda/wide_gpu_builder.h:217-231). */
+int bq_wide_free_f3(bq_wide_bvh3f *bvh, const bq_allocator *alloc, bq_stream_t stream);
+
+/* ---------------------------------------------------------------- */
 /* queries (batched; the reference offers per-thread device functions */
 /* that user kernels call one thread per query)                        */
 /* ---------------------------------------------------------------- */
@@ -203,6 +248,26 @@ int bq_box_query_count_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_b
 int bq_box_query_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t numQueries,
                     const uint32_t *offsets, uint64_t capacity, int32_t *ids, const bq_allocator *alloc,
                     bq_stream_t stream);
+
+/* Closest data point per query over a wide tree.  Replaces a user kernel
+   calling cuBQL::points::findClosest(WideBVH<float,3,W>, ...)
+   (cuBQL/queries/points/findClosest.h:365-386, traversal
+   cuBQL/traversal/shrinkingRadiusQuery.h:553-636).  Same contract as
+   bq_closest_point_f3; with BQ_TIES_REFERENCE the answer equals the
+   reference's on the same wide tree (same slot sort, same numbering). */
+int bq_wide_closest_point_f3(const bq_wide_bvh3f *bvh, int width, const float *points, const float *queries,
+                             uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg, int32_t *ids,
+                             float *sqrDist, const bq_allocator *alloc, bq_stream_t stream);
+
+/* Fixed-box query over a wide tree (cuBQL::fixedBoxQuery::forEachPrim for
+   WideBVH, cuBQL/traversal/fixedBoxQuery.h:161-277: depth first, slots
+   in order), two passes as bq_box_query_count_f3 / bq_box_query_f3. */
+int bq_wide_box_query_count_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes,
+                               const bq_box3f *queryBoxes, uint32_t numQueries, uint32_t *counts,
+                               const bq_allocator *alloc, bq_stream_t stream);
+int bq_wide_box_query_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                         uint32_t numQueries, const uint32_t *offsets, uint64_t capacity, int32_t *ids,
+                         const bq_allocator *alloc, bq_stream_t stream);
 
 /* k nearest data points per query (1 <= k <= 64), ascending by squared
    distance.  Replaces cuBQL::points::findKNN

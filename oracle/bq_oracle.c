@@ -868,6 +868,252 @@ int orc_box_query(const onode *nodes, uint32_t numNodes, const uint32_t *primIDs
 }
 
 /* ------------------------------------------------------------------ */
+/* wide BVHs: WideBVH<float,3,W> (cuBQL/bvh.h:113-141).  A slot is an   */
+/* onode whose word holds valid (bit 0), offset (bits 1-45), count      */
+/* (bits 46-61).                                                        */
+/* ------------------------------------------------------------------ */
+#define WS_MASK45 ((1ull << 45) - 1)
+#define WS_MAKE(off, cnt) (1ull | (((uint64_t)(off) & WS_MASK45) << 1) | ((uint64_t)((cnt) & 0xFFFFu) << 46))
+#define WS_VALID(w) ((w) & 1ull)
+#define WS_OFF(w) (((w) >> 1) & WS_MASK45)
+#define WS_CNT(w) ((uint32_t)((w) >> 46) & 0xFFFFu)
+#define WS_UNUSED ((0xFFFFFFFFull << 1) | (0xFFFFull << 46))
+#define WS_BITS(w) ((w) & ((1ull << 62) - 1)) /* the bit field's 62 bits */
+
+static int log2w(int W) { return W == 2 ? 1 : (W == 4 ? 2 : (W == 8 ? 3 : -1)); }
+
+/* Binary -> wide collapse, wide_gpu_builder.h:40-158: inner nodes at a
+   depth that is a multiple of log2(W) (and the root) root wide nodes,
+   numbered by increasing binary index; each wide node's slots are its
+   treelet's frontier in collapseExecute's stack order (:131-149).  Node 1
+   is skipped.  outSlots holds up to numNodes*W slots.  Returns the wide
+   node count, or -1 on a malformed tree. */
+int orc_wide_collapse(const onode *nodes, uint32_t numNodes, int W, onode *outSlots)
+{
+  int lg = log2w(W);
+  if (lg < 0) return -1;
+  if (numNodes == 0) return 0;
+  uint32_t *parent = (uint32_t *)malloc(sizeof(uint32_t) * numNodes);
+  uint32_t *wid = (uint32_t *)malloc(sizeof(uint32_t) * numNodes);
+  uint8_t *flag = (uint8_t *)calloc(numNodes, 1);
+  int rc = 0;
+  for (uint32_t i = 0; i < numNodes; i++) parent[i] = 0xFFFFFFFFu;
+  for (uint32_t i = 0; i < numNodes; i++) {
+    if (i == 1 || ADMIN_CNT(nodes[i].admin)) continue;
+    uint64_t off = ADMIN_OFF(nodes[i].admin);
+    if (off < 2 || off + 1 >= numNodes) { rc = -1; goto done; }
+    parent[off] = parent[off + 1] = i;
+  }
+  flag[0] = 1;
+  for (uint32_t i = 2; i < numNodes; i++) {
+    if (ADMIN_CNT(nodes[i].admin)) continue;
+    uint32_t n = i, depth = 0;
+    while (n != 0 && n < numNodes && depth <= numNodes) { n = parent[n]; depth++; }
+    if (n == 0 && depth % (uint32_t)lg == 0) flag[i] = 1;
+  }
+  uint32_t nw = 0;
+  for (uint32_t i = 0; i < numNodes; i++) { wid[i] = nw; nw += flag[i]; }
+  for (uint32_t i = 0; i < numNodes; i++) {
+    if (!flag[i]) continue;
+    onode *out = outSlots + (size_t)wid[i] * W;
+    uint32_t stack[8];
+    int sp = 0, written = 0;
+    stack[sp++] = i;
+    while (sp) {
+      uint32_t n = stack[--sp];
+      const onode *nd = &nodes[n];
+      uint32_t cnt = ADMIN_CNT(nd->admin);
+      if (cnt || (n != i && flag[n])) {
+        if (written >= W) { rc = -1; goto done; }
+        onode *o = &out[written++];
+        memcpy(o->lo, nd->lo, sizeof(o->lo));
+        memcpy(o->hi, nd->hi, sizeof(o->hi));
+        o->admin = cnt ? WS_MAKE(ADMIN_OFF(nd->admin), cnt) : WS_MAKE(wid[n], 0);
+      } else {
+        uint64_t off = ADMIN_OFF(nd->admin);
+        if (off + 1 >= numNodes || sp + 2 > 8) { rc = -1; goto done; }
+        stack[sp++] = (uint32_t)off;
+        stack[sp++] = (uint32_t)off + 1;
+      }
+    }
+    for (; written < W; written++) {
+      onode *o = &out[written];
+      o->lo[0] = o->lo[1] = o->lo[2] = INFINITY;
+      o->hi[0] = o->hi[1] = o->hi[2] = -INFINITY;
+      o->admin = WS_UNUSED;
+    }
+  }
+  rc = (int)nw;
+done:
+  free(parent); free(wid); free(flag);
+  return rc;
+}
+
+/* Canonical form of a wide tree: BFS from node 0, slots kept in order,
+   inner slots renumbered in BFS order, leaf prims laid out in BFS order,
+   bits 62-63 of every word cleared (the reference leaves them as they
+   were in memory).  Returns 0, or -1 on a malformed tree. */
+int orc_wide_canonicalize(const onode *slots, uint32_t numWide, int W, const uint32_t *primIDs, onode *outSlots,
+                          uint32_t *outPrimIDs, uint32_t *outNumPrims)
+{
+  if (numWide == 0) { *outNumPrims = 0; return 0; }
+  uint32_t *q = (uint32_t *)malloc(sizeof(uint32_t) * numWide);
+  uint32_t head = 0, tail = 0, primPos = 0;
+  q[tail++] = 0;
+  while (head < tail) {
+    uint32_t src = q[head], dst = head;
+    head++;
+    for (int c = 0; c < W; c++) {
+      const onode *s = &slots[(size_t)src * W + c];
+      onode *d = &outSlots[(size_t)dst * W + c];
+      *d = *s;
+      uint64_t w = WS_BITS(s->admin);
+      d->admin = w;
+      if (!WS_VALID(w)) continue;
+      if (WS_CNT(w)) {
+        uint64_t off = WS_OFF(w);
+        for (uint32_t j = 0; j < WS_CNT(w); j++) outPrimIDs[primPos + j] = primIDs[off + j];
+        d->admin = WS_MAKE(primPos, WS_CNT(w));
+        primPos += WS_CNT(w);
+      } else {
+        if (WS_OFF(w) >= numWide || tail >= numWide) { free(q); return -1; }
+        q[tail] = (uint32_t)WS_OFF(w);
+        d->admin = WS_MAKE(tail, 0);
+        tail++;
+      }
+    }
+  }
+  free(q);
+  *outNumPrims = primPos;
+  return tail == numWide ? 0 : -2;
+}
+
+/* Closest point over a wide tree (findClosest.h:228-270 and
+   shrinkingRadiusQuery.h:553-636); tie modes as orc_closest_point.
+   Unbounded stack. */
+int orc_wide_closest(const onode *slots, uint32_t numWide, int W, const uint32_t *primIDs, const float *points,
+                     const float *queries, uint32_t nq, float maxSqr, int fma_mode, int tie_mode, int32_t *ids,
+                     float *dists)
+{
+  int lg = log2w(W);
+  if (lg < 0) return -1;
+  for (uint32_t i = 0; i < nq; i++) {
+    const float *q = queries + 3 * (size_t)i;
+    int32_t best = -1;
+    float bestD = maxSqr, cull = maxSqr;
+    if (numWide) {
+      size_t cap = 256, sp = 0;
+      uint64_t *stack = (uint64_t *)malloc(sizeof(uint64_t) * cap);
+      uint32_t nodeID = 0;
+      for (;;) {
+        int done = 0;
+        for (;;) {
+          while (nodeID == 0xFFFFFFFFu) {
+            if (sp == 0) { done = 1; break; }
+            uint64_t tos = stack[--sp];
+            uint32_t db = (uint32_t)(tos >> 32);
+            float d;
+            memcpy(&d, &db, 4);
+            if (d > (tie_mode == 1 ? cull : lowest_slack(cull))) continue;
+            nodeID = (uint32_t)tos;
+          }
+          if (done || (nodeID & 0x80000000u)) break;
+          float cs = tie_mode == 1 ? cull : lowest_slack(cull);
+          uint64_t v[8];
+          for (int c = 0; c < W; c++) {
+            const onode *sl = &slots[(size_t)nodeID * W + c];
+            v[c] = ~0ull;
+            if (!WS_VALID(sl->admin)) continue;
+            float d = sqr_pbox(q, sl->lo, sl->hi, fma_mode);
+            if (d > cs) continue;
+            uint32_t payload = WS_CNT(sl->admin) ? (0x80000000u | (nodeID << lg) | (uint32_t)c)
+                                                  : (uint32_t)WS_OFF(sl->admin);
+            uint32_t db;
+            memcpy(&db, &d, 4);
+            v[c] = ((uint64_t)db << 32) | payload;
+          }
+          for (int a = W - 1; a > 0; --a)
+            for (int b = 0; b < a; b++) {
+              uint64_t c0 = v[b], c1 = v[b + 1];
+              v[b] = c0 < c1 ? c0 : c1;
+              v[b + 1] = c0 < c1 ? c1 : c0;
+            }
+          for (int c = W - 1; c > 0; --c) {
+            if (v[c] == ~0ull) continue;
+            if (sp == cap) { cap *= 2; stack = (uint64_t *)realloc(stack, sizeof(uint64_t) * cap); }
+            stack[sp++] = v[c];
+          }
+          nodeID = v[0] == ~0ull ? 0xFFFFFFFFu : (uint32_t)v[0];
+        }
+        if (done) break;
+        uint32_t c = nodeID & (uint32_t)(W - 1);
+        uint32_t n = (nodeID & 0x7fffffffu) >> lg;
+        uint64_t w = slots[(size_t)n * W + c].admin;
+        uint64_t off = WS_OFF(w);
+        float leaf = INFINITY;
+        for (uint32_t j = 0; j < WS_CNT(w); j++) {
+          uint32_t pid = primIDs[off + j];
+          float d = sqr_pp(points + 3 * (size_t)pid, q, fma_mode);
+          int take = tie_mode == 1 ? (d < bestD) : (d < bestD || (best >= 0 && d == bestD && (int32_t)pid < best));
+          if (take) { bestD = d; best = (int32_t)pid; }
+          leaf = fminf(leaf, bestD);
+        }
+        cull = fminf(cull, leaf);
+        nodeID = 0xFFFFFFFFu;
+      }
+      free(stack);
+    }
+    ids[i] = best;
+    dists[i] = best >= 0 ? bestD : INFINITY;
+  }
+  return 0;
+}
+
+/* fixedBoxQuery over a wide tree (fixedBoxQuery.h:161-277): depth first,
+   slots in order, per-prim box test as orc_box_query. */
+int orc_wide_box_query(const onode *slots, uint32_t numWide, int W, const uint32_t *primIDs, const obox *boxes,
+                       const obox *queryBoxes, uint32_t nq, uint32_t *counts, const uint64_t *offsets, int32_t *ids)
+{
+  size_t cap = 256;
+  uint64_t *stack = (uint64_t *)malloc(sizeof(uint64_t) * cap);
+  for (uint32_t qi = 0; qi < nq; qi++) {
+    const float *qlo = queryBoxes[qi].lo, *qhi = queryBoxes[qi].hi;
+    uint32_t cnt = 0;
+    size_t sp = 0;
+    uint64_t node = 0;
+    uint32_t c = 0;
+    while (numWide) {
+      const onode *sl = &slots[node * W + c];
+      if (WS_VALID(sl->admin) && box_ov(qlo, qhi, sl->lo, sl->hi)) {
+        if (WS_CNT(sl->admin) == 0) {
+          if (c + 1 < (uint32_t)W) {
+            if (sp == cap) { cap *= 2; stack = (uint64_t *)realloc(stack, sizeof(uint64_t) * cap); }
+            stack[sp++] = (node << 8) | (c + 1);
+          }
+          node = WS_OFF(sl->admin);
+          c = 0;
+          continue;
+        }
+        uint64_t off = WS_OFF(sl->admin);
+        for (uint32_t j = 0; j < WS_CNT(sl->admin); j++) {
+          uint32_t pid = primIDs[off + j];
+          if (box_ov(qlo, qhi, boxes[pid].lo, boxes[pid].hi)) {
+            if (ids) ids[offsets[qi] + cnt] = (int32_t)pid;
+            cnt++;
+          }
+        }
+      }
+      if (c + 1 < (uint32_t)W) c++;
+      else if (sp) { uint64_t e = stack[--sp]; node = e >> 8; c = (uint32_t)(e & 0xFF); }
+      else break;
+    }
+    counts[qi] = cnt;
+  }
+  free(stack);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* point-to-triangle closest point, FP32, as the reference computes it  */
 /* (cuBQL/queries/triangles/findClosest.h:56-152), without contraction. */
 /* Only compared at a tolerance.                                        */

@@ -174,6 +174,58 @@ class Oracle:
         self.lib.orc_box_query(*args, _p(counts), _p(offsets), _p(ids))
         return offsets.astype(np.int64), ids[:int(offsets[-1])]
 
+    # ---- wide trees (slots are NODE records whose admin word holds the
+    # valid/offset/count bit field of WideBVH::Node::Child) ----
+    def wide_collapse(self, nodes, width):
+        """Binary -> width-wide collapse; returns the slots (numWide*width)."""
+        nodes = np.ascontiguousarray(nodes, dtype=NODE)
+        out = np.zeros(max(len(nodes), 1) * width, dtype=NODE)
+        nw = self.lib.orc_wide_collapse(_p(nodes), ctypes.c_uint32(len(nodes)), ctypes.c_int(width), _p(out))
+        if nw < 0:
+            raise ValueError("binary tree is not valid for the collapse")
+        return out[: nw * width].copy()
+
+    def wide_canonicalize(self, slots, width, prims):
+        slots = np.ascontiguousarray(slots, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        out = np.zeros(len(slots), dtype=NODE)
+        outp = np.zeros(max(len(prims), 1), dtype=np.uint32)
+        npr = ctypes.c_uint32()
+        rc = self.lib.orc_wide_canonicalize(_p(slots), ctypes.c_uint32(len(slots) // width), ctypes.c_int(width),
+                                            _p(prims), _p(out), _p(outp), ctypes.byref(npr))
+        if rc != 0:
+            raise ValueError(f"not a valid wide tree (rc={rc})")
+        return out, outp[: npr.value].copy()
+
+    def wide_closest(self, slots, width, prims, points, queries, maxSqr=np.inf, fma_mode=1, tie_mode=0):
+        slots = np.ascontiguousarray(slots, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        rc = self.lib.orc_wide_closest(_p(slots), ctypes.c_uint32(len(slots) // width), ctypes.c_int(width),
+                                       _p(prims), _p(points), _p(queries), ctypes.c_uint32(nq),
+                                       ctypes.c_float(maxSqr), ctypes.c_int(fma_mode), ctypes.c_int(tie_mode),
+                                       _p(ids), _p(d))
+        assert rc == 0
+        return ids, d
+
+    def wide_box_query(self, slots, width, prims, boxes, query_boxes):
+        slots = np.ascontiguousarray(slots, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        boxes, qb = _f32(boxes).reshape(-1, 6), _f32(query_boxes).reshape(-1, 6)
+        nq = qb.shape[0]
+        counts = np.zeros(nq, dtype=np.uint32)
+        args = (_p(slots), ctypes.c_uint32(len(slots) // width), ctypes.c_int(width), _p(prims), _p(boxes), _p(qb),
+                ctypes.c_uint32(nq), _p(counts))
+        self.lib.orc_wide_box_query(*args, None, None)
+        offsets = np.zeros(nq + 1, dtype=np.uint64)
+        np.cumsum(counts, out=offsets[1:])
+        ids = np.zeros(max(int(offsets[-1]), 1), dtype=np.int32)
+        self.lib.orc_wide_box_query(*args, _p(offsets), _p(ids))
+        return offsets.astype(np.int64), ids[:int(offsets[-1])]
+
     def knn(self, nodes, prims, points, queries, k, maxSqr=np.inf, fma_mode=1, tie_mode=0, stack=64):
         nodes = np.ascontiguousarray(nodes, dtype=NODE)
         prims = np.ascontiguousarray(prims, dtype=np.uint32)
@@ -327,7 +379,7 @@ class RefCPU:
 
 class RefGPU:
     """The reference's GPU code (runs only where a GPU is present)."""
-    RADIX, SPATIAL_MEDIAN, REBIN = 0, 1, 2
+    RADIX, SPATIAL_MEDIAN, REBIN, WIDE4, WIDE8 = 0, 1, 2, 3, 4
 
     def __init__(self):
         self.lib = _load(REF_GPU_SO)
@@ -373,6 +425,59 @@ class RefGPU:
                                               _p(ex) if ex is not None else None, _p(ids), _p(d))
         assert rc == 0
         return ids, d
+
+    def build_wide(self, width, boxes, makeLeafThreshold=0):
+        """The reference's gpuBuilder into a WideBVH<float,3,width>:
+        (slots as NODE records, numWide*width of them; primIDs)."""
+        boxes = _f32(boxes).reshape(-1, 6)
+        n = boxes.shape[0]
+        slots = np.zeros((2 * n + 2) * width, dtype=NODE)
+        prims = np.zeros(max(n, 1), dtype=np.uint32)
+        nw, npr = ctypes.c_uint32(), ctypes.c_uint32()
+        rc = self.lib.ref_gpu_build_wide(ctypes.c_int(width), _p(boxes), ctypes.c_uint32(n),
+                                         ctypes.c_int(makeLeafThreshold), _p(slots), _p(prims), ctypes.byref(nw),
+                                         ctypes.byref(npr))
+        assert rc == 0, "reference wide build failed"
+        return slots[: nw.value * width].copy(), prims[: npr.value].copy()
+
+    def wide_closest(self, width, slots, prims, points, queries, maxSqr=np.inf):
+        slots = np.ascontiguousarray(slots, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        points, queries = _f32(points), _f32(queries)
+        nq = queries.shape[0]
+        ids = np.zeros(nq, dtype=np.int32)
+        d = np.zeros(nq, dtype=np.float32)
+        rc = self.lib.ref_gpu_wide_closest(ctypes.c_int(width), _p(slots), ctypes.c_uint32(len(slots) // width),
+                                           _p(prims), ctypes.c_uint32(len(prims)), _p(points),
+                                           ctypes.c_uint32(len(points)), _p(queries), ctypes.c_uint32(nq),
+                                           ctypes.c_float(maxSqr), _p(ids), _p(d))
+        assert rc == 0
+        return ids, d
+
+    def wide_box_query(self, width, slots, prims, boxes, query_boxes):
+        slots = np.ascontiguousarray(slots, dtype=NODE)
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        boxes, qb = _f32(boxes).reshape(-1, 6), _f32(query_boxes).reshape(-1, 6)
+        nq = qb.shape[0]
+        counts = np.zeros(nq, dtype=np.uint32)
+        args = (ctypes.c_int(width), _p(slots), ctypes.c_uint32(len(slots) // width), _p(prims),
+                ctypes.c_uint32(len(prims)), _p(boxes), ctypes.c_uint32(len(boxes)), _p(qb), ctypes.c_uint32(nq),
+                _p(counts))
+        assert self.lib.ref_gpu_wide_box_query(*args, None, None) == 0
+        offsets = np.zeros(nq + 1, dtype=np.uint64)
+        np.cumsum(counts, out=offsets[1:])
+        ids = np.zeros(max(int(offsets[-1]), 1), dtype=np.int32)
+        assert self.lib.ref_gpu_wide_box_query(*args, _p(offsets), _p(ids)) == 0
+        return offsets.astype(np.int64), ids[:int(offsets[-1])]
+
+    def time_wide_query(self, width, points, queries, makeLeafThreshold=0, reps=5):
+        points, queries = _f32(points), _f32(queries)
+        ms = ctypes.c_float()
+        rc = self.lib.ref_gpu_time_wide_query(ctypes.c_int(width), _p(points), ctypes.c_uint32(len(points)),
+                                              ctypes.c_int(makeLeafThreshold), _p(queries),
+                                              ctypes.c_uint32(len(queries)), ctypes.c_int(reps), ctypes.byref(ms))
+        assert rc == 0
+        return ms.value
 
     def box_query(self, nodes, prims, boxes, query_boxes):
         """The reference's fixedBoxQuery::forEachPrim in a kernel, one thread

@@ -18,6 +18,8 @@
 //   launched one thread per query as testing/points/closestPoint.cu:37-58)
 //   fixedBoxQuery::forEachPrim  cuBQL/traversal/fixedBoxQuery.h:139-156, with
 //   a lambda that keeps prims whose box overlaps the query box
+//   gpuBuilder(WideBVH<float,3,W>&) cuBQL/builder/cuda/wide_gpu_builder.h:162-213,
+//   points::findClosest(WideBVH) and fixedBoxQuery::forEachPrim(WideBVH)
 #define CUBQL_GPU_BUILDER_IMPLEMENTATION 1
 #include "cuBQL/bvh.h"
 #include "cuBQL/builder/cuda/radix.h"
@@ -151,6 +153,180 @@ __global__ void k_points_to_boxes(const vec3f *pts, box3f *boxes, int n)
   int tid = threadIdx.x + blockIdx.x * blockDim.x;
   if (tid >= n) return;
   boxes[tid] = box3f().including(pts[tid]);
+}
+
+// ---- wide trees ----
+template <int W>
+using wbvh = WideBVH<float, 3, W>;
+static_assert(sizeof(wbvh<4>::Node) == 4 * 32 && sizeof(wbvh<8>::Node) == 8 * 32, "wide node layout");
+
+template <int W>
+struct DeviceWide {
+  wbvh<W> bvh;
+  int upload(const void *slots, uint32_t numWide, const uint32_t *primIDs, uint32_t numPrims)
+  {
+    bvh.nodes = (typename wbvh<W>::Node *)dalloc_copy((const char *)slots, sizeof(typename wbvh<W>::Node) * numWide);
+    bvh.primIDs = dalloc_copy(primIDs, numPrims);
+    bvh.numNodes = numWide;
+    bvh.numPrims = numPrims;
+    return (bvh.nodes && bvh.primIDs) ? 0 : -1;
+  }
+  ~DeviceWide()
+  {
+    cudaFree(bvh.nodes);
+    cudaFree(bvh.primIDs);
+  }
+};
+
+template <int W>
+__global__ void k_wide_closest(wbvh<W> bvh, const vec3f *pts, const vec3f *qs, int nq, float maxSqr, int *ids,
+                               float *dists)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= nq) return;
+  int id = points::findClosest(bvh, pts, qs[tid], maxSqr);
+  ids[tid] = id;
+  dists[tid] = id < 0 ? INFINITY : fSqrDistance_rd(pts[id], qs[tid]);
+}
+
+template <int W>
+__global__ void k_wide_box(wbvh<W> bvh, const box3f *boxes, const box3f *qb, int nq,
+                           const unsigned long long *offsets, unsigned *counts, int *ids)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= nq) return;
+  const box3f q = qb[tid];
+  unsigned c = 0;
+  auto perPrim = [&](uint32_t primID) -> int {
+    if (q.overlaps(boxes[primID])) {
+      if (offsets) ids[offsets[tid] + c] = (int)primID;
+      c++;
+    }
+    return CUBQL_CONTINUE_TRAVERSAL;
+  };
+  fixedBoxQuery::forEachPrim(perPrim, bvh, q);
+  counts[tid] = c;
+}
+
+template <int W>
+int build_wide_t(const float *boxes, uint32_t n, int thr, void *slotsOut, uint32_t *primsOut, uint32_t *numWide,
+                 uint32_t *numPrims)
+{
+  box3f *d_boxes = dalloc_copy((const box3f *)boxes, n);
+  if (!d_boxes) return -1;
+  wbvh<W> bvh;
+  BuildConfig cfg;
+  cfg.makeLeafThreshold = thr;
+  gpuBuilder(bvh, d_boxes, n, cfg);
+  RCHECK(cudaDeviceSynchronize());
+  *numWide = bvh.numNodes;
+  *numPrims = bvh.numPrims;
+  if (bvh.numNodes)
+    RCHECK(cudaMemcpy(slotsOut, bvh.nodes, sizeof(typename wbvh<W>::Node) * bvh.numNodes, cudaMemcpyDeviceToHost));
+  if (bvh.numPrims) RCHECK(cudaMemcpy(primsOut, bvh.primIDs, sizeof(uint32_t) * bvh.numPrims, cudaMemcpyDeviceToHost));
+  cuBQL::cuda::free(bvh);
+  cudaFree(d_boxes);
+  return 0;
+}
+
+template <int W>
+int wide_closest_t(const void *slots, uint32_t numWide, const uint32_t *primIDs, uint32_t numPrims,
+                   const float *points, uint32_t np, const float *queries, uint32_t nq, float maxSqr, int32_t *ids,
+                   float *dists)
+{
+  DeviceWide<W> t;
+  if (t.upload(slots, numWide, primIDs, numPrims)) return -1;
+  vec3f *dp = dalloc_copy((const vec3f *)points, np), *dq = dalloc_copy((const vec3f *)queries, nq);
+  int *di = dalloc_copy<int>(nullptr, nq);
+  float *dd = dalloc_copy<float>(nullptr, nq);
+  k_wide_closest<W><<<(nq + 127) / 128, 128>>>(t.bvh, dp, dq, (int)nq, maxSqr, di, dd);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(ids, di, sizeof(int) * nq, cudaMemcpyDeviceToHost);
+  cudaMemcpy(dists, dd, sizeof(float) * nq, cudaMemcpyDeviceToHost);
+  cudaFree(dp); cudaFree(dq); cudaFree(di); cudaFree(dd);
+  return 0;
+}
+
+template <int W>
+int wide_box_t(const void *slots, uint32_t numWide, const uint32_t *primIDs, uint32_t numPrims, const float *boxes,
+               uint32_t nb, const float *queryBoxes, uint32_t nq, uint32_t *counts, const uint64_t *offsets,
+               int32_t *ids)
+{
+  DeviceWide<W> t;
+  if (t.upload(slots, numWide, primIDs, numPrims)) return -1;
+  box3f *db = dalloc_copy((const box3f *)boxes, nb), *dq = dalloc_copy((const box3f *)queryBoxes, nq);
+  unsigned *dc = dalloc_copy<unsigned>(nullptr, nq);
+  unsigned long long *doff = ids ? dalloc_copy((const unsigned long long *)offsets, nq + 1) : nullptr;
+  const size_t total = ids ? offsets[nq] : 0;
+  int *di = ids ? dalloc_copy<int>(nullptr, total) : nullptr;
+  k_wide_box<W><<<(nq + 127) / 128, 128>>>(t.bvh, db, dq, (int)nq, doff, dc, di);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(counts, dc, sizeof(unsigned) * nq, cudaMemcpyDeviceToHost);
+  if (ids && total) cudaMemcpy(ids, di, sizeof(int) * total, cudaMemcpyDeviceToHost);
+  cudaFree(db); cudaFree(dq); cudaFree(dc);
+  if (doff) cudaFree(doff);
+  if (di) cudaFree(di);
+  return 0;
+}
+
+template <int W>
+float time_wide_query_t(const float *points, uint32_t n, int thr, const float *queries, uint32_t nq, int reps)
+{
+  vec3f *dp = dalloc_copy((const vec3f *)points, n), *dq = dalloc_copy((const vec3f *)queries, nq);
+  box3f *db = dalloc_copy<box3f>(nullptr, n);
+  int *di = dalloc_copy<int>(nullptr, nq);
+  float *dd = dalloc_copy<float>(nullptr, nq);
+  if (!dp || !dq || !db || !di || !dd) return -1.f;
+  k_points_to_boxes<<<(n + 127) / 128, 128>>>(dp, db, (int)n);
+  wbvh<W> bvh;
+  BuildConfig cfg;
+  cfg.makeLeafThreshold = thr;
+  gpuBuilder(bvh, db, n, cfg);
+  if (cudaDeviceSynchronize() != cudaSuccess) return -1.f;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float total = 0.f;
+  for (int r = -1; r < reps; r++) {
+    cudaEventRecord(e0);
+    k_wide_closest<W><<<(nq + 127) / 128, 128>>>(bvh, dp, dq, (int)nq, INFINITY, di, dd);
+    cudaEventRecord(e1);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r >= 0) total += ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cuBQL::cuda::free(bvh);
+  cudaFree(dp); cudaFree(dq); cudaFree(db); cudaFree(di); cudaFree(dd);
+  return total / (reps > 0 ? reps : 1);
+}
+
+// CUDA-event time of gpuBuilder(WideBVH<float,3,W>&) (free not timed)
+template <int W>
+float time_wide_build_t(const box3f *db, uint32_t n, int thr, int reps)
+{
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float total = 0.f;
+  BuildConfig cfg;
+  cfg.makeLeafThreshold = thr;
+  for (int r = -1; r < reps; r++) {
+    wbvh<W> w;
+    cudaEventRecord(e0);
+    gpuBuilder(w, db, n, cfg);
+    cudaEventRecord(e1);
+    if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r >= 0) total += ms;
+    cuBQL::cuda::free(w);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return total / (reps > 0 ? reps : 1);
 }
 
 int run_build(int method, const box3f *d_boxes, uint32_t n, int leafThr, bvh3f &bvh)
@@ -324,6 +500,13 @@ int ref_gpu_time_build(int method, const float *points, uint32_t n, int makeLeaf
   if (!dp || !db) return -1;
   k_points_to_boxes<<<(n + 127) / 128, 128>>>(dp, db, (int)n);
   RCHECK(cudaDeviceSynchronize());
+  if (method == 3 || method == 4) {  // gpuBuilder into a WideBVH<float,3,4|8>
+    *ms_out = method == 3 ? time_wide_build_t<4>(db, n, makeLeafThreshold, reps)
+                          : time_wide_build_t<8>(db, n, makeLeafThreshold, reps);
+    cudaFree(dp);
+    cudaFree(db);
+    return *ms_out < 0.f ? -1 : 0;
+  }
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -433,6 +616,43 @@ int ref_gpu_time_box_query(int method, const float *points, uint32_t n, int make
   *ms_out = total / (reps > 0 ? reps : 1);
   *total_out = ho[nq];
   return 0;
+}
+
+// ---- wide trees (W = 4 or 8) ----
+// slotsOut holds (2n+2)*W slots, primsOut n entries
+int ref_gpu_build_wide(int W, const float *boxes, uint32_t n, int thr, void *slotsOut, uint32_t *primsOut,
+                       uint32_t *numWide, uint32_t *numPrims)
+{
+  if (W == 4) return build_wide_t<4>(boxes, n, thr, slotsOut, primsOut, numWide, numPrims);
+  if (W == 8) return build_wide_t<8>(boxes, n, thr, slotsOut, primsOut, numWide, numPrims);
+  return -1;
+}
+
+int ref_gpu_wide_closest(int W, const void *slots, uint32_t numWide, const uint32_t *primIDs, uint32_t numPrims,
+                         const float *points, uint32_t np, const float *queries, uint32_t nq, float maxSqr,
+                         int32_t *ids, float *dists)
+{
+  if (W == 4) return wide_closest_t<4>(slots, numWide, primIDs, numPrims, points, np, queries, nq, maxSqr, ids, dists);
+  if (W == 8) return wide_closest_t<8>(slots, numWide, primIDs, numPrims, points, np, queries, nq, maxSqr, ids, dists);
+  return -1;
+}
+
+int ref_gpu_wide_box_query(int W, const void *slots, uint32_t numWide, const uint32_t *primIDs, uint32_t numPrims,
+                           const float *boxes, uint32_t nb, const float *queryBoxes, uint32_t nq, uint32_t *counts,
+                           const uint64_t *offsets, int32_t *ids)
+{
+  if (W == 4) return wide_box_t<4>(slots, numWide, primIDs, numPrims, boxes, nb, queryBoxes, nq, counts, offsets, ids);
+  if (W == 8) return wide_box_t<8>(slots, numWide, primIDs, numPrims, boxes, nb, queryBoxes, nq, counts, offsets, ids);
+  return -1;
+}
+
+int ref_gpu_time_wide_query(int W, const float *points, uint32_t n, int thr, const float *queries, uint32_t nq,
+                            int reps, float *ms_out)
+{
+  float ms = W == 4 ? time_wide_query_t<4>(points, n, thr, queries, nq, reps)
+                    : (W == 8 ? time_wide_query_t<8>(points, n, thr, queries, nq, reps) : -1.f);
+  *ms_out = ms;
+  return ms < 0.f ? -1 : 0;
 }
 
 } // extern "C"

@@ -7,6 +7,8 @@
                                            # rebinRadixBuilder trees
   python tests/golden/make_golden.py gpu_boxquery   # on a B200: the
                                            # reference's fixedBoxQuery results
+  python tests/golden/make_golden.py gpu_wide   # on a B200: the reference's
+                                           # WideBVH builds and queries
 
 Both read oracle/_ref/ (the reference compiled from its own sources by
 oracle/build_ref.sh).  Inputs are the seeded generators of
@@ -167,5 +169,40 @@ def gpu_boxquery():
     np.savez_compressed(dest, **out)
 
 
+def gpu_wide():
+    """For uniform and GMM points (3000, unshifted): the reference's binary
+    spatial-median tree and its WideBVH<float,3,4|8> builds (leaf 1 and 8),
+    both BFS-renumbered, plus the raw wide trees with the reference's
+    closest-point and box-query results on them."""
+    from oracle.oracle import RefGPU
+    r = RefGPU()
+    o = Oracle()
+    out = {}
+    rng = np.random.default_rng(5)
+    for name, pts in (("u", W.uniform_points(3000)), ("g", W.gmm_points(3000, offset=0.0))):
+        b = W.point_boxes(pts)
+        q = W.uniform_points(600, W.SEED_QUERIES, -0.1, 1.1)
+        h = rng.uniform(0.0, 0.06, size=(600, 1)).astype(np.float32)
+        qb = np.concatenate([q - h, q + h], 1).astype(np.float32)
+        out[f"{name}_points"], out[f"{name}_queries"], out[f"{name}_qboxes"] = pts, q, qb
+        for thr in (0, 8):
+            n, pr = r.build(RefGPU.SPATIAL_MEDIAN, b, thr)
+            cn, cp = o.canonicalize(n, pr)
+            out[f"{name}{thr}_bin_nodes"], out[f"{name}{thr}_bin_prims"] = cn.view(np.uint8), cp
+            for width in (4, 8):
+                sl, wp = r.build_wide(width, b, thr)
+                cs, cwp = o.wide_canonicalize(sl, width, wp)
+                key = f"{name}{thr}_w{width}"
+                out[f"{key}_canon"], out[f"{key}_canon_prims"] = cs.view(np.uint8), cwp
+                out[f"{key}_raw"], out[f"{key}_raw_prims"] = sl.view(np.uint8), wp
+                ids, d = r.wide_closest(width, sl, wp, pts, q)
+                out[f"{key}_cp_ids"], out[f"{key}_cp_d"] = ids, d
+                off, bids = r.wide_box_query(width, sl, wp, b, qb)
+                out[f"{key}_box_off"], out[f"{key}_box_ids"] = off, bids
+    dest = sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu_wide.npz")
+    np.savez_compressed(dest, **out)
+
+
 if __name__ == "__main__":
-    {"cpu": cpu, "gpu": gpu, "gpu_rebin": gpu_rebin, "gpu_boxquery": gpu_boxquery}[sys.argv[1]]()
+    {"cpu": cpu, "gpu": gpu, "gpu_rebin": gpu_rebin, "gpu_boxquery": gpu_boxquery,
+     "gpu_wide": gpu_wide}[sys.argv[1]]()

@@ -294,3 +294,72 @@ def test_box_query_matches_reference_gpu_fixtures(oracle):
             assert np.array_equal(off, g[f"{name}{thr}_offsets"]), (name, thr)
             assert np.array_equal(ids, g[f"{name}{thr}_ids"]), (name, thr)
             assert off[-1] > 2 * len(q)
+
+
+def _wide_leaf_prims(slots, prims):
+    v = (slots["admin"] & np.uint64(1)).astype(bool)
+    cnt = ((slots["admin"] >> np.uint64(46)) & np.uint64(0xFFFF)).astype(np.int64)
+    off = ((slots["admin"] >> np.uint64(1)) & np.uint64((1 << 45) - 1)).astype(np.int64)
+    leaf = v & (cnt > 0)
+    return np.concatenate([prims[o:o + c] for o, c in zip(off[leaf], cnt[leaf])]) if leaf.any() else np.zeros(0)
+
+
+@pytest.mark.parametrize("width", [2, 4, 8])
+def test_wide_collapse_oracle_invariants(oracle, width):
+    """The collapse (wide_gpu_builder.h:40-158) restated: every prim reached
+    once, inner slots point at wide nodes, slot boxes are binary node boxes,
+    and the wide tree answers closest-point (lowest-id rule) and box
+    queries exactly as the binary tree it came from."""
+    pts = W.uniform_points(4000)
+    b = boxes_np(pts)
+    q = W.uniform_points(300, W.SEED_QUERIES, -0.1, 1.1)
+    qb = np.concatenate([q - 0.03, q + 0.03], 1).astype(np.float32)
+    for build in ("sm", "radix"):
+        for thr in (0, 8):
+            n, pr = oracle.sm_build(b, thr) if build == "sm" else oracle.radix_build(b, thr)
+            sl = oracle.wide_collapse(n, width)
+            nw = len(sl) // width
+            assert np.array_equal(np.sort(_wide_leaf_prims(sl, pr)), np.arange(len(pts)))
+            v = (sl["admin"] & np.uint64(1)).astype(bool)
+            cnt = (sl["admin"] >> np.uint64(46)) & np.uint64(0xFFFF)
+            off = (sl["admin"] >> np.uint64(1)) & np.uint64((1 << 45) - 1)
+            inner = v & (cnt == 0)
+            assert (off[inner] < nw).all() and (off[inner] > 0).all()
+            assert np.all(sl["lower"][~v] == np.inf) and np.all(sl["upper"][~v] == -np.inf)
+            cs, cp = oracle.wide_canonicalize(sl, width, pr)
+            assert len(cs) == len(sl)
+            bi, bd, _, _ = oracle.closest_point(n, pr, pts, q, fma_mode=1, tie_mode=0)
+            wi, wd = oracle.wide_closest(sl, width, pr, pts, q, fma_mode=1, tie_mode=0)
+            assert np.array_equal(bi, wi) and np.array_equal(bd, wd)
+            off_b, ids_b = oracle.box_query(n, pr, b, qb)
+            off_w, ids_w = oracle.wide_box_query(sl, width, pr, b, qb)
+            assert np.array_equal(off_b, off_w)
+            for i in range(len(q)):
+                assert np.array_equal(np.sort(ids_b[off_b[i]:off_b[i + 1]]), np.sort(ids_w[off_w[i]:off_w[i + 1]]))
+
+
+def test_wide_oracle_matches_reference_gpu_fixtures(oracle):
+    """Against the reference run on a B200 (gpuBuilder into WideBVH<float,3,
+    4|8>, uniform and GMM points, leaf 1 and 8): the oracle's collapse of the
+    reference's binary tree equals the reference's wide tree after BFS
+    renumbering; on the reference's own wide trees the oracle's closest point
+    (reference tie rule, device FMA shapes) and box query equal the
+    reference's kernels."""
+    g = _load("ref_gpu_wide.npz")
+    for name in ("u", "g"):
+        pts, q, qb = g[f"{name}_points"], g[f"{name}_queries"], g[f"{name}_qboxes"]
+        b = boxes_np(pts)
+        for thr in (0, 8):
+            n = g[f"{name}{thr}_bin_nodes"].view(NODE)
+            pr = g[f"{name}{thr}_bin_prims"]
+            for width in (4, 8):
+                key = f"{name}{thr}_w{width}"
+                sl = oracle.wide_collapse(n, width)
+                cs, cp = oracle.wide_canonicalize(sl, width, pr)
+                assert cs.tobytes() == g[f"{key}_canon"].tobytes(), key
+                assert np.array_equal(cp, g[f"{key}_canon_prims"]), key
+                raw, rp = g[f"{key}_raw"].view(NODE), g[f"{key}_raw_prims"]
+                ids, d = oracle.wide_closest(raw, width, rp, pts, q, fma_mode=1, tie_mode=1)
+                assert np.array_equal(ids, g[f"{key}_cp_ids"]) and np.array_equal(d, g[f"{key}_cp_d"]), key
+                off, bids = oracle.wide_box_query(raw, width, rp, b, qb)
+                assert np.array_equal(off, g[f"{key}_box_off"]) and np.array_equal(bids, g[f"{key}_box_ids"]), key
