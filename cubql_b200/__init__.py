@@ -133,6 +133,9 @@ _SIGS = {
     "bq_autotune_batched_knn_f3": [_P, _P, _P, _U, _U, _P, _P, _U, _I, _P, ctypes.POINTER(bq_allocator), _P],
     "bq_tri_boxes_f3": [_P, _P, _U, _P, _P],
     "bq_points_to_boxes_f3": [_P, _U, _P, _P],
+    "bq_load_binary": [ctypes.c_char_p, ctypes.c_size_t, _P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)],
+    "bq_save_binary": [ctypes.c_char_p, _P, ctypes.c_uint64, ctypes.c_size_t],
+    "bq_load_points_f64_as_f32": [ctypes.c_char_p, _I, _P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)],
     "bq_last_error_string": [],
     "bq_version": [],
     "bq_profile_enable": [_I],
@@ -655,6 +658,44 @@ def points_to_boxes(pts):
     out = torch.empty((pts.shape[0], 6), dtype=torch.float32, device=pts.device)
     _check(_lib.bq_points_to_boxes_f3(_ptr(pts), pts.shape[0], _ptr(out), _stream()))
     return out
+
+
+class io:
+    """The reference samples' binary-dump format (samples/common/IO.h:27-70):
+    an 8-byte count, then the raw elements."""
+
+    @staticmethod
+    def loadBinary(path, dtype):
+        """loadBinary<T>: a numpy array of `dtype` elements (a structured or
+        sub-array dtype for vector types, e.g. ('<f8', 3) for vec3d)."""
+        import numpy as np
+        dt = np.dtype(dtype)
+        n = ctypes.c_uint64()
+        _check(_lib.bq_load_binary(os.fsencode(path), dt.itemsize, None, 0, ctypes.byref(n)))
+        out = np.empty(n.value, dtype=dt)
+        _check(_lib.bq_load_binary(os.fsencode(path), dt.itemsize, out.ctypes.data_as(ctypes.c_void_p), n.value,
+                                   ctypes.byref(n)))
+        return out
+
+    @staticmethod
+    def saveBinary(path, data):
+        """saveBinary<T>: writes len(data) elements of data's dtype."""
+        import numpy as np
+        a = np.ascontiguousarray(data)
+        item = a.dtype.itemsize * int(np.prod(a.shape[1:], dtype=np.int64))  # one row per element
+        _check(_lib.bq_save_binary(os.fsencode(path), a.ctypes.data_as(ctypes.c_void_p), a.shape[0], item))
+
+    @staticmethod
+    def loadPoints(path, dims=3):
+        """A vec_t<double,dims> point file as float32 (N, dims):
+        loadBinary + convert<float,dims>."""
+        import numpy as np
+        n = ctypes.c_uint64()
+        _check(_lib.bq_load_points_f64_as_f32(os.fsencode(path), dims, None, 0, ctypes.byref(n)))
+        out = np.empty((n.value, dims), dtype=np.float32)
+        _check(_lib.bq_load_points_f64_as_f32(os.fsencode(path), dims, out.ctypes.data_as(ctypes.c_void_p), n.value,
+                                              ctypes.byref(n)))
+        return out
 
 
 def version():

@@ -269,6 +269,22 @@ int bq_wide_box_query_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *bo
                          uint32_t numQueries, const uint32_t *offsets, uint64_t capacity, int32_t *ids,
                          const bq_allocator *alloc, bq_stream_t stream);
 
+/* ---------------------------------------------------------------- */
+/* binary-dump files (host only, no GPU)                              */
+/* ---------------------------------------------------------------- */
+/* The format of cuBQL::samples::loadBinary / saveBinary
+   (samples/common/IO.h:27-58): an 8-byte element count N, then N raw
+   elements of itemBytes each.  With out == NULL only *count is set;
+   otherwise N must not exceed capacity (elements). */
+int bq_load_binary(const char *path, size_t itemBytes, void *out, uint64_t capacity, uint64_t *count);
+int bq_save_binary(const char *path, const void *data, uint64_t count, size_t itemBytes);
+
+/* A file of vec_t<double,dims> points (what the reference's point
+   generator writes) loaded as float points: loadBinary followed by
+   convert<float,dims> (samples/common/IO.h:60-68), each coordinate
+   rounded to the nearest float.  out holds capacity*dims floats. */
+int bq_load_points_f64_as_f32(const char *path, int dims, float *out, uint64_t capacity, uint64_t *count);
+
 /* k nearest data points per query (1 <= k <= 64), ascending by squared
    distance.  Replaces cuBQL::points::findKNN
    (cuBQL/queries/points/knn.h:75-116).  ids/sqrDist are numQueries*k

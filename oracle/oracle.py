@@ -349,6 +349,20 @@ class RefCPU:
                                          _p(ex) if ex is not None else None, _p(ids), _p(d), ctypes.c_int(threads))
         return ids, d
 
+    def save_points_f64(self, path, pts):
+        """samples::saveBinary of vec3d points."""
+        pts = np.ascontiguousarray(pts, dtype=np.float64)
+        assert self.lib.ref_cpu_save_points_f64(os.fsencode(path), _p(pts), ctypes.c_uint64(len(pts))) == 0
+
+    def load_points_f64_as_f32(self, path, capacity):
+        """samples::loadBinary<vec3d> then convert<float,3>."""
+        out = np.zeros((max(capacity, 1), 3), dtype=np.float32)
+        n = ctypes.c_uint64()
+        rc = self.lib.ref_cpu_load_points_f64_as_f32(os.fsencode(path), _p(out), ctypes.c_uint64(capacity),
+                                                    ctypes.byref(n))
+        assert rc == 0
+        return out[: n.value].copy()
+
     def knn(self, nodes, prims, points, queries, k, maxSqr=np.inf, threads=1):
         nodes = np.ascontiguousarray(nodes, dtype=NODE)
         prims = np.ascontiguousarray(prims, dtype=np.uint32)

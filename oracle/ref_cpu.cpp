@@ -21,6 +21,7 @@
 #define __device__
 #endif
 #include "cuBQL/queries/triangles/findClosest.h"
+#include "samples/common/IO.h"
 
 #include <chrono>
 #include <cstring>
@@ -188,6 +189,34 @@ int ref_cpu_tri_closest(const void *nodes, uint32_t numNodes, const uint32_t *pr
       P[3 * (size_t)i + 2] = r.P.z;
     }
   });
+  return 0;
+}
+
+// samples/common/IO.h: saveBinary / loadBinary of vec3d points and the
+// convert<float,3> the samples apply after loading
+int ref_cpu_save_points_f64(const char *path, const double *pts, uint64_t n)
+{
+  std::vector<vec3d> v(n);
+  for (uint64_t i = 0; i < n; i++) v[i] = vec3d(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+  cuBQL::samples::saveBinary(path, v);
+  return 0;
+}
+
+int ref_cpu_load_points_f64_as_f32(const char *path, float *out, uint64_t capacity, uint64_t *n)
+{
+  try {
+    std::vector<vec3d> v = cuBQL::samples::loadBinary<vec3d>(path);
+    std::vector<vec3f> f = cuBQL::samples::convert<float, 3>(v);
+    *n = f.size();
+    if (f.size() > capacity) return -1;
+    for (size_t i = 0; i < f.size(); i++) {
+      out[3 * i] = f[i].x;
+      out[3 * i + 1] = f[i].y;
+      out[3 * i + 2] = f[i].z;
+    }
+  } catch (...) {
+    return -1;
+  }
   return 0;
 }
 
