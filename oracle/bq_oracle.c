@@ -397,6 +397,182 @@ int orc_sm_build(const obox *boxes, uint32_t n, int makeLeafThreshold, onode *no
 }
 
 /* ------------------------------------------------------------------ */
+/* binned SAH GPU builder (cuBQL/builder/cuda/sah_builder.h:22-538,    */
+/* dispatch gpu_builder.h:41-53).  16 bins per axis over the node's     */
+/* centroid bounds; bin boxes are the union of the prim boxes,          */
+/* AtomicBox-encoded (builder_common.h:38-167, empty = +-FLT_MAX).      */
+/* ------------------------------------------------------------------ */
+#define SAH_BINS 16
+typedef struct { int32_t lo[3], hi[3]; int32_t count, pad; } osah_bin; /* 32 B, as SAHBins::bins[] */
+typedef struct { osah_bin b[3][SAH_BINS]; } osah_bins;
+
+/* surfaceArea(box3f) (cuBQL/math/box.h:198-205): sx*sy + sx*sz + sy*sz */
+static float sah_area(const float *lo, const float *hi, int fma_mode)
+{
+  float sx = hi[0] - lo[0], sy = hi[1] - lo[1], sz = hi[2] - lo[2];
+  if (fma_mode) return fmaf(sy, sz, fmaf(sx, sy, sx * sz));
+  return (sx * sy + sx * sz) + sy * sz;
+}
+
+float orc_sah_area(const float *lo, const float *hi, int fma_mode) { return sah_area(lo, hi, fma_mode); }
+
+/* evaluateSAH (sah_builder.h:61-104): returns the split dim (-1: leaf) and
+   *splitBin; costs lArea*lCount + rArea*rCount */
+int orc_sah_evaluate(const osah_bins *s, int fma_mode, int *splitBin)
+{
+  float bestCost = INFINITY;
+  int splitDim = -1;
+  float rAreas[SAH_BINS];
+  for (int d = 0; d < 3; d++) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    int rCount = 0;
+    for (int b = SAH_BINS - 1; b >= 0; --b) {
+      const osah_bin *bin = &s->b[d][b];
+      for (int k = 0; k < 3; k++) {
+        float bl = dec_f(bin->lo[k]), bh = dec_f(bin->hi[k]);
+        if (bl < lo[k]) lo[k] = bl;
+        if (bh > hi[k]) hi[k] = bh;
+      }
+      rCount += bin->count;
+      rAreas[b] = sah_area(lo, hi, fma_mode);
+    }
+    float leafCost = rAreas[0] * (float)rCount;
+    if (leafCost < bestCost) { bestCost = leafCost; splitDim = -1; }
+    lo[0] = lo[1] = lo[2] = INFINITY;
+    hi[0] = hi[1] = hi[2] = -INFINITY;
+    int lCount = 0;
+    for (int b = 0; b < SAH_BINS; b++) {
+      float rArea = rAreas[b];
+      float lArea = sah_area(lo, hi, fma_mode);
+      if (lCount > 0 && rCount > 0) {
+        float cost = fma_mode ? fmaf(lArea, (float)lCount, rArea * (float)rCount)
+                              : lArea * (float)lCount + rArea * (float)rCount;
+        if (cost < bestCost) { bestCost = cost; splitDim = d; *splitBin = b; }
+      }
+      const osah_bin *bin = &s->b[d][b];
+      for (int k = 0; k < 3; k++) {
+        float bl = dec_f(bin->lo[k]), bh = dec_f(bin->hi[k]);
+        if (bl < lo[k]) lo[k] = bl;
+        if (bh > hi[k]) hi[k] = bh;
+      }
+      lCount += bin->count;
+      rCount -= bin->count;
+    }
+  }
+  return splitDim;
+}
+
+/* bin of a centroid coordinate (binPrims :170-180, updatePrims :300-306) */
+static int sah_bin_of(float c, float lo, float hi)
+{
+  if (!(hi > lo)) return 0;
+  float rel = (c - lo) / ((hi - lo) + 1e-20f);
+  float f = rel * (float)SAH_BINS;
+  int bin = (f != f) ? 0 : (f >= 2147483647.f ? 2147483647 : (f <= -2147483648.f ? (-2147483647 - 1) : (int)f));
+  return bin < 0 ? 0 : (bin > SAH_BINS - 1 ? SAH_BINS - 1 : bin);
+}
+
+static void sah_center(const obox *b, int d, float *c) { *c = 0.5f * (b->lo[d] + b->hi[d]); }
+
+/* Level-synchronous, BFS numbering; partitions stable, so leaves list
+   their prims in ascending primID order (the reference's final
+   (nodeID, primID) sort, :446-473).  A node the heuristic would make a
+   leaf of more than 65535 prims (the 16-bit count) is split in halves
+   by position instead (the reference writes a truncated count). */
+int orc_sah_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int fma_mode, onode *nodes,
+                  uint32_t *primIDs, uint32_t *numNodes, uint32_t *numPrims)
+{
+  if (n == 0) { *numNodes = 0; *numPrims = 0; return 0; }
+  int thr = makeLeafThreshold;
+  uint32_t *cur = primIDs, *alt = (uint32_t *)malloc(sizeof(uint32_t) * n);
+  uint32_t nv = 0, ninv = 0;
+  for (uint32_t i = 0; i < n; i++)                     /* initPrims :124-146 */
+    if (boxes[i].lo[0] <= boxes[i].hi[0]) cur[nv++] = i;
+  for (uint32_t i = 0; i < n; i++)
+    if (!(boxes[i].lo[0] <= boxes[i].hi[0])) { cur[nv + ninv] = i; ninv++; }
+  uint64_t cap = 2ull * n + 2;
+  sm_open *lvl = (sm_open *)malloc(sizeof(sm_open) * cap);
+  uint32_t *lvlId = (uint32_t *)malloc(sizeof(uint32_t) * cap);
+  sm_open *nxt = (sm_open *)malloc(sizeof(sm_open) * cap);
+  uint32_t *nxtId = (uint32_t *)malloc(sizeof(uint32_t) * cap);
+  osah_bins *bins = (osah_bins *)malloc(sizeof(osah_bins));
+  memset(&nodes[0], 0, 2 * sizeof(onode));
+  uint64_t alloc = 2, nl = 1;
+  lvl[0].begin = 0; lvl[0].end = nv; lvlId[0] = 0;
+  sm_bounds(boxes, cur, 0, nv, &lvl[0]);
+  while (nl) {
+    uint64_t nn = 0;
+    for (uint64_t k = 0; k < nl; k++) {
+      sm_open *o = &lvl[k];
+      uint32_t id = lvlId[k], count = o->end - o->begin;
+      memset(&nodes[id], 0, sizeof(onode));
+      int dim = -1, sbin = 0;
+      float clo[3], chi[3];
+      for (int d = 0; d < 3; d++) { clo[d] = dec_f(o->cbLo[d]); chi[d] = dec_f(o->cbHi[d]); }
+      if ((int64_t)count > thr) {                       /* selectSplits :220-263 */
+        for (int d = 0; d < 3; d++)
+          for (int b = 0; b < SAH_BINS; b++) {
+            osah_bin *x = &bins->b[d][b];
+            for (int k = 0; k < 3; k++) { x->lo[k] = enc_f(FLT_MAX); x->hi[k] = enc_f(-FLT_MAX); }
+            x->count = 0;
+          }
+        for (uint32_t i = o->begin; i < o->end; i++) {  /* binPrims :148-197 */
+          const obox *pb = &boxes[cur[i]];
+          for (int d = 0; d < 3; d++) {
+            float c;
+            sah_center(pb, d, &c);
+            osah_bin *x = &bins->b[d][sah_bin_of(c, clo[d], chi[d])];
+            for (int k = 0; k < 3; k++) {
+              int32_t el = enc_f(pb->lo[k]), eh = enc_f(pb->hi[k]);
+              if (el < x->lo[k]) x->lo[k] = el;
+              if (eh > x->hi[k]) x->hi[k] = eh;
+            }
+            x->count++;
+          }
+        }
+        dim = orc_sah_evaluate(bins, fma_mode, &sbin);
+      }
+      int halves = dim < 0 && count > 65535u;
+      if (dim < 0 && !halves) { nodes[id].admin = ADMIN(o->begin, count); continue; }
+      /* updatePrims :266-310: side = (bin along dim >= split bin), stable */
+      uint32_t nLeft = 0;
+      for (uint32_t i = o->begin; i < o->end; i++) {
+        float c = 0.f;
+        if (!halves) sah_center(&boxes[cur[i]], dim, &c);
+        int side = halves ? (i - o->begin) >= count / 2 : sah_bin_of(c, clo[dim], chi[dim]) >= sbin;
+        if (!side) nLeft++;
+      }
+      uint32_t wl = o->begin, wr = o->begin + nLeft;
+      for (uint32_t i = o->begin; i < o->end; i++) {
+        float c = 0.f;
+        if (!halves) sah_center(&boxes[cur[i]], dim, &c);
+        int side = halves ? (i - o->begin) >= count / 2 : sah_bin_of(c, clo[dim], chi[dim]) >= sbin;
+        if (!side) alt[wl++] = cur[i]; else alt[wr++] = cur[i];
+      }
+      memcpy(cur + o->begin, alt + o->begin, sizeof(uint32_t) * count);
+      if (nLeft == 0 || nLeft == count) {             /* cannot happen: the split had both sides */
+        free(alt); free(lvl); free(lvlId); free(nxt); free(nxtId); free(bins);
+        return -1;
+      }
+      uint64_t c = alloc; alloc += 2;
+      nodes[id].admin = ADMIN(c, 0);
+      nxt[nn].begin = o->begin; nxt[nn].end = o->begin + nLeft; nxtId[nn] = (uint32_t)c;
+      sm_bounds(boxes, cur, nxt[nn].begin, nxt[nn].end, &nxt[nn]); nn++;
+      nxt[nn].begin = o->begin + nLeft; nxt[nn].end = o->end; nxtId[nn] = (uint32_t)c + 1;
+      sm_bounds(boxes, cur, nxt[nn].begin, nxt[nn].end, &nxt[nn]); nn++;
+    }
+    sm_open *t = lvl; lvl = nxt; nxt = t;
+    uint32_t *ti = lvlId; lvlId = nxtId; nxtId = ti;
+    nl = nn;
+  }
+  *numNodes = (uint32_t)alloc;
+  *numPrims = n;
+  refit_tree(nodes, *numNodes, cur, boxes);
+  free(alt); free(lvl); free(lvlId); free(nxt); free(nxtId); free(bins);
+  return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* host spatial-median builder cpuBuilder (cuBQL/builder/cpu/           */
 /* spatialMedian.h:45-180): recursive, DFS numbering, right side filled */
 /* from the end backwards.                                              */

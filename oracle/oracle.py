@@ -20,6 +20,10 @@ REF_GPU_SO = os.path.join(HERE, "_ref", "libref_gpu.so")
 
 NODE = np.dtype([("lower", "<f4", 3), ("upper", "<f4", 3), ("admin", "<u8")])
 assert NODE.itemsize == 32
+# one SAH bin (sah_builder.h:53-60): AtomicBox-encoded bounds + count, 32 B
+SAH_BIN = np.dtype([("lo", "<i4", 3), ("hi", "<i4", 3), ("count", "<i4"), ("pad", "<i4")])
+SAH_BINS = np.dtype([("b", SAH_BIN, (3, 16))])
+assert SAH_BINS.itemsize == 1536
 
 
 def _f32(a):
@@ -108,6 +112,28 @@ class Oracle:
 
     def sm_build(self, boxes, makeLeafThreshold=0):
         return self._tree(self.lib.orc_sm_build, boxes, ctypes.c_int(makeLeafThreshold))
+
+    def sah_build(self, boxes, makeLeafThreshold=0, fma_mode=1):
+        return self._tree(self.lib.orc_sah_build, boxes, ctypes.c_int(makeLeafThreshold), ctypes.c_int(fma_mode))
+
+    def sah_evaluate(self, bins, fma_mode=1):
+        """evaluateSAH per SAH_BINS record: (dims (-1 leaf), bins)."""
+        bins = np.ascontiguousarray(bins, dtype=SAH_BINS)
+        dims = np.zeros(len(bins), dtype=np.int32)
+        sb = np.zeros(len(bins), dtype=np.int32)
+        for i in range(len(bins)):
+            b = ctypes.c_int(0)
+            dims[i] = self.lib.orc_sah_evaluate(bins[i:i + 1].ctypes.data_as(ctypes.c_void_p), ctypes.c_int(fma_mode),
+                                                ctypes.byref(b))
+            sb[i] = b.value
+        return dims, sb
+
+    def sah_area(self, boxes, fma_mode=1):
+        f = self.lib.orc_sah_area
+        f.restype = ctypes.c_float
+        boxes = _f32(boxes).reshape(-1, 6)
+        return np.array([f(_p(boxes[i, :3].copy()), _p(boxes[i, 3:].copy()), ctypes.c_int(fma_mode))
+                         for i in range(len(boxes))], dtype=np.float32)
 
     def cpu_build(self, boxes, makeLeafThreshold=0):
         return self._tree(self.lib.orc_cpu_build, boxes, ctypes.c_int(makeLeafThreshold))
@@ -393,7 +419,7 @@ class RefCPU:
 
 class RefGPU:
     """The reference's GPU code (runs only where a GPU is present)."""
-    RADIX, SPATIAL_MEDIAN, REBIN, WIDE4, WIDE8 = 0, 1, 2, 3, 4
+    RADIX, SPATIAL_MEDIAN, REBIN, WIDE4, WIDE8, SAH = 0, 1, 2, 3, 4, 5
 
     def __init__(self):
         self.lib = _load(REF_GPU_SO)
@@ -439,6 +465,19 @@ class RefGPU:
                                               _p(ex) if ex is not None else None, _p(ids), _p(d))
         assert rc == 0
         return ids, d
+
+    def sah_pin(self, bins, boxes):
+        """The reference's evaluateSAH on each SAH_BINS record and its
+        surfaceArea on each box: (dims, splitBins, areas)."""
+        bins = np.ascontiguousarray(bins, dtype=SAH_BINS)
+        boxes = _f32(boxes).reshape(-1, 6)
+        dims = np.zeros(len(bins), dtype=np.int32)
+        sb = np.zeros(len(bins), dtype=np.int32)
+        areas = np.zeros(len(boxes), dtype=np.float32)
+        rc = self.lib.ref_gpu_sah_pin(_p(bins), ctypes.c_int(len(bins)), _p(dims), _p(sb), _p(boxes),
+                                      ctypes.c_int(len(boxes)), _p(areas))
+        assert rc == 0
+        return dims, sb, areas
 
     def build_wide(self, width, boxes, makeLeafThreshold=0):
         """The reference's gpuBuilder into a WideBVH<float,3,width>:

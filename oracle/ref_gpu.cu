@@ -111,6 +111,21 @@ __global__ void k_box(bvh3f bvh, const box3f *boxes, const box3f *qb, int nq, co
   counts[tid] = c;
 }
 
+// evaluateSAH and surfaceArea of the reference, for pinning their FMA shapes
+static_assert(sizeof(sahBuilder_impl::SAHBins) == 1536, "SAHBins layout");
+__global__ void k_sah_pin(const sahBuilder_impl::SAHBins *bins, int nb, int *dims, int *splitBins,
+                          const box3f *boxes, int nbox, float *areas)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid < nb) {
+    int splitDim = -1, splitBin = 0;
+    sahBuilder_impl::evaluateSAH(splitDim, splitBin, bins[tid]);
+    dims[tid] = splitDim;
+    splitBins[tid] = splitDim < 0 ? 0 : splitBin;
+  }
+  if (tid < nbox) areas[tid] = surfaceArea(boxes[tid]);
+}
+
 template <int KMAX>
 __global__ void k_knn(bvh3f bvh, const vec3f *pts, const vec3f *qs, int nq, int k, float maxSqr, int *ids,
                       float *dists, int *numFound)
@@ -333,7 +348,9 @@ int run_build(int method, const box3f *d_boxes, uint32_t n, int leafThr, bvh3f &
 {
   BuildConfig cfg;
   cfg.makeLeafThreshold = leafThr;
-  if (method == 0)
+  if (method == 5)
+    cuBQL::cuda::sahBuilder(bvh, d_boxes, n, cfg);
+  else if (method == 0)
     cuBQL::cuda::radixBuilder(bvh, d_boxes, n, cfg);
   else if (method == 1)
     gpuBuilder(bvh, d_boxes, n, cfg);
@@ -347,7 +364,8 @@ extern "C" {
 
 int ref_gpu_node_size(void) { return (int)sizeof(bvh3f::Node); }
 
-// method: 0 radixBuilder, 1 gpuBuilder (spatial median), 2 rebinRadixBuilder.
+// method: 0 radixBuilder, 1 gpuBuilder (spatial median), 2 rebinRadixBuilder,
+// 5 cuda::sahBuilder.
 // nodesOut must hold 2n+2 nodes, primIDsOut n entries.
 int ref_gpu_build(int method, const float *boxes, uint32_t n, int makeLeafThreshold, void *nodesOut,
                   uint32_t *primIDsOut, uint32_t *numNodes, uint32_t *numPrims)
@@ -615,6 +633,22 @@ int ref_gpu_time_box_query(int method, const float *points, uint32_t n, int make
   cudaFree(dp); cudaFree(db); cudaFree(dq); cudaFree(dc); cudaFree(doff); cudaFree(di);
   *ms_out = total / (reps > 0 ? reps : 1);
   *total_out = ho[nq];
+  return 0;
+}
+
+int ref_gpu_sah_pin(const void *bins, int nb, int *dims, int *splitBins, const float *boxes, int nbox, float *areas)
+{
+  auto *db = dalloc_copy((const sahBuilder_impl::SAHBins *)bins, nb);
+  box3f *dbox = dalloc_copy((const box3f *)boxes, nbox);
+  int *dd = dalloc_copy<int>(nullptr, nb), *ds = dalloc_copy<int>(nullptr, nb);
+  float *da = dalloc_copy<float>(nullptr, nbox);
+  const int n = nb > nbox ? nb : nbox;
+  k_sah_pin<<<(n + 127) / 128, 128>>>(db, nb, dd, ds, dbox, nbox, da);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(dims, dd, sizeof(int) * nb, cudaMemcpyDeviceToHost);
+  cudaMemcpy(splitBins, ds, sizeof(int) * nb, cudaMemcpyDeviceToHost);
+  cudaMemcpy(areas, da, sizeof(float) * nbox, cudaMemcpyDeviceToHost);
+  cudaFree(db); cudaFree(dbox); cudaFree(dd); cudaFree(ds); cudaFree(da);
   return 0;
 }
 

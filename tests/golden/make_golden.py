@@ -9,6 +9,8 @@
                                            # reference's fixedBoxQuery results
   python tests/golden/make_golden.py gpu_wide   # on a B200: the reference's
                                            # WideBVH builds and queries
+  python tests/golden/make_golden.py gpu_sah    # on a B200: the reference's
+                                           # SAH builds and evaluateSAH
 
 Both read oracle/_ref/ (the reference compiled from its own sources by
 oracle/build_ref.sh).  Inputs are the seeded generators of
@@ -203,6 +205,68 @@ def gpu_wide():
     np.savez_compressed(dest, **out)
 
 
+def sah_pin_inputs(n=4000, seed=9):
+    """Seeded SAH bin sets for pinning evaluateSAH: half with coordinates on
+    a 1/8 grid (many exactly equal costs: tie rules), half with full
+    mantissas (rounding shapes); counts 0..4, empty bins as AtomicBox
+    leaves them (+-FLT_MAX encoded); plus boxes for surfaceArea."""
+    from oracle.oracle import SAH_BINS
+
+    def enc(f):
+        b = np.asarray(f, np.float32).view(np.int32)
+        return np.where(b < 0, b ^ np.int32(0x7fffffff), b).astype(np.int32)
+
+    rng = np.random.default_rng(seed)
+    bins = np.zeros(n, dtype=SAH_BINS)
+    cnt = rng.integers(0, 5, size=(n, 3, 16))
+    cnt[rng.random((n, 3, 16)) < 0.3] = 0
+    lo = rng.random((n, 3, 16, 3)).astype(np.float32)
+    ext = (rng.random((n, 3, 16, 3)) * 0.3).astype(np.float32)
+    grid = np.arange(n) < n // 2
+    lo[grid] = np.floor(lo[grid] * 8) / 8
+    ext[grid] = np.floor(ext[grid] * 8) / 8
+    hi = (lo + ext).astype(np.float32)
+    empty = cnt == 0
+    flt_max = np.float32(3.4028234663852886e38)
+    lo[empty] = flt_max
+    hi[empty] = -flt_max
+    bins["b"]["lo"] = enc(lo)
+    bins["b"]["hi"] = enc(hi)
+    bins["b"]["count"] = cnt
+    bl = rng.random((n, 3)).astype(np.float32) * 10
+    boxes = np.concatenate([bl, bl + rng.random((n, 3)).astype(np.float32)], 1).astype(np.float32)
+    return bins, boxes
+
+
+def sah_tree_inputs():
+    """Point boxes (uniform, GMM), triangle boxes of an icosphere and boxes
+    with random extents."""
+    rng = np.random.default_rng(12)
+    verts, tris = W.icosphere(3)
+    tb = np.stack([verts[tris].min(1), verts[tris].max(1)], 1).reshape(-1, 6).astype(np.float32)
+    c = W.uniform_points(2000, 33)
+    h = (rng.random((2000, 3)) * 0.05).astype(np.float32)
+    return (("u", W.point_boxes(W.uniform_points(3000))), ("g", W.point_boxes(W.gmm_points(3000, offset=0.0))),
+            ("t", tb), ("e", np.concatenate([c - h, c + h], 1).astype(np.float32)))
+
+
+def gpu_sah():
+    from oracle.oracle import RefGPU
+    r = RefGPU()
+    o = Oracle()
+    out = {}
+    bins, boxes = sah_pin_inputs()
+    out["pin_dims"], out["pin_bins"], out["pin_areas"] = r.sah_pin(bins, boxes)
+    for name, b in sah_tree_inputs():
+        out[f"{name}_boxes"] = b
+        for thr in (0, 4):
+            n, pr = r.build(RefGPU.SAH, b, thr)
+            cn, cp = o.canonicalize(n, pr)
+            out[f"{name}{thr}_nodes"], out[f"{name}{thr}_prims"] = cn.view(np.uint8), cp
+    dest = sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu_sah.npz")
+    np.savez_compressed(dest, **out)
+
+
 if __name__ == "__main__":
     {"cpu": cpu, "gpu": gpu, "gpu_rebin": gpu_rebin, "gpu_boxquery": gpu_boxquery,
-     "gpu_wide": gpu_wide}[sys.argv[1]]()
+     "gpu_wide": gpu_wide, "gpu_sah": gpu_sah}[sys.argv[1]]()
