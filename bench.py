@@ -172,7 +172,29 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": "Mprims/s", "cores": threads, "kind": kind,
                              "sample": f"{threads} concurrent cpuBuilder builds of {sample} uniform points per step"},
             "e2e": {"value": value, "unit": "Mprims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_components:
+        line["reference_components"] = reference_components(W, args.n)
     print(json.dumps(line))
+
+
+def reference_components(W, n):
+    """The reference's own GPU code (compiled for sm_100a from its sources
+    into oracle/_ref) and host code on the workloads of our arm's
+    components: the same seeds and sizes."""
+    import numpy as np
+    from oracle.oracle import RefGPU, have_ref_gpu
+    comp = {}
+    pts_np = W.uniform_points(n, W.SEED_DATA)
+    reference_gpu(comp, pts_np, W)
+    comp["c1_reference"] = c1_reference(W, pts_np)
+    if have_ref_gpu():
+        verts, tris = W.icosphere(8)
+        tv = verts[tris]
+        tbox = np.concatenate([tv.min(1), tv.max(1)], 1).astype(np.float32)
+        comp["sah_build_triangles"] = {"triangles": int(len(tris)),
+                                       "reference_sahBuilder_ms": RefGPU().time_build_boxes(RefGPU.SAH, tbox, 0,
+                                                                                           reps=2)}
+    return comp
 
 
 def _timed(fn):
@@ -342,7 +364,16 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
         ids, d, _ = fwd()
         bq.triangles.distanceBackward(tt, tv, tq, ids, g1)
 
-    tb = bq.cuda.radixBuilder(bq.triangles.boxes(tt, tv))
+    # SAH and spatial-median builds over the triangle boxes (the SAH builder's use case)
+    tbox = bq.triangles.boxes(tt, tv)
+    ms_sah = ev_time(lambda: bq.cuda.sahBuilder(tbox).free())
+    ms_smt = ev_time(lambda: bq.gpuBuilder(tbox).free())
+    with bq.profile() as prof:
+        bq.cuda.sahBuilder(tbox).free()
+    comp["sah_build_triangles"] = {"triangles": int(len(tris)), "ms": ms_sah, "Mprims_s": len(tris) / ms_sah / 1e3,
+                                   "spatial_median_ms": ms_smt,
+                                   "phases_ms": {k: round(v[1], 4) for k, v in prof.table.items()}}
+    tb = bq.cuda.radixBuilder(tbox)
     ms_f = ev_time(lambda: bq.triangles.findClosest(tb, tt, tv, tq))
     ids, _, _ = bq.triangles.findClosest(tb, tt, tv, tq)
     ms_b = ev_time(lambda: bq.triangles.distanceBackward(tt, tv, tq, ids, g1))
@@ -377,9 +408,8 @@ def _ev_time(torch, fn, reps=3, warm=1):
 
 def c1_component(bq, W, torch, comp, pts_np, tp, boxes_t):
     """The 1M-point configuration: spatial-median build (leaf 8) and 1M
-    closest-point queries, ours against the reference's GPU builder and
-    kernel (sm_100a) and the reference's host builder and query (one core,
-    and all cores for the query)."""
+    closest-point queries (the reference's numbers for the same workload
+    are in the reference arm's line, c1_reference)."""
     n1 = 1_000_000
     b1, tp1 = boxes_t[:n1], tp[:n1]
     q1 = W.uniform_points(n1, W.SEED_QUERIES, -0.1, 1.1)
@@ -389,8 +419,17 @@ def c1_component(bq, W, torch, comp, pts_np, tp, boxes_t):
     t = bq.gpuBuilder(b1, cfg)
     ms_q = _ev_time(torch, lambda: bq.points.findClosest(t, tp1, tq1))
     t.free()
-    out = {"points": n1, "queries": n1, "leaf": 8, "build_ms": ms_b, "closest_point_ms": ms_q,
-           "build_Mprims_s": n1 / ms_b / 1e3, "Mqueries_s": n1 / ms_q / 1e3}
+    comp["c1_1M_points_leaf8"] = {"points": n1, "queries": n1, "leaf": 8, "build_ms": ms_b, "closest_point_ms": ms_q,
+                                  "build_Mprims_s": n1 / ms_b / 1e3, "Mqueries_s": n1 / ms_q / 1e3}
+
+
+def c1_reference(W, pts_np):
+    """The reference's GPU builder and kernel (sm_100a) and its host builder
+    and query (one core, and all cores for the query) on the 1M-point
+    configuration."""
+    n1 = 1_000_000
+    q1 = W.uniform_points(n1, W.SEED_QUERIES, -0.1, 1.1)
+    out = {}
     from oracle.oracle import RefCPU, RefGPU, have_ref_cpu, have_ref_gpu
     if have_ref_gpu():
         r = RefGPU()
@@ -411,7 +450,7 @@ def c1_component(bq, W, torch, comp, pts_np, tp, boxes_t):
         rc.closest_point(nodes, prims, pts_np[:n1], q1, threads=threads)
         out["reference_cpu_closest_point_ms_allcores"] = (time.perf_counter() - t0) * 1e3
         out["host_threads"] = threads
-    comp["c1_1M_points_leaf8"] = out
+    return out
 
 
 def batched_components(bq, W, torch, comp):
@@ -620,7 +659,6 @@ def run_ours(args):
         components(bq, W, torch, pts_np, tp, boxes_t, comp)
         c1_component(bq, W, torch, comp, pts_np, tp, boxes_t)
         batched_components(bq, W, torch, comp)
-        reference_gpu(comp, pts_np, W)
     if rank == 0:
         cpu_baseline = cpu_leg(W, pts_np)
     barrier(world)

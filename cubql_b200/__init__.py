@@ -95,6 +95,8 @@ _SIGS = {
                                    ctypes.POINTER(bq_allocator), _P],
     "bq_build_spatial_median_f3": [ctypes.POINTER(bq_bvh3f), _P, _U, ctypes.POINTER(bq_build_config),
                                    ctypes.POINTER(bq_allocator), _P],
+    "bq_build_sah_f3": [ctypes.POINTER(bq_bvh3f), _P, _U, ctypes.POINTER(bq_build_config), ctypes.POINTER(bq_allocator),
+                        _P],
     "bq_refit_f3": [ctypes.POINTER(bq_bvh3f), _P, ctypes.POINTER(bq_allocator), _P],
     "bq_refit_noalloc_f3": [ctypes.POINTER(bq_bvh3f), _P, _P],
     "bq_free_f3": [ctypes.POINTER(bq_bvh3f), ctypes.POINTER(bq_allocator), _P],
@@ -219,11 +221,18 @@ def default_allocator():
 class BuildConfig:
     """cuBQL::BuildConfig (cuBQL/bvh.h:31-64)."""
     SPATIAL_MEDIAN = 0
+    SAH = 1
+    ELH = 2
 
     def __init__(self, makeLeafThreshold=0, maxAllowedLeafSize=1 << 15, buildMethod=0):
         self.makeLeafThreshold = makeLeafThreshold
         self.maxAllowedLeafSize = maxAllowedLeafSize
         self.buildMethod = buildMethod
+
+    def enableSAH(self):
+        """BuildConfig::enableSAH (cuBQL/bvh.h:32)."""
+        self.buildMethod = BuildConfig.SAH
+        return self
 
     def c(self):
         return bq_build_config(self.maxAllowedLeafSize, self.makeLeafThreshold, self.buildMethod)
@@ -372,6 +381,11 @@ class cuda:
     def radixBuilder(boxes, config=None, allocator=None):
         """cuBQL::cuda::radixBuilder (cuBQL/builder/cuda.h:134-140), 63-bit keys."""
         return _build(_lib.bq_build_morton63_f3, boxes, config, allocator)
+
+    @staticmethod
+    def sahBuilder(boxes, config=None, allocator=None):
+        """cuBQL::cuda::sahBuilder (cuBQL/builder/cuda.h:118-129): binned SAH."""
+        return _build(_lib.bq_build_sah_f3, boxes, config, allocator)
 
     @staticmethod
     def rebinRadixBuilder(boxes, config=None, allocator=None):

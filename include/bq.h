@@ -47,6 +47,8 @@ extern "C" {
 
 /* build methods (cuBQL/bvh.h:38-55 BuildConfig::BuildMethod) */
 #define BQ_SPATIAL_MEDIAN 0
+#define BQ_SAH 1 /* binned surface-area heuristic (BuildConfig::SAH) */
+#define BQ_ELH 2 /* edge-length heuristic: not implemented (BQ_ERR_UNSUPPORTED) */
 #define BQ_MORTON63 16 /* cuda::radixBuilder */
 #define BQ_MORTON30 17 /* cuda::rebinRadixBuilder */
 
@@ -78,7 +80,7 @@ typedef struct bq_bvh3f {
 typedef struct bq_build_config {
   int maxAllowedLeafSize; /* default 1<<15 */
   int makeLeafThreshold;  /* 0 = builder default (1) */
-  int buildMethod;        /* BQ_SPATIAL_MEDIAN (gpuBuilder only) */
+  int buildMethod;        /* BQ_SPATIAL_MEDIAN or BQ_SAH (bq_build_spatial_median_f3 only) */
 } bq_build_config;
 
 /* replaces cuBQL::GpuMemoryResource (cuBQL/builder/cuda.h:31-78).
@@ -127,11 +129,24 @@ int bq_build_morton63_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims
 int bq_build_rebin_morton30_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
                                const bq_allocator *alloc, bq_stream_t stream);
 
-/* Spatial-median builder.  Replaces cuBQL::gpuBuilder<float,3>
-   (cuBQL/builder/cuda.h:91-99, cuBQL/builder/cuda/gpu_builder.h:31-67,
-   cuBQL/builder/cuda/sm_builder.h:469-614). */
+/* Replaces cuBQL::gpuBuilder<float,3> (cuBQL/builder/cuda.h:91-99,
+   cuBQL/builder/cuda/gpu_builder.h:31-67): cfg->buildMethod
+   BQ_SPATIAL_MEDIAN (default) is the spatial-median builder
+   (cuBQL/builder/cuda/sm_builder.h:469-614), BQ_SAH the SAH builder
+   (as bq_build_sah_f3), BQ_ELH is not implemented. */
 int bq_build_spatial_median_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
                                const bq_allocator *alloc, bq_stream_t stream);
+
+/* Binned SAH builder.  Replaces cuBQL::cuda::sahBuilder<float,3>
+   (cuBQL/builder/cuda.h:118-129, cuBQL/builder/cuda/sah_builder.h:
+   320-538): 16 centroid bins per axis, evaluateSAH's leaf-versus-split
+   costs with surfaceArea, prims with bin >= the split bin to the right.
+   The tree equals the reference's after BFS renumbering; leaves list their
+   prims in ascending primID order.  A node the heuristic would make a
+   leaf of more than 65535 prims (the reference's 16-bit count wraps) is
+   split in halves by position.  makeLeafThreshold 0 and 1 are the same. */
+int bq_build_sah_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
+                    const bq_allocator *alloc, bq_stream_t stream);
 
 /* Recomputes every node box bottom-up from `boxes`.  Replaces
    gpuBuilder_impl::refit (cuBQL/builder/cuda/sm_builder.h:677-693). */

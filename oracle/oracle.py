@@ -596,6 +596,14 @@ class RefGPU:
         assert rc == 0
         return ms.value
 
+    def time_build_boxes(self, method, boxes, makeLeafThreshold=0, reps=3):
+        boxes = _f32(boxes).reshape(-1, 6)
+        ms = ctypes.c_float()
+        rc = self.lib.ref_gpu_time_build_boxes(ctypes.c_int(method), _p(boxes), ctypes.c_uint32(len(boxes)),
+                                               ctypes.c_int(makeLeafThreshold), ctypes.c_int(reps), ctypes.byref(ms))
+        assert rc == 0
+        return ms.value
+
     def time_query(self, method, points, queries, kind, makeLeafThreshold=0, reps=5):
         points, queries = _f32(points), _f32(queries)
         ms = ctypes.c_float()

@@ -548,6 +548,34 @@ int ref_gpu_time_build(int method, const float *points, uint32_t n, int makeLeaf
   return 0;
 }
 
+// As ref_gpu_time_build, over given boxes (e.g. triangle boxes)
+int ref_gpu_time_build_boxes(int method, const float *boxes, uint32_t n, int makeLeafThreshold, int reps,
+                             float *ms_out)
+{
+  box3f *db = dalloc_copy((const box3f *)boxes, n);
+  if (!db) return -1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float total = 0.f;
+  for (int r = -1; r < reps; r++) {
+    bvh3f bvh;
+    cudaEventRecord(e0);
+    run_build(method, db, n, makeLeafThreshold, bvh);
+    cudaEventRecord(e1);
+    RCHECK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r >= 0) total += ms;
+    cuBQL::cuda::free(bvh);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(db);
+  *ms_out = total / (reps > 0 ? reps : 1);
+  return 0;
+}
+
 // Times one-thread-per-query reference kernels over a tree built with
 // `method` on the points: kind 0 closest point, kind k>0 kNN with that k.
 int ref_gpu_time_query(int method, const float *points, uint32_t n, int makeLeafThreshold, const float *queries,
