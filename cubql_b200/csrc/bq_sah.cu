@@ -43,7 +43,7 @@ namespace {
 constexpr int SAH_BINS = 16;
 constexpr int SAH_NB = 3 * SAH_BINS;         // bins per node (3 axes)
 constexpr int SAH_W = 7;                     // words per bin: lo[3], hi[3], count
-constexpr uint32_t SAH_WARP_MAX = 4096;      // subtrees up to this size: one warp
+constexpr uint32_t SAH_WARP_MAX = 128;       // subtrees up to this size: one warp
 constexpr uint32_t SAH_TILE = 4096;          // prims per tile in the global levels
 constexpr int SAH_BLOCK = 256;
 constexpr int SAHW_BLOCK = 128;
@@ -131,28 +131,29 @@ __device__ __forceinline__ void bins_add(int32_t *bins, const SahPrim &p, const 
   }
 }
 
-// evaluateSAH over 48 bins (bins[(d*16+b)*7 + ...]) by one warp: lane b
-// (and b+16) holds bin b of the current axis; unions and counts by
-// 16-lane scans; the first strictly cheapest candidate in (axis, bin)
-// order wins if cheaper than the leaf, as in the reference's serial loop.
-__device__ __forceinline__ SahDec sah_evaluate(const int32_t *bins)
+// evaluateSAH by one warp over per-lane bins.  Pass 0: lane L holds bin
+// L & 15 of axis L >> 4 (a*); pass 1: bin L & 15 of axis 2 (b*, lanes
+// 16..31 repeat it and propose nothing).  Unions and counts by 16-lane
+// scans; the first strictly cheapest candidate in (axis, bin) order wins
+// if it is cheaper than the leaf, as in the reference's serial loop.  Empty
+// bins are (+FLT_MAX, -FLT_MAX), as AtomicBox leaves them.
+__device__ __forceinline__ SahDec sah_evaluate_lanes(const float aLo[3], const float aHi[3], int aCnt,
+                                                     const float bLo[3], const float bHi[3], int bCnt)
 {
   const int lane = threadIdx.x & 31, b = lane & 15;
   float leafCost = INFINITY;
   float best = INFINITY;
   int bestIdx = INT_MAX;
-#pragma unroll 1
-  for (int d = 0; d < 3; d++) {
-    const int32_t *x = bins + (d * SAH_BINS + b) * SAH_W;
-    float lo[3], hi[3];
 #pragma unroll
-    for (int k = 0; k < 3; k++) { lo[k] = dec_f(x[k]); hi[k] = dec_f(x[3 + k]); }
-    const int cnt = x[6];
-    // inclusive prefix (bins 0..b) and suffix (bins b..15) unions / counts
+  for (int pass = 0; pass < 2; pass++) {
     float plo[3], phi[3], slo[3], shi[3];
-    int pc = cnt, sc = cnt;
+    int pc = pass ? bCnt : aCnt, sc = pc;
 #pragma unroll
-    for (int k = 0; k < 3; k++) { plo[k] = slo[k] = lo[k]; phi[k] = shi[k] = hi[k]; }
+    for (int k = 0; k < 3; k++) {
+      plo[k] = slo[k] = pass ? bLo[k] : aLo[k];
+      phi[k] = shi[k] = pass ? bHi[k] : aHi[k];
+    }
+    // inclusive prefix (bins 0..b) and suffix (bins b..15) unions / counts
 #pragma unroll
     for (int o = 1; o < 16; o <<= 1) {
       const int pcu = __shfl_up_sync(0xffffffffu, pc, o, 16);
@@ -169,7 +170,7 @@ __device__ __forceinline__ SahDec sah_evaluate(const int32_t *bins)
         if (b + o < 16) { slo[k] = fminf(slo[k], a2); shi[k] = fmaxf(shi[k], a3); }
       }
     }
-    // exclusive prefix: the union of bins 0..b-1 (empty: +inf / -inf)
+    // exclusive prefix: the union of bins 0..b-1 (b == 0: the empty box)
     float elo[3], ehi[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -183,18 +184,15 @@ __device__ __forceinline__ SahDec sah_evaluate(const int32_t *bins)
     const int rCount = sc;
     const float rArea = sah_area(slo[0], slo[1], slo[2], shi[0], shi[1], shi[2]);
     const float lArea = sah_area(elo[0], elo[1], elo[2], ehi[0], ehi[1], ehi[2]);
-    if (d == 0) {
-      // leafCost = rAreas[0] * rCount, from lane 0
-      const float lc = __fmul_rn(rArea, (float)rCount);
-      leafCost = __shfl_sync(0xffffffffu, lc, 0);
-    }
+    if (pass == 0) leafCost = __shfl_sync(0xffffffffu, __fmul_rn(rArea, (float)rCount), 0);  // rAreas[0]*rCount
+    const int dim = pass ? 2 : (lane >> 4);
     float cost = INFINITY;
-    if (lCount > 0 && rCount > 0 && lane < 16) {
+    if (lCount > 0 && rCount > 0 && (pass == 0 || lane < 16)) {
       cost = __fmaf_rn(lArea, (float)lCount, __fmul_rn(rArea, (float)rCount));
       if (cost != cost) cost = INFINITY;  // NaN never wins (cost < best is false)
     }
-    const int idx = d * SAH_BINS + b;
-    if (cost < best || (cost == best && idx < bestIdx && cost != INFINITY)) {
+    const int idx = dim * SAH_BINS + b;
+    if (cost < best || (cost == best && cost != INFINITY && idx < bestIdx)) {
       best = cost;
       bestIdx = idx;
     }
@@ -220,6 +218,21 @@ __device__ __forceinline__ SahDec sah_evaluate(const int32_t *bins)
     dec.bin = 0;
   }
   return dec;
+}
+
+// evaluateSAH over 48 encoded bins (bins[(d*16+b)*7 + ...], shared or global)
+__device__ __forceinline__ SahDec sah_evaluate(const int32_t *bins)
+{
+  const int lane = threadIdx.x & 31, b = lane & 15;
+  const int32_t *xa = bins + ((lane >> 4) * SAH_BINS + b) * SAH_W;
+  const int32_t *xb = bins + (2 * SAH_BINS + b) * SAH_W;
+  float aLo[3], aHi[3], bLo[3], bHi[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    aLo[k] = dec_f(xa[k]); aHi[k] = dec_f(xa[3 + k]);
+    bLo[k] = dec_f(xb[k]); bHi[k] = dec_f(xb[3 + k]);
+  }
+  return sah_evaluate_lanes(aLo, aHi, xa[6], bLo, bHi, xb[6]);
 }
 
 // running encoded min/max of the two children's centroids
@@ -573,9 +586,107 @@ __global__ void __launch_bounds__(SAH_BLOCK) k_sah_scatter(const SahNode *__rest
 // ------------------------------------------------------------------
 // warp phase: whole subtrees of at most SAH_WARP_MAX prims
 // ------------------------------------------------------------------
+// A subtree of at most 32 prims: lane j holds the prim at position
+// root.b + j in registers for the whole subtree.  A node's bins are
+// gathered by broadcasting its prims to the lanes that own the bins (no
+// shared atomics); partitions go through the 32-entry exchange buffer.
+__device__ void sah_small_subtree(const SahNode &root, const SahPrim *src, int thr, SahPrim *xbuf, SahNode *stk,
+                                  int stackLeft, Node *__restrict__ out, uint32_t *__restrict__ primIDs,
+                                  uint32_t *__restrict__ used, uint32_t *err)
+{
+  const int lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t base = root.b, cnt = root.e - root.b;
+  SahPrim p;
+  if (lane < (int)cnt) p = src[base + lane];
+  else p.a = p.b = make_float4(0.f, 0.f, 0.f, 0.f);
+  const uint32_t pos = base + lane;
+  const int dimA = lane >> 4, binL = lane & 15;
+  SahNode cur = root;
+  int sp = 0;
+  while (true) {
+    const uint32_t count = cur.e - cur.b;
+    const bool in = pos >= cur.b && pos < cur.e;
+    float clo[3], chi[3];
+    node_bounds(cur, clo, chi);
+    int mb[3] = {0, 0, 0};
+    if (in) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) mb[d] = sah_bin(prim_ctr(p, d), clo[d], chi[d]);
+    }
+    SahDec dec;
+    dec.dim = DEC_LEAF;
+    dec.bin = 0;
+    if ((int64_t)count > thr) {
+      float aLo[3], aHi[3], bLo[3], bHi[3];
+#pragma unroll
+      for (int k = 0; k < 3; k++) { aLo[k] = bLo[k] = FLT_MAX; aHi[k] = bHi[k] = -FLT_MAX; }
+      int aCnt = 0, bCnt = 0;
+      for (uint32_t j = cur.b - base; j < cur.e - base; j++) {
+        const float l0 = __shfl_sync(0xffffffffu, p.a.x, j), l1 = __shfl_sync(0xffffffffu, p.a.y, j);
+        const float l2 = __shfl_sync(0xffffffffu, p.a.z, j), h0 = __shfl_sync(0xffffffffu, p.b.x, j);
+        const float h1 = __shfl_sync(0xffffffffu, p.b.y, j), h2 = __shfl_sync(0xffffffffu, p.b.z, j);
+        const int j0 = __shfl_sync(0xffffffffu, mb[0], j), j1 = __shfl_sync(0xffffffffu, mb[1], j);
+        const int j2 = __shfl_sync(0xffffffffu, mb[2], j);
+        if ((dimA ? j1 : j0) == binL) {
+          aLo[0] = fminf(aLo[0], l0); aLo[1] = fminf(aLo[1], l1); aLo[2] = fminf(aLo[2], l2);
+          aHi[0] = fmaxf(aHi[0], h0); aHi[1] = fmaxf(aHi[1], h1); aHi[2] = fmaxf(aHi[2], h2);
+          aCnt++;
+        }
+        if (j2 == binL) {
+          bLo[0] = fminf(bLo[0], l0); bLo[1] = fminf(bLo[1], l1); bLo[2] = fminf(bLo[2], l2);
+          bHi[0] = fmaxf(bHi[0], h0); bHi[1] = fmaxf(bHi[1], h1); bHi[2] = fmaxf(bHi[2], h2);
+          bCnt++;
+        }
+      }
+      dec = sah_evaluate_lanes(aLo, aHi, aCnt, bLo, bHi, bCnt);
+    }
+    if (dec.dim == DEC_LEAF) {
+      if (lane == 0) leaf_node(out, cur.slot, cur.b, count);
+      if (sp == 0) break;
+      __syncwarp();
+      cur = stk[--sp];
+      __syncwarp();
+      continue;
+    }
+    const int myBin = dec.dim == 0 ? mb[0] : (dec.dim == 1 ? mb[1] : mb[2]);
+    const uint32_t side = in ? (myBin >= dec.bin ? 1u : 0u) : 0u;
+    const uint32_t balR = __ballot_sync(0xffffffffu, in && side);
+    const uint32_t balL = __ballot_sync(0xffffffffu, in && !side);
+    const uint32_t m = cur.e - __popc(balR);
+    if (balR == 0 || balL == 0) {  // unreachable: a chosen split has prims on both sides
+      if (lane == 0) atomicOr(err, DEV_ERR_RANGE);
+      break;
+    }
+    SideBounds sb;
+    sb.init();
+    if (in) sb.add(p, side);
+    sb.warp_reduce();
+    const uint32_t dest = !in ? (uint32_t)lane
+                              : (side ? (m - base) + __popc(balR & lt) : (cur.b - base) + __popc(balL & lt));
+    xbuf[dest] = p;
+    __syncwarp();
+    p = xbuf[lane];
+    __syncwarp();
+    if (lane == 0) internal_node(out, used, cur.slot, m);
+    SahNode c0, c1;
+    child_pair(cur, m, sb, c0, c1);
+    const bool leftSmaller = (m - cur.b) <= (cur.e - m);
+    if (sp >= stackLeft) {  // unreachable: the stacked child is always the larger one
+      if (lane == 0) atomicOr(err, DEV_ERR_RANGE);
+      break;
+    }
+    if (lane == 0) stk[sp] = leftSmaller ? c1 : c0;
+    sp++;
+    cur = leftSmaller ? c0 : c1;
+  }
+  if (lane < (int)cnt) primIDs[base + lane] = __float_as_uint(p.a.w);
+  __syncwarp();
+}
+
 __device__ void sah_warp_task(SahNode cur, int thr, SahPrim *buf0, SahPrim *buf1, Node *__restrict__ out,
                               uint32_t *__restrict__ primIDs, uint32_t *__restrict__ used, uint32_t *err,
-                              SahNode *stk, int32_t *bins)
+                              SahNode *stk, int32_t *bins, SahPrim *xbuf)
 {
   const int lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1u;
@@ -584,6 +695,14 @@ __device__ void sah_warp_task(SahNode cur, int thr, SahPrim *buf0, SahPrim *buf1
     const uint32_t count = cur.e - cur.b;
     const SahPrim *src = cur.parity ? buf1 : buf0;
     SahPrim *dst = cur.parity ? buf0 : buf1;
+    if ((int64_t)count > thr && count <= 32) {
+      sah_small_subtree(cur, src, thr, xbuf, stk + sp, SAHW_STACK - sp, out, primIDs, used, err);
+      if (sp == 0) return;
+      __syncwarp();
+      cur = stk[--sp];
+      __syncwarp();
+      continue;
+    }
     SahDec dec;
     dec.dim = DEC_LEAF;
     dec.bin = 0;
@@ -661,6 +780,7 @@ __global__ void __launch_bounds__(SAHW_BLOCK) k_sah_warp(const SahNode *__restri
 {
   __shared__ SahNode sStack[SAHW_WARPS][SAHW_STACK];
   __shared__ int32_t sBins[SAHW_WARPS][SAH_NB * SAH_W];
+  __shared__ SahPrim sX[SAHW_WARPS][32];
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
   const uint32_t numTasks = min(ctl->taskCount, taskCap);
   while (true) {
@@ -668,7 +788,7 @@ __global__ void __launch_bounds__(SAHW_BLOCK) k_sah_warp(const SahNode *__restri
     if (lane == 0) t = atomicAdd(&ctl->grab, 1u);
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= numTasks) return;  // whole warp
-    sah_warp_task(tasks[t], thr, buf0, buf1, out, primIDs, used, &ctl->err, sStack[wb], sBins[wb]);
+    sah_warp_task(tasks[t], thr, buf0, buf1, out, primIDs, used, &ctl->err, sStack[wb], sBins[wb], sX[wb]);
     __syncwarp();
   }
 }
