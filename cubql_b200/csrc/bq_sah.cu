@@ -15,7 +15,8 @@
 // records (box, primID) in two buffers and are partitioned stably, so every
 // node owns a contiguous range; children of the split at prim position m
 // take slots 2m, 2m+1 and one scan compacts the slots at the end.
-//   * nodes of more than SAH_WARP_MAX prims are split level by level over
+//   * nodes of more than warpMax prims (128..4096, about 64 subtrees per SM
+//     below it) are split level by level over
 //     the whole GPU in tiles of SAH_TILE prims: k_sah_bin (each warp bins
 //     into its own shared-memory bins, the block merges them, writes the
 //     tile's 48 bin counts and merges the bins into the node's with global
@@ -24,8 +25,9 @@
 //     parallel), k_sah_tile_right (right count per tile from its bin
 //     counts), one scan, k_sah_children, k_sah_scatter (stable scatter that
 //     also reduces the children's centroid bounds), k_sah_classify;
-//   * every subtree of at most SAH_WARP_MAX prims is finished by one warp of
-//     a persistent grid, depth first, smaller child first.
+//   * every subtree of at most warpMax prims is finished by one warp of a
+//     persistent grid, depth first, smaller child first; a subtree of at
+//     most 32 prims stays in registers (one prim per lane).
 // The reference can make a leaf of more than 65535 prims (its 16-bit count
 // then wraps); here such a node is split in two halves by position.
 #include <algorithm>
@@ -43,7 +45,8 @@ namespace {
 constexpr int SAH_BINS = 16;
 constexpr int SAH_NB = 3 * SAH_BINS;         // bins per node (3 axes)
 constexpr int SAH_W = 7;                     // words per bin: lo[3], hi[3], count
-constexpr uint32_t SAH_WARP_MAX = 128;       // subtrees up to this size: one warp
+constexpr uint32_t SAH_WARP_MIN = 128;       // warp subtrees: at most warpMax prims, warpMax in
+constexpr uint32_t SAH_WARP_CAP = 4096;      // [SAH_WARP_MIN, SAH_WARP_CAP], about 64 tasks per SM
 constexpr uint32_t SAH_TILE = 4096;          // prims per tile in the global levels
 constexpr int SAH_BLOCK = 256;
 constexpr int SAHW_BLOCK = 128;
@@ -333,7 +336,7 @@ __global__ void __launch_bounds__(256) k_sah_init(const bq_box3f *__restrict__ b
 }
 
 // ------------------------------------------------------------------
-// global levels (nodes with more than SAH_WARP_MAX prims)
+// global levels (nodes with more than warpMax prims)
 // ------------------------------------------------------------------
 struct SahCtl {
   uint32_t bigCount[2];
@@ -584,7 +587,7 @@ __global__ void __launch_bounds__(SAH_BLOCK) k_sah_scatter(const SahNode *__rest
 }
 
 // ------------------------------------------------------------------
-// warp phase: whole subtrees of at most SAH_WARP_MAX prims
+// warp phase: whole subtrees of at most warpMax prims
 // ------------------------------------------------------------------
 // A subtree of at most 32 prims: lane j holds the prim at position
 // root.b + j in registers for the whole subtree.  A node's bins are
@@ -716,7 +719,7 @@ __device__ void sah_warp_task(SahNode cur, int thr, SahPrim *buf0, SahPrim *buf1
       dec = sah_evaluate(bins);
       __syncwarp();  // bins are read before the next node clears them
     }
-    if (dec.dim == DEC_LEAF) {  // counts here are <= SAH_WARP_MAX, below the 16-bit limit
+    if (dec.dim == DEC_LEAF) {  // counts here are at most max(warpMax, thr) <= 65535
       for (uint32_t i = cur.b + lane; i < cur.e; i += 32) primIDs[i] = __float_as_uint(src[i].a.w);
       if (lane == 0) leaf_node(out, cur.slot, cur.b, count);
       if (sp == 0) return;
@@ -795,7 +798,8 @@ __global__ void __launch_bounds__(SAHW_BLOCK) k_sah_warp(const SahNode *__restri
 
 // children of the level's split nodes: to the next big list or to the tasks
 __global__ void k_sah_classify(const SahNode *__restrict__ next, SahCtl *ctl, int cur, uint32_t cap, int thr,
-                               SahNode *__restrict__ bigNext, SahNode *__restrict__ tasks, uint32_t taskCap)
+                               uint32_t warpMax, SahNode *__restrict__ bigNext, SahNode *__restrict__ tasks,
+                               uint32_t taskCap)
 {
   const uint32_t K = min(ctl->bigCount[cur], cap);
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -803,7 +807,7 @@ __global__ void k_sah_classify(const SahNode *__restrict__ next, SahCtl *ctl, in
   const SahNode c = next[j];
   const uint32_t size = c.e - c.b;
   if (size == 0) return;  // the node became a leaf
-  if (size > SAH_WARP_MAX && (int64_t)size > thr) {
+  if (size > warpMax && (int64_t)size > thr) {
     const uint32_t at = atomicAdd(&ctl->bigCount[cur ^ 1], 1u);
     if (at < cap) bigNext[at] = c;
     else atomicOr(&ctl->err, DEV_ERR_RANGE);
@@ -896,10 +900,14 @@ int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
   // ---- global levels, driven from device memory (as the spatial-median
   // builder: big nodes of a level are disjoint, so at most cap of them and
   // maxTiles tiles; the host looks at the counters every few levels) ----
-  const uint32_t cap = nv / (SAH_WARP_MAX + 1) + 1;
+  // warp subtrees small enough for about 64 of them per SM, so the warp
+  // phase has work for every warp
+  uint32_t warpMax = SAH_WARP_MIN;
+  while (warpMax < SAH_WARP_CAP && (uint64_t)warpMax * 2 * num_sms() * 64 <= nv) warpMax *= 2;
+  const uint32_t cap = nv / (warpMax + 1) + 1;
   const uint32_t maxTiles = nv / SAH_TILE + cap + 2;
   int nextCheck = 1;
-  while (nextCheck < 62 && ((uint64_t)SAH_WARP_MAX << nextCheck) < nv) nextCheck++;
+  while (nextCheck < 62 && ((uint64_t)warpMax << nextCheck) < nv) nextCheck++;
   const uint32_t taskCap =
       std::max<uint32_t>(16 * cap, 4096) + 2 * cap * (uint32_t)std::max(nextCheck, SAH_LEVELS_PER_CHECK);
   SahCtl *sc = nullptr;
@@ -917,7 +925,7 @@ int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
   SahNode root;
   root.b = 0; root.e = nv; root.slot = 0; root.parity = 0;
   for (int d = 0; d < 3; d++) { root.lo[d] = hctl[2 + d]; root.hi[d] = hctl[5 + d]; }
-  const bool rootBig = nv > SAH_WARP_MAX && (int64_t)nv > thr;
+  const bool rootBig = nv > warpMax && (int64_t)nv > thr;
   SahCtl hsc{};
   hsc.bigCount[0] = rootBig ? 1u : 0u;
   hsc.taskCount = rootBig ? 0u : 1u;
@@ -952,8 +960,8 @@ int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
                                                          used, next, &sc->err);
       k_sah_scatter<<<maxTiles, SAH_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, tileRight, decs, buf0,
                                                       buf1, next);
-      k_sah_classify<<<div_up(2ull * cap, 128), 128, 0, al.s>>>(next, sc, cur, cap, thr, bigList[cur ^ 1], tasks,
-                                                                taskCap);
+      k_sah_classify<<<div_up(2ull * cap, 128), 128, 0, al.s>>>(next, sc, cur, cap, thr, warpMax, bigList[cur ^ 1],
+                                                                tasks, taskCap);
       if ((ce = cudaMemsetAsync(&sc->bigCount[cur], 0, sizeof(uint32_t), al.s)) != cudaSuccess ||
           (ce = cudaGetLastError()) != cudaSuccess)
         return fail(cuda_error(ce, "sah level"));
