@@ -10,7 +10,8 @@
 // first node, the block's second node unused.
 //
 // Two kernels:
-//   k_agg_local   one CTA per chunk of AGG_CHUNK sorted prims.  Threads
+//   k_agg_local   one CTA per chunk of AGG_CHUNK (256) sorted prims, whose
+//                 split levels are staged in shared memory.  Threads
 //                 start at their leaf and climb; the first child to reach
 //                 a split parks its range end and box in shared memory and
 //                 stops, the second merges and climbs on.  Everything
@@ -67,7 +68,10 @@ __device__ __forceinline__ uint32_t run_end(const uint64_t *__restrict__ keys, u
   return lo;
 }
 
-constexpr int AGG_CHUNK = 512;
+#ifndef BQ_AGG_CHUNK
+#define BQ_AGG_CHUNK 256
+#endif
+constexpr int AGG_CHUNK = BQ_AGG_CHUNK;  // prims per CTA of the local phase
 constexpr uint32_t AGG_EMPTY = 0xffffffffu;
 
 // prim range of position i: [0, nv) or the cloud containing i
@@ -121,11 +125,16 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
 {
   __shared__ uint32_t sSlot[AGG_CHUNK + 1];
   __shared__ AggBox sBox[AGG_CHUNK + 1][2];
+  __shared__ LevT sLev[AGG_CHUNK + 2];  // delta[c0 - 1 .. c0 + AGG_CHUNK]
   const uint32_t nv = *a.nvPtr;
   const uint32_t c0 = blockIdx.x * AGG_CHUNK;
   if (c0 >= nv) return;  // whole CTA: no barrier below is skipped by part of it
   const uint32_t cEnd = c0 + AGG_CHUNK;  // first split position outside the chunk
   for (int j = threadIdx.x; j <= AGG_CHUNK; j += blockDim.x) sSlot[j] = AGG_EMPTY;
+  for (int j = threadIdx.x; j < AGG_CHUNK + 2; j += blockDim.x) {
+    const int64_t g = (int64_t)c0 - 1 + j;  // pairs (g, g+1) exist for 0 <= g < nv - 1
+    sLev[j] = (g >= 0 && g + 1 < (int64_t)nv) ? __ldg(a.delta + g) : (LevT)0;
+  }
   if (threadIdx.x < 2) a.pending[2 * blockIdx.x + threadIdx.x] = make_uint2(AGG_EMPTY, AGG_EMPTY);
   __syncthreads();
   const uint32_t i = c0 + threadIdx.x;
@@ -146,8 +155,8 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
         a.nodes[nodeBase] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
         break;
       }
-      const bool leftChild =
-          (l == b0) ? true : (r == e0 - 1) ? false : (__ldg(a.delta + l - 1) > __ldg(a.delta + r));
+      // c0 <= l <= r < cEnd here: delta[l - 1] and delta[r] are in sLev
+      const bool leftChild = (l == b0) ? true : (r == e0 - 1) ? false : (sLev[l - c0] > sLev[r - c0 + 1]);
       const uint32_t s = leftChild ? r + 1 : l;
       const uint32_t side = leftChild ? 0 : 1;
       a.nodes[2ull * s + side] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
