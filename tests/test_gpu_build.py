@@ -175,3 +175,68 @@ def test_refit_after_moving_prims(bq, oracle, builder):
     bq.refit(bvh, torch.from_numpy(moved).cuda())
     gn, gp = bvh.to_host()
     check_tree(gn, gp, moved, max_leaf=4)
+
+
+def _tree_properties_on_gpu(bq, bvh, boxes_t):
+    """Size-independent invariants checked on the device: primIDs are a
+    permutation, every node but 0 and 1 is the child of exactly one inner
+    node, leaves cover every sorted position once, and every inner node's
+    box is exactly the union of its children's (leaf boxes exactly the
+    prims' boxes)."""
+    n = boxes_t.shape[0]
+    nodes = bvh.nodes_tensor()  # (numNodes, 8) float32: lower, upper, admin words
+    admin = nodes[:, 6:8].contiguous().view(torch.int64).view(-1)
+    count = (admin >> 48) & 0xFFFF
+    off = admin & 0xFFFFFFFFFFFF
+    nn = nodes.shape[0]
+    prims = bvh.primids_tensor().long()
+    assert torch.equal(torch.sort(prims).values, torch.arange(n, device="cuda"))
+    inner = count == 0
+    inner[1] = False
+    io = off[inner]
+    assert bool(((io >= 2) & (io + 1 < nn) & (io % 2 == 0)).all())
+    refs = torch.zeros(nn, dtype=torch.int32, device="cuda")
+    one = torch.ones_like(io, dtype=torch.int32)
+    refs.index_add_(0, io, one)
+    refs.index_add_(0, io + 1, one)
+    assert bool((refs[2:] == 1).all()) and int(refs[0]) == 0
+    leaf = count > 0
+    lo, lc = off[leaf], count[leaf]
+    cover = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    cover.index_add_(0, lo, torch.ones_like(lo, dtype=torch.int32))
+    cover.index_add_(0, lo + lc, -torch.ones_like(lo, dtype=torch.int32))
+    assert bool((torch.cumsum(cover, 0)[:n] == 1).all())
+    box = nodes[:, :6]
+    step = 1 << 24
+    idx_inner = torch.nonzero(inner).view(-1)
+    for s in range(0, idx_inner.numel(), step):
+        p = idx_inner[s:s + step]
+        c0, c1 = box[off[p]], box[off[p] + 1]
+        u = torch.cat([torch.minimum(c0[:, :3], c1[:, :3]), torch.maximum(c0[:, 3:], c1[:, 3:])], 1)
+        assert torch.equal(u, box[p])
+    idx_leaf = torch.nonzero(leaf & (count == 1)).view(-1)
+    for s in range(0, idx_leaf.numel(), step):
+        p = idx_leaf[s:s + step]
+        assert torch.equal(box[p], boxes_t[prims[off[p]]])
+    root = box[0]
+    assert torch.equal(root[:3], boxes_t[:, :3].min(0).values) and torch.equal(root[3:], boxes_t[:, 3:].max(0).values)
+
+
+@pytest.mark.parametrize("builder", ["morton", "sm", "sah"])
+def test_builders_100m_properties(bq, builder):
+    """Ten times the benchmark size (100M point boxes, 2.4 GB; 200M nodes),
+    leaf 1: the trees' structural invariants, checked on the device."""
+    n = 100_000_000
+    free, _ = torch.cuda.mem_get_info()
+    if free < 40 << 30:
+        pytest.skip("needs 40 GB of free device memory")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(12345)
+    pts = torch.rand((n, 3), generator=g, device="cuda", dtype=torch.float32)
+    boxes_t = torch.cat([pts, pts], 1).contiguous()
+    del pts
+    build = {"morton": bq.cuda.radixBuilder, "sm": bq.gpuBuilder, "sah": bq.cuda.sahBuilder}[builder]
+    bvh = build(boxes_t)
+    assert bvh.numNodes == 2 * n and bvh.numPrims == n
+    _tree_properties_on_gpu(bq, bvh, boxes_t)
+    bvh.free()
