@@ -10,10 +10,11 @@
 //   k_keygen      stable compaction of valid prims, 63-bit Morton keys
 //                 (radix.h:41-62 Quantizer, 283-421 key generation) and the
 //                 digit histograms of the top key bits
-//   onesweep sort stable (key, primID) sort on key bits [39, 63) only: 3
-//                 digit passes instead of 8 (bq_sort.cu)
-//   k_fix_runs    runs of equal top bits are then ordered by the low 39
-//                 bits, stably: runs of up to 32 prims by one thread each
+//   onesweep sort stable (key, primID) sort on the top key bits only:
+//                 bits [39, 63) in 3 digit passes up to 2^24 prims, bits
+//                 [31, 63) in 4 passes above, instead of 8 (bq_sort.cu)
+//   k_fix_runs    runs of equal top bits are then ordered by the low bits,
+//                 stably: runs of up to 32 prims by one thread each
 //                 (on uniform data nearly all runs are of 1-4 prims),
 //                 longer runs by one segmented composite-key sort of just
 //                 their prims ((run, low bits) keys).  The result is the
@@ -62,10 +63,18 @@ namespace {
 constexpr int MB_BLOCK = 256;
 constexpr int MB_UNROLL = 4;
 constexpr uint32_t SLOT_EMPTY = 0xffffffffu;
-constexpr int MB_SORT_BEGIN = 39;   // the global sort covers key bits [39, 63): 24 bits
-constexpr int MB_HIST_PASSES = 3;   // its digit passes
-constexpr uint64_t MB_LOW_MASK = (1ull << MB_SORT_BEGIN) - 1;  // bits ordered inside runs
-__device__ __forceinline__ uint32_t key_hi(uint64_t k) { return (uint32_t)(k >> MB_SORT_BEGIN); }
+// The global sort covers key bits [SB, 63): SB = 39 (24 bits, 3 passes) up
+// to 2^24 prims, SB = 31 (32 bits, 4 passes) above, so that runs of equal
+// sorted bits stay short (on uniform data about n / 2^(63-SB) prims each);
+// the bits below SB are ordered inside those runs.
+constexpr int MB_SB3 = 39, MB_SB4 = 31;
+constexpr int MB_MAX_HIST_PASSES = 4;
+template <int SB>
+constexpr int hist_passes() { return (63 - SB + 7) / 8; }
+template <int SB>
+constexpr uint64_t low_mask() { return (1ull << SB) - 1; }
+template <int SB>
+__device__ __forceinline__ uint32_t key_hi(uint64_t k) { return (uint32_t)(k >> SB); }
 constexpr uint32_t MB_THREAD_RUN = 32;  // longest run of equal top bits one thread orders
 
 struct __align__(16) Partial {
@@ -208,15 +217,17 @@ __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict_
 // ------------------------------------------------------------------
 // pass 2: keys, compaction, digit histograms
 // ------------------------------------------------------------------
+template <int SB>
 __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
                                                      const uint32_t *__restrict__ blockOff, const BuildState *st,
                                                      uint64_t *__restrict__ keys, uint32_t *__restrict__ ids,
                                                      uint32_t *__restrict__ hist)
 {
-  __shared__ uint32_t sHist[MB_HIST_PASSES * 256];
+  constexpr int PASSES = hist_passes<SB>();
+  __shared__ uint32_t sHist[PASSES * 256];
   __shared__ uint32_t sWarpCnt[MB_UNROLL][MB_BLOCK / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = threadIdx.x; i < MB_HIST_PASSES * 256; i += MB_BLOCK) sHist[i] = 0;
+  for (int i = threadIdx.x; i < PASSES * 256; i += MB_BLOCK) sHist[i] = 0;
   const float bx = st->bias[0], by = st->bias[1], bz = st->bias[2], sc = st->scale;
   uint32_t running = blockOff[blockIdx.x];
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
@@ -267,12 +278,12 @@ __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict_
       keys[pos] = key;
       ids[pos] = (uint32_t)(i0 + (uint64_t)u * MB_BLOCK + threadIdx.x);
 #pragma unroll
-      for (int p = 0; p < MB_HIST_PASSES; p++)
-        atomicAdd(&sHist[p * 256 + ((key >> (MB_SORT_BEGIN + 8 * p)) & 0xff)], 1u);
+      for (int p = 0; p < PASSES; p++)
+        atomicAdd(&sHist[p * 256 + ((key >> (SB + 8 * p)) & 0xff)], 1u);
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < MB_HIST_PASSES * 256; i += MB_BLOCK)
+  for (int i = threadIdx.x; i < PASSES * 256; i += MB_BLOCK)
     if (sHist[i]) atomicAdd(&hist[i], sHist[i]);
 }
 
@@ -284,18 +295,19 @@ struct RunStats {
 };
 
 // one past the last index j >= i with key_hi(keys[j]) == hi (key_hi(keys[i]) == hi)
+template <int SB>
 __device__ __forceinline__ uint32_t hi_run_end(const uint64_t *__restrict__ keys, uint32_t i, uint32_t hi, uint32_t n)
 {
   uint32_t step = 1, lo = i + 1, up = n;
   while (lo < up) {
     const uint32_t probe = lo - 1 + min(step, up - lo + 1);
-    if (probe >= up || key_hi(keys[probe]) != hi) { up = min(probe, up); break; }
+    if (probe >= up || key_hi<SB>(keys[probe]) != hi) { up = min(probe, up); break; }
     lo = probe + 1;
     step <<= 1;
   }
   while (lo < up) {
     const uint32_t m = lo + ((up - lo) >> 1);
-    if (key_hi(keys[m]) == hi) lo = m + 1; else up = m;
+    if (key_hi<SB>(keys[m]) == hi) lo = m + 1; else up = m;
   }
   return lo;
 }
@@ -318,10 +330,11 @@ __device__ __forceinline__ uint8_t equal_run_level(uint64_t r0, uint64_t r1, uin
 }
 
 // The first position i of a run of at least two prims with equal top bits
-// (keys sorted on bits [MB_SORT_BEGIN, 63) only): orders the run on the low
+// (keys sorted on bits [SB, 63) only): orders the run on the low
 // bits (stable) and writes the levels of the pairs inside it.  Runs of up
 // to MB_THREAD_RUN prims are done here; longer ones are listed for a
 // segmented sort (their inner levels are written by k_delta afterwards).
+template <int SB>
 __device__ __forceinline__ void fix_run_at(uint32_t i, uint32_t nv, uint64_t *keys, uint32_t *ids,
                                            uint8_t *__restrict__ delta, RunStats *rs, uint4 *runs, uint32_t maxRuns)
 {
@@ -330,10 +343,10 @@ __device__ __forceinline__ void fix_run_at(uint32_t i, uint32_t nv, uint64_t *ke
   const uint64_t km = i > 0 ? keys[i - 1] : ~k0;
   const uint64_t k1 = i + 1 < nv ? keys[i + 1] : ~k0;
   const uint64_t k2 = i + 2 < nv ? keys[i + 2] : ~k0;
-  const uint32_t hi = key_hi(k0);
-  if (key_hi(km) == hi) return;  // not the first of its run
-  if (key_hi(k1) != hi) return;  // a run of one
-  if (key_hi(k2) != hi) {        // a run of two
+  const uint32_t hi = key_hi<SB>(k0);
+  if (key_hi<SB>(km) == hi) return;  // not the first of its run
+  if (key_hi<SB>(k1) != hi) return;  // a run of one
+  if (key_hi<SB>(k2) != hi) {        // a run of two
     uint64_t a = k0, b = k1;
     if (k0 > k1) {
       const uint32_t ia = ids[i], ib = ids[i + 1];
@@ -346,8 +359,8 @@ __device__ __forceinline__ void fix_run_at(uint32_t i, uint32_t nv, uint64_t *ke
   }
   const uint64_t k3 = i + 3 < nv ? keys[i + 3] : ~k0;
   const uint64_t k4 = i + 4 < nv ? keys[i + 4] : ~k0;
-  if (key_hi(k4) != hi) {  // a run of three or four: kept in registers
-    const uint32_t size = key_hi(k3) == hi ? 4u : 3u;
+  if (key_hi<SB>(k4) != hi) {  // a run of three or four: kept in registers
+    const uint32_t size = key_hi<SB>(k3) == hi ? 4u : 3u;
     uint64_t r[4] = {k0, k1, k2, size == 4 ? k3 : ~0ull};  // ~0: above every key, stays last
     uint32_t d[4];
 #pragma unroll
@@ -388,7 +401,7 @@ __device__ __forceinline__ void fix_run_at(uint32_t i, uint32_t nv, uint64_t *ke
     }
     return;
   }
-  const uint32_t size = hi_run_end(keys, i, hi, nv) - i;
+  const uint32_t size = hi_run_end<SB>(keys, i, hi, nv) - i;
   if (size > MB_THREAD_RUN) {
     const uint32_t slotIdx = atomicAdd(&rs->count, 1u);
     if (slotIdx < maxRuns) runs[slotIdx] = make_uint4(i, size, hi, 0);
@@ -446,6 +459,7 @@ __device__ __forceinline__ void fix_run_at(uint32_t i, uint32_t nv, uint64_t *ke
 // of a mostly idle warp.
 constexpr int FR_BLOCK = 256;
 constexpr int FR_ITEMS = 4;
+template <int SB>
 __global__ void __launch_bounds__(FR_BLOCK) k_fix_runs(uint64_t *keys, uint32_t *ids, const uint32_t *nvPtr,
                                                        uint8_t *__restrict__ delta, uint32_t *__restrict__ slot,
                                                        RunStats *rs, uint4 *runs, uint32_t maxRuns)
@@ -463,17 +477,18 @@ __global__ void __launch_bounds__(FR_BLOCK) k_fix_runs(uint64_t *keys, uint32_t 
     if (i < nv) {
       slot[i] = SLOT_EMPTY;
       const uint64_t k0 = keys[i];
-      const uint32_t hi = key_hi(k0);
-      const bool nextSame = i + 1 < nv && key_hi(keys[i + 1]) == hi;
+      const uint32_t hi = key_hi<SB>(k0);
+      const bool nextSame = i + 1 < nv && key_hi<SB>(keys[i + 1]) == hi;
       if (i + 1 < nv && !nextSame) delta[i] = key_level(k0, keys[i + 1]);  // pair across two runs
-      start = nextSame && (i == 0 || key_hi(keys[i - 1]) != hi);
+      start = nextSame && (i == 0 || key_hi<SB>(keys[i - 1]) != hi);
     }
     const uint32_t bal = __ballot_sync(0xffffffffu, start);
     if (start) sStarts[warp][numStarts + __popc(bal & lt)] = (uint32_t)i;
     numStarts += __popc(bal);
   }
   __syncwarp();
-  for (uint32_t k = lane; k < numStarts; k += 32) fix_run_at(sStarts[warp][k], nv, keys, ids, delta, rs, runs, maxRuns);
+  for (uint32_t k = lane; k < numStarts; k += 32)
+    fix_run_at<SB>(sStarts[warp][k], nv, keys, ids, delta, rs, runs, maxRuns);
 }
 
 __global__ void k_run_sizes(const uint4 *__restrict__ runs, uint32_t numRuns, uint32_t *__restrict__ sizes)
@@ -493,6 +508,7 @@ __device__ __forceinline__ uint32_t run_of(const uint32_t *__restrict__ off, uin
   return lo;
 }
 
+template <int SB>
 __global__ void k_run_gather(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off, uint32_t numRuns,
                              uint32_t numSlots, const uint64_t *__restrict__ keys, const uint32_t *__restrict__ ids,
                              uint64_t *__restrict__ kk, uint32_t *__restrict__ vv)
@@ -501,10 +517,11 @@ __global__ void k_run_gather(const uint4 *__restrict__ runs, const uint32_t *__r
   if (t >= numSlots) return;
   const uint32_t r = run_of(off, numRuns, t);
   const uint32_t pos = runs[r].x + (t - off[r]);
-  kk[t] = ((uint64_t)r << MB_SORT_BEGIN) | (keys[pos] & MB_LOW_MASK);
+  kk[t] = ((uint64_t)r << SB) | (keys[pos] & low_mask<SB>());
   vv[t] = ids[pos];
 }
 
+template <int SB>
 __global__ void k_run_scatter(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off, uint32_t numSlots,
                               const uint64_t *__restrict__ kk, const uint32_t *__restrict__ vv,
                               uint64_t *__restrict__ keys, uint32_t *__restrict__ ids)
@@ -512,10 +529,10 @@ __global__ void k_run_scatter(const uint4 *__restrict__ runs, const uint32_t *__
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numSlots) return;
   const uint64_t k = kk[t];
-  const uint32_t r = (uint32_t)(k >> MB_SORT_BEGIN);
+  const uint32_t r = (uint32_t)(k >> SB);
   const uint4 run = runs[r];
   const uint32_t pos = run.x + (t - off[r]);
-  keys[pos] = ((uint64_t)run.z << MB_SORT_BEGIN) | (k & MB_LOW_MASK);
+  keys[pos] = ((uint64_t)run.z << SB) | (k & low_mask<SB>());
   ids[pos] = vv[t];
 }
 
@@ -612,6 +629,7 @@ namespace {
 // Orders the runs of equal top bits and writes every split level and slot;
 // *longRuns tells whether runs above MB_THREAD_RUN were sorted (their inner
 // levels are then still to be written).
+template <int SB>
 int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *spareIds, uint32_t n,
                   const uint32_t *nvDev, uint8_t *delta, uint32_t *slot, uint32_t *err, bool *longRuns, Alloc &al)
 {
@@ -625,8 +643,8 @@ int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *
   BQ_CUDA(cudaMemsetAsync(rs, 0, sizeof(RunStats), al.s));
   {
     ProfScope ps("morton.runs", al.s);
-    k_fix_runs<<<div_up(n, FR_BLOCK * FR_ITEMS), FR_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs,
-                                                                     maxRuns);
+    k_fix_runs<SB><<<div_up(n, FR_BLOCK * FR_ITEMS), FR_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs,
+                                                                         maxRuns);
   }
   RunStats h{};
   BQ_CUDA(cudaMemcpyAsync(&h, rs, sizeof(h), cudaMemcpyDeviceToHost, al.s));
@@ -646,13 +664,13 @@ int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *
   BQ_TRY(tmp.get(&kk[1], P));
   BQ_TRY(tmp.get(&vv[1], P));
   ProfScope ps("morton.longruns", al.s, 2);
-  k_run_gather<<<div_up(P, 256), 256, 0, al.s>>>(runs, off, R, P, keys, ids, kk[0], vv[0]);
+  k_run_gather<SB><<<div_up(P, 256), 256, 0, al.s>>>(runs, off, R, P, keys, ids, kk[0], vv[0]);
   int runBits = 0;
   while (runBits < 32 && ((R - 1) >> runBits)) runBits++;
-  if (runBits > 64 - MB_SORT_BEGIN) return set_error(BQ_ERR_UNSUPPORTED, "too many long runs of equal keys");
+  if (runBits > 64 - SB) return set_error(BQ_ERR_UNSUPPORTED, "too many long runs of equal keys");
   int ksel = 0;
-  BQ_TRY(onesweep_sort_u64(kk, vv, P, nullptr, 0, MB_SORT_BEGIN + runBits, nullptr, &ksel, err, al));
-  k_run_scatter<<<div_up(P, 256), 256, 0, al.s>>>(runs, off, P, kk[ksel], vv[ksel], keys, ids);
+  BQ_TRY(onesweep_sort_u64(kk, vv, P, nullptr, 0, SB + runBits, nullptr, &ksel, err, al));
+  k_run_scatter<SB><<<div_up(P, 256), 256, 0, al.s>>>(runs, off, P, kk[ksel], vv[ksel], keys, ids);
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }
@@ -685,7 +703,11 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   BQ_TRY(tmp.get(&st, 1));
   BQ_TRY(tmp.get(&partials, grid));
   BQ_TRY(tmp.get(&blockOff, grid));
-  BQ_TRY(tmp.get(&hist, MB_HIST_PASSES * 256));
+  // more than 2^24 prims: sort 32 top bits in 4 passes instead of 24 in 3
+  const bool wide4 = n > (1u << 24);
+  const int sb = wide4 ? MB_SB4 : MB_SB3;
+  const int histWords = (wide4 ? hist_passes<MB_SB4>() : hist_passes<MB_SB3>()) * 256;
+  BQ_TRY(tmp.get(&hist, MB_MAX_HIST_PASSES * 256));
   BQ_TRY(tmp.get(&keysA, n));
   BQ_TRY(tmp.get(&keysB, n));
   BQ_TRY(tmp.get(&delta, n));
@@ -707,26 +729,29 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
 
   {
     ProfScope ps("morton.bounds", al.s);
-    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, MB_HIST_PASSES * 256);
+    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, histWords);
   }
   {
     ProfScope ps("morton.keygen", al.s);
-    k_keygen<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
+    if (wide4) k_keygen<MB_SB4><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
+    else k_keygen<MB_SB3><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
   }
   if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_bounds/k_keygen"));
 
   uint64_t *keys2[2] = {keysA, keysB};
   uint32_t *ids2[2] = {idsA, idsB};
   int sel = 0;
-  if ((s = onesweep_sort_u64(keys2, ids2, n, &st->numValid, MB_SORT_BEGIN, 63, hist, &sel, &st->err, al)) != BQ_OK)
+  if ((s = onesweep_sort_u64(keys2, ids2, n, &st->numValid, sb, 63, hist, &sel, &st->err, al)) != BQ_OK)
     return fail(s);
   uint64_t *keys = keys2[sel];
   uint32_t *ids = ids2[sel];
   uint32_t *idsOther = ids2[sel ^ 1];
   bool longRuns = false;
-  if ((s = sort_low_bits(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err, &longRuns,
-                         al)) != BQ_OK)
-    return fail(s);
+  s = wide4 ? sort_low_bits<MB_SB4>(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err,
+                                     &longRuns, al)
+            : sort_low_bits<MB_SB3>(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err,
+                                     &longRuns, al);
+  if (s != BQ_OK) return fail(s);
 
   if (longRuns) {  // levels inside the long runs (rewrites all levels and slots)
     ProfScope ps("morton.delta", al.s);

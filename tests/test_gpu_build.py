@@ -82,6 +82,19 @@ def test_morton_full_size_10m(bq, oracle):
     assert ok, msg
 
 
+@pytest.mark.parametrize("dist", ["uniform", "gmm"])
+def test_morton_4pass_matches_oracle(bq, oracle, dist):
+    """Above 2^24 prims the top 32 key bits are sorted (4 passes) instead of
+    24: 17M prims, uniform and the duplicate-heavy GMM (long runs)."""
+    b = boxes_np(_dist(dist, 17_000_000))
+    bvh = bq.cuda.radixBuilder(torch.from_numpy(b).cuda())
+    gn, gp = bvh.to_host()
+    on, op = oracle.radix_build(b)
+    ok, msg = same_tree(oracle, gn, gp, on, op)
+    assert ok, msg
+    bvh.free()
+
+
 def test_morton_is_deterministic(bq):
     b = torch.from_numpy(_boxes("gmm", 300000)).cuda()
     a = bq.cuda.radixBuilder(b).to_host()
