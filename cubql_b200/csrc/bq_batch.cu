@@ -379,9 +379,9 @@ __global__ void __launch_bounds__(128) k_seg_knn(const bq_bvh3f *__restrict__ bv
 #pragma unroll
       for (int j = 0; j < K; j++) {
         if (j >= K - k) {
-          const bool real = leaf.list.I[j] != 0x7fffffff && leaf.list.D[j] != INFINITY;
-          oi[j - (K - k)] = real ? leaf.list.I[j] : -1;
-          od[j - (K - k)] = real ? leaf.list.D[j] : INFINITY;
+          const bool real = leaf.list.real(j);
+          oi[j - (K - k)] = real ? leaf.list.id(j) : -1;
+          od[j - (K - k)] = real ? leaf.list.dist(j) : INFINITY;
           found += real ? 1 : 0;
         }
       }
@@ -423,9 +423,9 @@ __global__ void k_seg_knn_deep(const bq_bvh3f *__restrict__ bvhs, const uint32_t
     }
     int found = 0;
     for (int j = K - k; j < K; j++) {
-      const bool real = leaf.list.I[j] != 0x7fffffff && leaf.list.D[j] != INFINITY;
-      oi[j - (K - k)] = real ? leaf.list.I[j] : -1;
-      od[j - (K - k)] = real ? leaf.list.D[j] : INFINITY;
+      const bool real = leaf.list.real(j);
+      oi[j - (K - k)] = real ? leaf.list.id(j) : -1;
+      od[j - (K - k)] = real ? leaf.list.dist(j) : INFINITY;
       found += real ? 1 : 0;
     }
     if (numFound) numFound[qi] = found;

@@ -133,9 +133,9 @@ __device__ __forceinline__ bool run_knn(const Node *nodes, const uint32_t *primI
 #pragma unroll
   for (int j = 0; j < K; j++) {
     if (j >= K - k) {
-      const bool real = leaf.list.I[j] != 0x7fffffff && leaf.list.D[j] != INFINITY;
-      oi[j - (K - k)] = real ? leaf.list.I[j] : -1;
-      od[j - (K - k)] = real ? leaf.list.D[j] : INFINITY;
+      const bool real = leaf.list.real(j);
+      oi[j - (K - k)] = real ? leaf.list.id(j) : -1;
+      od[j - (K - k)] = real ? leaf.list.dist(j) : INFINITY;
       found += real ? 1 : 0;
     }
   }

@@ -146,6 +146,9 @@ struct KnnList {
     }
   }
   __device__ __forceinline__ float worst() const { return D[K - 1]; }
+  __device__ __forceinline__ float dist(int j) const { return D[j]; }
+  __device__ __forceinline__ int32_t id(int j) const { return I[j]; }
+  __device__ __forceinline__ bool real(int j) const { return I[j] != 0x7fffffff && D[j] != INFINITY; }
   // insert if it belongs to the list
   __device__ __forceinline__ void offer(float d, int32_t id)
   {
@@ -158,6 +161,35 @@ struct KnnList {
       const int32_t ni = fromPrev ? I[j > 0 ? j - 1 : 0] : (here ? id : I[j]);
       D[j] = nd;
       I[j] = ni;
+    }
+  }
+};
+
+// Lowest-id ties: a candidate is the 64-bit key (distance bits << 32 | id).
+// Distances are >= +0, so key order is (distance, id) order and one 64-bit
+// compare replaces the float compare, the equality test and the id compare.
+constexpr uint64_t KNN_KEY_EMPTY = (0x7f800000ull << 32) | 0xffffffffull;  // (+inf, above every id)
+template <int K>
+struct KnnList<K, TIE_LOWEST> {
+  uint64_t L[K];
+  __device__ __forceinline__ void init(int k)
+  {
+#pragma unroll
+    for (int j = 0; j < K; j++) L[j] = j < K - k ? 0ull : KNN_KEY_EMPTY;  // 0: below every candidate
+  }
+  __device__ __forceinline__ float worst() const { return __uint_as_float((uint32_t)(L[K - 1] >> 32)); }
+  __device__ __forceinline__ float dist(int j) const { return __uint_as_float((uint32_t)(L[j] >> 32)); }
+  __device__ __forceinline__ int32_t id(int j) const { return (int32_t)(uint32_t)L[j]; }
+  __device__ __forceinline__ bool real(int j) const { return L[j] != KNN_KEY_EMPTY; }
+  __device__ __forceinline__ void offer(float d, int32_t id)
+  {
+    const uint64_t key = ((uint64_t)__float_as_uint(d) << 32) | (uint32_t)id;
+    if (!(key < L[K - 1])) return;
+#pragma unroll
+    for (int j = K - 1; j >= 0; j--) {
+      const bool fromPrev = (j > 0) && key < L[j > 0 ? j - 1 : 0];
+      const bool here = key < L[j];
+      L[j] = fromPrev ? L[j > 0 ? j - 1 : 0] : (here ? key : L[j]);
     }
   }
 };
