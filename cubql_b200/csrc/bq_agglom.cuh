@@ -225,14 +225,22 @@ __global__ void k_agg_global(AggArgsT<LevT> a, uint32_t numPending)
   }
 }
 
-// launches both phases for nvMax (upper bound of *nvPtr) prims; split
+// launches both phases for nvMax (upper bound of *nvPtr) prims, each under
+// its own profiler scope; split
 // levels are 8-bit (Morton-63 builders) or 16-bit (rebin builder)
 template <bool SEG, typename LevT>
-inline int agglomerate(AggArgsT<LevT> a, uint32_t nvMax, cudaStream_t s)
+inline int agglomerate(AggArgsT<LevT> a, uint32_t nvMax, cudaStream_t s, const char *profLocal = nullptr,
+                       const char *profGlobal = nullptr)
 {
   const int chunks = div_up(nvMax, AGG_CHUNK);
-  k_agg_local<SEG, LevT><<<chunks, AGG_CHUNK, 0, s>>>(a);
-  k_agg_global<SEG, LevT><<<div_up(2 * chunks, 128), 128, 0, s>>>(a, 2u * chunks);
+  {
+    ProfScope ps(profLocal ? profLocal : "agg.local", s);
+    k_agg_local<SEG, LevT><<<chunks, AGG_CHUNK, 0, s>>>(a);
+  }
+  {
+    ProfScope ps(profGlobal ? profGlobal : "agg.global", s);
+    k_agg_global<SEG, LevT><<<div_up(2 * chunks, 128), 128, 0, s>>>(a, 2u * chunks);
+  }
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }

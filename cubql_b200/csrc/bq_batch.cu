@@ -554,17 +554,16 @@ int batched_build_morton63(const bq_box3f *boxes, const uint32_t *off, uint32_t 
   // so the sequence stays capturable)
   AggArgs ag{delta, slot, fids, boxes, (Node *)nodesOut, primIDs, off + numSegs, nullptr, pending, off, numSegs};
   if (thr == 1) {
-    ProfScope ps("batch.agglomerate", al.s, 2);
-    BQ_TRY(agglomerate<true>(ag, n, al.s));
+    BQ_TRY(agglomerate<true>(ag, n, al.s, "batch.agg_local", "batch.agg_global"));
   } else {
     BQ_TRY(tmp.get(&full, 2ull * n));
     BQ_TRY(tmp.get(&ranges, n));
     BQ_TRY(tmp.get(&kept, n + 1ull));
     BQ_TRY(tmp.get(&rank, n + 1ull));
-    ProfScope ps("batch.agglomerate", al.s, 4);
     ag.nodes = full;
     ag.ranges = ranges;
-    BQ_TRY(agglomerate<true>(ag, n, al.s));
+    BQ_TRY(agglomerate<true>(ag, n, al.s, "batch.agg_local", "batch.agg_global"));
+    ProfScope ps("batch.collapse", al.s, 6);  // kept, memset, scan (3), collapse
     k_seg_kept<<<div_up(n, 256), 256, 0, al.s>>>(ranges, n, off, numSegs, thr, kept);
     BQ_CUDA(cudaMemsetAsync(kept + n, 0, 4, al.s));
     BQ_TRY(exclusive_scan_u32(kept, rank, n + 1, nullptr, nullptr, al));

@@ -761,8 +761,7 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   if ((s = tmp.get(&pending, 2ull * div_up(n, AGG_CHUNK))) != BQ_OK) return fail(s);
   AggArgs ag{delta, slot, ids, boxes, nodes, nullptr, &st->numValid, nullptr, pending, nullptr, 0};
   if (thr == 1) {
-    ProfScope ps("morton.agglomerate", al.s, 2);
-    if ((s = agglomerate<false>(ag, n, al.s)) != BQ_OK) return fail(s);
+    if ((s = agglomerate<false>(ag, n, al.s, "morton.agg_local", "morton.agg_global")) != BQ_OK) return fail(s);
   } else {
     Node *full = nullptr;
     uint2 *ranges = nullptr;
@@ -776,7 +775,7 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
     if ((ce = cudaMemsetAsync(kept, 0, sizeof(uint32_t) * n, al.s)) != cudaSuccess) return fail(cuda_error(ce, "memset"));
     ag.nodes = full;
     ag.ranges = ranges;
-    if ((s = agglomerate<false>(ag, n, al.s)) != BQ_OK) return fail(s);
+    if ((s = agglomerate<false>(ag, n, al.s, "morton.agg_local", "morton.agg_global")) != BQ_OK) return fail(s);
     k_kept<<<div_up(n, 256), 256, 0, al.s>>>(ranges, &st->numValid, thr, kept);
     if ((s = exclusive_scan_u32(kept, rank, n > 1 ? n - 1 : 1, nullptr, total, al)) != BQ_OK) return fail(s);
     // the number of kept inner nodes decides the output size

@@ -652,9 +652,8 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   if (thr == 1) {
     if ((s = al.get(&nodes, 2ull * hnv)) != BQ_OK) return fail(s);
     {
-      ProfScope ps("rebin.agglomerate", al.s, 2);
       AggArgsT<uint16_t> ag{lev, slot, ids, boxes, nodes, nullptr, nvDev, nullptr, pending, nullptr, 0};
-      if ((s = agglomerate<false>(ag, hnv, al.s)) != BQ_OK) return fail(s);
+      if ((s = agglomerate<false>(ag, hnv, al.s, "rebin.agg_local", "rebin.agg_global")) != BQ_OK) return fail(s);
     }
     uint32_t hf[12];
     if ((ce = cudaMemcpyAsync(hf, ctl, sizeof(hf), cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
@@ -682,9 +681,8 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   if ((s = tmp.get(&kept, hnv)) != BQ_OK) return fail(s);
   if ((s = tmp.get(&rank, hnv)) != BQ_OK) return fail(s);
   {
-    ProfScope ps("rebin.agglomerate", al.s, 2);
     AggArgsT<uint16_t> ag{lev, slot, ids, boxes, full, nullptr, nvDev, ranges, pending, nullptr, 0};
-    if ((s = agglomerate<false>(ag, hnv, al.s)) != BQ_OK) return fail(s);
+    if ((s = agglomerate<false>(ag, hnv, al.s, "rebin.agg_local", "rebin.agg_global")) != BQ_OK) return fail(s);
   }
   if ((ce = cudaMemsetAsync(kept, 0, sizeof(uint32_t) * hnv, al.s)) != cudaSuccess)
     return fail(cuda_error(ce, "memset"));
