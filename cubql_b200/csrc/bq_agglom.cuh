@@ -159,17 +159,20 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
       const bool leftChild = (l == b0) ? true : (r == e0 - 1) ? false : (sLev[l - c0] > sLev[r - c0 + 1]);
       const uint32_t s = leftChild ? r + 1 : l;
       const uint32_t side = leftChild ? 0 : 1;
-      a.nodes[2ull * s + side] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
       if (s <= c0 || s >= cEnd) {  // sibling outside the chunk: global phase
+        a.nodes[2ull * s + side] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
         a.pending[2 * blockIdx.x + (s <= c0 ? 0 : 1)] = make_uint2(l, r);
         break;
       }
       const uint32_t js = s - c0;
       sBox[js][side] = box;
-      __threadfence_block();
-      const uint32_t other = atomicExch(&sSlot[js], leftChild ? l : r);
+      // block-scope release/acquire: the box is visible to the sibling that
+      // sees this exchange, and this thread sees the sibling's box
+      cuda::atomic_ref<uint32_t, cuda::thread_scope_block> slotRef(sSlot[js]);
+      const uint32_t other = slotRef.exchange(leftChild ? l : r, cuda::memory_order_acq_rel);
+      // the node itself is read only by the global phase (a later launch)
+      a.nodes[2ull * s + side] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
       if (other == AGG_EMPTY) break;  // parked; the sibling (here or in the global phase) carries on
-      __threadfence_block();
       const AggBox sib = sBox[js][side ^ 1];
       box = leftChild ? agg_union(box, sib) : agg_union(sib, box);
       if (leftChild) r = other; else l = other;
