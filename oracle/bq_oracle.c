@@ -398,13 +398,26 @@ int orc_sm_build(const obox *boxes, uint32_t n, int makeLeafThreshold, onode *no
 
 /* ------------------------------------------------------------------ */
 /* binned SAH GPU builder (cuBQL/builder/cuda/sah_builder.h:22-538,    */
-/* dispatch gpu_builder.h:41-53).  16 bins per axis over the node's     */
-/* centroid bounds; bin boxes are the union of the prim boxes,          */
-/* AtomicBox-encoded (builder_common.h:38-167, empty = +-FLT_MAX).      */
+/* dispatch gpu_builder.h:41-53) and its edge-length sibling, the ELH  */
+/* builder (cuBQL/builder/cuda/elh_builder.h:22-556, dispatch           */
+/* gpu_builder.h:54-59).  heur 0 = SAH: 16 bins per axis, bin          */
+/* denominator hi - lo + 1e-20, cost measure surfaceArea; heur 1 = ELH: */
+/* 8 bins, denominator hi - lo, measure edgeLengths (sx + sy + sz).     */
+/* Bin boxes are the union of the prim boxes, AtomicBox-encoded          */
+/* (builder_common.h:38-167, empty = +-FLT_MAX).                        */
 /* ------------------------------------------------------------------ */
 #define SAH_BINS 16
 typedef struct { int32_t lo[3], hi[3]; int32_t count, pad; } osah_bin; /* 32 B, as SAHBins::bins[] */
-typedef struct { osah_bin b[3][SAH_BINS]; } osah_bins;
+typedef struct { osah_bin b[3][SAH_BINS]; } osah_bins;                /* ELH uses b[d][0..7] */
+static int heur_bins(int heur) { return heur ? 8 : SAH_BINS; }
+
+/* edgeLengths(box) (elh_builder.h:66-76): sum += upper - lower, from 0 */
+static float elh_len(const float *lo, const float *hi)
+{
+  float sum = 0.f;
+  for (int k = 0; k < 3; k++) sum += hi[k] - lo[k];
+  return sum;
+}
 
 /* surfaceArea(box3f) (cuBQL/math/box.h:198-205): sx*sy + sx*sz + sy*sz */
 static float sah_area(const float *lo, const float *hi, int fma_mode)
@@ -416,17 +429,24 @@ static float sah_area(const float *lo, const float *hi, int fma_mode)
 
 float orc_sah_area(const float *lo, const float *hi, int fma_mode) { return sah_area(lo, hi, fma_mode); }
 
-/* evaluateSAH (sah_builder.h:61-104): returns the split dim (-1: leaf) and
-   *splitBin; costs lArea*lCount + rArea*rCount */
-int orc_sah_evaluate(const osah_bins *s, int fma_mode, int *splitBin)
+static float heur_measure(const float *lo, const float *hi, int fma_mode, int heur)
 {
+  return heur ? elh_len(lo, hi) : sah_area(lo, hi, fma_mode);
+}
+
+/* evaluateSAH (sah_builder.h:61-104) / evaluateELH (elh_builder.h:93-133):
+   returns the split dim (-1: leaf) and *splitBin; costs
+   lMeasure*lCount + rMeasure*rCount */
+int orc_heur_evaluate(const osah_bins *s, int fma_mode, int heur, int *splitBin)
+{
+  const int NB = heur_bins(heur);
   float bestCost = INFINITY;
   int splitDim = -1;
   float rAreas[SAH_BINS];
   for (int d = 0; d < 3; d++) {
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     int rCount = 0;
-    for (int b = SAH_BINS - 1; b >= 0; --b) {
+    for (int b = NB - 1; b >= 0; --b) {
       const osah_bin *bin = &s->b[d][b];
       for (int k = 0; k < 3; k++) {
         float bl = dec_f(bin->lo[k]), bh = dec_f(bin->hi[k]);
@@ -434,16 +454,16 @@ int orc_sah_evaluate(const osah_bins *s, int fma_mode, int *splitBin)
         if (bh > hi[k]) hi[k] = bh;
       }
       rCount += bin->count;
-      rAreas[b] = sah_area(lo, hi, fma_mode);
+      rAreas[b] = heur_measure(lo, hi, fma_mode, heur);
     }
     float leafCost = rAreas[0] * (float)rCount;
     if (leafCost < bestCost) { bestCost = leafCost; splitDim = -1; }
     lo[0] = lo[1] = lo[2] = INFINITY;
     hi[0] = hi[1] = hi[2] = -INFINITY;
     int lCount = 0;
-    for (int b = 0; b < SAH_BINS; b++) {
+    for (int b = 0; b < NB; b++) {
       float rArea = rAreas[b];
-      float lArea = sah_area(lo, hi, fma_mode);
+      float lArea = heur_measure(lo, hi, fma_mode, heur);
       if (lCount > 0 && rCount > 0) {
         float cost = fma_mode ? fmaf(lArea, (float)lCount, rArea * (float)rCount)
                               : lArea * (float)lCount + rArea * (float)rCount;
@@ -462,14 +482,21 @@ int orc_sah_evaluate(const osah_bins *s, int fma_mode, int *splitBin)
   return splitDim;
 }
 
-/* bin of a centroid coordinate (binPrims :170-180, updatePrims :300-306) */
-static int sah_bin_of(float c, float lo, float hi)
+int orc_sah_evaluate(const osah_bins *s, int fma_mode, int *splitBin)
+{
+  return orc_heur_evaluate(s, fma_mode, 0, splitBin);
+}
+
+/* bin of a centroid coordinate (SAH binPrims :170-180, updatePrims
+   :300-306; ELH :205-217, :343-351 divide by hi - lo alone) */
+static int sah_bin_of(float c, float lo, float hi, int heur)
 {
   if (!(hi > lo)) return 0;
-  float rel = (c - lo) / ((hi - lo) + 1e-20f);
-  float f = rel * (float)SAH_BINS;
+  const int NB = heur_bins(heur);
+  float rel = heur ? (c - lo) / (hi - lo) : (c - lo) / ((hi - lo) + 1e-20f);
+  float f = rel * (float)NB;
   int bin = (f != f) ? 0 : (f >= 2147483647.f ? 2147483647 : (f <= -2147483648.f ? (-2147483647 - 1) : (int)f));
-  return bin < 0 ? 0 : (bin > SAH_BINS - 1 ? SAH_BINS - 1 : bin);
+  return bin < 0 ? 0 : (bin > NB - 1 ? NB - 1 : bin);
 }
 
 static void sah_center(const obox *b, int d, float *c) { *c = 0.5f * (b->lo[d] + b->hi[d]); }
@@ -479,9 +506,10 @@ static void sah_center(const obox *b, int d, float *c) { *c = 0.5f * (b->lo[d] +
    (nodeID, primID) sort, :446-473).  A node the heuristic would make a
    leaf of more than 65535 prims (the 16-bit count) is split in halves
    by position instead (the reference writes a truncated count). */
-int orc_sah_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int fma_mode, onode *nodes,
-                  uint32_t *primIDs, uint32_t *numNodes, uint32_t *numPrims)
+int orc_heur_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int fma_mode, int heur, onode *nodes,
+                   uint32_t *primIDs, uint32_t *numNodes, uint32_t *numPrims)
 {
+  const int NB = heur_bins(heur);
   if (n == 0) { *numNodes = 0; *numPrims = 0; return 0; }
   int thr = makeLeafThreshold;
   uint32_t *cur = primIDs, *alt = (uint32_t *)malloc(sizeof(uint32_t) * n);
@@ -511,7 +539,7 @@ int orc_sah_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int fma_
       for (int d = 0; d < 3; d++) { clo[d] = dec_f(o->cbLo[d]); chi[d] = dec_f(o->cbHi[d]); }
       if ((int64_t)count > thr) {                       /* selectSplits :220-263 */
         for (int d = 0; d < 3; d++)
-          for (int b = 0; b < SAH_BINS; b++) {
+          for (int b = 0; b < NB; b++) {
             osah_bin *x = &bins->b[d][b];
             for (int k = 0; k < 3; k++) { x->lo[k] = enc_f(FLT_MAX); x->hi[k] = enc_f(-FLT_MAX); }
             x->count = 0;
@@ -521,7 +549,7 @@ int orc_sah_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int fma_
           for (int d = 0; d < 3; d++) {
             float c;
             sah_center(pb, d, &c);
-            osah_bin *x = &bins->b[d][sah_bin_of(c, clo[d], chi[d])];
+            osah_bin *x = &bins->b[d][sah_bin_of(c, clo[d], chi[d], heur)];
             for (int k = 0; k < 3; k++) {
               int32_t el = enc_f(pb->lo[k]), eh = enc_f(pb->hi[k]);
               if (el < x->lo[k]) x->lo[k] = el;
@@ -530,7 +558,7 @@ int orc_sah_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int fma_
             x->count++;
           }
         }
-        dim = orc_sah_evaluate(bins, fma_mode, &sbin);
+        dim = orc_heur_evaluate(bins, fma_mode, heur, &sbin);
       }
       int halves = dim < 0 && count > 65535u;
       if (dim < 0 && !halves) { nodes[id].admin = ADMIN(o->begin, count); continue; }
@@ -539,14 +567,14 @@ int orc_sah_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int fma_
       for (uint32_t i = o->begin; i < o->end; i++) {
         float c = 0.f;
         if (!halves) sah_center(&boxes[cur[i]], dim, &c);
-        int side = halves ? (i - o->begin) >= count / 2 : sah_bin_of(c, clo[dim], chi[dim]) >= sbin;
+        int side = halves ? (i - o->begin) >= count / 2 : sah_bin_of(c, clo[dim], chi[dim], heur) >= sbin;
         if (!side) nLeft++;
       }
       uint32_t wl = o->begin, wr = o->begin + nLeft;
       for (uint32_t i = o->begin; i < o->end; i++) {
         float c = 0.f;
         if (!halves) sah_center(&boxes[cur[i]], dim, &c);
-        int side = halves ? (i - o->begin) >= count / 2 : sah_bin_of(c, clo[dim], chi[dim]) >= sbin;
+        int side = halves ? (i - o->begin) >= count / 2 : sah_bin_of(c, clo[dim], chi[dim], heur) >= sbin;
         if (!side) alt[wl++] = cur[i]; else alt[wr++] = cur[i];
       }
       memcpy(cur + o->begin, alt + o->begin, sizeof(uint32_t) * count);
@@ -570,6 +598,12 @@ int orc_sah_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int fma_
   refit_tree(nodes, *numNodes, cur, boxes);
   free(alt); free(lvl); free(lvlId); free(nxt); free(nxtId); free(bins);
   return 0;
+}
+
+int orc_sah_build(const obox *boxes, uint32_t n, int makeLeafThreshold, int fma_mode, onode *nodes,
+                  uint32_t *primIDs, uint32_t *numNodes, uint32_t *numPrims)
+{
+  return orc_heur_build(boxes, n, makeLeafThreshold, fma_mode, 0, nodes, primIDs, numNodes, numPrims);
 }
 
 /* ------------------------------------------------------------------ */

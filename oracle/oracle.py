@@ -113,18 +113,21 @@ class Oracle:
     def sm_build(self, boxes, makeLeafThreshold=0):
         return self._tree(self.lib.orc_sm_build, boxes, ctypes.c_int(makeLeafThreshold))
 
-    def sah_build(self, boxes, makeLeafThreshold=0, fma_mode=1):
-        return self._tree(self.lib.orc_sah_build, boxes, ctypes.c_int(makeLeafThreshold), ctypes.c_int(fma_mode))
+    def sah_build(self, boxes, makeLeafThreshold=0, fma_mode=1, heur=0):
+        """heur 0: SAH builder; 1: ELH builder (8 bins, edge lengths)."""
+        return self._tree(self.lib.orc_heur_build, boxes, ctypes.c_int(makeLeafThreshold), ctypes.c_int(fma_mode),
+                          ctypes.c_int(heur))
 
-    def sah_evaluate(self, bins, fma_mode=1):
-        """evaluateSAH per SAH_BINS record: (dims (-1 leaf), bins)."""
+    def sah_evaluate(self, bins, fma_mode=1, heur=0):
+        """evaluateSAH (heur 0) / evaluateELH (heur 1, bins b[:, :8]) per
+        SAH_BINS record: (dims (-1 leaf), bins)."""
         bins = np.ascontiguousarray(bins, dtype=SAH_BINS)
         dims = np.zeros(len(bins), dtype=np.int32)
         sb = np.zeros(len(bins), dtype=np.int32)
         for i in range(len(bins)):
             b = ctypes.c_int(0)
-            dims[i] = self.lib.orc_sah_evaluate(bins[i:i + 1].ctypes.data_as(ctypes.c_void_p), ctypes.c_int(fma_mode),
-                                                ctypes.byref(b))
+            dims[i] = self.lib.orc_heur_evaluate(bins[i:i + 1].ctypes.data_as(ctypes.c_void_p),
+                                                 ctypes.c_int(fma_mode), ctypes.c_int(heur), ctypes.byref(b))
             sb[i] = b.value
         return dims, sb
 
@@ -419,7 +422,7 @@ class RefCPU:
 
 class RefGPU:
     """The reference's GPU code (runs only where a GPU is present)."""
-    RADIX, SPATIAL_MEDIAN, REBIN, WIDE4, WIDE8, SAH = 0, 1, 2, 3, 4, 5
+    RADIX, SPATIAL_MEDIAN, REBIN, WIDE4, WIDE8, SAH, ELH = 0, 1, 2, 3, 4, 5, 6
 
     def __init__(self):
         self.lib = _load(REF_GPU_SO)
@@ -465,6 +468,17 @@ class RefGPU:
                                               _p(ex) if ex is not None else None, _p(ids), _p(d))
         assert rc == 0
         return ids, d
+
+    def elh_pin(self, bins):
+        """The reference's evaluateELH on each record's first 8 bins per
+        axis: (dims, splitBins)."""
+        bins = np.ascontiguousarray(bins, dtype=SAH_BINS)
+        packed = np.ascontiguousarray(bins["b"][:, :, :8])  # ELHBins<float,3>: 3 x 8 bins of 32 B
+        dims = np.zeros(len(bins), dtype=np.int32)
+        sb = np.zeros(len(bins), dtype=np.int32)
+        rc = self.lib.ref_gpu_elh_pin(_p(packed), ctypes.c_int(len(bins)), _p(dims), _p(sb))
+        assert rc == 0
+        return dims, sb
 
     def sah_pin(self, bins, boxes):
         """The reference's evaluateSAH on each SAH_BINS record and its

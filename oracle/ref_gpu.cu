@@ -126,6 +126,17 @@ __global__ void k_sah_pin(const sahBuilder_impl::SAHBins *bins, int nb, int *dim
   if (tid < nbox) areas[tid] = surfaceArea(boxes[tid]);
 }
 
+static_assert(sizeof(elhBuilder_impl::ELHBins<float, 3>) == 768, "ELHBins layout");
+__global__ void k_elh_pin(const elhBuilder_impl::ELHBins<float, 3> *bins, int nb, int *dims, int *splitBins)
+{
+  int tid = threadIdx.x + blockIdx.x * blockDim.x;
+  if (tid >= nb) return;
+  int splitDim = -1, splitBin = 0;
+  elhBuilder_impl::evaluateELH<float, 3>(splitDim, splitBin, bins[tid]);
+  dims[tid] = splitDim;
+  splitBins[tid] = splitDim < 0 ? 0 : splitBin;
+}
+
 template <int KMAX>
 __global__ void k_knn(bvh3f bvh, const vec3f *pts, const vec3f *qs, int nq, int k, float maxSqr, int *ids,
                       float *dists, int *numFound)
@@ -350,6 +361,10 @@ int run_build(int method, const box3f *d_boxes, uint32_t n, int leafThr, bvh3f &
   cfg.makeLeafThreshold = leafThr;
   if (method == 5)
     cuBQL::cuda::sahBuilder(bvh, d_boxes, n, cfg);
+  else if (method == 6) {  // gpuBuilder with BuildConfig::ELH (gpu_builder.h:54-59)
+    cfg.buildMethod = BuildConfig::ELH;
+    gpuBuilder(bvh, d_boxes, n, cfg);
+  }
   else if (method == 0)
     cuBQL::cuda::radixBuilder(bvh, d_boxes, n, cfg);
   else if (method == 1)
@@ -365,7 +380,7 @@ extern "C" {
 int ref_gpu_node_size(void) { return (int)sizeof(bvh3f::Node); }
 
 // method: 0 radixBuilder, 1 gpuBuilder (spatial median), 2 rebinRadixBuilder,
-// 5 cuda::sahBuilder.
+// 5 cuda::sahBuilder, 6 gpuBuilder with BuildConfig::ELH.
 // nodesOut must hold 2n+2 nodes, primIDsOut n entries.
 int ref_gpu_build(int method, const float *boxes, uint32_t n, int makeLeafThreshold, void *nodesOut,
                   uint32_t *primIDsOut, uint32_t *numNodes, uint32_t *numPrims)
@@ -677,6 +692,18 @@ int ref_gpu_sah_pin(const void *bins, int nb, int *dims, int *splitBins, const f
   cudaMemcpy(splitBins, ds, sizeof(int) * nb, cudaMemcpyDeviceToHost);
   cudaMemcpy(areas, da, sizeof(float) * nbox, cudaMemcpyDeviceToHost);
   cudaFree(db); cudaFree(dbox); cudaFree(dd); cudaFree(ds); cudaFree(da);
+  return 0;
+}
+
+int ref_gpu_elh_pin(const void *bins, int nb, int *dims, int *splitBins)
+{
+  auto *db = dalloc_copy((const elhBuilder_impl::ELHBins<float, 3> *)bins, nb);
+  int *dd = dalloc_copy<int>(nullptr, nb), *ds = dalloc_copy<int>(nullptr, nb);
+  k_elh_pin<<<(nb + 127) / 128, 128>>>(db, nb, dd, ds);
+  RCHECK(cudaDeviceSynchronize());
+  cudaMemcpy(dims, dd, sizeof(int) * nb, cudaMemcpyDeviceToHost);
+  cudaMemcpy(splitBins, ds, sizeof(int) * nb, cudaMemcpyDeviceToHost);
+  cudaFree(db); cudaFree(dd); cudaFree(ds);
   return 0;
 }
 

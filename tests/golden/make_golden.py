@@ -10,7 +10,7 @@
   python tests/golden/make_golden.py gpu_wide   # on a B200: the reference's
                                            # WideBVH builds and queries
   python tests/golden/make_golden.py gpu_sah    # on a B200: the reference's
-                                           # SAH builds and evaluateSAH
+                                           # SAH and ELH builds, evaluateSAH/ELH
 
 Both read oracle/_ref/ (the reference compiled from its own sources by
 oracle/build_ref.sh).  Inputs are the seeded generators of
@@ -257,12 +257,16 @@ def gpu_sah():
     out = {}
     bins, boxes = sah_pin_inputs()
     out["pin_dims"], out["pin_bins"], out["pin_areas"] = r.sah_pin(bins, boxes)
+    out["elh_pin_dims"], out["elh_pin_bins"] = r.elh_pin(bins)
     for name, b in sah_tree_inputs():
         out[f"{name}_boxes"] = b
         for thr in (0, 4):
             n, pr = r.build(RefGPU.SAH, b, thr)
             cn, cp = o.canonicalize(n, pr)
             out[f"{name}{thr}_nodes"], out[f"{name}{thr}_prims"] = cn.view(np.uint8), cp
+            n, pr = r.build(RefGPU.ELH, b, thr)
+            cn, cp = o.canonicalize(n, pr)
+            out[f"{name}{thr}_elh_nodes"], out[f"{name}{thr}_elh_prims"] = cn.view(np.uint8), cp
     dest = sys.argv[2] if len(sys.argv) > 2 else os.path.join(HERE, "ref_gpu_sah.npz")
     np.savez_compressed(dest, **out)
 

@@ -407,12 +407,30 @@ def test_sah_oracle_matches_reference_gpu_fixtures(oracle):
     for name in ("u", "g", "t", "e"):
         b = g[f"{name}_boxes"]
         for thr in (0, 4):
-            n, pr = oracle.sah_build(b, thr)
-            cn, cp = oracle.canonicalize(n, pr)
-            ref = g[f"{name}{thr}_nodes"].view(NODE).copy()
-            cn = cn.copy()
-            cn[1] = np.zeros(1, dtype=NODE)
-            ref[1] = np.zeros(1, dtype=NODE)
-            assert len(cn) == len(ref), (name, thr)
-            assert cn.tobytes() == ref.tobytes(), (name, thr)
-            assert np.array_equal(cp, g[f"{name}{thr}_prims"]), (name, thr)
+            for heur, tag in ((0, ""), (1, "_elh")):
+                if f"{name}{thr}{tag}_nodes" not in g.files:
+                    continue
+                n, pr = oracle.sah_build(b, thr, heur=heur)
+                cn, cp = oracle.canonicalize(n, pr)
+                ref = g[f"{name}{thr}{tag}_nodes"].view(NODE).copy()
+                cn = cn.copy()
+                cn[1] = np.zeros(1, dtype=NODE)
+                ref[1] = np.zeros(1, dtype=NODE)
+                assert len(cn) == len(ref), (name, thr, heur)
+                assert cn.tobytes() == ref.tobytes(), (name, thr, heur)
+                assert np.array_equal(cp, g[f"{name}{thr}{tag}_prims"]), (name, thr, heur)
+
+
+def test_elh_oracle_matches_reference_gpu_fixtures(oracle):
+    """The edge-length heuristic (elh_builder.h, gpuBuilder with
+    BuildConfig::ELH): evaluateELH decisions on the seeded bin sets (first 8
+    bins per axis) against the reference's own device function; its trees are
+    checked in test_sah_oracle_matches_reference_gpu_fixtures."""
+    from tests.golden.make_golden import sah_pin_inputs
+    g = _load("ref_gpu_sah.npz")
+    if "elh_pin_dims" not in g.files:
+        pytest.skip("ELH fixtures not generated")
+    bins, _ = sah_pin_inputs()
+    dims, sb = oracle.sah_evaluate(bins, fma_mode=1, heur=1)
+    assert np.array_equal(dims, g["elh_pin_dims"])
+    assert np.array_equal(np.where(dims < 0, 0, sb), g["elh_pin_bins"])
