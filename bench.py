@@ -193,7 +193,9 @@ def reference_components(W, n):
         tbox = np.concatenate([tv.min(1), tv.max(1)], 1).astype(np.float32)
         comp["sah_build_triangles"] = {"triangles": int(len(tris)),
                                        "reference_sahBuilder_ms": RefGPU().time_build_boxes(RefGPU.SAH, tbox, 0,
-                                                                                           reps=2)}
+                                                                                           reps=2),
+                                       "reference_gpuBuilder_elh_ms": RefGPU().time_build_boxes(RefGPU.ELH, tbox, 0,
+                                                                                               reps=2)}
     return comp
 
 
@@ -368,11 +370,12 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
     # SAH and spatial-median builds over the triangle boxes (the SAH builder's use case)
     tbox = bq.triangles.boxes(tt, tv)
     ms_sah = ev_time(lambda: bq.cuda.sahBuilder(tbox).free())
+    ms_elh = ev_time(lambda: bq.gpuBuilder(tbox, bq.BuildConfig().enableELH()).free())
     ms_smt = ev_time(lambda: bq.gpuBuilder(tbox).free())
     with bq.profile() as prof:
         bq.cuda.sahBuilder(tbox).free()
     comp["sah_build_triangles"] = {"triangles": int(len(tris)), "ms": ms_sah, "Mprims_s": len(tris) / ms_sah / 1e3,
-                                   "spatial_median_ms": ms_smt,
+                                   "spatial_median_ms": ms_smt, "elh_ms": ms_elh,
                                    "phases_ms": {k: round(v[1], 4) for k, v in prof.table.items()}}
     tb = bq.cuda.radixBuilder(tbox)
     ms_f = ev_time(lambda: bq.triangles.findClosest(tb, tt, tv, tq))

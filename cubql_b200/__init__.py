@@ -234,6 +234,11 @@ class BuildConfig:
         self.buildMethod = BuildConfig.SAH
         return self
 
+    def enableELH(self):
+        """BuildConfig::enableELH (cuBQL/bvh.h:33)."""
+        self.buildMethod = BuildConfig.ELH
+        return self
+
     def c(self):
         return bq_build_config(self.maxAllowedLeafSize, self.makeLeafThreshold, self.buildMethod)
 

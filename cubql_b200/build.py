@@ -29,7 +29,8 @@ def sources():
 
 def _compile(src, ptxas_verbose):
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-    deps = [src] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    # every source of the directory: a .cu may include another (bq_elh.cu includes bq_sah.cu)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".cu"))]
     deps.append(os.path.join(HERE, "..", "include", "bq.h"))
     if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps):
         return obj, ""

@@ -19,6 +19,7 @@ int wide_box_query_fill(const bq_wide_bvh3f *bvh, int W, const bq_box3f *boxes, 
                         uint32_t nq, const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al);
 int collapse_wide(const bq_bvh3f *bin, int W, bq_wide_bvh3f *out, bool copyPrims, Alloc &al);
 int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
+int build_elh(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
 int build_wide(bq_wide_bvh3f *out, int W, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
 int wide_closest_point(const bq_wide_bvh3f *bvh, int W, const float *points, const float *queries, uint32_t nq,
                        float maxSqr, const bq_query_config *qcfg, int32_t *ids, float *d, Alloc &al);
@@ -135,10 +136,11 @@ int bq_build_spatial_median_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t nu
                                const bq_allocator *alloc, bq_stream_t stream)
 {
   BQ_TRY(check_build(bvh, boxes, numPrims));
-  if (cfg && cfg->buildMethod != BQ_SPATIAL_MEDIAN && cfg->buildMethod != BQ_SAH)
-    return set_error(BQ_ERR_UNSUPPORTED, "buildMethod must be BQ_SPATIAL_MEDIAN or BQ_SAH");
+  if (cfg && cfg->buildMethod != BQ_SPATIAL_MEDIAN && cfg->buildMethod != BQ_SAH && cfg->buildMethod != BQ_ELH)
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "buildMethod must be BQ_SPATIAL_MEDIAN, BQ_SAH or BQ_ELH");
   Alloc al = make_alloc(alloc, stream);
   if (cfg && cfg->buildMethod == BQ_SAH) return build_sah(bvh, boxes, numPrims, cfg, al);  // gpu_builder.h:41-53
+  if (cfg && cfg->buildMethod == BQ_ELH) return build_elh(bvh, boxes, numPrims, cfg, al);  // gpu_builder.h:54-59
   return build_spatial_median(bvh, boxes, numPrims, cfg, al);
 }
 

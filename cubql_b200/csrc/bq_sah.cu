@@ -30,6 +30,9 @@
 //     most 32 prims stays in registers (one prim per lane).
 // The reference can make a leaf of more than 65535 prims (its 16-bit count
 // then wraps); here such a node is split in two halves by position.
+//
+// Compiled twice: as itself (SAH) and, through bq_elh.cu with BQ_HEUR 1,
+// as the edge-length-heuristic builder (8 bins, edge-length measure).
 #include <algorithm>
 #include <cfloat>
 #include <climits>
@@ -42,8 +45,16 @@ int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al);
 
 namespace {
 
-constexpr int SAH_BINS = 16;
+// BQ_HEUR selects the heuristic of this translation unit: 0 = SAH (this
+// file), 1 = ELH (bq_elh.cu includes this file with BQ_HEUR 1).
+#ifndef BQ_HEUR
+#define BQ_HEUR 0
+#endif
+constexpr int HEUR = BQ_HEUR;
+constexpr int SAH_BINS = HEUR ? 8 : 16;      // bins per axis (SAHBins / ELHBins::numBins)
 constexpr int SAH_NB = 3 * SAH_BINS;         // bins per node (3 axes)
+constexpr int SAH_SEG = 32 / SAH_BINS;       // axes per warp pass in the evaluation
+constexpr int SAH_PASSES = (3 + SAH_SEG - 1) / SAH_SEG;
 constexpr int SAH_W = 7;                     // words per bin: lo[3], hi[3], count
 constexpr uint32_t SAH_WARP_MIN = 128;       // warp subtrees: at most warpMax prims, warpMax in
 constexpr uint32_t SAH_WARP_CAP = 4096;      // [SAH_WARP_MIN, SAH_WARP_CAP], about 64 tasks per SM
@@ -75,19 +86,24 @@ struct SahDec {
 
 __device__ __forceinline__ float sah_ctr(float l, float h) { return __fmul_rn(0.5f, __fadd_rn(l, h)); }
 
-// surfaceArea(box3f) (cuBQL/math/box.h:198-205) with the contraction nvcc
-// gives it in the reference's device code (pinned against its kernels)
+// The cost measure of a box.  SAH: surfaceArea(box3f) (cuBQL/math/box.h:
+// 198-205) with the contraction nvcc gives it in the reference's device
+// code (pinned against its kernels).  ELH: edgeLengths (cuBQL/builder/
+// cuda/elh_builder.h:66-76), a sum from 0 with no product to contract.
 __device__ __forceinline__ float sah_area(float lx, float ly, float lz, float hx, float hy, float hz)
 {
   const float sx = __fsub_rn(hx, lx), sy = __fsub_rn(hy, ly), sz = __fsub_rn(hz, lz);
+  if (HEUR) return __fadd_rn(__fadd_rn(__fadd_rn(0.f, sx), sy), sz);
   return __fmaf_rn(sy, sz, __fmaf_rn(sx, sy, __fmul_rn(sx, sz)));
 }
 
-// binPrims (:170-180) / updatePrims (:300-306)
+// binPrims (:170-180) / updatePrims (:300-306); ELH divides by hi - lo
+// alone (elh_builder.h:213-217, 347-351)
 __device__ __forceinline__ int sah_bin(float c, float lo, float hi)
 {
   if (!(hi > lo)) return 0;
-  const float rel = __fdiv_rn(__fsub_rn(c, lo), __fadd_rn(__fsub_rn(hi, lo), 1e-20f));
+  const float den = HEUR ? __fsub_rn(hi, lo) : __fadd_rn(__fsub_rn(hi, lo), 1e-20f);
+  const float rel = __fdiv_rn(__fsub_rn(c, lo), den);
   const int b = __float2int_rz(__fmul_rn(rel, (float)SAH_BINS));
   return max(0, min(SAH_BINS - 1, b));
 }
@@ -134,21 +150,22 @@ __device__ __forceinline__ void bins_add(int32_t *bins, const SahPrim &p, const 
   }
 }
 
-// evaluateSAH by one warp over per-lane bins.  Pass 0: lane L holds bin
-// L & 15 of axis L >> 4 (a*); pass 1: bin L & 15 of axis 2 (b*, lanes
-// 16..31 repeat it and propose nothing).  Unions and counts by 16-lane
-// scans; the first strictly cheapest candidate in (axis, bin) order wins
-// if it is cheaper than the leaf, as in the reference's serial loop.  Empty
-// bins are (+FLT_MAX, -FLT_MAX), as AtomicBox leaves them.
+// evaluateSAH / evaluateELH by one warp over per-lane bins.  In pass p,
+// lane L holds bin L % B of axis p * (32 / B) + L / B (B bins per axis;
+// lanes of a missing fourth axis propose nothing): for SAH axes 0 and 1,
+// then axis 2 (b*); for ELH all three axes in one pass.  Unions and counts
+// by B-lane scans; the first strictly cheapest candidate in (axis, bin)
+// order wins if it is cheaper than the leaf, as in the reference's serial
+// loop.  Empty bins are (+FLT_MAX, -FLT_MAX), as AtomicBox leaves them.
 __device__ __forceinline__ SahDec sah_evaluate_lanes(const float aLo[3], const float aHi[3], int aCnt,
                                                      const float bLo[3], const float bHi[3], int bCnt)
 {
-  const int lane = threadIdx.x & 31, b = lane & 15;
+  const int lane = threadIdx.x & 31, b = lane % SAH_BINS;
   float leafCost = INFINITY;
   float best = INFINITY;
   int bestIdx = INT_MAX;
 #pragma unroll
-  for (int pass = 0; pass < 2; pass++) {
+  for (int pass = 0; pass < SAH_PASSES; pass++) {
     float plo[3], phi[3], slo[3], shi[3];
     int pc = pass ? bCnt : aCnt, sc = pc;
 #pragma unroll
@@ -158,39 +175,39 @@ __device__ __forceinline__ SahDec sah_evaluate_lanes(const float aLo[3], const f
     }
     // inclusive prefix (bins 0..b) and suffix (bins b..15) unions / counts
 #pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-      const int pcu = __shfl_up_sync(0xffffffffu, pc, o, 16);
-      const int scd = __shfl_down_sync(0xffffffffu, sc, o, 16);
+    for (int o = 1; o < SAH_BINS; o <<= 1) {
+      const int pcu = __shfl_up_sync(0xffffffffu, pc, o, SAH_BINS);
+      const int scd = __shfl_down_sync(0xffffffffu, sc, o, SAH_BINS);
       if (b >= o) pc += pcu;
-      if (b + o < 16) sc += scd;
+      if (b + o < SAH_BINS) sc += scd;
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        const float a0 = __shfl_up_sync(0xffffffffu, plo[k], o, 16);
-        const float a1 = __shfl_up_sync(0xffffffffu, phi[k], o, 16);
-        const float a2 = __shfl_down_sync(0xffffffffu, slo[k], o, 16);
-        const float a3 = __shfl_down_sync(0xffffffffu, shi[k], o, 16);
+        const float a0 = __shfl_up_sync(0xffffffffu, plo[k], o, SAH_BINS);
+        const float a1 = __shfl_up_sync(0xffffffffu, phi[k], o, SAH_BINS);
+        const float a2 = __shfl_down_sync(0xffffffffu, slo[k], o, SAH_BINS);
+        const float a3 = __shfl_down_sync(0xffffffffu, shi[k], o, SAH_BINS);
         if (b >= o) { plo[k] = fminf(plo[k], a0); phi[k] = fmaxf(phi[k], a1); }
-        if (b + o < 16) { slo[k] = fminf(slo[k], a2); shi[k] = fmaxf(shi[k], a3); }
+        if (b + o < SAH_BINS) { slo[k] = fminf(slo[k], a2); shi[k] = fmaxf(shi[k], a3); }
       }
     }
     // exclusive prefix: the union of bins 0..b-1 (b == 0: the empty box)
     float elo[3], ehi[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-      const float a0 = __shfl_up_sync(0xffffffffu, plo[k], 1, 16);
-      const float a1 = __shfl_up_sync(0xffffffffu, phi[k], 1, 16);
+      const float a0 = __shfl_up_sync(0xffffffffu, plo[k], 1, SAH_BINS);
+      const float a1 = __shfl_up_sync(0xffffffffu, phi[k], 1, SAH_BINS);
       elo[k] = b > 0 ? a0 : INFINITY;
       ehi[k] = b > 0 ? a1 : -INFINITY;
     }
-    const int pcu = __shfl_up_sync(0xffffffffu, pc, 1, 16);
+    const int pcu = __shfl_up_sync(0xffffffffu, pc, 1, SAH_BINS);
     const int lCount = b > 0 ? pcu : 0;
     const int rCount = sc;
     const float rArea = sah_area(slo[0], slo[1], slo[2], shi[0], shi[1], shi[2]);
     const float lArea = sah_area(elo[0], elo[1], elo[2], ehi[0], ehi[1], ehi[2]);
     if (pass == 0) leafCost = __shfl_sync(0xffffffffu, __fmul_rn(rArea, (float)rCount), 0);  // rAreas[0]*rCount
-    const int dim = pass ? 2 : (lane >> 4);
+    const int dim = pass * SAH_SEG + lane / SAH_BINS;
     float cost = INFINITY;
-    if (lCount > 0 && rCount > 0 && (pass == 0 || lane < 16)) {
+    if (lCount > 0 && rCount > 0 && dim < 3) {
       cost = __fmaf_rn(lArea, (float)lCount, __fmul_rn(rArea, (float)rCount));
       if (cost != cost) cost = INFINITY;  // NaN never wins (cost < best is false)
     }
@@ -223,19 +240,28 @@ __device__ __forceinline__ SahDec sah_evaluate_lanes(const float aLo[3], const f
   return dec;
 }
 
-// evaluateSAH over 48 encoded bins (bins[(d*16+b)*7 + ...], shared or global)
+// evaluation over 3*B encoded bins (bins[(d*B+b)*7 + ...], shared or global)
 __device__ __forceinline__ SahDec sah_evaluate(const int32_t *bins)
 {
-  const int lane = threadIdx.x & 31, b = lane & 15;
-  const int32_t *xa = bins + ((lane >> 4) * SAH_BINS + b) * SAH_W;
-  const int32_t *xb = bins + (2 * SAH_BINS + b) * SAH_W;
+  const int lane = threadIdx.x & 31, b = lane % SAH_BINS;
+  const int da = lane / SAH_BINS, db = SAH_SEG + lane / SAH_BINS;  // axes of passes 0 and 1
   float aLo[3], aHi[3], bLo[3], bHi[3];
+  int aCnt = 0, bCnt = 0;
 #pragma unroll
-  for (int k = 0; k < 3; k++) {
-    aLo[k] = dec_f(xa[k]); aHi[k] = dec_f(xa[3 + k]);
-    bLo[k] = dec_f(xb[k]); bHi[k] = dec_f(xb[3 + k]);
+  for (int k = 0; k < 3; k++) { aLo[k] = bLo[k] = FLT_MAX; aHi[k] = bHi[k] = -FLT_MAX; }
+  if (da < 3) {
+    const int32_t *xa = bins + (da * SAH_BINS + b) * SAH_W;
+#pragma unroll
+    for (int k = 0; k < 3; k++) { aLo[k] = dec_f(xa[k]); aHi[k] = dec_f(xa[3 + k]); }
+    aCnt = xa[6];
   }
-  return sah_evaluate_lanes(aLo, aHi, xa[6], bLo, bHi, xb[6]);
+  if (SAH_PASSES > 1 && db < 3) {
+    const int32_t *xb = bins + (db * SAH_BINS + b) * SAH_W;
+#pragma unroll
+    for (int k = 0; k < 3; k++) { bLo[k] = dec_f(xb[k]); bHi[k] = dec_f(xb[3 + k]); }
+    bCnt = xb[6];
+  }
+  return sah_evaluate_lanes(aLo, aHi, aCnt, bLo, bHi, bCnt);
 }
 
 // running encoded min/max of the two children's centroids
@@ -604,7 +630,7 @@ __device__ void sah_small_subtree(const SahNode &root, const SahPrim *src, int t
   if (lane < (int)cnt) p = src[base + lane];
   else p.a = p.b = make_float4(0.f, 0.f, 0.f, 0.f);
   const uint32_t pos = base + lane;
-  const int dimA = lane >> 4, binL = lane & 15;
+  const int dimA = lane / SAH_BINS, dimB = SAH_SEG + lane / SAH_BINS, binL = lane % SAH_BINS;
   SahNode cur = root;
   int sp = 0;
   while (true) {
@@ -631,12 +657,14 @@ __device__ void sah_small_subtree(const SahNode &root, const SahPrim *src, int t
         const float h1 = __shfl_sync(0xffffffffu, p.b.y, j), h2 = __shfl_sync(0xffffffffu, p.b.z, j);
         const int j0 = __shfl_sync(0xffffffffu, mb[0], j), j1 = __shfl_sync(0xffffffffu, mb[1], j);
         const int j2 = __shfl_sync(0xffffffffu, mb[2], j);
-        if ((dimA ? j1 : j0) == binL) {
+        const int ja = dimA == 0 ? j0 : (dimA == 1 ? j1 : (dimA == 2 ? j2 : -1));
+        const int jb = dimB == 0 ? j0 : (dimB == 1 ? j1 : (dimB == 2 ? j2 : -1));
+        if (ja == binL) {
           aLo[0] = fminf(aLo[0], l0); aLo[1] = fminf(aLo[1], l1); aLo[2] = fminf(aLo[2], l2);
           aHi[0] = fmaxf(aHi[0], h0); aHi[1] = fmaxf(aHi[1], h1); aHi[2] = fmaxf(aHi[2], h2);
           aCnt++;
         }
-        if (j2 == binL) {
+        if (SAH_PASSES > 1 && jb == binL) {
           bLo[0] = fminf(bLo[0], l0); bLo[1] = fminf(bLo[1], l1); bLo[2] = fminf(bLo[2], l2);
           bHi[0] = fmaxf(bHi[0], h0); bHi[1] = fmaxf(bHi[1], h1); bHi[2] = fmaxf(bHi[2], h2);
           bCnt++;
@@ -849,7 +877,11 @@ __global__ void k_sah_compact(const Node *__restrict__ full, const uint32_t *__r
 
 namespace bq {
 
+#if BQ_HEUR == 0
 int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al)
+#else
+int build_elh(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al)
+#endif
 {
   const int thr = cfg ? cfg->makeLeafThreshold : 0;  // 0 and 1 build the same tree
   if (thr < 0 || thr > 65535)
@@ -879,7 +911,7 @@ int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
       (ce = cudaMemsetAsync(used, 0, sizeof(uint32_t) * n, al.s)) != cudaSuccess)
     return fail(cuda_error(ce, "sah set-up"));
   {
-    ProfScope ps("sah.setup", al.s, 5);
+    ProfScope ps(HEUR ? "elh.setup" : "sah.setup", al.s, 5);
     k_sah_valid<<<div_up(n, 256), 256, 0, al.s>>>(boxes, n, valid);
     if ((s = exclusive_scan_u32(valid, vpos, n, nullptr, ctl, al)) != BQ_OK) return fail(s);
     k_sah_init<<<std::min(div_up(n, 256), num_sms() * 8), 256, 0, al.s>>>(boxes, n, vpos, ctl, buf0, primIDs,
@@ -935,7 +967,7 @@ int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
     return fail(cuda_error(ce, "sah set-up"));
   const int warpGrid = num_sms() * 8;
   auto warp_phase = [&]() -> int {
-    ProfScope ps("sah.warps", al.s);
+    ProfScope ps(HEUR ? "elh.warps" : "sah.warps", al.s);
     k_sah_warp<<<warpGrid, SAHW_BLOCK, 0, al.s>>>(tasks, sc, taskCap, thr, buf0, buf1, full, primIDs, used);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemsetAsync(&sc->taskCount, 0, 2 * sizeof(uint32_t), al.s);  // taskCount, grab
@@ -944,7 +976,7 @@ int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
   int cur = 0;
   for (int level = 0; rootBig; level++) {
     {
-      ProfScope ps("sah.level", al.s, 12);
+      ProfScope ps(HEUR ? "elh.level" : "sah.level", al.s, 12);
       k_sah_tiles<<<cap, 128, 0, al.s>>>(bigList[cur], sc, cur, cap, tileCount, nodeBins);
       if ((s = exclusive_scan_u32(tileCount, first, cap, &sc->bigCount[cur], &sc->numTiles, al)) != BQ_OK)
         return fail(s);
@@ -981,7 +1013,7 @@ int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
   uint32_t *rank = nullptr;
   if ((s = tmp.get(&rank, nv)) != BQ_OK) return fail(s);
   {
-    ProfScope ps("sah.rank", al.s, 3);
+    ProfScope ps(HEUR ? "elh.rank" : "sah.rank", al.s, 3);
     if ((s = exclusive_scan_u32(used, rank, nv, nullptr, ctl + 2, al)) != BQ_OK) return fail(s);
   }
   uint32_t hres[2], herr = 0;
@@ -994,7 +1026,7 @@ int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
   Node *nodes = nullptr;
   if ((s = al.get(&nodes, numNodes)) != BQ_OK) return fail(s);
   {
-    ProfScope ps("sah.compact", al.s);
+    ProfScope ps(HEUR ? "elh.compact" : "sah.compact", al.s);
     k_sah_compact<<<div_up(nv, 256), 256, 0, al.s>>>(full, used, rank, nv, nodes);
   }
   bvh->nodes = reinterpret_cast<bq_node3f *>(nodes);

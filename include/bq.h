@@ -48,7 +48,7 @@ extern "C" {
 /* build methods (cuBQL/bvh.h:38-55 BuildConfig::BuildMethod) */
 #define BQ_SPATIAL_MEDIAN 0
 #define BQ_SAH 1 /* binned surface-area heuristic (BuildConfig::SAH) */
-#define BQ_ELH 2 /* edge-length heuristic: not implemented (BQ_ERR_UNSUPPORTED) */
+#define BQ_ELH 2 /* edge-length heuristic (BuildConfig::ELH) */
 #define BQ_MORTON63 16 /* cuda::radixBuilder */
 #define BQ_MORTON30 17 /* cuda::rebinRadixBuilder */
 
@@ -80,7 +80,7 @@ typedef struct bq_bvh3f {
 typedef struct bq_build_config {
   int maxAllowedLeafSize; /* default 1<<15 */
   int makeLeafThreshold;  /* 0 = builder default (1) */
-  int buildMethod;        /* BQ_SPATIAL_MEDIAN or BQ_SAH (bq_build_spatial_median_f3 only) */
+  int buildMethod;        /* BQ_SPATIAL_MEDIAN, BQ_SAH or BQ_ELH (bq_build_spatial_median_f3 only) */
 } bq_build_config;
 
 /* replaces cuBQL::GpuMemoryResource (cuBQL/builder/cuda.h:31-78).
@@ -133,7 +133,10 @@ int bq_build_rebin_morton30_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t nu
    cuBQL/builder/cuda/gpu_builder.h:31-67): cfg->buildMethod
    BQ_SPATIAL_MEDIAN (default) is the spatial-median builder
    (cuBQL/builder/cuda/sm_builder.h:469-614), BQ_SAH the SAH builder
-   (as bq_build_sah_f3), BQ_ELH is not implemented. */
+   (as bq_build_sah_f3), BQ_ELH the edge-length-heuristic builder
+   (cuBQL/builder/cuda/elh_builder.h:420-556: the SAH builder with 8 bins
+   per axis, bins at (c - lo) / (hi - lo) and edge-length sums as the cost
+   measure).  Other values give BQ_ERR_INVALID_ARGUMENT. */
 int bq_build_spatial_median_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
                                const bq_allocator *alloc, bq_stream_t stream);
 

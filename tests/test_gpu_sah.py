@@ -1,5 +1,6 @@
 """Binned SAH builder on the GPU (bq_build_sah_f3, and gpuBuilder with
-BuildConfig::SAH).
+BuildConfig::SAH) and its edge-length sibling (gpuBuilder with
+BuildConfig::ELH).
 
 Trees equal the oracle's restatement node for node (after BFS renumbering,
 leaf prim order included) and the reference's own sahBuilder compiled for
@@ -32,6 +33,13 @@ def _boxes(kind, n):
     raise ValueError(kind)
 
 
+def _heur_build(bq, heur, t, thr=0):
+    """heur 0: cuda::sahBuilder; 1: gpuBuilder with BuildConfig::ELH."""
+    if heur == 0:
+        return bq.cuda.sahBuilder(t, bq.BuildConfig(makeLeafThreshold=thr))
+    return bq.gpuBuilder(t, bq.BuildConfig(makeLeafThreshold=thr).enableELH())
+
+
 def _same(oracle, a, b):
     ca, pa = oracle.canonicalize(*a)
     cb, pb = oracle.canonicalize(*b)
@@ -42,22 +50,24 @@ def _same(oracle, a, b):
     return len(ca) == len(cb) and ca.tobytes() == cb.tobytes() and np.array_equal(pa, pb)
 
 
+@pytest.mark.parametrize("heur", [0, 1])
 @pytest.mark.parametrize("kind", ["uniform", "gmm", "dupes", "extents", "mesh"])
 @pytest.mark.parametrize("thr", [0, 1, 4, 8])
-def test_sah_matches_oracle(bq, oracle, kind, thr):
+def test_sah_matches_oracle(bq, oracle, heur, kind, thr):
     b = _boxes(kind, 60000)
-    bvh = bq.cuda.sahBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=thr))
-    assert _same(oracle, bvh.to_host(), oracle.sah_build(b, thr))
+    bvh = _heur_build(bq, heur, torch.from_numpy(b).cuda(), thr)
+    assert _same(oracle, bvh.to_host(), oracle.sah_build(b, thr, heur=heur))
     bvh.free()
 
 
+@pytest.mark.parametrize("heur", [0, 1])
 @pytest.mark.parametrize("kind", ["uniform", "gmm", "extents", "mesh"])
-def test_sah_matches_reference_builder(bq, oracle, ref_gpu, kind):
+def test_sah_matches_reference_builder(bq, oracle, ref_gpu, heur, kind):
     b = _boxes(kind, 40000)
     from oracle.oracle import RefGPU
     for thr in (0, 4):
-        bvh = bq.cuda.sahBuilder(torch.from_numpy(b).cuda(), bq.BuildConfig(makeLeafThreshold=thr))
-        assert _same(oracle, bvh.to_host(), ref_gpu.build(RefGPU.SAH, b, thr)), thr
+        bvh = _heur_build(bq, heur, torch.from_numpy(b).cuda(), thr)
+        assert _same(oracle, bvh.to_host(), ref_gpu.build(RefGPU.ELH if heur else RefGPU.SAH, b, thr)), thr
         bvh.free()
 
 
@@ -70,16 +80,17 @@ def test_gpubuilder_sah_dispatch(bq, oracle):
     c = bq.cuda.sahBuilder(t)
     assert _same(oracle, a.to_host(), c.to_host())
     with pytest.raises(bq.BQError):
-        bq.gpuBuilder(t, bq.BuildConfig(buildMethod=bq.BuildConfig.ELH))
+        bq.gpuBuilder(t, bq.BuildConfig(buildMethod=7))
 
 
-def test_sah_large_levels(bq, oracle):
+@pytest.mark.parametrize("heur", [0, 1])
+def test_sah_large_levels(bq, oracle, heur):
     """327,680 triangle boxes (icosphere level 7): several global levels
     before the warp phase."""
     verts, tris = W.icosphere(7)
     b = tri_boxes_np(verts, tris)
-    bvh = bq.cuda.sahBuilder(torch.from_numpy(b).cuda())
-    assert _same(oracle, bvh.to_host(), oracle.sah_build(b, 0))
+    bvh = _heur_build(bq, heur, torch.from_numpy(b).cuda())
+    assert _same(oracle, bvh.to_host(), oracle.sah_build(b, 0, heur=heur))
     bvh.free()
 
 
