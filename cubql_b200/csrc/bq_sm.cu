@@ -17,8 +17,9 @@
 //     counters; one scan over the used split positions compacts the slots at
 //     the end (children of the k-th used split at nodes 2+2k, 2+2k+1; node 1
 //     stays unused, as in the reference);
-//   * nodes with more than SM_WARP_MAX prims are split level by level over
-//     the whole GPU in tiles of SM_TILE prims: k_sm_tiles + one scan (tile
+//   * nodes with more than warpMax prims (256..4096, chosen from the prim
+//     count) are split level by level over the whole GPU in tiles of
+//     SM_TILE prims: k_sm_tiles + one scan (tile
 //     offsets), k_sm_count (right-side count per tile), one scan,
 //     k_sm_children, k_sm_scatter (stable scatter that also reduces the
 //     children's centroid bounds per tile and merges them with one
@@ -26,9 +27,10 @@
 //     is deterministic), k_sm_classify (children to the next level's list or
 //     to the warp tasks).  Lists and counts stay in device memory; the host
 //     reads the counters only every SM_LEVELS_PER_CHECK levels;
-//   * every subtree of at most SM_WARP_MAX prims is finished by one warp
-//     of a persistent grid (k_sm_warp takes tasks from a counter), depth first, smaller child first with the larger one on a
-//     per-warp shared-memory stack; a node of up to 32 prims is held in
+//   * every subtree of at most warpMax prims is finished by one warp
+//     of a persistent grid (k_sm_warp takes tasks from a counter), depth
+//     first, smaller child first with the larger one on a per-warp
+//     shared-memory stack; a node of up to 32 prims is held in
 //     registers, one prim per lane, and its whole subtree is partitioned
 //     with ballots and a 512-byte shared exchange buffer.
 // Degenerate nodes send their k-th prim (primID order) to side
@@ -51,7 +53,13 @@ int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al);
 
 namespace {
 
-constexpr uint32_t SM_WARP_MAX = 4096;  // subtrees up to this size: one warp
+// Warp subtrees hold at most warpMax prims: the largest power of two in
+// [SM_WARP_MIN, SM_WARP_MAX] that still leaves SM_WARP_TASKS subtrees per SM,
+// so small inputs do not end their global levels with a handful of warps
+// busy and large ones do not pay for extra global levels.
+constexpr uint32_t SM_WARP_MIN = 256;
+constexpr uint32_t SM_WARP_MAX = 4096;
+constexpr uint32_t SM_WARP_TASKS = 32;
 constexpr uint32_t SM_TILE = 4096;      // prims per tile in the global levels
 constexpr int SM_BLOCK = 256;           // global-level kernels
 constexpr int SMW_BLOCK = 128;          // warp-phase kernel
@@ -194,7 +202,7 @@ __global__ void __launch_bounds__(256) k_sm_init(const bq_box3f *__restrict__ bo
 }
 
 // ------------------------------------------------------------------
-// global levels (nodes with more than SM_WARP_MAX prims)
+// global levels (nodes with more than warpMax prims)
 // ------------------------------------------------------------------
 // Device-side state of the global levels.  The big-node lists ping-pong
 // between two buffers; their counts, the current level's tile count and
@@ -371,7 +379,7 @@ __global__ void __launch_bounds__(SM_BLOCK) k_sm_scatter(const SmNode *__restric
 }
 
 // ------------------------------------------------------------------
-// warp phase: whole subtrees of at most SM_WARP_MAX prims
+// warp phase: whole subtrees of at most warpMax prims
 // ------------------------------------------------------------------
 __device__ __forceinline__ void leaf_node(Node *out, uint32_t slot, uint32_t b, uint32_t count)
 {
@@ -433,7 +441,7 @@ __device__ void sm_small_subtree(const SmNode &root, const float4 *src, int thr,
   __syncwarp();
 }
 
-// one subtree of at most SM_WARP_MAX prims, by the calling warp; stk and
+// one subtree of at most warpMax prims, by the calling warp; stk and
 // xbuf are the warp's shared-memory stack and exchange buffer
 __device__ void sm_warp_task(SmNode cur, int thr, float4 *buf0, float4 *buf1, Node *__restrict__ out,
                              uint32_t *__restrict__ primIDs, uint32_t *__restrict__ used, uint32_t *err, SmNode *stk,
@@ -529,17 +537,18 @@ __global__ void __launch_bounds__(SMW_BLOCK) k_sm_warp(const SmNode *__restrict_
 
 // children of the level's big nodes: to the next big list or to the tasks
 __global__ void k_sm_classify(const SmNode *__restrict__ next, SmCtl *ctl, int cur, uint32_t cap, int thr,
-                              SmNode *__restrict__ bigNext, SmNode *__restrict__ tasks, uint32_t taskCap)
+                              uint32_t warpMax, SmNode *__restrict__ bigNext, SmNode *__restrict__ tasks,
+                              uint32_t taskCap)
 {
   const uint32_t K = min(ctl->bigCount[cur], cap);
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= 2 * K) return;
   const SmNode c = next[j];
   const uint32_t size = c.e - c.b;
-  if (size > SM_WARP_MAX && (int64_t)size > thr) {
+  if (size > warpMax && (int64_t)size > thr) {
     const uint32_t at = atomicAdd(&ctl->bigCount[cur ^ 1], 1u);
     if (at < cap) bigNext[at] = c;
-    else atomicOr(&ctl->err, DEV_ERR_RANGE);  // cannot happen: big nodes are disjoint and above SM_WARP_MAX
+    else atomicOr(&ctl->err, DEV_ERR_RANGE);  // cannot happen: big nodes are disjoint and above warpMax
   } else {
     const uint32_t at = atomicAdd(&ctl->taskCount, 1u);
     if (at < taskCap) tasks[at] = c;
@@ -625,16 +634,19 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   if ((s = tmp.get(&full, 2ull * nv)) != BQ_OK) return fail(s);
 
   // ---- global levels, driven from device memory ----
-  // Big nodes (more than SM_WARP_MAX prims) of one level are disjoint, so a
+  // Big nodes (more than warpMax prims) of one level are disjoint, so a
   // level holds at most cap of them and at most maxTiles tiles.  The host
   // looks at the counters first when perfectly balanced splits would be
   // done, then every SM_LEVELS_PER_CHECK levels; a level with no big node
   // left costs only its (empty) launches.  Every level adds at most 2 * cap
   // warp tasks, which bounds the task list between two looks.
-  const uint32_t cap = nv / (SM_WARP_MAX + 1) + 1;
+  // warp subtrees small enough that every SM gets several of them
+  uint32_t warpMax = SM_WARP_MIN;
+  while (warpMax < SM_WARP_MAX && (uint64_t)warpMax * 2 * num_sms() * SM_WARP_TASKS <= nv) warpMax *= 2;
+  const uint32_t cap = nv / (warpMax + 1) + 1;
   const uint32_t maxTiles = nv / SM_TILE + cap + 2;
   int nextCheck = 1;
-  while (nextCheck < 62 && ((uint64_t)SM_WARP_MAX << nextCheck) < nv) nextCheck++;
+  while (nextCheck < 62 && ((uint64_t)warpMax << nextCheck) < nv) nextCheck++;
   const uint32_t taskCap =
       std::max<uint32_t>(16 * cap, 4096) + 2 * cap * (uint32_t)std::max(nextCheck, SM_LEVELS_PER_CHECK);
   SmCtl *sc = nullptr;
@@ -648,7 +660,7 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   SmNode root;
   root.b = 0; root.e = nv; root.slot = 0; root.parity = 0;
   for (int d = 0; d < 3; d++) { root.lo[d] = hctl[2 + d]; root.hi[d] = hctl[5 + d]; }
-  const bool rootBig = nv > SM_WARP_MAX && (int64_t)nv > thr;
+  const bool rootBig = nv > warpMax && (int64_t)nv > thr;
   SmCtl hsc{};
   hsc.bigCount[0] = rootBig ? 1u : 0u;
   hsc.taskCount = rootBig ? 0u : 1u;
@@ -678,7 +690,7 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
                                                        next);
       k_sm_scatter<<<maxTiles, SM_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, tileRight, buf0, buf1,
                                                      next);
-      k_sm_classify<<<div_up(2ull * cap, 128), 128, 0, al.s>>>(next, sc, cur, cap, thr, bigList[cur ^ 1], tasks,
+      k_sm_classify<<<div_up(2ull * cap, 128), 128, 0, al.s>>>(next, sc, cur, cap, thr, warpMax, bigList[cur ^ 1], tasks,
                                                                taskCap);
       if ((ce = cudaMemsetAsync(&sc->bigCount[cur], 0, sizeof(uint32_t), al.s)) != cudaSuccess ||
           (ce = cudaGetLastError()) != cudaSuccess)
