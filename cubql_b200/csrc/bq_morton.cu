@@ -14,10 +14,12 @@
 //                 bits [39, 63) in 3 digit passes up to 2^24 prims, bits
 //                 [31, 63) in 4 passes above, instead of 8 (bq_sort.cu)
 //   k_fix_runs    runs of equal top bits are then ordered by the low bits,
-//                 stably: runs of up to 32 prims by one thread each
-//                 (on uniform data nearly all runs are of 1-4 prims),
-//                 longer runs by one segmented composite-key sort of just
-//                 their prims ((run, low bits) keys).  The result is the
+//                 stably, from shared memory: runs of 2..4 prims (on
+//                 uniform data nearly all runs) by one thread each, runs
+//                 of 5..32 by one warp each, grouped by size so that warps
+//                 do not diverge; longer runs by one segmented
+//                 composite-key sort of just their prims ((run, low bits)
+//                 keys).  The result is the
 //                 full stable 63-bit order, as cub's SortPairs gives.  The
 //                 same kernel writes the split levels (below) and slots
 //   k_delta       one byte per adjacent key pair: the level at which the
@@ -329,166 +331,226 @@ __device__ __forceinline__ uint8_t equal_run_level(uint64_t r0, uint64_t r1, uin
   return (uint8_t)(63 - depth);
 }
 
-// The first position i of a run of at least two prims with equal top bits
-// (keys sorted on bits [SB, 63) only): orders the run on the low
-// bits (stable) and writes the levels of the pairs inside it.  Runs of up
-// to MB_THREAD_RUN prims are done here; longer ones are listed for a
-// segmented sort (their inner levels are written by k_delta afterwards).
-template <int SB>
-__device__ __forceinline__ void fix_run_at(uint32_t i, uint32_t nv, uint64_t *keys, uint32_t *ids,
-                                           uint8_t *__restrict__ delta, RunStats *rs, uint4 *runs, uint32_t maxRuns)
+// Every sorted position: its agglomeration slot, the split level of the
+// pair (i, i+1), and the low-bit order inside runs of equal top bits.
+// One block covers FT_TILE consecutive positions, staged in shared memory
+// with FT_HALO positions after them:
+//   A. per position: the slot, the split level of a pair that lies across
+//      two runs (their highest differing bit is a top bit, so it does not
+//      depend on the order inside the runs) and, at the first position of a
+//      run, the run's size class -- 2, 3..4 or more prims -- appended to
+//      that class's list;
+//   B. the block then orders the listed runs class by class, so a warp
+//      runs one code path at a time: pairs and runs of 3..4 by one thread
+//      each in registers, runs of 5..32 by one warp each (a lane per prim
+//      takes its rank), all from shared memory; longer runs are listed for
+//      the segmented sort.
+// A run belongs to the tile holding its first position, including the part
+// of it that lies in the next tile; that tile reads only the top bits of
+// those prims, which the reordering leaves unchanged, and writes none of
+// their keys, ids or inner levels.
+constexpr int FT_BLOCK = 256;
+constexpr int FT_ITEMS = 4;
+constexpr uint32_t FT_TILE = FT_BLOCK * FT_ITEMS;
+constexpr uint32_t FT_HALO = 32;  // a run of up to 32 prims begun in the tile is staged whole
+
+// the pair / three-or-four run starting at sorted position i, keys r[] and
+// ids src[] in their current order: order it on the low bits (stable) and
+// write the levels of the pairs inside it
+__device__ __forceinline__ void order_run2(uint64_t a, uint64_t b, uint64_t i, const uint32_t *src, uint64_t *keys,
+                                           uint32_t *ids, uint8_t *__restrict__ delta)
 {
-  // the neighbouring keys are independent loads
-  const uint64_t k0 = keys[i];
-  const uint64_t km = i > 0 ? keys[i - 1] : ~k0;
-  const uint64_t k1 = i + 1 < nv ? keys[i + 1] : ~k0;
-  const uint64_t k2 = i + 2 < nv ? keys[i + 2] : ~k0;
-  const uint32_t hi = key_hi<SB>(k0);
-  if (key_hi<SB>(km) == hi) return;  // not the first of its run
-  if (key_hi<SB>(k1) != hi) return;  // a run of one
-  if (key_hi<SB>(k2) != hi) {        // a run of two
-    uint64_t a = k0, b = k1;
-    if (k0 > k1) {
-      const uint32_t ia = ids[i], ib = ids[i + 1];
-      keys[i] = k1; keys[i + 1] = k0;
-      ids[i] = ib; ids[i + 1] = ia;
-      a = k1; b = k0;
-    }
-    delta[i] = a != b ? key_level(a, b) : (uint8_t)63;  // equal: the midpoint of [i, i+2)
-    return;
+  if (a > b) {
+    const uint32_t ia = src[0], ib = src[1];
+    keys[i] = b; keys[i + 1] = a;
+    ids[i] = ib; ids[i + 1] = ia;
   }
-  const uint64_t k3 = i + 3 < nv ? keys[i + 3] : ~k0;
-  const uint64_t k4 = i + 4 < nv ? keys[i + 4] : ~k0;
-  if (key_hi<SB>(k4) != hi) {  // a run of three or four: kept in registers
-    const uint32_t size = key_hi<SB>(k3) == hi ? 4u : 3u;
-    uint64_t r[4] = {k0, k1, k2, size == 4 ? k3 : ~0ull};  // ~0: above every key, stays last
-    uint32_t d[4];
+  delta[i] = a != b ? key_level(a, b) : (uint8_t)63;  // equal: the midpoint of [i, i+2)
+}
+
+__device__ __forceinline__ void order_run34(uint64_t r[4], uint32_t size, uint64_t i, const uint32_t *src,
+                                            uint64_t *keys, uint32_t *ids, uint8_t *__restrict__ delta)
+{
+  if (size == 3) r[3] = ~0ull;  // above every key: stays last
+  uint32_t d[4] = {0u, 1u, 2u, 3u};
+  bool moved = false;
 #pragma unroll
-    for (int j = 0; j < 4; j++) d[j] = (uint32_t)j < size ? ids[i + j] : 0u;
-    bool moved = false;
+  for (int pass = 0; pass < 3; pass++)  // bubble sort: swaps on > only, so stable
 #pragma unroll
-    for (int pass = 0; pass < 3; pass++)  // bubble sort: swaps on > only, so stable
-#pragma unroll
-      for (int j = 0; j < 3; j++)
-        if (r[j] > r[j + 1]) {
-          const uint64_t t = r[j]; r[j] = r[j + 1]; r[j + 1] = t;
-          const uint32_t u = d[j]; d[j] = d[j + 1]; d[j + 1] = u;
-          moved = true;
-        }
-    if (moved) {
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        if ((uint32_t)j < size) {
-          keys[i + j] = r[j];
-          ids[i + j] = d[j];
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      if ((uint32_t)j + 1 >= size) break;
-      if (r[j] != r[j + 1]) {
-        delta[i + j] = key_level(r[j], r[j + 1]);
-      } else {
-        int e0 = j, e1 = j + 2;  // the run of keys equal to r[j] (constant indices only)
-#pragma unroll
-        for (int t = 2; t >= 0; t--)
-          if (t < j && e0 == t + 1 && r[t] == r[j]) e0 = t;
-#pragma unroll
-        for (int t = 2; t < 4; t++)
-          if (t >= j + 2 && e1 == t && (uint32_t)t < size && r[t] == r[j]) e1 = t + 1;
-        delta[i + j] = equal_run_level(i + e0, i + e1, (uint64_t)i + j + 1);
+    for (int j = 0; j < 3; j++)
+      if (r[j] > r[j + 1]) {
+        const uint64_t t = r[j]; r[j] = r[j + 1]; r[j + 1] = t;
+        const uint32_t u = d[j]; d[j] = d[j + 1]; d[j + 1] = u;
+        moved = true;
       }
-    }
-    return;
-  }
-  const uint32_t size = hi_run_end<SB>(keys, i, hi, nv) - i;
-  if (size > MB_THREAD_RUN) {
-    const uint32_t slotIdx = atomicAdd(&rs->count, 1u);
-    if (slotIdx < maxRuns) runs[slotIdx] = make_uint4(i, size, hi, 0);
-    else atomicOr(&rs->pad, 1u);  // cannot happen: maxRuns = nv / (MB_THREAD_RUN + 1) + 1
-    atomicAdd(&rs->elems, size);
-    atomicMax(&rs->maxSize, size);
-    return;
-  }
-  // whole keys (the top bits are equal inside the run) and ids
-  uint64_t kr[MB_THREAD_RUN];
-  uint32_t id[MB_THREAD_RUN];
-  bool sorted = true;
-  for (uint32_t j = 0; j < size; j++) {
-    kr[j] = keys[i + j];
-    id[j] = ids[i + j];
-    if (j && kr[j] < kr[j - 1]) sorted = false;
-  }
-  if (!sorted) {
-    for (uint32_t a = 1; a < size; a++) {  // insertion sort: stable
-      const uint64_t x = kr[a];
-      const uint32_t y = id[a];
-      uint32_t b = a;
-      while (b > 0 && kr[b - 1] > x) {
-        kr[b] = kr[b - 1];
-        id[b] = id[b - 1];
-        b--;
+  if (moved) {
+    uint32_t v[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) v[j] = (uint32_t)j < size ? src[d[j]] : 0u;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if ((uint32_t)j < size && d[j] != (uint32_t)j) {
+        keys[i + j] = r[j];
+        ids[i + j] = v[j];
       }
-      kr[b] = x;
-      id[b] = y;
-    }
-    for (uint32_t j = 0; j < size; j++) {
-      keys[i + j] = kr[j];
-      ids[i + j] = id[j];
-    }
   }
-  // levels of the pairs inside the run
-  for (uint32_t j = 0; j + 1 < size; j++) {
-    if (kr[j] != kr[j + 1]) {
-      delta[i + j] = key_level(kr[j], kr[j + 1]);
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    if ((uint32_t)j + 1 >= size) break;
+    if (r[j] != r[j + 1]) {
+      delta[i + j] = key_level(r[j], r[j + 1]);
     } else {
-      uint32_t e0 = j, e1 = j + 2;
-      while (e0 > 0 && kr[e0 - 1] == kr[j]) e0--;
-      while (e1 < size && kr[e1] == kr[j]) e1++;
-      delta[i + j] = equal_run_level(i + e0, i + e1, (uint64_t)i + j + 1);
+      int e0 = j, e1 = j + 2;  // the run of keys equal to r[j] (constant indices only)
+#pragma unroll
+      for (int t = 2; t >= 0; t--)
+        if (t < j && e0 == t + 1 && r[t] == r[j]) e0 = t;
+#pragma unroll
+      for (int t = 2; t < 4; t++)
+        if (t >= j + 2 && e1 == t && (uint32_t)t < size && r[t] == r[j]) e1 = t + 1;
+      delta[i + j] = equal_run_level(i + e0, i + e1, i + j + 1);
     }
   }
 }
 
-// Every sorted position: its agglomeration slot, and the split level of
-// the pair (i, i+1) when the two lie in different runs of equal top bits
-// (their highest differing bit is in the top bits, so the order inside the
-// runs does not change it).  Each warp covers FR_ITEMS * 32 consecutive
-// positions, collects the run starts among them in shared memory and then
-// hands one run to each lane, so the run work is not left to a few lanes
-// of a mostly idle warp.
-constexpr int FR_BLOCK = 256;
-constexpr int FR_ITEMS = 4;
+// a run of more than MB_THREAD_RUN prims starting at sorted position i: listed
+// for the segmented sort (its inner levels are written by k_delta after it)
 template <int SB>
-__global__ void __launch_bounds__(FR_BLOCK) k_fix_runs(uint64_t *keys, uint32_t *ids, const uint32_t *nvPtr,
+__device__ __forceinline__ void list_long_run(uint32_t i, uint32_t hi, uint32_t nv, const uint64_t *keys, RunStats *rs,
+                                              uint4 *runs, uint32_t maxRuns)
+{
+  const uint32_t size = hi_run_end<SB>(keys, i, hi, nv) - i;
+  const uint32_t slotIdx = atomicAdd(&rs->count, 1u);
+  if (slotIdx < maxRuns) runs[slotIdx] = make_uint4(i, size, hi, 0);
+  else atomicOr(&rs->pad, 1u);  // cannot happen: maxRuns = nv / (MB_THREAD_RUN + 1) + 1
+  atomicAdd(&rs->elems, size);
+  atomicMax(&rs->maxSize, size);
+}
+
+// 8 blocks per SM (32 registers): the kernel is latency-bound, and occupancy
+// pays more than the few spilled bytes cost
+template <int SB>
+__global__ void __launch_bounds__(FT_BLOCK, 8) k_fix_runs(uint64_t *keys, uint32_t *ids, const uint32_t *nvPtr,
                                                        uint8_t *__restrict__ delta, uint32_t *__restrict__ slot,
                                                        RunStats *rs, uint4 *runs, uint32_t maxRuns)
 {
-  __shared__ uint32_t sStarts[FR_BLOCK / 32][FR_ITEMS * 32];
+  __shared__ uint64_t sK[FT_TILE + FT_HALO + 1];  // [0]: position base-1, [1+j]: base+j
+  __shared__ uint16_t sR2[FT_TILE / 2], sR34[FT_TILE / 3 + 1], sRL[FT_TILE / 5 + 1];
+  __shared__ uint32_t sCnt[3];
+  __shared__ uint64_t sSorted[FT_BLOCK / 32][32];  // per warp: a run of 5..32 keys in order
   const uint32_t nv = *nvPtr;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint64_t warpBase = ((uint64_t)blockIdx.x * (FR_BLOCK / 32) + warp) * (FR_ITEMS * 32);
+  const uint64_t base = (uint64_t)blockIdx.x * FT_TILE;
+  if (base >= nv) return;
+  const uint32_t len = (uint32_t)min((uint64_t)FT_TILE, nv - base);
+  const uint32_t lenH = (uint32_t)min((uint64_t)(FT_TILE + FT_HALO), nv - base);  // staged positions
+  const int t = threadIdx.x, lane = t & 31;
   const uint32_t lt = (1u << lane) - 1u;
-  uint32_t numStarts = 0;
-#pragma unroll
-  for (int u = 0; u < FR_ITEMS; u++) {
-    const uint64_t i = warpBase + (uint64_t)u * 32 + lane;
-    bool start = false;
-    if (i < nv) {
-      slot[i] = SLOT_EMPTY;
-      const uint64_t k0 = keys[i];
-      const uint32_t hi = key_hi<SB>(k0);
-      const bool nextSame = i + 1 < nv && key_hi<SB>(keys[i + 1]) == hi;
-      if (i + 1 < nv && !nextSame) delta[i] = key_level(k0, keys[i + 1]);  // pair across two runs
-      start = nextSame && (i == 0 || key_hi<SB>(keys[i - 1]) != hi);
-    }
-    const uint32_t bal = __ballot_sync(0xffffffffu, start);
-    if (start) sStarts[warp][numStarts + __popc(bal & lt)] = (uint32_t)i;
-    numStarts += __popc(bal);
+
+  for (uint32_t j = t; j < lenH; j += FT_BLOCK) sK[j + 1] = keys[base + j];
+  if (t == 0) sK[0] = base > 0 ? keys[base - 1] : 0ull;
+  if (t < 3) sCnt[t] = 0u;
+  uint32_t *sl = slot + base;
+  if ((reinterpret_cast<uintptr_t>(sl) & 15u) == 0) {
+    const uint32_t n4 = len >> 2;
+    for (uint32_t j = t; j < n4; j += FT_BLOCK)
+      reinterpret_cast<uint4 *>(sl)[j] = make_uint4(SLOT_EMPTY, SLOT_EMPTY, SLOT_EMPTY, SLOT_EMPTY);
+    for (uint32_t j = (n4 << 2) + t; j < len; j += FT_BLOCK) sl[j] = SLOT_EMPTY;
+  } else {
+    for (uint32_t j = t; j < len; j += FT_BLOCK) sl[j] = SLOT_EMPTY;
   }
-  __syncwarp();
-  for (uint32_t k = lane; k < numStarts; k += 32)
-    fix_run_at<SB>(sStarts[warp][k], nv, keys, ids, delta, rs, runs, maxRuns);
+  __syncthreads();
+
+  // A. levels across runs; runs begun here, by size class
+#pragma unroll
+  for (int u = 0; u < FT_ITEMS; u++) {
+    const uint32_t j = u * FT_BLOCK + t;
+    int cls = -1;
+    if (j < len) {
+      const uint64_t k = sK[j + 1];
+      const uint32_t hi = key_hi<SB>(k);
+      const bool hasNext = j + 1 < lenH;
+      const uint64_t kn = sK[j + 2];
+      const bool nextSame = hasNext && key_hi<SB>(kn) == hi;
+      if (hasNext && !nextSame) delta[base + j] = key_level(k, kn);
+      const bool prevSame = (j > 0 || base > 0) && key_hi<SB>(sK[j]) == hi;
+      if (nextSame && !prevSame) {
+        uint32_t size = 2;
+        while (size < 5 && j + size < lenH && key_hi<SB>(sK[j + size + 1]) == hi) size++;
+        cls = size == 2 ? 0 : size < 5 ? 1 : 2;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const uint32_t m = __ballot_sync(0xffffffffu, cls == c);
+      if (m == 0) continue;
+      uint32_t at = 0;
+      if (lane == __ffs(m) - 1) at = atomicAdd(&sCnt[c], (uint32_t)__popc(m));
+      at = __shfl_sync(0xffffffffu, at, __ffs(m) - 1);
+      if (cls == c) {
+        uint16_t *list = c == 0 ? sR2 : c == 1 ? sR34 : sRL;
+        list[at + __popc(m & lt)] = (uint16_t)j;
+      }
+    }
+  }
+  __syncthreads();
+
+  // B. order the listed runs, one class at a time
+  const uint32_t n2 = sCnt[0], n34 = sCnt[1], nL = sCnt[2];
+  for (uint32_t r = t; r < n2; r += FT_BLOCK) {
+    const uint32_t j = sR2[r];
+    order_run2(sK[j + 1], sK[j + 2], base + j, ids + base + j, keys, ids, delta);
+  }
+  for (uint32_t r = t; r < n34; r += FT_BLOCK) {
+    const uint32_t j = sR34[r];
+    const uint32_t hi = key_hi<SB>(sK[j + 1]);
+    const uint32_t size = j + 3 < lenH && key_hi<SB>(sK[j + 4]) == hi ? 4u : 3u;
+    uint64_t rk[4] = {sK[j + 1], sK[j + 2], sK[j + 3], size == 4 ? sK[j + 4] : 0ull};
+    order_run34(rk, size, base + j, ids + base + j, keys, ids, delta);
+  }
+  // runs of 5..32 prims: one warp each, a lane per prim; longer ones are listed
+  const int warp = t >> 5;
+  uint64_t *scratch = sSorted[warp];
+  for (uint32_t r = warp; r < nL; r += FT_BLOCK / 32) {
+    const uint32_t j = sRL[r];
+    const uint32_t hi = key_hi<SB>(sK[j + 1]);
+    const uint32_t m = __ballot_sync(0xffffffffu, j + lane < lenH && key_hi<SB>(sK[j + lane + 1]) == hi);
+    if (m == 0xffffffffu && j + 32 < lenH && key_hi<SB>(sK[j + 33]) == hi) {
+      if (lane == 0) list_long_run<SB>((uint32_t)(base + j), hi, nv, keys, rs, runs, maxRuns);
+      continue;
+    }
+    const uint32_t size = m == 0xffffffffu ? 32u : (uint32_t)__ffs(~m) - 1u;
+    const bool in = (uint32_t)lane < size;
+    const uint64_t k = in ? sK[j + lane + 1] : ~0ull;
+    uint32_t rank = 0;
+    for (uint32_t q = 0; q < size; q++) {
+      const uint64_t x = __shfl_sync(0xffffffffu, k, (int)q);
+      rank += (x < k || (x == k && q < (uint32_t)lane)) ? 1u : 0u;
+    }
+    const uint64_t i0 = base + j;
+    if (__ballot_sync(0xffffffffu, in && rank != (uint32_t)lane)) {
+      const uint32_t id = in ? ids[i0 + lane] : 0u;
+      __syncwarp();
+      if (in && rank != (uint32_t)lane) {
+        keys[i0 + rank] = k;
+        ids[i0 + rank] = id;
+      }
+    }
+    if (in) scratch[rank] = k;
+    __syncwarp();
+    const uint64_t sk = in ? scratch[lane] : 0ull;
+    __syncwarp();
+    const uint64_t skPrev = __shfl_up_sync(0xffffffffu, sk, 1), skNext = __shfl_down_sync(0xffffffffu, sk, 1);
+    const uint32_t eqStart = __ballot_sync(0xffffffffu, in && (lane == 0 || sk != skPrev));
+    if ((uint32_t)lane + 1 < size) {
+      if (sk != skNext) {
+        delta[i0 + lane] = key_level(sk, skNext);
+      } else {  // the run of keys equal to sk: [e0, e1)
+        const uint32_t e0 = 31u - __clz(eqStart & ((2u << lane) - 1u));
+        const uint32_t above = eqStart & ~((2u << lane) - 1u);
+        const uint32_t e1 = above ? (uint32_t)__ffs(above) - 1u : size;
+        delta[i0 + lane] = equal_run_level(i0 + e0, i0 + e1, i0 + lane + 1);
+      }
+    }
+  }
 }
 
 __global__ void k_run_sizes(const uint4 *__restrict__ runs, uint32_t numRuns, uint32_t *__restrict__ sizes)
@@ -643,8 +705,7 @@ int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *
   BQ_CUDA(cudaMemsetAsync(rs, 0, sizeof(RunStats), al.s));
   {
     ProfScope ps("morton.runs", al.s);
-    k_fix_runs<SB><<<div_up(n, FR_BLOCK * FR_ITEMS), FR_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs,
-                                                                         maxRuns);
+    k_fix_runs<SB><<<div_up(n, FT_TILE), FT_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs, maxRuns);
   }
   RunStats h{};
   BQ_CUDA(cudaMemcpyAsync(&h, rs, sizeof(h), cudaMemcpyDeviceToHost, al.s));

@@ -95,6 +95,33 @@ def test_morton_4pass_matches_oracle(bq, oracle, dist):
     bvh.free()
 
 
+@pytest.mark.parametrize("seed", [0, 1])
+def test_morton_runs_across_tiles(bq, oracle, seed):
+    """Runs of equal top key bits of every length from 1 to 40 prims (an
+    8-bit-per-axis cell each, some points duplicated), so that runs of
+    every size begin, end and cross the run-ordering tiles (1024 sorted
+    positions) at every offset."""
+    rng = np.random.default_rng(100 + seed)
+    cells = rng.choice(256 ** 3, 6000, replace=False)
+    sizes = rng.integers(1, 41, len(cells))
+    cxyz = np.stack([cells % 256, (cells // 256) % 256, cells // 65536], 1).astype(np.float64)
+    pts = []
+    for c, k in zip(cxyz, sizes):
+        p = (c + 0.05 + 0.9 * rng.random((k, 3))) / 256.0
+        if k > 2 and rng.random() < 0.3:
+            p[1:k // 2 + 1] = p[0]  # identical points: equal full keys inside the run
+        pts.append(p)
+    p = np.concatenate(pts).astype(np.float32)
+    p = np.concatenate([p, np.float32([[0, 0, 0], [1, 1, 1]])])  # bounds: the unit cube
+    b = boxes_np(p[rng.permutation(len(p))])
+    bvh = bq.cuda.radixBuilder(torch.from_numpy(b).cuda())
+    gn, gp = bvh.to_host()
+    on, op = oracle.radix_build(b)
+    ok, msg = same_tree(oracle, gn, gp, on, op)
+    assert ok, msg
+    bvh.free()
+
+
 def test_morton_is_deterministic(bq):
     b = torch.from_numpy(_boxes("gmm", 300000)).cuda()
     a = bq.cuda.radixBuilder(b).to_host()
