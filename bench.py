@@ -342,14 +342,17 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
     # nearest other point of every data point (findClosest_exludeSelf)
     ms = ev_time(lambda: bq.points.findClosest_exludeSelf(bvh, tp, tp))
     comp["closest_point_exclude_self"] = {"ms": ms, "Mqueries_s": n / ms / 1e3, "queries": n}
-    # fixed-box queries: 1M boxes of half size 0.00585 (about 16 points each), count + scan + fill
+    # fixed-box queries: 1M boxes of half size 0.00585 (about 16 points each): one traversal into
+    # slab rows + scan + gather, and the two-pass form (count + scan + fill) beside it
     qb = box_queries(W, 1_000_000)
     qbt = torch.from_numpy(qb).cuda()
     ms = ev_time(lambda: bq.fixedBoxQuery.findPrims(bvh, boxes_t, qbt))
+    ms2 = ev_time(lambda: bq.fixedBoxQuery.findPrims(bvh, boxes_t, qbt, slabCap=0))
     off, _ = bq.fixedBoxQuery.findPrims(bvh, boxes_t, qbt)
     comp["box_query"] = {"ms": ms, "Mqueries_s": len(qb) / ms / 1e3, "queries": len(qb),
-                         "results": int(off[-1]), "half_size": BOX_HALF,
-                         "path": "fixedBoxQuery.findPrims: count kernel, cumsum, host read of the total, fill kernel"}
+                         "results": int(off[-1]), "half_size": BOX_HALF, "two_pass_ms": ms2,
+                         "path": "fixedBoxQuery.findPrims: slab kernel (one traversal, 64 ids per query kept), "
+                                 "cumsum, host read of the total, gather kernel (longer queries traversed again)"}
     del qbt, off
     bvh.free()
     # triangle-mesh distance forward + adjoint (icosphere, 1,310,720 triangles, 4M queries)

@@ -109,6 +109,10 @@ _SIGS = {
     "bq_box_query_count_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _P, ctypes.POINTER(bq_allocator), _P],
     "bq_box_query_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _P, ctypes.c_uint64, _P, ctypes.POINTER(bq_allocator),
                         _P],
+    "bq_box_query_slab_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _U, _P, _P, _P, ctypes.POINTER(bq_allocator),
+                             _P],
+    "bq_box_query_gather_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _U, _P, _P, _P, _P, ctypes.c_uint64, _P,
+                               ctypes.POINTER(bq_allocator), _P],
     "bq_build_wide_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, _P, _U, ctypes.POINTER(bq_build_config),
                          ctypes.POINTER(bq_allocator), _P],
     "bq_collapse_wide_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, ctypes.POINTER(bq_bvh3f), ctypes.POINTER(bq_allocator),
@@ -120,6 +124,10 @@ _SIGS = {
                                    _P],
     "bq_wide_box_query_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, _P, _P, _U, _P, ctypes.c_uint64, _P,
                              ctypes.POINTER(bq_allocator), _P],
+    "bq_wide_box_query_slab_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, _P, _P, _U, _U, _P, _P, _P,
+                                  ctypes.POINTER(bq_allocator), _P],
+    "bq_wide_box_query_gather_f3": [ctypes.POINTER(bq_wide_bvh3f), _I, _P, _P, _U, _U, _P, _P, _P, _P,
+                                    ctypes.c_uint64, _P, ctypes.POINTER(bq_allocator), _P],
     "bq_knn_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _I, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
                   ctypes.POINTER(bq_allocator), _P],
     "bq_tri_closest_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _P, _U, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
@@ -501,27 +509,62 @@ class fixedBoxQuery:
         return counts
 
     @staticmethod
-    def findPrims(bvh, boxes, queryBoxes):
-        """Both passes: returns (offsets int64 (nq+1,), ids int32); the prims of
-        query q are ids[offsets[q]:offsets[q+1]] in the reference's visiting
-        order (forEachLeaf: depth first, first child first)."""
+    def findPrims(bvh, boxes, queryBoxes, slabCap=None):
+        """Returns (offsets int64 (nq+1,), ids int32); the prims of query q are
+        ids[offsets[q]:offsets[q+1]] in the reference's visiting order
+        (forEachLeaf: depth first, first child first).
+
+        One traversal (bq_box_query_slab_f3, then bq_box_query_gather_f3): the
+        first slabCap ids of every query are kept in a slab during it
+        (default: up to 64 per query within 256 MB) and only queries with
+        more are traversed again.  slabCap=0 runs the two-pass form
+        (bq_box_query_count_f3, then bq_box_query_f3).  Same result."""
         boxes, queryBoxes = _as_boxes(boxes), _as_boxes(queryBoxes)
         nq = queryBoxes.shape[0]
-        counts = fixedBoxQuery.count(bvh, boxes, queryBoxes)
-        offsets = torch.zeros(nq + 1, dtype=torch.int64, device=queryBoxes.device)
+        dev = queryBoxes.device
+        wide = isinstance(bvh, WideBVH)
+        if slabCap is None:
+            slabCap = max(4, min(64, (1 << 26) // max(nq, 1)))
+        if slabCap < 0:
+            raise BQError(1, "slabCap must be >= 0")
+        if slabCap == 0:
+            counts = fixedBoxQuery.count(bvh, boxes, queryBoxes)
+        else:
+            slab = torch.empty(max(nq * slabCap, 1), dtype=torch.int32, device=dev)
+            counts = torch.empty(max(nq, 1), dtype=torch.int32, device=dev)
+            ovf = torch.empty(nq + 1, dtype=torch.int32, device=dev)
+            if wide:
+                _check(_lib.bq_wide_box_query_slab_f3(ctypes.byref(bvh.c), bvh.width, _ptr(boxes), _ptr(queryBoxes),
+                                                      nq, slabCap, _ptr(slab), _ptr(counts), _ptr(ovf),
+                                                      ctypes.byref(bvh.allocator.c), _stream()))
+            else:
+                _check(_lib.bq_box_query_slab_f3(ctypes.byref(bvh.c), _ptr(boxes), _ptr(queryBoxes), nq, slabCap,
+                                                 _ptr(slab), _ptr(counts), _ptr(ovf), ctypes.byref(bvh.allocator.c),
+                                                 _stream()))
+            counts = counts[:nq]
+        offsets = torch.zeros(nq + 1, dtype=torch.int64, device=dev)
         torch.cumsum(counts.to(torch.int64), 0, out=offsets[1:])
         total = int(offsets[-1].item())
         if total >= 1 << 32:
             raise BQError(1, "box query results exceed 2^32 entries")
-        ids = torch.empty(max(total, 1), dtype=torch.int32, device=queryBoxes.device)
+        ids = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
         off32 = offsets[:-1].to(torch.int32).contiguous()
-        if isinstance(bvh, WideBVH):
-            _check(_lib.bq_wide_box_query_f3(ctypes.byref(bvh.c), bvh.width, _ptr(boxes), _ptr(queryBoxes), nq,
-                                             _ptr(off32), total, _ptr(ids), ctypes.byref(bvh.allocator.c),
-                                             _stream()))
-            return offsets, ids[:total]
-        _check(_lib.bq_box_query_f3(ctypes.byref(bvh.c), _ptr(boxes), _ptr(queryBoxes), nq, _ptr(off32), total,
-                                    _ptr(ids), ctypes.byref(bvh.allocator.c), _stream()))
+        if slabCap == 0:
+            if wide:
+                _check(_lib.bq_wide_box_query_f3(ctypes.byref(bvh.c), bvh.width, _ptr(boxes), _ptr(queryBoxes), nq,
+                                                 _ptr(off32), total, _ptr(ids), ctypes.byref(bvh.allocator.c),
+                                                 _stream()))
+            else:
+                _check(_lib.bq_box_query_f3(ctypes.byref(bvh.c), _ptr(boxes), _ptr(queryBoxes), nq, _ptr(off32),
+                                            total, _ptr(ids), ctypes.byref(bvh.allocator.c), _stream()))
+        elif wide:
+            _check(_lib.bq_wide_box_query_gather_f3(ctypes.byref(bvh.c), bvh.width, _ptr(boxes), _ptr(queryBoxes), nq,
+                                                    slabCap, _ptr(slab), _ptr(counts), _ptr(ovf), _ptr(off32), total,
+                                                    _ptr(ids), ctypes.byref(bvh.allocator.c), _stream()))
+        else:
+            _check(_lib.bq_box_query_gather_f3(ctypes.byref(bvh.c), _ptr(boxes), _ptr(queryBoxes), nq, slabCap,
+                                               _ptr(slab), _ptr(counts), _ptr(ovf), _ptr(off32), total, _ptr(ids),
+                                               ctypes.byref(bvh.allocator.c), _stream()))
         return offsets, ids[:total]
 
 

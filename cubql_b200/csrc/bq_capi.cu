@@ -17,6 +17,16 @@ int wide_box_query_count(const bq_wide_bvh3f *bvh, int W, const bq_box3f *boxes,
                          uint32_t nq, uint32_t *counts, Alloc &al);
 int wide_box_query_fill(const bq_wide_bvh3f *bvh, int W, const bq_box3f *boxes, const bq_box3f *queryBoxes,
                         uint32_t nq, const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al);
+int box_query_slab(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t nq,
+                   uint32_t slabCap, int32_t *slab, uint32_t *counts, uint32_t *ovf, Alloc &al);
+int box_query_gather(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t nq,
+                     uint32_t slabCap, const int32_t *slab, const uint32_t *counts, const uint32_t *ovf,
+                     const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al);
+int wide_box_query_slab(const bq_wide_bvh3f *bvh, int W, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                        uint32_t nq, uint32_t slabCap, int32_t *slab, uint32_t *counts, uint32_t *ovf, Alloc &al);
+int wide_box_query_gather(const bq_wide_bvh3f *bvh, int W, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                          uint32_t nq, uint32_t slabCap, const int32_t *slab, const uint32_t *counts,
+                          const uint32_t *ovf, const uint32_t *offsets, uint64_t capacity, int32_t *ids, Alloc &al);
 int collapse_wide(const bq_bvh3f *bin, int W, bq_wide_bvh3f *out, bool copyPrims, Alloc &al);
 int build_sah(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
 int build_elh(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
@@ -240,6 +250,32 @@ int bq_wide_box_query_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *bo
   return wide_box_query_fill(bvh, width, boxes, queryBoxes, numQueries, offsets, capacity, ids, al);
 }
 
+int bq_wide_box_query_slab_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes,
+                              const bq_box3f *queryBoxes, uint32_t numQueries, uint32_t slabCap, int32_t *slab,
+                              uint32_t *counts, uint32_t *overflow, const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_wide(bvh, width));
+  if (numQueries && (!queryBoxes || !counts || !overflow || (slabCap && !slab) || (bvh->numNodes && !boxes)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return wide_box_query_slab(bvh, width, boxes, queryBoxes, numQueries, slabCap, slab, counts, overflow, al);
+}
+
+int bq_wide_box_query_gather_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes,
+                                const bq_box3f *queryBoxes, uint32_t numQueries, uint32_t slabCap,
+                                const int32_t *slab, const uint32_t *counts, const uint32_t *overflow,
+                                const uint32_t *offsets, uint64_t capacity, int32_t *ids, const bq_allocator *alloc,
+                                bq_stream_t stream)
+{
+  BQ_TRY(check_wide(bvh, width));
+  if (numQueries && (!queryBoxes || !counts || !overflow || !offsets || (slabCap && !slab) ||
+                     (bvh->numNodes && !boxes) || (capacity && !ids)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return wide_box_query_gather(bvh, width, boxes, queryBoxes, numQueries, slabCap, slab, counts, overflow, offsets,
+                               capacity, ids, al);
+}
+
 int bq_closest_point_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries,
                         float maxSqrDist, const bq_query_config *qcfg, int32_t *ids, float *sqrDist,
                         const bq_allocator *alloc, bq_stream_t stream)
@@ -292,6 +328,31 @@ int bq_box_query_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *
     return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
   Alloc al = make_alloc(alloc, stream);
   return box_query_fill(bvh, boxes, queryBoxes, numQueries, offsets, capacity, ids, al);
+}
+
+int bq_box_query_slab_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                         uint32_t numQueries, uint32_t slabCap, int32_t *slab, uint32_t *counts, uint32_t *overflow,
+                         const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (numQueries && (!queryBoxes || !counts || !overflow || (slabCap && !slab) || (bvh->numNodes && !boxes)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return box_query_slab(bvh, boxes, queryBoxes, numQueries, slabCap, slab, counts, overflow, al);
+}
+
+int bq_box_query_gather_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                           uint32_t numQueries, uint32_t slabCap, const int32_t *slab, const uint32_t *counts,
+                           const uint32_t *overflow, const uint32_t *offsets, uint64_t capacity, int32_t *ids,
+                           const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (numQueries && (!queryBoxes || !counts || !overflow || !offsets || (slabCap && !slab) ||
+                     (bvh->numNodes && !boxes) || (capacity && !ids)))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return box_query_gather(bvh, boxes, queryBoxes, numQueries, slabCap, slab, counts, overflow, offsets, capacity, ids,
+                          al);
 }
 
 int bq_knn_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries, int k,

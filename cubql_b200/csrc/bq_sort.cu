@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
     sGlobalBase[d] = gStart + excl - sTileStart[d];
   }
   __syncthreads();
-  if (sBad) return;  // a wait timed out: leave the output untouched, report
+  if (sBad) return;  // a wait timed out: k_sort_repair overwrites the output, the caller reports
 
   // 4. tile-local positions; then keys and values through shared memory
 #pragma unroll
@@ -289,6 +289,23 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
   }
 }
 
+// After the last pass.  A tile whose look-back gave up leaves its part of
+// that pass's output unwritten, so if any pass gave up (or scattered out of
+// range) the final output is overwritten with keys 0 and values 0..n-1:
+// the caller reports the error, and whatever runs on the stream before it
+// looks sees only in-range values.  Otherwise every thread returns at once.
+template <typename KeyT>
+__global__ void k_sort_repair(KeyT *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t nHost,
+                              const uint32_t *nDev, const uint32_t *abort, const uint32_t *err)
+{
+  if (ld_volatile(abort) == 0 && (!err || (ld_volatile(err) & DEV_ERR_RANGE) == 0)) return;
+  const uint32_t n = nDev ? *nDev : nHost;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    keys[i] = (KeyT)0;
+    vals[i] = (uint32_t)i;
+  }
+}
+
 template <typename KeyT>
 int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit, int endBit,
                   const uint32_t *preHist, int *outSel, uint32_t *dErr, Alloc &al)
@@ -332,6 +349,9 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
     BQ_CUDA(cudaGetLastError());
     sel ^= 1;
   }
+  k_sort_repair<KeyT><<<num_sms(), 256, 0, al.s>>>(keys[sel], vals[sel], nMax, nDev, ctl + statusWords + numPasses,
+                                                   dErr);
+  BQ_CUDA(cudaGetLastError());
   *outSel = sel;
   return BQ_OK;
 }

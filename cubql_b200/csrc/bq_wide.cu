@@ -264,24 +264,6 @@ __global__ void k_wide_closest_deep(const Node *__restrict__ slots, const uint32
   }
 }
 
-// union of the root's valid slots -> 6 floats (lower xyz, upper xyz)
-template <int W>
-__global__ void k_wide_root_box(const Node *__restrict__ slots, float *__restrict__ box)
-{
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (int c = 0; c < W; c++) {
-    const Node sl = ldg_node(slots + c);
-    if (!wslot_valid(node_admin(sl))) continue;
-    lo[0] = fminf(lo[0], sl.a.x); lo[1] = fminf(lo[1], sl.a.y); lo[2] = fminf(lo[2], sl.a.z);
-    hi[0] = fmaxf(hi[0], sl.a.w); hi[1] = fmaxf(hi[1], sl.b.x); hi[2] = fmaxf(hi[2], sl.b.y);
-  }
-  for (int d = 0; d < 3; d++) {
-    box[d] = lo[d];
-    box[3 + d] = hi[d];
-  }
-}
-
 template <int W, int TIE, int STACK>
 void launch_wide_cp(const bq_wide_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
                     int block, int32_t *ids, float *d, QueryScratch &qs, cudaStream_t s)

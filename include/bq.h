@@ -267,6 +267,25 @@ int bq_box_query_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *
                     const uint32_t *offsets, uint64_t capacity, int32_t *ids, const bq_allocator *alloc,
                     bq_stream_t stream);
 
+/* Fixed-box query in one traversal (same results as the two calls above):
+   the first slabCap ids of query q go to slab[q*slabCap ..], all its count
+   to counts[q]; the queries with more than slabCap prims are listed in
+   overflow[1 ..] (overflow[0] = how many; the array holds numQueries + 1
+   entries).  Synchronises the stream. */
+int bq_box_query_slab_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                         uint32_t numQueries, uint32_t slabCap, int32_t *slab, uint32_t *counts, uint32_t *overflow,
+                         const bq_allocator *alloc, bq_stream_t stream);
+
+/* Second step of the one-traversal query: the ids of query q go to
+   ids[offsets[q] .. offsets[q] + counts[q]) (offsets: the exclusive prefix
+   sum of counts; capacity: the length of ids) -- copied from its slab row,
+   or, for the listed queries, by traversing again.  Synchronises the
+   stream. */
+int bq_box_query_gather_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes,
+                           uint32_t numQueries, uint32_t slabCap, const int32_t *slab, const uint32_t *counts,
+                           const uint32_t *overflow, const uint32_t *offsets, uint64_t capacity, int32_t *ids,
+                           const bq_allocator *alloc, bq_stream_t stream);
+
 /* Closest data point per query over a wide tree.  Replaces a user kernel
    calling cuBQL::points::findClosest(WideBVH<float,3,W>, ...)
    (cuBQL/queries/points/findClosest.h:365-386, traversal
@@ -286,6 +305,16 @@ int bq_wide_box_query_count_f3(const bq_wide_bvh3f *bvh, int width, const bq_box
 int bq_wide_box_query_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes, const bq_box3f *queryBoxes,
                          uint32_t numQueries, const uint32_t *offsets, uint64_t capacity, int32_t *ids,
                          const bq_allocator *alloc, bq_stream_t stream);
+/* The one-traversal form over a wide tree: as bq_box_query_slab_f3 /
+   bq_box_query_gather_f3. */
+int bq_wide_box_query_slab_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes,
+                              const bq_box3f *queryBoxes, uint32_t numQueries, uint32_t slabCap, int32_t *slab,
+                              uint32_t *counts, uint32_t *overflow, const bq_allocator *alloc, bq_stream_t stream);
+int bq_wide_box_query_gather_f3(const bq_wide_bvh3f *bvh, int width, const bq_box3f *boxes,
+                                const bq_box3f *queryBoxes, uint32_t numQueries, uint32_t slabCap,
+                                const int32_t *slab, const uint32_t *counts, const uint32_t *overflow,
+                                const uint32_t *offsets, uint64_t capacity, int32_t *ids, const bq_allocator *alloc,
+                                bq_stream_t stream);
 
 /* ---------------------------------------------------------------- */
 /* binary-dump files (host only, no GPU)                              */

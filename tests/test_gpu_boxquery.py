@@ -1,4 +1,5 @@
-"""Fixed-box queries on the GPU (bq_box_query_count_f3 / bq_box_query_f3).
+"""Fixed-box queries on the GPU (bq_box_query_count_f3 / bq_box_query_f3,
+and the one-traversal bq_box_query_slab_f3 / bq_box_query_gather_f3).
 
 Bit-exact, visiting order included, against (a) the oracle's restatement
 of fixedBoxQuery::forEachPrim with a per-prim box test and (b) the
@@ -68,6 +69,26 @@ def test_box_query_matches_reference_kernel(bq, oracle, ref_gpu, kind):
     roff, rids = ref_gpu.box_query(n, pr, boxes, q)
     assert np.array_equal(off.cpu().numpy(), roff)
     assert np.array_equal(ids.cpu().numpy(), rids)
+
+
+@pytest.mark.parametrize("width", [0, 4, 8])
+@pytest.mark.parametrize("cap", [0, 1, 4, 17, None])
+def test_box_query_slab_capacities(bq, oracle, width, cap):
+    """The one-traversal form (slab rows of `cap` ids, overflowing queries
+    traversed again) equals the two-pass form (cap 0) and the oracle, for
+    every row size: none, some or all of the queries overflow."""
+    boxes, q = _boxes("extents", 40000), _queries(4000, seed=21)
+    bvh = _build(bq, "morton", boxes, 8)
+    n, pr = bvh.to_host()
+    t = bvh if width == 0 else bq.collapse(bvh, width)
+    off, ids = bq.fixedBoxQuery.findPrims(t, torch.from_numpy(boxes).cuda(), torch.from_numpy(q).cuda(), slabCap=cap)
+    if width == 0:
+        ooff, oids = oracle.box_query(n, pr, boxes, q)
+    else:
+        ws, wp = t.to_host()
+        ooff, oids = oracle.wide_box_query(ws, width, wp, boxes, q)
+    assert np.array_equal(off.cpu().numpy(), ooff)
+    assert np.array_equal(ids.cpu().numpy(), oids)
 
 
 def test_box_query_sets_match_brute_force(bq):
