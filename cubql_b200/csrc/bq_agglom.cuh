@@ -10,7 +10,7 @@
 // first node, the block's second node unused.
 //
 // Two kernels:
-//   k_agg_local   one CTA per chunk of AGG_CHUNK (256) sorted prims, whose
+//   k_agg_local   one CTA per chunk of AGG_CHUNK (128) sorted prims, whose
 //                 split levels are staged in shared memory.  Threads
 //                 start at their leaf and climb; the first child to reach
 //                 a split parks its range end and box in shared memory and
@@ -68,10 +68,7 @@ __device__ __forceinline__ uint32_t run_end(const uint64_t *__restrict__ keys, u
   return lo;
 }
 
-#ifndef BQ_AGG_CHUNK
-#define BQ_AGG_CHUNK 256
-#endif
-constexpr int AGG_CHUNK = BQ_AGG_CHUNK;  // prims per CTA of the local phase
+constexpr int AGG_CHUNK = 128;  // prims per CTA of the local phase
 constexpr uint32_t AGG_EMPTY = 0xffffffffu;
 
 // prim range of position i: [0, nv) or the cloud containing i
@@ -124,7 +121,7 @@ template <bool SEG, typename LevT>
 __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
 {
   __shared__ uint32_t sSlot[AGG_CHUNK + 1];
-  __shared__ AggBox sBox[AGG_CHUNK + 1][2];
+  __shared__ float4 sBox[AGG_CHUNK + 1][2][2];  // a box as two 16-byte words: lx ly lz hx | hy hz - -
   __shared__ LevT sLev[AGG_CHUNK + 2];  // delta[c0 - 1 .. c0 + AGG_CHUNK]
   const uint32_t nv = *a.nvPtr;
   const uint32_t c0 = blockIdx.x * AGG_CHUNK;
@@ -165,7 +162,8 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
         break;
       }
       const uint32_t js = s - c0;
-      sBox[js][side] = box;
+      sBox[js][side][0] = make_float4(box.lx, box.ly, box.lz, box.hx);
+      sBox[js][side][1] = make_float4(box.hy, box.hz, 0.f, 0.f);
       // block-scope release/acquire: the box is visible to the sibling that
       // sees this exchange, and this thread sees the sibling's box
       cuda::atomic_ref<uint32_t, cuda::thread_scope_block> slotRef(sSlot[js]);
@@ -173,7 +171,8 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
       // the node itself is read only by the global phase (a later launch)
       a.nodes[2ull * s + side] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
       if (other == AGG_EMPTY) break;  // parked; the sibling (here or in the global phase) carries on
-      const AggBox sib = sBox[js][side ^ 1];
+      const float4 s0 = sBox[js][side ^ 1][0], s1 = sBox[js][side ^ 1][1];
+      const AggBox sib{s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};
       box = leftChild ? agg_union(box, sib) : agg_union(sib, box);
       if (leftChild) r = other; else l = other;
       if (a.ranges) a.ranges[s] = make_uint2(l, r);

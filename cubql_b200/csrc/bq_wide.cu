@@ -158,6 +158,87 @@ constexpr uint64_t WKEY_NONE = ~0ull;
 constexpr uint32_t WNODE_NONE = 0xFFFFFFFFu;
 constexpr uint32_t WLEAF_BIT = 0x80000000u;
 
+__device__ __forceinline__ void cex(uint64_t &a, uint64_t &b)
+{
+  const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+  a = lo;
+  b = hi;
+}
+
+// ascending sort of W unique keys: 1, 5 and 19 compare-exchanges (Batcher's
+// odd-even merge for 8)
+template <int W>
+__device__ __forceinline__ void sort_keys(uint64_t v[W])
+{
+  if constexpr (W == 2) {
+    cex(v[0], v[1]);
+  } else if constexpr (W == 4) {
+    cex(v[0], v[1]); cex(v[2], v[3]);
+    cex(v[0], v[2]); cex(v[1], v[3]);
+    cex(v[1], v[2]);
+  } else {
+    static_assert(W == 8, "width 2, 4 or 8");
+    cex(v[0], v[1]); cex(v[2], v[3]); cex(v[4], v[5]); cex(v[6], v[7]);
+    cex(v[0], v[2]); cex(v[1], v[3]); cex(v[4], v[6]); cex(v[5], v[7]);
+    cex(v[1], v[2]); cex(v[5], v[6]);
+    cex(v[0], v[4]); cex(v[1], v[5]); cex(v[2], v[6]); cex(v[3], v[7]);
+    cex(v[2], v[4]); cex(v[3], v[5]);
+    cex(v[1], v[2]); cex(v[3], v[4]); cex(v[5], v[6]);
+  }
+}
+
+// Closest-point traversal of a WideBVH for the lowest-id tie rule, whose
+// answer does not depend on the visiting order: leaf slots inside the
+// (slack-widened) cull radius are processed as they are met, the nearest
+// inner child is descended and the other inner children are pushed
+// unsorted; popped entries beyond the shrunken radius are skipped.  Stack entries are
+// (distance bits << 32 | wide node).  Returns false on stack overflow.
+template <int W, typename Stack, typename Leaf>
+__device__ __forceinline__ bool wide_traverse_lowest(const Node *__restrict__ slots, float qx, float qy, float qz,
+                                                     float cull, Stack &st, Leaf &leaf)
+{
+  uint32_t nodeID = 0;
+  while (true) {
+    const Node *nd = slots + (size_t)nodeID * W;
+    float cs = lowest_slack(cull);
+    float nearD = INFINITY;
+    uint32_t nearN = WNODE_NONE;
+#pragma unroll
+    for (int c = 0; c < W; c++) {
+      const Node sl = ldg_node(nd + c);
+      const uint64_t word = node_admin(sl);
+      if (!wslot_valid(word)) continue;
+      const float d = sqr_pbox(qx, qy, qz, sl.a.x, sl.a.y, sl.a.z, sl.a.w, sl.b.x, sl.b.y);
+      if (d > cs) continue;
+      if (wslot_count(word)) {  // a leaf: at once, so the radius shrinks before the next slots
+        cull = fminf(cull, leaf(wslot_offset(word), wslot_count(word)));
+        cs = lowest_slack(cull);
+        continue;
+      }
+      const uint32_t child = (uint32_t)wslot_offset(word);
+      if (d < nearD) {
+        if (nearN != WNODE_NONE && !st.push(((uint64_t)__float_as_uint(nearD) << 32) | nearN)) return false;
+        nearD = d;
+        nearN = child;
+      } else if (!st.push(((uint64_t)__float_as_uint(d) << 32) | child)) {
+        return false;
+      }
+    }
+    if (nearN != WNODE_NONE && !(nearD > lowest_slack(cull))) {
+      nodeID = nearN;
+      continue;
+    }
+    while (true) {
+      if (st.empty()) return true;
+      const uint64_t tos = st.pop();
+      if (__uint_as_float((uint32_t)(tos >> 32)) <= lowest_slack(cull)) {
+        nodeID = (uint32_t)tos;
+        break;
+      }
+    }
+  }
+}
+
 // shrinkingRadiusQuery::forEachLeaf over a WideBVH (:553-636).  Leaf
 // functor as in bq_traverse.cuh.  Returns false on stack overflow.
 template <int W, int TIE, typename Stack, typename Leaf>
@@ -192,16 +273,10 @@ __device__ __forceinline__ bool wide_traverse(const Node *__restrict__ slots, fl
           }
         }
       }
-      // sort(ChildOrder<W>) (:525-538): the same exchange network
-#pragma unroll
-      for (int i = W - 1; i > 0; --i) {
-#pragma unroll
-        for (int j = 0; j < i; j++) {
-          const uint64_t c0 = v[j], c1 = v[j + 1];
-          v[j] = c0 < c1 ? c0 : c1;
-          v[j + 1] = c0 < c1 ? c1 : c0;
-        }
-      }
+      // sort(ChildOrder<W>) (:525-538).  The keys are unique (the payload
+      // differs per slot), so any sorting network gives the reference's
+      // exchange-network order; these are the shortest ones.
+      sort_keys<W>(v);
 #pragma unroll
       for (int c = W - 1; c > 0; --c)
         if (v[c] != WKEY_NONE && !st.push(v[c])) return false;
@@ -222,7 +297,11 @@ __device__ __forceinline__ bool run_wide_cp(const Node *slots, const uint32_t *p
 {
   const float *q = queries + 3ull * qi;
   CPLeaf<TIE> leaf{primIDs, points, __ldg(q), __ldg(q + 1), __ldg(q + 2), maxSqr, -1, -1, 0};
-  if (!wide_traverse<W, TIE>(slots, leaf.qx, leaf.qy, leaf.qz, maxSqr, st, leaf)) return false;
+  if constexpr (TIE == TIE_LOWEST) {
+    if (!wide_traverse_lowest<W>(slots, leaf.qx, leaf.qy, leaf.qz, maxSqr, st, leaf)) return false;
+  } else {
+    if (!wide_traverse<W, TIE>(slots, leaf.qx, leaf.qy, leaf.qz, maxSqr, st, leaf)) return false;
+  }
   outIds[qi] = leaf.id;
   outD[qi] = leaf.id >= 0 ? leaf.best : INFINITY;
   return true;
