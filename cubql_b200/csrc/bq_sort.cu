@@ -349,8 +349,11 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
     BQ_CUDA(cudaGetLastError());
     sel ^= 1;
   }
-  k_sort_repair<KeyT><<<num_sms(), 256, 0, al.s>>>(keys[sel], vals[sel], nMax, nDev, ctl + statusWords + numPasses,
-                                                   dErr);
+  {
+    ProfScope ps("sort.repair", al.s);
+    k_sort_repair<KeyT><<<num_sms(), 256, 0, al.s>>>(keys[sel], vals[sel], nMax, nDev, ctl + statusWords + numPasses,
+                                                     dErr);
+  }
   BQ_CUDA(cudaGetLastError());
   *outSel = sel;
   return BQ_OK;
