@@ -19,9 +19,10 @@
 //     stays unused, as in the reference);
 //   * nodes with more than warpMax prims (256..4096, chosen from the prim
 //     count) are split level by level over the whole GPU in tiles of
-//     SM_TILE prims: k_sm_tiles + one scan (tile
-//     offsets), k_sm_count (right-side count per tile), one scan,
-//     k_sm_children, k_sm_scatter (stable scatter that also reduces the
+//     SM_TILE prims: k_sm_tiles + one scan (tile offsets; one block,
+//     k_sm_tiles_scan, up to SM_FUSED_MAX nodes), k_sm_count (right-side
+//     count per tile), one scan + k_sm_children (one block,
+//     k_sm_scan_children), k_sm_scatter (stable scatter that also reduces the
 //     children's centroid bounds per tile and merges them with one
 //     atomicMin/Max per tile -- min/max is order-independent, so the result
 //     is deterministic), k_sm_classify (children to the next level's list or
@@ -66,6 +67,8 @@ constexpr int SMW_BLOCK = 128;          // warp-phase kernel
 constexpr int SMW_WARPS = SMW_BLOCK / 32;
 constexpr int SMW_STACK = 24;           // >= log2(SM_WARP_MAX) + 1
 constexpr int SM_LEVELS_PER_CHECK = 2;  // global levels between two host looks at the counters
+constexpr int SM_SCAN_THREADS = 1024;   // one-block scans of a level's node and tile arrays
+constexpr uint32_t SM_FUSED_MAX = 56u * 1024u;  // longest array such a scan keeps in shared memory
 
 // A node still to be split: prim range [b, e) in buffer `parity`, its slot,
 // and its prims' centroid bounds (encoded, see enc_f).
@@ -251,7 +254,70 @@ __global__ void k_sm_tiles(const SmNode *__restrict__ nodes, SmCtl *ctl, int cur
   tileCount[k] = (nodes[k].e - nodes[k].b + SM_TILE - 1) / SM_TILE;
 }
 
-// grid: maxTiles blocks; blocks past the level's tile count leave at once
+// Exclusive scan of s[0 .. L) in place by one block of SM_SCAN_THREADS
+// threads (each a contiguous segment); returns the total.  sWarp: 33 words.
+__device__ uint32_t block_scan_smem(uint32_t *s, uint32_t L, uint32_t *sWarp)
+{
+  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint32_t per = (L + SM_SCAN_THREADS - 1) / SM_SCAN_THREADS;
+  const uint32_t b = min(t * per, L), e = min(b + per, L);
+  uint32_t sum = 0;
+  for (uint32_t i = b; i < e; i++) sum += s[i];
+  uint32_t x = sum;  // inclusive scan over the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if ((int)lane >= o) x += y;
+  }
+  if (lane == 31) sWarp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = sWarp[lane];
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+      if ((int)lane >= o) wi += y;
+    }
+    sWarp[lane] = wi - w;
+    if (lane == 31) sWarp[32] = wi;
+  }
+  __syncthreads();
+  uint32_t run = sWarp[warp] + x - sum;
+  for (uint32_t i = b; i < e; i++) {
+    const uint32_t v = s[i];
+    s[i] = run;
+    run += v;
+  }
+  const uint32_t total = sWarp[32];
+  __syncthreads();
+  return total;
+}
+
+// k_sm_tiles and the scan of its counts in one block (the level's big
+// nodes, at most cap <= SM_FUSED_MAX, counted in shared memory)
+__global__ void __launch_bounds__(SM_SCAN_THREADS) k_sm_tiles_scan(const SmNode *__restrict__ nodes, SmCtl *ctl,
+                                                                   int cur, uint32_t cap, uint32_t maxTiles,
+                                                                   uint32_t *__restrict__ first)
+{
+  extern __shared__ uint32_t sVal[];  // cap entries
+  __shared__ uint32_t sWarp[33];
+  uint32_t K = ctl->bigCount[cur];
+  if (K > cap) {
+    if (threadIdx.x == 0) atomicOr(&ctl->err, DEV_ERR_RANGE);
+    K = cap;
+  }
+  for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) sVal[k] = (nodes[k].e - nodes[k].b + SM_TILE - 1) / SM_TILE;
+  __syncthreads();
+  const uint32_t T = block_scan_smem(sVal, K, sWarp);
+  for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) first[k] = sVal[k];
+  if (threadIdx.x == 0) {
+    if (T >= maxTiles) atomicOr(&ctl->err, DEV_ERR_RANGE);
+    ctl->numTiles = min(T, maxTiles - 1);
+  }
+}
+
+// right-side count per tile; the blocks walk the level's tiles
 __global__ void __launch_bounds__(SM_BLOCK) k_sm_count(const SmNode *__restrict__ nodes,
                                                        const uint32_t *__restrict__ first, SmCtl *ctl, int cur,
                                                        uint32_t maxTiles, const float4 *__restrict__ buf0,
@@ -264,21 +330,23 @@ __global__ void __launch_bounds__(SM_BLOCK) k_sm_count(const SmNode *__restrict_
     else tileRight[T] = 0;  // the scan's total slot
     ctl->scanLen = min(T, maxTiles - 1) + 1;
   }
-  if (blockIdx.x >= T || blockIdx.x >= maxTiles - 1) return;  // whole block
-  const SmTileInfo t = tile_info(nodes, first, K, blockIdx.x);
-  const SmNode nd = nodes[t.node];
-  const SmSplit sp = choose_split(nd);
-  const float4 *src = nd.parity ? buf1 : buf0;
-  uint32_t c = 0;
+  for (uint32_t tile = blockIdx.x; tile < T && tile < maxTiles - 1; tile += gridDim.x) {  // whole block
+    const SmTileInfo t = tile_info(nodes, first, K, tile);
+    const SmNode nd = nodes[t.node];
+    const SmSplit sp = choose_split(nd);
+    const float4 *src = nd.parity ? buf1 : buf0;
+    uint32_t c = 0;
 #pragma unroll 4
-  for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += SM_BLOCK) c += side_of(src[i], i - nd.b, sp);
-  c = __reduce_add_sync(0xffffffffu, c);
-  if ((threadIdx.x & 31) == 0) sCnt[threadIdx.x >> 5] = c;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t s = 0;
-    for (int w = 0; w < SM_BLOCK / 32; w++) s += sCnt[w];
-    tileRight[blockIdx.x] = s;
+    for (uint32_t i = t.begin + threadIdx.x; i < t.end; i += SM_BLOCK) c += side_of(src[i], i - nd.b, sp);
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0) sCnt[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t s = 0;
+      for (int w = 0; w < SM_BLOCK / 32; w++) s += sCnt[w];
+      tileRight[tile] = s;
+    }
+    __syncthreads();
   }
 }
 
@@ -303,24 +371,57 @@ __global__ void k_sm_children(const SmNode *__restrict__ nodes, const SmCtl *ctl
   next[2 * k + 1] = c1;
 }
 
-__global__ void __launch_bounds__(SM_BLOCK) k_sm_scatter(const SmNode *__restrict__ nodes,
-                                                         const uint32_t *__restrict__ first, const SmCtl *ctl,
-                                                         int cur, uint32_t maxTiles,
-                                                         const uint32_t *__restrict__ rightScan, float4 *buf0,
-                                                         float4 *buf1, SmNode *next)
+// the scan of the tiles' right counts and k_sm_children in one block
+// (numTiles + 1 <= SM_FUSED_MAX entries in shared memory)
+__global__ void __launch_bounds__(SM_SCAN_THREADS) k_sm_scan_children(const SmNode *__restrict__ nodes,
+                                                                      const SmCtl *ctl, int cur, uint32_t cap,
+                                                                      const uint32_t *__restrict__ first,
+                                                                      uint32_t *__restrict__ tileRight,
+                                                                      Node *__restrict__ out,
+                                                                      uint32_t *__restrict__ used,
+                                                                      SmNode *__restrict__ next)
 {
-  __shared__ uint32_t sWarp[SM_BLOCK / 32];
-  __shared__ int32_t sRed[12][SM_BLOCK / 32];
-  const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
-  if (blockIdx.x >= T || blockIdx.x >= maxTiles - 1) return;  // whole block
-  const SmTileInfo t = tile_info(nodes, first, K, blockIdx.x);
+  extern __shared__ uint32_t sScan[];  // numTiles + 1 entries
+  __shared__ uint32_t sWarp[33];
+  const uint32_t K = min(ctl->bigCount[cur], cap), T = ctl->numTiles;
+  for (uint32_t i = threadIdx.x; i < T; i += blockDim.x) sScan[i] = tileRight[i];
+  __syncthreads();
+  const uint32_t total = block_scan_smem(sScan, T, sWarp);
+  for (uint32_t i = threadIdx.x; i < T; i += blockDim.x) tileRight[i] = sScan[i];
+  if (threadIdx.x == 0) {
+    tileRight[T] = total;
+    sScan[T] = total;
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) {
+    const SmNode nd = nodes[k];
+    const uint32_t nR = sScan[first_end(first, K, T, k)] - sScan[first[k]];
+    const uint32_t m = nd.e - nR;  // left child is [b, m)
+    internal_node(out, used, nd.slot, m);
+    SideBounds sb;
+    sb.init();
+    SmNode c0, c1;
+    child_pair(nd, m, sb, c0, c1);
+    next[2 * k] = c0;
+    next[2 * k + 1] = c1;
+  }
+}
+
+// one tile of k_sm_scatter: the stable scatter of its prims and the
+// children's centroid bounds (one atomicMin/Max per component)
+__device__ __forceinline__ void scatter_tile(const SmNode *__restrict__ nodes, const uint32_t *__restrict__ first,
+                                             uint32_t K, uint32_t T, uint32_t tile,
+                                             const uint32_t *__restrict__ rightScan, float4 *buf0, float4 *buf1,
+                                             SmNode *next, uint32_t *sWarp, int32_t (*sRed)[SM_BLOCK / 32])
+{
+  const SmTileInfo t = tile_info(nodes, first, K, tile);
   const SmNode nd = nodes[t.node];
   const SmSplit sp = choose_split(nd);
   const float4 *src = nd.parity ? buf1 : buf0;
   float4 *dst = nd.parity ? buf0 : buf1;
   const uint32_t nodeRight0 = rightScan[first[t.node]];
   const uint32_t m = nd.e - (rightScan[first_end(first, K, T, t.node)] - nodeRight0);
-  uint32_t rBefore = rightScan[blockIdx.x] - nodeRight0;  // this node's rights before the tile
+  uint32_t rBefore = rightScan[tile] - nodeRight0;  // this node's rights before the tile
   uint32_t lBefore = (t.begin - nd.b) - rBefore;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
@@ -376,6 +477,20 @@ __global__ void __launch_bounds__(SM_BLOCK) k_sm_scatter(const SmNode *__restric
       if (v != INT_MIN) atomicMax(&child->hi[comp - 3], v);
     }
   }
+  __syncthreads();  // sWarp and sRed are reused by the block's next tile
+}
+
+__global__ void __launch_bounds__(SM_BLOCK) k_sm_scatter(const SmNode *__restrict__ nodes,
+                                                         const uint32_t *__restrict__ first, const SmCtl *ctl,
+                                                         int cur, uint32_t maxTiles,
+                                                         const uint32_t *__restrict__ rightScan, float4 *buf0,
+                                                         float4 *buf1, SmNode *next)
+{
+  __shared__ uint32_t sWarp[SM_BLOCK / 32];
+  __shared__ int32_t sRed[12][SM_BLOCK / 32];
+  const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
+  for (uint32_t tile = blockIdx.x; tile < T && tile < maxTiles - 1; tile += gridDim.x)  // whole block
+    scatter_tile(nodes, first, K, T, tile, rightScan, buf0, buf1, next, sWarp, sRed);
 }
 
 // ------------------------------------------------------------------
@@ -669,6 +784,18 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
       (ce = cudaMemcpyAsync(sc, &hsc, sizeof(hsc), cudaMemcpyHostToDevice, al.s)) != cudaSuccess)
     return fail(cuda_error(ce, "spatial median set-up"));
   const int warpGrid = num_sms() * 8;
+  // the level's tile kernels walk the tiles with at most 8 blocks per SM; with
+  // at most SM_FUSED_MAX nodes and tiles a level's two scans run inside one
+  // block each (5 launches per level instead of 11)
+  const int levelGrid = std::max(1, std::min<int>((int)maxTiles, num_sms() * 8));
+  const bool fused = cap <= SM_FUSED_MAX && maxTiles <= SM_FUSED_MAX;
+  if (fused) {
+    if ((ce = cudaFuncSetAttribute(k_sm_tiles_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(uint32_t) * cap))) != cudaSuccess ||
+        (ce = cudaFuncSetAttribute(k_sm_scan_children, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(uint32_t) * maxTiles))) != cudaSuccess)
+      return fail(cuda_error(ce, "spatial median set-up"));
+  }
   auto warp_phase = [&]() -> int {  // every waiting subtree, then an empty task list
     ProfScope ps("sm.warps", al.s);
     k_sm_warp<<<warpGrid, SMW_BLOCK, 0, al.s>>>(tasks, sc, taskCap, thr, buf0, buf1, full, primIDs, used);
@@ -679,17 +806,28 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   int cur = 0;
   for (int level = 0; rootBig; level++) {
     {
-      ProfScope ps("sm.level", al.s, 11);
-      k_sm_tiles<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, tileCount);
-      if ((s = exclusive_scan_u32(tileCount, first, cap, &sc->bigCount[cur], &sc->numTiles, al)) != BQ_OK)
-        return fail(s);
-      k_sm_count<<<maxTiles, SM_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, buf0, buf1, tileRight);
-      if ((s = exclusive_scan_u32(tileRight, tileRight, maxTiles, &sc->scanLen, nullptr, al)) != BQ_OK)
-        return fail(s);
-      k_sm_children<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, first, tileRight, full, used,
-                                                       next);
-      k_sm_scatter<<<maxTiles, SM_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, tileRight, buf0, buf1,
-                                                     next);
+      ProfScope ps("sm.level", al.s, fused ? 5 : 11);
+      if (fused) {
+        k_sm_tiles_scan<<<1, SM_SCAN_THREADS, sizeof(uint32_t) * cap, al.s>>>(bigList[cur], sc, cur, cap, maxTiles,
+                                                                            first);
+      } else {
+        k_sm_tiles<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, tileCount);
+        if ((s = exclusive_scan_u32(tileCount, first, cap, &sc->bigCount[cur], &sc->numTiles, al)) != BQ_OK)
+          return fail(s);
+      }
+      k_sm_count<<<levelGrid, SM_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, buf0, buf1, tileRight);
+      if (fused) {
+        k_sm_scan_children<<<1, SM_SCAN_THREADS, sizeof(uint32_t) * maxTiles, al.s>>>(bigList[cur], sc, cur, cap,
+                                                                                     first, tileRight, full, used,
+                                                                                     next);
+      } else {
+        if ((s = exclusive_scan_u32(tileRight, tileRight, maxTiles, &sc->scanLen, nullptr, al)) != BQ_OK)
+          return fail(s);
+        k_sm_children<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, first, tileRight, full, used,
+                                                         next);
+      }
+      k_sm_scatter<<<levelGrid, SM_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, tileRight, buf0, buf1,
+                                                      next);
       k_sm_classify<<<div_up(2ull * cap, 128), 128, 0, al.s>>>(next, sc, cur, cap, thr, warpMax, bigList[cur ^ 1], tasks,
                                                                taskCap);
       if ((ce = cudaMemsetAsync(&sc->bigCount[cur], 0, sizeof(uint32_t), al.s)) != cudaSuccess ||
