@@ -17,13 +17,15 @@
 //                 stably, from shared memory: runs of 2..4 prims (on
 //                 uniform data nearly all runs) by one thread each, runs
 //                 of 5..32 by one warp each, grouped by size so that warps
-//                 do not diverge; longer runs by one segmented
-//                 composite-key sort of just their prims ((run, low bits)
-//                 keys).  The result is the
-//                 full stable 63-bit order, as cub's SortPairs gives.  The
-//                 same kernel writes the split levels (below) and slots
-//   k_delta       one byte per adjacent key pair: the level at which the
-//                 reference's top-down split would separate them
+//                 do not diverge; longer runs, if they hold differing
+//                 keys, by one segmented composite-key sort of just their
+//                 prims ((run, low bits) keys) -- a run of identical keys
+//                 is already in order.  The result is the full stable
+//                 63-bit order, as cub's SortPairs gives.  The same kernel
+//                 writes the slots and the split levels: one byte per
+//                 adjacent key pair, the level at which the reference's
+//                 top-down split would separate them (k_run_levels writes
+//                 those inside the longer runs)
 //   agglomerate   bottom-up construction of topology and boxes
 //                 (bq_agglom.cuh: per-chunk in shared memory, then the few
 //                 chunk-crossing nodes device-wide)
@@ -413,7 +415,7 @@ __device__ __forceinline__ void order_run34(uint64_t r[4], uint32_t size, uint64
 }
 
 // a run of more than MB_THREAD_RUN prims starting at sorted position i: listed
-// for the segmented sort (its inner levels are written by k_delta after it)
+// for sort_low_bits (its inner levels are written by k_run_levels)
 template <int SB>
 __device__ __forceinline__ void list_long_run(uint32_t i, uint32_t hi, uint32_t nv, const uint64_t *keys, RunStats *rs,
                                               uint4 *runs, uint32_t maxRuns)
@@ -570,26 +572,49 @@ __device__ __forceinline__ uint32_t run_of(const uint32_t *__restrict__ off, uin
   return lo;
 }
 
-template <int SB>
-__global__ void k_run_gather(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off, uint32_t numRuns,
-                             uint32_t numSlots, const uint64_t *__restrict__ keys, const uint32_t *__restrict__ ids,
-                             uint64_t *__restrict__ kk, uint32_t *__restrict__ vv)
+// long run r (of R) holds differing keys: mixed[r] = 1 (every writer stores 1)
+__global__ void k_run_mixed(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off, uint32_t R, uint32_t P,
+                            const uint64_t *__restrict__ keys, uint32_t *__restrict__ mixed)
 {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= numSlots) return;
-  const uint32_t r = run_of(off, numRuns, t);
+  if (t >= P) return;
+  const uint32_t r = run_of(off, R, t);
+  const uint4 run = runs[r];
+  if (keys[run.x + (t - off[r])] != keys[run.x]) mixed[r] = 1u;
+}
+
+// the mixed runs, compacted in run order, and their sizes
+__global__ void k_run_pick(const uint4 *__restrict__ runs, const uint32_t *__restrict__ mixed,
+                           const uint32_t *__restrict__ rank, uint32_t R, uint4 *__restrict__ runsM,
+                           uint32_t *__restrict__ sizesM)
+{
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R || !mixed[r]) return;
+  runsM[rank[r]] = runs[r];
+  sizesM[rank[r]] = runs[r].y;
+}
+
+// cnt[0] runs (cnt[1] prims, both on the device): composite (run, low bits) keys
+template <int SB>
+__global__ void k_run_gather(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off,
+                             const uint32_t *__restrict__ cnt, const uint64_t *__restrict__ keys,
+                             const uint32_t *__restrict__ ids, uint64_t *__restrict__ kk, uint32_t *__restrict__ vv)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cnt[1]) return;
+  const uint32_t r = run_of(off, cnt[0], t);
   const uint32_t pos = runs[r].x + (t - off[r]);
   kk[t] = ((uint64_t)r << SB) | (keys[pos] & low_mask<SB>());
   vv[t] = ids[pos];
 }
 
 template <int SB>
-__global__ void k_run_scatter(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off, uint32_t numSlots,
-                              const uint64_t *__restrict__ kk, const uint32_t *__restrict__ vv,
-                              uint64_t *__restrict__ keys, uint32_t *__restrict__ ids)
+__global__ void k_run_scatter(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off,
+                              const uint32_t *__restrict__ cnt, const uint64_t *__restrict__ kk,
+                              const uint32_t *__restrict__ vv, uint64_t *__restrict__ keys, uint32_t *__restrict__ ids)
 {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= numSlots) return;
+  if (t >= cnt[1]) return;
   const uint64_t k = kk[t];
   const uint32_t r = (uint32_t)(k >> SB);
   const uint4 run = runs[r];
@@ -598,38 +623,32 @@ __global__ void k_run_scatter(const uint4 *__restrict__ runs, const uint32_t *__
   ids[pos] = vv[t];
 }
 
-// ------------------------------------------------------------------
-// pass 3: adjacent-pair split levels
-// ------------------------------------------------------------------
-// split level of the boundary between sorted positions i and i+1
-__device__ __forceinline__ uint8_t split_level(const uint64_t *__restrict__ keys, uint32_t nv, uint32_t i)
+// Split levels of the pairs inside the long runs (the pairs at their ends,
+// which lie across runs, and every slot were written by k_fix_runs).  A run
+// of identical keys is split at (b+e)/2 recursively (radix.h:455-465); in a
+// mixed run, equal neighbours are looked up inside the run.
+__global__ void k_run_levels(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off, uint32_t R,
+                             uint32_t P, const uint32_t *__restrict__ mixed, const uint64_t *__restrict__ keys,
+                             uint8_t *__restrict__ delta)
 {
-  const uint64_t a = keys[i], b = keys[i + 1];
-  if (a != b) return (uint8_t)(64 + (63 - __clzll(a ^ b)));
-  // equal keys: the run [r0, r1) containing i, i+1
-  const uint32_t r0 = run_begin(keys, 0, i, a);
-  const uint32_t r1 = run_end(keys, i + 1, nv, a);
-  // depth of split position s = i+1 in the (b+e)/2 recursion over [r0,r1)
-  const uint64_t s = (uint64_t)i + 1;
-  uint64_t bb = r0, ee = r1;
-  int depth = 0;
-  while (true) {
-    const uint64_t m = (bb + ee) / 2;
-    if (s == m) break;
-    if (s < m) ee = m; else bb = m;
-    depth++;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= P) return;
+  const uint32_t r = run_of(off, R, t);
+  const uint4 run = runs[r];
+  const uint32_t pos = run.x + (t - off[r]), end = run.x + run.y;
+  if (pos + 1 >= end) return;
+  if (!mixed[r]) {
+    delta[pos] = equal_run_level(run.x, end, (uint64_t)pos + 1);
+    return;
   }
-  return (uint8_t)(63 - depth);
-}
-
-__global__ void __launch_bounds__(256) k_delta(const uint64_t *__restrict__ keys, const uint32_t *nvPtr,
-                                               uint8_t *__restrict__ delta, uint32_t *__restrict__ slot)
-{
-  const uint32_t nv = *nvPtr;
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nv) return;
-  slot[i] = SLOT_EMPTY;
-  if (i + 1 < nv) delta[i] = split_level(keys, nv, i);
+  const uint64_t a = keys[pos], b = keys[pos + 1];
+  if (a != b) {
+    delta[pos] = key_level(a, b);
+  } else {
+    const uint32_t r0 = run_begin(keys, run.x, pos, a);
+    const uint32_t r1 = run_end(keys, pos + 1, end, a);
+    delta[pos] = equal_run_level(r0, r1, (uint64_t)pos + 1);
+  }
 }
 
 // ------------------------------------------------------------------
@@ -685,17 +704,14 @@ __global__ void k_collapse(const Node *__restrict__ full, const uint2 *__restric
 } // namespace
 
 // ------------------------------------------------------------------
-// low-bit order inside runs of equal top bits (after the 4-pass sort)
+// low-bit order inside runs of equal top bits (after the top-bit sort)
 // ------------------------------------------------------------------
 namespace {
-// Orders the runs of equal top bits and writes every split level and slot;
-// *longRuns tells whether runs above MB_THREAD_RUN were sorted (their inner
-// levels are then still to be written).
+// Orders the runs of equal top bits and writes every split level and slot.
 template <int SB>
 int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *spareIds, uint32_t n,
-                  const uint32_t *nvDev, uint8_t *delta, uint32_t *slot, uint32_t *err, bool *longRuns, Alloc &al)
+                  const uint32_t *nvDev, uint8_t *delta, uint32_t *slot, uint32_t *err, Alloc &al)
 {
-  *longRuns = false;
   const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
   TempSet tmp(al);
   RunStats *rs = nullptr;
@@ -712,26 +728,45 @@ int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *
   BQ_CUDA(cudaStreamSynchronize(al.s));
   if (h.pad) return set_error(BQ_ERR_CUDA, "run list overflow in the Morton build");
   if (h.count == 0) return BQ_OK;
-  *longRuns = true;
-  // runs longer than MB_THREAD_RUN: one stable sort of (run, low bits)
-  // over just their prims, written back into each run's range
+  // runs longer than MB_THREAD_RUN.  Those holding differing keys get one
+  // stable sort of (run, low bits) over just their prims, written back into
+  // each run's range; runs of identical keys are already in order (the sort
+  // of the top bits is stable).  Then the levels inside all of them.
   const uint32_t R = h.count, P = h.elems;
-  uint32_t *off = nullptr;
+  uint32_t *off = nullptr, *mixed = nullptr, *rank = nullptr, *sizesM = nullptr, *offM = nullptr, *cnt = nullptr;
+  uint4 *runsM = nullptr;
   BQ_TRY(tmp.get(&off, R + 1ull));
-  k_run_sizes<<<div_up(R, 256), 256, 0, al.s>>>(runs, R, off);
-  BQ_TRY(exclusive_scan_u32(off, off, R, nullptr, off + R, al));
+  BQ_TRY(tmp.get(&mixed, R));
+  BQ_TRY(tmp.get(&rank, R));
+  BQ_TRY(tmp.get(&runsM, R));
+  BQ_TRY(tmp.get(&sizesM, R));
+  BQ_TRY(tmp.get(&offM, R));
+  BQ_TRY(tmp.get(&cnt, 2));  // mixed runs, their prims
   uint64_t *kk[2] = {spareKeys, nullptr};
   uint32_t *vv[2] = {spareIds, nullptr};
   BQ_TRY(tmp.get(&kk[1], P));
   BQ_TRY(tmp.get(&vv[1], P));
-  ProfScope ps("morton.longruns", al.s, 2);
-  k_run_gather<SB><<<div_up(P, 256), 256, 0, al.s>>>(runs, off, R, P, keys, ids, kk[0], vv[0]);
   int runBits = 0;
   while (runBits < 32 && ((R - 1) >> runBits)) runBits++;
   if (runBits > 64 - SB) return set_error(BQ_ERR_UNSUPPORTED, "too many long runs of equal keys");
+  BQ_CUDA(cudaMemsetAsync(mixed, 0, sizeof(uint32_t) * R, al.s));
+  {
+    ProfScope ps("morton.longruns", al.s, 6);
+    k_run_sizes<<<div_up(R, 256), 256, 0, al.s>>>(runs, R, off);
+    BQ_TRY(exclusive_scan_u32(off, off, R, nullptr, off + R, al));
+    k_run_mixed<<<div_up(P, 256), 256, 0, al.s>>>(runs, off, R, P, keys, mixed);
+    BQ_TRY(exclusive_scan_u32(mixed, rank, R, nullptr, cnt, al));
+    k_run_pick<<<div_up(R, 256), 256, 0, al.s>>>(runs, mixed, rank, R, runsM, sizesM);
+    BQ_TRY(exclusive_scan_u32(sizesM, offM, R, cnt, cnt + 1, al));
+    k_run_gather<SB><<<div_up(P, 256), 256, 0, al.s>>>(runsM, offM, cnt, keys, ids, kk[0], vv[0]);
+  }
   int ksel = 0;
-  BQ_TRY(onesweep_sort_u64(kk, vv, P, nullptr, 0, SB + runBits, nullptr, &ksel, err, al));
-  k_run_scatter<SB><<<div_up(P, 256), 256, 0, al.s>>>(runs, off, P, kk[ksel], vv[ksel], keys, ids);
+  BQ_TRY(onesweep_sort_u64(kk, vv, P, cnt + 1, 0, SB + runBits, nullptr, &ksel, err, al));
+  {
+    ProfScope ps("morton.runlevels", al.s, 2);
+    k_run_scatter<SB><<<div_up(P, 256), 256, 0, al.s>>>(runsM, offM, cnt, kk[ksel], vv[ksel], keys, ids);
+    k_run_levels<<<div_up(P, 256), 256, 0, al.s>>>(runs, off, R, P, mixed, keys, delta);
+  }
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }
@@ -807,17 +842,9 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   uint64_t *keys = keys2[sel];
   uint32_t *ids = ids2[sel];
   uint32_t *idsOther = ids2[sel ^ 1];
-  bool longRuns = false;
-  s = wide4 ? sort_low_bits<MB_SB4>(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err,
-                                     &longRuns, al)
-            : sort_low_bits<MB_SB3>(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err,
-                                     &longRuns, al);
+  s = wide4 ? sort_low_bits<MB_SB4>(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err, al)
+            : sort_low_bits<MB_SB3>(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err, al);
   if (s != BQ_OK) return fail(s);
-
-  if (longRuns) {  // levels inside the long runs (rewrites all levels and slots)
-    ProfScope ps("morton.delta", al.s);
-    k_delta<<<div_up(n, 256), 256, 0, al.s>>>(keys, &st->numValid, delta, slot);
-  }
   uint2 *pending = nullptr;
   if ((s = tmp.get(&pending, 2ull * div_up(n, AGG_CHUNK))) != BQ_OK) return fail(s);
   AggArgs ag{delta, slot, ids, boxes, nodes, nullptr, &st->numValid, nullptr, pending, nullptr, 0};
