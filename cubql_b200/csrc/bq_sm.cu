@@ -63,6 +63,7 @@ constexpr uint32_t SM_WARP_MAX = 4096;
 constexpr uint32_t SM_WARP_TASKS = 32;
 constexpr uint32_t SM_TILE = 4096;      // prims per tile in the global levels
 constexpr int SM_BLOCK = 256;           // global-level kernels
+constexpr int SM_SCAT_GROUP = 4;        // chunks of SM_BLOCK prims k_sm_scatter loads at once
 constexpr int SMW_BLOCK = 128;          // warp-phase kernel
 constexpr int SMW_WARPS = SMW_BLOCK / 32;
 constexpr int SMW_STACK = 24;           // >= log2(SM_WARP_MAX) + 1
@@ -427,33 +428,45 @@ __device__ __forceinline__ void scatter_tile(const SmNode *__restrict__ nodes, c
   const uint32_t lt = (1u << lane) - 1u;
   SideBounds sb;
   sb.init();
-  for (uint32_t base = t.begin; base < t.end; base += SM_BLOCK) {
-    const uint32_t i = base + threadIdx.x;
-    const bool valid = i < t.end;
-    float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
-    uint32_t side = 0;
-    if (valid) {
-      c = src[i];
-      side = side_of(c, i - nd.b, sp);
-    }
-    const uint32_t bal = __ballot_sync(0xffffffffu, valid && side);
-    if (lane == 0) sWarp[warp] = __popc(bal);
-    __syncthreads();
-    uint32_t rw = 0, rtot = 0;
+  // SM_SCAT_GROUP chunks of SM_BLOCK prims per round: their loads are in
+  // flight together and one barrier pair ranks all of them
+  for (uint32_t base = t.begin; base < t.end; base += SM_BLOCK * SM_SCAT_GROUP) {
+    float4 c[SM_SCAT_GROUP];
+    uint32_t side[SM_SCAT_GROUP], bal[SM_SCAT_GROUP];
 #pragma unroll
-    for (int w = 0; w < SM_BLOCK / 32; w++) {
-      const uint32_t x = sWarp[w];
-      rw += (w < warp) ? x : 0u;
-      rtot += x;
+    for (int g = 0; g < SM_SCAT_GROUP; g++) {
+      const uint32_t i = base + g * SM_BLOCK + threadIdx.x;
+      c[g] = i < t.end ? src[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    if (valid) {
-      const uint32_t rMine = rw + __popc(bal & lt);  // rights of this chunk before me
-      dst[side ? m + rBefore + rMine : nd.b + lBefore + (threadIdx.x - rMine)] = c;
-      sb.add(c, side);
+#pragma unroll
+    for (int g = 0; g < SM_SCAT_GROUP; g++) {
+      const uint32_t i = base + g * SM_BLOCK + threadIdx.x;
+      const bool valid = i < t.end;
+      side[g] = valid ? side_of(c[g], i - nd.b, sp) : 0u;
+      bal[g] = __ballot_sync(0xffffffffu, valid && side[g]);
+      if (lane == 0) sWarp[g * (SM_BLOCK / 32) + warp] = __popc(bal[g]);
     }
-    const uint32_t chunk = min((uint32_t)SM_BLOCK, t.end - base);
-    rBefore += rtot;
-    lBefore += chunk - rtot;
+    __syncthreads();
+#pragma unroll
+    for (int g = 0; g < SM_SCAT_GROUP; g++) {
+      const uint32_t cb = base + g * SM_BLOCK;
+      if (cb >= t.end) break;  // the same for the whole block
+      uint32_t rw = 0, rtot = 0;
+#pragma unroll
+      for (int w = 0; w < SM_BLOCK / 32; w++) {
+        const uint32_t x = sWarp[g * (SM_BLOCK / 32) + w];
+        rw += (w < warp) ? x : 0u;
+        rtot += x;
+      }
+      if (cb + threadIdx.x < t.end) {
+        const uint32_t rMine = rw + __popc(bal[g] & lt);  // rights of this chunk before me
+        dst[side[g] ? m + rBefore + rMine : nd.b + lBefore + (threadIdx.x - rMine)] = c[g];
+        sb.add(c[g], side[g]);
+      }
+      const uint32_t chunk = min((uint32_t)SM_BLOCK, t.end - cb);
+      rBefore += rtot;
+      lBefore += chunk - rtot;
+    }
     __syncthreads();
   }
   sb.warp_reduce();
@@ -480,13 +493,15 @@ __device__ __forceinline__ void scatter_tile(const SmNode *__restrict__ nodes, c
   __syncthreads();  // sWarp and sRed are reused by the block's next tile
 }
 
-__global__ void __launch_bounds__(SM_BLOCK) k_sm_scatter(const SmNode *__restrict__ nodes,
+// 4 blocks per SM (at most 64 registers): the four chunks' loads in flight
+// pay more than a fifth block would
+__global__ void __launch_bounds__(SM_BLOCK, 4) k_sm_scatter(const SmNode *__restrict__ nodes,
                                                          const uint32_t *__restrict__ first, const SmCtl *ctl,
                                                          int cur, uint32_t maxTiles,
                                                          const uint32_t *__restrict__ rightScan, float4 *buf0,
                                                          float4 *buf1, SmNode *next)
 {
-  __shared__ uint32_t sWarp[SM_BLOCK / 32];
+  __shared__ uint32_t sWarp[SM_SCAT_GROUP * SM_BLOCK / 32];
   __shared__ int32_t sRed[12][SM_BLOCK / 32];
   const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
   for (uint32_t tile = blockIdx.x; tile < T && tile < maxTiles - 1; tile += gridDim.x)  // whole block

@@ -191,8 +191,9 @@ __device__ __forceinline__ void sort_keys(uint64_t v[W])
 // answer does not depend on the visiting order: leaf slots inside the
 // (slack-widened) cull radius are processed as they are met, the nearest
 // inner child is descended and the other inner children are pushed
-// unsorted; popped entries beyond the shrunken radius are skipped.  Stack entries are
-// (distance bits << 32 | wide node).  Returns false on stack overflow.
+// unsorted; popped entries beyond the shrunken radius are skipped.  Stack
+// entries are (distance bits << 32 | wide node).  Returns false on stack
+// overflow.
 template <int W, typename Stack, typename Leaf>
 __device__ __forceinline__ bool wide_traverse_lowest(const Node *__restrict__ slots, float qx, float qy, float qz,
                                                      float cull, Stack &st, Leaf &leaf)
