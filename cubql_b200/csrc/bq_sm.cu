@@ -545,19 +545,39 @@ __device__ void sm_small_subtree(const SmNode &root, const float4 *src, int thr,
     const uint32_t balR = __ballot_sync(0xffffffffu, in && side);
     const uint32_t balL = __ballot_sync(0xffffffffu, in && !side);
     const uint32_t m = cur.e - __popc(balR);
+    // a child of at most thr prims is a leaf: written here, never split, so
+    // its centroid bounds are not needed
+    const bool leafL = (int64_t)(m - cur.b) <= thr, leafR = (int64_t)(cur.e - m) <= thr;
     SideBounds sb;
     sb.init();
-    if (in) sb.add(c, side);
-    sb.warp_reduce();
+    if (!(leafL && leafR)) {
+      if (in) sb.add(c, side);
+      sb.warp_reduce();
+    }
     const uint32_t dest = !in ? (uint32_t)lane
                               : (side ? (m - base) + __popc(balR & lt) : (cur.b - base) + __popc(balL & lt));
     xbuf[dest] = c;
     __syncwarp();
     c = xbuf[lane];
     __syncwarp();
-    if (lane == 0) internal_node(out, used, cur.slot, m);
     SmNode c0, c1;
     child_pair(cur, m, sb, c0, c1);
+    if (lane == 0) {
+      internal_node(out, used, cur.slot, m);
+      if (leafL) leaf_node(out, c0.slot, c0.b, c0.e - c0.b);
+      if (leafR) leaf_node(out, c1.slot, c1.b, c1.e - c1.b);
+    }
+    if (leafL && leafR) {
+      if (sp == 0) break;
+      __syncwarp();
+      cur = stk[--sp];
+      __syncwarp();
+      continue;
+    }
+    if (leafL || leafR) {
+      cur = leafL ? c1 : c0;
+      continue;
+    }
     const bool leftSmaller = (m - cur.b) <= (cur.e - m);
     if (sp >= stackLeft) {  // unreachable: the stacked child is always the larger one
       if (lane == 0) atomicOr(err, DEV_ERR_RANGE);
