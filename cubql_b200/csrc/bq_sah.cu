@@ -646,7 +646,7 @@ __device__ void sah_small_subtree(const SahNode &root, const SahPrim *src, int t
     SahDec dec;
     dec.dim = DEC_LEAF;
     dec.bin = 0;
-    if ((int64_t)count > thr) {
+    if ((int64_t)count > thr && count > 1) {  // one prim cannot be split: a leaf
       float aLo[3], aHi[3], bLo[3], bHi[3];
 #pragma unroll
       for (int k = 0; k < 3; k++) { aLo[k] = bLo[k] = FLT_MAX; aHi[k] = bHi[k] = -FLT_MAX; }
@@ -689,20 +689,41 @@ __device__ void sah_small_subtree(const SahNode &root, const SahPrim *src, int t
       if (lane == 0) atomicOr(err, DEV_ERR_RANGE);
       break;
     }
+    // a child of at most thr prims, or of one, is a leaf: written here, never
+    // evaluated, so its bounds are not needed
+    const uint32_t nL = m - cur.b, nR = cur.e - m;
+    const bool leafL = (int64_t)nL <= thr || nL == 1, leafR = (int64_t)nR <= thr || nR == 1;
     SideBounds sb;
     sb.init();
-    if (in) sb.add(p, side);
-    sb.warp_reduce();
+    if (!(leafL && leafR)) {
+      if (in) sb.add(p, side);
+      sb.warp_reduce();
+    }
     const uint32_t dest = !in ? (uint32_t)lane
                               : (side ? (m - base) + __popc(balR & lt) : (cur.b - base) + __popc(balL & lt));
     xbuf[dest] = p;
     __syncwarp();
     p = xbuf[lane];
     __syncwarp();
-    if (lane == 0) internal_node(out, used, cur.slot, m);
     SahNode c0, c1;
     child_pair(cur, m, sb, c0, c1);
-    const bool leftSmaller = (m - cur.b) <= (cur.e - m);
+    if (lane == 0) {
+      internal_node(out, used, cur.slot, m);
+      if (leafL) leaf_node(out, c0.slot, c0.b, nL);
+      if (leafR) leaf_node(out, c1.slot, c1.b, nR);
+    }
+    if (leafL && leafR) {
+      if (sp == 0) break;
+      __syncwarp();
+      cur = stk[--sp];
+      __syncwarp();
+      continue;
+    }
+    if (leafL || leafR) {
+      cur = leafL ? c1 : c0;
+      continue;
+    }
+    const bool leftSmaller = nL <= nR;
     if (sp >= stackLeft) {  // unreachable: the stacked child is always the larger one
       if (lane == 0) atomicOr(err, DEV_ERR_RANGE);
       break;
