@@ -270,6 +270,53 @@ struct ProfScope {
 };
 
 // ------------------------------------------------------------------
+// one-block scans of short per-level arrays kept in shared memory (the
+// spatial-median and SAH level loops)
+// ------------------------------------------------------------------
+constexpr int BQ_SCAN_THREADS = 1024;
+constexpr uint32_t BQ_SCAN_SMEM_MAX = 56u * 1024u;  // longest array such a scan keeps in shared memory
+
+// Exclusive scan of s[0 .. L) in place by one block of BQ_SCAN_THREADS
+// threads (each a contiguous segment); returns the total.  sWarp: 33 words.
+__device__ __forceinline__ uint32_t block_scan_smem(uint32_t *s, uint32_t L, uint32_t *sWarp)
+{
+  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint32_t per = (L + BQ_SCAN_THREADS - 1) / BQ_SCAN_THREADS;
+  const uint32_t b = min(t * per, L), e = min(b + per, L);
+  uint32_t sum = 0;
+  for (uint32_t i = b; i < e; i++) sum += s[i];
+  uint32_t x = sum;  // inclusive scan over the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if ((int)lane >= o) x += y;
+  }
+  if (lane == 31) sWarp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = sWarp[lane];
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+      if ((int)lane >= o) wi += y;
+    }
+    sWarp[lane] = wi - w;
+    if (lane == 31) sWarp[32] = wi;
+  }
+  __syncthreads();
+  uint32_t run = sWarp[warp] + x - sum;
+  for (uint32_t i = b; i < e; i++) {
+    const uint32_t v = s[i];
+    s[i] = run;
+    run += v;
+  }
+  const uint32_t total = sWarp[32];
+  __syncthreads();
+  return total;
+}
+
+// ------------------------------------------------------------------
 // onesweep LSD radix sort (bq_sort.cu)
 // ------------------------------------------------------------------
 // Sorts (key, value) pairs by bits [beginBit, endBit) of the key, stably.

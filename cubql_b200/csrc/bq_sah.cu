@@ -478,19 +478,31 @@ __global__ void k_sah_decide(const SahNode *__restrict__ nodes, const SahCtl *ct
   if (lane == 0) decs[k] = dec;
 }
 
-// right-side count of every tile from its bin counts
-__global__ void k_sah_tile_right(const SahNode *__restrict__ nodes, const uint32_t *__restrict__ first, SahCtl *ctl,
-                                 int cur, uint32_t maxTiles, const SahDec *__restrict__ decs,
-                                 const uint32_t *__restrict__ tileCnt, uint32_t *__restrict__ tileRight)
+// the scan of the level's tile counts in one block (at most
+// BQ_SCAN_SMEM_MAX nodes, counted in shared memory)
+__global__ void __launch_bounds__(BQ_SCAN_THREADS) k_sah_tiles_scan(SahCtl *ctl, int cur, uint32_t cap,
+                                                                    uint32_t maxTiles,
+                                                                    const uint32_t *__restrict__ tileCount,
+                                                                    uint32_t *__restrict__ first)
 {
-  const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t == 0) {
+  extern __shared__ uint32_t sVal[];  // cap entries
+  __shared__ uint32_t sWarp[33];
+  const uint32_t K = min(ctl->bigCount[cur], cap);
+  for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) sVal[k] = tileCount[k];
+  __syncthreads();
+  const uint32_t T = block_scan_smem(sVal, K, sWarp);
+  for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) first[k] = sVal[k];
+  if (threadIdx.x == 0) {
     if (T >= maxTiles) atomicOr(&ctl->err, DEV_ERR_RANGE);
-    else tileRight[T] = 0;
-    ctl->scanLen = min(T, maxTiles - 1) + 1;
+    ctl->numTiles = min(T, maxTiles - 1);
   }
-  if (t >= T || t >= maxTiles - 1) return;
+}
+
+// right-side count of a tile from its bin counts
+__device__ __forceinline__ uint32_t sah_tile_right(const SahNode *__restrict__ nodes, const uint32_t *__restrict__ first,
+                                                   uint32_t K, uint32_t t, const SahDec *__restrict__ decs,
+                                                   const uint32_t *__restrict__ tileCnt)
+{
   const TileInfo ti = tile_info(nodes, first, K, t);
   const SahDec dec = decs[ti.node];
   uint32_t r = 0;
@@ -501,19 +513,17 @@ __global__ void k_sah_tile_right(const SahNode *__restrict__ nodes, const uint32
     const uint32_t half = nd.b + (nd.e - nd.b) / 2;  // positions >= half go right
     r = ti.end > max(ti.begin, half) ? ti.end - max(ti.begin, half) : 0u;
   }
-  tileRight[t] = r;
+  return r;
 }
 
 // per split node: the split position, the internal node, the two child
 // records (bounds start empty); leaves get an empty pair
-__global__ void k_sah_children(const SahNode *__restrict__ nodes, const SahCtl *ctl, int cur, uint32_t cap,
-                               const uint32_t *__restrict__ first, const uint32_t *__restrict__ rightScan,
-                               const SahDec *__restrict__ decs, Node *__restrict__ out, uint32_t *__restrict__ used,
-                               SahNode *__restrict__ next, uint32_t *err)
+__device__ __forceinline__ void sah_node_children(const SahNode *__restrict__ nodes, uint32_t K, uint32_t T, uint32_t k,
+                                                  const uint32_t *__restrict__ first, const uint32_t *rightScan,
+                                                  const SahDec *__restrict__ decs, Node *__restrict__ out,
+                                                  uint32_t *__restrict__ used, SahNode *__restrict__ next,
+                                                  uint32_t *err)
 {
-  const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= K || k >= cap) return;
   const SahNode nd = nodes[k];
   SahNode c0, c1;
   if (decs[k].dim == DEC_LEAF) {
@@ -531,6 +541,62 @@ __global__ void k_sah_children(const SahNode *__restrict__ nodes, const SahCtl *
   child_pair(nd, m, sb, c0, c1);
   next[2 * k] = c0;
   next[2 * k + 1] = c1;
+}
+
+// k_sah_tile_right, the scan of its counts and k_sah_children in one block
+// (numTiles + 1 <= BQ_SCAN_SMEM_MAX entries in shared memory)
+__global__ void __launch_bounds__(BQ_SCAN_THREADS) k_sah_right_children(const SahNode *__restrict__ nodes,
+                                                                        const uint32_t *__restrict__ first,
+                                                                        SahCtl *ctl, int cur, uint32_t cap,
+                                                                        const SahDec *__restrict__ decs,
+                                                                        const uint32_t *__restrict__ tileCnt,
+                                                                        uint32_t *__restrict__ tileRight,
+                                                                        Node *__restrict__ out,
+                                                                        uint32_t *__restrict__ used,
+                                                                        SahNode *__restrict__ next)
+{
+  extern __shared__ uint32_t sScan[];  // numTiles + 1 entries
+  __shared__ uint32_t sWarp[33];
+  const uint32_t K = min(ctl->bigCount[cur], cap), T = ctl->numTiles;
+  for (uint32_t t = threadIdx.x; t < T; t += blockDim.x) sScan[t] = sah_tile_right(nodes, first, K, t, decs, tileCnt);
+  __syncthreads();
+  const uint32_t total = block_scan_smem(sScan, T, sWarp);
+  for (uint32_t t = threadIdx.x; t < T; t += blockDim.x) tileRight[t] = sScan[t];
+  if (threadIdx.x == 0) {
+    tileRight[T] = total;
+    sScan[T] = total;
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < K; k += blockDim.x)
+    sah_node_children(nodes, K, T, k, first, sScan, decs, out, used, next, &ctl->err);
+}
+
+// right-side count of every tile from its bin counts
+__global__ void k_sah_tile_right(const SahNode *__restrict__ nodes, const uint32_t *__restrict__ first, SahCtl *ctl,
+                                 int cur, uint32_t maxTiles, const SahDec *__restrict__ decs,
+                                 const uint32_t *__restrict__ tileCnt, uint32_t *__restrict__ tileRight)
+{
+  const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    if (T >= maxTiles) atomicOr(&ctl->err, DEV_ERR_RANGE);
+    else tileRight[T] = 0;
+    ctl->scanLen = min(T, maxTiles - 1) + 1;
+  }
+  if (t >= T || t >= maxTiles - 1) return;
+  tileRight[t] = sah_tile_right(nodes, first, K, t, decs, tileCnt);
+}
+
+// sah_node_children for every big node of the level
+__global__ void k_sah_children(const SahNode *__restrict__ nodes, const SahCtl *ctl, int cur, uint32_t cap,
+                               const uint32_t *__restrict__ first, const uint32_t *__restrict__ rightScan,
+                               const SahDec *__restrict__ decs, Node *__restrict__ out, uint32_t *__restrict__ used,
+                               SahNode *__restrict__ next, uint32_t *err)
+{
+  const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K || k >= cap) return;
+  sah_node_children(nodes, K, T, k, first, rightScan, decs, out, used, next, err);
 }
 
 __global__ void __launch_bounds__(SAH_BLOCK) k_sah_scatter(const SahNode *__restrict__ nodes,
@@ -987,6 +1053,16 @@ int build_elh(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
       (ce = cudaMemcpyAsync(sc, &hsc, sizeof(hsc), cudaMemcpyHostToDevice, al.s)) != cudaSuccess)
     return fail(cuda_error(ce, "sah set-up"));
   const int warpGrid = num_sms() * 8;
+  // with at most BQ_SCAN_SMEM_MAX big nodes and tiles a level's two scans run
+  // inside one block each (7 launches per level instead of 12)
+  const bool fused = cap <= BQ_SCAN_SMEM_MAX && maxTiles <= BQ_SCAN_SMEM_MAX;
+  if (fused) {
+    if ((ce = cudaFuncSetAttribute(k_sah_tiles_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(uint32_t) * cap))) != cudaSuccess ||
+        (ce = cudaFuncSetAttribute(k_sah_right_children, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(uint32_t) * maxTiles))) != cudaSuccess)
+      return fail(cuda_error(ce, "sah set-up"));
+  }
   auto warp_phase = [&]() -> int {
     ProfScope ps(HEUR ? "elh.warps" : "sah.warps", al.s);
     k_sah_warp<<<warpGrid, SAHW_BLOCK, 0, al.s>>>(tasks, sc, taskCap, thr, buf0, buf1, full, primIDs, used);
@@ -997,20 +1073,29 @@ int build_elh(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
   int cur = 0;
   for (int level = 0; rootBig; level++) {
     {
-      ProfScope ps(HEUR ? "elh.level" : "sah.level", al.s, 12);
+      ProfScope ps(HEUR ? "elh.level" : "sah.level", al.s, fused ? 7 : 12);
       k_sah_tiles<<<cap, 128, 0, al.s>>>(bigList[cur], sc, cur, cap, tileCount, nodeBins);
-      if ((s = exclusive_scan_u32(tileCount, first, cap, &sc->bigCount[cur], &sc->numTiles, al)) != BQ_OK)
+      if (fused) {
+        k_sah_tiles_scan<<<1, BQ_SCAN_THREADS, sizeof(uint32_t) * cap, al.s>>>(sc, cur, cap, maxTiles, tileCount,
+                                                                             first);
+      } else if ((s = exclusive_scan_u32(tileCount, first, cap, &sc->bigCount[cur], &sc->numTiles, al)) != BQ_OK) {
         return fail(s);
+      }
       k_sah_bin<<<maxTiles, SAH_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, buf0, buf1, tileCnt,
                                                   nodeBins);
       k_sah_decide<<<div_up(cap, 4), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, thr, nodeBins, decs, buf0, buf1,
                                                     full, primIDs);
-      k_sah_tile_right<<<div_up(maxTiles, 128), 128, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, decs,
-                                                                tileCnt, tileRight);
-      if ((s = exclusive_scan_u32(tileRight, tileRight, maxTiles, &sc->scanLen, nullptr, al)) != BQ_OK)
-        return fail(s);
-      k_sah_children<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, first, tileRight, decs, full,
-                                                         used, next, &sc->err);
+      if (fused) {
+        k_sah_right_children<<<1, BQ_SCAN_THREADS, sizeof(uint32_t) * maxTiles, al.s>>>(
+            bigList[cur], first, sc, cur, cap, decs, tileCnt, tileRight, full, used, next);
+      } else {
+        k_sah_tile_right<<<div_up(maxTiles, 128), 128, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, decs,
+                                                                  tileCnt, tileRight);
+        if ((s = exclusive_scan_u32(tileRight, tileRight, maxTiles, &sc->scanLen, nullptr, al)) != BQ_OK)
+          return fail(s);
+        k_sah_children<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, first, tileRight, decs, full,
+                                                           used, next, &sc->err);
+      }
       k_sah_scatter<<<maxTiles, SAH_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, tileRight, decs, buf0,
                                                       buf1, next);
       k_sah_classify<<<div_up(2ull * cap, 128), 128, 0, al.s>>>(next, sc, cur, cap, thr, warpMax, bigList[cur ^ 1],

@@ -68,8 +68,8 @@ constexpr int SMW_BLOCK = 128;          // warp-phase kernel
 constexpr int SMW_WARPS = SMW_BLOCK / 32;
 constexpr int SMW_STACK = 24;           // >= log2(SM_WARP_MAX) + 1
 constexpr int SM_LEVELS_PER_CHECK = 2;  // global levels between two host looks at the counters
-constexpr int SM_SCAN_THREADS = 1024;   // one-block scans of a level's node and tile arrays
-constexpr uint32_t SM_FUSED_MAX = 56u * 1024u;  // longest array such a scan keeps in shared memory
+constexpr int SM_SCAN_THREADS = BQ_SCAN_THREADS;  // one-block scans of a level's node and tile arrays
+constexpr uint32_t SM_FUSED_MAX = BQ_SCAN_SMEM_MAX;
 
 // A node still to be split: prim range [b, e) in buffer `parity`, its slot,
 // and its prims' centroid bounds (encoded, see enc_f).
@@ -253,46 +253,6 @@ __global__ void k_sm_tiles(const SmNode *__restrict__ nodes, SmCtl *ctl, int cur
   if (k == 0 && K > cap) atomicOr(&ctl->err, DEV_ERR_RANGE);
   if (k >= K || k >= cap) return;
   tileCount[k] = (nodes[k].e - nodes[k].b + SM_TILE - 1) / SM_TILE;
-}
-
-// Exclusive scan of s[0 .. L) in place by one block of SM_SCAN_THREADS
-// threads (each a contiguous segment); returns the total.  sWarp: 33 words.
-__device__ uint32_t block_scan_smem(uint32_t *s, uint32_t L, uint32_t *sWarp)
-{
-  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const uint32_t per = (L + SM_SCAN_THREADS - 1) / SM_SCAN_THREADS;
-  const uint32_t b = min(t * per, L), e = min(b + per, L);
-  uint32_t sum = 0;
-  for (uint32_t i = b; i < e; i++) sum += s[i];
-  uint32_t x = sum;  // inclusive scan over the warp
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if ((int)lane >= o) x += y;
-  }
-  if (lane == 31) sWarp[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    const uint32_t w = sWarp[lane];
-    uint32_t wi = w;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
-      if ((int)lane >= o) wi += y;
-    }
-    sWarp[lane] = wi - w;
-    if (lane == 31) sWarp[32] = wi;
-  }
-  __syncthreads();
-  uint32_t run = sWarp[warp] + x - sum;
-  for (uint32_t i = b; i < e; i++) {
-    const uint32_t v = s[i];
-    s[i] = run;
-    run += v;
-  }
-  const uint32_t total = sWarp[32];
-  __syncthreads();
-  return total;
 }
 
 // k_sm_tiles and the scan of its counts in one block (the level's big
