@@ -71,7 +71,7 @@ FREE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctype
 
 
 class bq_allocator(ctypes.Structure):
-    _fields_ = [("ctx", ctypes.c_void_p), ("malloc", MALLOC_FN), ("free", FREE_FN)]
+    _fields_ = [("ctx", ctypes.c_void_p), ("malloc", MALLOC_FN), ("free", FREE_FN), ("scratchFromPool", ctypes.c_int)]
 
 
 class bq_tuning(ctypes.Structure):
@@ -193,7 +193,8 @@ class TorchAllocator:
         self.live = {}
         self._m = MALLOC_FN(self._malloc)
         self._f = FREE_FN(self._free)
-        self.c = bq_allocator(None, self._m, self._f)
+        # temporaries from libbq's stream-ordered pool; trees from torch
+        self.c = bq_allocator(None, self._m, self._f, 1)
 
     def _malloc(self, ctx, out, size, stream):
         try:

@@ -81,7 +81,7 @@ void keep_pool_memory()
 
 Alloc make_alloc(const bq_allocator *a, bq_stream_t s)
 {
-  if (!a || !a->malloc) keep_pool_memory();
+  if (!a || !a->malloc || a->scratchFromPool) keep_pool_memory();
   Alloc al;
   al.a = (a && a->malloc && a->free) ? a : nullptr;
   al.s = (cudaStream_t)s;

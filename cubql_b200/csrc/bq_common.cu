@@ -47,6 +47,24 @@ int Alloc::free_bytes(void *p)
   return e == cudaSuccess ? BQ_OK : cuda_error(e, "cudaFreeAsync");
 }
 
+int Alloc::scratch_malloc(void **p, size_t bytes)
+{
+  if (a && a->scratchFromPool) {
+    Alloc pool{nullptr, s};
+    return pool.malloc_bytes(p, bytes);
+  }
+  return malloc_bytes(p, bytes);
+}
+
+int Alloc::scratch_free(void *p)
+{
+  if (a && a->scratchFromPool) {
+    Alloc pool{nullptr, s};
+    return pool.free_bytes(p);
+  }
+  return free_bytes(p);
+}
+
 int num_sms()
 {
   int dev = 0, n = 148;

@@ -46,6 +46,10 @@ struct Alloc {
   cudaStream_t s;
   int malloc_bytes(void **p, size_t bytes);
   int free_bytes(void *p);
+  // temporaries: from the caller's allocator, or from the pool when it
+  // asks for that (bq_allocator::scratchFromPool)
+  int scratch_malloc(void **p, size_t bytes);
+  int scratch_free(void *p);
   template <typename T>
   int get(T **p, size_t count) { return malloc_bytes((void **)p, sizeof(T) * (count ? count : 1)); }
 };
@@ -59,13 +63,13 @@ struct TempSet {
   template <typename T>
   int get(T **p, size_t count)
   {
-    int s = al.get(p, count);
+    int s = al.scratch_malloc((void **)p, sizeof(T) * (count ? count : 1));
     if (s == BQ_OK) ptrs[n++] = (void *)*p;
     return s;
   }
   ~TempSet()
   {
-    for (int i = n - 1; i >= 0; i--) al.free_bytes(ptrs[i]);
+    for (int i = n - 1; i >= 0; i--) al.scratch_free(ptrs[i]);
   }
 };
 

@@ -89,6 +89,12 @@ typedef struct bq_allocator {
   void *ctx;
   int (*malloc)(void *ctx, void **ptr, size_t size, bq_stream_t stream); /* 0 on success */
   int (*free)(void *ctx, void *ptr, bq_stream_t stream);
+  /* 0 (the default of a zero-initialised struct): every allocation, the
+     call's temporaries included, goes through malloc/free, as with the
+     reference's GpuMemoryResource.  1: only the arrays handed back (tree
+     nodes, primIDs) do; temporaries come from the library's stream-ordered
+     pool (cudaMallocAsync), which saves a callback per temporary. */
+  int scratchFromPool;
 } bq_allocator;
 
 /* traversal knobs; NULL = defaults (ties lowest-ID, Morton-ordered

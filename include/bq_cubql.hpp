@@ -53,7 +53,7 @@ struct ResourceAdapter {
   {
     return static_cast<MemRes *>(ctx)->free(ptr, (cudaStream_t)s) == cudaSuccess ? 0 : 1;
   }
-  static bq_allocator make(MemRes &m) { return bq_allocator{&m, &mallocFn, &freeFn}; }
+  static bq_allocator make(MemRes &m) { return bq_allocator{&m, &mallocFn, &freeFn, 0}; }
 };
 
 template <class BVH>
