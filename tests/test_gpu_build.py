@@ -122,6 +122,28 @@ def test_morton_runs_across_tiles(bq, oracle, seed):
     bvh.free()
 
 
+@pytest.mark.parametrize("builder", ["morton", "sm", "sah"])
+def test_allocator_scratch_modes(bq, oracle, builder):
+    """bq_allocator::scratchFromPool 0 (every temporary through the torch
+    callbacks) and 1 (temporaries from the library's pool) give the same
+    tree; the returned arrays always come from the callbacks."""
+    b = torch.from_numpy(_boxes("gmm", 50000)).cuda()
+    trees = []
+    for mode in (0, 1):
+        a = bq.TorchAllocator()
+        a.c.scratchFromPool = mode
+        if builder == "morton":
+            t = bq.cuda.radixBuilder(b, allocator=a)
+        elif builder == "sm":
+            t = bq.gpuBuilder(b, bq.BuildConfig(makeLeafThreshold=4), allocator=a)
+        else:
+            t = bq.cuda.sahBuilder(b, allocator=a)
+        assert t.c.nodes in a.live and t.c.primIDs in a.live
+        trees.append(t.to_host())
+        t.free()
+    assert trees[0][0].tobytes() == trees[1][0].tobytes() and np.array_equal(trees[0][1], trees[1][1])
+
+
 def test_morton_is_deterministic(bq):
     b = torch.from_numpy(_boxes("gmm", 300000)).cuda()
     a = bq.cuda.radixBuilder(b).to_host()
