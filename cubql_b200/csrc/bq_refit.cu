@@ -3,11 +3,14 @@
 // Replaces gpuBuilder_impl::refit (cuBQL/builder/cuda/sm_builder.h:616-693):
 // parent links from the admin words, then one thread per leaf computes its
 // box from the prim boxes and climbs; at each parent the first arriving
-// child stops and the second merges both children (a per-node counter, one
-// atomicAdd per arrival).  min/max are exact, so the boxes equal the
+// child stops and the second merges its own box (kept in registers) with
+// its sibling's (a per-node counter, one device-scope acquire/release
+// fetch_add per arrival).  min/max are exact, so the boxes equal the
 // reference's bit for bit regardless of arrival order.  The admin words are
 // never modified, so the same tree can be refitted after every vertex
 // update of a fitting loop.
+#include <cuda/atomic>
+
 #include "bq_internal.cuh"
 
 namespace bq {
@@ -59,15 +62,22 @@ __global__ void k_refit_climb(Node *nodes, uint32_t numNodes, const uint32_t *__
   while (true) {
     const uint32_t p = parent[i];
     if (p == NO_PARENT) return;
-    __threadfence();
-    if (atomicAdd(&counter[p], 1u) == 0) return;  // sibling still pending: it carries on
-    __threadfence();
-    const Node pn = ldcg_node(nodes + p);
-    const uint64_t pa = node_admin(pn);
+    // device-scope release of this node's box / acquire of the sibling's
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrived(counter[p]);
+    if (arrived.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;  // sibling still pending: it carries on
+    const float4 pb = __ldcg(&nodes[p].b);  // from L2: the box half of this word is being written
+    const uint64_t pa = ((uint64_t)__float_as_uint(pb.w) << 32) | __float_as_uint(pb.z);
     const uint64_t c0 = admin_offset(pa);
-    const Node l = ldcg_node(nodes + c0), r = ldcg_node(nodes + c0 + 1);
-    store_bounds(nodes + p, fminf(l.a.x, r.a.x), fminf(l.a.y, r.a.y), fminf(l.a.z, r.a.z), fmaxf(l.a.w, r.a.w),
-                 fmaxf(l.b.x, r.b.x), fmaxf(l.b.y, r.b.y), pa);
+    const Node s = ldcg_node(nodes + (c0 == i ? c0 + 1 : c0));  // the sibling's box, from L2
+    // union in child order (left, right), as the reference's min/max calls
+    if (c0 == i) {
+      lx = fminf(lx, s.a.x); ly = fminf(ly, s.a.y); lz = fminf(lz, s.a.z);
+      hx = fmaxf(hx, s.a.w); hy = fmaxf(hy, s.b.x); hz = fmaxf(hz, s.b.y);
+    } else {
+      lx = fminf(s.a.x, lx); ly = fminf(s.a.y, ly); lz = fminf(s.a.z, lz);
+      hx = fmaxf(s.a.w, hx); hy = fmaxf(s.b.x, hy); hz = fmaxf(s.b.y, hz);
+    }
+    store_bounds(nodes + p, lx, ly, lz, hx, hy, hz, pa);
     i = p;
   }
 }
