@@ -11,6 +11,8 @@
 // directly because the query returns global triangle ids).
 #include <algorithm>
 
+#include <cuda/atomic>
+
 #include "bq_traverse.cuh"
 
 namespace bq {
@@ -86,15 +88,21 @@ __global__ void k_brefit_climb(Node *nodes, uint32_t numSlots, const bq_bvh3f *_
   while (true) {
     const uint32_t p = parent[j];
     if (p == BR_NO_PARENT) return;
-    __threadfence();
-    if (atomicAdd(&counter[p], 1u) == 0) return;
-    __threadfence();
-    const Node pn = ldcg_node(nodes + p);
-    const uint64_t pa = node_admin(pn);
+    // device-scope release of this node's box / acquire of the sibling's
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrived(counter[p]);
+    if (arrived.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;  // the sibling finishes this parent
+    const float4 pb = __ldcg(&nodes[p].b);  // from L2: the box half of this word is being written
+    const uint64_t pa = ((uint64_t)__float_as_uint(pb.w) << 32) | __float_as_uint(pb.z);
     const uint64_t c0 = base + admin_offset(pa);
-    const Node l = ldcg_node(nodes + c0), r = ldcg_node(nodes + c0 + 1);
-    nodes[p] = make_node(fminf(l.a.x, r.a.x), fminf(l.a.y, r.a.y), fminf(l.a.z, r.a.z), fmaxf(l.a.w, r.a.w),
-                         fmaxf(l.b.x, r.b.x), fmaxf(l.b.y, r.b.y), pa);
+    const Node sib = ldcg_node(nodes + (c0 == j ? c0 + 1 : c0));
+    if (c0 == j) {  // union in child order (left, right)
+      lx = fminf(lx, sib.a.x); ly = fminf(ly, sib.a.y); lz = fminf(lz, sib.a.z);
+      hx = fmaxf(hx, sib.a.w); hy = fmaxf(hy, sib.b.x); hz = fmaxf(hz, sib.b.y);
+    } else {
+      lx = fminf(sib.a.x, lx); ly = fminf(sib.a.y, ly); lz = fminf(sib.a.z, lz);
+      hx = fmaxf(sib.a.w, hx); hy = fmaxf(sib.b.x, hy); hz = fmaxf(sib.b.y, hz);
+    }
+    nodes[p] = make_node(lx, ly, lz, hx, hy, hz, pa);
     j = p;
   }
 }

@@ -23,6 +23,8 @@
 // Nothing here calls cudaMalloc, cudaFree or any allocating routine.
 #include <mutex>
 
+#include <cuda/atomic>
+
 #include "bq_internal.cuh"
 
 namespace bq {
@@ -72,15 +74,21 @@ __global__ void k_na_climb(Node *nodes, uint32_t numNodes, const uint32_t *__res
   while (true) {
     const uint32_t p = parent[i];
     if (p == NA_NO_PARENT) return;
-    __threadfence();
-    if (atomicAdd(&counter[p], 1u) == 0) return;  // the sibling finishes this parent
-    __threadfence();
-    const Node pn = ldcg_node(nodes + p);
-    const uint64_t pa = node_admin(pn);
+    // device-scope release of this node's box / acquire of the sibling's
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrived(counter[p]);
+    if (arrived.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;  // the sibling finishes this parent
+    const float4 pb = __ldcg(&nodes[p].b);  // from L2: the box half of this word is being written
+    const uint64_t pa = ((uint64_t)__float_as_uint(pb.w) << 32) | __float_as_uint(pb.z);
     const uint64_t c0 = admin_offset(pa);
-    const Node l = ldcg_node(nodes + c0), r = ldcg_node(nodes + c0 + 1);
-    nodes[p] = make_node(fminf(l.a.x, r.a.x), fminf(l.a.y, r.a.y), fminf(l.a.z, r.a.z), fmaxf(l.a.w, r.a.w),
-                         fmaxf(l.b.x, r.b.x), fmaxf(l.b.y, r.b.y), pa);
+    const Node sib = ldcg_node(nodes + (c0 == i ? c0 + 1 : c0));
+    if (c0 == i) {  // union in child order (left, right)
+      lx = fminf(lx, sib.a.x); ly = fminf(ly, sib.a.y); lz = fminf(lz, sib.a.z);
+      hx = fmaxf(hx, sib.a.w); hy = fmaxf(hy, sib.b.x); hz = fmaxf(hz, sib.b.y);
+    } else {
+      lx = fminf(sib.a.x, lx); ly = fminf(sib.a.y, ly); lz = fminf(sib.a.z, lz);
+      hx = fmaxf(sib.a.w, hx); hy = fmaxf(sib.b.x, hy); hz = fmaxf(sib.b.y, hz);
+    }
+    nodes[p] = make_node(lx, ly, lz, hx, hy, hz, pa);
     i = p;
   }
 }
