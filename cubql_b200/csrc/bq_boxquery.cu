@@ -354,8 +354,10 @@ int box_query_order(const Node *nodes, const bq_box3f *queryBoxes, uint32_t nq, 
   }
   BQ_CUDA(cudaGetLastError());
   int sel = 0;
-  // the order only steers performance: the top 24 key bits (3 passes) suffice
-  BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, 6, 30, nullptr, &sel, err, al));
+  // the order only steers performance: the top 24 key bits (3 passes)
+  // suffice; up to 2M queries the top 16 (2 passes) do as well
+  const int loBit = nq <= (1u << 21) ? 14 : 6;
+  BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, loBit, 30, nullptr, &sel, err, al));
   *order = idx[sel];
   return BQ_OK;
 }

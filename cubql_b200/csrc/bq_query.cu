@@ -263,8 +263,10 @@ int prepare_queries(const float *rootBox, const float *queries, uint32_t nq, boo
     }
     BQ_CUDA(cudaGetLastError());
     int sel = 0;
-    // the order only steers performance: the top 24 key bits (3 passes) suffice
-    BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, 6, 30, nullptr, &sel, qs.err, al));
+    // the order only steers performance: the top 24 key bits (3 passes)
+    // suffice; up to 2M queries the top 16 (2 passes) do as well
+    const int loBit = nq <= (1u << 21) ? 14 : 6;
+    BQ_TRY(onesweep_sort_u32(keys, idx, nq, nullptr, loBit, 30, nullptr, &sel, qs.err, al));
     qs.order = idx[sel];
   }
   return BQ_OK;
