@@ -3,28 +3,32 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Headline workload (the 10M-point configuration): a step is one Morton
-(radix, 63-bit) BVH build, leaf threshold 1, over 10,000,000 uniformly
-distributed points (seeded, U[0,1]^3), inputs already in HBM.  `value` is
-build throughput in Mprims/s summed over ranks (each rank builds its own
-10M-point set: weak scaling, no data-path collective).  The line also
-carries, measured in the same run:
+Headline workload (the 10M-point configuration): a step is one BVH build,
+leaf threshold 1, over 10,000,000 uniformly distributed points (seeded,
+U[0,1]^3), inputs already in HBM.  Ours is the Morton (radix, 63-bit)
+builder; `value` is build throughput in Mprims/s summed over ranks (each
+rank builds its own 10M-point set: weak scaling, no data-path collective).
+The line also carries, measured in the same run:
   * e2e        the same build through the public API from pinned host
                boxes, the tree copied back to host every step;
   * roofline   for the dominant kernel (CUDA events on the library's own
                stream via the libbq phase profiler), against the measured
-               HBM copy bandwidth;
+               HBM copy bandwidth, and for every component below;
   * components spatial-median build, 10M closest-point and 10M kNN(k=16)
-               queries, triangle-mesh distance forward+adjoint, the
-               reference's own GPU kernels compiled for sm_100a;
-  * cpu_baseline the reference's host builder (cpuBuilder) on a 1M-point
-               sample, one core.
+               queries on uniform and Gaussian-mixture points,
+               triangle-mesh distance forward+adjoint, the batched
+               configurations; the reference's own GPU kernels compiled
+               for sm_100a are timed on the same inputs by the reference arm;
+  * cpu_baseline the reference's host builder (cpuBuilder) on the same 10M
+               points, one core.
 Inputs (240 MB of boxes) are larger than the 126 MB L2, so no flush is
 needed between steps.
 
---impl reference times the reference's CPU build path on this host with
-all cores (concurrent cpuBuilder builds of a 1M-point sample) and prints
-the same metric.
+--impl reference times the reference's own CPU build path (cpuBuilder,
+compiled from the reference's sources into oracle/_ref) on this host with
+all cores: every step runs one concurrent 10M-point build per host thread.
+It prints the same metric and config, and never loads this repository's
+library.
 """
 import argparse
 import json
@@ -140,15 +144,32 @@ def barrier(world):
 # ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
+def workloads():
+    """cubql_b200/workloads.py loaded by path: the seeded generators, without
+    the package (whose import loads libbq.so)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bq_workloads", os.path.join(ROOT, "cubql_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def bench_config(n, seed):
+    """The workload both arms run (identical in both lines)."""
+    return {"workload": f"BVH build, leaf threshold 1, over {n} uniform points U[0,1]^3 (seeded)",
+            "points_per_gpu": n, "seed": seed,
+            "l2": "inputs (240 MB boxes per GPU) larger than the 126 MB L2; no flush"}
+
+
 def run_reference(args):
     rank, world, _ = dist_info()
     if rank != 0:
         return
-    from cubql_b200 import workloads as W
+    W = workloads()
     from oracle.oracle import RefCPU, have_ref_cpu, Oracle
-    sample = 1_000_000
-    boxes = W.point_boxes(W.uniform_points(sample))
-    threads = os.cpu_count() or 1
+    n = args.n
+    boxes = W.point_boxes(W.uniform_points(n, W.SEED_DATA))
+    threads = max(1, min(os.cpu_count() or 1, 16))
     if have_ref_cpu():
         r = RefCPU()
         kind = "reference"
@@ -162,18 +183,18 @@ def run_reference(args):
         run()
     secs = [run() for _ in range(args.steps)]
     t = sum(secs) / len(secs)
-    value = threads * sample / t / 1e6
+    value = threads * n / t / 1e6
+    sample = f"{threads} concurrent cpuBuilder builds (spatial median, leaf 1) of all {n} points per step"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mprims/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "Morton-order BVH build of uniform points U[0,1]^3 (reference: host cpuBuilder, "
-                                   "spatial median, leaf 1)", "points": sample, "sample_of": args.n,
-                       "parallelism": f"{threads} concurrent host builds"},
-            "cpu_baseline": {"value": value, "unit": "Mprims/s", "cores": threads, "kind": kind,
-                             "sample": f"{threads} concurrent cpuBuilder builds of {sample} uniform points per step"},
+            "config": bench_config(n, W.SEED_DATA),
+            "impl_detail": {"builder": "reference cpuBuilder (host, single-threaded by design), one build per "
+                                       "host thread", "threads": threads},
+            "cpu_baseline": {"value": value, "unit": "Mprims/s", "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "Mprims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if not args.no_components:
-        line["reference_components"] = reference_components(W, args.n)
+        line["reference_components"] = reference_components(W, n)
     print(json.dumps(line))
 
 
@@ -188,14 +209,27 @@ def reference_components(W, n):
     reference_gpu(comp, pts_np, W)
     comp["c1_reference"] = c1_reference(W, pts_np)
     if have_ref_gpu():
+        r = RefGPU()
         verts, tris = W.icosphere(8)
         tv = verts[tris]
         tbox = np.concatenate([tv.min(1), tv.max(1)], 1).astype(np.float32)
         comp["sah_build_triangles"] = {"triangles": int(len(tris)),
-                                       "reference_sahBuilder_ms": RefGPU().time_build_boxes(RefGPU.SAH, tbox, 0,
-                                                                                           reps=2),
-                                       "reference_gpuBuilder_elh_ms": RefGPU().time_build_boxes(RefGPU.ELH, tbox, 0,
-                                                                                               reps=2)}
+                                       "reference_sahBuilder_ms": r.time_build_boxes(RefGPU.SAH, tbox, 0, reps=2),
+                                       "reference_gpuBuilder_elh_ms": r.time_build_boxes(RefGPU.ELH, tbox, 0,
+                                                                                        reps=2)}
+        tq = W.uniform_points(4_000_000, W.SEED_QUERIES, -1.5, 1.5)
+        comp["triangle_distance"] = {"triangles": int(len(tris)), "queries": int(len(tq)),
+                                     "reference_findClosest_ms": r.time_tri(RefGPU.RADIX, tris, verts, tq, reps=2),
+                                     "note": "reference triangles::findClosest kernel, one thread per query, over "
+                                             "its radixBuilder tree of the triangle boxes (build not timed)"}
+        del tq
+        g = W.gmm_points(n)
+        gq = W.gmm_points(n, sample_seed=W.SEED_GMM_QUERIES)
+        comp["gmm10m"] = {"points": n, "queries": n,
+                          "reference_radixBuilder_ms": r.time_build(RefGPU.RADIX, g, 0, reps=2),
+                          "reference_gpuBuilder_leaf8_ms": r.time_build(RefGPU.SPATIAL_MEDIAN, g, 8, reps=2),
+                          "reference_findClosest_ms": r.time_query(RefGPU.RADIX, g, gq, 0, reps=2),
+                          "reference_findKNN16_ms": r.time_query(RefGPU.RADIX, g, gq, 16, reps=2)}
     return comp
 
 
@@ -274,6 +308,51 @@ PHASE_BYTES = {
 }
 
 
+def hbm_frac(nbytes, ms, peak):
+    gbs = nbytes / ms / 1e6
+    return {"bound": "hbm", "alg_bytes": int(nbytes), "achieved": gbs, "peak": peak, "unit": "GB/s",
+            "frac": gbs / peak}
+
+
+def query_roofline(counts, nq, out_bytes, prim_bytes, ms, peak, compulsory):
+    """Touched bytes of a traversal batch from its visit counts: 64 B per
+    inner node expanded (both 32-byte children), 16 B per admin load,
+    prim_bytes per prim tested, and each query's input (12 B) and output;
+    beside it the compulsory bytes (every input and the tree read once)."""
+    touched = 64 * counts["inner_nodes"] + 16 * counts["admin_loads"] + prim_bytes * counts["prims"] + \
+        nq * (12 + out_bytes)
+    r = hbm_frac(touched, ms, peak)
+    r.update({"model": "touched bytes B_t (mostly served from L1/L2, so frac may exceed 1)",
+              "visit_counts": counts, "compulsory_bytes": int(compulsory),
+              "compulsory_frac": compulsory / ms / 1e6 / peak})
+    return r
+
+
+def morton_build_bytes(n, num_nodes):
+    """The fixed accounting model of a Morton build: 288 B per prim + 64 B per node."""
+    return 288 * n + 64 * num_nodes
+
+
+def open_prim_levels(nodes_f32):
+    """Sum over levels of the prims still in open (inner) nodes: the sum of
+    the prim counts of all inner nodes, from the tree's admin words."""
+    import numpy as np
+    adm = nodes_f32.view(np.uint64).reshape(-1, 4)[:, 3]
+    cnt = (adm >> np.uint64(48)).astype(np.int64)
+    off = (adm & np.uint64(0xFFFFFFFFFFFF)).astype(np.int64)
+    size = np.where(cnt > 0, cnt, 0)
+    # parents before children is not guaranteed: iterate until sizes settle (depth passes)
+    inner = np.nonzero(cnt == 0)[0]
+    inner = inner[inner != 1]
+    for _ in range(200):
+        new = size.copy()
+        new[inner] = size[off[inner]] + size[off[inner] + 1]
+        if np.array_equal(new, size):
+            break
+        size = new
+    return int(size[inner].sum())
+
+
 def components(bq, W, torch, pts_np, tp, boxes_t, comp):
     import numpy as np
     n = len(pts_np)
@@ -295,8 +374,16 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
     def smb():
         bq.gpuBuilder(boxes_t, bq.BuildConfig(makeLeafThreshold=8)).free()
     ms = ev_time(smb)
+    peak, _ = hbm_peak()
+    smt = bq.gpuBuilder(boxes_t, bq.BuildConfig(makeLeafThreshold=8))
+    sm_nodes = smt.nodes_tensor().cpu().numpy()
+    smt.free()
+    a_sum = open_prim_levels(sm_nodes)
     comp["spatial_median_build"] = {"ms": ms, "Mprims_s": n / ms / 1e3, "leaf": 8,
-                                    "vs_published_reference_13ms": 13.0 / ms}
+                                    "vs_published_reference_13ms": 13.0 / ms,
+                                    "roofline": dict(hbm_frac(n * (24 + 28) + 40 * a_sum + 64 * len(sm_nodes), ms, peak),
+                                                     model="N*(24+28) + sum_levels A_l*(24+8+8) + 64*M",
+                                                     sum_levels_open_prims=a_sum, nodes=len(sm_nodes))}
     with bq.profile() as prof:
         smb()
     comp["spatial_median_build"]["phases_ms"] = {k: round(v[1], 4) for k, v in prof.table.items()}
@@ -318,13 +405,31 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
     bvh = bq.cuda.radixBuilder(boxes_t)
     qs = torch.from_numpy(W.uniform_points(n, W.SEED_QUERIES)).cuda()
     ms = ev_time(lambda: bq.points.findClosest(bvh, tp, qs))
-    comp["closest_point"] = {"ms": ms, "Mqueries_s": n / ms / 1e3, "queries": n}
+    nn = bvh.numNodes
+    cpc = bq.points.visitCounts(bvh, tp, qs, 0)
+    comp["closest_point"] = {"ms": ms, "Mqueries_s": n / ms / 1e3, "queries": n,
+                             "roofline": query_roofline(cpc, n, 8, 16, ms, peak, n * 20 + 32 * nn + 16 * n)}
     ms = ev_time(lambda: bq.points.findKNN(bvh, tp, qs, 16))
-    comp["knn16"] = {"ms": ms, "Mqueries_s": n / ms / 1e3, "queries": n, "k": 16}
+    knc = bq.points.visitCounts(bvh, tp, qs, 16)
+    comp["knn16"] = {"ms": ms, "Mqueries_s": n / ms / 1e3, "queries": n, "k": 16,
+                     "roofline": query_roofline(knc, n, 8 * 16 + 4, 16, ms, peak, n * (12 + 132) + 32 * nn + 16 * n)}
     with bq.profile() as prof:
         bq.points.findClosest(bvh, tp, qs)
         bq.points.findKNN(bvh, tp, qs, 16)
     comp["query_phases_ms"] = {k: round(v[1], 4) for k, v in prof.table.items()}
+    # the single-tree autotuner's launch shape for the same workloads (build + query)
+    from cubql_b200 import tuning
+    for name, kk in (("closest_point", 0), ("knn16", 16)):
+        t = tuning.tuned_query(boxes_t, tp, qs, kk)
+        tcfg = bq.BuildConfig(makeLeafThreshold=t["makeLeafThreshold"])
+        tt = bq.cuda.radixBuilder(boxes_t, tcfg)
+        qc = tuning.query_config_of(t)
+        run = (lambda: bq.points.findClosest(tt, tp, qs, qcfg=qc)) if kk == 0 else \
+            (lambda: bq.points.findKNN(tt, tp, qs, kk, qcfg=qc))
+        ms_t = ev_time(run)
+        tt.free()
+        comp[name]["tuned"] = {k: v for k, v in t.items() if k != "key"}
+        comp[name]["tuned_query_ms"] = ms_t
     # wide trees: gpuBuilder(WideBVH<float,3,W>) with the default config (leaf 1) and closest point
     for width in (4, 8):
         ms_b = ev_time(lambda: bq.gpuBuilderWide(boxes_t, width).free())
@@ -394,9 +499,23 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
                 qq[:, a] += s
                 bq.triangles.findClosest(tb, tt, tv, qq)
     ms_fd = ev_time(fd, reps=2)
-    comp["triangle_distance"] = {"triangles": int(len(tris)), "queries": int(len(tq)), "forward_ms": ms_f,
-                                 "backward_ms": ms_b, "fwd_bwd_queries_s": len(tq) / (ms_f + ms_b) * 1e3,
-                                 "forward_plus_fd_ms": ms_fd, "speedup_vs_forward_plus_fd": ms_fd / (ms_f + ms_b)}
+    nq, nv, nt = len(tq), len(verts), len(tris)
+    trc = bq.triangles.visitCounts(tb, tt, tv, tq)
+    # forward: per triangle tested its id (4), index triple (12) and 3 vertices (36); output id, sqrDist, P
+    fwd_roof = query_roofline(trc, nq, 20, 52, ms_f, peak, nq * 32 + 32 * tb.numNodes + 52 * nt)
+    # adjoint: pairs kernel (q, id, g, triangle, vertices read; gradQ, 3 keys, 3 values, 3 contributions written),
+    # 3 sort passes of the 3Q (u32, u32) pairs + histogram, the reduce (sorted pairs, contributions) and gradV
+    bwd_bytes = nq * (12 + 4 + 4 + 12 + 36 + 12 + 12 + 12 + 36) + 3 * nq * (3 * 16 + 4) + 3 * nq * (8 + 12) + 12 * nv
+    comp["triangle_distance"] = {"triangles": int(nt), "queries": int(nq), "forward_ms": ms_f,
+                                 "backward_ms": ms_b, "fwd_bwd_queries_s": nq / (ms_f + ms_b) * 1e3,
+                                 "forward_plus_fd_ms": ms_fd, "speedup_vs_forward_plus_fd": ms_fd / (ms_f + ms_b),
+                                 "fd_baseline": "forward + central differences of the query coordinates only "
+                                                "(7 forwards); a vertex-gradient FD would need 6 forwards per "
+                                                "vertex, so the ratio is against the cheaper baseline",
+                                 "forward_roofline": fwd_roof,
+                                 "backward_roofline": dict(hbm_frac(bwd_bytes, ms_b, peak),
+                                                           model="pairs kernel 140 B/query + 3 sort passes and a "
+                                                                 "histogram of 3Q pairs + reduce 60 B/query + 12 B/vertex")}
     tb.free()
 
 
@@ -411,6 +530,40 @@ def _ev_time(torch, fn, reps=3, warm=1):
     b.record()
     torch.cuda.synchronize()
     return a.elapsed_time(b) / reps
+
+
+def gmm_component(bq, W, torch, comp, n):
+    """The 10M-point Gaussian-mixture configuration (64 components, sigma
+    log-uniform in [1e-4, 1e-1], coordinates offset by 1e5: many exact
+    duplicates and long runs of equal Morton keys): Morton and
+    spatial-median (leaf 8) builds, then 10M closest-point and 10M kNN(16)
+    queries drawn from the same mixture."""
+    peak, _ = hbm_peak()
+    pts = torch.from_numpy(W.gmm_points(n)).cuda()
+    qs = torch.from_numpy(W.gmm_points(n, sample_seed=W.SEED_GMM_QUERIES)).cuda()
+    boxes = bq.points_to_boxes(pts)
+    ms_m = _ev_time(torch, lambda: bq.cuda.radixBuilder(boxes).free())
+    with bq.profile() as prof:
+        bq.cuda.radixBuilder(boxes).free()
+    ms_s = _ev_time(torch, lambda: bq.gpuBuilder(boxes, bq.BuildConfig(makeLeafThreshold=8)).free())
+    bvh = bq.cuda.radixBuilder(boxes)
+    nn = bvh.numNodes
+    ms_cp = _ev_time(torch, lambda: bq.points.findClosest(bvh, pts, qs), reps=2)
+    ms_knn = _ev_time(torch, lambda: bq.points.findKNN(bvh, pts, qs, 16), reps=2)
+    cpc = bq.points.visitCounts(bvh, pts, qs, 0)
+    knc = bq.points.visitCounts(bvh, pts, qs, 16)
+    bvh.free()
+    comp["gmm10m"] = {
+        "points": n, "queries": n,
+        "morton_build_ms": ms_m, "morton_build_Mprims_s": n / ms_m / 1e3,
+        "morton_build_roofline": dict(hbm_frac(morton_build_bytes(n, nn), ms_m, peak), model="288 N + 64 M"),
+        "morton_phases_ms": {k: round(v[1], 4) for k, v in prof.table.items()},
+        "spatial_median_leaf8_ms": ms_s, "spatial_median_Mprims_s": n / ms_s / 1e3,
+        "closest_point_ms": ms_cp, "closest_point_Mqueries_s": n / ms_cp / 1e3,
+        "closest_point_roofline": query_roofline(cpc, n, 8, 16, ms_cp, peak, n * 20 + 32 * nn + 16 * n),
+        "knn16_ms": ms_knn, "knn16_Mqueries_s": n / ms_knn / 1e3,
+        "knn16_roofline": query_roofline(knc, n, 132, 16, ms_knn, peak, n * 144 + 32 * nn + 16 * n)}
+    del pts, qs, boxes
 
 
 def c1_component(bq, W, torch, comp, pts_np, tp, boxes_t):
@@ -473,19 +626,25 @@ def batched_components(bq, W, torch, comp):
     b = torch.from_numpy(W.point_boxes(pts)).cuda()
     tp, tq = torch.from_numpy(pts).cuda(), torch.from_numpy(qs).cuda()
     toff, tqoff = torch.from_numpy(off).cuda().int(), torch.from_numpy(qoff).cuda().int()
+    # launch shape from the autotuner (JSON cache; tuned here on a cache miss, untimed)
+    from cubql_b200 import tuning
+    tuned = tuning.tuned_batched_knn(b, tp, toff, tq, tqoff, 16)
+    bcfg = bq.BuildConfig(makeLeafThreshold=tuned["makeLeafThreshold"])
+    qcfg = tuning.query_config_of(tuned)
     side = torch.cuda.Stream()
     side.wait_stream(torch.cuda.current_stream())
     with torch.cuda.stream(side):  # first use of the stream-ordered pool, outside the capture
-        bq.batched_knn(bq.Batch(b, toff, stream_alloc_null=True), tp, toff, tq, tqoff, 16, stream_alloc_null=True)
+        bq.batched_knn(bq.Batch(b, toff, bcfg, stream_alloc_null=True), tp, toff, tq, tqoff, 16, qcfg=qcfg,
+                       stream_alloc_null=True)
     torch.cuda.current_stream().wait_stream(side)
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph):
-        gbatch = bq.Batch(b, toff, stream_alloc_null=True)
-        gout = bq.batched_knn(gbatch, tp, toff, tq, tqoff, 16, stream_alloc_null=True)
+        gbatch = bq.Batch(b, toff, bcfg, stream_alloc_null=True)
+        gout = bq.batched_knn(gbatch, tp, toff, tq, tqoff, 16, qcfg=qcfg, stream_alloc_null=True)
     ms_graph = _ev_time(torch, graph.replay)
-    ms_build = _ev_time(torch, lambda: bq.Batch(b, toff))
-    bat = bq.Batch(b, toff)
-    ms_query = _ev_time(torch, lambda: bq.batched_knn(bat, tp, toff, tq, tqoff, 16))
+    ms_build = _ev_time(torch, lambda: bq.Batch(b, toff, bcfg))
+    bat = bq.Batch(b, toff, bcfg)
+    ms_query = _ev_time(torch, lambda: bq.batched_knn(bat, tp, toff, tq, tqoff, 16, qcfg=qcfg))
 
     def loop():
         for c in range(len(off) - 1):
@@ -495,7 +654,9 @@ def batched_components(bq, W, torch, comp):
             t.free()
     ms_loop = _ev_time(torch, loop, reps=1, warm=1)
     same = True
-    for c in (0, len(off) // 2, len(off) - 2):  # spot check: batched answers == per-cloud answers
+    graph.replay()
+    torch.cuda.synchronize()
+    for c in range(len(off) - 1):  # every cloud: batched answers == per-cloud answers
         sl, ql = slice(int(off[c]), int(off[c + 1])), slice(int(qoff[c]), int(qoff[c + 1]))
         t = bq.cuda.radixBuilder(b[sl])
         si, sd, _ = bq.points.findKNN(t, tp[sl], tq[ql], 16)
@@ -507,7 +668,8 @@ def batched_components(bq, W, torch, comp):
         "graph_ms": ms_graph, "build_ms": ms_build, "query_ms": ms_query,
         "Mqueries_s": nq / ms_graph / 1e3, "build_Mprims_s": n / ms_build / 1e3,
         "per_cloud_loop_ms": ms_loop, "speedup_vs_per_cloud_loop": ms_loop / ms_graph,
-        "matches_per_cloud_answers": same}
+        "matches_per_cloud_answers": same, "clouds_compared": len(off) - 1,
+        "tuned": {k: v for k, v in tuned.items() if k != "key"}, "tuning_key": tuned["key"]}
     del b, tp, tq, bat, gbatch, gout
 
     verts, tris, toffm, qsm, qoffm = W.mesh_batch()
@@ -518,26 +680,30 @@ def batched_components(bq, W, torch, comp):
     g = torch.full((len(qsm),), 1.0 / len(qsm), device="cuda")
     state = {"v": tv}
 
-    def step():
+    def step(check=False):
         v = state["v"]
         boxes = bq.triangles.boxes(tt, v)
         bq.batched_refit(batch, boxes)
         ids, d, _ = bq.batched_tri_closest(batch, tt, v, tqm, qoff_t)
+        ok = True
+        if check:  # the refitted trees' forward against trees rebuilt from scratch
+            fresh = bq.Batch(boxes, toff_t)
+            fi, fd, _ = bq.batched_tri_closest(fresh, tt, v, tqm, qoff_t)
+            ok = bool(torch.equal(ids, fi) and torch.equal(d, fd))
+            del fresh
         _, gv = bq.triangles.distanceBackward(tt, v, tqm, ids, g)
         state["v"] = v - 0.5 * gv
-        return ids, d
-    ms_step = _ev_time(torch, step, reps=100, warm=3)
-    # the refitted trees against trees rebuilt from scratch, at the current vertices
-    v = state["v"]
-    boxes = bq.triangles.boxes(tt, v)
-    bq.batched_refit(batch, boxes)
-    ids2, d2, _ = bq.batched_tri_closest(batch, tt, v, tqm, qoff_t)
-    fresh = bq.Batch(boxes, toff_t)
-    fi, fd, _ = bq.batched_tri_closest(fresh, tt, v, tqm, qoff_t)
+        return ok
+
+    steps = 100
+    # untimed run: every step's forward checked against a rebuild
+    all_equal = all([step(check=True) for _ in range(steps)])
+    state["v"] = tv  # the timed run repeats the same 100 steps from the same vertices
+    ms_step = _ev_time(torch, step, reps=steps, warm=0)
     comp["fit_loop_128_meshes"] = {
-        "meshes": len(toffm) - 1, "triangles": int(len(tris)), "queries_per_step": int(len(qsm)), "steps": 100,
+        "meshes": len(toffm) - 1, "triangles": int(len(tris)), "queries_per_step": int(len(qsm)), "steps": steps,
         "ms_per_step": ms_step, "fwd_bwd_queries_s": len(qsm) / ms_step * 1e3,
-        "refit_forward_equals_rebuild": bool(torch.equal(ids2, fi) and torch.equal(d2, fd))}
+        "refit_forward_equals_rebuild": all_equal, "steps_checked": steps}
 
 
 BOX_HALF = 0.00585
@@ -665,6 +831,7 @@ def run_ours(args):
     if rank == 0 and not args.no_components:
         components(bq, W, torch, pts_np, tp, boxes_t, comp)
         c1_component(bq, W, torch, comp, pts_np, tp, boxes_t)
+        gmm_component(bq, W, torch, comp, n)
         batched_components(bq, W, torch, comp)
     if rank == 0:
         cpu_baseline = cpu_leg(W, pts_np)
@@ -673,9 +840,9 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": "Mprims/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "Morton (radix, 63-bit) BVH build over uniform points U[0,1]^3, leaf 1",
-                           "points_per_gpu": n, "seed": W.SEED_DATA, "parallelism": f"{world} independent builds",
-                           "l2": "inputs (240 MB boxes per GPU) larger than the 126 MB L2; no flush"},
+                "config": bench_config(n, W.SEED_DATA),
+                "impl_detail": {"builder": "Morton (radix, 63-bit) builder, C ABI bq_build_morton63_f3",
+                                "parallelism": f"{world} independent builds, one per GPU"},
                 "e2e": e2e, "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu_baseline,
                 "gpu_launches": int(round(launches_per_step * args.steps)), "clocks": clk, "components": comp}
         print(json.dumps(line))
@@ -737,9 +904,10 @@ def e2e_pipelined(bq, torch, boxes_np, n, steps, warmup, world):
 
 
 def cpu_leg(W, pts_np):
+    """The reference's host builder on the benchmark's own points (all of
+    them), one core: the median of 3 builds."""
     from oracle.oracle import Oracle, RefCPU, have_ref_cpu
-    sample = 1_000_000
-    boxes = W.point_boxes(pts_np[:sample])
+    boxes = W.point_boxes(pts_np)
     if have_ref_cpu():
         r = RefCPU()
         kind = "reference"
@@ -748,11 +916,10 @@ def cpu_leg(W, pts_np):
         o = Oracle()
         kind = "port"
         fn = lambda: o.cpu_build(boxes, 0)  # noqa: E731
-    fn()
     secs = [_timed(fn) for _ in range(3)]
     t = statistics.median(secs)
-    return {"value": sample / t / 1e6, "unit": "Mprims/s", "cores": 1, "kind": kind,
-            "sample": f"cpuBuilder (spatial median, leaf 1) over the first {sample} of the benchmark's points, "
+    return {"value": len(pts_np) / t / 1e6, "unit": "Mprims/s", "cores": 1, "kind": kind,
+            "sample": f"cpuBuilder (spatial median, leaf 1) over all {len(pts_np)} benchmark points, "
                       f"median of 3 builds, {t:.3f} s each"}
 
 

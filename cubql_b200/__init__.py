@@ -133,6 +133,10 @@ _SIGS = {
     "bq_tri_closest_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _P, _U, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
                           ctypes.POINTER(bq_allocator), _P],
     "bq_tri_distance_bwd_f3": [_P, _P, _U, _P, _U, _P, _P, _P, _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_query_visit_counts_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _U, _I, _F, ctypes.POINTER(bq_query_config),
+                                 ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(bq_allocator), _P],
+    "bq_tri_visit_counts_f3": [ctypes.POINTER(bq_bvh3f), _P, _P, _P, _U, _F, ctypes.POINTER(bq_query_config),
+                               ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(bq_allocator), _P],
     "bq_batched_build_morton63_f3": [_P, _P, _U, _U, ctypes.POINTER(bq_build_config), _P, _P, _P, _P,
                                      ctypes.POINTER(bq_allocator), _P],
     "bq_batched_knn_f3": [_P, _P, _P, _P, _P, _U, _U, _I, _F, ctypes.POINTER(bq_query_config), _P, _P, _P, _P,
@@ -141,11 +145,13 @@ _SIGS = {
     "bq_batched_tri_closest_f3": [_P, _P, _P, _P, _P, _P, _U, _U, _F, ctypes.POINTER(bq_query_config), _P, _P, _P,
                                   _P, ctypes.POINTER(bq_allocator), _P],
     "bq_autotune_batched_knn_f3": [_P, _P, _P, _U, _U, _P, _P, _U, _I, _P, ctypes.POINTER(bq_allocator), _P],
+    "bq_autotune_query_f3": [_P, _P, _U, _P, _U, _I, _P, ctypes.POINTER(bq_allocator), _P],
     "bq_tri_boxes_f3": [_P, _P, _U, _P, _P],
     "bq_points_to_boxes_f3": [_P, _U, _P, _P],
     "bq_load_binary": [ctypes.c_char_p, ctypes.c_size_t, _P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)],
     "bq_save_binary": [ctypes.c_char_p, _P, ctypes.c_uint64, ctypes.c_size_t],
     "bq_load_points_f64_as_f32": [ctypes.c_char_p, _I, _P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)],
+    "bq_debug_inject_sort_timeout": [_I],
     "bq_last_error_string": [],
     "bq_version": [],
     "bq_profile_enable": [_I],
@@ -489,6 +495,21 @@ class points:
                               _ptr(ids), _ptr(d), _ptr(nf), ctypes.byref(bvh.allocator.c), _stream()))
         return ids, d, nf
 
+    @staticmethod
+    def visitCounts(bvh, data, queries, k=0, maxSqrDist=float("inf"), qcfg=None):
+        """Traversal visit counts of findClosest (k == 0) or findKNN (k > 0)
+        over the queries, as the reference's buildQual / checkBuilders
+        traversal-step counters: dict with the inner nodes expanded (two
+        32-byte children loaded each), the node admin words loaded (16 B) and
+        the prims tested."""
+        data, queries = _vec3(data, "points"), _vec3(queries, "queries")
+        out = (ctypes.c_uint64 * 3)()
+        q = qcfg or query_config()
+        _check(_lib.bq_query_visit_counts_f3(ctypes.byref(bvh.c), _ptr(data), _ptr(queries), queries.shape[0], k,
+                                             maxSqrDist, ctypes.byref(q), out, ctypes.byref(bvh.allocator.c),
+                                             _stream()))
+        return {"inner_nodes": out[0], "admin_loads": out[1], "prims": out[2]}
+
 
 class fixedBoxQuery:
     """cuBQL::fixedBoxQuery::forEachPrim (cuBQL/traversal/fixedBoxQuery.h:143-156)
@@ -592,6 +613,18 @@ class triangles:
                                       _ptr(queries), nq, maxSqrDist, ctypes.byref(q), _ptr(ids), _ptr(d), _ptr(P),
                                       ctypes.byref(bvh.allocator.c), _stream()))
         return ids, d, P
+
+    @staticmethod
+    def visitCounts(bvh, tris, verts, queries, maxSqrDist=float("inf"), qcfg=None):
+        """Traversal visit counts of findClosest over the queries (see
+        points.visitCounts); 'prims' counts triangles tested."""
+        queries = _vec3(queries, "queries")
+        out = (ctypes.c_uint64 * 3)()
+        q = qcfg or query_config()
+        _check(_lib.bq_tri_visit_counts_f3(ctypes.byref(bvh.c), _ptr(tris.contiguous()), _ptr(verts.contiguous()),
+                                           _ptr(queries), queries.shape[0], maxSqrDist, ctypes.byref(q), out,
+                                           ctypes.byref(bvh.allocator.c), _stream()))
+        return {"inner_nodes": out[0], "admin_loads": out[1], "prims": out[2]}
 
     @staticmethod
     def distanceBackward(tris, verts, queries, ids, gradSqr, allocator=None):

@@ -114,6 +114,7 @@ struct AggArgsT {
   uint2 *pending;         // 2 per chunk: nodes handed to the global phase
   const uint32_t *off;    // SEG: cloud offsets
   uint32_t numSegs;
+  const uint32_t *skipIf = nullptr;  // optional: both phases do nothing while *skipIf != 0
 };
 using AggArgs = AggArgsT<uint8_t>;
 
@@ -126,6 +127,7 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
   const uint32_t nv = *a.nvPtr;
   const uint32_t c0 = blockIdx.x * AGG_CHUNK;
   if (c0 >= nv) return;  // whole CTA: no barrier below is skipped by part of it
+  if (a.skipIf && *a.skipIf) return;  // whole CTA, as above
   const uint32_t cEnd = c0 + AGG_CHUNK;  // first split position outside the chunk
   for (int j = threadIdx.x; j <= AGG_CHUNK; j += blockDim.x) sSlot[j] = AGG_EMPTY;
   for (int j = threadIdx.x; j < AGG_CHUNK + 2; j += blockDim.x) {
@@ -192,6 +194,7 @@ __global__ void k_agg_global(AggArgsT<LevT> a, uint32_t numPending)
 {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numPending) return;
+  if (a.skipIf && *a.skipIf) return;  // the local phase did nothing either
   const uint32_t nv = *a.nvPtr;
   if ((uint64_t)(t / 2) * AGG_CHUNK >= nv) return;  // chunk had no prims: entry never written
   const uint2 pr = a.pending[t];

@@ -8,7 +8,7 @@ namespace bq {
 int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
 int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
 int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_config *cfg, Alloc &al);
-int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al);
+int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al, bool check);
 int box_query_count(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t nq,
                     uint32_t *counts, Alloc &al);
 int box_query_fill(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_box3f *queryBoxes, uint32_t nq,
@@ -40,6 +40,10 @@ int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t
         const bq_query_config *qcfg, int32_t *ids, float *d, int32_t *numFound, Alloc &al);
 int tri_closest(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, const float *queries, uint32_t nq,
                 float maxSqr, const bq_query_config *qcfg, int32_t *ids, float *d, float *P, Alloc &al);
+int query_visit_counts(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, int k,
+                       float maxSqr, const bq_query_config *qcfg, uint64_t *hostCounts, Alloc &al);
+int tri_visit_counts(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, const float *queries, uint32_t nq,
+                     float maxSqr, const bq_query_config *qcfg, uint64_t *hostCounts, Alloc &al);
 int tri_distance_bwd(const int32_t *tris, const float *verts, uint32_t numVerts, const float *queries, uint32_t nq,
                      const int32_t *ids, const float *gradSqr, float *gradQ, float *gradV, Alloc &al);
 int tri_boxes(const int32_t *tris, const float *verts, uint32_t nt, bq_box3f *boxes, cudaStream_t s);
@@ -55,6 +59,8 @@ int batched_refit(const bq_bvh3f *bvhs, const uint32_t *off, uint32_t numSegs, u
 int batched_tri_closest(const bq_bvh3f *bvhs, const uint32_t *triOff, const int32_t *tris, const float *verts,
                         const float *queries, const uint32_t *qoff, uint32_t numSegs, uint32_t nq, float maxSqr,
                         const bq_query_config *qcfg, int32_t *ids, float *d, float *P, uint32_t *errOut, Alloc &al);
+int autotune_query(const bq_box3f *boxes, const float *points, uint32_t n, const float *queries, uint32_t nq, int k,
+                   bq_tuning *best, Alloc &al);
 int autotune_batched_knn(const bq_box3f *boxes, const float *points, const uint32_t *off, uint32_t numSegs,
                          uint32_t n, const float *queries, const uint32_t *qoff, uint32_t nq, int k, bq_tuning *best,
                          Alloc &al);
@@ -167,7 +173,7 @@ int bq_refit_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_allocator *
   BQ_TRY(check_tree(bvh));
   if (bvh->numNodes && !boxes) return set_error(BQ_ERR_INVALID_ARGUMENT, "boxes is NULL");
   Alloc al = make_alloc(alloc, stream);
-  return refit(bvh, boxes, al);
+  return refit(bvh, boxes, al, true);
 }
 
 int bq_free_f3(bq_bvh3f *bvh, const bq_allocator *alloc, bq_stream_t stream)
@@ -377,6 +383,29 @@ int bq_tri_closest_f3(const bq_bvh3f *bvh, const int32_t *tris, const float *ver
   return tri_closest(bvh, tris, verts, queries, numQueries, maxSqrDist, qcfg, ids, sqrDist, P, al);
 }
 
+int bq_query_visit_counts_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries,
+                             int k, float maxSqrDist, const bq_query_config *qcfg, uint64_t *counts,
+                             const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (!counts) return set_error(BQ_ERR_INVALID_ARGUMENT, "counts is NULL");
+  if (numQueries && (!queries || (bvh->numNodes && !points))) return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return query_visit_counts(bvh, points, queries, numQueries, k, maxSqrDist, qcfg, counts, al);
+}
+
+int bq_tri_visit_counts_f3(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, const float *queries,
+                           uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg, uint64_t *counts,
+                           const bq_allocator *alloc, bq_stream_t stream)
+{
+  BQ_TRY(check_tree(bvh));
+  if (!counts) return set_error(BQ_ERR_INVALID_ARGUMENT, "counts is NULL");
+  if (numQueries && (!queries || (bvh->numNodes && (!tris || !verts))))
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL array argument");
+  Alloc al = make_alloc(alloc, stream);
+  return tri_visit_counts(bvh, tris, verts, queries, numQueries, maxSqrDist, qcfg, counts, al);
+}
+
 int bq_tri_distance_bwd_f3(const int32_t *tris, const float *verts, uint32_t numVerts, const float *queries,
                            uint32_t numQueries, const int32_t *ids, const float *gradSqr, float *gradQueries,
                            float *gradVerts, const bq_allocator *alloc, bq_stream_t stream)
@@ -448,6 +477,14 @@ int bq_autotune_batched_knn_f3(const bq_box3f *boxes, const float *points, const
   Alloc al = make_alloc(alloc, stream);
   return autotune_batched_knn(boxes, points, segOffsets, numSegs, numPrims, queries, queryOffsets, numQueries, k,
                               best, al);
+}
+
+int bq_autotune_query_f3(const bq_box3f *boxes, const float *points, uint32_t numPrims, const float *queries,
+                         uint32_t numQueries, int k, bq_tuning *best, const bq_allocator *alloc, bq_stream_t stream)
+{
+  if (!boxes || !points || !queries || !best) return set_error(BQ_ERR_INVALID_ARGUMENT, "NULL argument");
+  Alloc al = make_alloc(alloc, stream);
+  return autotune_query(boxes, points, numPrims, queries, numQueries, k, best, al);
 }
 
 int bq_tri_boxes_f3(const int32_t *tris, const float *verts, uint32_t numTris, bq_box3f *boxes, bq_stream_t stream)

@@ -707,31 +707,31 @@ __global__ void k_collapse(const Node *__restrict__ full, const uint2 *__restric
 // low-bit order inside runs of equal top bits (after the top-bit sort)
 // ------------------------------------------------------------------
 namespace {
-// Orders the runs of equal top bits and writes every split level and slot.
+// Orders the runs of equal top bits of at most MB_THREAD_RUN prims and writes
+// every split level and slot (k_fix_runs); longer runs are listed in `runs`
+// and counted in *rs for long_runs.  Nothing waits here.
 template <int SB>
-int sort_low_bits(uint64_t *keys, uint32_t *ids, uint64_t *spareKeys, uint32_t *spareIds, uint32_t n,
-                  const uint32_t *nvDev, uint8_t *delta, uint32_t *slot, uint32_t *err, Alloc &al)
+int fix_runs(uint64_t *keys, uint32_t *ids, uint32_t n, const uint32_t *nvDev, uint8_t *delta, uint32_t *slot,
+             RunStats *rs, uint4 *runs, uint32_t maxRuns, Alloc &al)
 {
-  const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
-  TempSet tmp(al);
-  RunStats *rs = nullptr;
-  uint4 *runs = nullptr;
-  BQ_TRY(tmp.get(&rs, 1));
-  BQ_TRY(tmp.get(&runs, maxRuns));
   BQ_CUDA(cudaMemsetAsync(rs, 0, sizeof(RunStats), al.s));
-  {
-    ProfScope ps("morton.runs", al.s);
-    k_fix_runs<SB><<<div_up(n, FT_TILE), FT_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs, maxRuns);
-  }
-  RunStats h{};
-  BQ_CUDA(cudaMemcpyAsync(&h, rs, sizeof(h), cudaMemcpyDeviceToHost, al.s));
-  BQ_CUDA(cudaStreamSynchronize(al.s));
-  if (h.pad) return set_error(BQ_ERR_CUDA, "run list overflow in the Morton build");
+  ProfScope ps("morton.runs", al.s);
+  k_fix_runs<SB><<<div_up(n, FT_TILE), FT_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs, maxRuns);
+  BQ_CUDA(cudaGetLastError());
+  return BQ_OK;
+}
+
+// The runs longer than MB_THREAD_RUN (h: their statistics, read back).
+// Those holding differing keys get one stable sort of (run, low bits) over
+// just their prims, written back into each run's range; runs of identical
+// keys are already in order (the sort of the top bits is stable).  Then the
+// levels inside all of them.
+template <int SB>
+int long_runs(const RunStats &h, const uint4 *runs, uint64_t *keys, uint32_t *ids, uint64_t *spareKeys,
+              uint32_t *spareIds, uint8_t *delta, uint32_t *err, Alloc &al)
+{
   if (h.count == 0) return BQ_OK;
-  // runs longer than MB_THREAD_RUN.  Those holding differing keys get one
-  // stable sort of (run, low bits) over just their prims, written back into
-  // each run's range; runs of identical keys are already in order (the sort
-  // of the top bits is stable).  Then the levels inside all of them.
+  TempSet tmp(al);
   const uint32_t R = h.count, P = h.elems;
   uint32_t *off = nullptr, *mixed = nullptr, *rank = nullptr, *sizesM = nullptr, *offM = nullptr, *cnt = nullptr;
   uint4 *runsM = nullptr;
@@ -842,15 +842,48 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   uint64_t *keys = keys2[sel];
   uint32_t *ids = ids2[sel];
   uint32_t *idsOther = ids2[sel ^ 1];
-  s = wide4 ? sort_low_bits<MB_SB4>(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err, al)
-            : sort_low_bits<MB_SB3>(keys, ids, keys2[sel ^ 1], idsOther, n, &st->numValid, delta, slot, &st->err, al);
+  const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
+  RunStats *rs = nullptr;
+  uint4 *runs = nullptr;
+  if ((s = tmp.get(&rs, 1)) != BQ_OK || (s = tmp.get(&runs, maxRuns)) != BQ_OK) return fail(s);
+  s = wide4 ? fix_runs<MB_SB4>(keys, ids, n, &st->numValid, delta, slot, rs, runs, maxRuns, al)
+            : fix_runs<MB_SB3>(keys, ids, n, &st->numValid, delta, slot, rs, runs, maxRuns, al);
   if (s != BQ_OK) return fail(s);
   uint2 *pending = nullptr;
   if ((s = tmp.get(&pending, 2ull * div_up(n, AGG_CHUNK))) != BQ_OK) return fail(s);
   AggArgs ag{delta, slot, ids, boxes, nodes, nullptr, &st->numValid, nullptr, pending, nullptr, 0};
+  // what the host reads back: the long-run statistics, the valid count, the error word
+  struct { RunStats runs; uint32_t nv, err; } h = {};
+  auto read_back = [&]() -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(&h.runs, rs, sizeof(RunStats), cudaMemcpyDeviceToHost, al.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h.nv, &st->numValid, 4, cudaMemcpyDeviceToHost, al.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h.err, &st->err, 4, cudaMemcpyDeviceToHost, al.s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(al.s);
+    return e;
+  };
+  auto do_long_runs = [&]() -> int {
+    return wide4 ? long_runs<MB_SB4>(h.runs, runs, keys, ids, keys2[sel ^ 1], idsOther, delta, &st->err, al)
+                 : long_runs<MB_SB3>(h.runs, runs, keys, ids, keys2[sel ^ 1], idsOther, delta, &st->err, al);
+  };
   if (thr == 1) {
+    // Leaf 1: the agglomeration is queued at once and does nothing if long
+    // runs turn up (their levels are not written yet); then the one read
+    // back of the common case.  With long runs: their pass, the
+    // agglomeration again, a second read back.
+    ag.skipIf = &rs->count;
     if ((s = agglomerate<false>(ag, n, al.s, "morton.agg_local", "morton.agg_global")) != BQ_OK) return fail(s);
+    if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
+    if (h.runs.pad) return fail(set_error(BQ_ERR_CUDA, "run list overflow in the Morton build"));
+    if (h.runs.count) {
+      if ((s = do_long_runs()) != BQ_OK) return fail(s);
+      ag.skipIf = nullptr;
+      if ((s = agglomerate<false>(ag, n, al.s, "morton.agg_local", "morton.agg_global")) != BQ_OK) return fail(s);
+      if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
+    }
   } else {
+    if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
+    if (h.runs.pad) return fail(set_error(BQ_ERR_CUDA, "run list overflow in the Morton build"));
+    if ((s = do_long_runs()) != BQ_OK) return fail(s);
     Node *full = nullptr;
     uint2 *ranges = nullptr;
     uint32_t *kept = nullptr, *rank = nullptr, *total = nullptr;
@@ -876,11 +909,8 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
     k_collapse<<<div_up(n, 256), 256, 0, al.s>>>(full, ranges, kept, rank, &st->numValid, thr, nodes);
     if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_collapse"));
     if (hostNv > 0) bvh->numNodes = (uint32_t)numNodes;
+    if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
   }
-  struct { uint32_t nv, err; } h = {0, 0};
-  cudaMemcpyAsync(&h.nv, &st->numValid, 4, cudaMemcpyDeviceToHost, al.s);
-  cudaMemcpyAsync(&h.err, &st->err, 4, cudaMemcpyDeviceToHost, al.s);
-  if ((ce = cudaStreamSynchronize(al.s)) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
   if (h.err & DEV_ERR_TIMEOUT) return fail(set_error(BQ_ERR_TIMEOUT, "radix sort look-back timed out"));
   if (h.err) return fail(set_error(BQ_ERR_CUDA, "device-side range check failed in the Morton build"));
   al.free_bytes(idsOther);

@@ -232,6 +232,63 @@ void dispatch_knn_tie(int tie, int stack, const bq_bvh3f *bvh, const float *poin
     dispatch_knn_stack<K, TIE_LOWEST>(stack, bvh, points, queries, nq, k, maxSqr, block, ids, d, nf, qs, s);
 }
 
+// ------------------------------------------------------------------
+// visit counts (the measurement pass of the query rooflines): the same
+// traversal per query, in input order, counting node pairs loaded, admin
+// loads and prims tested.  A query whose 128-entry stack overflows
+// contributes what it visited until then.
+// ------------------------------------------------------------------
+template <int TIE, int K>
+__global__ void __launch_bounds__(128) k_visit_count(const Node *__restrict__ nodes,
+                                                     const uint32_t *__restrict__ primIDs,
+                                                     const float *__restrict__ points,
+                                                     const float *__restrict__ queries, uint32_t nq, int k,
+                                                     float maxSqr, unsigned long long *out)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  VisitCount vc;
+  uint32_t prims = 0;
+  if (t < nq) {  // no early return: every lane takes part in the warp sum below
+    const float *q = queries + 3ull * t;
+    LocalStack<128> st;
+    if constexpr (K == 0) {
+      CPLeaf<TIE> leaf{primIDs, points, __ldg(q), __ldg(q + 1), __ldg(q + 2), maxSqr, -1, -1, 0};
+      CountingLeaf<CPLeaf<TIE>> cl{leaf};
+      traverse_counted<TIE>(nodes, leaf.qx, leaf.qy, leaf.qz, maxSqr, st, cl, vc);
+      prims = cl.prims;
+    } else {
+      KnnLeaf<K, TIE> leaf;
+      leaf.primIDs = primIDs;
+      leaf.points = points;
+      leaf.qx = __ldg(q);
+      leaf.qy = __ldg(q + 1);
+      leaf.qz = __ldg(q + 2);
+      leaf.maxSqr = maxSqr;
+      leaf.list.init(k);
+      CountingLeaf<KnnLeaf<K, TIE>> cl{leaf};
+      traverse_counted<TIE>(nodes, leaf.qx, leaf.qy, leaf.qz, maxSqr, st, cl, vc);
+      prims = cl.prims;
+    }
+  }
+  add_visit_counts(vc.pairs, vc.admins, prims, out);
+}
+
+template <int TIE>
+void launch_visit_count(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, int k,
+                        float maxSqr, unsigned long long *out, cudaStream_t s)
+{
+  const Node *nodes = (const Node *)bvh->nodes;
+  const int g = div_up(nq, 128);
+#define BQ_VC(KK) k_visit_count<TIE, KK><<<g, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, nq, k, maxSqr, out)
+  if (k == 0) BQ_VC(0);
+  else if (k <= 4) BQ_VC(4);
+  else if (k <= 8) BQ_VC(8);
+  else if (k <= 16) BQ_VC(16);
+  else if (k <= 32) BQ_VC(32);
+  else BQ_VC(64);
+#undef BQ_VC
+}
+
 } // namespace
 
 __global__ void k_fill_empty(uint32_t nq, int k, int32_t *ids, float *d, int32_t *numFound)
@@ -354,6 +411,28 @@ int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t
   else dispatch_knn_tie<64>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
   BQ_CUDA(cudaGetLastError());
   return finish_queries(qs, al);
+}
+
+int query_visit_counts(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, int k,
+                       float maxSqr, const bq_query_config *qcfg, uint64_t *hostCounts, Alloc &al)
+{
+  bq_query_config c;
+  BQ_TRY(query_config(qcfg, c));
+  if (k < 0 || k > 64) return set_error(BQ_ERR_INVALID_ARGUMENT, "k must be 0 (closest point) or in [1, 64]");
+  hostCounts[0] = hostCounts[1] = hostCounts[2] = 0;
+  if (nq == 0 || bvh->numNodes == 0) return BQ_OK;
+  TempSet tmp(al);
+  unsigned long long *out = nullptr;
+  BQ_TRY(tmp.get(&out, 3));
+  BQ_CUDA(cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long), al.s));
+  if (c.tieMode == BQ_TIES_REFERENCE) launch_visit_count<TIE_REFERENCE>(bvh, points, queries, nq, k, maxSqr, out, al.s);
+  else launch_visit_count<TIE_LOWEST>(bvh, points, queries, nq, k, maxSqr, out, al.s);
+  BQ_CUDA(cudaGetLastError());
+  unsigned long long h[3];
+  BQ_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, al.s));
+  BQ_CUDA(cudaStreamSynchronize(al.s));
+  for (int i = 0; i < 3; i++) hostCounts[i] = h[i];
+  return BQ_OK;
 }
 
 } // namespace bq

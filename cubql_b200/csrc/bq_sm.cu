@@ -50,7 +50,7 @@
 #include "bq_internal.cuh"
 
 namespace bq {
-int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al);
+int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al, bool check);
 
 namespace {
 
@@ -866,7 +866,7 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   bvh->numNodes = numNodes;
   bvh->primIDs = primIDs;
   bvh->numPrims = n;  // sm_builder.h:584: invalid prims stay listed after the valid ones
-  if ((s = refit(bvh, boxes, al)) != BQ_OK) {
+  if ((s = refit(bvh, boxes, al, false)) != BQ_OK) {
     al.free_bytes(nodes);
     bvh->nodes = nullptr; bvh->numNodes = 0; bvh->primIDs = nullptr; bvh->numPrims = 0;
     return fail(s);

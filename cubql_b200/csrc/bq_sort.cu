@@ -20,6 +20,7 @@
 // The per-pass digit histograms come from one counting pass over all
 // digits (or from the producer of the keys, see *_prehist).
 #include <algorithm>
+#include <atomic>
 
 #include "bq_internal.cuh"
 
@@ -110,6 +111,8 @@ struct PassCtl {
   uint32_t *abort;     // shared abort flag (all passes)
   uint32_t *err;       // caller's device error word
   const uint32_t *hist;// 256 counters of this pass's digit
+  uint32_t spinLimit;  // polls of one look-back wait before it gives up
+  int holdTile0;       // test hook: tile 0 never publishes (every wait on it runs out)
 };
 
 template <typename KeyT, int ITEMS>
@@ -203,7 +206,7 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
   // 3. decoupled look-back (thread d owns digit d)
   uint32_t *st = ctl.status;
   if (tile == 0) {
-    __stcg(&st[d], ST_INC | cnt);
+    if (!ctl.holdTile0) __stcg(&st[d], ST_INC | cnt);
     sGlobalBase[d] = gStart - sTileStart[d];  // global position = this + tile position
   } else {
     __stcg(&st[(uint64_t)tile * 256 + d], ST_AGG | cnt);
@@ -214,7 +217,7 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
       uint32_t v = ld_volatile(&st[(uint64_t)j * 256 + d]);
       uint32_t spins = 0;
       while ((v & ~ST_VAL) == 0) {
-        if (++spins > SPIN_LIMIT || ld_volatile(ctl.abort)) {
+        if (++spins > ctl.spinLimit || ld_volatile(ctl.abort)) {
           bad = true;
           break;
         }
@@ -306,6 +309,10 @@ __global__ void k_sort_repair(KeyT *__restrict__ keys, uint32_t *__restrict__ va
   }
 }
 
+// test hook (bq_debug_inject_sort_timeout): sorts left to start with a held tile 0
+std::atomic<int> g_injectSortTimeout{0};
+constexpr uint32_t INJECTED_SPIN_LIMIT = 4096;
+
 template <typename KeyT>
 int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit, int endBit,
                   const uint32_t *preHist, int *outSel, uint32_t *dErr, Alloc &al)
@@ -333,6 +340,10 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
                                                                                 numPasses, hist);
     BQ_CUDA(cudaGetLastError());
   }
+  // the test hook is taken by the first sort that runs after it was set
+  int inject = g_injectSortTimeout.load();
+  while (inject > 0 && !g_injectSortTimeout.compare_exchange_weak(inject, inject - 1)) {
+  }
   const size_t smemBytes = (sizeof(KeyT) + sizeof(uint32_t)) * TILE;
   BQ_CUDA(cudaFuncSetAttribute(k_onesweep<KeyT, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes));
   int sel = 0;
@@ -343,6 +354,8 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
     c.abort = ctl + statusWords + numPasses;
     c.err = dErr;
     c.hist = hist + p * 256;
+    c.spinLimit = inject > 0 ? INJECTED_SPIN_LIMIT : SPIN_LIMIT;
+    c.holdTile0 = inject > 0 && p == 0 && numTiles > 1;
     ProfScope ps(sizeof(KeyT) == 8 ? "sort.onesweep64" : "sort.onesweep32", al.s);
     k_onesweep<KeyT, ITEMS><<<numTiles, SORT_BLOCK, smemBytes, al.s>>>(keys[sel], keys[sel ^ 1], vals[sel],
                                                                        vals[sel ^ 1], nMax, nDev, beginBit + 8 * p, c);
@@ -374,3 +387,10 @@ int onesweep_sort_u32(uint32_t *keys[2], uint32_t *vals[2], uint32_t nMax, const
 }
 
 } // namespace bq
+
+extern "C" int bq_debug_inject_sort_timeout(int count)
+{
+  if (count < 0) return bq::set_error(BQ_ERR_INVALID_ARGUMENT, "count must be >= 0");
+  bq::g_injectSortTimeout.store(count);
+  return BQ_OK;
+}

@@ -73,21 +73,38 @@ __device__ __forceinline__ uint64_t ldg_admin(const Node *p)
 // answer is decided by the exact per-prim comparisons.
 __device__ __forceinline__ float lowest_slack(float c) { return __fmaf_rn(c, 0x1p-20f, c); }
 
+// Node-visit counters of the traversal (the measurement pass of the query
+// rooflines counts with VisitCount; the query kernels use NoVisitCount,
+// which compiles to nothing).  pair(): both children of an inner node
+// loaded (2 x 32 B); admin(): the admin half of one node loaded (16 B: the
+// root, and every popped entry that is descended).
+struct NoVisitCount {
+  __device__ __forceinline__ void pair() {}
+  __device__ __forceinline__ void admin() {}
+};
+struct VisitCount {
+  uint32_t pairs = 0, admins = 0;
+  __device__ __forceinline__ void pair() { pairs++; }
+  __device__ __forceinline__ void admin() { admins++; }
+};
+
 // Leaf functor contract: float operator()(uint64_t offset, uint32_t count)
 // processes primIDs[offset .. offset+count) and returns the new cull
 // radius proposal.  Returns false if the stack overflowed (the query then
 // has to be re-run with a deeper stack; its partial state is discarded).
-template <int TIE, typename Stack, typename Leaf>
-__device__ __forceinline__ bool traverse(const Node *__restrict__ nodes, float qx, float qy, float qz, float cull,
-                                         Stack &stack, Leaf &leaf)
+template <int TIE, typename Stack, typename Leaf, typename Count>
+__device__ __forceinline__ bool traverse_counted(const Node *__restrict__ nodes, float qx, float qy, float qz,
+                                                 float cull, Stack &stack, Leaf &leaf, Count &count)
 {
   uint64_t admin = ldg_admin(nodes);
+  count.admin();
   while (true) {
     bool dead = false;
     while (admin_count(admin) == 0) {
       const uint64_t off = admin_offset(admin);
       const Node n0 = ldg_node(nodes + off);
       const Node n1 = ldg_node(nodes + off + 1);
+      count.pair();
       const float d0 = sqr_pbox(qx, qy, qz, n0.a.x, n0.a.y, n0.a.z, n0.a.w, n0.b.x, n0.b.y);
       const float d1 = sqr_pbox(qx, qy, qz, n1.a.x, n1.a.y, n1.a.z, n1.a.w, n1.b.x, n1.b.y);
       const float dmin = fminf(d0, d1), dmax = fmaxf(d0, d1);
@@ -114,9 +131,49 @@ __device__ __forceinline__ bool traverse(const Node *__restrict__ nodes, float q
       const StackEntry e = stack.pop();
       if (e.dist <= (TIE == TIE_REFERENCE ? cull : lowest_slack(cull))) {
         admin = ldg_admin(nodes + e.idx);
+        count.admin();
         break;
       }
     }
+  }
+}
+
+template <int TIE, typename Stack, typename Leaf>
+__device__ __forceinline__ bool traverse(const Node *__restrict__ nodes, float qx, float qy, float qz, float cull,
+                                         Stack &stack, Leaf &leaf)
+{
+  NoVisitCount none;
+  return traverse_counted<TIE>(nodes, qx, qy, qz, cull, stack, leaf, none);
+}
+
+// a leaf functor that also counts the prims it is handed
+template <typename Leaf>
+struct CountingLeaf {
+  Leaf &inner;
+  uint32_t prims = 0;
+  __device__ __forceinline__ float operator()(uint64_t off, uint32_t cnt)
+  {
+    prims += cnt;
+    return inner(off, cnt);
+  }
+};
+
+// adds one thread's counts to out[0..2] (node pairs, admin loads, prims),
+// one atomic per warp and counter
+__device__ __forceinline__ void add_visit_counts(uint32_t pairs, uint32_t admins, uint32_t prims,
+                                                 unsigned long long *out)
+{
+  unsigned long long a = pairs, b = admins, c = prims;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+    c += __shfl_down_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(out, a);
+    atomicAdd(out + 1, b);
+    atomicAdd(out + 2, c);
   }
 }
 

@@ -186,6 +186,31 @@ __global__ void k_tri_deep(const Node *__restrict__ nodes, const uint32_t *__res
   }
 }
 
+// visit counts of the triangle traversal (measurement pass of the forward's
+// roofline): node pairs loaded, admin loads, triangles tested
+template <int TIE>
+__global__ void __launch_bounds__(128) k_tri_visit_count(const Node *__restrict__ nodes,
+                                                         const uint32_t *__restrict__ primIDs,
+                                                         const int32_t *__restrict__ tris,
+                                                         const float *__restrict__ verts,
+                                                         const float *__restrict__ queries, uint32_t nq, float maxSqr,
+                                                         unsigned long long *out)
+{
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  VisitCount vc;
+  uint32_t prims = 0;
+  if (t < nq) {  // no early return: every lane takes part in the warp sum below
+    const float *qp = queries + 3ull * t;
+    TriLeaf<TIE> leaf{primIDs, tris, verts, V3{__ldg(qp), __ldg(qp + 1), __ldg(qp + 2)}, maxSqr, -1,
+                      V3{0.f, 0.f, 0.f}};
+    CountingLeaf<TriLeaf<TIE>> cl{leaf};
+    LocalStack<128> st;
+    traverse_counted<TIE>(nodes, leaf.q.x, leaf.q.y, leaf.q.z, maxSqr, st, cl, vc);
+    prims = cl.prims;
+  }
+  add_visit_counts(vc.pairs, vc.admins, prims, out);
+}
+
 __global__ void k_tri_keys(const Node *__restrict__ nodes, const float *__restrict__ queries, uint32_t nq,
                            uint32_t *__restrict__ keys, uint32_t *__restrict__ idx)
 {
@@ -413,6 +438,32 @@ int tri_boxes(const int32_t *tris, const float *verts, uint32_t nt, bq_box3f *bo
   if (nt == 0) return BQ_OK;
   k_tri_boxes<<<div_up(nt, 256), 256, 0, s>>>(tris, verts, nt, boxes);
   BQ_CUDA(cudaGetLastError());
+  return BQ_OK;
+}
+
+int tri_visit_counts(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, const float *queries, uint32_t nq,
+                     float maxSqr, const bq_query_config *qcfg, uint64_t *hostCounts, Alloc &al)
+{
+  bq_query_config c;
+  BQ_TRY(query_config(qcfg, c));
+  hostCounts[0] = hostCounts[1] = hostCounts[2] = 0;
+  if (nq == 0 || bvh->numNodes == 0) return BQ_OK;
+  TempSet tmp(al);
+  unsigned long long *out = nullptr;
+  BQ_TRY(tmp.get(&out, 3));
+  BQ_CUDA(cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long), al.s));
+  const Node *nodes = (const Node *)bvh->nodes;
+  if (c.tieMode == BQ_TIES_REFERENCE)
+    k_tri_visit_count<TIE_REFERENCE><<<div_up(nq, 128), 128, 0, al.s>>>(nodes, bvh->primIDs, tris, verts, queries, nq,
+                                                                        maxSqr, out);
+  else
+    k_tri_visit_count<TIE_LOWEST><<<div_up(nq, 128), 128, 0, al.s>>>(nodes, bvh->primIDs, tris, verts, queries, nq,
+                                                                     maxSqr, out);
+  BQ_CUDA(cudaGetLastError());
+  unsigned long long h[3];
+  BQ_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, al.s));
+  BQ_CUDA(cudaStreamSynchronize(al.s));
+  for (int i = 0; i < 3; i++) hostCounts[i] = h[i];
   return BQ_OK;
 }
 

@@ -12,6 +12,7 @@ import numpy as np
 SEED_DATA = 290374      # samples/s01_closestPoint_points_gpu/closestPoint.cu:77
 SEED_QUERIES = 1234567  # samples/s01_closestPoint_points_gpu/closestPoint.cu:83
 SEED_GMM = 7
+SEED_GMM_QUERIES = 8  # fresh samples of the same mixture (queries)
 SEED_MESH = 11
 SEED_BATCH = 13
 
@@ -48,15 +49,17 @@ def uniform_points(n, seed=SEED_DATA, lo=0.0, hi=1.0):
     return (lo + u * (hi - lo)).astype(np.float32)
 
 
-def gmm_points(n, seed=SEED_GMM, components=64, offset=1e5, sigma_lo=1e-4, sigma_hi=1e-1):
+def gmm_points(n, seed=SEED_GMM, components=64, offset=1e5, sigma_lo=1e-4, sigma_hi=1e-1, sample_seed=None):
     """(n,3) float32 from a `components`-Gaussian mixture: centres U[0,1]^3,
     sigma log-uniform in [sigma_lo, sigma_hi], equal weights, every
     coordinate shifted by `offset` (at 1e5 the float spacing is ~0.0078, so
-    the tight clusters collapse into exact duplicates)."""
+    the tight clusters collapse into exact duplicates).  The mixture comes
+    from `seed`, the samples from `sample_seed` (default: `seed`), so queries
+    from the same distribution are gmm_points(nq, sample_seed=...)."""
     c = lcg_streams(components, seed ^ 0x5bd1e995, 4).astype(np.float64)
     centres = c[:, :3]
     sig = np.exp(np.log(sigma_lo) + c[:, 3] * (np.log(sigma_hi) - np.log(sigma_lo)))
-    u = lcg_streams(n, seed, 7).astype(np.float64)
+    u = lcg_streams(n, seed if sample_seed is None else sample_seed, 7).astype(np.float64)
     comp = np.minimum((u[:, 0] * components).astype(np.int64), components - 1)
     u1 = np.maximum(u[:, 1:4], 1e-12)
     u2 = u[:, 4:7]

@@ -9,8 +9,15 @@
  *   - returns an int status (BQ_OK or one of the BQ_ERR_* codes below);
  *     bq_last_error_string() gives the message of the calling thread's
  *     last failure.  Nothing aborts or raises.
- * The library keeps no mutable global state between calls except the
- * per-thread error string, so calls on different streams may run
+ * Mutable global state kept between calls:
+ *   - the per-thread error string;
+ *   - the flag that records that the default stream-ordered pool's
+ *     release threshold was raised (set once per device);
+ *   - the phase profiler's event pool (bq_profile_*, per thread, only
+ *     while profiling is enabled);
+ *   - the fixed scratch array of bq_refit_noalloc_f3 (shared by all of
+ *     its calls; see there).
+ * Apart from bq_refit_noalloc_f3, calls on different streams may run
  * concurrently.
  *
  * Memory layout (identical to the reference, so trees built here can be
@@ -158,7 +165,14 @@ int bq_build_sah_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, con
                     const bq_allocator *alloc, bq_stream_t stream);
 
 /* Recomputes every node box bottom-up from `boxes`.  Replaces
-   gpuBuilder_impl::refit (cuBQL/builder/cuda/sm_builder.h:677-693). */
+   gpuBuilder_impl::refit (cuBQL/builder/cuda/sm_builder.h:677-693).
+   Every index read from the tree is range-checked on the device: an inner
+   node whose children are not in [2, numNodes), a leaf whose prims are not
+   in [0, numPrims), or a cycle of parent links gives
+   BQ_ERR_INVALID_ARGUMENT (the bad access is skipped, never made).  To
+   report that, the call waits for the refit to finish; while the stream is
+   being captured into a graph it does not wait and reports nothing.
+   primIDs must index `boxes`. */
 int bq_refit_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_allocator *alloc, bq_stream_t stream);
 
 /* bq_refit_f3 without any device allocation (no counterpart in the
@@ -167,11 +181,17 @@ int bq_refit_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, const bq_allocator *
    front, a real-time loop where cudaMalloc could stall or fail mid-frame,
    or a framework that only permits allocation during its set-up.  Its
    scratch (two words per node) is one fixed array inside the library,
-   sized for BQ_NOALLOC_REFIT_MAX_NODES nodes (8 MiB held on every GPU that
-   loads the library until exit).  Larger trees are rejected with
-   BQ_ERR_INVALID_ARGUMENT.  The first call on a device looks up the
-   array's address; make it before any stream capture.  All calls share
-   the array: calls that overlap on the GPU race, so serialise them. */
+   sized for BQ_NOALLOC_REFIT_MAX_NODES nodes (8 MiB); larger trees are
+   rejected with BQ_ERR_INVALID_ARGUMENT.
+   Set-up: call it once per device, with that device current and
+   numNodes == 0 (the other fields are not read), during set-up, before
+   any stream capture and before reserving the rest of the GPU's memory.
+   That call places the array on the device (with the CUDA runtime's
+   default lazy module loading nothing is placed before) and loads the
+   kernels; the device then holds the 8 MiB until the process exits.
+   All calls share the array and each call clears what it needs: calls
+   that overlap on the GPU race, so serialise them.  Like bq_refit_f3 it
+   range-checks the tree and waits for the refit to finish. */
 #define BQ_NOALLOC_REFIT_MAX_NODES (1u << 20)
 int bq_refit_noalloc_f3(const bq_bvh3f *bvh, const bq_box3f *boxes, bq_stream_t stream);
 
@@ -323,6 +343,18 @@ int bq_wide_box_query_gather_f3(const bq_wide_bvh3f *bvh, int width, const bq_bo
                                 bq_stream_t stream);
 
 /* ---------------------------------------------------------------- */
+/* test hook                                                          */
+/* ---------------------------------------------------------------- */
+/* The next `count` radix sorts (of any call, any thread) start with the
+   first pass's first tile holding back its digit totals, so every
+   look-back wait on it runs out after a short spin (a few milliseconds)
+   instead of the normal limit: the pass aborts, the sort's output is
+   overwritten with in-range values (keys 0, values 0..n-1) and the call
+   returns BQ_ERR_TIMEOUT.  Exercises the bounded-wait error path without
+   any fault; no counterpart in the reference.  0 switches it off. */
+int bq_debug_inject_sort_timeout(int count);
+
+/* ---------------------------------------------------------------- */
 /* binary-dump files (host only, no GPU)                              */
 /* ---------------------------------------------------------------- */
 /* The format of cuBQL::samples::loadBinary / saveBinary
@@ -361,6 +393,23 @@ int bq_tri_closest_f3(const bq_bvh3f *bvh, const int32_t *tris, const float *ver
 int bq_tri_distance_bwd_f3(const int32_t *tris, const float *verts, uint32_t numVerts, const float *queries,
                            uint32_t numQueries, const int32_t *ids, const float *gradSqr, float *gradQueries,
                            float *gradVerts, const bq_allocator *alloc, bq_stream_t stream);
+
+/* Traversal visit counts of a query batch, the measurement behind the
+   query rooflines.  Replaces the reference's traversal-step counters
+   (testing/bvh/buildQual.h:65-126 NUM_TRAVERSAL_STEPS,
+   testing/bvh/checkBuilders.cu:110-143 node/prim visit counts).  The same
+   traversal as bq_closest_point_f3 (k == 0) or bq_knn_f3 (k in [1, 64]),
+   or bq_tri_closest_f3 for the _tri_ form, is run once more, counting; the
+   answers are discarded.  counts (HOST array of 3): [0] inner nodes
+   expanded (each loads both 32-byte children), [1] node admin words
+   loaded (16 B: the root and every stack entry descended), [2] prims
+   tested.  Waits for the stream. */
+int bq_query_visit_counts_f3(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t numQueries,
+                             int k, float maxSqrDist, const bq_query_config *qcfg, uint64_t *counts,
+                             const bq_allocator *alloc, bq_stream_t stream);
+int bq_tri_visit_counts_f3(const bq_bvh3f *bvh, const int32_t *tris, const float *verts, const float *queries,
+                           uint32_t numQueries, float maxSqrDist, const bq_query_config *qcfg, uint64_t *counts,
+                           const bq_allocator *alloc, bq_stream_t stream);
 
 /* ---------------------------------------------------------------- */
 /* batches of clouds (no counterpart in the reference, which builds    */
@@ -432,6 +481,14 @@ int bq_autotune_batched_knn_f3(const bq_box3f *boxes, const float *points, const
                                uint32_t numSegs, uint32_t numPrims, const float *queries, const uint32_t *queryOffsets,
                                uint32_t numQueries, int k, bq_tuning *best, const bq_allocator *alloc,
                                bq_stream_t stream);
+
+/* The same for one tree: Morton builds with leaf threshold {1,2,4,8},
+   each queried with stack depth {32,64,128} x block size {64,128}, closest
+   point (k == 0) or kNN (k in [1, 64]); best->queriesPerWarp is 32 (the
+   single-tree kernels take one query per thread).  The fastest build +
+   query is returned with its two times. */
+int bq_autotune_query_f3(const bq_box3f *boxes, const float *points, uint32_t numPrims, const float *queries,
+                         uint32_t numQueries, int k, bq_tuning *best, const bq_allocator *alloc, bq_stream_t stream);
 
 /* ---------------------------------------------------------------- */
 /* input helpers                                                      */

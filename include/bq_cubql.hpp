@@ -78,6 +78,24 @@ inline bq_build_config to_c_cfg(const Cfg &c)
   return bq_build_config{c.maxAllowedLeafSize, c.makeLeafThreshold, (int)c.buildMethod};
 }
 
+/*! cuBQL::gpuBuilder(WideBVH<float,3,W>&) (cuBQL/builder/cuda.h:100-116):
+    a binary spatial-median build collapsed into a W-wide tree (W = 4, 8) */
+template <template <typename, int, int> class WideBVH, typename T, int D, int W, class Box, class Cfg, class MemRes>
+inline void gpuBuilder(WideBVH<T, D, W> &bvh, const Box *boxes, uint32_t numBoxes, Cfg cfg, cudaStream_t s,
+                       MemRes &mem)
+{
+  static_assert(sizeof(Box) == 24, "box_t<float,3> layout");
+  static_assert(sizeof(typename WideBVH<T, D, W>::Node) == 32 * W, "WideBVH<float,3,W>::Node layout");
+  bq_wide_bvh3f c{};
+  bq_build_config cc = to_c_cfg(cfg);
+  bq_allocator a = ResourceAdapter<MemRes>::make(mem);
+  check(bq_build_wide_f3(&c, W, (const bq_box3f *)boxes, numBoxes, &cc, &a, s), "gpuBuilder(WideBVH)");
+  bvh.nodes = (typename WideBVH<T, D, W>::Node *)c.nodes;
+  bvh.numNodes = c.numNodes;
+  bvh.primIDs = c.primIDs;
+  bvh.numPrims = c.numPrims;
+}
+
 /*! cuBQL::gpuBuilder (cuBQL/builder/cuda.h:91-99): spatial median */
 template <class BVH, class Box, class Cfg, class MemRes>
 inline void gpuBuilder(BVH &bvh, const Box *boxes, uint32_t numBoxes, Cfg cfg, cudaStream_t s, MemRes &mem)
@@ -103,6 +121,18 @@ inline void radixBuilder(BVH &bvh, const Box *boxes, uint32_t numPrims, Cfg cfg,
   from_c(bvh, c);
 }
 
+/*! cuBQL::cuda::sahBuilder (cuBQL/builder/cuda.h:118-129): binned SAH */
+template <class BVH, class Box, class Cfg, class MemRes>
+inline void sahBuilder(BVH &bvh, const Box *boxes, uint32_t numPrims, Cfg cfg, cudaStream_t s, MemRes &mem)
+{
+  static_assert(sizeof(Box) == 24, "box_t<float,3> layout");
+  bq_bvh3f c{};
+  bq_build_config cc = to_c_cfg(cfg);
+  bq_allocator a = ResourceAdapter<MemRes>::make(mem);
+  check(bq_build_sah_f3(&c, (const bq_box3f *)boxes, numPrims, &cc, &a, s), "sahBuilder");
+  from_c(bvh, c);
+}
+
 /*! cuBQL::cuda::rebinRadixBuilder (cuBQL/builder/cuda.h:143-154) */
 template <class BVH, class Box, class Cfg, class MemRes>
 inline void rebinRadixBuilder(BVH &bvh, const Box *boxes, uint32_t numPrims, Cfg cfg, cudaStream_t s, MemRes &mem)
@@ -124,6 +154,20 @@ inline void free(BVH &bvh, cudaStream_t s, MemRes &mem)
   check(bq_free_f3(&c, &a, s), "free");
   cudaStreamSynchronize(s);  // cuda::free synchronises (gpu_builder.h:86)
   from_c(bvh, c);
+}
+
+/*! cuBQL::cuda::free(WideBVH&) (cuBQL/builder/cuda/wide_gpu_builder.h:217-231) */
+template <template <typename, int, int> class WideBVH, typename T, int D, int W, class MemRes>
+inline void free(WideBVH<T, D, W> &bvh, cudaStream_t s, MemRes &mem)
+{
+  bq_wide_bvh3f c{(bq_wide_child3f *)bvh.nodes, bvh.numNodes, bvh.primIDs, bvh.numPrims};
+  bq_allocator a = ResourceAdapter<MemRes>::make(mem);
+  check(bq_wide_free_f3(&c, &a, s), "free(WideBVH)");
+  cudaStreamSynchronize(s);
+  bvh.nodes = nullptr;
+  bvh.numNodes = 0;
+  bvh.primIDs = nullptr;
+  bvh.numPrims = 0;
 }
 } // namespace cuda
 
@@ -151,6 +195,20 @@ inline void findClosest(const BVH &bvh, const Vec *points, const Vec *queries, u
   check(bq_closest_point_f3(&c, (const float *)points, (const float *)queries, numQueries, maxSqrDist, &q, ids,
                             sqrDist, nullptr, s),
         "findClosest");
+}
+
+/*! batched cuBQL::points::findClosest(WideBVH<float,3,W>) (findClosest.h:363-386) */
+template <template <typename, int, int> class WideBVH, typename T, int D, int W, class Vec>
+inline void findClosest(const WideBVH<T, D, W> &bvh, const Vec *points, const Vec *queries, uint32_t numQueries,
+                        int32_t *ids, float *sqrDist, float maxSqrDist = INFINITY, cudaStream_t s = 0,
+                        int tieMode = BQ_TIES_LOWEST_ID)
+{
+  static_assert(sizeof(Vec) == 12, "vec3f layout");
+  bq_wide_bvh3f c{(bq_wide_child3f *)bvh.nodes, bvh.numNodes, bvh.primIDs, bvh.numPrims};
+  bq_query_config q{tieMode, 0, 0, 1, 0};
+  check(bq_wide_closest_point_f3(&c, W, (const float *)points, (const float *)queries, numQueries, maxSqrDist, &q,
+                                 ids, sqrDist, nullptr, s),
+        "findClosest(WideBVH)");
 }
 
 /*! batched cuBQL::points::findKNN; ids/sqrDist are numQueries*k */
@@ -197,6 +255,26 @@ inline void findClosest_exludeSelf(const BVH &bvh, const Vec *points, const Vec 
         "findClosest_exludeSelf");
 }
 } // namespace points
+
+namespace triangles {
+/*! batched cuBQL::triangles::findClosest (queries/triangles/findClosest.h:132-152)
+    over an indexed mesh: tris holds 3 vertex indices per triangle into
+    verts (float triples), where the reference's Triangle array holds the
+    3 vertices themselves; ids, sqrDist and the closest points P (may be
+    NULL) per query, -1 / +inf where nothing is closer than maxSqrDist */
+template <class BVH, class Vec>
+inline void findClosest(const BVH &bvh, const int32_t *tris, const Vec *verts, const Vec *queries,
+                        uint32_t numQueries, int32_t *ids, float *sqrDist, Vec *P = nullptr,
+                        float maxSqrDist = INFINITY, cudaStream_t s = 0, int tieMode = BQ_TIES_LOWEST_ID)
+{
+  static_assert(sizeof(Vec) == 12, "vec3f layout");
+  bq_bvh3f c = to_c(bvh);
+  bq_query_config q{tieMode, 0, 0, 1, 0};
+  check(bq_tri_closest_f3(&c, tris, (const float *)verts, (const float *)queries, numQueries, maxSqrDist, &q, ids,
+                          sqrDist, (float *)P, nullptr, s),
+        "triangles::findClosest");
+}
+} // namespace triangles
 
 namespace fixedBoxQuery {
 /*! batched cuBQL::fixedBoxQuery::forEachPrim (traversal/fixedBoxQuery.h:139-156)

@@ -1,7 +1,9 @@
 #!/bin/sh
 # Compiles the reference library's own code paths, directly from the
-# unmodified reference sources at $REF (default /root/reference), into
-# oracle/_ref/.  Test / baseline infrastructure only; nothing from the
+# unmodified reference sources, into oracle/_ref/.
+#   sh oracle/build_ref.sh <reference source tree>   (or REF=<tree> sh ...)
+# Without a tree (or where it has no cuBQL/ directory) the existing
+# oracle/_ref is kept.  Test / baseline infrastructure only; nothing from the
 # reference is copied into this repository.
 #   libref_cpu.so  cpuBuilder + host findClosest/findKNN/triangles (g++)
 #   libref_gpu.so  gpuBuilder, radixBuilder, rebinRadixBuilder and the
@@ -9,7 +11,11 @@
 # Both are built with FMA contraction as each compiler does by default for
 # that code: g++ on x86-64 (no -mfma) emits none, nvcc contracts.
 set -e
-REF="${REF:-/root/reference}"
+REF="${1:-${REF:-}}"
+if [ -z "$REF" ]; then
+  echo "no reference source tree given; keeping existing oracle/_ref" >&2
+  exit 0
+fi
 here="$(cd "$(dirname "$0")" && pwd)"
 if [ ! -d "$REF/cuBQL" ]; then
   echo "reference sources not found at $REF; keeping existing oracle/_ref" >&2

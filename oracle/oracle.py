@@ -34,12 +34,13 @@ def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
 
 
-def build():
-    """Compile the oracle (always) and the reference libraries (if the
-    reference sources are present)."""
+def build(reference_dir=None):
+    """Compile the oracle (always) and the reference libraries from the
+    reference source tree `reference_dir` (when given and present)."""
     import subprocess
     subprocess.run(["sh", os.path.join(HERE, "build_oracle.sh")], check=True)
-    subprocess.run(["sh", os.path.join(HERE, "build_ref.sh")], check=True)
+    if reference_dir and os.path.isdir(os.path.join(reference_dir, "cuBQL")):
+        subprocess.run(["sh", os.path.join(HERE, "build_ref.sh"), reference_dir], check=True)
 
 
 _libs = {}
@@ -627,6 +628,18 @@ class RefGPU:
         assert rc == 0
         return ms.value
 
+    def time_tri(self, method, tris, verts, queries, reps=3):
+        """ms of the reference's triangles::findClosest kernel over a tree
+        built with `method` on the triangle boxes (build not timed)."""
+        tris = np.ascontiguousarray(tris, dtype=np.int32)
+        verts, queries = _f32(verts), _f32(queries)
+        ms = ctypes.c_float()
+        rc = self.lib.ref_gpu_time_tri(ctypes.c_int(method), _p(tris), ctypes.c_uint32(len(tris)), _p(verts),
+                                       _p(queries), ctypes.c_uint32(len(queries)), ctypes.c_int(reps),
+                                       ctypes.byref(ms))
+        assert rc == 0
+        return ms.value
+
     def time_box_query(self, method, points, query_boxes, makeLeafThreshold=0, reps=5):
         """(ms of count + fill kernels, total results) for the reference box
         query over a tree built on the point boxes."""
@@ -708,3 +721,21 @@ class RefShim:
                                        _p(ri), _p(rd), _p(oi), _p(od), _p(nn))
         assert rc == 0
         return ri, rd, oi, od, nn
+
+    def compare_more(self, points, queries, tris, verts, tri_queries):
+        """(ids (6, rows), d (6, rows), numNodes (4,)): rows 0/1 the reference's
+        findClosest on its SAH tree / ours, 2/3 its wide findClosest on its
+        WideBVH<4> / ours, 4/5 its triangles::findClosest kernel / the batched
+        bq_cubql::triangles::findClosest, on one tree (ref_shim.cu)."""
+        points, queries, verts, tq = _f32(points), _f32(queries), _f32(verts), _f32(tri_queries)
+        tris = np.ascontiguousarray(tris, dtype=np.int32)
+        rows = max(len(queries), len(tq))
+        ids = np.zeros((6, rows), np.int32)
+        d = np.zeros((6, rows), np.float32)
+        nn = np.zeros(4, np.uint32)
+        rc = self.lib.ref_shim_compare_more(_p(points), ctypes.c_uint32(len(points)), _p(queries),
+                                            ctypes.c_uint32(len(queries)), _p(tris), ctypes.c_uint32(len(tris)),
+                                            _p(verts), ctypes.c_uint32(len(verts)), _p(tq), ctypes.c_uint32(len(tq)),
+                                            _p(ids), _p(d), _p(nn))
+        assert rc == 0
+        return ids, d, nn

@@ -634,6 +634,51 @@ int ref_gpu_time_query(int method, const float *points, uint32_t n, int makeLeaf
   return 0;
 }
 
+// Times the reference's per-thread triangles::findClosest kernel
+// (<<<ceil(Q/128),128>>>) over a tree built with `method` on the triangle
+// boxes; the tree build is not timed.
+int ref_gpu_time_tri(int method, const int32_t *tris, uint32_t nt, const float *verts, const float *queries,
+                     uint32_t nq, int reps, float *ms_out)
+{
+  std::vector<Triangle> T(nt);
+  std::vector<box3f> B(nt);
+  const vec3f *V = (const vec3f *)verts;
+  for (uint32_t i = 0; i < nt; i++) {
+    T[i].a = V[tris[3 * i + 0]];
+    T[i].b = V[tris[3 * i + 1]];
+    T[i].c = V[tris[3 * i + 2]];
+    B[i] = box3f().including(T[i].a).including(T[i].b).including(T[i].c);
+  }
+  Triangle *dt = dalloc_copy(T.data(), nt);
+  box3f *db = dalloc_copy(B.data(), nt);
+  vec3f *dq = dalloc_copy((const vec3f *)queries, nq), *dP = dalloc_copy<vec3f>(nullptr, nq);
+  int *di = dalloc_copy<int>(nullptr, nq);
+  float *dd = dalloc_copy<float>(nullptr, nq);
+  if (!dt || !db || !dq || !dP || !di || !dd) return -1;
+  bvh3f bvh;
+  run_build(method, db, nt, 0, bvh);
+  RCHECK(cudaDeviceSynchronize());
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float total = 0.f;
+  for (int r = -1; r < reps; r++) {
+    cudaEventRecord(e0);
+    k_tri<<<(nq + 127) / 128, 128>>>(bvh, dt, dq, (int)nq, INFINITY, di, dd, dP);
+    cudaEventRecord(e1);
+    RCHECK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r >= 0) total += ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cuBQL::cuda::free(bvh);
+  cudaFree(dt); cudaFree(db); cudaFree(dq); cudaFree(dP); cudaFree(di); cudaFree(dd);
+  *ms_out = total / (reps > 0 ? reps : 1);
+  return 0;
+}
+
 // Times the reference box query (count kernel + fill kernel, offsets from
 // an untimed count pass) over a tree of `method` built on point boxes.
 int ref_gpu_time_box_query(int method, const float *points, uint32_t n, int makeLeafThreshold,

@@ -20,3 +20,25 @@ def test_reference_query_kernel_on_our_tree():
     ri, rd, oi, od, nn = RefShim().compare(pts, qs)
     assert nn[0] == nn[1] == 600000
     assert np.array_equal(ri, oi) and np.array_equal(rd, od)
+
+
+def test_shim_sah_wide_and_triangles_against_reference():
+    """The rest of the builder entry points (cuda::sahBuilder,
+    gpuBuilder(WideBVH<float,3,4>&), cuda::free of both) and the batched
+    triangle query, called through include/bq_cubql.hpp with the reference's
+    own types: the reference's query kernels answer on our trees exactly as
+    on its own, and the batched triangle query (reference tie rule) equals
+    the reference's per-thread kernel on the same tree."""
+    from oracle.oracle import RefShim, have_ref_shim
+    if not have_ref_shim():
+        pytest.skip("oracle/_ref/libref_shim.so not built (reference sources unavailable)")
+    pts = W.uniform_points(200000)
+    qs = W.uniform_points(50000, W.SEED_QUERIES, -0.1, 1.1)
+    verts, tris = W.icosphere(5)
+    tq = W.uniform_points(40000, 3, -1.5, 1.5)
+    ids, d, nn = RefShim().compare_more(pts, qs, tris, verts, tq)
+    nq, ntq = len(qs), len(tq)
+    assert nn[0] == nn[1] and nn[2] == nn[3]
+    assert np.array_equal(ids[0, :nq], ids[1, :nq]) and np.array_equal(d[0, :nq], d[1, :nq]), "SAH"
+    assert np.array_equal(ids[2, :nq], ids[3, :nq]) and np.array_equal(d[2, :nq], d[3, :nq]), "wide"
+    assert np.array_equal(ids[4, :ntq], ids[5, :ntq]) and np.array_equal(d[4, :ntq], d[5, :ntq]), "triangles"

@@ -214,3 +214,22 @@ def test_closest_exclude_variants_match_reference_kernels(bq, oracle, ref_gpu, d
     ids, d = bq.points.findClosest_exludeSelf(bvh, tp, tq, qcfg=qc)
     ri, rd = ref_gpu.closest_point_exclude(n, pr, pts, qs)
     assert np.array_equal(ids.cpu().numpy(), ri) and np.array_equal(d.cpu().numpy(), rd)
+
+
+@pytest.mark.parametrize("tie", [0, 1])
+@pytest.mark.parametrize("dist", ["uniform", "gmm"])
+def test_visit_counts_match_oracle_traversal(bq, oracle, tie, dist):
+    """The measurement pass behind the query rooflines counts exactly the
+    node pairs the oracle's traversal expands (it counts 2 per expansion)."""
+    pts, qs = _data(dist, 50000, 8000)
+    bvh = _tree(bq, "morton", pts)
+    n, pr = bvh.to_host()
+    c = bq.points.visitCounts(bvh, torch.from_numpy(pts).cuda(), torch.from_numpy(qs).cuda(), 0,
+                              qcfg=bq.query_config(tieMode=tie))
+    _, _, ovf, vis = oracle.closest_point(n, pr, pts, qs, tie_mode=tie, stack=128)
+    assert not ovf.any()
+    assert c["inner_nodes"] == int(vis.astype(np.int64).sum()) // 2
+    assert c["admin_loads"] >= len(qs) and c["prims"] >= len(qs)
+    k16 = bq.points.visitCounts(bvh, torch.from_numpy(pts).cuda(), torch.from_numpy(qs).cuda(), 16,
+                                qcfg=bq.query_config(tieMode=tie))
+    assert k16["inner_nodes"] > c["inner_nodes"] and k16["prims"] >= 16 * len(qs)
