@@ -57,7 +57,13 @@ def parse():
     ap.add_argument("--only-queries", action="store_true",
                     help="build one tree, then time closest-point and kNN(16) queries only (the short program "
                          "the query ncu captures run)")
-    ap.add_argument("--queries", type=int, default=N_POINTS, help="query count for --only-queries")
+    ap.add_argument("--queries", type=int, default=N_POINTS, help="query count for --only-queries/-tri/-wide")
+    ap.add_argument("--only-tri", action="store_true",
+                    help="triangle forward only: icosphere of --mesh-level over --queries queries in [-1.5,1.5]^3 "
+                         "(the short program the triangle ncu captures run)")
+    ap.add_argument("--mesh-level", type=int, default=8)
+    ap.add_argument("--only-wide", action="store_true",
+                    help="build one 4-wide tree, then time wide closest-point queries only")
     ap.add_argument("--only-build", action="store_true",
                     help="time the build loop only (no profile pass, e2e, components or CPU leg): "
                          "the short program the ncu captures run")
@@ -411,8 +417,12 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
                              "roofline": query_roofline(cpc, n, 8, 16, ms, peak, n * 20 + 32 * nn + 16 * n)}
     ms = ev_time(lambda: bq.points.findKNN(bvh, tp, qs, 16))
     knc = bq.points.visitCounts(bvh, tp, qs, 16)
+    # the warp-cooperative form: a group of lanes per query, the top-k list one candidate per lane
+    lane_ms = {g: ev_time(lambda: bq.points.findKNN(bvh, tp, qs, 16, qcfg=bq.query_config(lanesPerQuery=g)))
+               for g in (16, 32)}
     comp["knn16"] = {"ms": ms, "Mqueries_s": n / ms / 1e3, "queries": n, "k": 16,
-                     "roofline": query_roofline(knc, n, 8 * 16 + 4, 16, ms, peak, n * (12 + 132) + 32 * nn + 16 * n)}
+                     "roofline": query_roofline(knc, n, 8 * 16 + 4, 16, ms, peak, n * (12 + 132) + 32 * nn + 16 * n),
+                     "lane_group_ms": {f"lanesPerQuery={g}": v for g, v in lane_ms.items()}}
     with bq.profile() as prof:
         bq.points.findClosest(bvh, tp, qs)
         bq.points.findKNN(bvh, tp, qs, 16)
@@ -548,10 +558,18 @@ def gmm_component(bq, W, torch, comp, n):
     ms_s = _ev_time(torch, lambda: bq.gpuBuilder(boxes, bq.BuildConfig(makeLeafThreshold=8)).free())
     bvh = bq.cuda.radixBuilder(boxes)
     nn = bvh.numNodes
-    ms_cp = _ev_time(torch, lambda: bq.points.findClosest(bvh, pts, qs), reps=2)
-    ms_knn = _ev_time(torch, lambda: bq.points.findKNN(bvh, pts, qs, 16), reps=2)
-    cpc = bq.points.visitCounts(bvh, pts, qs, 0)
-    knc = bq.points.visitCounts(bvh, pts, qs, 16)
+    # Queries under the reference's tie rule (answers bit-identical to the reference's kernels).  The
+    # lowest-id rule has to look at every point at the tied distance, and here tight clusters collapse
+    # into ~1e5 identical points, so it is timed on a 100k-query sample only.
+    ref = bq.query_config(tieMode=bq.TIES_REFERENCE)
+    ms_cp = _ev_time(torch, lambda: bq.points.findClosest(bvh, pts, qs, qcfg=ref), reps=2)
+    ms_knn = _ev_time(torch, lambda: bq.points.findKNN(bvh, pts, qs, 16, qcfg=ref), reps=2)
+    cpc = bq.points.visitCounts(bvh, pts, qs, 0, qcfg=ref)
+    knc = bq.points.visitCounts(bvh, pts, qs, 16, qcfg=ref)
+    qsam = qs[:100_000]
+    ms_cp_low = _ev_time(torch, lambda: bq.points.findClosest(bvh, pts, qsam), reps=1)
+    ms_knn_low = _ev_time(torch, lambda: bq.points.findKNN(bvh, pts, qsam, 16), reps=1)
+    low = bq.points.visitCounts(bvh, pts, qsam, 0)
     bvh.free()
     comp["gmm10m"] = {
         "points": n, "queries": n,
@@ -559,10 +577,13 @@ def gmm_component(bq, W, torch, comp, n):
         "morton_build_roofline": dict(hbm_frac(morton_build_bytes(n, nn), ms_m, peak), model="288 N + 64 M"),
         "morton_phases_ms": {k: round(v[1], 4) for k, v in prof.table.items()},
         "spatial_median_leaf8_ms": ms_s, "spatial_median_Mprims_s": n / ms_s / 1e3,
+        "query_tie_rule": "reference (BQ_TIES_REFERENCE)",
         "closest_point_ms": ms_cp, "closest_point_Mqueries_s": n / ms_cp / 1e3,
         "closest_point_roofline": query_roofline(cpc, n, 8, 16, ms_cp, peak, n * 20 + 32 * nn + 16 * n),
         "knn16_ms": ms_knn, "knn16_Mqueries_s": n / ms_knn / 1e3,
-        "knn16_roofline": query_roofline(knc, n, 132, 16, ms_knn, peak, n * 144 + 32 * nn + 16 * n)}
+        "knn16_roofline": query_roofline(knc, n, 132, 16, ms_knn, peak, n * 144 + 32 * nn + 16 * n),
+        "lowest_id_rule_100k_sample": {"closest_point_ms": ms_cp_low, "knn16_ms": ms_knn_low,
+                                       "prims_tested_per_query": low["prims"] / len(qsam)}}
     del pts, qs, boxes
 
 
@@ -767,6 +788,24 @@ def run_ours(args):
     sptr = ctypes.c_void_p(stream.cuda_stream)
     cb = CBuild(bq, boxes_t, n)
 
+    if args.only_tri:
+        verts, tris = W.icosphere(args.mesh_level)
+        tv, tt = torch.from_numpy(verts).cuda(), torch.from_numpy(tris).cuda()
+        tq = torch.from_numpy(W.uniform_points(args.queries, W.SEED_QUERIES, -1.5, 1.5)).cuda()
+        tb = bq.cuda.radixBuilder(bq.triangles.boxes(tt, tv))
+        ms_t = time_loop(lambda: bq.triangles.findClosest(tb, tt, tv, tq), args.steps, args.warmup, world)
+        if rank == 0:
+            print(json.dumps({"only_tri": True, "triangles": len(tris), "queries": args.queries, "forward_ms": ms_t}))
+        tb.free()
+        return
+    if args.only_wide:
+        wb = bq.gpuBuilderWide(boxes_t, 4)
+        qs = torch.from_numpy(W.uniform_points(args.queries, W.SEED_QUERIES)).cuda()
+        ms_w = time_loop(lambda: bq.points.findClosest(wb, tp, qs), args.steps, args.warmup, world)
+        if rank == 0:
+            print(json.dumps({"only_wide": True, "points": n, "queries": args.queries, "wide4_closest_point_ms": ms_w}))
+        wb.free()
+        return
     if args.only_queries:
         bvh = bq.cuda.radixBuilder(boxes_t)
         qs = torch.from_numpy(W.uniform_points(args.queries, W.SEED_QUERIES)).cuda()

@@ -81,7 +81,7 @@ class bq_tuning(ctypes.Structure):
 
 class bq_query_config(ctypes.Structure):
     _fields_ = [("tieMode", ctypes.c_int), ("stackDepth", ctypes.c_int), ("blockSize", ctypes.c_int),
-                ("reorder", ctypes.c_int), ("queriesPerWarp", ctypes.c_int)]
+                ("reorder", ctypes.c_int), ("queriesPerWarp", ctypes.c_int), ("lanesPerQuery", ctypes.c_int)]
 
 
 _P = ctypes.c_void_p
@@ -419,8 +419,8 @@ class cuda:
         bvh.free()
 
 
-def query_config(tieMode=TIES_LOWEST_ID, stackDepth=64, blockSize=128, reorder=1, queriesPerWarp=32):
-    return bq_query_config(tieMode, stackDepth, blockSize, reorder, queriesPerWarp)
+def query_config(tieMode=TIES_LOWEST_ID, stackDepth=64, blockSize=128, reorder=1, queriesPerWarp=32, lanesPerQuery=1):
+    return bq_query_config(tieMode, stackDepth, blockSize, reorder, queriesPerWarp, lanesPerQuery)
 
 
 def _vec3(t, name):

@@ -181,6 +181,163 @@ __global__ void k_knn_deep(const Node *__restrict__ nodes, const uint32_t *__res
   }
 }
 
+// ------------------------------------------------------------------
+// kNN with G lanes per query: the group walks the tree together (every
+// lane runs the same traversal on the same query, so the group never
+// diverges and node loads are broadcast) and holds the sorted top-k list
+// one candidate per lane (lane j: the j-th best).  A leaf's prims are
+// tested G at a time, one per lane; each candidate that beats the k-th best
+// is placed with one ballot (how many entries it follows) and moved in with
+// one __shfl_up_sync.  k <= G.
+// ------------------------------------------------------------------
+template <int G, int TIE>
+struct GroupKnnLeaf {
+  const uint32_t *__restrict__ primIDs;
+  const float *__restrict__ points;
+  float qx, qy, qz;
+  float maxSqr;
+  int k;
+  uint32_t lane;   // lane in the group
+  uint32_t gmask;  // the group's lanes in the warp
+  float D;         // this lane's list entry
+  int32_t I;
+  __device__ __forceinline__ bool before(float d, int32_t id, float D2, int32_t I2) const
+  {
+    return cand_before<TIE>(d, id, D2, I2);
+  }
+  __device__ __forceinline__ float worst() const { return __shfl_sync(gmask, D, k - 1, G); }
+  // place candidate (d, id), already known to beat the k-th best
+  __device__ __forceinline__ void insert(float d, int32_t id)
+  {
+    // entries the candidate stays behind: all lanes below its position
+    const uint32_t behind = __ballot_sync(gmask, lane < (uint32_t)k && !before(d, id, D, I)) & gmask;
+    const uint32_t pos = __popc(behind);
+    const float upD = __shfl_up_sync(gmask, D, 1, G);
+    const int32_t upI = __shfl_up_sync(gmask, I, 1, G);
+    if (lane == pos) {
+      D = d;
+      I = id;
+    } else if (lane > pos) {
+      D = upD;
+      I = upI;
+    }
+  }
+  __device__ __forceinline__ float operator()(uint64_t off, uint32_t cnt)
+  {
+    float w = worst();
+    for (uint32_t base = 0; base < cnt; base += G) {
+      float d = INFINITY;
+      int32_t pid = 0x7fffffff;
+      const bool mine = base + lane < cnt;
+      if (mine) {
+        pid = (int32_t)__ldg(primIDs + off + base + lane);
+        const float *p = points + 3ull * pid;
+        d = sqr_pp(__ldg(p), __ldg(p + 1), __ldg(p + 2), qx, qy, qz);
+      }
+      const bool ok = mine && (TIE == TIE_REFERENCE || d < maxSqr);
+      // candidates of this round that beat the k-th best, handled in prim order
+      uint32_t m = __ballot_sync(gmask, ok && before(d, pid, w, __shfl_sync(gmask, I, k - 1, G))) & gmask;
+      while (m) {
+        const int src = __ffs(m) - 1;
+        const float cd = __shfl_sync(gmask, d, src & (G - 1), G);
+        const int32_t ci = __shfl_sync(gmask, pid, src & (G - 1), G);
+        insert(cd, ci);
+        w = worst();
+        const int32_t wi = __shfl_sync(gmask, I, k - 1, G);
+        m &= ~(1u << src);
+        m &= __ballot_sync(gmask, ok && before(d, pid, w, wi)) & gmask;
+      }
+    }
+    return fminf(maxSqr, w);
+  }
+};
+
+template <int G, int TIE, int STACK>
+__global__ void __launch_bounds__(128) k_knn_group(const Node *__restrict__ nodes, const uint32_t *__restrict__ primIDs,
+                                                   const float *__restrict__ points, const float *__restrict__ queries,
+                                                   const uint32_t *__restrict__ order, uint32_t nq, int k,
+                                                   float maxSqr, int32_t *__restrict__ outIds,
+                                                   float *__restrict__ outD, int32_t *__restrict__ numFound,
+                                                   uint32_t *__restrict__ ovfList, uint32_t *ovfCount)
+{
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t t = gt / G;  // the group's query slot (whole groups leave together)
+  if (t >= nq) return;
+  const uint32_t lane = threadIdx.x & (G - 1);
+  const uint32_t gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1) << ((threadIdx.x & 31) & ~(G - 1)));
+  const uint32_t qi = order ? __ldg(order + t) : t;
+  const float *q = queries + 3ull * qi;
+  GroupKnnLeaf<G, TIE> leaf;
+  leaf.primIDs = primIDs;
+  leaf.points = points;
+  leaf.qx = __ldg(q);
+  leaf.qy = __ldg(q + 1);
+  leaf.qz = __ldg(q + 2);
+  leaf.maxSqr = maxSqr;
+  leaf.k = k;
+  leaf.lane = lane;
+  leaf.gmask = gmask;
+  // lanes past k hold a sentinel that every candidate stays behind
+  leaf.D = lane < (uint32_t)k ? INFINITY : -1.0f;
+  leaf.I = lane < (uint32_t)k ? 0x7fffffff : -1;
+  LocalStack<STACK> st;
+  if (!traverse<TIE>(nodes, leaf.qx, leaf.qy, leaf.qz, maxSqr, st, leaf)) {
+    if (lane == 0) ovfList[atomicAdd(ovfCount, 1u)] = qi;
+    return;
+  }
+  const bool real = leaf.I != 0x7fffffff && leaf.D != INFINITY;
+  if (lane < (uint32_t)k) {
+    outIds[(size_t)qi * k + lane] = real ? leaf.I : -1;
+    outD[(size_t)qi * k + lane] = real ? leaf.D : INFINITY;
+  }
+  const uint32_t found = __popc(__ballot_sync(gmask, lane < (uint32_t)k && real) & gmask);
+  if (numFound && lane == 0) numFound[qi] = (int32_t)found;
+}
+
+template <int G, int TIE, int STACK>
+void launch_knn_group(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, int k,
+                      float maxSqr, int block, int32_t *ids, float *d, int32_t *nf, QueryScratch &qs, cudaStream_t s)
+{
+  const Node *nodes = (const Node *)bvh->nodes;
+  {
+    ProfScope ps("query.knn_group", s);
+    k_knn_group<G, TIE, STACK><<<div_up((uint64_t)nq * G, block), block, 0, s>>>(
+        nodes, bvh->primIDs, points, queries, qs.order, nq, k, maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount);
+  }
+  // overflowing queries: the per-thread deep-stack kernel (same answers)
+  ProfScope ps("query.deep", s);
+  if (k <= 4)
+    k_knn_deep<4, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d,
+                                                          nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+  else if (k <= 8)
+    k_knn_deep<8, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d,
+                                                          nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+  else if (k <= 16)
+    k_knn_deep<16, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d,
+                                                           nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+  else
+    k_knn_deep<32, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d,
+                                                           nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+}
+
+template <int TIE>
+void dispatch_knn_group(int G, int stack, const bq_bvh3f *bvh, const float *points, const float *queries,
+                        uint32_t nq, int k, float maxSqr, int block, int32_t *ids, float *d, int32_t *nf,
+                        QueryScratch &qs, cudaStream_t s)
+{
+#define BQ_KG(GG)                                                                                              \
+  do {                                                                                                         \
+    if (stack <= 32) launch_knn_group<GG, TIE, 32>(bvh, points, queries, nq, k, maxSqr, block, ids, d, nf, qs, s);  \
+    else if (stack <= 64) launch_knn_group<GG, TIE, 64>(bvh, points, queries, nq, k, maxSqr, block, ids, d, nf, qs, s); \
+    else launch_knn_group<GG, TIE, 128>(bvh, points, queries, nq, k, maxSqr, block, ids, d, nf, qs, s);          \
+  } while (0)
+  if (G == 4) BQ_KG(4);
+  else if (G == 8) BQ_KG(8);
+  else if (G == 16) BQ_KG(16);
+  else BQ_KG(32);
+#undef BQ_KG
+}
+
 template <int TIE, int STACK>
 void launch_cp(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t nq, float maxSqr,
                int block, int32_t *ids, float *d, QueryScratch &qs, cudaStream_t s, CpExclude ex)
@@ -347,6 +504,10 @@ int query_config(const bq_query_config *q, bq_query_config &out)
   out.blockSize = (q && q->blockSize) ? q->blockSize : 128;
   out.reorder = q ? q->reorder : 1;
   out.queriesPerWarp = (q && q->queriesPerWarp) ? q->queriesPerWarp : 32;
+  out.lanesPerQuery = (q && q->lanesPerQuery) ? q->lanesPerQuery : 1;
+  if (out.lanesPerQuery != 1 && out.lanesPerQuery != 4 && out.lanesPerQuery != 8 && out.lanesPerQuery != 16 &&
+      out.lanesPerQuery != 32)
+    return set_error(BQ_ERR_INVALID_ARGUMENT, "lanesPerQuery must be 1, 4, 8, 16 or 32");
   if (out.tieMode != BQ_TIES_LOWEST_ID && out.tieMode != BQ_TIES_REFERENCE)
     return set_error(BQ_ERR_INVALID_ARGUMENT, "tieMode must be BQ_TIES_LOWEST_ID or BQ_TIES_REFERENCE");
   if (out.stackDepth != 32 && out.stackDepth != 64 && out.stackDepth != 128)
@@ -404,6 +565,17 @@ int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t
   QueryScratch qs;
   BQ_TRY(prepare_queries((const float *)bvh->nodes, queries, nq, c.reorder != 0, tmp, al, qs));
   const int tie = c.tieMode, st = c.stackDepth, b = c.blockSize;
+  if (c.lanesPerQuery > 1) {
+    if (k > c.lanesPerQuery) return set_error(BQ_ERR_INVALID_ARGUMENT, "lanesPerQuery must be at least k");
+    if (tie == BQ_TIES_REFERENCE)
+      dispatch_knn_group<TIE_REFERENCE>(c.lanesPerQuery, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound,
+                                        qs, al.s);
+    else
+      dispatch_knn_group<TIE_LOWEST>(c.lanesPerQuery, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound,
+                                     qs, al.s);
+    BQ_CUDA(cudaGetLastError());
+    return finish_queries(qs, al);
+  }
   if (k <= 4) dispatch_knn_tie<4>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
   else if (k <= 8) dispatch_knn_tie<8>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);
   else if (k <= 16) dispatch_knn_tie<16>(tie, st, bvh, points, queries, nq, k, maxSqr, b, ids, d, numFound, qs, al.s);

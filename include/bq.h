@@ -113,6 +113,11 @@ typedef struct bq_query_config {
   int reorder;       /* 1 = process queries in Morton order, 0 = input order */
   int queriesPerWarp;/* one thread per query; queries a warp takes per work grab in the
                         persistent batched kernel (multiple of 32, <= 1024; 0 = 32) */
+  int lanesPerQuery; /* bq_knn_f3 only.  0 or 1: one thread per query, its top-k list in
+                        that thread's registers.  4, 8, 16 or 32 (at least k): a group of
+                        that many lanes per query walks the tree together and holds the
+                        sorted top-k list one candidate per lane; a new candidate is
+                        placed by one ballot and moved in by one warp shuffle */
 } bq_query_config;
 
 /* ---------------------------------------------------------------- */

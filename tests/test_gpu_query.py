@@ -233,3 +233,30 @@ def test_visit_counts_match_oracle_traversal(bq, oracle, tie, dist):
     k16 = bq.points.visitCounts(bvh, torch.from_numpy(pts).cuda(), torch.from_numpy(qs).cuda(), 16,
                                 qcfg=bq.query_config(tieMode=tie))
     assert k16["inner_nodes"] > c["inner_nodes"] and k16["prims"] >= 16 * len(qs)
+
+
+@pytest.mark.parametrize("lanes,k", [(4, 4), (8, 5), (16, 16), (32, 16), (32, 32)])
+@pytest.mark.parametrize("tie", [0, 1])
+@pytest.mark.parametrize("dist", ["uniform", "gmm"])
+def test_knn_lane_groups_match_oracle(bq, oracle, lanes, k, tie, dist):
+    """kNN with a group of lanes per query (the top-k list spread over the
+    group, one candidate per lane, merged by warp shuffles) gives exactly the
+    per-thread answers, on leaf-1 and leaf-8 trees."""
+    pts, qs = _data(dist, 30000, 5000)
+    for thr in (0, 8):
+        bvh = _tree(bq, "morton", pts, thr)
+        n, pr = bvh.to_host()
+        ids, d, nf = bq.points.findKNN(bvh, torch.from_numpy(pts).cuda(), torch.from_numpy(qs).cuda(), k,
+                                       qcfg=bq.query_config(tieMode=tie, lanesPerQuery=lanes))
+        oi, od, onf, _ = oracle.knn(n, pr, pts, qs, k, fma_mode=1, tie_mode=tie)
+        assert np.array_equal(ids.cpu().numpy(), oi), f"leaf {thr}"
+        assert np.array_equal(d.cpu().numpy(), od)
+        assert np.array_equal(nf.cpu().numpy(), onf)
+
+
+def test_knn_lane_groups_reject_k_above_group(bq):
+    pts, qs = _data("uniform", 1000, 100)
+    bvh = _tree(bq, "morton", pts)
+    with pytest.raises(bq.BQError):
+        bq.points.findKNN(bvh, torch.from_numpy(pts).cuda(), torch.from_numpy(qs).cuda(), 16,
+                          qcfg=bq.query_config(lanesPerQuery=8))
