@@ -114,7 +114,6 @@ struct AggArgsT {
   uint2 *pending;         // 2 per chunk: nodes handed to the global phase
   const uint32_t *off;    // SEG: cloud offsets
   uint32_t numSegs;
-  const uint32_t *skipIf = nullptr;  // optional: both phases do nothing while *skipIf != 0
 };
 using AggArgs = AggArgsT<uint8_t>;
 
@@ -127,8 +126,19 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
   const uint32_t nv = *a.nvPtr;
   const uint32_t c0 = blockIdx.x * AGG_CHUNK;
   if (c0 >= nv) return;  // whole CTA: no barrier below is skipped by part of it
-  if (a.skipIf && *a.skipIf) return;  // whole CTA, as above
   const uint32_t cEnd = c0 + AGG_CHUNK;  // first split position outside the chunk
+  // this thread's prim id and its box (a random gather) first, so that their
+  // latency overlaps the staging of the chunk's levels below
+  const uint32_t i = c0 + threadIdx.x;
+  uint32_t id = 0;
+  float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0;
+  if (i < nv) {
+    id = __ldg(a.ids + i);
+    const float2 *bp = reinterpret_cast<const float2 *>(a.boxes + id);
+    p0 = __ldg(bp);
+    p1 = __ldg(bp + 1);
+    p2 = __ldg(bp + 2);
+  }
   for (int j = threadIdx.x; j <= AGG_CHUNK; j += blockDim.x) sSlot[j] = AGG_EMPTY;
   for (int j = threadIdx.x; j < AGG_CHUNK + 2; j += blockDim.x) {
     const int64_t g = (int64_t)c0 - 1 + j;  // pairs (g, g+1) exist for 0 <= g < nv - 1
@@ -136,16 +146,12 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
   }
   if (threadIdx.x < 2) a.pending[2 * blockIdx.x + threadIdx.x] = make_uint2(AGG_EMPTY, AGG_EMPTY);
   __syncthreads();
-  const uint32_t i = c0 + threadIdx.x;
   if (i < nv) {
     uint32_t b0, e0;
     agg_range<SEG>(i, nv, a.off, a.numSegs, b0, e0);
     const uint64_t nodeBase = SEG ? 2ull * b0 : 0ull;
-    const uint32_t id = __ldg(a.ids + i);
     if (SEG) a.primIDsOut[i] = id - b0;
     if (i == b0) a.nodes[nodeBase + 1] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0);
-    const float2 *bp = reinterpret_cast<const float2 *>(a.boxes + id);
-    const float2 p0 = __ldg(bp), p1 = __ldg(bp + 1), p2 = __ldg(bp + 2);
     AggBox box{p0.x, p0.y, p1.x, p1.y, p2.x, p2.y};
     uint32_t l = i, r = i;
     uint64_t admin = make_admin(i - b0, 1);
@@ -194,7 +200,6 @@ __global__ void k_agg_global(AggArgsT<LevT> a, uint32_t numPending)
 {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numPending) return;
-  if (a.skipIf && *a.skipIf) return;  // the local phase did nothing either
   const uint32_t nv = *a.nvPtr;
   if ((uint64_t)(t / 2) * AGG_CHUNK >= nv) return;  // chunk had no prims: entry never written
   const uint2 pr = a.pending[t];

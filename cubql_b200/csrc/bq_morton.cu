@@ -791,12 +791,20 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   grid = div_up(n, chunk);
 
   TempSet tmp(al);
+  // the build's state and the long-run statistics side by side, so that
+  // one copy reads back everything the host needs
+  struct Ctl {
+    BuildState st;
+    RunStats runs;
+  };
+  Ctl *ctl = nullptr;
   BuildState *st = nullptr;
   Partial *partials = nullptr;
   uint32_t *blockOff = nullptr, *hist = nullptr, *slot = nullptr;
   uint64_t *keysA = nullptr, *keysB = nullptr;
   uint8_t *delta = nullptr;
-  BQ_TRY(tmp.get(&st, 1));
+  BQ_TRY(tmp.get(&ctl, 1));
+  st = &ctl->st;
   BQ_TRY(tmp.get(&partials, grid));
   BQ_TRY(tmp.get(&blockOff, grid));
   // more than 2^24 prims: sort 32 top bits in 4 passes instead of 24 in 3
@@ -843,47 +851,39 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   uint32_t *ids = ids2[sel];
   uint32_t *idsOther = ids2[sel ^ 1];
   const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
-  RunStats *rs = nullptr;
+  RunStats *rs = &ctl->runs;
   uint4 *runs = nullptr;
-  if ((s = tmp.get(&rs, 1)) != BQ_OK || (s = tmp.get(&runs, maxRuns)) != BQ_OK) return fail(s);
+  if ((s = tmp.get(&runs, maxRuns)) != BQ_OK) return fail(s);
   s = wide4 ? fix_runs<MB_SB4>(keys, ids, n, &st->numValid, delta, slot, rs, runs, maxRuns, al)
             : fix_runs<MB_SB3>(keys, ids, n, &st->numValid, delta, slot, rs, runs, maxRuns, al);
   if (s != BQ_OK) return fail(s);
   uint2 *pending = nullptr;
   if ((s = tmp.get(&pending, 2ull * div_up(n, AGG_CHUNK))) != BQ_OK) return fail(s);
   AggArgs ag{delta, slot, ids, boxes, nodes, nullptr, &st->numValid, nullptr, pending, nullptr, 0};
-  // what the host reads back: the long-run statistics, the valid count, the error word
+  // what the host reads back (one copy): the long-run statistics, the valid
+  // count, the error word
   struct { RunStats runs; uint32_t nv, err; } h = {};
   auto read_back = [&]() -> cudaError_t {
-    cudaError_t e = cudaMemcpyAsync(&h.runs, rs, sizeof(RunStats), cudaMemcpyDeviceToHost, al.s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&h.nv, &st->numValid, 4, cudaMemcpyDeviceToHost, al.s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&h.err, &st->err, 4, cudaMemcpyDeviceToHost, al.s);
+    Ctl hc;
+    cudaError_t e = cudaMemcpyAsync(&hc, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, al.s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(al.s);
+    h.runs = hc.runs;
+    h.nv = hc.st.numValid;
+    h.err = hc.st.err;
     return e;
   };
   auto do_long_runs = [&]() -> int {
     return wide4 ? long_runs<MB_SB4>(h.runs, runs, keys, ids, keys2[sel ^ 1], idsOther, delta, &st->err, al)
                  : long_runs<MB_SB3>(h.runs, runs, keys, ids, keys2[sel ^ 1], idsOther, delta, &st->err, al);
   };
+  // the long-run statistics decide what runs next (one read back)
+  if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
+  if (h.runs.pad) return fail(set_error(BQ_ERR_CUDA, "run list overflow in the Morton build"));
+  if ((s = do_long_runs()) != BQ_OK) return fail(s);
   if (thr == 1) {
-    // Leaf 1: the agglomeration is queued at once and does nothing if long
-    // runs turn up (their levels are not written yet); then the one read
-    // back of the common case.  With long runs: their pass, the
-    // agglomeration again, a second read back.
-    ag.skipIf = &rs->count;
     if ((s = agglomerate<false>(ag, n, al.s, "morton.agg_local", "morton.agg_global")) != BQ_OK) return fail(s);
     if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
-    if (h.runs.pad) return fail(set_error(BQ_ERR_CUDA, "run list overflow in the Morton build"));
-    if (h.runs.count) {
-      if ((s = do_long_runs()) != BQ_OK) return fail(s);
-      ag.skipIf = nullptr;
-      if ((s = agglomerate<false>(ag, n, al.s, "morton.agg_local", "morton.agg_global")) != BQ_OK) return fail(s);
-      if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
-    }
   } else {
-    if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
-    if (h.runs.pad) return fail(set_error(BQ_ERR_CUDA, "run list overflow in the Morton build"));
-    if ((s = do_long_runs()) != BQ_OK) return fail(s);
     Node *full = nullptr;
     uint2 *ranges = nullptr;
     uint32_t *kept = nullptr, *rank = nullptr, *total = nullptr;

@@ -23,6 +23,15 @@
 namespace bq {
 namespace {
 
+// stack entries a closest-point thread keeps in shared memory (the top of
+// its traversal stack); the rest of the stack is in local memory.  8 took
+// 10M closest-point queries from 4.17 to 3.69 ms (4: 3.92, 12: 3.83, 16:
+// 3.99).  The kNN kernel, at 62 registers and fewer threads per SM, gained
+// nothing from it (29.7 ms with none, 29.8-30.3 with 4..16), so its stack
+// stays in local memory.
+constexpr int SMEM_STACK = 8;
+constexpr int KNN_SMEM_STACK = 0;
+
 // rootBox: lower xyz, upper xyz (the first 24 bytes of a binary root node)
 __global__ void k_query_keys(const float *__restrict__ rootBox, const float *__restrict__ queries, uint32_t nq,
                              uint32_t *__restrict__ keys, uint32_t *__restrict__ idx)
@@ -64,7 +73,8 @@ __global__ void __launch_bounds__(128) k_closest(const Node *__restrict__ nodes,
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const uint32_t qi = order ? __ldg(order + t) : t;
-  LocalStack<STACK> st;
+  extern __shared__ StackEntry sStack[];
+  HybridStack<SMEM_STACK, STACK> st(sStack);
   if (!run_cp<TIE>(nodes, primIDs, points, queries, qi, maxSqr, st, outIds, outD, ex))
     ovfList[atomicAdd(ovfCount, 1u)] = qi;
 }
@@ -154,7 +164,8 @@ __global__ void __launch_bounds__(128) k_knn(const Node *__restrict__ nodes, con
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const uint32_t qi = order ? __ldg(order + t) : t;
-  LocalStack<STACK> st;
+  extern __shared__ StackEntry sStack[];
+  HybridStack<KNN_SMEM_STACK, STACK> st(sStack);
   if (!run_knn<K, TIE>(nodes, primIDs, points, queries, qi, k, maxSqr, st, outIds, outD, numFound))
     ovfList[atomicAdd(ovfCount, 1u)] = qi;
 }
@@ -224,7 +235,10 @@ struct GroupKnnLeaf {
   }
   __device__ __forceinline__ float operator()(uint64_t off, uint32_t cnt)
   {
+    // every shuffle below runs on all lanes of the group (never inside a
+    // condition that only some lanes take)
     float w = worst();
+    int32_t wi = __shfl_sync(gmask, I, k - 1, G);
     for (uint32_t base = 0; base < cnt; base += G) {
       float d = INFINITY;
       int32_t pid = 0x7fffffff;
@@ -236,14 +250,14 @@ struct GroupKnnLeaf {
       }
       const bool ok = mine && (TIE == TIE_REFERENCE || d < maxSqr);
       // candidates of this round that beat the k-th best, handled in prim order
-      uint32_t m = __ballot_sync(gmask, ok && before(d, pid, w, __shfl_sync(gmask, I, k - 1, G))) & gmask;
+      uint32_t m = __ballot_sync(gmask, ok && before(d, pid, w, wi)) & gmask;
       while (m) {
         const int src = __ffs(m) - 1;
         const float cd = __shfl_sync(gmask, d, src & (G - 1), G);
         const int32_t ci = __shfl_sync(gmask, pid, src & (G - 1), G);
         insert(cd, ci);
         w = worst();
-        const int32_t wi = __shfl_sync(gmask, I, k - 1, G);
+        wi = __shfl_sync(gmask, I, k - 1, G);
         m &= ~(1u << src);
         m &= __ballot_sync(gmask, ok && before(d, pid, w, wi)) & gmask;
       }
@@ -345,8 +359,8 @@ void launch_cp(const bq_bvh3f *bvh, const float *points, const float *queries, u
   const Node *nodes = (const Node *)bvh->nodes;
   {
     ProfScope ps("query.closest", s);
-    k_closest<TIE, STACK><<<div_up(nq, block), block, 0, s>>>(nodes, bvh->primIDs, points, queries, qs.order, nq,
-                                                             maxSqr, ids, d, qs.ovfList, qs.ovfCount, ex);
+    k_closest<TIE, STACK><<<div_up(nq, block), block, SMEM_STACK * sizeof(StackEntry) * block, s>>>(
+        nodes, bvh->primIDs, points, queries, qs.order, nq, maxSqr, ids, d, qs.ovfList, qs.ovfCount, ex);
   }
   ProfScope ps("query.deep", s);
   k_closest_deep<TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, maxSqr, ids, d,
@@ -360,8 +374,8 @@ void launch_knn(const bq_bvh3f *bvh, const float *points, const float *queries, 
   const Node *nodes = (const Node *)bvh->nodes;
   {
     ProfScope ps("query.knn", s);
-    k_knn<K, TIE, STACK><<<div_up(nq, block), block, 0, s>>>(nodes, bvh->primIDs, points, queries, qs.order, nq, k,
-                                                            maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount);
+    k_knn<K, TIE, STACK><<<div_up(nq, block), block, KNN_SMEM_STACK * sizeof(StackEntry) * block, s>>>(
+        nodes, bvh->primIDs, points, queries, qs.order, nq, k, maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount);
   }
   ProfScope ps("query.deep", s);
   k_knn_deep<K, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d, nf,

@@ -8,10 +8,12 @@
 // tile of TILE = 256*ITEMS pairs (tile order from an atomic counter, so a
 // tile only ever waits on tiles that already started):
 //   1. loads its keys (warp-contiguous, coalesced),
-//   2. ranks them stably with __match_any_sync: per warp, per round of 32
-//      consecutive keys, peers with the same digit share one update of a
-//      warp-private digit histogram in shared memory; each warp runs two
-//      such chains (first and second half of its keys) interleaved,
+//   2. ranks them stably: per warp, per round of 32 consecutive keys, the
+//      lanes holding the same digit (found with __match_any_sync, or with
+//      nine ballots when the warp's first round shows many distinct digits:
+//      match-any gets slower the more groups a round has) share one update
+//      of a warp-private digit histogram in shared memory; each warp runs
+//      two such chains (first and second half of its keys) interleaved,
 //   3. publishes its 256 digit counts and resolves its global digit
 //      offsets by decoupled look-back over earlier tiles (one thread per
 //      digit; every wait is bounded and aborts the whole pass on timeout),
@@ -21,6 +23,7 @@
 // digits (or from the producer of the keys, see *_prehist).
 #include <algorithm>
 #include <atomic>
+#include <type_traits>
 
 #include "bq_internal.cuh"
 
@@ -45,6 +48,24 @@ __device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p)
 {
   return *(const volatile uint32_t *)p;
 }
+
+
+// lanes holding the same value v in [0, 512): nine ballots (warp multi-split)
+__device__ __forceinline__ uint32_t match9(uint32_t v)
+{
+  uint32_t peers = 0xffffffffu;
+#pragma unroll
+  for (int b = 0; b < 9; b++) {
+    const bool bit = (v >> b) & 1u;
+    const uint32_t m = __ballot_sync(0xffffffffu, bit);
+    peers &= bit ? m : ~m;
+  }
+  return peers;
+}
+
+// a warp whose first round holds more distinct digits than this ranks the
+// rest of its keys with ballots instead of match-any
+constexpr int MATCH_GROUPS_MAX = 12;
 
 template <typename KeyT>
 __device__ __forceinline__ uint32_t digit_of(KeyT k, int shift)
@@ -115,7 +136,11 @@ struct PassCtl {
   int holdTile0;       // test hook: tile 0 never publishes (every wait on it runs out)
 };
 
-template <typename KeyT, int ITEMS>
+// WORD: -1 ranks on the whole key; 0 / 1 on the low / high 32-bit word of a
+// 64-bit key when the pass's digit lies inside that word.  Ranking on one
+// word holds half the registers (no spills at 64 registers a thread); the
+// whole keys are read again, from L2, when they are staged for the scatter.
+template <typename KeyT, int ITEMS, int WORD>
 __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restrict__ keysIn, KeyT *__restrict__ keysOut,
                                                             const uint32_t *__restrict__ valsIn,
                                                             uint32_t *__restrict__ valsOut, uint32_t nHost,
@@ -152,12 +177,19 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
   const uint32_t tile = sTile;
   const uint64_t warpBase = (uint64_t)tile * TILE + (uint64_t)warp * WARP_ITEMS;
 
-  // 1. keys (warp-contiguous sub-tiles, coalesced)
-  KeyT key[ITEMS];
+  // 1. keys (warp-contiguous sub-tiles, coalesced), or the word of each key
+  // that holds the digit
+  static_assert(WORD < 0 || sizeof(KeyT) == 8, "word ranking is for 64-bit keys");
+  using RankT = typename std::conditional<(WORD >= 0), uint32_t, KeyT>::type;
+  const int rshift = WORD == 1 ? shift - 32 : shift;
+  RankT key[ITEMS];
 #pragma unroll
   for (int r = 0; r < ITEMS; r++) {
     const uint64_t idx = warpBase + (uint64_t)r * 32 + lane;
-    key[r] = idx < n ? keysIn[idx] : (KeyT)0;
+    if constexpr (WORD >= 0)
+      key[r] = idx < n ? __ldg(reinterpret_cast<const uint32_t *>(keysIn) + 2 * idx + WORD) : 0u;
+    else
+      key[r] = idx < n ? keysIn[idx] : (KeyT)0;
   }
 
   // 2. stable ranking inside each warp, as two independent chains (rounds
@@ -171,14 +203,26 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
   // within (warp, chain, digit), later the tile-local position (< 2^16;
   // 0xffff marks an item past the end)
   uint32_t pos2[HALF];
+  bool byBallot = false;  // warp-uniform, chosen in round 0
 #pragma unroll
   for (int r = 0; r < HALF; r++) {
     const bool v0 = warpBase + (uint64_t)r * 32 + lane < n;
     const bool v1 = warpBase + (uint64_t)(r + HALF) * 32 + lane < n;
-    const uint32_t d0 = v0 ? digit_of(key[r], shift) : 256u;  // 256: padding slot, never read back
-    const uint32_t d1 = v1 ? digit_of(key[r + HALF], shift) : 256u;
-    const uint32_t p0 = __match_any_sync(0xffffffffu, d0);
-    const uint32_t p1 = __match_any_sync(0xffffffffu, d1);
+    const uint32_t d0 = v0 ? digit_of(key[r], rshift) : 256u;  // 256: padding slot, never read back
+    const uint32_t d1 = v1 ? digit_of(key[r + HALF], rshift) : 256u;
+    uint32_t p0, p1;
+    if (r == 0) {
+      p0 = __match_any_sync(0xffffffffu, d0);
+      p1 = __match_any_sync(0xffffffffu, d1);
+      const uint32_t groups = __popc(__ballot_sync(0xffffffffu, (p0 & geMask) == (1u << lane)));
+      byBallot = groups > MATCH_GROUPS_MAX;
+    } else if (byBallot) {
+      p0 = match9(d0);
+      p1 = match9(d1);
+    } else {
+      p0 = __match_any_sync(0xffffffffu, d0);
+      p1 = __match_any_sync(0xffffffffu, d1);
+    }
     const uint32_t b0 = wh0[d0];
     const uint32_t b1 = wh1[d1];
     __syncwarp();
@@ -247,17 +291,20 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
     uint32_t lo = pos2[r] & 0xffffu, hi = pos2[r] >> 16;
     const bool v0 = warpBase + (uint64_t)r * 32 + lane < n;
     const bool v1 = warpBase + (uint64_t)(r + HALF) * 32 + lane < n;
-    const uint32_t d0 = digit_of(key[r], shift), d1 = digit_of(key[r + HALF], shift);
+    const uint32_t d0 = digit_of(key[r], rshift), d1 = digit_of(key[r + HALF], rshift);
     lo = v0 ? sTileStart[d0] + sWarpHist[(2 * warp) * 257 + d0] + lo : 0xffffu;
     hi = v1 ? sTileStart[d1] + sWarpHist[(2 * warp + 1) * 257 + d1] + hi : 0xffffu;
     pos2[r] = lo | (hi << 16);
   }
   __syncthreads();  // histograms dead: the tile buffers may be written now
+  // the whole keys, read again (from L2): the ranking copies are dead after
+  // the positions, so nothing is held in registers across the look-back
 #pragma unroll
   for (int r = 0; r < HALF; r++) {
     const uint32_t lo = pos2[r] & 0xffffu, hi = pos2[r] >> 16;
-    if (lo != 0xffffu) sKeys[lo] = key[r];
-    if (hi != 0xffffu) sKeys[hi] = key[r + HALF];
+    const uint64_t i0 = warpBase + (uint64_t)r * 32 + lane, i1 = warpBase + (uint64_t)(r + HALF) * 32 + lane;
+    if (lo != 0xffffu) sKeys[lo] = keysIn[i0];
+    if (hi != 0xffffu) sKeys[hi] = keysIn[i1];
   }
   uint32_t val[ITEMS];
 #pragma unroll
@@ -345,7 +392,14 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
   while (inject > 0 && !g_injectSortTimeout.compare_exchange_weak(inject, inject - 1)) {
   }
   const size_t smemBytes = (sizeof(KeyT) + sizeof(uint32_t)) * TILE;
-  BQ_CUDA(cudaFuncSetAttribute(k_onesweep<KeyT, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemBytes));
+  BQ_CUDA(cudaFuncSetAttribute(k_onesweep<KeyT, ITEMS, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smemBytes));
+  if constexpr (sizeof(KeyT) == 8) {
+    BQ_CUDA(cudaFuncSetAttribute(k_onesweep<KeyT, ITEMS, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smemBytes));
+    BQ_CUDA(cudaFuncSetAttribute(k_onesweep<KeyT, ITEMS, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smemBytes));
+  }
   int sel = 0;
   for (int p = 0; p < numPasses; p++) {
     PassCtl c;
@@ -357,8 +411,24 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
     c.spinLimit = inject > 0 ? INJECTED_SPIN_LIMIT : SPIN_LIMIT;
     c.holdTile0 = inject > 0 && p == 0 && numTiles > 1;
     ProfScope ps(sizeof(KeyT) == 8 ? "sort.onesweep64" : "sort.onesweep32", al.s);
-    k_onesweep<KeyT, ITEMS><<<numTiles, SORT_BLOCK, smemBytes, al.s>>>(keys[sel], keys[sel ^ 1], vals[sel],
-                                                                       vals[sel ^ 1], nMax, nDev, beginBit + 8 * p, c);
+    const int sh = beginBit + 8 * p;
+    // the 32-bit word of a 64-bit key that holds this pass's digit, if one does
+    const int word = sizeof(KeyT) != 8 ? -1 : sh >= 32 ? 1 : sh + 8 <= 32 ? 0 : -1;
+    bool launched = false;
+    if constexpr (sizeof(KeyT) == 8) {
+      if (word >= 0) {
+        if (word == 1)
+          k_onesweep<KeyT, ITEMS, 1><<<numTiles, SORT_BLOCK, smemBytes, al.s>>>(keys[sel], keys[sel ^ 1], vals[sel],
+                                                                              vals[sel ^ 1], nMax, nDev, sh, c);
+        else
+          k_onesweep<KeyT, ITEMS, 0><<<numTiles, SORT_BLOCK, smemBytes, al.s>>>(keys[sel], keys[sel ^ 1], vals[sel],
+                                                                              vals[sel ^ 1], nMax, nDev, sh, c);
+        launched = true;
+      }
+    }
+    if (!launched)
+      k_onesweep<KeyT, ITEMS, -1><<<numTiles, SORT_BLOCK, smemBytes, al.s>>>(keys[sel], keys[sel ^ 1], vals[sel],
+                                                                           vals[sel ^ 1], nMax, nDev, sh, c);
     BQ_CUDA(cudaGetLastError());
     sel ^= 1;
   }

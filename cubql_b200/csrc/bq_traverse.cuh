@@ -42,6 +42,35 @@ struct LocalStack {
   __device__ __forceinline__ StackEntry pop() { return e[--sp]; }
 };
 
+// S entries in shared memory (this thread's column of a [S][blockDim]
+// array, so a warp's accesses to the same depth hit 32 different banks
+// pairs), the rest of N in local memory.  Shallow traversals never touch
+// local memory.
+template <int S, int N>
+struct HybridStack {
+  static_assert(S < N, "the shared part is the top of a deeper stack");
+  StackEntry *sh;  // &shared[0][threadIdx.x]
+  uint32_t stride; // blockDim.x
+  StackEntry e[N - S];
+  int sp = 0;
+  __device__ __forceinline__ HybridStack(StackEntry *base) : sh(base + threadIdx.x), stride(blockDim.x) {}
+  __device__ __forceinline__ bool push(uint32_t i, float d)
+  {
+    if (sp >= N) return false;
+    const StackEntry x{i, d};
+    if (sp < S) sh[(uint32_t)sp * stride] = x;
+    else e[sp - S] = x;
+    sp++;
+    return true;
+  }
+  __device__ __forceinline__ bool empty() const { return sp == 0; }
+  __device__ __forceinline__ StackEntry pop()
+  {
+    --sp;
+    return sp < S ? sh[(uint32_t)sp * stride] : e[sp - S];
+  }
+};
+
 // deep stack in a caller-provided global-memory slice
 struct GlobalStack {
   StackEntry *e;

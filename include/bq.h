@@ -16,7 +16,9 @@
  *   - the phase profiler's event pool (bq_profile_*, per thread, only
  *     while profiling is enabled);
  *   - the fixed scratch array of bq_refit_noalloc_f3 (shared by all of
- *     its calls; see there).
+ *     its calls; see there);
+ *   - the count of bq_debug_inject_sort_timeout (a test hook, 0 unless a
+ *     test sets it).
  * Apart from bq_refit_noalloc_f3, calls on different streams may run
  * concurrently.
  *
