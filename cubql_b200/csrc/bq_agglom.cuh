@@ -208,8 +208,13 @@ __global__ void k_agg_global(AggArgsT<LevT> a, uint32_t numPending)
   uint32_t b0, e0;
   agg_range<SEG>(l, nv, a.off, a.numSegs, b0, e0);
   const uint64_t nodeBase = SEG ? 2ull * b0 : 0ull;
+  // the split levels at the range's two boundaries, kept across steps: a
+  // step changes one boundary, so it loads one level, together with the
+  // sibling's box (one round trip to L2 per step besides the exchange)
+  LevT dl = l > b0 ? __ldg(a.delta + l - 1) : (LevT)0;
+  LevT dr = r < e0 - 1 ? __ldg(a.delta + r) : (LevT)0;
   // the node was written by the local phase: recover its box and admin
-  bool leftChild = (l == b0) ? true : (r == e0 - 1) ? false : (__ldg(a.delta + l - 1) > __ldg(a.delta + r));
+  bool leftChild = (l == b0) ? true : (r == e0 - 1) ? false : (dl > dr);
   uint32_t s = leftChild ? r + 1 : l;
   const Node me = ldcg_node(a.nodes + 2ull * s + (leftChild ? 0 : 1));
   AggBox box{me.a.x, me.a.y, me.a.z, me.a.w, me.b.x, me.b.y};
@@ -219,17 +224,20 @@ __global__ void k_agg_global(AggArgsT<LevT> a, uint32_t numPending)
       a.nodes[nodeBase] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
       return;
     }
-    leftChild = (l == b0) ? true : (r == e0 - 1) ? false : (__ldg(a.delta + l - 1) > __ldg(a.delta + r));
+    leftChild = (l == b0) ? true : (r == e0 - 1) ? false : (dl > dr);
     s = leftChild ? r + 1 : l;
     const uint64_t myPos = 2ull * s + (leftChild ? 0 : 1);
     a.nodes[myPos] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
     cuda::atomic_ref<uint32_t, cuda::thread_scope_device> slotRef(a.slot[s]);
     const uint32_t other = slotRef.exchange(leftChild ? l : r, cuda::memory_order_acq_rel);
     if (other == AGG_EMPTY) return;
+    if (leftChild) r = other; else l = other;
+    // independent loads: the sibling's box and the new boundary's level
     const Node sn = ldcg_node(a.nodes + (myPos ^ 1));
+    if (leftChild) dr = r < e0 - 1 ? __ldg(a.delta + r) : (LevT)0;
+    else dl = l > b0 ? __ldg(a.delta + l - 1) : (LevT)0;
     const AggBox sib{sn.a.x, sn.a.y, sn.a.z, sn.a.w, sn.b.x, sn.b.y};
     box = leftChild ? agg_union(box, sib) : agg_union(sib, box);
-    if (leftChild) r = other; else l = other;
     if (a.ranges) a.ranges[s] = make_uint2(l, r);
     admin = make_admin(2ull * s - nodeBase, 0);
   }
