@@ -60,7 +60,6 @@
 #include <cfloat>
 
 #include "bq_agglom.cuh"
-#include "bq_bulk.cuh"
 
 namespace bq {
 namespace {
@@ -99,94 +98,8 @@ __device__ __forceinline__ void load_box(const bq_box3f *boxes, uint64_t i, floa
 __device__ __forceinline__ float ctr(float lo, float hi) { return __fdiv_rn(__fadd_rn(lo, hi), 2.0f); }
 
 // ------------------------------------------------------------------
-// Boxes of a block's chunk, tile by tile (MB_BLOCK * MB_UNROLL boxes).
-// With BULK the tiles are streamed into shared memory by 1D bulk async
-// copies, double-buffered (the next tile is in flight while this one is
-// read); the odd last box of a chunk, if any, is read from global memory.
-// Without, every box is read from global memory.  Every wait is bounded:
-// a copy that never completes sets DEV_ERR_TIMEOUT, the block stops
-// reading, waits (bounded) for what it still has in flight and finishes its
-// reduction with what it has (the host reports the error).
-// ------------------------------------------------------------------
-constexpr int MB_TILE = MB_BLOCK * MB_UNROLL;
-constexpr uint32_t MB_WAIT_POLLS = 1u << 20;
-constexpr size_t MB_BULK_SMEM = 2ull * MB_TILE * sizeof(bq_box3f);  // two tile buffers, 48 KB
-
-template <bool BULK>
-struct BoxTiles {
-  const bq_box3f *boxes;
-  uint64_t begin, end;
-  uint32_t numTiles;
-  bq_box3f *buf;   // BULK: [2][MB_TILE] in shared memory
-  uint64_t *bar;   // BULK: two mbarriers in shared memory
-  uint32_t issued; // BULK, thread 0: tiles whose copies were issued
-
-  __device__ __forceinline__ uint32_t count(uint32_t k) const
-  {
-    return (uint32_t)min((uint64_t)MB_TILE, end - (begin + (uint64_t)k * MB_TILE));
-  }
-  // boxes of tile k copied by the bulk copy: an even count (a multiple of 16 bytes)
-  __device__ __forceinline__ uint32_t copied(uint32_t k) const { return BULK ? (count(k) & ~1u) : 0u; }
-  __device__ __forceinline__ void issue(uint32_t k)  // thread 0
-  {
-    const uint32_t c = copied(k);
-    if (c) bulk_load(buf + (size_t)(k & 1) * MB_TILE, boxes + begin + (uint64_t)k * MB_TILE,
-                     c * (uint32_t)sizeof(bq_box3f), &bar[k & 1]);
-    issued = k + 1;
-  }
-  // all threads: set up; thread 0 starts the first two copies
-  __device__ __forceinline__ void start()
-  {
-    if (!BULK) return;
-    if (threadIdx.x == 0) {
-      bulk_bar_init(&bar[0]);
-      bulk_bar_init(&bar[1]);
-      bulk_bar_init_fence();
-      issued = 0;
-      if (numTiles > 0) issue(0);
-      if (numTiles > 1) issue(1);
-    }
-    __syncthreads();
-  }
-  // all threads, before reading tile k: false if its copy never completed
-  __device__ __forceinline__ bool wait(uint32_t k) const
-  {
-    if (!BULK || copied(k) == 0) return true;
-    return bulk_wait(&bar[k & 1], (k >> 1) & 1u, MB_WAIT_POLLS);
-  }
-  __device__ __forceinline__ void load(uint32_t k, uint32_t local, float &lx, float &ly, float &lz, float &hx,
-                                       float &hy, float &hz) const
-  {
-    if (BULK && local < copied(k)) {
-      const float2 *p = reinterpret_cast<const float2 *>(buf + (size_t)(k & 1) * MB_TILE + local);
-      const float2 a = p[0], b = p[1], c = p[2];
-      lx = a.x; ly = a.y; lz = b.x; hx = b.y; hy = c.x; hz = c.y;
-    } else {
-      load_box(boxes, begin + (uint64_t)k * MB_TILE + local, lx, ly, lz, hx, hy, hz);
-    }
-  }
-  // all threads, after tile k was read by every thread (a barrier in between):
-  // thread 0 refills its buffer with tile k + 2
-  __device__ __forceinline__ void release(uint32_t k)
-  {
-    if (BULK && threadIdx.x == 0 && k + 2 < numTiles) {
-      bulk_proxy_fence();
-      issue(k + 2);
-    }
-  }
-  // thread 0, after a timed-out wait: wait (bounded) for the copies still in flight
-  __device__ __forceinline__ void drain(uint32_t from)
-  {
-    if (!BULK || threadIdx.x != 0) return;
-    for (uint32_t k = from; k < issued; k++)
-      if (copied(k)) bulk_wait(&bar[k & 1], (k >> 1) & 1u, MB_WAIT_POLLS);
-  }
-};
-
-// ------------------------------------------------------------------
 // pass 1: bounds
 // ------------------------------------------------------------------
-template <bool BULK>
 __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
                                                      Partial *__restrict__ partials, uint32_t *__restrict__ blockOff,
                                                      BuildState *st, uint32_t *__restrict__ hist, int histWords)
@@ -194,28 +107,17 @@ __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict_
   __shared__ int32_t sLo[3][MB_BLOCK / 32], sHi[3][MB_BLOCK / 32];
   __shared__ uint32_t sCnt[MB_BLOCK / 32];
   __shared__ uint32_t sLast;
-  __shared__ uint64_t sBar[2];
-  extern __shared__ __align__(16) unsigned char sTiles[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = min((uint64_t)n, begin + chunk);
   int32_t lo0 = INT_MAX, lo1 = INT_MAX, lo2 = INT_MAX, hi0 = INT_MIN, hi1 = INT_MIN, hi2 = INT_MIN;
   uint32_t cnt = 0;
-  BoxTiles<BULK> bt{boxes, begin, end, end > begin ? (uint32_t)((end - begin + MB_TILE - 1) / MB_TILE) : 0u,
-                    reinterpret_cast<bq_box3f *>(sTiles), sBar, 0};
-  bt.start();
-  for (uint32_t k = 0; k < bt.numTiles; k++) {
-    if (BULK && !__syncthreads_and(bt.wait(k))) {  // a copy never completed
-      if (threadIdx.x == 0) atomicOr(&st->err, DEV_ERR_TIMEOUT);
-      bt.drain(k);
-      break;
-    }
-    const uint32_t tc = bt.count(k);
+  for (uint64_t i0 = begin + threadIdx.x; i0 < end; i0 += (uint64_t)MB_BLOCK * MB_UNROLL) {
     float b[MB_UNROLL][6];
 #pragma unroll
     for (int u = 0; u < MB_UNROLL; u++) {
-      const uint32_t local = (uint32_t)u * MB_BLOCK + threadIdx.x;
-      if (local < tc) bt.load(k, local, b[u][0], b[u][1], b[u][2], b[u][3], b[u][4], b[u][5]);
+      uint64_t i = i0 + (uint64_t)u * MB_BLOCK;
+      if (i < end) load_box(boxes, i, b[u][0], b[u][1], b[u][2], b[u][3], b[u][4], b[u][5]);
       else b[u][0] = 1.f, b[u][3] = 0.f;  // empty
     }
 #pragma unroll
@@ -226,10 +128,6 @@ __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict_
         hi0 = max(hi0, cx); hi1 = max(hi1, cy); hi2 = max(hi2, cz);
         cnt++;
       }
-    }
-    if (BULK) {
-      __syncthreads();  // every thread is done with this tile's buffer
-      bt.release(k);
     }
   }
   lo0 = __reduce_min_sync(0xffffffffu, lo0); lo1 = __reduce_min_sync(0xffffffffu, lo1);
@@ -323,45 +221,33 @@ __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict_
 // ------------------------------------------------------------------
 // pass 2: keys, compaction, digit histograms
 // ------------------------------------------------------------------
-template <int SB, bool BULK>
+template <int SB>
 __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
-                                                     const uint32_t *__restrict__ blockOff, BuildState *st,
+                                                     const uint32_t *__restrict__ blockOff, const BuildState *st,
                                                      uint64_t *__restrict__ keys, uint32_t *__restrict__ ids,
                                                      uint32_t *__restrict__ hist)
 {
   constexpr int PASSES = hist_passes<SB>();
   __shared__ uint32_t sHist[PASSES * 256];
   __shared__ uint32_t sWarpCnt[MB_UNROLL][MB_BLOCK / 32];
-  __shared__ uint64_t sBar[2];
-  extern __shared__ __align__(16) unsigned char sTiles[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < PASSES * 256; i += MB_BLOCK) sHist[i] = 0;
   const float bx = st->bias[0], by = st->bias[1], bz = st->bias[2], sc = st->scale;
   uint32_t running = blockOff[blockIdx.x];
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = min((uint64_t)n, begin + chunk);
-  BoxTiles<BULK> bt{boxes, begin, end, end > begin ? (uint32_t)((end - begin + MB_TILE - 1) / MB_TILE) : 0u,
-                    reinterpret_cast<bq_box3f *>(sTiles), sBar, 0};
-  bt.start();
   __syncthreads();
   const uint32_t lt = (1u << lane) - 1u;
-  for (uint32_t k = 0; k < bt.numTiles; k++) {
-    if (BULK && !__syncthreads_and(bt.wait(k))) {  // a copy never completed
-      if (threadIdx.x == 0) atomicOr(&st->err, DEV_ERR_TIMEOUT);
-      bt.drain(k);
-      break;
-    }
-    const uint64_t i0 = begin + (uint64_t)k * MB_TILE;
-    const uint32_t tc = bt.count(k);
+  for (uint64_t i0 = begin; i0 < end; i0 += (uint64_t)MB_BLOCK * MB_UNROLL) {
     float b[MB_UNROLL][6];
     bool valid[MB_UNROLL];
     uint32_t wpre[MB_UNROLL];
 #pragma unroll
     for (int u = 0; u < MB_UNROLL; u++) {
-      const uint32_t local = (uint32_t)u * MB_BLOCK + threadIdx.x;
+      uint64_t i = i0 + (uint64_t)u * MB_BLOCK + threadIdx.x;
       valid[u] = false;
-      if (local < tc) {
-        bt.load(k, local, b[u][0], b[u][1], b[u][2], b[u][3], b[u][4], b[u][5]);
+      if (i < end) {
+        load_box(boxes, i, b[u][0], b[u][1], b[u][2], b[u][3], b[u][4], b[u][5]);
         valid[u] = !(b[u][0] > b[u][3]);
       }
       uint32_t bal = __ballot_sync(0xffffffffu, valid[u]);
@@ -384,8 +270,7 @@ __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict_
       acc += tot;
     }
     running = acc;
-    __syncthreads();  // (with BULK: every thread is also done with this tile's buffer)
-    bt.release(k);
+    __syncthreads();
 #pragma unroll
     for (int u = 0; u < MB_UNROLL; u++) {
       if (!valid[u]) continue;
@@ -887,20 +772,6 @@ int long_runs(const RunStats &h, const uint4 *runs, uint64_t *keys, uint32_t *id
 }
 } // namespace
 
-namespace {
-// the bulk-copy kernels take their two tile buffers (48 KB) as dynamic
-// shared memory on top of their static arrays
-cudaError_t set_bulk_smem()
-{
-  cudaError_t e = cudaFuncSetAttribute(k_bounds<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MB_BULK_SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_keygen<MB_SB3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MB_BULK_SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_keygen<MB_SB4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MB_BULK_SMEM);
-  return e;
-}
-} // namespace
-
 // ------------------------------------------------------------------
 // host entry
 // ------------------------------------------------------------------
@@ -960,28 +831,14 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   cudaError_t ce = cudaMemsetAsync(st, 0, sizeof(BuildState), al.s);
   if (ce != cudaSuccess) return fail(cuda_error(ce, "memset"));
 
-  // the box chunks stream through shared memory by bulk copies when the
-  // array is 16-byte aligned (a tile of 1024 boxes is then too)
-  const bool bulk = (reinterpret_cast<uintptr_t>(boxes) & 15u) == 0;
-  if (bulk && (ce = set_bulk_smem()) != cudaSuccess) return fail(cuda_error(ce, "cudaFuncSetAttribute"));
   {
     ProfScope ps("morton.bounds", al.s);
-    if (bulk)
-      k_bounds<true><<<grid, MB_BLOCK, MB_BULK_SMEM, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, histWords);
-    else
-      k_bounds<false><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, histWords);
+    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, histWords);
   }
   {
     ProfScope ps("morton.keygen", al.s);
-    const size_t sm = bulk ? MB_BULK_SMEM : 0;
-    if (wide4 && bulk)
-      k_keygen<MB_SB4, true><<<grid, MB_BLOCK, sm, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
-    else if (wide4)
-      k_keygen<MB_SB4, false><<<grid, MB_BLOCK, sm, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
-    else if (bulk)
-      k_keygen<MB_SB3, true><<<grid, MB_BLOCK, sm, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
-    else
-      k_keygen<MB_SB3, false><<<grid, MB_BLOCK, sm, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
+    if (wide4) k_keygen<MB_SB4><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
+    else k_keygen<MB_SB3><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
   }
   if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_bounds/k_keygen"));
 
