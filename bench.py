@@ -231,6 +231,13 @@ def reference_components(W, n):
         del tq
         g = W.gmm_points(n)
         gq = W.gmm_points(n, sample_seed=W.SEED_GMM_QUERIES)
+        pb, ob, qb, qob = W.cloud_batch()
+        comp["batched_knn_512_clouds"] = {"clouds": len(ob) - 1, "points": int(len(pb)), "queries": int(len(qb)),
+                                          "k": 16,
+                                          "reference_per_cloud_loop_ms": r.time_batched_knn(pb, ob, qb, qob, 16),
+                                          "note": "for every cloud: the reference's radixBuilder, its findKNN "
+                                                  "kernel over the cloud's queries, cuda::free"}
+        del pb, qb
         comp["gmm10m"] = {"points": n, "queries": n,
                           "reference_radixBuilder_ms": r.time_build(RefGPU.RADIX, g, 0, reps=2),
                           "reference_gpuBuilder_leaf8_ms": r.time_build(RefGPU.SPATIAL_MEDIAN, g, 8, reps=2),

@@ -54,6 +54,21 @@ struct Alloc {
   int get(T **p, size_t count) { return malloc_bytes((void **)p, sizeof(T) * (count ? count : 1)); }
 };
 
+// Carves one allocation into 256-byte aligned pieces (first pass: sizing
+// with base == nullptr; second pass: the pointers)
+struct Carver {
+  char *base;
+  size_t off = 0;
+  explicit Carver(void *b) : base((char *)b) {}
+  template <typename T>
+  void take(T **p, size_t count)
+  {
+    off = (off + 255) & ~(size_t)255;
+    *p = base ? (T *)(base + off) : nullptr;
+    off += sizeof(T) * (count ? count : 1);
+  }
+};
+
 // RAII list of temporaries freed (stream-ordered) at scope exit
 struct TempSet {
   Alloc &al;
@@ -328,8 +343,13 @@ __device__ __forceinline__ uint32_t block_scan_smem(uint32_t *s, uint32_t L, uin
 // The element count is nDev[0] when nDev is given (nMax bounds it),
 // else nMax.  dHist (optional) holds the per-pass 256-bin digit
 // histograms, already counted by the producer of the keys.
+// ctlWs (optional): onesweep_ctl_words(nMax, beginBit, endBit) words of
+// device memory the sort uses for its look-back state instead of
+// allocating them.
 int onesweep_sort_u64(uint64_t *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit,
-                      int endBit, const uint32_t *dHist, int *outSel, uint32_t *dErr, Alloc &al);
+                      int endBit, const uint32_t *dHist, int *outSel, uint32_t *dErr, Alloc &al,
+                      uint32_t *ctlWs = nullptr);
+size_t onesweep_ctl_words(uint32_t nMax, int beginBit, int endBit);
 int onesweep_sort_u32(uint32_t *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit,
                       int endBit, const uint32_t *dHist, int *outSel, uint32_t *dErr, Alloc &al);
 

@@ -223,7 +223,8 @@ __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict_
 // ------------------------------------------------------------------
 template <int SB>
 __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
-                                                     const uint32_t *__restrict__ blockOff, const BuildState *st,
+                                                     const uint32_t *__restrict__ blockOff,
+                                                     const Partial *__restrict__ partials, const BuildState *st,
                                                      uint64_t *__restrict__ keys, uint32_t *__restrict__ ids,
                                                      uint32_t *__restrict__ hist)
 {
@@ -236,7 +237,31 @@ __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict_
   uint32_t running = blockOff[blockIdx.x];
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = min((uint64_t)n, begin + chunk);
+  // every box of the chunk valid (the common case): prim i goes to position
+  // running + (i - begin), with no compaction ballots or barriers
+  const bool allValid = __ldg(&partials[blockIdx.x].cnt) == (uint32_t)(end - begin);
   __syncthreads();
+  if (allValid) {
+#pragma unroll 4
+    for (uint64_t i = begin + threadIdx.x; i < end; i += MB_BLOCK) {
+      float lx, ly, lz, hx, hy, hz;
+      load_box(boxes, i, lx, ly, lz, hx, hy, hz);
+      const float cx = ctr(lx, hx), cy = ctr(ly, hy), cz = ctr(lz, hz);
+      const uint64_t key = spread21(quant_cell(cx, bx, sc, 2097151u)) |
+                           (spread21(quant_cell(cy, by, sc, 2097151u)) << 1) |
+                           (spread21(quant_cell(cz, bz, sc, 2097151u)) << 2);
+      const uint32_t pos = running + (uint32_t)(i - begin);
+      keys[pos] = key;
+      ids[pos] = (uint32_t)i;
+#pragma unroll
+      for (int p = 0; p < PASSES; p++)
+        atomicAdd(&sHist[p * 256 + ((key >> (SB + 8 * p)) & 0xff)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < PASSES * 256; i += MB_BLOCK)
+      if (sHist[i]) atomicAdd(&hist[i], sHist[i]);
+    return;
+  }
   const uint32_t lt = (1u << lane) - 1u;
   for (uint64_t i0 = begin; i0 < end; i0 += (uint64_t)MB_BLOCK * MB_UNROLL) {
     float b[MB_UNROLL][6];
@@ -797,25 +822,39 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
     BuildState st;
     RunStats runs;
   };
-  Ctl *ctl = nullptr;
-  BuildState *st = nullptr;
-  Partial *partials = nullptr;
-  uint32_t *blockOff = nullptr, *hist = nullptr, *slot = nullptr;
-  uint64_t *keysA = nullptr, *keysB = nullptr;
-  uint8_t *delta = nullptr;
-  BQ_TRY(tmp.get(&ctl, 1));
-  st = &ctl->st;
-  BQ_TRY(tmp.get(&partials, grid));
-  BQ_TRY(tmp.get(&blockOff, grid));
-  // more than 2^24 prims: sort 32 top bits in 4 passes instead of 24 in 3
-  const bool wide4 = n > (1u << 24);
+  // all temporaries of the build in one allocation (one call to the
+  // allocator instead of a dozen before the first kernel can start)
+  const bool wide4 = n > (1u << 24);  // more than 2^24 prims: sort 32 top bits in 4 passes instead of 24 in 3
   const int sb = wide4 ? MB_SB4 : MB_SB3;
   const int histWords = (wide4 ? hist_passes<MB_SB4>() : hist_passes<MB_SB3>()) * 256;
-  BQ_TRY(tmp.get(&hist, MB_MAX_HIST_PASSES * 256));
-  BQ_TRY(tmp.get(&keysA, n));
-  BQ_TRY(tmp.get(&keysB, n));
-  BQ_TRY(tmp.get(&delta, n));
-  BQ_TRY(tmp.get(&slot, n));
+  const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
+  Ctl *ctl = nullptr;
+  Partial *partials = nullptr;
+  uint32_t *blockOff = nullptr, *hist = nullptr, *slot = nullptr, *sortCtl = nullptr;
+  uint64_t *keysA = nullptr, *keysB = nullptr;
+  uint8_t *delta = nullptr;
+  uint4 *runs = nullptr;
+  uint2 *pending = nullptr;
+  auto carve = [&](Carver &c) {
+    c.take(&ctl, 1);
+    c.take(&partials, grid);
+    c.take(&blockOff, grid);
+    c.take(&hist, MB_MAX_HIST_PASSES * 256);
+    c.take(&keysA, n);
+    c.take(&keysB, n);
+    c.take(&delta, n);
+    c.take(&slot, n);
+    c.take(&runs, maxRuns);
+    c.take(&pending, 2ull * div_up(n, AGG_CHUNK));
+    c.take(&sortCtl, onesweep_ctl_words(n, sb, 63));
+  };
+  Carver sizing(nullptr);
+  carve(sizing);
+  char *arena = nullptr;
+  BQ_TRY(tmp.get(&arena, sizing.off));
+  Carver cut(arena);
+  carve(cut);
+  BuildState *st = &ctl->st;
   uint32_t *idsA = nullptr, *idsB = nullptr;
   Node *nodes = nullptr;
   BQ_TRY(al.get(&idsA, n));
@@ -837,28 +876,25 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   }
   {
     ProfScope ps("morton.keygen", al.s);
-    if (wide4) k_keygen<MB_SB4><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
-    else k_keygen<MB_SB3><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, st, keysA, idsA, hist);
+    if (wide4)
+      k_keygen<MB_SB4><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, partials, st, keysA, idsA, hist);
+    else
+      k_keygen<MB_SB3><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, partials, st, keysA, idsA, hist);
   }
   if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_bounds/k_keygen"));
 
   uint64_t *keys2[2] = {keysA, keysB};
   uint32_t *ids2[2] = {idsA, idsB};
   int sel = 0;
-  if ((s = onesweep_sort_u64(keys2, ids2, n, &st->numValid, sb, 63, hist, &sel, &st->err, al)) != BQ_OK)
+  if ((s = onesweep_sort_u64(keys2, ids2, n, &st->numValid, sb, 63, hist, &sel, &st->err, al, sortCtl)) != BQ_OK)
     return fail(s);
   uint64_t *keys = keys2[sel];
   uint32_t *ids = ids2[sel];
   uint32_t *idsOther = ids2[sel ^ 1];
-  const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
   RunStats *rs = &ctl->runs;
-  uint4 *runs = nullptr;
-  if ((s = tmp.get(&runs, maxRuns)) != BQ_OK) return fail(s);
   s = wide4 ? fix_runs<MB_SB4>(keys, ids, n, &st->numValid, delta, slot, rs, runs, maxRuns, al)
             : fix_runs<MB_SB3>(keys, ids, n, &st->numValid, delta, slot, rs, runs, maxRuns, al);
   if (s != BQ_OK) return fail(s);
-  uint2 *pending = nullptr;
-  if ((s = tmp.get(&pending, 2ull * div_up(n, AGG_CHUNK))) != BQ_OK) return fail(s);
   AggArgs ag{delta, slot, ids, boxes, nodes, nullptr, &st->numValid, nullptr, pending, nullptr, 0};
   // what the host reads back (one copy): the long-run statistics, the valid
   // count, the error word

@@ -31,6 +31,7 @@ namespace bq {
 namespace {
 
 constexpr int SORT_BLOCK = 256;
+constexpr int SORT_ITEMS = 16;  // keys a thread ranks per tile
 constexpr int SORT_WARPS = SORT_BLOCK / 32;
 constexpr uint32_t ST_AGG = 1u << 30;
 constexpr uint32_t ST_INC = 2u << 30;
@@ -362,19 +363,19 @@ constexpr uint32_t INJECTED_SPIN_LIMIT = 4096;
 
 template <typename KeyT>
 int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit, int endBit,
-                  const uint32_t *preHist, int *outSel, uint32_t *dErr, Alloc &al)
+                  const uint32_t *preHist, int *outSel, uint32_t *dErr, Alloc &al, uint32_t *ctlWs)
 {
-  constexpr int ITEMS = 16;
+  constexpr int ITEMS = SORT_ITEMS;
   constexpr int TILE = SORT_BLOCK * ITEMS;
   *outSel = 0;
   if ((nMax <= 1 && !nDev) || nMax == 0 || endBit <= beginBit) return BQ_OK;
   const int numPasses = (endBit - beginBit + 7) / 8;
   const int numTiles = div_up(nMax, TILE);
   TempSet tmp(al);
-  uint32_t *hist = nullptr, *ctl = nullptr;
+  uint32_t *hist = nullptr, *ctl = ctlWs;
   // ctl layout: [status: numPasses*numTiles*256][tileCtr: numPasses][abort: 1]
   const size_t statusWords = (size_t)numPasses * numTiles * 256;
-  BQ_TRY(tmp.get(&ctl, statusWords + numPasses + 1));
+  if (!ctl) BQ_TRY(tmp.get(&ctl, statusWords + numPasses + 1));
   BQ_CUDA(cudaMemsetAsync(ctl, 0, sizeof(uint32_t) * (statusWords + numPasses + 1), al.s));
   if (preHist) {
     hist = const_cast<uint32_t *>(preHist);
@@ -445,15 +446,22 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
 } // namespace
 
 int onesweep_sort_u64(uint64_t *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit,
-                      int endBit, const uint32_t *dHist, int *outSel, uint32_t *dErr, Alloc &al)
+                      int endBit, const uint32_t *dHist, int *outSel, uint32_t *dErr, Alloc &al, uint32_t *ctlWs)
 {
-  return onesweep_impl<uint64_t>(keys, vals, nMax, nDev, beginBit, endBit, dHist, outSel, dErr, al);
+  return onesweep_impl<uint64_t>(keys, vals, nMax, nDev, beginBit, endBit, dHist, outSel, dErr, al, ctlWs);
 }
 
 int onesweep_sort_u32(uint32_t *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit,
                       int endBit, const uint32_t *dHist, int *outSel, uint32_t *dErr, Alloc &al)
 {
-  return onesweep_impl<uint32_t>(keys, vals, nMax, nDev, beginBit, endBit, dHist, outSel, dErr, al);
+  return onesweep_impl<uint32_t>(keys, vals, nMax, nDev, beginBit, endBit, dHist, outSel, dErr, al, nullptr);
+}
+
+size_t onesweep_ctl_words(uint32_t nMax, int beginBit, int endBit)
+{
+  constexpr int TILE = SORT_BLOCK * SORT_ITEMS;
+  const int numPasses = endBit > beginBit ? (endBit - beginBit + 7) / 8 : 0;
+  return (size_t)numPasses * div_up(nMax, TILE) * 256 + numPasses + 1;
 }
 
 } // namespace bq

@@ -640,6 +640,18 @@ class RefGPU:
         assert rc == 0
         return ms.value
 
+    def time_batched_knn(self, points, offsets, queries, query_offsets, k):
+        """ms of the reference serving a batch cloud by cloud: radixBuilder,
+        its findKNN kernel over the cloud's queries, cuda::free."""
+        points, queries = _f32(points), _f32(queries)
+        off = np.ascontiguousarray(offsets, dtype=np.uint32)
+        qoff = np.ascontiguousarray(query_offsets, dtype=np.uint32)
+        ms = ctypes.c_float()
+        rc = self.lib.ref_gpu_time_batched_knn(_p(points), _p(off), _p(queries), _p(qoff),
+                                               ctypes.c_uint32(len(off) - 1), ctypes.c_int(k), ctypes.byref(ms))
+        assert rc == 0
+        return ms.value
+
     def time_box_query(self, method, points, query_boxes, makeLeafThreshold=0, reps=5):
         """(ms of count + fill kernels, total results) for the reference box
         query over a tree built on the point boxes."""

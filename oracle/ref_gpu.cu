@@ -679,6 +679,48 @@ int ref_gpu_time_tri(int method, const int32_t *tris, uint32_t nt, const float *
   return 0;
 }
 
+// Times the reference's way of serving a batch of clouds: for every cloud,
+// radixBuilder over its point boxes, then its per-thread findKNN kernel
+// (<<<ceil(Q/128),128>>>) over its queries, then cuda::free; one CUDA event
+// pair around the whole loop (the builder's own host syncs included).
+// Points and queries are stored back to back; off / qoff hold numSegs+1
+// offsets each.
+int ref_gpu_time_batched_knn(const float *points, const uint32_t *off, const float *queries, const uint32_t *qoff,
+                             uint32_t numSegs, int k, float *ms_out)
+{
+  const uint32_t n = off[numSegs], nq = qoff[numSegs];
+  vec3f *dp = dalloc_copy((const vec3f *)points, n), *dq = dalloc_copy((const vec3f *)queries, nq);
+  box3f *db = dalloc_copy<box3f>(nullptr, n);
+  int *di = dalloc_copy<int>(nullptr, (size_t)nq * k), *dn = dalloc_copy<int>(nullptr, nq);
+  float *dd = dalloc_copy<float>(nullptr, (size_t)nq * k);
+  if (!dp || !dq || !db || !di || !dn || !dd || k > 16) return -1;
+  k_points_to_boxes<<<(n + 127) / 128, 128>>>(dp, db, (int)n);
+  RCHECK(cudaDeviceSynchronize());
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float total = 0.f;
+  for (int r = -1; r < 1; r++) {  // one warm-up loop, one timed loop
+    cudaEventRecord(e0);
+    for (uint32_t c = 0; c < numSegs; c++) {
+      const uint32_t cn = off[c + 1] - off[c], cq = qoff[c + 1] - qoff[c];
+      bvh3f bvh;
+      cuBQL::cuda::radixBuilder(bvh, db + off[c], cn, BuildConfig());
+      k_knn<16><<<(cq + 127) / 128, 128>>>(bvh, dp + off[c], dq + qoff[c], (int)cq, k, INFINITY,
+                                         di + (size_t)qoff[c] * k, dd + (size_t)qoff[c] * k, dn + qoff[c]);
+      cuBQL::cuda::free(bvh);
+    }
+    cudaEventRecord(e1);
+    RCHECK(cudaEventSynchronize(e1));
+    cudaEventElapsedTime(&total, e0, e1);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(dp); cudaFree(dq); cudaFree(db); cudaFree(di); cudaFree(dn); cudaFree(dd);
+  *ms_out = total;
+  return 0;
+}
+
 // Times the reference box query (count kernel + fill kernel, offsets from
 // an untimed count pass) over a tree of `method` built on point boxes.
 int ref_gpu_time_box_query(int method, const float *points, uint32_t n, int makeLeafThreshold,
