@@ -104,7 +104,7 @@ __device__ __forceinline__ AggBox agg_union(const AggBox &left, const AggBox &ri
 template <typename LevT>
 struct AggArgsT {
   const LevT *delta;      // split level of pair (i, i+1)
-  uint32_t *slot;         // global slots, AGG_EMPTY on entry
+  uint32_t *slot;         // global slots (one per split position), set by the local phase
   const uint32_t *ids;    // sorted prim ids (global indices)
   const bq_box3f *boxes;
   Node *nodes;            // output (full tree layout)
@@ -188,11 +188,13 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
     }
   }
   __syncthreads();
-  // children parked at splits whose sibling never came: publish for the global phase
-  for (int j = threadIdx.x + 1; j < AGG_CHUNK; j += blockDim.x) {
-    const uint32_t v = sSlot[j];
-    if (v != AGG_EMPTY) a.slot[c0 + j] = v;
-  }
+  // The global slots of this chunk's splits, for the global phase (a later
+  // launch): a child parked at a split whose sibling never came publishes
+  // its range end there; every other slot, the chunk's first split (on its
+  // boundary) included, starts empty.  (A slot whose two children met here
+  // keeps the second one's end: no global climb ever reaches that split.)
+  for (int j = threadIdx.x; j < AGG_CHUNK; j += blockDim.x)
+    if (c0 + j < nv) a.slot[c0 + j] = j == 0 ? AGG_EMPTY : sSlot[j];
 }
 
 template <bool SEG, typename LevT>

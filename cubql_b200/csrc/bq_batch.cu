@@ -43,8 +43,6 @@ int query_config(const bq_query_config *q, bq_query_config &out);
 
 namespace {
 
-constexpr uint32_t SLOT_EMPTY = 0xffffffffu;
-
 __device__ __forceinline__ uint32_t seg_of(const uint32_t *__restrict__ off, uint32_t numSegs, uint32_t i)
 {
   // largest s with off[s] <= i
@@ -196,11 +194,10 @@ __device__ __forceinline__ uint8_t seg_split_level(const uint64_t *__restrict__ 
 }
 
 __global__ void k_seg_delta(const uint64_t *__restrict__ keys, uint32_t n, const uint32_t *__restrict__ off,
-                            uint32_t numSegs, uint8_t *__restrict__ delta, uint32_t *__restrict__ slot)
+                            uint32_t numSegs, uint8_t *__restrict__ delta)
 {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  slot[i] = SLOT_EMPTY;
   const uint32_t s = seg_of(off, numSegs, i);
   const uint32_t b0 = __ldg(off + s), e0 = __ldg(off + s + 1);
   if (i + 1 < e0) delta[i] = seg_split_level(keys, b0, e0, i);
@@ -546,7 +543,7 @@ int batched_build_morton63(const bq_box3f *boxes, const uint32_t *off, uint32_t 
   }
   {
     ProfScope ps("batch.delta", al.s);
-    k_seg_delta<<<div_up(n, 256), 256, 0, al.s>>>(fkeys, n, off, numSegs, delta, slot);
+    k_seg_delta<<<div_up(n, 256), 256, 0, al.s>>>(fkeys, n, off, numSegs, delta);
   }
   uint2 *pending = nullptr;
   BQ_TRY(tmp.get(&pending, 2ull * div_up(n, AGG_CHUNK)));

@@ -22,7 +22,7 @@
 //                 prims ((run, low bits) keys) -- a run of identical keys
 //                 is already in order.  The result is the full stable
 //                 63-bit order, as cub's SortPairs gives.  The same kernel
-//                 writes the slots and the split levels: one byte per
+//                 writes the split levels: one byte per
 //                 adjacent key pair, the level at which the reference's
 //                 top-down split would separate them (k_run_levels writes
 //                 those inside the longer runs)
@@ -66,7 +66,6 @@ namespace {
 
 constexpr int MB_BLOCK = 256;
 constexpr int MB_UNROLL = 4;
-constexpr uint32_t SLOT_EMPTY = 0xffffffffu;
 // The global sort covers key bits [SB, 63): SB = 39 (24 bits, 3 passes) up
 // to 2^24 prims, SB = 31 (32 bits, 4 passes) above, so that runs of equal
 // sorted bits stay short (on uniform data about n / 2^(63-SB) prims each);
@@ -358,11 +357,11 @@ __device__ __forceinline__ uint8_t equal_run_level(uint64_t r0, uint64_t r1, uin
   return (uint8_t)(63 - depth);
 }
 
-// Every sorted position: its agglomeration slot, the split level of the
-// pair (i, i+1), and the low-bit order inside runs of equal top bits.
+// Every sorted position: the split level of the pair (i, i+1), and the
+// low-bit order inside runs of equal top bits.
 // One block covers FT_TILE consecutive positions, staged in shared memory
 // with FT_HALO positions after them:
-//   A. per position: the slot, the split level of a pair that lies across
+//   A. per position: the split level of a pair that lies across
 //      two runs (their highest differing bit is a top bit, so it does not
 //      depend on the order inside the runs) and, at the first position of a
 //      run, the run's size class -- 2, 3..4 or more prims -- appended to
@@ -457,7 +456,7 @@ __device__ __forceinline__ void list_long_run(uint32_t i, uint32_t hi, uint32_t 
 // pays more than the few spilled bytes cost
 template <int SB>
 __global__ void __launch_bounds__(FT_BLOCK, 8) k_fix_runs(uint64_t *keys, uint32_t *ids, const uint32_t *nvPtr,
-                                                       uint8_t *__restrict__ delta, uint32_t *__restrict__ slot,
+                                                       uint8_t *__restrict__ delta,
                                                        RunStats *rs, uint4 *runs, uint32_t maxRuns)
 {
   __shared__ uint64_t sK[FT_TILE + FT_HALO + 1];  // [0]: position base-1, [1+j]: base+j
@@ -475,15 +474,6 @@ __global__ void __launch_bounds__(FT_BLOCK, 8) k_fix_runs(uint64_t *keys, uint32
   for (uint32_t j = t; j < lenH; j += FT_BLOCK) sK[j + 1] = keys[base + j];
   if (t == 0) sK[0] = base > 0 ? keys[base - 1] : 0ull;
   if (t < 3) sCnt[t] = 0u;
-  uint32_t *sl = slot + base;
-  if ((reinterpret_cast<uintptr_t>(sl) & 15u) == 0) {
-    const uint32_t n4 = len >> 2;
-    for (uint32_t j = t; j < n4; j += FT_BLOCK)
-      reinterpret_cast<uint4 *>(sl)[j] = make_uint4(SLOT_EMPTY, SLOT_EMPTY, SLOT_EMPTY, SLOT_EMPTY);
-    for (uint32_t j = (n4 << 2) + t; j < len; j += FT_BLOCK) sl[j] = SLOT_EMPTY;
-  } else {
-    for (uint32_t j = t; j < len; j += FT_BLOCK) sl[j] = SLOT_EMPTY;
-  }
   __syncthreads();
 
   // A. levels across runs; runs begun here, by size class
@@ -649,7 +639,7 @@ __global__ void k_run_scatter(const uint4 *__restrict__ runs, const uint32_t *__
 }
 
 // Split levels of the pairs inside the long runs (the pairs at their ends,
-// which lie across runs, and every slot were written by k_fix_runs).  A run
+// which lie across runs, were written by k_fix_runs).  A run
 // of identical keys is split at (b+e)/2 recursively (radix.h:455-465); in a
 // mixed run, equal neighbours are looked up inside the run.
 __global__ void k_run_levels(const uint4 *__restrict__ runs, const uint32_t *__restrict__ off, uint32_t R,
@@ -733,15 +723,15 @@ __global__ void k_collapse(const Node *__restrict__ full, const uint2 *__restric
 // ------------------------------------------------------------------
 namespace {
 // Orders the runs of equal top bits of at most MB_THREAD_RUN prims and writes
-// every split level and slot (k_fix_runs); longer runs are listed in `runs`
+// every split level (k_fix_runs); longer runs are listed in `runs`
 // and counted in *rs for long_runs.  Nothing waits here.
 template <int SB>
-int fix_runs(uint64_t *keys, uint32_t *ids, uint32_t n, const uint32_t *nvDev, uint8_t *delta, uint32_t *slot,
-             RunStats *rs, uint4 *runs, uint32_t maxRuns, Alloc &al)
+int fix_runs(uint64_t *keys, uint32_t *ids, uint32_t n, const uint32_t *nvDev, uint8_t *delta, RunStats *rs,
+             uint4 *runs, uint32_t maxRuns, Alloc &al)
 {
   BQ_CUDA(cudaMemsetAsync(rs, 0, sizeof(RunStats), al.s));
   ProfScope ps("morton.runs", al.s);
-  k_fix_runs<SB><<<div_up(n, FT_TILE), FT_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, slot, rs, runs, maxRuns);
+  k_fix_runs<SB><<<div_up(n, FT_TILE), FT_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, rs, runs, maxRuns);
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }
@@ -892,8 +882,8 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   uint32_t *ids = ids2[sel];
   uint32_t *idsOther = ids2[sel ^ 1];
   RunStats *rs = &ctl->runs;
-  s = wide4 ? fix_runs<MB_SB4>(keys, ids, n, &st->numValid, delta, slot, rs, runs, maxRuns, al)
-            : fix_runs<MB_SB3>(keys, ids, n, &st->numValid, delta, slot, rs, runs, maxRuns, al);
+  s = wide4 ? fix_runs<MB_SB4>(keys, ids, n, &st->numValid, delta, rs, runs, maxRuns, al)
+            : fix_runs<MB_SB3>(keys, ids, n, &st->numValid, delta, rs, runs, maxRuns, al);
   if (s != BQ_OK) return fail(s);
   AggArgs ag{delta, slot, ids, boxes, nodes, nullptr, &st->numValid, nullptr, pending, nullptr, 0};
   // what the host reads back (one copy): the long-run statistics, the valid

@@ -113,13 +113,11 @@ __global__ void k_rb_keys(const bq_box3f *__restrict__ boxes, uint32_t n, const 
   ids[p] = i;
 }
 
-__global__ void k_rb_levels0(const uint32_t *__restrict__ keys, const uint32_t *nvPtr, uint16_t *__restrict__ lev,
-                             uint32_t *__restrict__ slot)
+__global__ void k_rb_levels0(const uint32_t *__restrict__ keys, const uint32_t *nvPtr, uint16_t *__restrict__ lev)
 {
   const uint32_t nv = *nvPtr;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
-  slot[i] = AGG_EMPTY;
   if (i + 1 < nv) {
     const uint32_t x = keys[i] ^ keys[i + 1];
     lev[i] = x ? broad_level(0, 31 - __clz(x)) : (uint16_t)0;
@@ -558,7 +556,7 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   }
   {
     ProfScope ps("rebin.levels", al.s);
-    k_rb_levels0<<<div_up(n, 256), 256, 0, al.s>>>(keys, nvDev, lev, slot);
+    k_rb_levels0<<<div_up(n, 256), 256, 0, al.s>>>(keys, nvDev, lev);
   }
   // ---- broad-phase rebinning ----
   uint32_t *flag = nullptr, *runIdx = nullptr, *starts = nullptr, *big = nullptr, *bigSize = nullptr;
@@ -669,8 +667,6 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     }
     al.free_bytes(nodes);  // rare: multi-prim leaves, go through the collapse below
     nodes = nullptr;
-    if ((ce = cudaMemsetAsync(slot, 0xff, sizeof(uint32_t) * hnv, al.s)) != cudaSuccess)
-      return fail(cuda_error(ce, "memset"));
   }
   // ---- full tree, then collapse ----
   Node *full = nullptr;
