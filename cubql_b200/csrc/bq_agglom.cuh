@@ -132,8 +132,11 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
   const uint32_t i = c0 + threadIdx.x;
   uint32_t id = 0;
   float2 p0 = make_float2(0.f, 0.f), p1 = p0, p2 = p0;
+  // the ids are read once and the nodes written once: evict_first in L2, so
+  // that the boxes (gathered at random, 2-3 to a 64-byte line) stay longer
+  const uint64_t once = l2_policy_evict_first();
   if (i < nv) {
-    id = __ldg(a.ids + i);
+    id = ldg_u32_policy(a.ids + i, once);
     const float2 *bp = reinterpret_cast<const float2 *>(a.boxes + id);
     p0 = __ldg(bp);
     p1 = __ldg(bp + 1);
@@ -157,7 +160,7 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
     uint64_t admin = make_admin(i - b0, 1);
     while (true) {
       if (l == b0 && r == e0 - 1) {  // root of the whole range
-        a.nodes[nodeBase] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
+        st_node_policy(a.nodes + nodeBase, make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin), once);
         break;
       }
       // c0 <= l <= r < cEnd here: delta[l - 1] and delta[r] are in sLev
@@ -165,7 +168,8 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
       const uint32_t s = leftChild ? r + 1 : l;
       const uint32_t side = leftChild ? 0 : 1;
       if (s <= c0 || s >= cEnd) {  // sibling outside the chunk: global phase
-        a.nodes[2ull * s + side] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
+        st_node_policy(a.nodes + 2ull * s + side, make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin),
+                       once);
         a.pending[2 * blockIdx.x + (s <= c0 ? 0 : 1)] = make_uint2(l, r);
         break;
       }
@@ -177,7 +181,8 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
       cuda::atomic_ref<uint32_t, cuda::thread_scope_block> slotRef(sSlot[js]);
       const uint32_t other = slotRef.exchange(leftChild ? l : r, cuda::memory_order_acq_rel);
       // the node itself is read only by the global phase (a later launch)
-      a.nodes[2ull * s + side] = make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin);
+      st_node_policy(a.nodes + 2ull * s + side, make_node(box.lx, box.ly, box.lz, box.hx, box.hy, box.hz, admin),
+                     once);
       if (other == AGG_EMPTY) break;  // parked; the sibling (here or in the global phase) carries on
       const float4 s0 = sBox[js][side ^ 1][0], s1 = sBox[js][side ^ 1][1];
       const AggBox sib{s0.x, s0.y, s0.z, s0.w, s1.x, s1.y};

@@ -138,6 +138,33 @@ __device__ __forceinline__ Node ldcg_node(const Node *p)
   return n;
 }
 
+// L2 eviction priority (createpolicy): a kernel that streams data it
+// touches once (evict_first) past data it reads at random and may hit
+// again keeps more of the latter in L2
+__device__ __forceinline__ uint64_t l2_policy_evict_first()
+{
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// read-only load with an L2 policy
+__device__ __forceinline__ uint32_t ldg_u32_policy(const uint32_t *p, uint64_t pol)
+{
+  uint32_t v;
+  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+// 32-byte node store with an L2 policy (two 16-byte stores)
+__device__ __forceinline__ void st_node_policy(Node *p, const Node &n, uint64_t pol)
+{
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(&p->a), "f"(n.a.x), "f"(n.a.y),
+               "f"(n.a.z), "f"(n.a.w), "l"(pol)
+               : "memory");
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(&p->b), "f"(n.b.x), "f"(n.b.y),
+               "f"(n.b.z), "f"(n.b.w), "l"(pol)
+               : "memory");
+}
+
 // ------------------------------------------------------------------
 // order-preserving float <-> int32 (min/max over encoded ints equals a
 // total-order min/max over the floats; -0 < +0)
