@@ -315,7 +315,7 @@ PHASE_BYTES = {
     "morton.bounds": 24,            # box read
     "morton.keygen": 24 + 12,       # box read, key + id written
     "sort.onesweep64": 24,          # per pass: key+id read, key+id written
-    "morton.runs": 8 + 1 + 4,       # keys read, split level + slot written (+ rewrites inside runs)
+    "morton.runs": 8 + 1,           # keys read, split level written (+ rewrites inside runs)
     "morton.agg_local": 4 + 24 + 1 + 64 + 32,  # id, box gather, level, 2N nodes written, siblings read
     # morton.agg_global: the few chunk-crossing nodes, negligible bytes
 }
