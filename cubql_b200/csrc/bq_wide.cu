@@ -126,18 +126,32 @@ __global__ void k_wc_emit(const Node *__restrict__ nodes, uint32_t numNodes, con
 // ------------------------------------------------------------------
 // closest point over a wide tree
 // ------------------------------------------------------------------
-template <int N>
-struct WLocalStack {
-  uint64_t e[N];
+// the top WIDE_SMEM_STACK entries in shared memory (one column per thread,
+// so a warp's pushes and pops are conflict-free), the rest in local memory:
+// most wide traversals never go deeper than the shared part
+constexpr int WIDE_SMEM_STACK = 8;
+template <int S, int N>
+struct WHybridStack {
+  static_assert(S < N, "the shared part is the top of a deeper stack");
+  uint64_t *sh;     // &shared[0][threadIdx.x]
+  uint32_t stride;  // blockDim.x
+  uint64_t e[N - S];
   int sp = 0;
+  __device__ __forceinline__ explicit WHybridStack(uint64_t *base) : sh(base + threadIdx.x), stride(blockDim.x) {}
   __device__ __forceinline__ bool push(uint64_t v)
   {
     if (sp >= N) return false;
-    e[sp++] = v;
+    if (sp < S) sh[(uint32_t)sp * stride] = v;
+    else e[sp - S] = v;
+    sp++;
     return true;
   }
   __device__ __forceinline__ bool empty() const { return sp == 0; }
-  __device__ __forceinline__ uint64_t pop() { return e[--sp]; }
+  __device__ __forceinline__ uint64_t pop()
+  {
+    --sp;
+    return sp < S ? sh[(uint32_t)sp * stride] : e[sp - S];
+  }
 };
 
 struct WGlobalStack {
@@ -320,7 +334,8 @@ __global__ void __launch_bounds__(128) k_wide_closest(const Node *__restrict__ s
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const uint32_t qi = order ? __ldg(order + t) : t;
-  WLocalStack<STACK> st;
+  extern __shared__ uint64_t sWideStack[];
+  WHybridStack<WIDE_SMEM_STACK, STACK> st(sWideStack);
   if (!run_wide_cp<W, TIE>(slots, primIDs, points, queries, qi, maxSqr, st, outIds, outD))
     ovfList[atomicAdd(ovfCount, 1u)] = qi;
 }
@@ -351,9 +366,8 @@ void launch_wide_cp(const bq_wide_bvh3f *bvh, const float *points, const float *
   const Node *slots = (const Node *)bvh->nodes;
   {
     ProfScope ps("wide.closest", s);
-    k_wide_closest<W, TIE, STACK><<<div_up(nq, block), block, 0, s>>>(slots, bvh->primIDs, points, queries,
-                                                                      qs.order, nq, maxSqr, ids, d, qs.ovfList,
-                                                                      qs.ovfCount);
+    k_wide_closest<W, TIE, STACK><<<div_up(nq, block), block, WIDE_SMEM_STACK * sizeof(uint64_t) * block, s>>>(
+        slots, bvh->primIDs, points, queries, qs.order, nq, maxSqr, ids, d, qs.ovfList, qs.ovfCount);
   }
   ProfScope ps("wide.deep", s);
   k_wide_closest_deep<W, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(slots, bvh->primIDs, points, queries, maxSqr, ids,
