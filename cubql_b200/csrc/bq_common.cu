@@ -65,6 +65,32 @@ int Alloc::scratch_free(void *p)
   return free_bytes(p);
 }
 
+void *host_readback_buffer(size_t bytes)
+{
+  struct Buf {
+    void *p = nullptr;
+    size_t cap = 0;
+    ~Buf()
+    {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  static thread_local Buf b;
+  if (bytes > b.cap) {
+    if (b.p) cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    void *q = nullptr;
+    if (cudaMallocHost(&q, std::max(bytes, (size_t)256)) != cudaSuccess) {
+      cudaGetLastError();  // not sticky: clear it
+      return nullptr;
+    }
+    b.p = q;
+    b.cap = std::max(bytes, (size_t)256);
+  }
+  return b.p;
+}
+
 int num_sms()
 {
   int dev = 0, n = 148;

@@ -289,6 +289,11 @@ struct BuildState {
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 int num_sms();
+// a pinned host buffer of at least `bytes`, one per host thread (reused by
+// every call of that thread; nullptr if pinned memory cannot be had): the
+// builders' read-backs of their device counters land here directly instead
+// of being staged through pageable memory
+void *host_readback_buffer(size_t bytes);
 
 // ------------------------------------------------------------------
 // phase profiler (the counterpart of the reference's CUBQL_PROFILE,
@@ -371,8 +376,8 @@ __device__ __forceinline__ uint32_t block_scan_smem(uint32_t *s, uint32_t L, uin
 // else nMax.  dHist (optional) holds the per-pass 256-bin digit
 // histograms, already counted by the producer of the keys.
 // ctlWs (optional): onesweep_ctl_words(nMax, beginBit, endBit) words of
-// device memory the sort uses for its look-back state instead of
-// allocating them.
+// device memory, zeroed by the caller, that the sort uses for its
+// look-back state instead of allocating them.
 int onesweep_sort_u64(uint64_t *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_t *nDev, int beginBit,
                       int endBit, const uint32_t *dHist, int *outSel, uint32_t *dErr, Alloc &al,
                       uint32_t *ctlWs = nullptr);

@@ -101,8 +101,18 @@ __device__ __forceinline__ float ctr(float lo, float hi) { return __fdiv_rn(__fa
 // ------------------------------------------------------------------
 __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
                                                      Partial *__restrict__ partials, uint32_t *__restrict__ blockOff,
-                                                     BuildState *st, uint32_t *__restrict__ hist, int histWords)
+                                                     BuildState *st, uint32_t *__restrict__ hist, int histWords,
+                                                     uint32_t *__restrict__ zero, uint64_t zeroWords)
 {
+  // the sort's look-back state (16-byte aligned), zeroed here rather than by
+  // a memset launch of its own
+  {
+    uint4 *z4 = reinterpret_cast<uint4 *>(zero);
+    const uint64_t n4 = zeroWords / 4;
+    for (uint64_t i = (uint64_t)blockIdx.x * MB_BLOCK + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * MB_BLOCK)
+      z4[i] = make_uint4(0u, 0u, 0u, 0u);
+    if (blockIdx.x == 0 && threadIdx.x < (zeroWords & 3)) zero[n4 * 4 + threadIdx.x] = 0u;
+  }
   __shared__ int32_t sLo[3][MB_BLOCK / 32], sHi[3][MB_BLOCK / 32];
   __shared__ uint32_t sCnt[MB_BLOCK / 32];
   __shared__ uint32_t sLast;
@@ -724,12 +734,12 @@ __global__ void k_collapse(const Node *__restrict__ full, const uint2 *__restric
 namespace {
 // Orders the runs of equal top bits of at most MB_THREAD_RUN prims and writes
 // every split level (k_fix_runs); longer runs are listed in `runs`
-// and counted in *rs for long_runs.  Nothing waits here.
+// and counted in *rs (zeroed by the caller) for long_runs.  Nothing waits
+// here.
 template <int SB>
 int fix_runs(uint64_t *keys, uint32_t *ids, uint32_t n, const uint32_t *nvDev, uint8_t *delta, RunStats *rs,
              uint4 *runs, uint32_t maxRuns, Alloc &al)
 {
-  BQ_CUDA(cudaMemsetAsync(rs, 0, sizeof(RunStats), al.s));
   ProfScope ps("morton.runs", al.s);
   k_fix_runs<SB><<<div_up(n, FT_TILE), FT_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, rs, runs, maxRuns);
   BQ_CUDA(cudaGetLastError());
@@ -817,6 +827,7 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   const bool wide4 = n > (1u << 24);  // more than 2^24 prims: sort 32 top bits in 4 passes instead of 24 in 3
   const int sb = wide4 ? MB_SB4 : MB_SB3;
   const int histWords = (wide4 ? hist_passes<MB_SB4>() : hist_passes<MB_SB3>()) * 256;
+  const size_t sortCtlWords = onesweep_ctl_words(n, sb, 63);
   const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
   Ctl *ctl = nullptr;
   Partial *partials = nullptr;
@@ -836,7 +847,7 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
     c.take(&slot, n);
     c.take(&runs, maxRuns);
     c.take(&pending, 2ull * div_up(n, AGG_CHUNK));
-    c.take(&sortCtl, onesweep_ctl_words(n, sb, 63));
+    c.take(&sortCtl, sortCtlWords);
   };
   Carver sizing(nullptr);
   carve(sizing);
@@ -857,12 +868,13 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   if (thr == 1) {
     if ((s = al.get(&nodes, 2ull * n)) != BQ_OK) return fail(s);
   }
-  cudaError_t ce = cudaMemsetAsync(st, 0, sizeof(BuildState), al.s);
+  cudaError_t ce = cudaMemsetAsync(ctl, 0, sizeof(Ctl), al.s);  // build state and run statistics
   if (ce != cudaSuccess) return fail(cuda_error(ce, "memset"));
 
   {
     ProfScope ps("morton.bounds", al.s);
-    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, histWords);
+    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, histWords, sortCtl,
+                                          sortCtlWords);
   }
   {
     ProfScope ps("morton.keygen", al.s);
@@ -889,8 +901,10 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   // what the host reads back (one copy): the long-run statistics, the valid
   // count, the error word
   struct { RunStats runs; uint32_t nv, err; } h = {};
+  Ctl *pinned = static_cast<Ctl *>(host_readback_buffer(sizeof(Ctl)));
   auto read_back = [&]() -> cudaError_t {
-    Ctl hc;
+    Ctl local;
+    Ctl &hc = pinned ? *pinned : local;
     cudaError_t e = cudaMemcpyAsync(&hc, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, al.s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(al.s);
     h.runs = hc.runs;

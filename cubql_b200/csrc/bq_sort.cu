@@ -375,8 +375,10 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
   uint32_t *hist = nullptr, *ctl = ctlWs;
   // ctl layout: [status: numPasses*numTiles*256][tileCtr: numPasses][abort: 1]
   const size_t statusWords = (size_t)numPasses * numTiles * 256;
-  if (!ctl) BQ_TRY(tmp.get(&ctl, statusWords + numPasses + 1));
-  BQ_CUDA(cudaMemsetAsync(ctl, 0, sizeof(uint32_t) * (statusWords + numPasses + 1), al.s));
+  if (!ctl) {  // a caller's workspace comes zeroed
+    BQ_TRY(tmp.get(&ctl, statusWords + numPasses + 1));
+    BQ_CUDA(cudaMemsetAsync(ctl, 0, sizeof(uint32_t) * (statusWords + numPasses + 1), al.s));
+  }
   if (preHist) {
     hist = const_cast<uint32_t *>(preHist);
   } else {

@@ -15,6 +15,8 @@
  *     release threshold was raised (set once per device);
  *   - the phase profiler's event pool (bq_profile_*, per thread, only
  *     while profiling is enabled);
+ *   - a small pinned host buffer per thread that the builders read their
+ *     device-side counters back into (allocated on first use);
  *   - the fixed scratch array of bq_refit_noalloc_f3 (shared by all of
  *     its calls; see there);
  *   - the count of bq_debug_inject_sort_timeout (a test hook, 0 unless a
