@@ -916,13 +916,21 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
     return wide4 ? long_runs<MB_SB4>(h.runs, runs, keys, ids, keys2[sel ^ 1], idsOther, delta, &st->err, al)
                  : long_runs<MB_SB3>(h.runs, runs, keys, ids, keys2[sel ^ 1], idsOther, delta, &st->err, al);
   };
-  // the long-run statistics decide what runs next (one read back)
+  // The one read-back of a build: the valid count, the sort's error word
+  // and the long-run statistics, which decide what runs next.  Without long
+  // runs nothing after this point can fail on the device, so the
+  // agglomeration is left running on the stream (stream-ordered, like the
+  // reference builder, which returns before its refit completes); with them
+  // a second read-back collects the long-run sort's error word.
   if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
   if (h.runs.pad) return fail(set_error(BQ_ERR_CUDA, "run list overflow in the Morton build"));
+  if (h.err & DEV_ERR_TIMEOUT) return fail(set_error(BQ_ERR_TIMEOUT, "radix sort look-back timed out"));
+  if (h.err) return fail(set_error(BQ_ERR_CUDA, "device-side range check failed in the Morton build"));
+  const bool longRuns = h.runs.count > 0;
   if ((s = do_long_runs()) != BQ_OK) return fail(s);
   if (thr == 1) {
     if ((s = agglomerate<false>(ag, n, al.s, "morton.agg_local", "morton.agg_global")) != BQ_OK) return fail(s);
-    if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
+    if (longRuns && (ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
   } else {
     Node *full = nullptr;
     uint2 *ranges = nullptr;
@@ -949,7 +957,7 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
     k_collapse<<<div_up(n, 256), 256, 0, al.s>>>(full, ranges, kept, rank, &st->numValid, thr, nodes);
     if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_collapse"));
     if (hostNv > 0) bvh->numNodes = (uint32_t)numNodes;
-    if ((ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
+    if (longRuns && (ce = read_back()) != cudaSuccess) return fail(cuda_error(ce, "build sync"));
   }
   if (h.err & DEV_ERR_TIMEOUT) return fail(set_error(BQ_ERR_TIMEOUT, "radix sort look-back timed out"));
   if (h.err) return fail(set_error(BQ_ERR_CUDA, "device-side range check failed in the Morton build"));

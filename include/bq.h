@@ -95,7 +95,10 @@ typedef struct bq_build_config {
 } bq_build_config;
 
 /* replaces cuBQL::GpuMemoryResource (cuBQL/builder/cuda.h:31-78).
-   NULL = cudaMallocAsync / cudaFreeAsync on the call's stream. */
+   NULL = cudaMallocAsync / cudaFreeAsync on the call's stream.  Frees are
+   stream-ordered: free(ctx, ptr, stream) may be called while work queued
+   on `stream` still uses ptr, so the memory must not go to other streams
+   before that work completes (as with cudaFreeAsync). */
 typedef struct bq_allocator {
   void *ctx;
   int (*malloc)(void *ctx, void **ptr, size_t size, bq_stream_t stream); /* 0 on success */
@@ -133,8 +136,12 @@ typedef struct bq_query_config {
    implementation cuBQL/builder/cuda/radix.h:591-771).  The tree equals
    the reference's node for node after BFS renumbering.  Empty boxes
    (lower.x > upper.x) are left out.  Allocates bvh->nodes and
-   bvh->primIDs with `alloc`; synchronises `stream` once at the end to
-   learn the node count. */
+   bvh->primIDs with `alloc`.  Synchronises `stream` once, after the
+   sort, to learn the valid-prim count, the sort's status and whether
+   long runs of equal keys need their extra pass (and once more at the end
+   when they do); otherwise the bottom-up agglomeration is still running
+   on `stream` when the call returns (stream-ordered, as the reference's
+   builder returns before its refit completes). */
 int bq_build_morton63_f3(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t numPrims, const bq_build_config *cfg,
                          const bq_allocator *alloc, bq_stream_t stream);
 
