@@ -54,7 +54,8 @@ __device__ __forceinline__ uint32_t seg_of(const uint32_t *__restrict__ off, uin
   return lo;
 }
 
-__device__ __forceinline__ float ctr(float lo, float hi) { return __fdiv_rn(__fadd_rn(lo, hi), 2.0f); }
+// box center (lower + upper) / 2, as a multiply by 0.5: the same float
+__device__ __forceinline__ float ctr(float lo, float hi) { return __fmul_rn(__fadd_rn(lo, hi), 0.5f); }
 
 struct SegQuant {
   float bias[3];

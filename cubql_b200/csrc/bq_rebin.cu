@@ -52,13 +52,14 @@ __host__ __device__ constexpr uint16_t broad_level(int depth, int bit)
   return (uint16_t)(64 + (REBIN_MAX_DEPTH - depth) * 32 + bit);
 }
 
-// box.center() = (lower+upper)/2 (cuBQL/math/box.h:146-147)
+// box.center() = (lower+upper)/2 (cuBQL/math/box.h:146-147), as a multiply
+// by 0.5 (the same float: both round the same real number)
 __device__ __forceinline__ float3 rb_center(const bq_box3f *__restrict__ boxes, uint32_t id)
 {
   const float2 *bp = reinterpret_cast<const float2 *>(boxes + id);
   const float2 p0 = __ldg(bp), p1 = __ldg(bp + 1), p2 = __ldg(bp + 2);
-  return make_float3(__fdiv_rn(__fadd_rn(p0.x, p1.y), 2.0f), __fdiv_rn(__fadd_rn(p0.y, p2.x), 2.0f),
-                     __fdiv_rn(__fadd_rn(p1.x, p2.y), 2.0f));
+  return make_float3(__fmul_rn(__fadd_rn(p0.x, p1.y), 0.5f), __fmul_rn(__fadd_rn(p0.y, p2.x), 0.5f),
+                     __fmul_rn(__fadd_rn(p1.x, p2.y), 0.5f));
 }
 
 // Quantizer<float,3>::init over [lo, hi] (rebinMortonBuilder.h:40-47):

@@ -89,7 +89,8 @@ struct SmSplit {
   uint32_t tb;
 };
 
-__device__ __forceinline__ float ctr2(float lo, float hi) { return __fdiv_rn(__fadd_rn(lo, hi), 2.0f); }
+// box center (lower + upper) / 2, as a multiply by 0.5: the same float
+__device__ __forceinline__ float ctr2(float lo, float hi) { return __fmul_rn(__fadd_rn(lo, hi), 0.5f); }
 
 // selectSplits (sm_builder.h:192-219)
 __device__ __forceinline__ SmSplit choose_split(const SmNode &nd)
