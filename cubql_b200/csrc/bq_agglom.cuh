@@ -120,6 +120,7 @@ using AggArgs = AggArgsT<uint8_t>;
 template <bool SEG, typename LevT>
 __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
 {
+  griddep_wait();
   __shared__ uint32_t sSlot[AGG_CHUNK + 1];
   __shared__ float4 sBox[AGG_CHUNK + 1][2][2];  // a box as two 16-byte words: lx ly lz hx | hy hz - -
   __shared__ LevT sLev[AGG_CHUNK + 2];  // delta[c0 - 1 .. c0 + AGG_CHUNK]
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(AGG_CHUNK) k_agg_local(AggArgsT<LevT> a)
 template <bool SEG, typename LevT>
 __global__ void k_agg_global(AggArgsT<LevT> a, uint32_t numPending)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numPending) return;
   const uint32_t nv = *a.nvPtr;
@@ -260,11 +262,11 @@ inline int agglomerate(AggArgsT<LevT> a, uint32_t nvMax, cudaStream_t s, const c
   const int chunks = div_up(nvMax, AGG_CHUNK);
   {
     ProfScope ps(profLocal ? profLocal : "agg.local", s);
-    k_agg_local<SEG, LevT><<<chunks, AGG_CHUNK, 0, s>>>(a);
+    BQ_CUDA(launch_pdl(k_agg_local<SEG, LevT>, dim3(chunks), dim3(AGG_CHUNK), 0, s, a));
   }
   {
     ProfScope ps(profGlobal ? profGlobal : "agg.global", s);
-    k_agg_global<SEG, LevT><<<div_up(2 * chunks, 128), 128, 0, s>>>(a, 2u * chunks);
+    BQ_CUDA(launch_pdl(k_agg_global<SEG, LevT>, dim3(div_up(2 * chunks, 128)), dim3(128), 0, s, a, 2u * chunks));
   }
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;

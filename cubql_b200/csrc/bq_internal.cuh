@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <utility>
 
 #include "../../include/bq.h"
 
@@ -302,6 +303,34 @@ void *host_readback_buffer(size_t bytes);
 // stream synchronised) turns them into per-name launch counts and times.
 // Off by default; costs one branch per phase when off.
 // ------------------------------------------------------------------
+// ------------------------------------------------------------------
+// programmatic dependent launch (sm_90 and later): a kernel launched with
+// launch_pdl may be scheduled as soon as the previous kernel on the stream
+// has let its blocks finish, before that grid has fully completed; it
+// must call griddep_wait() before it touches any memory the previous
+// kernels write or read.  griddep_wait() returns at once in a kernel
+// launched the ordinary way, so a kernel that calls it first thing may be
+// launched either way.
+// ------------------------------------------------------------------
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args &&...args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 bool prof_enabled();
 void prof_record(const char *name, cudaStream_t s, bool begin, int launches);
 void prof_flush();

@@ -3,11 +3,11 @@
 // Builds the same tree as cuBQL::cuda::radixBuilder<float,3>
 // (cuBQL/builder/cuda/radix.h:591-771), without its per-level host loop:
 //
-//   k_bounds      centroid bounds of the valid prims, valid count per block
-//                 and, in the last block to finish, the global bounds,
-//                 the per-block compaction offsets and the quantizer
+//   k_bounds      centroid bounds and valid count of each block's chunk
 //                 (radix.h:185-241 fillBuildState/finishBuildState)
-//   k_keygen      stable compaction of valid prims, 63-bit Morton keys
+//   k_keygen      every block first reduces those partials to the global
+//                 bounds, the quantizer and its own compaction offset; then
+//                 stable compaction of valid prims, 63-bit Morton keys
 //                 (radix.h:41-62 Quantizer, 283-421 key generation) and the
 //                 digit histograms of the top key bits
 //   onesweep sort stable (key, primID) sort on the top key bits only:
@@ -103,9 +103,8 @@ __device__ __forceinline__ float ctr(float lo, float hi) { return __fmul_rn(__fa
 // pass 1: bounds
 // ------------------------------------------------------------------
 __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
-                                                     Partial *__restrict__ partials, uint32_t *__restrict__ blockOff,
-                                                     BuildState *st, uint32_t *__restrict__ hist, int histWords,
-                                                     uint32_t *__restrict__ zero, uint64_t zeroWords)
+                                                     Partial *__restrict__ partials, uint32_t *__restrict__ hist,
+                                                     int histWords, uint32_t *__restrict__ zero, uint64_t zeroWords)
 {
   // the sort's look-back state (16-byte aligned), zeroed here rather than by
   // a memset launch of its own
@@ -115,10 +114,10 @@ __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict_
     for (uint64_t i = (uint64_t)blockIdx.x * MB_BLOCK + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * MB_BLOCK)
       z4[i] = make_uint4(0u, 0u, 0u, 0u);
     if (blockIdx.x == 0 && threadIdx.x < (zeroWords & 3)) zero[n4 * 4 + threadIdx.x] = 0u;
+    for (int i = blockIdx.x * MB_BLOCK + threadIdx.x; i < histWords; i += gridDim.x * MB_BLOCK) hist[i] = 0;
   }
   __shared__ int32_t sLo[3][MB_BLOCK / 32], sHi[3][MB_BLOCK / 32];
   __shared__ uint32_t sCnt[MB_BLOCK / 32];
-  __shared__ uint32_t sLast;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = min((uint64_t)n, begin + chunk);
@@ -162,72 +161,72 @@ __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict_
       p.cnt += sCnt[w];
     }
     partials[blockIdx.x] = p;
-    __threadfence();
-    sLast = (atomicAdd(&st->ticket, 1u) == gridDim.x - 1);
   }
-  __syncthreads();
-  if (!sLast) return;
-  // ---- last block: global reduction, compaction offsets, quantizer ----
-  __threadfence();
-  __shared__ uint32_t sScan[MB_BLOCK / 32];
-  uint32_t carry = 0;
-  int32_t glo[3] = {INT_MAX, INT_MAX, INT_MAX}, ghi[3] = {INT_MIN, INT_MIN, INT_MIN};
-  for (uint32_t b0 = 0; b0 < gridDim.x; b0 += MB_BLOCK) {
-    uint32_t b = b0 + threadIdx.x;
-    uint32_t c = 0;
-    if (b < gridDim.x) {
-      const Partial *pp = partials + b;
-      c = __ldcg(&pp->cnt);
-      for (int d = 0; d < 3; d++) {
-        glo[d] = min(glo[d], __ldcg(&pp->lo[d]));
-        ghi[d] = max(ghi[d], __ldcg(&pp->hi[d]));
-      }
-    }
-    // block exclusive scan of c
-    uint32_t x = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) sScan[warp] = x;
-    __syncthreads();
-    uint32_t wbase = 0, tot = 0;
-    for (int w = 0; w < MB_BLOCK / 32; w++) {
-      if (w < warp) wbase += sScan[w];
-      tot += sScan[w];
-    }
-    if (b < gridDim.x) blockOff[b] = carry + wbase + x - c;
-    carry += tot;
-    __syncthreads();
+}
+
+// The global centroid bounds, the quantizer (Quantizer<float,3>::init,
+// radix.h:46-53) and this block's compaction offset, reduced from the
+// per-block partials of k_bounds by every block of k_keygen (gridDim.x x
+// 32 B from L2): k_bounds then has no serial last block.  Block 0 also
+// records them in *st for the later kernels and the host.
+struct KeyQuant {
+  float bias[3], scale;
+  uint32_t before, total;  // valid prims of the blocks before this one; of all blocks
+};
+__device__ __forceinline__ KeyQuant reduce_partials(const Partial *__restrict__ partials, BuildState *st)
+{
+  __shared__ int32_t sLo[3][MB_BLOCK / 32], sHi[3][MB_BLOCK / 32];
+  __shared__ uint32_t sTot[MB_BLOCK / 32], sBefore[MB_BLOCK / 32];
+  __shared__ KeyQuant sQ;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int32_t lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+  uint32_t tot = 0, before = 0;
+  for (uint32_t b = threadIdx.x; b < gridDim.x; b += MB_BLOCK) {
+    const int4 *pp = reinterpret_cast<const int4 *>(partials + b);
+    const int4 q0 = __ldg(pp), q1 = __ldg(pp + 1);  // lo[3] hi[0] | hi[1] hi[2] cnt pad
+    lo[0] = min(lo[0], q0.x); lo[1] = min(lo[1], q0.y); lo[2] = min(lo[2], q0.z);
+    hi[0] = max(hi[0], q0.w); hi[1] = max(hi[1], q1.x); hi[2] = max(hi[2], q1.y);
+    tot += (uint32_t)q1.z;
+    if (b < blockIdx.x) before += (uint32_t)q1.z;
   }
   for (int d = 0; d < 3; d++) {
-    glo[d] = __reduce_min_sync(0xffffffffu, glo[d]);
-    ghi[d] = __reduce_max_sync(0xffffffffu, ghi[d]);
+    lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
+    hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
   }
-  if (lane == 0)
-    for (int d = 0; d < 3; d++) { sLo[d][warp] = glo[d]; sHi[d][warp] = ghi[d]; }
+  tot = __reduce_add_sync(0xffffffffu, tot);
+  before = __reduce_add_sync(0xffffffffu, before);
+  if (lane == 0) {
+    for (int d = 0; d < 3; d++) { sLo[d][warp] = lo[d]; sHi[d][warp] = hi[d]; }
+    sTot[warp] = tot;
+    sBefore[warp] = before;
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < histWords; i += MB_BLOCK) hist[i] = 0;
   if (threadIdx.x == 0) {
-    float lo[3], sz[3];
+    KeyQuant q;
+    q.total = 0;
+    q.before = 0;
+    for (int w = 0; w < MB_BLOCK / 32; w++) { q.total += sTot[w]; q.before += sBefore[w]; }
+    int32_t a[3], b[3];
+    float sz[3];
     for (int d = 0; d < 3; d++) {
-      int32_t a = INT_MAX, b = INT_MIN;
-      for (int w = 0; w < MB_BLOCK / 32; w++) { a = min(a, sLo[d][w]); b = max(b, sHi[d][w]); }
-      if (carry == 0) { a = enc_f(FLT_MAX); b = enc_f(-FLT_MAX); }  // AtomicBox::set_empty
-      st->cbLo[d] = a;
-      st->cbHi[d] = b;
-      lo[d] = dec_f(a);
-      sz[d] = __fsub_rn(dec_f(b), lo[d]);
+      a[d] = INT_MAX;
+      b[d] = INT_MIN;
+      for (int w = 0; w < MB_BLOCK / 32; w++) { a[d] = min(a[d], sLo[d][w]); b[d] = max(b[d], sHi[d][w]); }
+      if (q.total == 0) { a[d] = enc_f(FLT_MAX); b[d] = enc_f(-FLT_MAX); }  // AtomicBox::set_empty
+      q.bias[d] = dec_f(a[d]);
+      sz[d] = __fsub_rn(dec_f(b[d]), q.bias[d]);
     }
-    // Quantizer<float,3>::init (radix.h:46-53)
     const float ext = fmaxf(fmaxf(sz[0], sz[1]), sz[2]);
-    const float rc = __fdiv_rn(1.0f, fmaxf(ext, 1e-20f));
-    for (int d = 0; d < 3; d++) st->bias[d] = lo[d];
-    st->scale = __fmul_rn(2097152.0f, rc);
-    st->numValid = carry;
-    st->ticket = 0;
+    q.scale = __fmul_rn(2097152.0f, __fdiv_rn(1.0f, fmaxf(ext, 1e-20f)));
+    sQ = q;
+    if (blockIdx.x == 0) {
+      for (int d = 0; d < 3; d++) { st->cbLo[d] = a[d]; st->cbHi[d] = b[d]; st->bias[d] = q.bias[d]; }
+      st->scale = q.scale;
+      st->numValid = q.total;
+    }
   }
+  __syncthreads();
+  return sQ;
 }
 
 // ------------------------------------------------------------------
@@ -235,18 +234,19 @@ __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict_
 // ------------------------------------------------------------------
 template <int SB>
 __global__ void __launch_bounds__(MB_BLOCK) k_keygen(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
-                                                     const uint32_t *__restrict__ blockOff,
-                                                     const Partial *__restrict__ partials, const BuildState *st,
+                                                     const Partial *__restrict__ partials, BuildState *st,
                                                      uint64_t *__restrict__ keys, uint32_t *__restrict__ ids,
                                                      uint32_t *__restrict__ hist)
 {
+  griddep_wait();
   constexpr int PASSES = hist_passes<SB>();
   __shared__ uint32_t sHist[PASSES * 256];
   __shared__ uint32_t sWarpCnt[MB_UNROLL][MB_BLOCK / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = threadIdx.x; i < PASSES * 256; i += MB_BLOCK) sHist[i] = 0;
-  const float bx = st->bias[0], by = st->bias[1], bz = st->bias[2], sc = st->scale;
-  uint32_t running = blockOff[blockIdx.x];
+  const KeyQuant q = reduce_partials(partials, st);
+  const float bx = q.bias[0], by = q.bias[1], bz = q.bias[2], sc = q.scale;
+  uint32_t running = q.before;
   const uint64_t begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t end = min((uint64_t)n, begin + chunk);
   // every box of the chunk valid (the common case): prim i goes to position
@@ -472,6 +472,7 @@ __global__ void __launch_bounds__(FT_BLOCK, 8) k_fix_runs(uint64_t *keys, uint32
                                                        uint8_t *__restrict__ delta,
                                                        RunStats *rs, uint4 *runs, uint32_t maxRuns)
 {
+  griddep_wait();
   __shared__ uint64_t sK[FT_TILE + FT_HALO + 1];  // [0]: position base-1, [1+j]: base+j
   __shared__ uint16_t sR2[FT_TILE / 2], sR34[FT_TILE / 3 + 1], sRL[FT_TILE / 5 + 1];
   __shared__ uint32_t sCnt[3];
@@ -744,7 +745,8 @@ int fix_runs(uint64_t *keys, uint32_t *ids, uint32_t n, const uint32_t *nvDev, u
              uint4 *runs, uint32_t maxRuns, Alloc &al)
 {
   ProfScope ps("morton.runs", al.s);
-  k_fix_runs<SB><<<div_up(n, FT_TILE), FT_BLOCK, 0, al.s>>>(keys, ids, nvDev, delta, rs, runs, maxRuns);
+  BQ_CUDA(launch_pdl(k_fix_runs<SB>, dim3(div_up(n, FT_TILE)), dim3(FT_BLOCK), 0, al.s, keys, ids, nvDev, delta, rs,
+                     runs, maxRuns));
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }
@@ -834,7 +836,7 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   const uint32_t maxRuns = n / (MB_THREAD_RUN + 1) + 1;
   Ctl *ctl = nullptr;
   Partial *partials = nullptr;
-  uint32_t *blockOff = nullptr, *hist = nullptr, *slot = nullptr, *sortCtl = nullptr;
+  uint32_t *hist = nullptr, *slot = nullptr, *sortCtl = nullptr;
   uint64_t *keysA = nullptr, *keysB = nullptr;
   uint8_t *delta = nullptr;
   uint4 *runs = nullptr;
@@ -842,7 +844,6 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   auto carve = [&](Carver &c) {
     c.take(&ctl, 1);
     c.take(&partials, grid);
-    c.take(&blockOff, grid);
     c.take(&hist, MB_MAX_HIST_PASSES * 256);
     c.take(&keysA, n);
     c.take(&keysB, n);
@@ -876,17 +877,19 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
 
   {
     ProfScope ps("morton.bounds", al.s);
-    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, blockOff, st, hist, histWords, sortCtl,
-                                          sortCtlWords);
+    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, hist, histWords, sortCtl, sortCtlWords);
   }
   {
     ProfScope ps("morton.keygen", al.s);
     if (wide4)
-      k_keygen<MB_SB4><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, partials, st, keysA, idsA, hist);
+      ce = launch_pdl(k_keygen<MB_SB4>, dim3(grid), dim3(MB_BLOCK), 0, al.s, boxes, n, chunk, (const Partial *)partials,
+                      st, keysA, idsA, hist);
     else
-      k_keygen<MB_SB3><<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, blockOff, partials, st, keysA, idsA, hist);
+      ce = launch_pdl(k_keygen<MB_SB3>, dim3(grid), dim3(MB_BLOCK), 0, al.s, boxes, n, chunk, (const Partial *)partials,
+                      st, keysA, idsA, hist);
   }
-  if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_bounds/k_keygen"));
+  if (ce == cudaSuccess) ce = cudaGetLastError();
+  if (ce != cudaSuccess) return fail(cuda_error(ce, "k_bounds/k_keygen"));
 
   uint64_t *keys2[2] = {keysA, keysB};
   uint32_t *ids2[2] = {idsA, idsB};

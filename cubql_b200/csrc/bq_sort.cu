@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(SORT_BLOCK, 4) k_onesweep(const KeyT *__restri
                                                             uint32_t *__restrict__ valsOut, uint32_t nHost,
                                                             const uint32_t *nDev, int shift, PassCtl ctl)
 {
+  griddep_wait();  // the previous pass (or the keys' producer) has finished
   const uint32_t n = nDev ? *nDev : nHost;
   constexpr int TILE = SORT_BLOCK * ITEMS;
   constexpr int WARP_ITEMS = 32 * ITEMS;
@@ -349,6 +350,7 @@ template <typename KeyT>
 __global__ void k_sort_repair(KeyT *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t nHost,
                               const uint32_t *nDev, const uint32_t *abort, const uint32_t *err)
 {
+  griddep_wait();
   if (ld_volatile(abort) == 0 && (!err || (ld_volatile(err) & DEV_ERR_RANGE) == 0)) return;
   const uint32_t n = nDev ? *nDev : nHost;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -417,28 +419,26 @@ int onesweep_impl(KeyT *keys[2], uint32_t *vals[2], uint32_t nMax, const uint32_
     const int sh = beginBit + 8 * p;
     // the 32-bit word of a 64-bit key that holds this pass's digit, if one does
     const int word = sizeof(KeyT) != 8 ? -1 : sh >= 32 ? 1 : sh + 8 <= 32 ? 0 : -1;
-    bool launched = false;
+    // each pass may be scheduled while the one before drains (it waits for
+    // it before its first access)
+    auto launch = [&](auto kernel) {
+      return launch_pdl(kernel, dim3(numTiles), dim3(SORT_BLOCK), smemBytes, al.s, (const KeyT *)keys[sel],
+                        keys[sel ^ 1], (const uint32_t *)vals[sel], vals[sel ^ 1], nMax, nDev, sh, c);
+    };
+    cudaError_t le = cudaSuccess;
     if constexpr (sizeof(KeyT) == 8) {
-      if (word >= 0) {
-        if (word == 1)
-          k_onesweep<KeyT, ITEMS, 1><<<numTiles, SORT_BLOCK, smemBytes, al.s>>>(keys[sel], keys[sel ^ 1], vals[sel],
-                                                                              vals[sel ^ 1], nMax, nDev, sh, c);
-        else
-          k_onesweep<KeyT, ITEMS, 0><<<numTiles, SORT_BLOCK, smemBytes, al.s>>>(keys[sel], keys[sel ^ 1], vals[sel],
-                                                                              vals[sel ^ 1], nMax, nDev, sh, c);
-        launched = true;
-      }
+      le = word == 1 ? launch(k_onesweep<KeyT, ITEMS, 1>)
+                     : word == 0 ? launch(k_onesweep<KeyT, ITEMS, 0>) : launch(k_onesweep<KeyT, ITEMS, -1>);
+    } else {
+      le = launch(k_onesweep<KeyT, ITEMS, -1>);
     }
-    if (!launched)
-      k_onesweep<KeyT, ITEMS, -1><<<numTiles, SORT_BLOCK, smemBytes, al.s>>>(keys[sel], keys[sel ^ 1], vals[sel],
-                                                                           vals[sel ^ 1], nMax, nDev, sh, c);
-    BQ_CUDA(cudaGetLastError());
+    BQ_CUDA(le);
     sel ^= 1;
   }
   {
     ProfScope ps("sort.repair", al.s);
-    k_sort_repair<KeyT><<<num_sms(), 256, 0, al.s>>>(keys[sel], vals[sel], nMax, nDev, ctl + statusWords + numPasses,
-                                                     dErr);
+    BQ_CUDA(launch_pdl(k_sort_repair<KeyT>, dim3(num_sms()), dim3(256), 0, al.s, keys[sel], vals[sel], nMax, nDev,
+                       (const uint32_t *)(ctl + statusWords + numPasses), (const uint32_t *)dErr));
   }
   BQ_CUDA(cudaGetLastError());
   *outSel = sel;
