@@ -104,11 +104,16 @@ __device__ __forceinline__ float ctr(float lo, float hi) { return __fmul_rn(__fa
 // ------------------------------------------------------------------
 __global__ void __launch_bounds__(MB_BLOCK) k_bounds(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t chunk,
                                                      Partial *__restrict__ partials, uint32_t *__restrict__ hist,
-                                                     int histWords, uint32_t *__restrict__ zero, uint64_t zeroWords)
+                                                     int histWords, uint32_t *__restrict__ zero, uint64_t zeroWords,
+                                                     uint32_t *__restrict__ ctl, int ctlWords)
 {
-  // the sort's look-back state (16-byte aligned), zeroed here rather than by
-  // a memset launch of its own
+  griddep_wait();  // the previous work on the stream (its memory may be reused here) is done
+  // the build state and run statistics, the digit histograms and the sort's
+  // look-back state (16-byte aligned), zeroed here rather than by memset
+  // launches of their own
   {
+    if (blockIdx.x == 0)
+      for (int i = threadIdx.x; i < ctlWords; i += MB_BLOCK) ctl[i] = 0u;
     uint4 *z4 = reinterpret_cast<uint4 *>(zero);
     const uint64_t n4 = zeroWords / 4;
     for (uint64_t i = (uint64_t)blockIdx.x * MB_BLOCK + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * MB_BLOCK)
@@ -827,6 +832,7 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
     BuildState st;
     RunStats runs;
   };
+  static_assert(sizeof(Ctl) % 4 == 0, "k_bounds zeroes the control block as words");
   // all temporaries of the build in one allocation (one call to the
   // allocator instead of a dozen before the first kernel can start)
   const bool wide4 = n > (1u << 24);  // more than 2^24 prims: sort 32 top bits in 4 passes instead of 24 in 3
@@ -872,14 +878,14 @@ int build_morton63(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_bu
   if (thr == 1) {
     if ((s = al.get(&nodes, 2ull * n)) != BQ_OK) return fail(s);
   }
-  cudaError_t ce = cudaMemsetAsync(ctl, 0, sizeof(Ctl), al.s);  // build state and run statistics
-  if (ce != cudaSuccess) return fail(cuda_error(ce, "memset"));
+  cudaError_t ce = cudaSuccess;
 
   {
     ProfScope ps("morton.bounds", al.s);
-    k_bounds<<<grid, MB_BLOCK, 0, al.s>>>(boxes, n, chunk, partials, hist, histWords, sortCtl, sortCtlWords);
+    ce = launch_pdl(k_bounds, dim3(grid), dim3(MB_BLOCK), 0, al.s, boxes, n, chunk, partials, hist, histWords, sortCtl,
+                    (uint64_t)sortCtlWords, reinterpret_cast<uint32_t *>(ctl), (int)(sizeof(Ctl) / 4));
   }
-  {
+  if (ce == cudaSuccess) {
     ProfScope ps("morton.keygen", al.s);
     if (wide4)
       ce = launch_pdl(k_keygen<MB_SB4>, dim3(grid), dim3(MB_BLOCK), 0, al.s, boxes, n, chunk, (const Partial *)partials,
