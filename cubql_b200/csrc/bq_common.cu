@@ -138,6 +138,7 @@ __device__ __forceinline__ uint32_t block_excl(uint32_t v, uint32_t *sh, uint32_
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_reduce(const uint32_t *in, uint32_t nMax, const uint32_t *nDev,
                                                             uint32_t *blockSums)
 {
+  griddep_wait();
   __shared__ uint32_t sh[8];
   const uint32_t n = nDev ? min(*nDev, nMax) : nMax;  // never past the buffers
   const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE;
@@ -154,6 +155,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_reduce(const uint32_t *in, 
 
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_blocks(uint32_t *blockSums, int numBlocks, uint32_t *dTotal)
 {
+  griddep_wait();
   __shared__ uint32_t sh[8];
   uint32_t carry = 0;
   for (int b0 = 0; b0 < numBlocks; b0 += SCAN_BLOCK) {
@@ -170,6 +172,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_blocks(uint32_t *blockSums,
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_final(const uint32_t *in, uint32_t *out, uint32_t nMax,
                                                            const uint32_t *nDev, const uint32_t *blockOffsets)
 {
+  griddep_wait();
   __shared__ uint32_t sh[8];
   const uint32_t n = nDev ? min(*nDev, nMax) : nMax;  // never past the buffers
   const uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
@@ -205,9 +208,9 @@ int exclusive_scan_u32(const uint32_t *in, uint32_t *out, uint32_t nMax, const u
   TempSet tmp(al);
   uint32_t *sums = nullptr;
   BQ_TRY(tmp.get(&sums, numBlocks));
-  k_scan_reduce<<<numBlocks, SCAN_BLOCK, 0, al.s>>>(in, nMax, nDev, sums);
-  k_scan_blocks<<<1, SCAN_BLOCK, 0, al.s>>>(sums, numBlocks, dTotal);
-  k_scan_final<<<numBlocks, SCAN_BLOCK, 0, al.s>>>(in, out, nMax, nDev, sums);
+  launch_pdl(k_scan_reduce, dim3(numBlocks), dim3(SCAN_BLOCK), 0, al.s, in, nMax, nDev, sums);
+  launch_pdl(k_scan_blocks, dim3(1), dim3(SCAN_BLOCK), 0, al.s, sums, numBlocks, dTotal);
+  launch_pdl(k_scan_final, dim3(numBlocks), dim3(SCAN_BLOCK), 0, al.s, in, out, nMax, nDev, sums);
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }

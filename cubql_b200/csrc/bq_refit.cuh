@@ -35,6 +35,7 @@ constexpr uint32_t RF_NO_PARENT = 0xffffffffu;
 __global__ void k_refit_init(uint32_t numNodes, uint32_t *__restrict__ parent, uint32_t *__restrict__ counter,
                              uint32_t *__restrict__ err)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) *err = 0;
   if (i >= numNodes) return;
@@ -45,6 +46,7 @@ __global__ void k_refit_init(uint32_t numNodes, uint32_t *__restrict__ parent, u
 __global__ void k_refit_parents(const Node *__restrict__ nodes, uint32_t numNodes, uint32_t *__restrict__ parent,
                                 uint32_t *__restrict__ err)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= numNodes || i == 1) return;
   const uint64_t a = node_admin(nodes[i]);
@@ -62,6 +64,7 @@ __global__ void k_refit_climb(Node *nodes, uint32_t numNodes, const uint32_t *__
                               const bq_box3f *__restrict__ boxes, const uint32_t *__restrict__ parent,
                               uint32_t *counter, uint32_t *__restrict__ err)
 {
+  griddep_wait();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= numNodes || i == 1) return;
   const uint64_t a = node_admin(nodes[i]);
@@ -110,10 +113,10 @@ __global__ void k_refit_climb(Node *nodes, uint32_t numNodes, const uint32_t *__
 inline void launch_refit(Node *nodes, uint32_t numNodes, const uint32_t *primIDs, uint32_t numPrims,
                          const bq_box3f *boxes, uint32_t *parent, uint32_t *counter, uint32_t *err, cudaStream_t s)
 {
-  k_refit_init<<<div_up(numNodes, 256), 256, 0, s>>>(numNodes, parent, counter, err);
-  k_refit_parents<<<div_up(numNodes, 256), 256, 0, s>>>(nodes, numNodes, parent, err);
-  k_refit_climb<<<div_up(numNodes, 128), 128, 0, s>>>(nodes, numNodes, primIDs, numPrims, boxes, parent, counter,
-                                                      err);
+  launch_pdl(k_refit_init, dim3(div_up(numNodes, 256)), dim3(256), 0, s, numNodes, parent, counter, err);
+  launch_pdl(k_refit_parents, dim3(div_up(numNodes, 256)), dim3(256), 0, s, nodes, numNodes, parent, err);
+  launch_pdl(k_refit_climb, dim3(div_up(numNodes, 128)), dim3(128), 0, s, nodes, numNodes, primIDs, numPrims, boxes,
+             parent, counter, err);
 }
 
 } // namespace

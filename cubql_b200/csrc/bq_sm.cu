@@ -173,6 +173,7 @@ __device__ __forceinline__ void child_pair(const SmNode &nd, uint32_t m, const S
 // ------------------------------------------------------------------
 __global__ void k_sm_valid(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t *__restrict__ valid)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float2 a = *reinterpret_cast<const float2 *>(boxes + i);
@@ -187,6 +188,7 @@ __global__ void __launch_bounds__(256) k_sm_init(const bq_box3f *__restrict__ bo
                                                  float4 *__restrict__ pc, uint32_t *__restrict__ primIDs,
                                                  int32_t *rootLoHi)
 {
+  griddep_wait();
   const uint32_t nv = *nvPtr;
   int32_t lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -249,9 +251,11 @@ __device__ __forceinline__ SmTileInfo tile_info(const SmNode *__restrict__ nodes
 __global__ void k_sm_tiles(const SmNode *__restrict__ nodes, SmCtl *ctl, int cur, uint32_t cap,
                            uint32_t *__restrict__ tileCount)
 {
+  griddep_wait();
   const uint32_t K = ctl->bigCount[cur];
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k == 0 && K > cap) atomicOr(&ctl->err, DEV_ERR_RANGE);
+  if (k == 0) ctl->bigCount[cur ^ 1] = 0;  // the list this level's k_sm_classify fills (last read a level ago)
   if (k >= K || k >= cap) return;
   tileCount[k] = (nodes[k].e - nodes[k].b + SM_TILE - 1) / SM_TILE;
 }
@@ -262,6 +266,7 @@ __global__ void __launch_bounds__(SM_SCAN_THREADS) k_sm_tiles_scan(const SmNode 
                                                                    int cur, uint32_t cap, uint32_t maxTiles,
                                                                    uint32_t *__restrict__ first)
 {
+  griddep_wait();
   extern __shared__ uint32_t sVal[];  // cap entries
   __shared__ uint32_t sWarp[33];
   uint32_t K = ctl->bigCount[cur];
@@ -269,6 +274,7 @@ __global__ void __launch_bounds__(SM_SCAN_THREADS) k_sm_tiles_scan(const SmNode 
     if (threadIdx.x == 0) atomicOr(&ctl->err, DEV_ERR_RANGE);
     K = cap;
   }
+  if (threadIdx.x == 0) ctl->bigCount[cur ^ 1] = 0;  // the list this level's k_sm_classify fills (last read a level ago)
   for (uint32_t k = threadIdx.x; k < K; k += blockDim.x) sVal[k] = (nodes[k].e - nodes[k].b + SM_TILE - 1) / SM_TILE;
   __syncthreads();
   const uint32_t T = block_scan_smem(sVal, K, sWarp);
@@ -285,6 +291,7 @@ __global__ void __launch_bounds__(SM_BLOCK) k_sm_count(const SmNode *__restrict_
                                                        uint32_t maxTiles, const float4 *__restrict__ buf0,
                                                        const float4 *__restrict__ buf1, uint32_t *__restrict__ tileRight)
 {
+  griddep_wait();
   __shared__ uint32_t sCnt[SM_BLOCK / 32];
   const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -318,6 +325,7 @@ __global__ void k_sm_children(const SmNode *__restrict__ nodes, const SmCtl *ctl
                               const uint32_t *__restrict__ first, const uint32_t *__restrict__ rightScan,
                               Node *__restrict__ out, uint32_t *__restrict__ used, SmNode *__restrict__ next)
 {
+  griddep_wait();
   const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K || k >= cap) return;
@@ -343,6 +351,7 @@ __global__ void __launch_bounds__(SM_SCAN_THREADS) k_sm_scan_children(const SmNo
                                                                       uint32_t *__restrict__ used,
                                                                       SmNode *__restrict__ next)
 {
+  griddep_wait();
   extern __shared__ uint32_t sScan[];  // numTiles + 1 entries
   __shared__ uint32_t sWarp[33];
   const uint32_t K = min(ctl->bigCount[cur], cap), T = ctl->numTiles;
@@ -462,6 +471,7 @@ __global__ void __launch_bounds__(SM_BLOCK, 4) k_sm_scatter(const SmNode *__rest
                                                          const uint32_t *__restrict__ rightScan, float4 *buf0,
                                                          float4 *buf1, SmNode *next)
 {
+  griddep_wait();
   __shared__ uint32_t sWarp[SM_SCAT_GROUP * SM_BLOCK / 32];
   __shared__ int32_t sRed[12][SM_BLOCK / 32];
   const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
@@ -632,6 +642,7 @@ __global__ void __launch_bounds__(SMW_BLOCK) k_sm_warp(const SmNode *__restrict_
                                                        int thr, float4 *buf0, float4 *buf1, Node *__restrict__ out,
                                                        uint32_t *__restrict__ primIDs, uint32_t *__restrict__ used)
 {
+  griddep_wait();
   __shared__ SmNode sStack[SMW_WARPS][SMW_STACK];
   __shared__ float4 sX[SMW_WARPS][32];
   const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
@@ -651,6 +662,7 @@ __global__ void k_sm_classify(const SmNode *__restrict__ next, SmCtl *ctl, int c
                               uint32_t warpMax, SmNode *__restrict__ bigNext, SmNode *__restrict__ tasks,
                               uint32_t taskCap)
 {
+  griddep_wait();
   const uint32_t K = min(ctl->bigCount[cur], cap);
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= 2 * K) return;
@@ -681,6 +693,7 @@ __device__ __forceinline__ Node sm_remap(const Node &c, const uint32_t *__restri
 __global__ void k_sm_compact(const Node *__restrict__ full, const uint32_t *__restrict__ used,
                              const uint32_t *__restrict__ rank, uint32_t nv, Node *__restrict__ out)
 {
+  griddep_wait();
   const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m == 0) {
     out[0] = sm_remap(full[0], rank);
@@ -727,10 +740,10 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     return fail(cuda_error(ce, "spatial median set-up"));
   {
     ProfScope ps("sm.setup", al.s, 5);
-    k_sm_valid<<<div_up(n, 256), 256, 0, al.s>>>(boxes, n, valid);
+    launch_pdl(k_sm_valid, dim3(div_up(n, 256)), dim3(256), 0, al.s, boxes, n, valid);
     if ((s = exclusive_scan_u32(valid, vpos, n, nullptr, ctl, al)) != BQ_OK) return fail(s);
-    k_sm_init<<<std::min(div_up(n, 256), num_sms() * 8), 256, 0, al.s>>>(boxes, n, vpos, ctl, buf0, primIDs,
-                                                                       (int32_t *)(ctl + 2));
+    launch_pdl(k_sm_init, dim3(std::min(div_up(n, 256), num_sms() * 8)), dim3(256), 0, al.s, boxes, n, vpos, ctl,
+               buf0, primIDs, (int32_t *)(ctl + 2));
   }
   int32_t hctl[8];
   if ((ce = cudaMemcpyAsync(hctl, ctl, 32, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
@@ -794,7 +807,8 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   }
   auto warp_phase = [&]() -> int {  // every waiting subtree, then an empty task list
     ProfScope ps("sm.warps", al.s);
-    k_sm_warp<<<warpGrid, SMW_BLOCK, 0, al.s>>>(tasks, sc, taskCap, thr, buf0, buf1, full, primIDs, used);
+    launch_pdl(k_sm_warp, dim3(warpGrid), dim3(SMW_BLOCK), 0, al.s, tasks, sc, taskCap, thr, buf0, buf1, full,
+               primIDs, used);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemsetAsync(&sc->taskCount, 0, 2 * sizeof(uint32_t), al.s);  // taskCount, grab
     return e == cudaSuccess ? BQ_OK : cuda_error(e, "k_sm_warp");
@@ -804,31 +818,29 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     {
       ProfScope ps("sm.level", al.s, fused ? 5 : 11);
       if (fused) {
-        k_sm_tiles_scan<<<1, SM_SCAN_THREADS, sizeof(uint32_t) * cap, al.s>>>(bigList[cur], sc, cur, cap, maxTiles,
-                                                                            first);
+        launch_pdl(k_sm_tiles_scan, dim3(1), dim3(SM_SCAN_THREADS), sizeof(uint32_t) * cap, al.s, bigList[cur], sc,
+                   cur, cap, maxTiles, first);
       } else {
-        k_sm_tiles<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, tileCount);
+        launch_pdl(k_sm_tiles, dim3(div_up(cap, 128)), dim3(128), 0, al.s, bigList[cur], sc, cur, cap, tileCount);
         if ((s = exclusive_scan_u32(tileCount, first, cap, &sc->bigCount[cur], &sc->numTiles, al)) != BQ_OK)
           return fail(s);
       }
-      k_sm_count<<<levelGrid, SM_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, buf0, buf1, tileRight);
+      launch_pdl(k_sm_count, dim3(levelGrid), dim3(SM_BLOCK), 0, al.s, bigList[cur], first, sc, cur, maxTiles, buf0,
+                 buf1, tileRight);
       if (fused) {
-        k_sm_scan_children<<<1, SM_SCAN_THREADS, sizeof(uint32_t) * maxTiles, al.s>>>(bigList[cur], sc, cur, cap,
-                                                                                     first, tileRight, full, used,
-                                                                                     next);
+        launch_pdl(k_sm_scan_children, dim3(1), dim3(SM_SCAN_THREADS), sizeof(uint32_t) * maxTiles, al.s,
+                   bigList[cur], sc, cur, cap, first, tileRight, full, used, next);
       } else {
         if ((s = exclusive_scan_u32(tileRight, tileRight, maxTiles, &sc->scanLen, nullptr, al)) != BQ_OK)
           return fail(s);
-        k_sm_children<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, first, tileRight, full, used,
-                                                         next);
+        launch_pdl(k_sm_children, dim3(div_up(cap, 128)), dim3(128), 0, al.s, bigList[cur], sc, cur, cap, first,
+                   tileRight, full, used, next);
       }
-      k_sm_scatter<<<levelGrid, SM_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, tileRight, buf0, buf1,
-                                                      next);
-      k_sm_classify<<<div_up(2ull * cap, 128), 128, 0, al.s>>>(next, sc, cur, cap, thr, warpMax, bigList[cur ^ 1], tasks,
-                                                               taskCap);
-      if ((ce = cudaMemsetAsync(&sc->bigCount[cur], 0, sizeof(uint32_t), al.s)) != cudaSuccess ||
-          (ce = cudaGetLastError()) != cudaSuccess)
-        return fail(cuda_error(ce, "spatial median level"));
+      launch_pdl(k_sm_scatter, dim3(levelGrid), dim3(SM_BLOCK), 0, al.s, bigList[cur], first, sc, cur, maxTiles,
+                 tileRight, buf0, buf1, next);
+      launch_pdl(k_sm_classify, dim3(div_up(2ull * cap, 128)), dim3(128), 0, al.s, next, sc, cur, cap, thr, warpMax,
+                 bigList[cur ^ 1], tasks, taskCap);
+      if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "spatial median level"));
     }
     cur ^= 1;
     if (level + 1 < nextCheck) continue;
@@ -861,7 +873,7 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   if ((s = al.get(&nodes, numNodes)) != BQ_OK) return fail(s);
   {
     ProfScope ps("sm.compact", al.s);
-    k_sm_compact<<<div_up(nv, 256), 256, 0, al.s>>>(full, used, rank, nv, nodes);
+    launch_pdl(k_sm_compact, dim3(div_up(nv, 256)), dim3(256), 0, al.s, full, used, rank, nv, nodes);
   }
   bvh->nodes = reinterpret_cast<bq_node3f *>(nodes);
   bvh->numNodes = numNodes;
