@@ -64,6 +64,7 @@ struct SegQuant {
 
 __global__ void k_seg_bounds_init(int32_t *segLoHi, uint32_t numSegs)
 {
+  griddep_wait();
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= numSegs) return;
   for (int d = 0; d < 3; d++) {
@@ -78,6 +79,7 @@ __global__ void __launch_bounds__(256) k_seg_bounds(const bq_box3f *__restrict__
                                                     const uint32_t *__restrict__ off, uint32_t numSegs,
                                                     int32_t *segLoHi)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < n;
   uint32_t s = valid ? seg_of(off, numSegs, i) : 0xffffffffu;
@@ -111,6 +113,7 @@ __global__ void __launch_bounds__(256) k_seg_bounds(const bq_box3f *__restrict__
 
 __global__ void k_seg_quant(const int32_t *__restrict__ segLoHi, uint32_t numSegs, SegQuant *__restrict__ q)
 {
+  griddep_wait();
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= numSegs) return;
   float lo[3], sz[3];
@@ -131,6 +134,7 @@ __global__ void __launch_bounds__(256) k_seg_keygen(const bq_box3f *__restrict__
                                                     const SegQuant *__restrict__ quant, uint64_t *__restrict__ keys,
                                                     uint32_t *__restrict__ ids, uint32_t *__restrict__ hist)
 {
+  griddep_wait();
   __shared__ uint32_t sh[8 * 256];
   for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) sh[j] = 0;
   __syncthreads();
@@ -155,6 +159,7 @@ __global__ void __launch_bounds__(256) k_seg_keygen(const bq_box3f *__restrict__
 __global__ void k_seg_ids(const uint32_t *__restrict__ idsSorted, uint32_t n, const uint32_t *__restrict__ off,
                           uint32_t numSegs, uint32_t *__restrict__ segKey, uint32_t *__restrict__ pos)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   segKey[i] = seg_of(off, numSegs, idsSorted[i]);
@@ -165,6 +170,7 @@ __global__ void k_seg_gather(const uint32_t *__restrict__ pos, const uint64_t *_
                              const uint32_t *__restrict__ idsMorton, uint32_t n, uint64_t *__restrict__ keys,
                              uint32_t *__restrict__ ids)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t p = pos[i];
@@ -197,6 +203,7 @@ __device__ __forceinline__ uint8_t seg_split_level(const uint64_t *__restrict__ 
 __global__ void k_seg_delta(const uint64_t *__restrict__ keys, uint32_t n, const uint32_t *__restrict__ off,
                             uint32_t numSegs, uint8_t *__restrict__ delta)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t s = seg_of(off, numSegs, i);
@@ -208,6 +215,7 @@ __global__ void k_seg_delta(const uint64_t *__restrict__ keys, uint32_t n, const
 __global__ void k_seg_kept(const uint2 *__restrict__ ranges, uint32_t n, const uint32_t *__restrict__ off,
                            uint32_t numSegs, int thr, uint32_t *__restrict__ kept)
 {
+  griddep_wait();
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   uint32_t k = 0;
@@ -225,6 +233,7 @@ __global__ void k_seg_collapse(const Node *__restrict__ full, const uint2 *__res
                                const uint32_t *__restrict__ kept, const uint32_t *__restrict__ rank, uint32_t n,
                                const uint32_t *__restrict__ off, uint32_t numSegs, int thr, Node *__restrict__ out)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const uint32_t sg = seg_of(off, numSegs, t);
@@ -269,6 +278,7 @@ __global__ void k_seg_desc(const uint32_t *__restrict__ off, uint32_t numSegs, u
                            const uint32_t *__restrict__ rank, bq_node3f *nodes, uint32_t *primIDs,
                            bq_bvh3f *__restrict__ bvhs)
 {
+  griddep_wait();
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= numSegs) return;
   const uint32_t b0 = off[s], e0 = off[s + 1], nv = e0 - b0;
@@ -293,6 +303,7 @@ __global__ void k_seg_query_keys(const bq_bvh3f *__restrict__ bvhs, const float 
                                  const uint32_t *__restrict__ qoff, uint32_t numSegs, uint64_t *__restrict__ keys,
                                  uint32_t *__restrict__ idx)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const uint32_t s = seg_of(qoff, numSegs, t);
@@ -343,6 +354,7 @@ __global__ void __launch_bounds__(128) k_seg_knn(const bq_bvh3f *__restrict__ bv
                                                  int32_t *__restrict__ numFound, uint32_t *__restrict__ ovfList,
                                                  uint32_t *ovfCount)
 {
+  griddep_wait();
   const int lane = threadIdx.x & 31;
   while (true) {
     uint32_t base = 0;
@@ -396,6 +408,7 @@ __global__ void k_seg_knn_deep(const bq_bvh3f *__restrict__ bvhs, const uint32_t
                                int32_t *__restrict__ numFound, const uint32_t *ovfList, const uint32_t *ovfCount,
                                StackEntry *stacks, int cap, uint32_t *err)
 {
+  griddep_wait();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t cnt = *ovfCount;
   for (uint32_t w = tid; w < cnt; w += gridDim.x * blockDim.x) {
@@ -444,12 +457,12 @@ int launch_seg_knn(const bq_bvh3f *bvhs, const uint32_t *poff, const float *poin
   const int grid = std::max(1, std::min(num_sms() * std::max(perSm, 1), div_up(nq, block)));
   {
     ProfScope ps("batch.knn", s);
-    k_seg_knn<K, TIE, STACK><<<grid, block, 0, s>>>(bvhs, poff, points, queries, skeys, order, nq, k, maxSqr, chunk,
-                                                    workCtr, ids, d, nf, ovfList, ovfCount);
+    launch_pdl(k_seg_knn<K, TIE, STACK>, dim3(grid), dim3(block), 0, s, bvhs, poff, points, queries, skeys, order, nq,
+               k, maxSqr, chunk, workCtr, ids, d, nf, ovfList, ovfCount);
   }
   ProfScope ps("batch.deep", s);
-  k_seg_knn_deep<K, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(bvhs, poff, points, queries, skeys, order, k, maxSqr,
-                                                             ids, d, nf, ovfList, ovfCount, deep, DEEP_STACK, err);
+  launch_pdl(k_seg_knn_deep<K, TIE>, dim3(DEEP_THREADS / 128), dim3(128), 0, s, bvhs, poff, points, queries, skeys,
+             order, k, maxSqr, ids, d, nf, ovfList, ovfCount, deep, DEEP_STACK, err);
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }
@@ -496,7 +509,8 @@ int batched_build_morton63(const bq_box3f *boxes, const uint32_t *off, uint32_t 
   BQ_TRY(tmp.get(&hist, 8 * 256));
   BQ_TRY(tmp.get(&err, 1));
   if (n == 0) {
-    k_seg_desc<<<div_up(numSegs, 128), 128, 0, al.s>>>(off, numSegs, n, thr, nullptr, nodesOut, primIDs, bvhs);
+    launch_pdl(k_seg_desc, dim3(div_up(numSegs, 128)), dim3(128), 0, al.s, off, numSegs, n, thr, nullptr, nodesOut,
+               primIDs, bvhs);
     BQ_CUDA(cudaGetLastError());
     return BQ_OK;
   }
@@ -517,13 +531,14 @@ int batched_build_morton63(const bq_box3f *boxes, const uint32_t *off, uint32_t 
   BQ_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * 8 * 256, al.s));
   {
     ProfScope ps("batch.bounds", al.s, 3);
-    k_seg_bounds_init<<<div_up(numSegs, 128), 128, 0, al.s>>>(segLoHi, numSegs);
-    k_seg_bounds<<<div_up(n, 256), 256, 0, al.s>>>(boxes, n, off, numSegs, segLoHi);
-    k_seg_quant<<<div_up(numSegs, 128), 128, 0, al.s>>>(segLoHi, numSegs, quant);
+    launch_pdl(k_seg_bounds_init, dim3(div_up(numSegs, 128)), dim3(128), 0, al.s, segLoHi, numSegs);
+    launch_pdl(k_seg_bounds, dim3(div_up(n, 256)), dim3(256), 0, al.s, boxes, n, off, numSegs, segLoHi);
+    launch_pdl(k_seg_quant, dim3(div_up(numSegs, 128)), dim3(128), 0, al.s, segLoHi, numSegs, quant);
   }
   {
     ProfScope ps("batch.keygen", al.s);
-    k_seg_keygen<<<div_up(n, 256), 256, 0, al.s>>>(boxes, n, off, numSegs, quant, keys[0], ids[0], hist);
+    launch_pdl(k_seg_keygen, dim3(div_up(n, 256)), dim3(256), 0, al.s, boxes, n, off, numSegs, quant, keys[0], ids[0],
+               hist);
   }
   BQ_CUDA(cudaGetLastError());
   int sel = 0;
@@ -534,17 +549,17 @@ int batched_build_morton63(const bq_box3f *boxes, const uint32_t *off, uint32_t 
   while (segBits < 32 && (1ull << segBits) < numSegs) segBits++;
   {
     ProfScope ps("batch.segkeys", al.s);
-    k_seg_ids<<<div_up(n, 256), 256, 0, al.s>>>(mi, n, off, numSegs, segKey[0], pos[0]);
+    launch_pdl(k_seg_ids, dim3(div_up(n, 256)), dim3(256), 0, al.s, mi, n, off, numSegs, segKey[0], pos[0]);
   }
   int sel2 = 0;
   BQ_TRY(onesweep_sort_u32(segKey, pos, n, nullptr, 0, segBits, nullptr, &sel2, dErr, al));
   {
     ProfScope ps("batch.gather", al.s);
-    k_seg_gather<<<div_up(n, 256), 256, 0, al.s>>>(pos[sel2], mk, mi, n, fkeys, fids);
+    launch_pdl(k_seg_gather, dim3(div_up(n, 256)), dim3(256), 0, al.s, pos[sel2], mk, mi, n, fkeys, fids);
   }
   {
     ProfScope ps("batch.delta", al.s);
-    k_seg_delta<<<div_up(n, 256), 256, 0, al.s>>>(fkeys, n, off, numSegs, delta);
+    launch_pdl(k_seg_delta, dim3(div_up(n, 256)), dim3(256), 0, al.s, fkeys, n, off, numSegs, delta);
   }
   uint2 *pending = nullptr;
   BQ_TRY(tmp.get(&pending, 2ull * div_up(n, AGG_CHUNK)));
@@ -562,12 +577,14 @@ int batched_build_morton63(const bq_box3f *boxes, const uint32_t *off, uint32_t 
     ag.ranges = ranges;
     BQ_TRY(agglomerate<true>(ag, n, al.s, "batch.agg_local", "batch.agg_global"));
     ProfScope ps("batch.collapse", al.s, 6);  // kept, memset, scan (3), collapse
-    k_seg_kept<<<div_up(n, 256), 256, 0, al.s>>>(ranges, n, off, numSegs, thr, kept);
+    launch_pdl(k_seg_kept, dim3(div_up(n, 256)), dim3(256), 0, al.s, ranges, n, off, numSegs, thr, kept);
     BQ_CUDA(cudaMemsetAsync(kept + n, 0, 4, al.s));
     BQ_TRY(exclusive_scan_u32(kept, rank, n + 1, nullptr, nullptr, al));
-    k_seg_collapse<<<div_up(n, 256), 256, 0, al.s>>>(full, ranges, kept, rank, n, off, numSegs, thr, (Node *)nodesOut);
+    launch_pdl(k_seg_collapse, dim3(div_up(n, 256)), dim3(256), 0, al.s, full, ranges, kept, rank, n, off, numSegs,
+               thr, (Node *)nodesOut);
   }
-  k_seg_desc<<<div_up(numSegs, 128), 128, 0, al.s>>>(off, numSegs, n, thr, rank, nodesOut, primIDs, bvhs);
+  launch_pdl(k_seg_desc, dim3(div_up(numSegs, 128)), dim3(128), 0, al.s, off, numSegs, n, thr, rank, nodesOut,
+             primIDs, bvhs);
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }
@@ -596,7 +613,8 @@ int batched_knn(const bq_bvh3f *bvhs, const uint32_t *poff, const float *points,
   uint32_t *dErr = errOut ? errOut : ctl + 2;
   {
     ProfScope ps("batch.query_keys", al.s);
-    k_seg_query_keys<<<div_up(nq, 256), 256, 0, al.s>>>(bvhs, queries, nq, qoff, numSegs, keys[0], idx[0]);
+    launch_pdl(k_seg_query_keys, dim3(div_up(nq, 256)), dim3(256), 0, al.s, bvhs, queries, nq, qoff, numSegs, keys[0],
+               idx[0]);
   }
   int segBits = 1;
   while (segBits < 32 && (1ull << segBits) < numSegs) segBits++;

@@ -48,6 +48,7 @@ __global__ void k_brefit_parents(const Node *__restrict__ nodes, uint32_t numSlo
                                  const uint32_t *__restrict__ off, uint32_t numSegs, uint32_t *__restrict__ parent,
                                  uint32_t *__restrict__ counter)
 {
+  griddep_wait();
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= numSlots) return;
   counter[j] = 0;
@@ -69,6 +70,7 @@ __global__ void k_brefit_climb(Node *nodes, uint32_t numSlots, const bq_bvh3f *_
                                const bq_box3f *__restrict__ boxes, const uint32_t *__restrict__ parent,
                                uint32_t *counter)
 {
+  griddep_wait();
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= numSlots) return;
   uint32_t s, local;
@@ -224,6 +226,7 @@ __global__ void __launch_bounds__(128) k_btri(const bq_bvh3f *__restrict__ bvhs,
                                               float *__restrict__ outP, uint32_t *__restrict__ ovfList,
                                               uint32_t *ovfCount)
 {
+  griddep_wait();
   const uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x;
   if (qi >= nq) return;
   const uint32_t s = seg_find(qoff, numSegs, qi);
@@ -240,6 +243,7 @@ __global__ void k_btri_deep(const bq_bvh3f *__restrict__ bvhs, const uint32_t *_
                             int32_t *__restrict__ outIds, float *__restrict__ outD, float *__restrict__ outP,
                             const uint32_t *ovfList, const uint32_t *ovfCount, StackEntry *stacks, uint32_t *err)
 {
+  griddep_wait();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t cnt = *ovfCount;
   for (uint32_t w = tid; w < cnt; w += gridDim.x * blockDim.x) {
@@ -266,10 +270,10 @@ int batched_refit(const bq_bvh3f *bvhs, const uint32_t *off, uint32_t numSegs, u
   BQ_TRY(tmp.get(&parent, slots));
   BQ_TRY(tmp.get(&counter, slots));
   ProfScope ps("batch.refit", al.s, 2);
-  k_brefit_parents<<<div_up(slots, 256), 256, 0, al.s>>>((const Node *)nodes, slots, bvhs, off, numSegs, parent,
-                                                         counter);
-  k_brefit_climb<<<div_up(slots, 128), 128, 0, al.s>>>((Node *)nodes, slots, bvhs, off, numSegs, primIDs, boxes,
-                                                       parent, counter);
+  launch_pdl(k_brefit_parents, dim3(div_up(slots, 256)), dim3(256), 0, al.s, (const Node *)nodes, slots, bvhs, off,
+             numSegs, parent, counter);
+  launch_pdl(k_brefit_climb, dim3(div_up(slots, 128)), dim3(128), 0, al.s, (Node *)nodes, slots, bvhs, off, numSegs,
+             primIDs, boxes, parent, counter);
   BQ_CUDA(cudaGetLastError());
   return BQ_OK;
 }

@@ -153,6 +153,7 @@ __global__ void __launch_bounds__(128) k_box_count(const Node *__restrict__ node
                                                    const bq_box3f *__restrict__ queryBoxes, uint32_t nq,
                                                    uint32_t *__restrict__ counts, uint32_t *err)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nq) return;
   float q[6];
@@ -173,6 +174,7 @@ __global__ void __launch_bounds__(128) k_box_fill(const Node *__restrict__ nodes
                                                   const uint32_t *__restrict__ offsets, uint64_t capacity,
                                                   int32_t *__restrict__ ids, uint32_t *err)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nq) return;
   float q[6];
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(128) k_box_fill(const Node *__restrict__ nodes
 __global__ void k_box_query_keys(const float *__restrict__ rootBox, const bq_box3f *__restrict__ qb, uint32_t nq,
                                  uint32_t *__restrict__ keys, uint32_t *__restrict__ idx)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const float lx = __ldg(rootBox), ly = __ldg(rootBox + 1), lz = __ldg(rootBox + 2);
@@ -222,6 +225,7 @@ __global__ void __launch_bounds__(128) k_box_slab(const Node *__restrict__ nodes
                                                   int32_t *__restrict__ slab, uint32_t *__restrict__ counts,
                                                   uint32_t *__restrict__ ovf, uint32_t *err)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const uint32_t i = order ? __ldg(order + t) : t;
@@ -255,6 +259,7 @@ __global__ void __launch_bounds__(128) k_box_gather(const Node *__restrict__ nod
                                                     const uint32_t *__restrict__ offsets, uint64_t capacity,
                                                     int32_t *__restrict__ ids, uint32_t copyBlocks, uint32_t *err)
 {
+  griddep_wait();
   if (blockIdx.x < copyBlocks) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)copyBlocks * (blockDim.x / 32);
@@ -296,7 +301,8 @@ int count_impl(const Node *nodes, const uint32_t *primIDs, const bq_box3f *boxes
   BQ_CUDA(cudaMemsetAsync(err, 0, 4, al.s));
   {
     ProfScope ps("boxquery.count", al.s);
-    k_box_count<W><<<div_up(nq, 128), 128, 0, al.s>>>(nodes, primIDs, boxes, queryBoxes, nq, counts, err);
+    launch_pdl(k_box_count<W>, dim3(div_up(nq, 128)), dim3(128), 0, al.s, nodes, primIDs, boxes, queryBoxes, nq,
+               counts, err);
   }
   BQ_CUDA(cudaGetLastError());
   uint32_t herr = 0;
@@ -316,8 +322,8 @@ int fill_impl(const Node *nodes, const uint32_t *primIDs, const bq_box3f *boxes,
   BQ_CUDA(cudaMemsetAsync(err, 0, 4, al.s));
   {
     ProfScope ps("boxquery.fill", al.s);
-    k_box_fill<W><<<div_up(nq, 128), 128, 0, al.s>>>(nodes, primIDs, boxes, queryBoxes, nq, offsets, capacity, ids,
-                                                      err);
+    launch_pdl(k_box_fill<W>, dim3(div_up(nq, 128)), dim3(128), 0, al.s, nodes, primIDs, boxes, queryBoxes, nq,
+               offsets, capacity, ids, err);
   }
   BQ_CUDA(cudaGetLastError());
   uint32_t herr = 0;
@@ -340,7 +346,7 @@ int box_query_order(const Node *nodes, const bq_box3f *queryBoxes, uint32_t nq, 
   if (W != 0) {
     float *rb = nullptr;
     BQ_TRY(tmp.get(&rb, 6));
-    k_wide_root_box<W == 0 ? 2 : W><<<1, 32, 0, al.s>>>(nodes, rb);
+    launch_pdl(k_wide_root_box<W == 0 ? 2 : W>, dim3(1), dim3(32), 0, al.s, nodes, rb);
     rootBox = rb;
   }
   uint32_t *keys[2], *idx[2];
@@ -350,7 +356,7 @@ int box_query_order(const Node *nodes, const bq_box3f *queryBoxes, uint32_t nq, 
   BQ_TRY(tmp.get(&idx[1], nq));
   {
     ProfScope ps("boxquery.keys", al.s);
-    k_box_query_keys<<<div_up(nq, 256), 256, 0, al.s>>>(rootBox, queryBoxes, nq, keys[0], idx[0]);
+    launch_pdl(k_box_query_keys, dim3(div_up(nq, 256)), dim3(256), 0, al.s, rootBox, queryBoxes, nq, keys[0], idx[0]);
   }
   BQ_CUDA(cudaGetLastError());
   int sel = 0;
@@ -375,8 +381,8 @@ int slab_impl(const Node *nodes, const uint32_t *primIDs, const bq_box3f *boxes,
   BQ_TRY(box_query_order<W>(nodes, queryBoxes, nq, err, tmp, al, &order));
   {
     ProfScope ps("boxquery.slab", al.s);
-    k_box_slab<W><<<div_up(nq, 128), 128, 0, al.s>>>(nodes, primIDs, boxes, queryBoxes, nq, order, slabCap, slab,
-                                                      counts, ovf, err);
+    launch_pdl(k_box_slab<W>, dim3(div_up(nq, 128)), dim3(128), 0, al.s, nodes, primIDs, boxes, queryBoxes, nq, order,
+               slabCap, slab, counts, ovf, err);
   }
   BQ_CUDA(cudaGetLastError());
   uint32_t herr = 0;
@@ -402,8 +408,8 @@ int gather_impl(const Node *nodes, const uint32_t *primIDs, const bq_box3f *boxe
   const uint64_t blocks = copyBlocks + (uint64_t)div_up(maxOvf, 128);
   {
     ProfScope ps("boxquery.gather", al.s);
-    k_box_gather<W><<<(unsigned)blocks, 128, 0, al.s>>>(nodes, primIDs, boxes, queryBoxes, nq, slabCap, slab, counts,
-                                                         ovf, offsets, capacity, ids, copyBlocks, err);
+    launch_pdl(k_box_gather<W>, dim3((unsigned)blocks), dim3(128), 0, al.s, nodes, primIDs, boxes, queryBoxes, nq,
+               slabCap, slab, counts, ovf, offsets, capacity, ids, copyBlocks, err);
   }
   BQ_CUDA(cudaGetLastError());
   uint32_t herr = 0;

@@ -36,6 +36,7 @@ constexpr int KNN_SMEM_STACK = 0;
 __global__ void k_query_keys(const float *__restrict__ rootBox, const float *__restrict__ queries, uint32_t nq,
                              uint32_t *__restrict__ keys, uint32_t *__restrict__ idx)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const float lx = __ldg(rootBox), ly = __ldg(rootBox + 1), lz = __ldg(rootBox + 2);
@@ -70,6 +71,7 @@ __global__ void __launch_bounds__(128) k_closest(const Node *__restrict__ nodes,
                                                  int32_t *__restrict__ outIds, float *__restrict__ outD,
                                                  uint32_t *__restrict__ ovfList, uint32_t *ovfCount, CpExclude ex)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const uint32_t qi = order ? __ldg(order + t) : t;
@@ -85,6 +87,7 @@ __global__ void k_closest_deep(const Node *__restrict__ nodes, const uint32_t *_
                                int32_t *__restrict__ outIds, float *__restrict__ outD, const uint32_t *ovfList,
                                const uint32_t *ovfCount, StackEntry *stacks, uint32_t *err, CpExclude ex)
 {
+  griddep_wait();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t cnt = *ovfCount;
   for (uint32_t w = tid; w < cnt; w += gridDim.x * blockDim.x) {
@@ -161,6 +164,7 @@ __global__ void __launch_bounds__(128) k_knn(const Node *__restrict__ nodes, con
                                              int32_t *__restrict__ numFound, uint32_t *__restrict__ ovfList,
                                              uint32_t *ovfCount)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const uint32_t qi = order ? __ldg(order + t) : t;
@@ -176,6 +180,7 @@ __global__ void k_knn_deep(const Node *__restrict__ nodes, const uint32_t *__res
                            int32_t *__restrict__ outIds, float *__restrict__ outD, int32_t *__restrict__ numFound,
                            const uint32_t *ovfList, const uint32_t *ovfCount, StackEntry *stacks, uint32_t *err)
 {
+  griddep_wait();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t cnt = *ovfCount;
   for (uint32_t w = tid; w < cnt; w += gridDim.x * blockDim.x) {
@@ -274,6 +279,7 @@ __global__ void __launch_bounds__(128) k_knn_group(const Node *__restrict__ node
                                                    float *__restrict__ outD, int32_t *__restrict__ numFound,
                                                    uint32_t *__restrict__ ovfList, uint32_t *ovfCount)
 {
+  griddep_wait();
   const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t t = gt / G;  // the group's query slot (whole groups leave together)
   if (t >= nq) return;
@@ -315,23 +321,23 @@ void launch_knn_group(const bq_bvh3f *bvh, const float *points, const float *que
   const Node *nodes = (const Node *)bvh->nodes;
   {
     ProfScope ps("query.knn_group", s);
-    k_knn_group<G, TIE, STACK><<<div_up((uint64_t)nq * G, block), block, 0, s>>>(
-        nodes, bvh->primIDs, points, queries, qs.order, nq, k, maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount);
+    launch_pdl(k_knn_group<G, TIE, STACK>, dim3(div_up((uint64_t)nq * G, block)), dim3(block), 0, s, nodes,
+               bvh->primIDs, points, queries, qs.order, nq, k, maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount);
   }
   // overflowing queries: the per-thread deep-stack kernel (same answers)
   ProfScope ps("query.deep", s);
   if (k <= 4)
-    k_knn_deep<4, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d,
-                                                          nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+    launch_pdl(k_knn_deep<4, TIE>, dim3(DEEP_THREADS / 128), dim3(128), 0, s, nodes, bvh->primIDs, points, queries, k,
+               maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
   else if (k <= 8)
-    k_knn_deep<8, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d,
-                                                          nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+    launch_pdl(k_knn_deep<8, TIE>, dim3(DEEP_THREADS / 128), dim3(128), 0, s, nodes, bvh->primIDs, points, queries, k,
+               maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
   else if (k <= 16)
-    k_knn_deep<16, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d,
-                                                           nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+    launch_pdl(k_knn_deep<16, TIE>, dim3(DEEP_THREADS / 128), dim3(128), 0, s, nodes, bvh->primIDs, points, queries,
+               k, maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
   else
-    k_knn_deep<32, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d,
-                                                           nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+    launch_pdl(k_knn_deep<32, TIE>, dim3(DEEP_THREADS / 128), dim3(128), 0, s, nodes, bvh->primIDs, points, queries,
+               k, maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
 }
 
 template <int TIE>
@@ -359,12 +365,12 @@ void launch_cp(const bq_bvh3f *bvh, const float *points, const float *queries, u
   const Node *nodes = (const Node *)bvh->nodes;
   {
     ProfScope ps("query.closest", s);
-    k_closest<TIE, STACK><<<div_up(nq, block), block, SMEM_STACK * sizeof(StackEntry) * block, s>>>(
-        nodes, bvh->primIDs, points, queries, qs.order, nq, maxSqr, ids, d, qs.ovfList, qs.ovfCount, ex);
+    launch_pdl(k_closest<TIE, STACK>, dim3(div_up(nq, block)), dim3(block), SMEM_STACK * sizeof(StackEntry) * block,
+               s, nodes, bvh->primIDs, points, queries, qs.order, nq, maxSqr, ids, d, qs.ovfList, qs.ovfCount, ex);
   }
   ProfScope ps("query.deep", s);
-  k_closest_deep<TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, maxSqr, ids, d,
-                                                         qs.ovfList, qs.ovfCount, qs.deep, qs.err, ex);
+  launch_pdl(k_closest_deep<TIE>, dim3(DEEP_THREADS / 128), dim3(128), 0, s, nodes, bvh->primIDs, points, queries,
+             maxSqr, ids, d, qs.ovfList, qs.ovfCount, qs.deep, qs.err, ex);
 }
 
 template <int K, int TIE, int STACK>
@@ -374,12 +380,13 @@ void launch_knn(const bq_bvh3f *bvh, const float *points, const float *queries, 
   const Node *nodes = (const Node *)bvh->nodes;
   {
     ProfScope ps("query.knn", s);
-    k_knn<K, TIE, STACK><<<div_up(nq, block), block, KNN_SMEM_STACK * sizeof(StackEntry) * block, s>>>(
-        nodes, bvh->primIDs, points, queries, qs.order, nq, k, maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount);
+    launch_pdl(k_knn<K, TIE, STACK>, dim3(div_up(nq, block)), dim3(block),
+               KNN_SMEM_STACK * sizeof(StackEntry) * block, s, nodes, bvh->primIDs, points, queries, qs.order, nq, k,
+               maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount);
   }
   ProfScope ps("query.deep", s);
-  k_knn_deep<K, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(nodes, bvh->primIDs, points, queries, k, maxSqr, ids, d, nf,
-                                                        qs.ovfList, qs.ovfCount, qs.deep, qs.err);
+  launch_pdl(k_knn_deep<K, TIE>, dim3(DEEP_THREADS / 128), dim3(128), 0, s, nodes, bvh->primIDs, points, queries, k,
+             maxSqr, ids, d, nf, qs.ovfList, qs.ovfCount, qs.deep, qs.err);
 }
 
 template <int K, int TIE>
@@ -416,6 +423,7 @@ __global__ void __launch_bounds__(128) k_visit_count(const Node *__restrict__ no
                                                      const float *__restrict__ queries, uint32_t nq, int k,
                                                      float maxSqr, unsigned long long *out)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   VisitCount vc;
   uint32_t prims = 0;
@@ -464,6 +472,7 @@ void launch_visit_count(const bq_bvh3f *bvh, const float *points, const float *q
 
 __global__ void k_fill_empty(uint32_t nq, int k, int32_t *ids, float *d, int32_t *numFound)
 {
+  griddep_wait();
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (uint64_t)nq * k) return;
   ids[t] = -1;
@@ -487,7 +496,7 @@ int prepare_queries(const float *rootBox, const float *queries, uint32_t nq, boo
     BQ_TRY(tmp.get(&idx[1], nq));
     {
       ProfScope ps("query.keys", al.s);
-      k_query_keys<<<div_up(nq, 256), 256, 0, al.s>>>(rootBox, queries, nq, keys[0], idx[0]);
+      launch_pdl(k_query_keys, dim3(div_up(nq, 256)), dim3(256), 0, al.s, rootBox, queries, nq, keys[0], idx[0]);
     }
     BQ_CUDA(cudaGetLastError());
     int sel = 0;
@@ -542,7 +551,7 @@ int closest_point(const bq_bvh3f *bvh, const float *points, const float *queries
   BQ_TRY(query_config(qcfg, c));
   if (nq == 0) return BQ_OK;
   if (bvh->numNodes == 0) {
-    k_fill_empty<<<div_up(nq, 256), 256, 0, al.s>>>(nq, 1, ids, d, nullptr);
+    launch_pdl(k_fill_empty, dim3(div_up(nq, 256)), dim3(256), 0, al.s, nq, 1, ids, d, nullptr);
     BQ_CUDA(cudaGetLastError());
     return BQ_OK;
   }
@@ -571,7 +580,7 @@ int knn(const bq_bvh3f *bvh, const float *points, const float *queries, uint32_t
   if (k < 1 || k > 64) return set_error(BQ_ERR_INVALID_ARGUMENT, "k must be in [1, 64]");
   if (nq == 0) return BQ_OK;
   if (bvh->numNodes == 0) {
-    k_fill_empty<<<div_up((uint64_t)nq * k, 256), 256, 0, al.s>>>(nq, k, ids, d, numFound);
+    launch_pdl(k_fill_empty, dim3(div_up((uint64_t)nq * k, 256)), dim3(256), 0, al.s, nq, k, ids, d, numFound);
     BQ_CUDA(cudaGetLastError());
     return BQ_OK;
   }

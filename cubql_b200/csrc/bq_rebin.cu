@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(256) k_rb_valid(const bq_box3f *__restrict__ b
                                                   uint32_t *__restrict__ valid,
                                                   int32_t *bounds /* lo xyz, hi xyz, encoded */)
 {
+  griddep_wait();
   int32_t lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const bq_box3f b = boxes[i];
@@ -105,6 +106,7 @@ __global__ void k_rb_keys(const bq_box3f *__restrict__ boxes, uint32_t n, const 
                           const uint32_t *__restrict__ vpos, const int32_t *__restrict__ bounds,
                           uint32_t *__restrict__ keys, uint32_t *__restrict__ ids)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !valid[i]) return;
   const Quant30 q = make_quant30(dec_f(bounds[0]), dec_f(bounds[1]), dec_f(bounds[2]), dec_f(bounds[3]),
@@ -116,6 +118,7 @@ __global__ void k_rb_keys(const bq_box3f *__restrict__ boxes, uint32_t n, const 
 
 __global__ void k_rb_levels0(const uint32_t *__restrict__ keys, const uint32_t *nvPtr, uint16_t *__restrict__ lev)
 {
+  griddep_wait();
   const uint32_t nv = *nvPtr;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
@@ -130,6 +133,7 @@ __global__ void k_rb_levels0(const uint32_t *__restrict__ keys, const uint32_t *
 // ------------------------------------------------------------------
 __global__ void k_rb_run_flags(const uint16_t *__restrict__ lev, const uint32_t *nvPtr, uint32_t *__restrict__ flag)
 {
+  griddep_wait();
   const uint32_t nv = *nvPtr;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
@@ -139,6 +143,7 @@ __global__ void k_rb_run_flags(const uint16_t *__restrict__ lev, const uint32_t 
 __global__ void k_rb_run_starts(const uint32_t *__restrict__ flag, const uint32_t *__restrict__ runIdx,
                                 const uint32_t *nvPtr, uint32_t *__restrict__ starts)
 {
+  griddep_wait();
   const uint32_t nv = *nvPtr;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
@@ -150,6 +155,7 @@ __global__ void k_rb_run_starts(const uint32_t *__restrict__ flag, const uint32_
 __global__ void k_rb_big(const uint32_t *__restrict__ starts, const uint32_t *numRunsPtr, uint32_t bigMin,
                          uint32_t *__restrict__ big, uint32_t *__restrict__ bigSize)
 {
+  griddep_wait();
   const uint32_t R = *numRunsPtr;
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= R) return;
@@ -169,6 +175,7 @@ __global__ void k_rb_jobs(const uint32_t *__restrict__ starts, const uint32_t *n
                           const uint32_t *__restrict__ bigOff, RebinJob *__restrict__ jobs,
                           uint32_t *__restrict__ jobOff)
 {
+  griddep_wait();
   const uint32_t R = *numRunsPtr;
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= R || !big[r]) return;
@@ -196,6 +203,7 @@ __device__ __forceinline__ uint32_t job_of(const uint32_t *__restrict__ jobOff, 
 __global__ void k_rb_domains(RebinJob *jobs, const uint32_t *__restrict__ jobOff, uint32_t numJobs,
                              uint32_t numSlots, const uint32_t *__restrict__ ids, const bq_box3f *__restrict__ boxes)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   const bool in = t < numSlots;
   uint32_t q = 0;
@@ -233,6 +241,7 @@ __global__ void k_rb_newkeys(const RebinJob *__restrict__ jobs, const uint32_t *
                              const bq_box3f *__restrict__ boxes, bool atDepthCap, uint64_t *__restrict__ kk,
                              uint32_t *__restrict__ vv)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numSlots) return;
   const uint32_t q = job_of(jobOff, numJobs, t);
@@ -255,6 +264,7 @@ __global__ void k_rb_writeback(const RebinJob *__restrict__ jobs, const uint32_t
                                uint32_t numSlots, const uint64_t *__restrict__ kk, const uint32_t *__restrict__ vv,
                                uint32_t *__restrict__ keys, uint32_t *__restrict__ ids)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numSlots) return;
   const uint64_t k = kk[t];
@@ -268,6 +278,7 @@ __global__ void k_rb_newlevels(const RebinJob *__restrict__ jobs, const uint32_t
                                uint32_t numJobs, uint32_t numSlots, const uint32_t *__restrict__ keys, int depth,
                                uint16_t *__restrict__ lev)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numSlots) return;
   const uint32_t q = job_of(jobOff, numJobs, t);
@@ -297,6 +308,7 @@ __device__ __forceinline__ uint32_t run_size_at(const uint16_t *__restrict__ lev
 __global__ void k_rb_detect(const uint16_t *__restrict__ lev, const uint32_t *nvPtr, uint32_t bigMin,
                             uint32_t *numBig)
 {
+  griddep_wait();
   const uint32_t nv = *nvPtr;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
@@ -397,6 +409,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rb_find_runs(const uint32_t *nvPtr
                                                            const uint16_t *__restrict__ lev, uint2 *__restrict__ list,
                                                            uint32_t *listCount)
 {
+  griddep_wait();
   const uint32_t nv = *nvPtr;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint64_t warpBase = ((uint64_t)blockIdx.x * (RT_BLOCK / 32) + warp) * (RT_ITEMS * 32);
@@ -426,6 +439,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rb_thread(const uint2 *__restrict_
                                                         uint32_t *__restrict__ ids, uint16_t *__restrict__ lev,
                                                         uint8_t *__restrict__ forced, uint32_t *numForced)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= min(*listCount, listCap)) return;
   const uint2 r = list[t];
@@ -438,6 +452,7 @@ __global__ void __launch_bounds__(RT_BLOCK) k_rb_thread(const uint2 *__restrict_
 __global__ void k_rb_kept(const uint2 *__restrict__ ranges, const uint8_t *__restrict__ forced, const uint32_t *nvPtr,
                           int thr, uint32_t *__restrict__ kept)
 {
+  griddep_wait();
   const uint32_t nv = *nvPtr;
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x + 1;  // split positions 1..nv-1
   if (s >= nv) return;
@@ -458,6 +473,7 @@ __global__ void k_rb_collapse(const Node *__restrict__ full, const uint2 *__rest
                               const uint8_t *__restrict__ forced, const uint32_t *nvPtr, int thr,
                               Node *__restrict__ out)
 {
+  griddep_wait();
   const uint32_t nv = *nvPtr;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) {
@@ -540,9 +556,10 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   int32_t *bounds = (int32_t *)(ctl + 2);
   {
     ProfScope ps("rebin.keys", al.s, 5);
-    k_rb_valid<<<std::min(div_up(n, 256), num_sms() * 8), 256, 0, al.s>>>(boxes, n, valid, bounds);
+    launch_pdl(k_rb_valid, dim3(std::min(div_up(n, 256), num_sms() * 8)), dim3(256), 0, al.s, boxes, n, valid,
+               bounds);
     if ((s = exclusive_scan_u32(valid, vpos, n, nullptr, nvDev, al)) != BQ_OK) return fail(s);
-    k_rb_keys<<<div_up(n, 256), 256, 0, al.s>>>(boxes, n, valid, vpos, bounds, keysA, idsA);
+    launch_pdl(k_rb_keys, dim3(div_up(n, 256)), dim3(256), 0, al.s, boxes, n, valid, vpos, bounds, keysA, idsA);
   }
   uint32_t *keys2[2] = {keysA, keysB};
   uint32_t *ids2[2] = {idsA, idsB};
@@ -557,7 +574,7 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   }
   {
     ProfScope ps("rebin.levels", al.s);
-    k_rb_levels0<<<div_up(n, 256), 256, 0, al.s>>>(keys, nvDev, lev);
+    launch_pdl(k_rb_levels0, dim3(div_up(n, 256)), dim3(256), 0, al.s, keys, nvDev, lev);
   }
   // ---- broad-phase rebinning ----
   uint32_t *flag = nullptr, *runIdx = nullptr, *starts = nullptr, *big = nullptr, *bigSize = nullptr;
@@ -571,7 +588,7 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     if ((ce = cudaMemsetAsync(ctl + 9, 0, 4, al.s)) != cudaSuccess) return fail(cuda_error(ce, "memset"));
     {
       ProfScope ps("rebin.detect", al.s);
-      k_rb_detect<<<div_up(n, 256), 256, 0, al.s>>>(lev, nvDev, bigMin, ctl + 9);
+      launch_pdl(k_rb_detect, dim3(div_up(n, 256)), dim3(256), 0, al.s, lev, nvDev, bigMin, ctl + 9);
     }
     uint32_t h[10];
     if ((ce = cudaMemcpyAsync(h, ctl, sizeof(h), cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
@@ -599,10 +616,10 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     }
     {
       ProfScope ps("rebin.runs", al.s, 12);
-      k_rb_run_flags<<<div_up(n, 256), 256, 0, al.s>>>(lev, nvDev, flag);
+      launch_pdl(k_rb_run_flags, dim3(div_up(n, 256)), dim3(256), 0, al.s, lev, nvDev, flag);
       if ((s = exclusive_scan_u32(flag, runIdx, n, nvDev, ctl + 8, al)) != BQ_OK) return fail(s);
-      k_rb_run_starts<<<div_up(n, 256), 256, 0, al.s>>>(flag, runIdx, nvDev, starts);
-      k_rb_big<<<div_up(n, 256), 256, 0, al.s>>>(starts, ctl + 8, bigMin, big, bigSize);
+      launch_pdl(k_rb_run_starts, dim3(div_up(n, 256)), dim3(256), 0, al.s, flag, runIdx, nvDev, starts);
+      launch_pdl(k_rb_big, dim3(div_up(n, 256)), dim3(256), 0, al.s, starts, ctl + 8, bigMin, big, bigSize);
       if ((s = exclusive_scan_u32(big, bigRank, n, ctl + 8, ctl + 9, al)) != BQ_OK) return fail(s);
       if ((s = exclusive_scan_u32(bigSize, bigOff, n, ctl + 8, ctl + 10, al)) != BQ_OK) return fail(s);
     }
@@ -614,17 +631,21 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     const int next = depth + 1;
     const bool cap = next >= REBIN_MAX_DEPTH;
     ProfScope ps2("rebin.rebin", al.s, 5);
-    k_rb_jobs<<<div_up(n, 256), 256, 0, al.s>>>(starts, ctl + 8, big, bigRank, bigOff, jobs, jobOff);
-    k_rb_domains<<<div_up(numSlots, 256), 256, 0, al.s>>>(jobs, jobOff, numJobs, numSlots, ids, boxes);
-    k_rb_newkeys<<<div_up(numSlots, 256), 256, 0, al.s>>>(jobs, jobOff, numJobs, numSlots, ids, boxes, cap, kk[0],
-                                                          vv[0]);
+    launch_pdl(k_rb_jobs, dim3(div_up(n, 256)), dim3(256), 0, al.s, starts, ctl + 8, big, bigRank, bigOff, jobs,
+               jobOff);
+    launch_pdl(k_rb_domains, dim3(div_up(numSlots, 256)), dim3(256), 0, al.s, jobs, jobOff, numJobs, numSlots, ids,
+               boxes);
+    launch_pdl(k_rb_newkeys, dim3(div_up(numSlots, 256)), dim3(256), 0, al.s, jobs, jobOff, numJobs, numSlots, ids,
+               boxes, cap, kk[0], vv[0]);
     int jobBits = 0;
     while (jobBits < 32 && (numJobs - 1) >> jobBits) jobBits++;
     int ksel = 0;
     if ((s = onesweep_sort_u64(kk, vv, numSlots, nullptr, 0, 32 + jobBits, nullptr, &ksel, ctl + 1, al)) != BQ_OK)
       return fail(s);
-    k_rb_writeback<<<div_up(numSlots, 256), 256, 0, al.s>>>(jobs, jobOff, numSlots, kk[ksel], vv[ksel], keys, ids);
-    k_rb_newlevels<<<div_up(numSlots, 256), 256, 0, al.s>>>(jobs, jobOff, numJobs, numSlots, keys, next, lev);
+    launch_pdl(k_rb_writeback, dim3(div_up(numSlots, 256)), dim3(256), 0, al.s, jobs, jobOff, numSlots, kk[ksel],
+               vv[ksel], keys, ids);
+    launch_pdl(k_rb_newlevels, dim3(div_up(numSlots, 256)), dim3(256), 0, al.s, jobs, jobOff, numJobs, numSlots, keys,
+               next, lev);
     if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "rebin"));
   }
   if (hnv == 0) {
@@ -640,9 +661,10 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     uint2 *list = nullptr;
     if ((s = tmp.get(&list, listCap)) != BQ_OK) return fail(s);
     if ((ce = cudaMemsetAsync(ctl + 12, 0, 4, al.s)) != cudaSuccess) return fail(cuda_error(ce, "memset"));
-    k_rb_find_runs<<<div_up(hnv, RT_BLOCK * RT_ITEMS), RT_BLOCK, 0, al.s>>>(nvDev, thr, lev, list, ctl + 12);
-    k_rb_thread<<<div_up(listCap, RT_BLOCK), RT_BLOCK, 0, al.s>>>(list, ctl + 12, listCap, thr, boxes, ids, lev,
-                                                                 forced, ctl + 11);
+    launch_pdl(k_rb_find_runs, dim3(div_up(hnv, RT_BLOCK * RT_ITEMS)), dim3(RT_BLOCK), 0, al.s, nvDev, thr, lev, list,
+               ctl + 12);
+    launch_pdl(k_rb_thread, dim3(div_up(listCap, RT_BLOCK)), dim3(RT_BLOCK), 0, al.s, list, ctl + 12, listCap, thr,
+               boxes, ids, lev, forced, ctl + 11);
   }
   uint2 *pending = nullptr;
   if ((s = tmp.get(&pending, 2ull * div_up(hnv, AGG_CHUNK))) != BQ_OK) return fail(s);
@@ -685,7 +707,7 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
     return fail(cuda_error(ce, "memset"));
   {
     ProfScope ps("rebin.collapse", al.s, 4);
-    k_rb_kept<<<div_up(hnv, 256), 256, 0, al.s>>>(ranges, forced, nvDev, thr, kept);
+    launch_pdl(k_rb_kept, dim3(div_up(hnv, 256)), dim3(256), 0, al.s, ranges, forced, nvDev, thr, kept);
     if ((s = exclusive_scan_u32(kept, rank, hnv > 1 ? hnv - 1 : 1, nullptr, ctl + 9, al)) != BQ_OK) return fail(s);
   }
   uint32_t hk[2];
@@ -696,7 +718,8 @@ int build_rebin_morton30(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   // (then no split is kept); otherwise every kept split owns a node pair
   const uint64_t numNodes = 2ull + 2ull * hk[1];
   if ((s = al.get(&nodes, numNodes)) != BQ_OK) return fail(s);
-  k_rb_collapse<<<div_up(hnv, 256), 256, 0, al.s>>>(full, ranges, kept, rank, forced, nvDev, thr, nodes);
+  launch_pdl(k_rb_collapse, dim3(div_up(hnv, 256)), dim3(256), 0, al.s, full, ranges, kept, rank, forced, nvDev, thr,
+             nodes);
   if ((ce = cudaGetLastError()) != cudaSuccess) return fail(cuda_error(ce, "k_rb_collapse"));
   bvh->nodes = reinterpret_cast<bq_node3f *>(nodes);
   bvh->numNodes = (uint32_t)numNodes;

@@ -330,6 +330,7 @@ __device__ __forceinline__ void node_bounds(const SahNode &nd, float lo[3], floa
 // ------------------------------------------------------------------
 __global__ void k_sah_valid(const bq_box3f *__restrict__ boxes, uint32_t n, uint32_t *__restrict__ valid)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   valid[i] = (boxes[i].lower[0] <= boxes[i].upper[0]) ? 1u : 0u;  // initPrims (:139)
@@ -340,6 +341,7 @@ __global__ void __launch_bounds__(256) k_sah_init(const bq_box3f *__restrict__ b
                                                   SahPrim *__restrict__ recs, uint32_t *__restrict__ primIDs,
                                                   int32_t *rootLoHi)
 {
+  griddep_wait();
   const uint32_t nv = *nvPtr;
   int32_t lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -400,6 +402,7 @@ __device__ __forceinline__ TileInfo tile_info(const SahNode *__restrict__ nodes,
 __global__ void k_sah_tiles(const SahNode *__restrict__ nodes, SahCtl *ctl, int cur, uint32_t cap,
                             uint32_t *__restrict__ tileCount, int32_t *__restrict__ nodeBins)
 {
+  griddep_wait();
   const uint32_t K = ctl->bigCount[cur];
   const uint32_t k = blockIdx.x;
   if (k == 0 && threadIdx.x == 0 && K > cap) atomicOr(&ctl->err, DEV_ERR_RANGE);
@@ -416,6 +419,7 @@ __global__ void __launch_bounds__(SAH_BLOCK) k_sah_bin(const SahNode *__restrict
                                                        const SahPrim *__restrict__ buf1,
                                                        uint32_t *__restrict__ tileCnt, int32_t *__restrict__ nodeBins)
 {
+  griddep_wait();
   constexpr int WARPS = SAH_BLOCK / 32;
   __shared__ int32_t sBins[WARPS][SAH_NB * SAH_W];
   const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
@@ -456,6 +460,7 @@ __global__ void k_sah_decide(const SahNode *__restrict__ nodes, const SahCtl *ct
                              const SahPrim *__restrict__ buf0, const SahPrim *__restrict__ buf1,
                              Node *__restrict__ out, uint32_t *__restrict__ primIDs)
 {
+  griddep_wait();
   const uint32_t K = min(ctl->bigCount[cur], cap);
   const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -485,6 +490,7 @@ __global__ void __launch_bounds__(BQ_SCAN_THREADS) k_sah_tiles_scan(SahCtl *ctl,
                                                                     const uint32_t *__restrict__ tileCount,
                                                                     uint32_t *__restrict__ first)
 {
+  griddep_wait();
   extern __shared__ uint32_t sVal[];  // cap entries
   __shared__ uint32_t sWarp[33];
   const uint32_t K = min(ctl->bigCount[cur], cap);
@@ -555,6 +561,7 @@ __global__ void __launch_bounds__(BQ_SCAN_THREADS) k_sah_right_children(const Sa
                                                                         uint32_t *__restrict__ used,
                                                                         SahNode *__restrict__ next)
 {
+  griddep_wait();
   extern __shared__ uint32_t sScan[];  // numTiles + 1 entries
   __shared__ uint32_t sWarp[33];
   const uint32_t K = min(ctl->bigCount[cur], cap), T = ctl->numTiles;
@@ -576,6 +583,7 @@ __global__ void k_sah_tile_right(const SahNode *__restrict__ nodes, const uint32
                                  int cur, uint32_t maxTiles, const SahDec *__restrict__ decs,
                                  const uint32_t *__restrict__ tileCnt, uint32_t *__restrict__ tileRight)
 {
+  griddep_wait();
   const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) {
@@ -593,6 +601,7 @@ __global__ void k_sah_children(const SahNode *__restrict__ nodes, const SahCtl *
                                const SahDec *__restrict__ decs, Node *__restrict__ out, uint32_t *__restrict__ used,
                                SahNode *__restrict__ next, uint32_t *err)
 {
+  griddep_wait();
   const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K || k >= cap) return;
@@ -606,6 +615,7 @@ __global__ void __launch_bounds__(SAH_BLOCK) k_sah_scatter(const SahNode *__rest
                                                            const SahDec *__restrict__ decs, SahPrim *buf0,
                                                            SahPrim *buf1, SahNode *next)
 {
+  griddep_wait();
   __shared__ uint32_t sWarp[SAH_BLOCK / 32];
   __shared__ int32_t sRed[12][SAH_BLOCK / 32];
   const uint32_t K = ctl->bigCount[cur], T = ctl->numTiles;
@@ -896,6 +906,7 @@ __global__ void __launch_bounds__(SAHW_BLOCK) k_sah_warp(const SahNode *__restri
                                                          Node *__restrict__ out, uint32_t *__restrict__ primIDs,
                                                          uint32_t *__restrict__ used)
 {
+  griddep_wait();
   __shared__ SahNode sStack[SAHW_WARPS][SAHW_STACK];
   __shared__ int32_t sBins[SAHW_WARPS][SAH_NB * SAH_W];
   __shared__ SahPrim sX[SAHW_WARPS][32];
@@ -916,6 +927,7 @@ __global__ void k_sah_classify(const SahNode *__restrict__ next, SahCtl *ctl, in
                                uint32_t warpMax, SahNode *__restrict__ bigNext, SahNode *__restrict__ tasks,
                                uint32_t taskCap)
 {
+  griddep_wait();
   const uint32_t K = min(ctl->bigCount[cur], cap);
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= 2 * K) return;
@@ -947,6 +959,7 @@ __device__ __forceinline__ Node sah_remap(const Node &c, const uint32_t *__restr
 __global__ void k_sah_compact(const Node *__restrict__ full, const uint32_t *__restrict__ used,
                               const uint32_t *__restrict__ rank, uint32_t nv, Node *__restrict__ out)
 {
+  griddep_wait();
   const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m == 0) {
     out[0] = sah_remap(full[0], rank);
@@ -999,10 +1012,10 @@ int build_elh(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
     return fail(cuda_error(ce, "sah set-up"));
   {
     ProfScope ps(HEUR ? "elh.setup" : "sah.setup", al.s, 5);
-    k_sah_valid<<<div_up(n, 256), 256, 0, al.s>>>(boxes, n, valid);
+    launch_pdl(k_sah_valid, dim3(div_up(n, 256)), dim3(256), 0, al.s, boxes, n, valid);
     if ((s = exclusive_scan_u32(valid, vpos, n, nullptr, ctl, al)) != BQ_OK) return fail(s);
-    k_sah_init<<<std::min(div_up(n, 256), num_sms() * 8), 256, 0, al.s>>>(boxes, n, vpos, ctl, buf0, primIDs,
-                                                                        (int32_t *)(ctl + 2));
+    launch_pdl(k_sah_init, dim3(std::min(div_up(n, 256), num_sms() * 8)), dim3(256), 0, al.s, boxes, n, vpos, ctl,
+               buf0, primIDs, (int32_t *)(ctl + 2));
   }
   int32_t hctl[8];
   if ((ce = cudaMemcpyAsync(hctl, ctl, 32, cudaMemcpyDeviceToHost, al.s)) != cudaSuccess ||
@@ -1065,7 +1078,8 @@ int build_elh(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
   }
   auto warp_phase = [&]() -> int {
     ProfScope ps(HEUR ? "elh.warps" : "sah.warps", al.s);
-    k_sah_warp<<<warpGrid, SAHW_BLOCK, 0, al.s>>>(tasks, sc, taskCap, thr, buf0, buf1, full, primIDs, used);
+    launch_pdl(k_sah_warp, dim3(warpGrid), dim3(SAHW_BLOCK), 0, al.s, tasks, sc, taskCap, thr, buf0, buf1, full,
+               primIDs, used);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemsetAsync(&sc->taskCount, 0, 2 * sizeof(uint32_t), al.s);  // taskCount, grab
     return e == cudaSuccess ? BQ_OK : cuda_error(e, "k_sah_warp");
@@ -1074,32 +1088,32 @@ int build_elh(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
   for (int level = 0; rootBig; level++) {
     {
       ProfScope ps(HEUR ? "elh.level" : "sah.level", al.s, fused ? 7 : 12);
-      k_sah_tiles<<<cap, 128, 0, al.s>>>(bigList[cur], sc, cur, cap, tileCount, nodeBins);
+      launch_pdl(k_sah_tiles, dim3(cap), dim3(128), 0, al.s, bigList[cur], sc, cur, cap, tileCount, nodeBins);
       if (fused) {
-        k_sah_tiles_scan<<<1, BQ_SCAN_THREADS, sizeof(uint32_t) * cap, al.s>>>(sc, cur, cap, maxTiles, tileCount,
-                                                                             first);
+        launch_pdl(k_sah_tiles_scan, dim3(1), dim3(BQ_SCAN_THREADS), sizeof(uint32_t) * cap, al.s, sc, cur, cap,
+                   maxTiles, tileCount, first);
       } else if ((s = exclusive_scan_u32(tileCount, first, cap, &sc->bigCount[cur], &sc->numTiles, al)) != BQ_OK) {
         return fail(s);
       }
-      k_sah_bin<<<maxTiles, SAH_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, buf0, buf1, tileCnt,
-                                                  nodeBins);
-      k_sah_decide<<<div_up(cap, 4), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, thr, nodeBins, decs, buf0, buf1,
-                                                    full, primIDs);
+      launch_pdl(k_sah_bin, dim3(maxTiles), dim3(SAH_BLOCK), 0, al.s, bigList[cur], first, sc, cur, maxTiles, buf0,
+                 buf1, tileCnt, nodeBins);
+      launch_pdl(k_sah_decide, dim3(div_up(cap, 4)), dim3(128), 0, al.s, bigList[cur], sc, cur, cap, thr, nodeBins,
+                 decs, buf0, buf1, full, primIDs);
       if (fused) {
-        k_sah_right_children<<<1, BQ_SCAN_THREADS, sizeof(uint32_t) * maxTiles, al.s>>>(
-            bigList[cur], first, sc, cur, cap, decs, tileCnt, tileRight, full, used, next);
+        launch_pdl(k_sah_right_children, dim3(1), dim3(BQ_SCAN_THREADS), sizeof(uint32_t) * maxTiles, al.s,
+                   bigList[cur], first, sc, cur, cap, decs, tileCnt, tileRight, full, used, next);
       } else {
-        k_sah_tile_right<<<div_up(maxTiles, 128), 128, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, decs,
-                                                                  tileCnt, tileRight);
+        launch_pdl(k_sah_tile_right, dim3(div_up(maxTiles, 128)), dim3(128), 0, al.s, bigList[cur], first, sc, cur,
+                   maxTiles, decs, tileCnt, tileRight);
         if ((s = exclusive_scan_u32(tileRight, tileRight, maxTiles, &sc->scanLen, nullptr, al)) != BQ_OK)
           return fail(s);
-        k_sah_children<<<div_up(cap, 128), 128, 0, al.s>>>(bigList[cur], sc, cur, cap, first, tileRight, decs, full,
-                                                           used, next, &sc->err);
+        launch_pdl(k_sah_children, dim3(div_up(cap, 128)), dim3(128), 0, al.s, bigList[cur], sc, cur, cap, first,
+                   tileRight, decs, full, used, next, &sc->err);
       }
-      k_sah_scatter<<<maxTiles, SAH_BLOCK, 0, al.s>>>(bigList[cur], first, sc, cur, maxTiles, tileRight, decs, buf0,
-                                                      buf1, next);
-      k_sah_classify<<<div_up(2ull * cap, 128), 128, 0, al.s>>>(next, sc, cur, cap, thr, warpMax, bigList[cur ^ 1],
-                                                                tasks, taskCap);
+      launch_pdl(k_sah_scatter, dim3(maxTiles), dim3(SAH_BLOCK), 0, al.s, bigList[cur], first, sc, cur, maxTiles,
+                 tileRight, decs, buf0, buf1, next);
+      launch_pdl(k_sah_classify, dim3(div_up(2ull * cap, 128)), dim3(128), 0, al.s, next, sc, cur, cap, thr, warpMax,
+                 bigList[cur ^ 1], tasks, taskCap);
       if ((ce = cudaMemsetAsync(&sc->bigCount[cur], 0, sizeof(uint32_t), al.s)) != cudaSuccess ||
           (ce = cudaGetLastError()) != cudaSuccess)
         return fail(cuda_error(ce, "sah level"));
@@ -1133,7 +1147,7 @@ int build_elh(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const bq_build_c
   if ((s = al.get(&nodes, numNodes)) != BQ_OK) return fail(s);
   {
     ProfScope ps(HEUR ? "elh.compact" : "sah.compact", al.s);
-    k_sah_compact<<<div_up(nv, 256), 256, 0, al.s>>>(full, used, rank, nv, nodes);
+    launch_pdl(k_sah_compact, dim3(div_up(nv, 256)), dim3(256), 0, al.s, full, used, rank, nv, nodes);
   }
   bvh->nodes = reinterpret_cast<bq_node3f *>(nodes);
   bvh->numNodes = numNodes;

@@ -43,6 +43,7 @@ constexpr uint32_t WC_MAX_DEPTH = 1u << 16;
 __global__ void k_wc_parent(const Node *__restrict__ nodes, uint32_t numNodes, uint32_t *__restrict__ parent,
                             uint32_t *err)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= numNodes || i == 1) return;  // node 1 is unused
   const uint64_t admin = node_admin(ldg_node(nodes + i));
@@ -60,6 +61,7 @@ __global__ void k_wc_parent(const Node *__restrict__ nodes, uint32_t numNodes, u
 __global__ void k_wc_flag(const Node *__restrict__ nodes, uint32_t numNodes, const uint32_t *__restrict__ parent,
                           int logW, uint32_t *__restrict__ flag, uint32_t *err)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= numNodes) return;
   uint32_t f = 0;
@@ -86,6 +88,7 @@ __global__ void k_wc_emit(const Node *__restrict__ nodes, uint32_t numNodes, con
                           const uint32_t *__restrict__ wideId, Node *__restrict__ wide, uint32_t numWide,
                           uint32_t *err)
 {
+  griddep_wait();
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= numNodes || !__ldg(flag + i)) return;
   const uint32_t w = __ldg(wideId + i);
@@ -331,6 +334,7 @@ __global__ void __launch_bounds__(128) k_wide_closest(const Node *__restrict__ s
                                                       int32_t *__restrict__ outIds, float *__restrict__ outD,
                                                       uint32_t *__restrict__ ovfList, uint32_t *ovfCount)
 {
+  griddep_wait();
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nq) return;
   const uint32_t qi = order ? __ldg(order + t) : t;
@@ -346,6 +350,7 @@ __global__ void k_wide_closest_deep(const Node *__restrict__ slots, const uint32
                                     int32_t *__restrict__ outIds, float *__restrict__ outD, const uint32_t *ovfList,
                                     const uint32_t *ovfCount, uint64_t *stacks, uint32_t *err)
 {
+  griddep_wait();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t cnt = *ovfCount;
   for (uint32_t w = tid; w < cnt; w += gridDim.x * blockDim.x) {
@@ -366,13 +371,13 @@ void launch_wide_cp(const bq_wide_bvh3f *bvh, const float *points, const float *
   const Node *slots = (const Node *)bvh->nodes;
   {
     ProfScope ps("wide.closest", s);
-    k_wide_closest<W, TIE, STACK><<<div_up(nq, block), block, WIDE_SMEM_STACK * sizeof(uint64_t) * block, s>>>(
-        slots, bvh->primIDs, points, queries, qs.order, nq, maxSqr, ids, d, qs.ovfList, qs.ovfCount);
+    launch_pdl(k_wide_closest<W, TIE, STACK>, dim3(div_up(nq, block)), dim3(block),
+               WIDE_SMEM_STACK * sizeof(uint64_t) * block, s, slots, bvh->primIDs, points, queries, qs.order, nq,
+               maxSqr, ids, d, qs.ovfList, qs.ovfCount);
   }
   ProfScope ps("wide.deep", s);
-  k_wide_closest_deep<W, TIE><<<DEEP_THREADS / 128, 128, 0, s>>>(slots, bvh->primIDs, points, queries, maxSqr, ids,
-                                                                 d, qs.ovfList, qs.ovfCount, (uint64_t *)qs.deep,
-                                                                 qs.err);
+  launch_pdl(k_wide_closest_deep<W, TIE>, dim3(DEEP_THREADS / 128), dim3(128), 0, s, slots, bvh->primIDs, points,
+             queries, maxSqr, ids, d, qs.ovfList, qs.ovfCount, (uint64_t *)qs.deep, qs.err);
 }
 
 template <int W>
@@ -402,7 +407,7 @@ int wide_closest_point(const bq_wide_bvh3f *bvh, int W, const float *points, con
   if (W != 2 && W != 4 && W != 8) return set_error(BQ_ERR_INVALID_ARGUMENT, "width must be 2, 4 or 8");
   if (nq == 0) return BQ_OK;
   if (bvh->numNodes == 0) {
-    k_fill_empty<<<div_up(nq, 256), 256, 0, al.s>>>(nq, 1, ids, d, nullptr);
+    launch_pdl(k_fill_empty, dim3(div_up(nq, 256)), dim3(256), 0, al.s, nq, 1, ids, d, nullptr);
     BQ_CUDA(cudaGetLastError());
     return BQ_OK;
   }
@@ -410,9 +415,9 @@ int wide_closest_point(const bq_wide_bvh3f *bvh, int W, const float *points, con
   float *rootBox = nullptr;
   BQ_TRY(tmp.get(&rootBox, 6));
   const Node *slots = (const Node *)bvh->nodes;
-  if (W == 2) k_wide_root_box<2><<<1, 32, 0, al.s>>>(slots, rootBox);
-  else if (W == 4) k_wide_root_box<4><<<1, 32, 0, al.s>>>(slots, rootBox);
-  else k_wide_root_box<8><<<1, 32, 0, al.s>>>(slots, rootBox);
+  if (W == 2) launch_pdl(k_wide_root_box<2>, dim3(1), dim3(32), 0, al.s, slots, rootBox);
+  else if (W == 4) launch_pdl(k_wide_root_box<4>, dim3(1), dim3(32), 0, al.s, slots, rootBox);
+  else launch_pdl(k_wide_root_box<8>, dim3(1), dim3(32), 0, al.s, slots, rootBox);
   BQ_CUDA(cudaGetLastError());
   QueryScratch qs;
   BQ_TRY(prepare_queries(rootBox, queries, nq, c.reorder != 0, tmp, al, qs));
@@ -446,8 +451,8 @@ int collapse_wide(const bq_bvh3f *bin, int W, bq_wide_bvh3f *out, bool copyPrims
   BQ_CUDA(cudaMemsetAsync(ctl, 0, 8, al.s));
   {
     ProfScope ps("wide.flags", al.s, 2);
-    k_wc_parent<<<div_up(nn, 256), 256, 0, al.s>>>(nodes, nn, parent, ctl + 1);
-    k_wc_flag<<<div_up(nn, 256), 256, 0, al.s>>>(nodes, nn, parent, logW, flag, ctl + 1);
+    launch_pdl(k_wc_parent, dim3(div_up(nn, 256)), dim3(256), 0, al.s, nodes, nn, parent, ctl + 1);
+    launch_pdl(k_wc_flag, dim3(div_up(nn, 256)), dim3(256), 0, al.s, nodes, nn, parent, logW, flag, ctl + 1);
   }
   BQ_CUDA(cudaGetLastError());
   {
@@ -477,9 +482,12 @@ int collapse_wide(const bq_bvh3f *bin, int W, bq_wide_bvh3f *out, bool copyPrims
   }
   {
     ProfScope ps("wide.emit", al.s);
-    if (W == 2) k_wc_emit<2><<<div_up(nn, 256), 256, 0, al.s>>>(nodes, nn, flag, wid, wide, numWide, ctl + 1);
-    else if (W == 4) k_wc_emit<4><<<div_up(nn, 256), 256, 0, al.s>>>(nodes, nn, flag, wid, wide, numWide, ctl + 1);
-    else k_wc_emit<8><<<div_up(nn, 256), 256, 0, al.s>>>(nodes, nn, flag, wid, wide, numWide, ctl + 1);
+    if (W == 2) launch_pdl(k_wc_emit<2>, dim3(div_up(nn, 256)), dim3(256), 0, al.s, nodes, nn, flag, wid, wide,
+                           numWide, ctl + 1);
+    else if (W == 4) launch_pdl(k_wc_emit<4>, dim3(div_up(nn, 256)), dim3(256), 0, al.s, nodes, nn, flag, wid, wide,
+                                numWide, ctl + 1);
+    else launch_pdl(k_wc_emit<8>, dim3(div_up(nn, 256)), dim3(256), 0, al.s, nodes, nn, flag, wid, wide, numWide,
+                    ctl + 1);
   }
   cudaError_t ce = cudaGetLastError();
   if (ce == cudaSuccess) ce = cudaMemcpyAsync(&h[1], ctl + 1, 4, cudaMemcpyDeviceToHost, al.s);

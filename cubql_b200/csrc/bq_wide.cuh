@@ -37,6 +37,7 @@ struct WideLog<8> { enum { value = 3 }; };
 template <int W>
 __global__ void k_wide_root_box(const Node *__restrict__ slots, float *__restrict__ box)
 {
+  griddep_wait();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (int c = 0; c < W; c++) {
