@@ -504,8 +504,9 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
                                    "phases_ms": {k: round(v[1], 4) for k, v in prof.table.items()}}
     tb = bq.cuda.radixBuilder(tbox)
     ms_f = ev_time(lambda: bq.triangles.findClosest(tb, tt, tv, tq))
-    ids, _, _ = bq.triangles.findClosest(tb, tt, tv, tq)
+    ids, dsq, _ = bq.triangles.findClosest(tb, tt, tv, tq)
     ms_b = ev_time(lambda: bq.triangles.distanceBackward(tt, tv, tq, ids, g1))
+    other_trees = tri_forward_other_trees(bq, torch, tbox, tt, tv, tq, ids, dsq, ev_time)
     h = 1e-3
 
     def fd():  # forward + central differences for the query gradient: 7 forwards
@@ -529,7 +530,7 @@ def components(bq, W, torch, pts_np, tp, boxes_t, comp):
                                  "fd_baseline": "forward + central differences of the query coordinates only "
                                                 "(7 forwards); a vertex-gradient FD would need 6 forwards per "
                                                 "vertex, so the ratio is against the cheaper baseline",
-                                 "forward_roofline": fwd_roof,
+                                 "forward_roofline": fwd_roof, **other_trees,
                                  "backward_roofline": dict(hbm_frac(bwd_bytes, ms_b, peak),
                                                            model="pairs kernel 140 B/query + 3 sort passes and a "
                                                                  "histogram of 3Q pairs + reduce 60 B/query + 12 B/vertex")}
@@ -638,6 +639,22 @@ def c1_reference(W, pts_np):
         rc.closest_point(nodes, prims, pts_np[:n1], q1, threads=threads)
         out["reference_cpu_closest_point_ms_allcores"] = (time.perf_counter() - t0) * 1e3
         out["host_threads"] = threads
+    return out
+
+
+def tri_forward_other_trees(bq, torch, tbox, tt, tv, tq, ids, d, timer):
+    """The triangle forward over SAH and spatial-median trees of the same
+    triangle boxes (the benchmark's own tree is the Morton one, as in the
+    reference's timing): time, and whether the answers equal the Morton
+    tree's (under the default lowest-id tie rule they do not depend on the
+    tree)."""
+    out = {}
+    for name, build in (("sah", lambda: bq.cuda.sahBuilder(tbox)), ("spatial_median", lambda: bq.gpuBuilder(tbox))):
+        t = build()
+        out[f"forward_{name}_tree_ms"] = timer(lambda: bq.triangles.findClosest(t, tt, tv, tq))
+        i2, d2, _ = bq.triangles.findClosest(t, tt, tv, tq)
+        out[f"forward_{name}_tree_same_answers"] = bool(torch.equal(i2, ids) and torch.equal(d2, d))
+        t.free()
     return out
 
 
@@ -799,10 +816,15 @@ def run_ours(args):
         verts, tris = W.icosphere(args.mesh_level)
         tv, tt = torch.from_numpy(verts).cuda(), torch.from_numpy(tris).cuda()
         tq = torch.from_numpy(W.uniform_points(args.queries, W.SEED_QUERIES, -1.5, 1.5)).cuda()
-        tb = bq.cuda.radixBuilder(bq.triangles.boxes(tt, tv))
+        tbox = bq.triangles.boxes(tt, tv)
+        tb = bq.cuda.radixBuilder(tbox)
         ms_t = time_loop(lambda: bq.triangles.findClosest(tb, tt, tv, tq), args.steps, args.warmup, world)
+        ids, dsq, _ = bq.triangles.findClosest(tb, tt, tv, tq)
+        other = tri_forward_other_trees(bq, torch, tbox, tt, tv, tq, ids, dsq,
+                                        lambda fn: time_loop(fn, args.steps, args.warmup, world))
         if rank == 0:
-            print(json.dumps({"only_tri": True, "triangles": len(tris), "queries": args.queries, "forward_ms": ms_t}))
+            print(json.dumps({"only_tri": True, "triangles": len(tris), "queries": args.queries, "forward_ms": ms_t,
+                              **other}))
         tb.free()
         return
     if args.only_wide:
