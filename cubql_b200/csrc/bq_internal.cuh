@@ -275,16 +275,15 @@ __device__ __forceinline__ uint32_t quant_cell(float c, float bias, float scale,
   return min(__float2uint_rz(f), maxCell);
 }
 
-// per-build summary written by the bounds pass
+// per-build summary of the Morton build: the centroid bounds, valid count
+// and quantizer (written by block 0 of the key pass) and the device error
+// word (zeroed by the bounds pass)
 struct BuildState {
   int32_t cbLo[3], cbHi[3];  // encoded centroid bounds of valid prims
   uint32_t numValid;
   float bias[3];
   float scale;
-  uint32_t ticket;            // last-block-done counter (self-resetting)
   uint32_t err;               // DEV_ERR_* bits
-  uint32_t numNodes;          // written by the topology pass
-  uint32_t pad[2];
 };
 
 inline int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
