@@ -48,9 +48,9 @@
 #include <vector>
 
 #include "bq_internal.cuh"
+#include "bq_refit.cuh"
 
 namespace bq {
-int refit(const bq_bvh3f *bvh, const bq_box3f *boxes, Alloc &al, bool check);
 
 namespace {
 
@@ -690,20 +690,46 @@ __device__ __forceinline__ Node sm_remap(const Node &c, const uint32_t *__restri
   return make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, make_admin(2ull + 2ull * rank[cm], 0));
 }
 
+// an inner node written at index q is its children's parent
+__device__ __forceinline__ void sm_link_children(const Node &c, uint32_t q, uint32_t *__restrict__ parent)
+{
+  const uint64_t a = node_admin(c);
+  if (admin_count(a)) return;
+  const uint64_t o = admin_offset(a);
+  parent[o] = q;
+  parent[o + 1] = q;
+}
+
+// Also writes what the refit's climb needs, which the generic refit would
+// find with two more passes over the nodes: every node's parent and a zero
+// arrival counter (the climb is k_refit_climb of bq_refit.cuh).
 __global__ void k_sm_compact(const Node *__restrict__ full, const uint32_t *__restrict__ used,
-                             const uint32_t *__restrict__ rank, uint32_t nv, Node *__restrict__ out)
+                             const uint32_t *__restrict__ rank, uint32_t nv, Node *__restrict__ out,
+                             uint32_t *__restrict__ parent, uint32_t *__restrict__ counter, uint32_t *__restrict__ err)
 {
   griddep_wait();
   const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m == 0) {
-    out[0] = sm_remap(full[0], rank);
+    const Node root = sm_remap(full[0], rank);
+    out[0] = root;
     out[1] = make_node(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0);
+    parent[0] = RF_NO_PARENT;
+    parent[1] = RF_NO_PARENT;
+    counter[0] = 0;
+    counter[1] = 0;
+    *err = 0;
+    sm_link_children(root, 0, parent);
     return;
   }
   if (m >= nv || !used[m]) return;
-  const uint64_t pair = 2ull + 2ull * rank[m];
-  out[pair] = sm_remap(full[2ull * m], rank);
-  out[pair + 1] = sm_remap(full[2ull * m + 1], rank);
+  const uint32_t pair = 2u + 2u * rank[m];
+#pragma unroll
+  for (uint32_t side = 0; side < 2; side++) {
+    const Node c = sm_remap(full[2ull * m + side], rank);
+    out[pair + side] = c;
+    counter[pair + side] = 0;
+    sm_link_children(c, pair + side, parent);
+  }
 }
 
 } // namespace
@@ -870,20 +896,29 @@ int build_spatial_median(bq_bvh3f *bvh, const bq_box3f *boxes, uint32_t n, const
   if (hres[0] || herr) return fail(set_error(BQ_ERR_CUDA, "spatial-median build failed a range or capacity check"));
   const uint32_t numNodes = 2 + 2 * hres[1];
   Node *nodes = nullptr;
+  uint32_t *rfParent = nullptr;  // parent[numNodes], counter[numNodes], err[1]
+  if ((s = tmp.get(&rfParent, 2ull * numNodes + 1)) != BQ_OK) return fail(s);
+  uint32_t *rfCounter = rfParent + numNodes, *rfErr = rfParent + 2ull * numNodes;
   if ((s = al.get(&nodes, numNodes)) != BQ_OK) return fail(s);
   {
     ProfScope ps("sm.compact", al.s);
-    launch_pdl(k_sm_compact, dim3(div_up(nv, 256)), dim3(256), 0, al.s, full, used, rank, nv, nodes);
+    launch_pdl(k_sm_compact, dim3(div_up(nv, 256)), dim3(256), 0, al.s, full, used, rank, nv, nodes, rfParent,
+               rfCounter, rfErr);
+  }
+  {
+    // the bottom-up boxes (sm_builder.h:616-693), over the links written above
+    ProfScope ps("refit", al.s);
+    launch_pdl(k_refit_climb, dim3(div_up(numNodes, 128)), dim3(128), 0, al.s, nodes, numNodes, primIDs, n, boxes,
+               rfParent, rfCounter, rfErr);
+  }
+  if ((ce = cudaGetLastError()) != cudaSuccess) {
+    al.free_bytes(nodes);
+    return fail(cuda_error(ce, "spatial median refit"));
   }
   bvh->nodes = reinterpret_cast<bq_node3f *>(nodes);
   bvh->numNodes = numNodes;
   bvh->primIDs = primIDs;
   bvh->numPrims = n;  // sm_builder.h:584: invalid prims stay listed after the valid ones
-  if ((s = refit(bvh, boxes, al, false)) != BQ_OK) {
-    al.free_bytes(nodes);
-    bvh->nodes = nullptr; bvh->numNodes = 0; bvh->primIDs = nullptr; bvh->numPrims = 0;
-    return fail(s);
-  }
   return BQ_OK;
 }
 
